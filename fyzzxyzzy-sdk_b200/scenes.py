@@ -1,0 +1,257 @@
+"""Seeded synthetic rigid-body workloads.
+
+Every workload is produced on the host from a numpy ``Generator(PCG64(seed))``
+and fed identically to the B200 world and to the NativeCpu reference.  The
+record layout is the one both C ABIs consume:
+
+* ``bodies``   (nb, 14) float32: position(3) orientation xyzw(4) linear
+  velocity(3) angular velocity(3) density(1)
+* ``shape_body`` (ns,) uint32: owning dynamic-body index (grouped, ascending)
+* ``shape_type`` (ns,) uint32: 0 = box, 1 = sphere
+* ``shape_geom`` (ns, 4) float32: half extents (box) or radius (sphere)
+* ``shape_local`` (ns, 7) float32: shape pose in the body frame
+* ``shape_mat``  (ns, 3) float32: static friction, dynamic friction, restitution
+* ``joints`` (nj, 2) uint32 and ``joint_dist`` (nj,) float32: centre-anchored
+  distance constraints (``World::add_center_distance_constraint``)
+* ``floor``: static floor height or ``None``.  When present the floor is the
+  first actor (BodyId 0, ShapeId 0), so dynamic body ``i`` is BodyId ``i+1``;
+  ``floor_mat`` is its (static friction, dynamic friction, restitution).
+
+The workloads follow the five benchmark configurations of the rigid-body step
+(plain single scene, plain at scale, batched forward, differentiable rollout,
+batched differentiable at scale); sizes are parameters so tests can run the
+same distributions small.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+import numpy as np
+
+BOX, SPHERE = 0, 1
+
+
+@dataclass
+class SceneSpec:
+    bodies: np.ndarray
+    shape_body: np.ndarray
+    shape_type: np.ndarray
+    shape_geom: np.ndarray
+    shape_local: np.ndarray
+    shape_mat: np.ndarray
+    joints: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.uint32))
+    joint_dist: np.ndarray = field(default_factory=lambda: np.zeros((0,), np.float32))
+    floor: float | None = 0.0
+    floor_mat: tuple = (0.5, 0.5, 0.0)
+
+    @property
+    def n_bodies(self) -> int:
+        return int(self.bodies.shape[0])
+
+    @property
+    def n_shapes(self) -> int:
+        return int(self.shape_body.shape[0])
+
+    @property
+    def n_actors(self) -> int:
+        return self.n_bodies + (1 if self.floor is not None else 0)
+
+    def validate(self) -> "SceneSpec":
+        assert self.bodies.dtype == np.float32 and self.bodies.shape[1] == 14
+        assert self.shape_body.dtype == np.uint32
+        assert np.all(np.diff(self.shape_body.astype(np.int64)) >= 0)
+        assert self.shape_geom.shape == (self.n_shapes, 4)
+        assert self.shape_local.shape == (self.n_shapes, 7)
+        assert self.shape_mat.shape == (self.n_shapes, 3)
+        return self
+
+
+IDENTITY = np.array([0, 0, 0, 0, 0, 0, 1], np.float32)
+
+
+def random_quaternions(rng: np.random.Generator, n: int) -> np.ndarray:
+    """Uniform unit quaternions: normalised 4-vectors of i.i.d. N(0,1)."""
+    q = rng.standard_normal((n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    return q.astype(np.float32)
+
+
+def _assemble(pos, quat, vel, ang, density, shapes, mat_per_body, joints=None,
+              joint_dist=None, floor=0.0) -> SceneSpec:
+    """shapes: list per body of (type, geom4, local7)."""
+    nb = pos.shape[0]
+    bodies = np.zeros((nb, 14), np.float32)
+    bodies[:, 0:3] = pos
+    bodies[:, 3:7] = quat
+    bodies[:, 7:10] = vel
+    bodies[:, 10:13] = ang
+    bodies[:, 13] = density
+    sb, st, sg, sl, sm = [], [], [], [], []
+    for b, lst in enumerate(shapes):
+        for (t, g, l) in lst:
+            sb.append(b); st.append(t); sg.append(g); sl.append(l)
+            sm.append(mat_per_body[b])
+    spec = SceneSpec(
+        bodies=bodies,
+        shape_body=np.asarray(sb, np.uint32),
+        shape_type=np.asarray(st, np.uint32),
+        shape_geom=np.asarray(sg, np.float32).reshape(-1, 4),
+        shape_local=np.asarray(sl, np.float32).reshape(-1, 7),
+        shape_mat=np.asarray(sm, np.float32).reshape(-1, 3),
+        joints=np.zeros((0, 2), np.uint32) if joints is None else np.asarray(joints, np.uint32).reshape(-1, 2),
+        joint_dist=np.zeros((0,), np.float32) if joint_dist is None else np.asarray(joint_dist, np.float32),
+        floor=floor,
+    )
+    return spec.validate()
+
+
+def _box(h):
+    return (BOX, np.array([h[0], h[1], h[2], 0.0], np.float32), IDENTITY)
+
+
+def _sphere(r, local=IDENTITY):
+    return (SPHERE, np.array([r, 0.0, 0.0, 0.0], np.float32), local)
+
+
+def random_boxes(n: int = 1000, seed: int = 0, half=(0.1, 0.5), xz=10.0,
+                 y=(1.0, 21.0), density=1000.0, friction=0.5) -> SceneSpec:
+    """Plain single scene: n random dynamic boxes above a floor at y=0
+    (half extents U[0.1,0.5] per axis, centres x,z in U[-10,10], y in U[1,21],
+    random orientations, zero velocity, density 1000, friction 0.5,
+    restitution 0)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    h = rng.uniform(half[0], half[1], (n, 3)).astype(np.float32)
+    pos = np.stack([rng.uniform(-xz, xz, n), rng.uniform(y[0], y[1], n),
+                    rng.uniform(-xz, xz, n)], 1).astype(np.float32)
+    quat = random_quaternions(rng, n)
+    z = np.zeros((n, 3), np.float32)
+    mats = np.tile(np.array([friction, friction, 0.0], np.float32), (n, 1))
+    return _assemble(pos, quat, z, z, density, [[_box(h[i])] for i in range(n)], mats)
+
+
+def mixed_scale(n: int = 131072, seed: int = 1, region=(200.0, 50.0, 200.0),
+                frac_box=0.7, frac_sphere=0.2, joint_frac=0.02,
+                size=(0.05, 0.3), density=1000.0) -> SceneSpec:
+    """Plain method at scale: 70% boxes, 20% spheres, 10% box+sphere
+    compounds (sphere at a local offset in a 0.5 m cube), random
+    orientations, v0 ~ N(0,1) per axis, friction U[0.3,0.8] per body, and
+    2% of bodies in pairs joined by distance constraints whose rest length is
+    the initial separation.  Bodies fill a 200 x 50 x 200 m region above the
+    floor."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    kind = rng.uniform(0, 1, n)
+    pos = np.stack([rng.uniform(-region[0] / 2, region[0] / 2, n),
+                    rng.uniform(1.0, 1.0 + region[1], n),
+                    rng.uniform(-region[2] / 2, region[2] / 2, n)], 1)
+    n_pairs = int(round(n * joint_frac / 2))
+    perm = rng.permutation(n)[: 2 * n_pairs].reshape(-1, 2)
+    # The partner of each constrained pair starts 0.8-1.5 m from its anchor.
+    d = rng.standard_normal((n_pairs, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    d *= rng.uniform(0.8, 1.5, (n_pairs, 1))
+    pos[perm[:, 1]] = pos[perm[:, 0]] + d
+    pos = pos.astype(np.float32)
+    quat = random_quaternions(rng, n)
+    vel = rng.standard_normal((n, 3)).astype(np.float32)
+    ang = np.zeros((n, 3), np.float32)
+    mu = rng.uniform(0.3, 0.8, n).astype(np.float32)
+    mats = np.stack([mu, mu, np.zeros(n, np.float32)], 1)
+    shapes = []
+    for i in range(n):
+        if kind[i] < frac_box:
+            shapes.append([_box(rng.uniform(size[0], size[1], 3))])
+        elif kind[i] < frac_box + frac_sphere:
+            shapes.append([_sphere(rng.uniform(size[0], size[1]))])
+        else:
+            off = rng.uniform(-0.25, 0.25, 3)
+            local = np.array([off[0], off[1], off[2], 0, 0, 0, 1], np.float32)
+            shapes.append([_box(rng.uniform(size[0], size[1], 3)),
+                           _sphere(rng.uniform(size[0], size[1]), local)])
+    dist = np.linalg.norm(pos[perm[:, 0]] - pos[perm[:, 1]], axis=1).astype(np.float32)
+    return _assemble(pos, quat, vel, ang, density, shapes, mats,
+                     joints=perm.astype(np.uint32), joint_dist=dist)
+
+
+def box_stack_scene(n: int, seed: int, height_range=(5, 20), jitter=1.0e-3,
+                    density=1000.0, friction=0.5) -> SceneSpec:
+    """Towers of unit cubes 5-20 high, resting on the floor, with N(0, 1 mm)
+    placement jitter; towers stand on a 2 m grid."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    hgt = int(rng.integers(height_range[0], height_range[1] + 1))
+    towers = (n + hgt - 1) // hgt
+    side = int(np.ceil(np.sqrt(towers)))
+    pos = np.zeros((n, 3), np.float32)
+    for i in range(n):
+        t, k = divmod(i, hgt)
+        gx, gz = divmod(t, side)
+        pos[i] = (2.0 * gx, 0.5 + 1.0 * k, 2.0 * gz)
+    pos += rng.normal(0.0, jitter, (n, 3)).astype(np.float32)
+    pos[:, 1] = np.maximum(pos[:, 1], 0.5)
+    quat = np.tile(np.array([0, 0, 0, 1], np.float32), (n, 1))
+    z = np.zeros((n, 3), np.float32)
+    mats = np.tile(np.array([friction, friction, 0.0], np.float32), (n, 1))
+    return _assemble(pos, quat, z, z, density,
+                     [[_box((0.5, 0.5, 0.5))] for _ in range(n)], mats)
+
+
+def batched_scenes(n_scenes: int = 4096, low: int = 16, high: int = 512,
+                   base_seed: int = 0) -> list[SceneSpec]:
+    """Batched forward: per-scene body count log-uniform in [low, high];
+    even scenes are random piles (the plain scene scaled so the region side
+    grows as n^(1/3)), odd scenes are unit-cube stacks.  Scene i uses seed
+    base_seed + i and its own floor."""
+    out = []
+    for s in range(n_scenes):
+        rng = np.random.Generator(np.random.PCG64(base_seed + s))
+        n = int(np.exp(rng.uniform(np.log(low), np.log(high + 1))))
+        n = max(low, min(high, n))
+        if s % 2 == 0:
+            scale = (n / 1000.0) ** (1.0 / 3.0)
+            out.append(random_boxes(n, seed=base_seed + s, xz=10.0 * scale,
+                                    y=(1.0, 1.0 + 20.0 * scale)))
+        else:
+            out.append(box_stack_scene(n, seed=base_seed + s))
+    return out
+
+
+def loose_piles(n_scenes: int = 1024, n_boxes: int = 64, base_seed: int = 0) -> list[SceneSpec]:
+    """Differentiable rollout scenes: 64 boxes (half extents U[0.1,0.3]) in a
+    loose pile, v0 and w0 ~ N(0, 0.5), per-body mass log-uniform in [0.5, 5]
+    kg (density = mass / volume), per-scene friction U[0.2, 1.0]."""
+    out = []
+    for s in range(n_scenes):
+        rng = np.random.Generator(np.random.PCG64(base_seed + s))
+        h = rng.uniform(0.1, 0.3, (n_boxes, 3)).astype(np.float32)
+        side = 1.2
+        pos = np.stack([rng.uniform(-side, side, n_boxes),
+                        rng.uniform(0.4, 2.4, n_boxes),
+                        rng.uniform(-side, side, n_boxes)], 1).astype(np.float32)
+        quat = random_quaternions(rng, n_boxes)
+        vel = rng.normal(0, 0.5, (n_boxes, 3)).astype(np.float32)
+        ang = rng.normal(0, 0.5, (n_boxes, 3)).astype(np.float32)
+        mass = np.exp(rng.uniform(np.log(0.5), np.log(5.0), n_boxes))
+        dens = (mass / (8.0 * h.prod(1))).astype(np.float32)
+        mu = np.float32(rng.uniform(0.2, 1.0))
+        mats = np.tile(np.array([mu, mu, 0.0], np.float32), (n_boxes, 1))
+        spec = _assemble(pos, quat, vel, ang, 1.0,
+                         [[_box(h[i])] for i in range(n_boxes)], mats)
+        spec.bodies[:, 13] = dens
+        out.append(spec)
+    return out
+
+
+def mixed_batched(n_scenes: int = 16384, low: int = 8, high: int = 256,
+                  base_seed: int = 0) -> list[SceneSpec]:
+    """Batched and differentiable at scale: per-scene counts log-uniform in
+    [8, 256]; 60% boxes, 25% spheres, 15% compounds, 5% distance pairs,
+    friction U[0.2, 1.0]."""
+    out = []
+    for s in range(n_scenes):
+        rng = np.random.Generator(np.random.PCG64(base_seed + s))
+        n = int(np.exp(rng.uniform(np.log(low), np.log(high + 1))))
+        n = max(low, min(high, n))
+        scale = (n / 1000.0) ** (1.0 / 3.0)
+        out.append(mixed_scale(n, seed=base_seed + s,
+                               region=(20.0 * scale, 20.0 * scale, 20.0 * scale),
+                               frac_box=0.6, frac_sphere=0.25, joint_frac=0.05,
+                               size=(0.05, 0.3)))
+    return out

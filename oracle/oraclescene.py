@@ -1,0 +1,188 @@
+"""Test infrastructure: ctypes access to the C restatement oracle
+(``oracle/_build/liboracle.so``, built by ``oracle/Makefile``).
+
+Only tests, ``smoke()`` and ``bench.py``'s CPU-baseline leg use this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        vp, u32, u64, f32, i32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_float, C.c_int
+        L.fo_error.restype = C.c_char_p
+        L.fo_scene_create.restype = vp
+        L.fo_scene_create.argtypes = [u32, vp, u32, vp, vp, vp, vp, vp, u32, vp, vp, i32, f32, vp]
+        L.fo_scene_destroy.argtypes = [vp]
+        L.fo_scene_step.argtypes = [vp, f32, vp, u64, vp, u64]
+        L.fo_scene_advance_collision.argtypes = [vp]
+        for n in ("fo_scene_counts", "fo_scene_body_states", "fo_scene_set_body_states",
+                  "fo_scene_mass_props", "fo_scene_encoded_bounds"):
+            getattr(L, n).argtypes = [vp, vp]
+        L.fo_scene_pairs.restype = u64
+        L.fo_scene_pairs.argtypes = [vp, i32, vp]
+        L.fo_scene_manifolds.restype = u64
+        L.fo_scene_manifolds.argtypes = [vp, vp, vp, vp, vp]
+        L.fo_scene_partitions.restype = u64
+        L.fo_scene_partitions.argtypes = [vp, vp, vp]
+        L.fo_scene_normal_impulses.restype = u64
+        L.fo_scene_normal_impulses.argtypes = [vp, vp]
+        L.fo_scene_sorted_min_x.restype = u64
+        L.fo_scene_sorted_min_x.argtypes = [vp, vp, vp]
+        L.fo_encode_min.restype = u32
+        L.fo_encode_min.argtypes = [f32]
+        L.fo_encode_max.restype = u32
+        L.fo_encode_max.argtypes = [f32]
+        L.fo_pcm_box_box_candidates.argtypes = [vp, vp, f32, vp, i32, vp]
+        L.fo_pcm_batch_selection.argtypes = [vp, i32, f32, vp]
+        L.fo_pcm_box_box_gjk_epa.argtypes = [vp, vp, f32, vp]
+        L.fo_pcm_sphere_sphere.argtypes = [vp, f32, vp, f32, f32, vp]
+        L.fo_pcm_sphere_plane.argtypes = [vp, f32, f32, f32, vp]
+        L.fo_pcm_sphere_box.argtypes = [vp, f32, vp, f32, vp]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None and a.size else None
+
+
+class OracleScene:
+    def __init__(self, spec):
+        L = lib()
+        self.spec = spec
+        arrs = [np.ascontiguousarray(x) for x in (
+            spec.bodies, spec.shape_body, spec.shape_type, spec.shape_geom,
+            spec.shape_local, spec.shape_mat, spec.joints, spec.joint_dist)]
+        self._keep = arrs
+        self._floor_mat = np.asarray(spec.floor_mat, np.float32)
+        self.h = L.fo_scene_create(spec.n_bodies, _p(arrs[0]), spec.n_shapes, _p(arrs[1]),
+                                   _p(arrs[2]), _p(arrs[3]), _p(arrs[4]), _p(arrs[5]),
+                                   arrs[6].shape[0], _p(arrs[6]), _p(arrs[7]),
+                                   0 if spec.floor is None else 1,
+                                   0.0 if spec.floor is None else float(spec.floor),
+                                   _p(self._floor_mat))
+        if not self.h:
+            raise RuntimeError(L.fo_error().decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fo_scene_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def _check(self, rc):
+        if rc:
+            raise RuntimeError(f"oracle error {rc}: {lib().fo_error().decode()}")
+
+    def step(self, dt: float = 1.0 / 120.0, manager_order=None, joint_order=None):
+        mo = None if manager_order is None else np.ascontiguousarray(manager_order, np.uint64)
+        jo = None if joint_order is None else np.ascontiguousarray(joint_order, np.uint64)
+        rc = lib().fo_scene_step(self.h, dt, None if mo is None else mo.ctypes.data_as(C.c_void_p),
+                                 0 if mo is None else mo.size,
+                                 None if jo is None else jo.ctypes.data_as(C.c_void_p),
+                                 0 if jo is None else jo.size)
+        self._check(rc)
+
+    def advance_collision(self):
+        self._check(lib().fo_scene_advance_collision(self.h))
+
+    def counts(self) -> dict:
+        out = np.zeros(10, np.uint64)
+        lib().fo_scene_counts(self.h, _p(out))
+        keys = ["actors", "shapes", "pairs", "found", "lost", "manifolds",
+                "points", "partitions", "ordered", "tasks"]
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def body_states(self) -> np.ndarray:
+        out = np.zeros((self.counts()["actors"], 14), np.float32)
+        lib().fo_scene_body_states(self.h, _p(out))
+        return out
+
+    def set_body_states(self, st: np.ndarray):
+        st = np.ascontiguousarray(st, np.float32)
+        lib().fo_scene_set_body_states(self.h, _p(st))
+
+    def mass_props(self) -> np.ndarray:
+        out = np.zeros((self.counts()["actors"], 11), np.float32)
+        lib().fo_scene_mass_props(self.h, _p(out))
+        return out
+
+    def encoded_bounds(self) -> np.ndarray:
+        out = np.zeros((self.counts()["shapes"], 6), np.uint32)
+        lib().fo_scene_encoded_bounds(self.h, _p(out))
+        return out
+
+    def pairs(self, which: int = 0) -> np.ndarray:
+        n = lib().fo_scene_pairs(self.h, which, None)
+        out = np.zeros((n, 2), np.uint32)
+        lib().fo_scene_pairs(self.h, which, _p(out))
+        return out
+
+    def manifolds(self):
+        n = lib().fo_scene_manifolds(self.h, None, None, None, None)
+        pairs = np.zeros((n, 2), np.uint32)
+        counts = np.zeros(n, np.uint32)
+        rev = np.zeros(n, np.uint32)
+        pts = np.zeros((n, 4, 7), np.float32)
+        lib().fo_scene_manifolds(self.h, _p(pairs), _p(counts), _p(rev), _p(pts))
+        return pairs, counts, rev, pts
+
+    def partitions(self):
+        c = self.counts()
+        d = np.zeros((c["ordered"], 4), np.uint32)
+        e = np.zeros(c["partitions"], np.uint64)
+        lib().fo_scene_partitions(self.h, _p(d), _p(e))
+        return d, e
+
+    def normal_impulses(self) -> np.ndarray:
+        n = lib().fo_scene_normal_impulses(self.h, None)
+        out = np.zeros(n, np.float64)
+        lib().fo_scene_normal_impulses(self.h, _p(out))
+        return out
+
+    def sorted_min_x(self):
+        n = lib().fo_scene_sorted_min_x(self.h, None, None)
+        v = np.zeros(n, np.uint32); i = np.zeros(n, np.uint32)
+        lib().fo_scene_sorted_min_x(self.h, _p(v), _p(i))
+        return v, i
+
+
+def pcm_box_box_candidates(a, b, cd):
+    out = np.zeros((64, 10), np.float32)
+    cnt = np.zeros(1, np.int32)
+    ok = lib().fo_pcm_box_box_candidates(_p(np.asarray(a, np.float32)), _p(np.asarray(b, np.float32)),
+                                         cd, _p(out), 64, _p(cnt))
+    if ok < 0:
+        raise RuntimeError("oracle candidate overflow")
+    return bool(ok), out[: int(cnt[0])]
+
+
+def pcm_batch_selection(cands):
+    out = np.zeros(4, np.uint8)
+    c = np.ascontiguousarray(cands, np.float32)
+    lib().fo_pcm_batch_selection(_p(c), c.shape[0], 1.0, _p(out))
+    return out
+
+
+def pcm_box_box_gjk_epa(a, b, cd):
+    out = np.zeros(10, np.float32)
+    ok = lib().fo_pcm_box_box_gjk_epa(_p(np.asarray(a, np.float32)), _p(np.asarray(b, np.float32)), cd, _p(out))
+    return bool(ok), out

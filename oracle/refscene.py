@@ -1,0 +1,222 @@
+"""Test infrastructure: ctypes access to the reference SDK's NativeCpu scene.
+
+Loads ``oracle/_ref/libfyzz_ref.so`` (built by ``oracle/Makefile`` from the
+reference sources plus ``ref_harness.cpp``).  Only tests, ``smoke()`` and the
+CPU-baseline leg of ``bench.py`` use this module; the product never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libfyzz_ref.so")
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise RuntimeError(f"reference harness not built: {LIB_PATH}")
+        L = C.CDLL(LIB_PATH)
+        vp, u32, u64, f32, i32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_float, C.c_int
+        P = C.POINTER
+        L.fz_ref_error.restype = C.c_char_p
+        L.fz_ref_create.restype = vp
+        L.fz_ref_create.argtypes = [i32]
+        L.fz_ref_destroy.argtypes = [vp]
+        L.fz_ref_build.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, vp, u32, vp, vp, i32, f32, vp]
+        L.fz_ref_step.argtypes = [vp, f32, i32]
+        L.fz_ref_advance_collision.argtypes = [vp]
+        L.fz_ref_counts.argtypes = [vp, vp]
+        L.fz_ref_body_states.argtypes = [vp, vp]
+        L.fz_ref_mass_props.argtypes = [vp, vp]
+        L.fz_ref_encoded_bounds.argtypes = [vp, vp]
+        for name in ("fz_ref_endpoints",):
+            getattr(L, name).restype = u64
+        L.fz_ref_endpoints.argtypes = [vp, i32, vp, vp, vp]
+        L.fz_ref_pairs.restype = u64
+        L.fz_ref_pairs.argtypes = [vp, i32, vp]
+        L.fz_ref_manifolds.restype = u64
+        L.fz_ref_manifolds.argtypes = [vp, vp, vp, vp, vp]
+        L.fz_ref_manager_order.restype = u64
+        L.fz_ref_manager_order.argtypes = [vp, vp]
+        L.fz_ref_joint_order.restype = u64
+        L.fz_ref_joint_order.argtypes = [vp, vp]
+        L.fz_ref_partitions.restype = u64
+        L.fz_ref_partitions.argtypes = [vp, vp, vp]
+        L.fz_ref_normal_impulses.restype = u64
+        L.fz_ref_normal_impulses.argtypes = [vp, vp]
+        L.fz_ref_contact_events.restype = u64
+        L.fz_ref_contact_events.argtypes = [vp, vp, vp]
+        L.fz_ref_pcm_box_box_candidates.argtypes = [vp, vp, f32, vp, vp]
+        L.fz_ref_pcm_batch_selection.argtypes = [vp, u32, vp]
+        L.fz_ref_pcm_box_box_gjk_epa.argtypes = [vp, vp, f32, vp]
+        L.fz_ref_pcm_sphere_sphere.argtypes = [vp, f32, vp, f32, f32, vp]
+        L.fz_ref_pcm_sphere_box.argtypes = [vp, f32, vp, f32, vp]
+        L.fz_ref_step_many.argtypes = [P(vp), u32, f32, i32, i32]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None and a.size else None
+
+
+class RefScene:
+    """One reference NativeCpu scene built from a SceneSpec."""
+
+    def __init__(self, spec, contact_notifications: bool = False):
+        L = lib()
+        self.spec = spec
+        self.h = L.fz_ref_create(1 if contact_notifications else 0)
+        arrs = [np.ascontiguousarray(x) for x in (
+            spec.bodies, spec.shape_body, spec.shape_type, spec.shape_geom,
+            spec.shape_local, spec.shape_mat, spec.joints, spec.joint_dist)]
+        self._keep = arrs
+        self._floor_mat = np.asarray(spec.floor_mat, np.float32)
+        rc = L.fz_ref_build(self.h, spec.n_bodies, _p(arrs[0]), spec.n_shapes,
+                            _p(arrs[1]), _p(arrs[2]), _p(arrs[3]), _p(arrs[4]),
+                            _p(arrs[5]), arrs[6].shape[0], _p(arrs[6]), _p(arrs[7]),
+                            0 if spec.floor is None else 1,
+                            0.0 if spec.floor is None else float(spec.floor),
+                            _p(self._floor_mat))
+        self._check(rc)
+
+    def _check(self, rc):
+        if rc:
+            raise RuntimeError(f"reference error {rc}: {lib().fz_ref_error().decode()}")
+
+    def close(self):
+        if self.h:
+            lib().fz_ref_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def step(self, dt: float = 1.0 / 120.0, steps: int = 1):
+        self._check(lib().fz_ref_step(self.h, dt, steps))
+
+    def advance_collision(self):
+        self._check(lib().fz_ref_advance_collision(self.h))
+
+    def counts(self) -> dict:
+        out = np.zeros(10, np.uint64)
+        lib().fz_ref_counts(self.h, _p(out))
+        keys = ["actors", "shapes", "pairs", "found", "lost", "manifolds",
+                "points", "partitions", "ordered", "tasks"]
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def body_states(self) -> np.ndarray:
+        n = self.counts()["actors"]
+        out = np.zeros((n, 14), np.float32)
+        lib().fz_ref_body_states(self.h, _p(out))
+        return out
+
+    def mass_props(self) -> np.ndarray:
+        n = self.counts()["actors"]
+        out = np.zeros((n, 11), np.float32)
+        lib().fz_ref_mass_props(self.h, _p(out))
+        return out
+
+    def encoded_bounds(self) -> np.ndarray:
+        n = self.counts()["shapes"]
+        out = np.zeros((n, 6), np.uint32)
+        lib().fz_ref_encoded_bounds(self.h, _p(out))
+        return out
+
+    def endpoints(self, axis: int = 0):
+        n = lib().fz_ref_endpoints(self.h, axis, None, None, None)
+        v = np.zeros(n, np.uint32); i = np.zeros(n, np.uint32); m = np.zeros(n, np.uint8)
+        lib().fz_ref_endpoints(self.h, axis, _p(v), _p(i), _p(m))
+        return v, i, m
+
+    def pairs(self, which: int = 0) -> np.ndarray:
+        n = lib().fz_ref_pairs(self.h, which, None)
+        out = np.zeros((n, 2), np.uint32)
+        lib().fz_ref_pairs(self.h, which, _p(out))
+        return out
+
+    def manifolds(self):
+        n = lib().fz_ref_manifolds(self.h, None, None, None, None)
+        pairs = np.zeros((n, 2), np.uint32)
+        counts = np.zeros(n, np.uint32)
+        rev = np.zeros(n, np.uint32)
+        pts = np.zeros((n, 4, 7), np.float32)
+        lib().fz_ref_manifolds(self.h, _p(pairs), _p(counts), _p(rev), _p(pts))
+        return pairs, counts, rev, pts
+
+    def manager_order(self) -> np.ndarray:
+        n = lib().fz_ref_manager_order(self.h, None)
+        out = np.zeros(n, np.uint64)
+        lib().fz_ref_manager_order(self.h, _p(out))
+        return out
+
+    def joint_order(self) -> np.ndarray:
+        n = lib().fz_ref_joint_order(self.h, None)
+        out = np.zeros(n, np.uint64)
+        lib().fz_ref_joint_order(self.h, _p(out))
+        return out
+
+    def partitions(self):
+        c = self.counts()
+        d = np.zeros((c["ordered"], 4), np.uint32)
+        e = np.zeros(c["partitions"], np.uint64)
+        lib().fz_ref_partitions(self.h, _p(d), _p(e))
+        return d, e
+
+    def normal_impulses(self) -> np.ndarray:
+        n = lib().fz_ref_normal_impulses(self.h, None)
+        out = np.zeros(n, np.float64)
+        lib().fz_ref_normal_impulses(self.h, _p(out))
+        return out
+
+    def contact_events(self):
+        n = lib().fz_ref_contact_events(self.h, None, None)
+        ev = np.zeros((n, 7), np.uint32)
+        imp = np.zeros(n, np.float64)
+        lib().fz_ref_contact_events(self.h, _p(ev), _p(imp))
+        return ev, imp
+
+
+def step_many(scenes, dt: float, steps: int, threads: int) -> None:
+    arr = (C.c_void_p * len(scenes))(*[s.h for s in scenes])
+    rc = lib().fz_ref_step_many(arr, len(scenes), dt, steps, threads)
+    if rc:
+        raise RuntimeError(f"reference error {rc}: {lib().fz_ref_error().decode()}")
+
+
+def box_record(h, p, q):
+    return np.array([*h, *p, *q], np.float32)
+
+
+def pcm_box_box_candidates(a, b, cd):
+    out = np.zeros((64, 10), np.float32)
+    cnt = np.zeros(1, np.uint32)
+    ok = lib().fz_ref_pcm_box_box_candidates(_p(a), _p(b), cd, _p(out), _p(cnt))
+    if ok < 0:
+        raise RuntimeError(lib().fz_ref_error().decode())
+    return bool(ok), out[: int(cnt[0])]
+
+
+def pcm_batch_selection(cands):
+    out = np.zeros(4, np.uint8)
+    c = np.ascontiguousarray(cands, np.float32)
+    rc = lib().fz_ref_pcm_batch_selection(_p(c), c.shape[0], _p(out))
+    if rc:
+        raise RuntimeError(lib().fz_ref_error().decode())
+    return out
+
+
+def pcm_box_box_gjk_epa(a, b, cd):
+    out = np.zeros(10, np.float32)
+    ok = lib().fz_ref_pcm_box_box_gjk_epa(_p(a), _p(b), cd, _p(out))
+    if ok < 0:
+        raise RuntimeError(lib().fz_ref_error().decode())
+    return bool(ok), out
