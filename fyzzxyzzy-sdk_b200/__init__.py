@@ -1,0 +1,299 @@
+"""B200 rigid-body step: Python mirror of fyzz::World over the C ABI.
+
+The product is ``lib/libfyzz_b200.so`` (CUDA kernels for sm_100a + the C++23
+host engine); this module only binds its ``extern "C"`` entry points
+(``include/fyzz_b200.h``).  There is no CPU fallback: creating a world raises
+when the library or a CUDA device is missing.
+
+Errors follow the reference's exception types (status 1 ValueError for
+std::invalid_argument, 2 RuntimeError for std::logic_error, 3 OverflowError
+for std::overflow_error, 4 RuntimeError for std::runtime_error).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libfyzz_b200.so")
+_lib = None
+
+# Every entry point declared in include/fyzz_b200.h.
+EXPORTS = (
+    "fyzz_b200_create", "fyzz_b200_destroy", "fyzz_b200_last_error", "fyzz_b200_error_bits",
+    "fyzz_b200_begin_scene", "fyzz_b200_add_static_floor", "fyzz_b200_create_dynamic_body",
+    "fyzz_b200_attach_box_shape", "fyzz_b200_attach_sphere_shape",
+    "fyzz_b200_update_mass_properties", "fyzz_b200_body_mass_properties",
+    "fyzz_b200_set_shape_material", "fyzz_b200_set_body_velocity",
+    "fyzz_b200_set_body_angular_velocity", "fyzz_b200_add_center_distance_constraint",
+    "fyzz_b200_add_scene", "fyzz_b200_step", "fyzz_b200_step_n", "fyzz_b200_collide",
+    "fyzz_b200_synchronize", "fyzz_b200_body_state", "fyzz_b200_read_bodies",
+    "fyzz_b200_write_velocities", "fyzz_b200_counts", "fyzz_b200_device_view",
+    "fyzz_b200_read_pairs", "fyzz_b200_read_manifolds", "fyzz_b200_read_encoded_bounds",
+    "fyzz_b200_read_sorted_min_x", "fyzz_b200_read_levels",
+)
+
+
+def build() -> str:
+    from importlib import import_module
+    return import_module(__name__ + ".build").build()
+
+
+class BodyState(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("velocity", C.c_float * 3),
+                ("orientation", C.c_float * 4), ("angular_velocity", C.c_float * 3),
+                ("sleeping", C.c_uint32)]
+
+
+class Material(C.Structure):
+    _fields_ = [("static_friction", C.c_float), ("dynamic_friction", C.c_float),
+                ("restitution", C.c_float)]
+
+
+class DeviceView(C.Structure):
+    _fields_ = [("position", C.c_void_p), ("orientation", C.c_void_p),
+                ("velocity", C.c_void_p), ("angular_velocity", C.c_void_p),
+                ("n_bodies", C.c_uint32), ("n_shapes", C.c_uint32), ("stream", C.c_void_p)]
+
+
+def lib():
+    """Load the in-tree library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"B200 library missing: {LIB_PATH} (run build())")
+        L = C.CDLL(LIB_PATH)
+        vp, u32, u64, f32, i32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_float, C.c_int
+        P = C.POINTER
+        L.fyzz_b200_create.argtypes = [i32, P(vp)]
+        L.fyzz_b200_destroy.argtypes = [vp]
+        L.fyzz_b200_last_error.argtypes = [vp]
+        L.fyzz_b200_last_error.restype = C.c_char_p
+        L.fyzz_b200_error_bits.argtypes = [vp, P(u32)]
+        L.fyzz_b200_begin_scene.argtypes = [vp, P(u32)]
+        L.fyzz_b200_add_static_floor.argtypes = [vp, f32, P(u32)]
+        L.fyzz_b200_create_dynamic_body.argtypes = [vp, vp, P(u32)]
+        L.fyzz_b200_attach_box_shape.argtypes = [vp, u32, vp, vp, P(u32)]
+        L.fyzz_b200_attach_sphere_shape.argtypes = [vp, u32, f32, vp, P(u32)]
+        L.fyzz_b200_update_mass_properties.argtypes = [vp, u32, f32]
+        L.fyzz_b200_body_mass_properties.argtypes = [vp, u32, vp]
+        L.fyzz_b200_set_shape_material.argtypes = [vp, u32, P(Material)]
+        L.fyzz_b200_set_body_velocity.argtypes = [vp, u32, vp]
+        L.fyzz_b200_set_body_angular_velocity.argtypes = [vp, u32, vp]
+        L.fyzz_b200_add_center_distance_constraint.argtypes = [vp, u32, u32, f32, P(u64)]
+        L.fyzz_b200_add_scene.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, vp, u32, vp, vp, i32, f32, vp, P(u32)]
+        L.fyzz_b200_step.argtypes = [vp, f32]
+        L.fyzz_b200_step_n.argtypes = [vp, f32, u32]
+        L.fyzz_b200_collide.argtypes = [vp]
+        L.fyzz_b200_synchronize.argtypes = [vp]
+        L.fyzz_b200_body_state.argtypes = [vp, u32, P(BodyState)]
+        L.fyzz_b200_read_bodies.argtypes = [vp, vp, u32]
+        L.fyzz_b200_write_velocities.argtypes = [vp, vp, u32]
+        L.fyzz_b200_counts.argtypes = [vp, vp]
+        L.fyzz_b200_device_view.argtypes = [vp, P(DeviceView)]
+        L.fyzz_b200_read_pairs.argtypes = [vp, i32, vp, u64]
+        L.fyzz_b200_read_pairs.restype = u64
+        L.fyzz_b200_read_manifolds.argtypes = [vp, vp, vp, vp, u64]
+        L.fyzz_b200_read_manifolds.restype = u64
+        L.fyzz_b200_read_encoded_bounds.argtypes = [vp, vp, u32]
+        L.fyzz_b200_read_sorted_min_x.argtypes = [vp, u32, vp, vp, u64]
+        L.fyzz_b200_read_sorted_min_x.restype = u64
+        L.fyzz_b200_read_levels.argtypes = [vp, vp, u64]
+        L.fyzz_b200_read_levels.restype = u64
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None and a.size else None
+
+
+def _f32(x, n):
+    a = np.ascontiguousarray(np.asarray(x, np.float32).reshape(-1))
+    if a.size != n:
+        raise ValueError(f"expected {n} floats")
+    return a
+
+
+_IDENTITY = np.array([0, 0, 0, 0, 0, 0, 1], np.float32)
+
+
+class World:
+    """One B200 world: a batch of independent scenes stepped together.
+
+    Mirrors fyzz::World (reference include/fyzzxyzzy/world.h:396-510) for the
+    operations the rigid-body step supports."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        rc = lib().fyzz_b200_create(device, C.byref(h))
+        if rc:
+            raise RuntimeError(f"fyzz_b200_create failed ({rc}): no CUDA device or context")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fyzz_b200_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def _check(self, rc):
+        if rc == 0:
+            return
+        msg = lib().fyzz_b200_last_error(self.h).decode()
+        if rc == 1:
+            raise ValueError(msg)
+        if rc == 3:
+            raise OverflowError(msg)
+        raise RuntimeError(msg)
+
+    # ---- authoring ----
+    def begin_scene(self) -> int:
+        out = C.c_uint32()
+        self._check(lib().fyzz_b200_begin_scene(self.h, C.byref(out)))
+        return out.value
+
+    def add_static_floor(self, height: float) -> int:
+        out = C.c_uint32()
+        self._check(lib().fyzz_b200_add_static_floor(self.h, height, C.byref(out)))
+        return out.value
+
+    def create_dynamic_body(self, pose=_IDENTITY) -> int:
+        p = _f32(pose, 7)
+        out = C.c_uint32()
+        self._check(lib().fyzz_b200_create_dynamic_body(self.h, _p(p), C.byref(out)))
+        return out.value
+
+    def attach_box_shape(self, body: int, half_extents, local_pose=_IDENTITY) -> int:
+        h, l = _f32(half_extents, 3), _f32(local_pose, 7)
+        out = C.c_uint32()
+        self._check(lib().fyzz_b200_attach_box_shape(self.h, body, _p(h), _p(l), C.byref(out)))
+        return out.value
+
+    def attach_sphere_shape(self, body: int, radius: float, local_pose=_IDENTITY) -> int:
+        l = _f32(local_pose, 7)
+        out = C.c_uint32()
+        self._check(lib().fyzz_b200_attach_sphere_shape(self.h, body, radius, _p(l), C.byref(out)))
+        return out.value
+
+    def update_mass_properties(self, body: int, density: float):
+        self._check(lib().fyzz_b200_update_mass_properties(self.h, body, density))
+
+    def body_mass_properties(self, body: int) -> np.ndarray:
+        out = np.zeros(11, np.float32)
+        self._check(lib().fyzz_b200_body_mass_properties(self.h, body, _p(out)))
+        return out
+
+    def set_shape_material(self, shape: int, static_friction=0.5, dynamic_friction=0.5, restitution=0.2):
+        m = Material(static_friction, dynamic_friction, restitution)
+        self._check(lib().fyzz_b200_set_shape_material(self.h, shape, C.byref(m)))
+
+    def set_body_velocity(self, body: int, v):
+        a = _f32(v, 3)
+        self._check(lib().fyzz_b200_set_body_velocity(self.h, body, _p(a)))
+
+    def set_body_angular_velocity(self, body: int, v):
+        a = _f32(v, 3)
+        self._check(lib().fyzz_b200_set_body_angular_velocity(self.h, body, _p(a)))
+
+    def add_center_distance_constraint(self, a: int, b: int, distance: float) -> int:
+        out = C.c_uint64()
+        self._check(lib().fyzz_b200_add_center_distance_constraint(self.h, a, b, distance, C.byref(out)))
+        return out.value
+
+    def add_scene(self, spec) -> int:
+        """Author one seeded scene (fyzzxyzzy-sdk_b200.scenes.SceneSpec);
+        returns the BodyId of its first dynamic body."""
+        arrs = [np.ascontiguousarray(x) for x in (
+            spec.bodies, spec.shape_body, spec.shape_type, spec.shape_geom,
+            spec.shape_local, spec.shape_mat, spec.joints, spec.joint_dist)]
+        fm = np.asarray(spec.floor_mat, np.float32)
+        out = C.c_uint32()
+        self._check(lib().fyzz_b200_add_scene(
+            self.h, spec.n_bodies, _p(arrs[0]), spec.n_shapes, _p(arrs[1]), _p(arrs[2]),
+            _p(arrs[3]), _p(arrs[4]), _p(arrs[5]), arrs[6].shape[0], _p(arrs[6]), _p(arrs[7]),
+            0 if spec.floor is None else 1, 0.0 if spec.floor is None else float(spec.floor),
+            _p(fm), C.byref(out)))
+        return out.value
+
+    # ---- stepping ----
+    def step(self, seconds: float = 1.0 / 120.0, steps: int = 1):
+        if steps == 1:
+            self._check(lib().fyzz_b200_step(self.h, seconds))
+        else:
+            self._check(lib().fyzz_b200_step_n(self.h, seconds, steps))
+
+    def collide(self):
+        self._check(lib().fyzz_b200_collide(self.h))
+
+    def synchronize(self):
+        self._check(lib().fyzz_b200_synchronize(self.h))
+
+    # ---- results ----
+    def counts(self) -> dict:
+        out = np.zeros(10, np.uint64)
+        self._check(lib().fyzz_b200_counts(self.h, _p(out)))
+        keys = ["bodies", "shapes", "scenes", "pairs", "managers", "points",
+                "descriptors", "islands", "joints", "steps"]
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def body_state(self, body: int) -> BodyState:
+        out = BodyState()
+        self._check(lib().fyzz_b200_body_state(self.h, body, C.byref(out)))
+        return out
+
+    def read_bodies(self, out: np.ndarray | None = None) -> np.ndarray:
+        n = self.counts()["bodies"] if out is None else out.shape[0]
+        if out is None:
+            out = np.zeros((n, 14), np.float32)
+        self._check(lib().fyzz_b200_read_bodies(self.h, _p(out), n))
+        return out
+
+    def write_velocities(self, v6: np.ndarray):
+        v6 = np.ascontiguousarray(v6, np.float32)
+        self._check(lib().fyzz_b200_write_velocities(self.h, _p(v6), v6.shape[0]))
+
+    def device_view(self) -> DeviceView:
+        out = DeviceView()
+        self._check(lib().fyzz_b200_device_view(self.h, C.byref(out)))
+        return out
+
+    def pairs(self, which: int = 0) -> np.ndarray:
+        n = lib().fyzz_b200_read_pairs(self.h, which, None, 0)
+        out = np.zeros((n, 2), np.uint32)
+        lib().fyzz_b200_read_pairs(self.h, which, _p(out), n)
+        return out
+
+    def manifolds(self):
+        n = lib().fyzz_b200_read_manifolds(self.h, None, None, None, 0)
+        pairs = np.zeros((n, 2), np.uint32)
+        counts = np.zeros(n, np.uint32)
+        pts = np.zeros((n, 4, 7), np.float32)
+        lib().fyzz_b200_read_manifolds(self.h, _p(pairs), _p(counts), _p(pts), n)
+        return pairs, counts, pts
+
+    def encoded_bounds(self) -> np.ndarray:
+        n = self.counts()["shapes"]
+        out = np.zeros((n, 6), np.uint32)
+        self._check(lib().fyzz_b200_read_encoded_bounds(self.h, _p(out), n))
+        return out
+
+    def sorted_min_x(self, scene: int = 0):
+        n = lib().fyzz_b200_read_sorted_min_x(self.h, scene, None, None, 0)
+        v = np.zeros(n, np.uint32)
+        i = np.zeros(n, np.uint32)
+        lib().fyzz_b200_read_sorted_min_x(self.h, scene, _p(v), _p(i), n)
+        return v, i
+
+    def levels(self) -> np.ndarray:
+        n = lib().fyzz_b200_read_levels(self.h, None, 0)
+        out = np.zeros(n, np.uint32)
+        lib().fyzz_b200_read_levels(self.h, _p(out), n)
+        return out
+
+    def error_bits(self) -> int:
+        out = C.c_uint32()
+        lib().fyzz_b200_error_bits(self.h, C.byref(out))
+        return out.value

@@ -1,0 +1,239 @@
+// Broadphase: shape poses, integer-encoded AABBs, the sorted x-axis sweep
+// and canonical overlap-pair publication (found / lost against the
+// previous generation).
+//
+// Reference behaviour (src/native/scene.cpp):
+//   encode_float/min/max             26-35
+//   Scene::update_shape_bounds       1233-1316   (box basis extent, sphere r,
+//                                                 plus contact offset)
+//   Scene::update_bounds endpoint order 1341-1345 (value, min-before-max, id)
+//   Scene::update_pairs full sweep   2635-2704   (y/z test, different bodies,
+//                                                 at least one dynamic; planes
+//                                                 pair with every dynamic volume)
+//   Scene::publish_pairs             3230-3304   (sorted merge -> found / lost)
+//
+// B200 layout: min-x keys are sorted per scene (one CTA per scene when the
+// scene fits in shared memory, otherwise the device-wide radix sort); the
+// sweep then reads y/z bounds gathered into sorted order so the candidate
+// scan is a contiguous read.  Pairs are emitted into per-owner buckets
+// (owner = lower shape id) so the published list is already in canonical
+// (a, b) order after a per-bucket sort, without a device-wide pair sort.
+#include "state.h"
+
+namespace fyzz::b200 {
+namespace {
+
+__device__ __forceinline__ uint32_t encode_float(float v) {
+    const uint32_t bits = __float_as_uint(v);
+    return (bits & 0x80000000u) ? ~bits : (bits | 0x80000000u);
+}
+__device__ __forceinline__ uint32_t encode_min(float v) { return ((encode_float(v) >> 4) - 1u) << 4; }
+__device__ __forceinline__ uint32_t encode_max(float v) { return (((encode_float(v) >> 4) + 1u) << 4) | 4u; }
+
+__global__ void k_shape_bounds(DevState s) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.n_shapes) return;
+    const uint32_t b = s.s_body[i];
+    const v3 bp = ld3(s.b_p[b]);
+    const qt bq = ldq(s.b_q[b]);
+    const float4 lp = s.s_lp[i];
+    const v3 wp = vadd(bp, rot_sc(bq, ld3(lp)));           // scene.cpp:366-371
+    const qt wq = qmul(bq, ldq(s.s_lq[i]));
+    s.s_wp[i] = st4(wp, 0.0f);
+    s.s_wq[i] = stq(wq);
+    const uint32_t type = s.s_type[i];
+    if (type == kPlane) return;
+    const float4 g = s.s_geom[i];
+    const v3 h = {g.x, g.y, g.z};
+    v3 e = type == kSphere ? v3{g.w, g.w, g.w} : h;
+    if (type == kBox && (wq.x != 0.0f || wq.y != 0.0f || wq.z != 0.0f || wq.w != 1.0f)) {
+        const v3 x = rot_sc(wq, {1, 0, 0}), y = rot_sc(wq, {0, 1, 0}), z = rot_sc(wq, {0, 0, 1});
+        e = {fabsf(x.x) * h.x + fabsf(y.x) * h.y + fabsf(z.x) * h.z,
+             fabsf(x.y) * h.x + fabsf(y.y) * h.y + fabsf(z.y) * h.z,
+             fabsf(x.z) * h.x + fabsf(y.z) * h.y + fabsf(z.z) * h.z};
+    }
+    const float co = lp.w;
+    e.x += co; e.y += co; e.z += co;
+    const float lo[3] = {wp.x - e.x, wp.y - e.y, wp.z - e.z};
+    const float hi[3] = {wp.x + e.x, wp.y + e.y, wp.z + e.z};
+    if (!(isfinite(lo[0]) && isfinite(lo[1]) && isfinite(lo[2]) &&
+          isfinite(hi[0]) && isfinite(hi[1]) && isfinite(hi[2])))
+        atomicOr(s.err, kErrNonFinite);
+    const uint4 elo = make_uint4(encode_min(lo[0]), encode_min(lo[1]), encode_min(lo[2]), 0u);
+    const uint4 ehi = make_uint4(encode_max(hi[0]), encode_max(hi[1]), encode_max(hi[2]), 0u);
+    s.s_lo[i] = elo;
+    s.s_hi[i] = ehi;
+    const int32_t f = s.s_frank[i];
+    s.srt_key[f] = elo.x;
+    s.srt_id[f] = i;
+}
+
+// One CTA sorts one scene's min-x endpoints by (value, shape id): bitonic
+// sort of 64-bit keys in shared memory.
+constexpr int kSmallSortThreads = 1024;
+__global__ void __launch_bounds__(kSmallSortThreads) k_sort_small(DevState s) {
+    extern __shared__ unsigned long long sk[];
+    const uint32_t scene = s.small_scenes[blockIdx.x];
+    const uint32_t begin = s.sc_fbegin[scene], end = s.sc_fbegin[scene + 1];
+    const uint32_t n = end - begin;
+    uint32_t m = 1;
+    while (m < n) m <<= 1;
+    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x)
+        sk[i] = i < n ? ((unsigned long long)s.srt_key[begin + i] << 32) | s.srt_id[begin + i]
+                      : ~0ull;
+    __syncthreads();
+    for (uint32_t k = 2; k <= m; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+                const uint32_t ixj = i ^ j;
+                if (ixj > i) {
+                    const unsigned long long a = sk[i], b = sk[ixj];
+                    const bool up = (i & k) == 0;
+                    if ((a > b) == up) { sk[i] = b; sk[ixj] = a; }
+                }
+            }
+            __syncthreads();
+        }
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        s.srt_key[begin + i] = uint32_t(sk[i] >> 32);
+        s.srt_id[begin + i] = uint32_t(sk[i]);
+    }
+}
+
+// Gather the sweep records into sorted order: (min y, max y, min z, max z)
+// and (max x, body | dynamic << 31).
+__global__ void k_sweep_gather(DevState s, uint4* rec, uint2* meta) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.n_finite) return;
+    const uint32_t id = s.srt_id[i];
+    const uint4 lo = s.s_lo[id], hi = s.s_hi[id];
+    const uint32_t body = s.s_body[id];
+    const uint32_t dyn = s.b_flags[body] & kBodyDynamic;
+    rec[i] = make_uint4(lo.y, hi.y, lo.z, hi.z);
+    meta[i] = make_uint2(hi.x, body | (dyn << 31));
+}
+
+__global__ void k_sweep(DevState s, const uint4* __restrict__ rec, const uint2* __restrict__ meta,
+                        int fill) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    uint64_t* keys = s.cur.key;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n_finite; i += stride) {
+        const uint32_t id = s.srt_id[i];
+        const uint32_t scene = s.s_scene[id];
+        const uint32_t end = s.sc_fbegin[scene + 1];
+        const uint4 a = rec[i];
+        const uint2 am = meta[i];
+        const uint32_t abody = am.y & 0x7fffffffu;
+        const bool adyn = (am.y >> 31) != 0u;
+        for (uint32_t j = i + 1; j < end; ++j) {
+            if (s.srt_key[j] > am.x) break;
+            const uint2 bm = meta[j];
+            const uint32_t bbody = bm.y & 0x7fffffffu;
+            if (bbody == abody) continue;
+            if (!adyn && (bm.y >> 31) == 0u) continue;
+            const uint4 b = rec[j];
+            if (a.x > b.y || b.x > a.y || a.z > b.w || b.z > a.w) continue;
+            const uint32_t other = s.srt_id[j];
+            const uint32_t owner = min(id, other), partner = max(id, other);
+            if (!fill) {
+                atomicAdd(&s.own_cnt[owner], 1u);
+            } else {
+                const uint32_t pos = s.own_off[owner] + s.s_static_pairs[owner] + atomicAdd(&s.own_cur[owner], 1u);
+                if (pos < s.pair_cap) keys[pos] = (uint64_t(owner) << 32) | partner;
+                else atomicOr(s.err, kErrPairCapacity);
+            }
+        }
+        if (fill && adyn) {
+            const int32_t p = s.sc_plane[scene];
+            if (p >= 0) {
+                const uint32_t pp = uint32_t(p);
+                const uint32_t pos = pp < id ? s.own_off[pp] + uint32_t(s.s_dynrank[id]) : s.own_off[id];
+                const uint32_t owner = min(pp, id), partner = max(pp, id);
+                if (pos < s.pair_cap) keys[pos] = (uint64_t(owner) << 32) | partner;
+                else atomicOr(s.err, kErrPairCapacity);
+            }
+        }
+    }
+}
+
+// Sort each owner's bucket by partner id.  Plane owners are filled in
+// ascending order already.
+__global__ void k_owner_sort(DevState s) {
+    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= s.n_shapes || s.s_type[o] == kPlane) return;
+    const uint32_t n = s.s_static_pairs[o] + s.own_cur[o];
+    if (n < 2) return;
+    const uint32_t b = s.own_off[o];
+    if (b + n > s.pair_cap) return;
+    uint64_t* k = s.cur.key + b;
+    for (uint32_t i = 1; i < n; ++i) {
+        const uint64_t v = k[i];
+        uint32_t j = i;
+        while (j > 0 && k[j - 1] > v) { k[j] = k[j - 1]; --j; }
+        k[j] = v;
+    }
+}
+
+__global__ void k_pair_total(DevState s) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        const uint32_t total = *s.cur.n;
+        if (total > s.pair_cap) {
+            atomicOr(s.err, kErrPairCapacity);
+            *s.cur.n = s.pair_cap;
+        }
+    }
+}
+
+__device__ __forceinline__ int32_t find_key(const uint64_t* keys, uint32_t n, uint64_t key) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (keys[mid] < key) lo = mid + 1; else hi = mid;
+    }
+    return (lo < n && keys[lo] == key) ? int32_t(lo) : -1;
+}
+
+__global__ void k_pair_match(DevState s) {
+    const uint32_t n = *s.cur.n, np = *s.prev.n;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+        const int32_t j = find_key(s.prev.key, np, s.cur.key[k]);
+        s.prev_idx[k] = j;
+        s.found_flag[k] = j < 0 ? 1u : 0u;
+    }
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += stride)
+        s.lost_flag[k] = find_key(s.cur.key, n, s.prev.key[k]) < 0 ? 1u : 0u;
+}
+
+}  // namespace
+
+void enqueue_broadphase(const DevState& s, cudaStream_t st) {
+    uint4* rec = s.sw_rec;
+    uint2* meta = s.sw_meta;
+    const int T = 256;
+    k_shape_bounds<<<(s.n_shapes + T - 1) / T, T, 0, st>>>(s);
+    if (s.n_small) {
+        uint32_t m = 1;
+        while (m < s.max_small_scene) m <<= 1;
+        k_sort_small<<<s.n_small, kSmallSortThreads, m * sizeof(unsigned long long), st>>>(s);
+    }
+    for (uint32_t i = 0; i < s.n_large; ++i)
+        radix_sort_pairs(s.srt_key + s.large_begin[i], s.srt_id + s.large_begin[i],
+                         s.srt_key2, s.srt_id2, s.large_n[i], nullptr, 0, 32,
+                         s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st);
+    if (s.n_finite) {
+        k_sweep_gather<<<(s.n_finite + T - 1) / T, T, 0, st>>>(s, rec, meta);
+    }
+    cudaMemcpyAsync(s.own_cnt, s.s_static_pairs, size_t(s.n_shapes) * 4, cudaMemcpyDeviceToDevice, st);
+    cudaMemsetAsync(s.own_cur, 0, size_t(s.n_shapes) * 4, st);
+    const uint32_t sweep_blocks = s.n_finite ? (s.n_finite + T - 1) / T : 0;
+    if (sweep_blocks) k_sweep<<<sweep_blocks, T, 0, st>>>(s, rec, meta, 0);
+    scan_exclusive(s.own_cnt, s.own_off, s.n_shapes, nullptr, s.cur.n, s.scan_tmp, s.scan_tmp_words, st);
+    k_pair_total<<<1, 32, 0, st>>>(s);
+    if (sweep_blocks) k_sweep<<<sweep_blocks, T, 0, st>>>(s, rec, meta, 1);
+    k_owner_sort<<<(s.n_shapes + T - 1) / T, T, 0, st>>>(s);
+    const uint32_t mb = (s.pair_cap + T - 1) / T;
+    k_pair_match<<<mb < 1184 ? mb : 1184, T, 0, st>>>(s);
+}
+
+}  // namespace fyzz::b200

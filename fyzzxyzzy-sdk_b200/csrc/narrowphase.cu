@@ -1,0 +1,1053 @@
+// Narrowphase: persistent-contact-manifold (PCM) contact generation for every
+// broadphase pair, one thread per pair.
+//
+// Reference routines (paths relative to the reference project):
+//   src/native/GuPCMContactBoxBox.cpp:301-436  box/box SAT, reference face,
+//                                              incident clipping (<= 64 cands)
+//   src/native/GuPCMContactBoxBox.cpp:185-297  batch reduction to 4
+//   src/native/GuPCMGjkEpa.cpp:44-570          GJK / EPA zero-face continuation
+//   src/native/GuPCMContactSphere.cpp:49-130   sphere/sphere, sphere/plane,
+//                                              sphere/box
+//   src/native/scene.cpp:3432-3465             manifold refresh
+//   src/native/scene.cpp:3319-3431             fifth-point reduction
+//   src/native/scene.cpp:3466-3654             box/box manifold lifecycle
+//   src/native/scene.cpp:3774-3955             plane/box manifold lifecycle
+//   src/native/scene.cpp:4012-4700             per-pair dispatch, Gu order
+//                                              (statics second, dynamics by
+//                                              descending body id), normal flips
+// The manifold cache of each pair is gathered from the previous generation
+// through prev_idx and written to the current one, so the step never reads
+// and writes the same record.
+#include "state.h"
+#include <cfloat>
+
+namespace fyzz::b200 {
+namespace {
+
+struct Cand { v3 la, lb, nb; float sep; };
+
+// ---------------- box/box face contacts ----------------
+struct GBox { v3 half, pos; qt rot; v3 axis[3]; };
+__device__ GBox make_box(v3 h, v3 p, qt q) {
+    GBox b;
+    b.half = h; b.pos = p; b.rot = q;
+    b.axis[0] = rot_gu(q, {1, 0, 0});
+    b.axis[1] = rot_gu(q, {0, 1, 0});
+    b.axis[2] = rot_gu(q, {0, 0, 1});
+    return b;
+}
+struct Frame { v3 x, y, z, p; };
+__device__ __forceinline__ v3 fr_project(const Frame& f, v3 w) {
+    const v3 d = vsub(w, f.p);
+    return {vdot(d, f.x), vdot(d, f.y), vdot(d, f.z)};
+}
+__device__ __forceinline__ v3 fr_unproject(const Frame& f, v3 v) {
+    return vadd(f.p, vadd(vadd(vmul(f.x, v.x), vmul(f.y, v.y)), vmul(f.z, v.z)));
+}
+__device__ bool poly_contains(const v3* poly, v3 p, v3 low, v3 high) {
+    if (p.x < low.x || p.y < low.y || p.x > high.x || p.y > high.y) return false;
+    unsigned hits = 0;
+    const float eps = FLT_EPSILON;
+    for (unsigned i = 0, j = 3; i < 4; j = i++) {
+        const v3 a = poly[j], b = poly[i];
+        if ((p.x == a.x && p.y == a.y) || (p.x == b.x && p.y == b.y)) return true;
+        if ((a.y > p.y) != (b.y > p.y)) {
+            const float dx = b.x - a.x, dy = b.y - a.y;
+            const float part = (p.y - a.y) * dx + (a.x + eps) * dy;
+            const float target = p.x * dy;
+            const bool inter = dy > 0.0f ? part >= target : target >= part;
+            if (inter && ++hits == 2) return false;
+        }
+    }
+    return hits > 0;
+}
+__device__ bool seg_aabb(v3 p, v3 delta, v3 high, v3 low, float& enter, float& exit_) {
+    enter = 0.0f;
+    exit_ = 1.0f;
+    for (unsigned axis = 0; axis < 3; ++axis) {
+        const float x = vcomp(p, axis), d = vcomp(delta, axis);
+        const float mn = vcomp(low, axis), mx = vcomp(high, axis);
+        if (fabsf(d) < 1.0e-6f) {
+            if (x < mn || x > mx) return false;
+            continue;
+        }
+        const float one = (mn - x) / d, two = (mx - x) / d;
+        enter = smax(enter, smin(one, two));
+        exit_ = smin(exit_, smax(one, two));
+    }
+    return enter <= exit_ && enter <= 1.0f;
+}
+struct Gen {
+    const GBox* a; const GBox* b; Cand* out; int count; bool overflow;
+    __device__ void emit(const Frame& f, v3 reference, v3 incident, v3 normal, float sep, bool flipped) {
+        if (count >= 64) { overflow = true; return; }
+        const v3 w0 = fr_unproject(f, flipped ? incident : reference);
+        const v3 w1 = fr_unproject(f, flipped ? reference : incident);
+        Cand& c = out[count++];
+        c.la = rotinv_gu(a->rot, vsub(w0, a->pos));
+        c.lb = rotinv_gu(b->rot, vsub(w1, b->pos));
+        c.nb = rotinv_gu(b->rot, normal);
+        c.sep = sep;
+    }
+};
+__device__ void gen_calculate(Gen& g, const Frame& f, const v3* poly, v3 inc_n, float fx, float fy,
+                              v3 normal, float cd, bool flipped) {
+    fx *= 1.0001f;
+    fy *= 1.0001f;
+    bool pen[4] = {false, false, false, false}, ins[4] = {false, false, false, false};
+    v3 mn = {FLT_MAX, FLT_MAX, FLT_MAX};
+    v3 mx = vneg(mn);
+    const v3 high = {fx, fy, FLT_MAX};
+    for (unsigned i = 0; i < 4; ++i) {
+        const v3 p = poly[i];
+        mn.x = smin(mn.x, p.x); mn.y = smin(mn.y, p.y);
+        mx.x = smax(mx.x, p.x); mx.y = smax(mx.y, p.y);
+        if (-p.z < cd) {
+            pen[i] = true;
+            ins[i] = fabsf(p.x) <= fx && fabsf(p.y) <= fy;
+            if (ins[i]) g.emit(f, {p.x, p.y, 0}, p, normal, -p.z, flipped);
+        }
+    }
+    if (g.count == 4) return;
+    if (inc_n.z != 0.0f) {
+        const v3 corners[4] = {{fx, fy, 0}, {fx, -fy, 0}, {-fx, fy, 0}, {-fx, -fy, 0}};
+        for (int k = 0; k < 4; ++k) {
+            const v3 c = corners[k];
+            if (!poly_contains(poly, c, mn, mx)) continue;
+            const float nom = vdot(inc_n, vsub(poly[0], c));
+            const float t = nom / inc_n.z;
+            const float sep = -t;
+            if (cd > sep) g.emit(f, c, {c.x, c.y, t}, normal, sep, flipped);
+        }
+    }
+    const v3 low = {-fx, -fy, -cd - FLT_EPSILON};
+    for (unsigned start = 0, end = 3; start < 4; end = start++) {
+        if (!pen[start] && !pen[end]) continue;
+        const bool c0 = pen[start] && ins[start];
+        const bool c1 = pen[end] && ins[end];
+        if (c0 && c1) continue;
+        const v3 edge = vsub(poly[end], poly[start]);
+        float t0, t1;
+        if (!seg_aabb(poly[start], edge, high, low, t0, t1)) continue;
+        if (!c0) {
+            const v3 p = vadd(poly[start], vmul(edge, t0));
+            g.emit(f, {p.x, p.y, 0}, p, normal, -p.z, flipped);
+        }
+        if (!c1) {
+            const v3 p = vadd(poly[start], vmul(edge, t1));
+            g.emit(f, {p.x, p.y, 0}, p, normal, -p.z, flipped);
+        }
+    }
+}
+// Returns 0 separated, 1 overlapping (count candidates), -1 overflow.
+__device__ int box_box_candidates(v3 h0, v3 p0, qt q0, v3 h1, v3 p1, qt q1, float cd,
+                                  Cand* out, int& count) {
+    const GBox a = make_box(h0, p0, q0), b = make_box(h1, p1, q1);
+    Gen g{&a, &b, out, 0, false};
+    const v3 delta = vsub(b.pos, a.pos);
+    float sign[6], overlap[6];
+    const float se = 1.0e-6f;
+    count = 0;
+    for (unsigned i = 0; i < 6; ++i) {
+        const bool first = i < 3;
+        const GBox& ref = first ? a : b;
+        const GBox& inc = first ? b : a;
+        const unsigned axis = i % 3;
+        const v3 n = ref.axis[axis];
+        sign[i] = vdot(delta, n);
+        const float rad = (fabsf(vdot(n, inc.axis[0])) + se) * inc.half.x +
+                          (fabsf(vdot(n, inc.axis[1])) + se) * inc.half.y +
+                          (fabsf(vdot(n, inc.axis[2])) + se) * inc.half.z;
+        overlap[i] = vcomp(ref.half, axis) + rad - fabsf(sign[i]) + cd;
+        if (overlap[i] < 0.0f) return 0;
+    }
+    for (unsigned i = 0; i < 3; ++i)
+        for (unsigned j = 0; j < 3; ++j) {
+            const v3 ca = vcross(a.axis[i], b.axis[j]);
+            float rA = 0.0f, rB = 0.0f;
+            for (unsigned k = 0; k < 3; ++k) {
+                if (k != i) rA += (fabsf(vdot(ca, a.axis[k])) + se) * vcomp(a.half, k);
+                if (k != j) rB += (fabsf(vdot(ca, b.axis[k])) + se) * vcomp(b.half, k);
+            }
+            if (fabsf(vdot(delta, ca)) > rA + rB + cd) return 0;
+        }
+    unsigned feature = 0;
+    float mo = overlap[0];
+    for (unsigned i = 1; i < 6; ++i)
+        if (mo > overlap[i]) { mo = overlap[i]; feature = i; }
+    const bool flipped = feature >= 3;
+    const GBox& inc = flipped ? a : b;
+    const bool np = sign[feature] <= 0.0f;
+    Frame fr;
+    v3 normal;
+    float fx, fy;
+    switch (feature) {
+    case 0:
+        normal = np ? a.axis[0] : vneg(a.axis[0]);
+        fr = {np ? vneg(a.axis[2]) : a.axis[2], a.axis[1], normal,
+              vadd(a.pos, vmul(a.axis[0], np ? -a.half.x : a.half.x))};
+        fx = a.half.z; fy = a.half.y; break;
+    case 1:
+        normal = np ? a.axis[1] : vneg(a.axis[1]);
+        fr = {a.axis[0], np ? vneg(a.axis[2]) : a.axis[2], normal,
+              vadd(a.pos, vmul(a.axis[1], np ? -a.half.y : a.half.y))};
+        fx = a.half.x; fy = a.half.z; break;
+    case 2:
+        normal = np ? a.axis[2] : vneg(a.axis[2]);
+        fr = {a.axis[0], np ? a.axis[1] : vneg(a.axis[1]), normal,
+              vadd(a.pos, vmul(a.axis[2], np ? -a.half.z : a.half.z))};
+        fx = a.half.x; fy = a.half.y; break;
+    case 3:
+        normal = np ? b.axis[0] : vneg(b.axis[0]);
+        fr = {np ? b.axis[2] : vneg(b.axis[2]), b.axis[1], vneg(normal),
+              vadd(b.pos, vmul(b.axis[0], np ? b.half.x : -b.half.x))};
+        fx = b.half.z; fy = b.half.y; break;
+    case 4:
+        normal = np ? b.axis[1] : vneg(b.axis[1]);
+        fr = {b.axis[0], np ? b.axis[2] : vneg(b.axis[2]), vneg(normal),
+              vadd(b.pos, vmul(b.axis[1], np ? b.half.y : -b.half.y))};
+        fx = b.half.x; fy = b.half.z; break;
+    default:
+        normal = np ? b.axis[2] : vneg(b.axis[2]);
+        fr = {b.axis[0], np ? vneg(b.axis[1]) : b.axis[1], vneg(normal),
+              vadd(b.pos, vmul(b.axis[2], np ? b.half.z : -b.half.z))};
+        fx = b.half.x; fy = b.half.y; break;
+    }
+    const v3 search = vneg(fr.z);
+    const float dx = fabsf(vdot(search, inc.axis[0]));
+    const float dy = fabsf(vdot(search, inc.axis[1]));
+    const float dz = fabsf(vdot(search, inc.axis[2]));
+    const unsigned ia = dx >= dy && dx >= dz ? 0 : (dy >= dz ? 1 : 2);
+    const float facing = vdot(search, inc.axis[ia]);
+    const float sext = facing > 0.0f ? -vcomp(inc.half, ia) : vcomp(inc.half, ia);
+    const v3 fc = vadd(inc.pos, vmul(inc.axis[ia], sext));
+    const unsigned ua = ia == 0 ? 1 : 0;
+    const unsigned va = ia == 2 ? 1 : 2;
+    const v3 u = vmul(inc.axis[ua], vcomp(inc.half, ua));
+    const v3 v = vmul(inc.axis[va], vcomp(inc.half, va));
+    const v3 pw[4] = {vadd(fc, vadd(u, v)), vadd(fc, vsub(u, v)), vsub(fc, vadd(u, v)), vsub(fc, vsub(u, v))};
+    v3 poly[4];
+    for (int i = 0; i < 4; ++i) poly[i] = fr_project(fr, pw[i]);
+    const v3 fn = fr_project(fr, vadd(fr.p, facing > 0.0f ? vneg(inc.axis[ia]) : inc.axis[ia]));
+    gen_calculate(g, fr, poly, fn, fx, fy, normal, cd, flipped);
+    if (g.overflow) return -1;
+    count = g.count;
+    return 1;
+}
+
+__device__ void batch_selection(const Cand* c, int n, float tol, int sel[4]) {
+    uint8_t avail[64];
+    for (int i = 0; i < n; ++i) avail[i] = uint8_t(i);
+    int remaining = n;
+    float deepest_depth = c[0].sep, shallowest = deepest_depth;
+    int deepest = 0;
+    for (int i = 1; i < remaining; ++i) {
+        const float d = c[i].sep;
+        shallowest = smax(shallowest, d);
+        if (deepest_depth > d) { deepest_depth = d; deepest = i; }
+    }
+    sel[0] = deepest;
+    avail[deepest] = avail[--remaining];
+    int fpos = 0;
+    float far2 = vlen2(vsub(c[avail[0]].lb, c[sel[0]].lb));
+    for (int i = 1; i < remaining; ++i) {
+        const float val = vlen2(vsub(c[avail[i]].lb, c[sel[0]].lb));
+        if (val > far2) { far2 = val; fpos = i; }
+    }
+    sel[1] = avail[fpos];
+    avail[fpos] = avail[--remaining];
+    const v3 base = vsub(c[sel[1]].lb, c[sel[0]].lb);
+    v3 tr = vcross(base, c[sel[0]].nb);
+    const float tr2 = vlen2(tr);
+    if (tr2 > 0.0f) {
+        const float inv = 1.0f / sqrtf(tr2);
+        tr = {tr.x * inv, tr.y * inv, tr.z * inv};
+    } else {
+        tr = c[sel[0]].nb;
+    }
+    float greatest = -FLT_MAX, least = FLT_MAX;
+    int gpos = 0, lpos = 0;
+    for (int i = 0; i < remaining; ++i) {
+        const float side = vdot(vsub(c[avail[i]].lb, c[sel[0]].lb), tr);
+        if (side > greatest) { greatest = side; gpos = i; }
+        if (side < least) { least = side; lpos = i; }
+    }
+    sel[2] = avail[gpos];
+    avail[gpos] = avail[--remaining];
+    if (lpos == remaining) lpos = gpos;
+    if (least * greatest > 0.0f) {
+        greatest = -FLT_MAX;
+        for (int i = 0; i < remaining; ++i) {
+            const float side = vdot(vsub(c[avail[i]].lb, c[sel[0]].lb), tr);
+            if (side > greatest) { greatest = side; lpos = i; }
+        }
+    }
+    sel[3] = avail[lpos];
+    avail[lpos] = avail[--remaining];
+    const float thr = tol * 0.02f;
+    if (deepest_depth < thr && shallowest > thr) {
+        for (int i = 0; i < 4; ++i) {
+            float depth = c[sel[i]].sep;
+            if (depth > thr) {
+                int rep = remaining;
+                for (int j = 0; j < remaining; ++j) {
+                    const float cand = c[avail[j]].sep;
+                    if (depth > cand && thr > cand) { depth = cand; rep = j; }
+                }
+                if (rep < remaining) {
+                    const uint8_t t = uint8_t(sel[i]);
+                    sel[i] = avail[rep];
+                    avail[rep] = t;
+                }
+            }
+        }
+    }
+}
+
+// ---------------- GJK / EPA ----------------
+struct Sup { v3 a, b, q; uint32_t ai, bi; };
+struct BPair { v3 ha, hb, a_in_b; qt rel; };
+__device__ __forceinline__ v3 box_vertex(v3 e, v3 d, uint32_t& idx) {
+    const bool x = d.x > 0.f, y = d.y > 0.f, z = d.z > 0.f;
+    idx = (x ? 1u : 0u) | (y ? 2u : 0u) | (z ? 4u : 0u);
+    return {x ? e.x : -e.x, y ? e.y : -e.y, z ? e.z : -e.z};
+}
+__device__ Sup bp_support(const BPair& p, v3 dir) {
+    Sup s;
+    const v3 da = rotinv_gu(p.rel, dir);
+    const v3 pa = box_vertex(p.ha, da, s.ai);
+    s.b = box_vertex(p.hb, vneg(dir), s.bi);
+    s.a = vadd(p.a_in_b, rot_gu(p.rel, pa));
+    s.q = vsub(s.a, s.b);
+    return s;
+}
+__device__ __forceinline__ v3 bp_local_a(const BPair& p, v3 pb) { return rotinv_gu(p.rel, vsub(pb, p.a_in_b)); }
+__device__ __forceinline__ float box_min_margin(v3 h) { return 0.05f * smin(smin(h.x, h.y), h.z); }
+__device__ bool solve_small(int n, float a[3][4], float r[3]) {
+    float scale = 0.0f;
+    for (int i = 0; i < n; ++i) scale = smax(scale, fabsf(a[i][i]));
+    if (!(scale > 0.0f) || !isfinite(scale)) return false;
+    const float tol = FLT_EPSILON * scale;
+    for (int col = 0; col < n; ++col) {
+        int piv = col;
+        for (int row = col + 1; row < n; ++row)
+            if (fabsf(a[row][col]) > fabsf(a[piv][col])) piv = row;
+        if (!(fabsf(a[piv][col]) > tol)) return false;
+        for (int j = col; j <= n; ++j) { const float t = a[col][j]; a[col][j] = a[piv][j]; a[piv][j] = t; }
+        const float div = a[col][col];
+        for (int j = col; j <= n; ++j) a[col][j] /= div;
+        for (int row = 0; row < n; ++row)
+            if (row != col) {
+                const float f = a[row][col];
+                for (int j = col; j <= n; ++j) a[row][j] = fmaf(-f, a[col][j], a[row][j]);
+            }
+    }
+    for (int i = 0; i < n; ++i) r[i] = a[i][n];
+    return true;
+}
+struct Closest { v3 point, a, b; float w[4]; unsigned mask; float dist2; };
+__device__ Closest closest_simplex(const Sup* s, int count) {
+    Closest best;
+    best.point = best.a = best.b = {0, 0, 0};
+    best.w[0] = best.w[1] = best.w[2] = best.w[3] = 0.0f;
+    best.mask = 0;
+    best.dist2 = FLT_MAX;
+    for (unsigned mask = 1; mask < (1u << count); ++mask) {
+        int ids[4] = {0, 0, 0, 0}, n = 0;
+        for (int i = 0; i < count; ++i)
+            if (mask & (1u << i)) ids[n++] = i;
+        float w[4] = {0, 0, 0, 0};
+        w[ids[0]] = 1.0f;
+        if (n > 1) {
+            const v3 base = s[ids[0]].q;
+            v3 dirs[3];
+            float m[3][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
+            for (int i = 1; i < n; ++i) dirs[i - 1] = vsub(s[ids[i]].q, base);
+            for (int i = 1; i < n; ++i) {
+                for (int j = 1; j < n; ++j) m[i - 1][j - 1] = vdot(dirs[i - 1], dirs[j - 1]);
+                m[i - 1][n - 1] = -vdot(dirs[i - 1], base);
+            }
+            float coef[3] = {0, 0, 0};
+            if (!solve_small(n - 1, m, coef)) continue;
+            for (int i = 1; i < n; ++i) {
+                w[ids[i]] = coef[i - 1];
+                w[ids[0]] -= coef[i - 1];
+            }
+        }
+        bool feasible = true;
+        for (int i = 0; i < n; ++i)
+            if (w[ids[i]] < -1.0e-5f) feasible = false;
+        if (!feasible) continue;
+        v3 q = {0, 0, 0}, pa = {0, 0, 0}, pb = {0, 0, 0};
+        for (int i = 0; i < count; ++i) {
+            q = vadd(q, vmul(s[i].q, w[i]));
+            pa = vadd(pa, vmul(s[i].a, w[i]));
+            pb = vadd(pb, vmul(s[i].b, w[i]));
+        }
+        const float d = vlen2(q);
+        if (d < best.dist2) {
+            best.point = q; best.a = pa; best.b = pb;
+            for (int i = 0; i < 4; ++i) best.w[i] = w[i];
+            best.mask = mask; best.dist2 = d;
+        }
+    }
+    return best;
+}
+__device__ void compact_simplex(Sup* s, int& count, const Closest& c) {
+    int write = 0;
+    for (int read = 0; read < count; ++read)
+        if ((c.mask & (1u << read)) && c.w[read] > 1.0e-6f) s[write++] = s[read];
+    if (write == 0 && count > 0) write = 1;
+    count = write;
+}
+__device__ bool contact_from_gjk(const BPair& p, const Closest& n, Cand& out) {
+    const float dist = sqrtf(n.dist2);
+    if (!(dist > 0.0f) || !isfinite(dist)) return false;
+    const v3 normal = vmul(n.point, 1.0f / dist);
+    out = {bp_local_a(p, n.a), n.b, normal, dist};
+    return true;
+}
+struct Facet { int i, j, k; v3 normal; float distance; bool valid, in_heap; };
+__device__ Facet make_facet(const Sup* vtx, int i, int j, int k) {
+    Facet f;
+    f.i = f.j = f.k = 0; f.normal = {0, 0, 0}; f.distance = 0.0f; f.valid = false; f.in_heap = true;
+    const v3 a = vtx[i].q, b = vtx[j].q, c = vtx[k].q;
+    const v3 e0 = vsub(b, a), e1 = vsub(c, a);
+    v3 n = vcross(e0, e1);
+    const float norm2 = vlen2(n);
+    if (!(norm2 > FLT_EPSILON)) return f;
+    n = vmul(n, 1.0f / sqrtf(norm2));
+    f.i = i; f.j = j; f.k = k; f.normal = n; f.distance = vdot(n, a); f.valid = true;
+    return f;
+}
+__device__ bool init_epa(const BPair& p, Sup* vtx, int& count, Facet* facets, int& fc) {
+    if (count <= 0 || count > 4) return false;
+    if (count == 1) {
+        const Sup nx = bp_support(p, {1, 0, 0});
+        if (vlen2(vsub(nx.q, vtx[0].q)) == 0.0f) return false;
+        vtx[count++] = nx;
+    }
+    if (count == 2) {
+        const v3 edge = vsub(vtx[1].q, vtx[0].q);
+        const v3 ab = {fabsf(edge.x), fabsf(edge.y), fabsf(edge.z)};
+        v3 axis = {1, 0, 0};
+        if (ab.x > ab.y && ab.z > ab.y) axis = {0, 1, 0};
+        else if (ab.x > ab.z) axis = {0, 0, 1};
+        v3 perp = vcross(axis, edge);
+        const float sq = vlen2(perp);
+        if (!(sq > 0.0f)) return false;
+        perp = vmul(perp, 1.0f / sqrtf(sq));
+        vtx[count++] = bp_support(p, perp);
+    }
+    if (count == 3) {
+        const Facet f0 = make_facet(vtx, 0, 1, 2), f1 = make_facet(vtx, 1, 0, 2);
+        if (!f0.valid || !f1.valid) return false;
+        facets[fc++] = f0;
+        facets[fc++] = f1;
+        return true;
+    }
+    const v3 p0 = vtx[0].q;
+    const v3 v1 = vsub(vtx[1].q, p0), v2 = vsub(vtx[2].q, p0);
+    if (vdot(vcross(v1, v2), vsub(vtx[3].q, p0)) > 0.0f) {
+        const Sup t = vtx[1]; vtx[1] = vtx[2]; vtx[2] = t;
+    }
+    const int faces[4][3] = {{0, 1, 2}, {0, 3, 1}, {0, 2, 3}, {1, 3, 2}};
+    for (int i = 0; i < 4; ++i) {
+        const Facet f = make_facet(vtx, faces[i][0], faces[i][1], faces[i][2]);
+        if (!f.valid) return false;
+        facets[fc++] = f;
+    }
+    return true;
+}
+__device__ bool contact_from_facet(const BPair& p, const Sup* vtx, const Facet& f, Cand& out) {
+    const Sup& P = vtx[f.i];
+    const Sup& Qv = vtx[f.j];
+    const Sup& R = vtx[f.k];
+    const v3 e0 = vsub(Qv.q, P.q), e1 = vsub(R.q, P.q);
+    const float a = vdot(e0, e0), b = vdot(e0, e1), c = vdot(e1, e1);
+    const float den = a * c - b * b;
+    if (!(den > FLT_EPSILON * a * c)) return false;
+    const float x = -vdot(P.q, e0), y = -vdot(P.q, e1);
+    const float u = (x * c - y * b) / den;
+    const float v = (y * a - x * b) / den;
+    const float w = 1.0f - u - v;
+    const v3 pa = vadd(vadd(vmul(P.a, w), vmul(Qv.a, u)), vmul(R.a, v));
+    const v3 pb = vadd(vadd(vmul(P.b, w), vmul(Qv.b, u)), vmul(R.b, v));
+    if (!isfinite(pa.x) || !isfinite(pb.x) || !isfinite(f.distance)) return false;
+    const float depth = fabsf(f.distance);
+    out = {bp_local_a(p, pa), pb, vneg(f.normal), -depth};
+    return sqrtf(vlen2(vsub(pa, pb))) <= depth + 1.0e-3f;
+}
+__device__ bool run_epa(const BPair& p, const Sup* simplex, int sc, Cand& out) {
+    Sup vtx[64];
+    int vc = sc;
+    for (int i = 0; i < sc; ++i) vtx[i] = simplex[i];
+    Facet facets[64];
+    int fc = 0;
+    if (!init_epa(p, vtx, vc, facets, fc)) return false;
+    const float eps = 0.1f * smin(box_min_margin(p.ha), box_min_margin(p.hb));
+    int bfrom[32], bto[32];
+    float upper = FLT_MAX;
+    for (int it = 0; it < 60; ++it) {
+        int closest = -1;
+        float dist = FLT_MAX;
+        for (int i = 0; i < fc; ++i)
+            if (facets[i].valid && facets[i].in_heap && facets[i].distance < dist) {
+                closest = i;
+                dist = facets[i].distance;
+            }
+        if (closest < 0) return false;
+        const Facet sel = facets[closest];
+        const Sup np = bp_support(p, sel.normal);
+        const float proj = vdot(np.q, sel.normal);
+        if (fabsf(proj - dist) <= eps) return contact_from_facet(p, vtx, sel, out);
+        if (vc == 64) return false;
+        upper = smin(upper, proj);
+        for (int i = 0; i < vc; ++i)
+            if (vtx[i].ai == np.ai && vtx[i].bi == np.bi) return contact_from_facet(p, vtx, sel, out);
+        const int ni = vc++;
+        vtx[ni] = np;
+        int bc = 0;
+        for (int i = 0; i < fc; ++i) {
+            Facet& f = facets[i];
+            if (!f.valid) continue;
+            if (vdot(f.normal, vsub(np.q, vtx[f.i].q)) < 0.0f) continue;
+            f.valid = false;
+            const int ef[3] = {f.i, f.j, f.k}, et[3] = {f.j, f.k, f.i};
+            for (int e = 0; e < 3; ++e) {
+                int rev = -1;
+                for (int j = 0; j < bc; ++j)
+                    if (bfrom[j] == et[e] && bto[j] == ef[e]) { rev = j; break; }
+                if (rev >= 0) {
+                    --bc;
+                    bfrom[rev] = bfrom[bc];
+                    bto[rev] = bto[bc];
+                } else {
+                    if (bc == 32) return false;
+                    bfrom[bc] = ef[e];
+                    bto[bc] = et[e];
+                    ++bc;
+                }
+            }
+        }
+        if (bc == 0) return false;
+        int avail = 64 - fc;
+        for (int i = 0; i < fc; ++i) avail += !facets[i].valid;
+        if (bc > avail) return false;
+        for (int i = 0; i < bc; ++i) {
+            Facet f = make_facet(vtx, bfrom[i], bto[i], ni);
+            if (!f.valid) return false;
+            f.in_heap = f.distance <= upper;
+            int slot = -1;
+            for (int j = 0; j < fc; ++j)
+                if (!facets[j].valid) { slot = j; break; }
+            if (slot < 0) slot = fc++;
+            facets[slot] = f;
+        }
+    }
+    return false;
+}
+__device__ bool gjk_epa(const BPair& p, float cd, Cand& out) {
+    const float eps = 0.1f * smin(box_min_margin(p.ha), box_min_margin(p.hb));
+    const float progress = 1.0f - 0.000225f;
+    Sup simplex[4];
+    int count = 0;
+    v3 closest = vlen2(p.a_in_b) > 0.0f ? p.a_in_b : v3{1, 0, 0};
+    float previous = FLT_MAX;
+    for (int it = 0; it < 32; ++it) {
+        const float dist = sqrtf(vlen2(closest));
+        if (count > 0 && dist <= eps) return run_epa(p, simplex, count, out);
+        if (dist <= 0.0f) return false;
+        const v3 normal = vmul(closest, 1.0f / dist);
+        const Sup s = bp_support(p, vneg(closest));
+        const float proj = vdot(normal, s.q);
+        if (proj > cd) return false;
+        if (count > 0 && proj > dist * progress) {
+            const Closest cur = closest_simplex(simplex, count);
+            return cur.mask && contact_from_gjk(p, cur, out);
+        }
+        for (int i = 0; i < count; ++i)
+            if (s.ai == simplex[i].ai && s.bi == simplex[i].bi) {
+                if (proj > 0.f) {
+                    const Closest cur = closest_simplex(simplex, count);
+                    return cur.mask && contact_from_gjk(p, cur, out) && out.sep <= cd;
+                }
+                return false;
+            }
+        if (count == 4) return run_epa(p, simplex, count, out);
+        simplex[count++] = s;
+        const Closest nx = closest_simplex(simplex, count);
+        if (!nx.mask) return false;
+        closest = nx.point;
+        const float nd = sqrtf(nx.dist2);
+        compact_simplex(simplex, count, nx);
+        if (nd >= previous) return false;
+        previous = nd;
+    }
+    return false;
+}
+__device__ bool box_box_gjk_epa(v3 h0, v3 p0, qt q0, v3 h1, v3 p1, qt q1, float cd, Cand& out) {
+    BPair p;
+    p.ha = h0;
+    p.hb = h1;
+    p.a_in_b = rotinv_gu(q1, vsub(p0, p1));
+    p.rel = qmul(qconj(q1), q0);
+    out = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0.0f};
+    if (!gjk_epa(p, cd, out)) return false;
+    return out.sep <= cd;
+}
+
+// ---------------- persistent manifolds ----------------
+__device__ __forceinline__ v3 lv(const float* f) { return {f[0], f[1], f[2]}; }
+__device__ __forceinline__ void sv(float* f, v3 v) { f[0] = v.x; f[1] = v.y; f[2] = v.z; }
+__device__ __forceinline__ PcmPoint to_pt(const Cand& c) {
+    PcmPoint p;
+    sv(p.la, c.la); sv(p.lb, c.lb); sv(p.nb, c.nb); p.sep = c.sep;
+    return p;
+}
+__device__ __forceinline__ uint32_t cache_count(const PcmCache& c) { return c.meta & 255u; }
+__device__ __forceinline__ bool cache_init(const PcmCache& c) { return (c.meta >> 8) & 1u; }
+__device__ __forceinline__ void set_meta(PcmCache& c, uint32_t count, bool init) {
+    c.meta = count | (init ? 256u : 0u);
+}
+
+__device__ void refresh_points(PcmCache& c, v3 pa_in_b, qt ra_in_b, float brk) {
+    const float brk2 = brk * brk;
+    uint32_t count = cache_count(c);
+    for (uint32_t i = count; i > 0; --i) {
+        PcmPoint& pt = c.pts[i - 1];
+        const v3 rr = rot_sc(ra_in_b, lv(pt.la));
+        const v3 lab = {pa_in_b.x + rr.x, pa_in_b.y + rr.y, pa_in_b.z + rr.z};
+        const v3 nb = lv(pt.nb), lb = lv(pt.lb);
+        const v3 v = {lab.x - lb.x, lab.y - lb.y, lab.z - lb.z};
+        const float dist = v.x * nb.x + v.y * nb.y + v.z * nb.z;
+        const v3 pd = {v.x - nb.x * dist, v.y - nb.y * dist, v.z - nb.z * dist};
+        const float t2 = pd.x * pd.x + pd.y * pd.y + pd.z * pd.z;
+        if (t2 > brk2) c.pts[i - 1] = c.pts[--count];
+        else pt.sep = dist;
+    }
+    c.meta = (c.meta & ~255u) | count;
+}
+__device__ float seg_sq(v3 p, v3 a, v3 b) {
+    const v3 ab = vsub(b, a), ap = vsub(p, a);
+    const float den = vlen2(ab);
+    const float t = den == 0.0f ? 0.0f : sclamp(vdot(ap, ab) / den, 0.0f, 1.0f);
+    const v3 d = {ap.x - t * ab.x, ap.y - t * ab.y, ap.z - t * ab.z};
+    return vlen2(d);
+}
+__device__ float tri_sq(v3 p, v3 a, v3 b, v3 c) {
+    const v3 ab = vsub(b, a), ac = vsub(c, a);
+    const v3 ap = vsub(p, a), bp = vsub(p, b), cp = vsub(p, c);
+    const float d1 = vdot(ab, ap), d2 = vdot(ac, ap);
+    const float d3 = vdot(ab, bp), d4 = vdot(ac, bp);
+    const float d5 = vdot(ab, cp), d6 = vdot(ac, cp);
+    if (d1 < 0.0f && d2 < 0.0f) return vlen2(ap);
+    if (d3 >= 0.0f && d3 >= d4) return vlen2(bp);
+    if (d6 >= 0.0f && d6 >= d5) return vlen2(cp);
+    const float vc = d1 * d4 - d3 * d2;
+    if (vc < 0.0f && d1 >= 0.0f && d3 < 0.0f) return seg_sq(p, a, b);
+    const float va = d3 * d6 - d5 * d4;
+    if (va < 0.0f && d4 >= d3 && d5 >= d6) return seg_sq(p, b, c);
+    const float vb = d5 * d2 - d1 * d6;
+    if (vb < 0.0f && d2 >= 0.0f && d6 < 0.0f) return seg_sq(p, a, c);
+    const v3 n = {ab.y * ac.z - ab.z * ac.y, ab.z * ac.x - ab.x * ac.z, ab.x * ac.y - ab.y * ac.x};
+    const float den = vlen2(n);
+    if (den == 0.0f) return 0.0f;
+    const float pr = vdot(n, ap);
+    return pr * pr / den;
+}
+__device__ void reduce_five(PcmCache& c, const PcmPoint& nw) {
+    PcmPoint cand[5];
+    bool chosen[5] = {false, false, false, false, false};
+    int sel[4] = {0, 0, 0, 0};
+    for (int i = 0; i < 4; ++i) cand[i] = c.pts[i];
+    cand[4] = nw;
+    int deepest = 4;
+    for (int i = 0; i < 4; ++i)
+        if (cand[i].sep < cand[deepest].sep) deepest = i;
+    sel[0] = deepest;
+    chosen[deepest] = true;
+    int farthest = 0;
+    float largest = vlen2(vsub(lv(cand[0].lb), lv(cand[deepest].lb)));
+    for (int i = 1; i < 5; ++i)
+        if (!chosen[i]) {
+            const float v = vlen2(vsub(lv(cand[i].lb), lv(cand[deepest].lb)));
+            if (v > largest) { largest = v; farthest = i; }
+        }
+    sel[1] = farthest;
+    chosen[farthest] = true;
+    largest = -FLT_MAX;
+    int third = 0;
+    for (int i = 0; i < 5; ++i)
+        if (!chosen[i]) {
+            const float v = seg_sq(lv(cand[i].lb), lv(cand[deepest].lb), lv(cand[farthest].lb));
+            if (v > largest) { largest = v; third = i; }
+        }
+    sel[2] = third;
+    chosen[third] = true;
+    largest = -FLT_MAX;
+    int fourth = third;
+    for (int i = 0; i < 5; ++i)
+        if (!chosen[i]) {
+            const float v = tri_sq(lv(cand[i].lb), lv(cand[sel[0]].lb), lv(cand[sel[1]].lb), lv(cand[sel[2]].lb));
+            if (v > largest) { largest = v; fourth = i; }
+        }
+    if (chosen[fourth]) {
+        for (int i = 0; i < 3; ++i) c.pts[i] = cand[sel[i]];
+        c.meta = (c.meta & ~255u) | 3u;
+        return;
+    }
+    sel[3] = fourth;
+    chosen[fourth] = true;
+    for (int i = 0; i < 4; ++i) c.pts[i] = cand[sel[i]];
+    c.meta = (c.meta & ~255u) | 4u;
+    int un = -1;
+    for (int i = 0; i < 5; ++i)
+        if (!chosen[i]) { un = i; break; }
+    if (un < 0) return;
+    float closest = FLT_MAX;
+    int rep = 0;
+    for (int i = 0; i < 4; ++i) {
+        const float d = vlen2(vsub(lv(c.pts[i].la), lv(cand[un].la)));
+        if (d < closest) { closest = d; rep = i; }
+    }
+    if (cand[un].sep < c.pts[rep].sep) c.pts[rep] = cand[un];
+}
+__device__ __forceinline__ float pcm_box_margin(v3 h) { return smin(0.15f * smin(smin(h.x, h.y), h.z), 0.15f); }
+
+// Returns the emitted count, or -1 on an invalid manifold normal / overflow.
+__device__ int generate_box_box(v3 h0, v3 p0, qt q0, v3 h1, v3 p1, qt q1, float cd, PcmCache& cache,
+                                ContactPt* out) {
+    const v3 delta = {p0.x - p1.x, p0.y - p1.y, p0.z - p1.z};
+    const v3 relative = rotinv_sc(q1, delta);
+    const qt rotation = qmul(qconj(q1), q0);
+    const float mm = smin(pcm_box_margin(h0), pcm_box_margin(h1));
+    const uint32_t initial = cache_count(cache);
+    refresh_points(cache, relative, rotation, mm * 0.8f);
+    const bool lost = cache_count(cache) != initial;
+    const float thr[5] = {0.5f, 0.125f, 0.25f, 0.375f, 0.375f};
+    const float qthr[5] = {0.9998f, 0.9999f, 0.9999f, 0.9999f, 0.9999f};
+    const bool init = cache_init(cache);
+    float tdelta = INFINITY;
+    if (init)
+        tdelta = smax(smax(fabsf(relative.x - cache.rel_p[0]), fabsf(relative.y - cache.rel_p[1])),
+                      fabsf(relative.z - cache.rel_p[2]));
+    const float qa = qdot(q0, {cache.qa[0], cache.qa[1], cache.qa[2], cache.qa[3]});
+    const float qb = qdot(q1, {cache.qb[0], cache.qb[1], cache.qb[2], cache.qb[3]});
+    const uint32_t cc = cache_count(cache);
+    const float tp = mm * thr[cc];
+    bool regen = !init || lost || tdelta > tp || qa < qthr[cc] || qb < qthr[cc];
+    if (!regen) {
+        const float a0 = qa < 1.0f ? acosf(smax(-1.0f, qa)) : 0.0f;
+        const float a1 = qb < 1.0f ? acosf(smax(-1.0f, qb)) : 0.0f;
+        regen = a0 * sqrtf(h0.x * h0.x + h0.y * h0.y + h0.z * h0.z) > tp ||
+                a1 * sqrtf(h1.x * h1.x + h1.y * h1.y + h1.z * h1.z) > tp;
+    }
+    bool direct = false, gjk = false;
+    v3 gjk_n = {0, 0, 0};
+    if (regen) {
+        sv(cache.rel_p, relative);
+        cache.rel_q[0] = rotation.x; cache.rel_q[1] = rotation.y; cache.rel_q[2] = rotation.z; cache.rel_q[3] = rotation.w;
+        cache.qa[0] = q0.x; cache.qa[1] = q0.y; cache.qa[2] = q0.z; cache.qa[3] = q0.w;
+        cache.qb[0] = q1.x; cache.qb[1] = q1.y; cache.qb[2] = q1.z; cache.qb[3] = q1.w;
+        set_meta(cache, cache_count(cache), true);
+        Cand cands[64];
+        int count = 0;
+        const int ov = box_box_candidates(h0, p0, q0, h1, p1, q1, cd, cands, count);
+        if (ov < 0) return -1;
+        if (ov == 0) {
+            set_meta(cache, 0, true);
+            return 0;
+        }
+        if (count == 0) {
+            Cand w;
+            if (!box_box_gjk_epa(h0, p0, q0, h1, p1, q1, cd, w)) {
+                set_meta(cache, 0, true);
+                return 0;
+            }
+            gjk = true;
+            gjk_n = w.nb;
+            const float rb = mm * 0.05f;
+            const float rsq = rb * rb;
+            bool replaced = false;
+            const uint32_t n0 = cache_count(cache);
+            for (uint32_t i = 0; i < n0; ++i) {
+                const PcmPoint& o = cache.pts[i];
+                if (smin(vlen2(vsub(lv(o.la), w.la)), vlen2(vsub(lv(o.lb), w.lb))) < rsq) {
+                    cache.pts[i] = to_pt(w);
+                    replaced = true;
+                    break;
+                }
+            }
+            if (!replaced) {
+                if (n0 < 4) {
+                    cache.pts[n0] = to_pt(w);
+                    set_meta(cache, n0 + 1, true);
+                } else {
+                    reduce_five(cache, to_pt(w));
+                }
+            }
+        } else if (count <= 4) {
+            for (int i = 0; i < count; ++i) cache.pts[i] = to_pt(cands[i]);
+            set_meta(cache, uint32_t(count), true);
+        } else {
+            int sel[4];
+            batch_selection(cands, count, 1.0f, sel);
+            for (int i = 0; i < 4; ++i) cache.pts[i] = to_pt(cands[sel[i]]);
+            set_meta(cache, 4, true);
+        }
+        direct = count > 0;
+    }
+    const uint32_t n = cache_count(cache);
+    if (n == 0) return 0;
+    v3 nb = {0, 0, 0};
+    if (gjk) nb = gjk_n;
+    else if (direct) nb = lv(cache.pts[0].nb);
+    else
+        for (uint32_t i = 0; i < n; ++i) {
+            nb.x += cache.pts[i].nb[0];
+            nb.y += cache.pts[i].nb[1];
+            nb.z += cache.pts[i].nb[2];
+        }
+    const float nsq = nb.x * nb.x + nb.y * nb.y + nb.z * nb.z;
+    if (!(nsq > 0.0f) || !isfinite(nsq)) return -1;
+    const float il = 1.0f / sqrtf(nsq);
+    const v3 normal = rot_sc(q1, {nb.x * il, nb.y * il, nb.z * il});
+    int emitted = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const PcmPoint& p = cache.pts[i];
+        if (!direct && p.sep > cd) continue;
+        const v3 r = rot_sc(q1, lv(p.lb));
+        ContactPt& o = out[emitted++];
+        o.p[0] = r.x + p1.x; o.p[1] = r.y + p1.y; o.p[2] = r.z + p1.z;
+        o.n[0] = normal.x; o.n[1] = normal.y; o.n[2] = normal.z;
+        o.sep = p.sep;
+    }
+    return emitted;
+}
+
+__device__ int generate_plane_box(v3 pp, v3 h, v3 bp, qt q, float cd, PcmCache& cache, ContactPt* out) {
+    const v3 rel = {bp.x - pp.x, bp.y - pp.y, bp.z - pp.z};
+    const float margin = pcm_box_margin(h);
+    const float brk = margin * 0.2f;
+    const uint32_t prev = cache_count(cache);
+    refresh_points(cache, rel, q, brk);
+    const bool init = cache_init(cache);
+    float md = INFINITY;
+    if (init)
+        md = smax(smax(fabsf(rel.x - cache.rel_p[0]), fabsf(rel.y - cache.rel_p[1])), fabsf(rel.z - cache.rel_p[2]));
+    const float rd = q.x * cache.rel_q[0] + q.y * cache.rel_q[1] + q.z * cache.rel_q[2] + q.w * cache.rel_q[3];
+    const bool regen = !init || cache_count(cache) != prev || md > brk || rd < 0.99996f;
+    if (regen) {
+        sv(cache.rel_p, rel);
+        cache.rel_q[0] = q.x; cache.rel_q[1] = q.y; cache.rel_q[2] = q.z; cache.rel_q[3] = q.w;
+        Cand cands[8];
+        int n = 0;
+        for (unsigned corner = 0; corner < 8u; ++corner) {
+            const v3 local = {(corner & 4u) ? -h.x : h.x, (corner & 2u) ? -h.y : h.y, (corner & 1u) ? -h.z : h.z};
+            const v3 r = rot_sc(q, local);
+            const v3 ip = {rel.x + r.x, rel.y + r.y, rel.z + r.z};
+            if (ip.y >= cd) continue;
+            cands[n++] = {local, {ip.x, 0.0f, ip.z}, {0.0f, 1.0f, 0.0f}, ip.y};
+        }
+        if (n <= 4) {
+            for (int i = 0; i < n; ++i) cache.pts[i] = to_pt(cands[i]);
+            set_meta(cache, uint32_t(n), true);
+        } else {
+            bool chosen[8] = {false, false, false, false, false, false, false, false};
+            int idx[4];
+            int first = 0;
+            for (int i = 1; i < n; ++i)
+                if (cands[i].sep < cands[first].sep) first = i;
+            idx[0] = first;
+            chosen[first] = true;
+            int far = 0;
+            float maxd = vlen2(vsub(cands[0].lb, cands[first].lb));
+            for (int i = 1; i < n; ++i) {
+                const float d = vlen2(vsub(cands[i].lb, cands[first].lb));
+                if (d > maxd) { maxd = d; far = i; }
+            }
+            idx[1] = far;
+            chosen[far] = true;
+            const v3 seg = vsub(cands[far].lb, cands[first].lb);
+            v3 side = {-seg.z, 0.0f, seg.x};
+            const float ns = vlen2(side);
+            if (ns > 0.0f) {
+                const float inv = 1.0f / sqrtf(ns);
+                side = {side.x * inv, 0.0f, side.z * inv};
+            } else {
+                side = {0.0f, 1.0f, 0.0f};
+            }
+            float largest = -FLT_MAX, smallest = FLT_MAX;
+            int third = 0, fourth = 0;
+            for (int i = 0; i < n; ++i) {
+                if (chosen[i]) continue;
+                const float d = vdot(vsub(cands[i].lb, cands[first].lb), side);
+                if (d > largest) { largest = d; third = i; }
+                if (d < smallest) { smallest = d; fourth = i; }
+            }
+            idx[2] = third;
+            chosen[third] = true;
+            if (smallest * largest > 0.0f) {
+                largest = -FLT_MAX;
+                for (int i = 0; i < n; ++i) {
+                    if (chosen[i]) continue;
+                    const float d = vdot(vsub(cands[i].lb, cands[first].lb), side);
+                    if (d > largest) { largest = d; fourth = i; }
+                }
+            }
+            idx[3] = fourth;
+            chosen[fourth] = true;
+            Cand centers[4];
+            for (int k = 0; k < 4; ++k) centers[k] = cands[idx[k]];
+            for (int i = 0; i < n; ++i) {
+                if (chosen[i]) continue;
+                float nearest = FLT_MAX;
+                int slot = 0;
+                for (int j = 0; j < 4; ++j) {
+                    const float d = vlen2(vsub(cands[i].lb, centers[j].lb));
+                    if (d < nearest) { nearest = d; slot = j; }
+                }
+                if (cands[i].sep < cands[idx[slot]].sep) idx[slot] = i;
+            }
+            for (int k = 0; k < 4; ++k) cache.pts[k] = to_pt(cands[idx[k]]);
+            set_meta(cache, 4, true);
+        }
+    }
+    int emitted = 0;
+    const uint32_t n = cache_count(cache);
+    for (uint32_t k = 0; k < n; ++k) {
+        const PcmPoint& pt = cache.pts[k];
+        if (pt.sep > cd) continue;
+        ContactPt& o = out[emitted++];
+        o.p[0] = pp.x + pt.lb[0]; o.p[1] = pp.y; o.p[2] = pp.z + pt.lb[2];
+        // Plane manifolds are published with the flipped (+y) normal
+        // (scene.cpp:4670-4677).
+        o.n[0] = 0.0f; o.n[1] = 1.0f; o.n[2] = 0.0f;
+        o.sep = pt.sep;
+    }
+    return emitted;
+}
+
+__device__ int sphere_sphere(v3 a, float r0, v3 b, float r1, float cd, ContactPt& o) {
+    const v3 delta = vsub(a, b);
+    const float d2 = vdot(delta, delta);
+    const float rs = r0 + r1;
+    const float infl = rs + cd;
+    if (!(infl * infl > d2)) return 0;
+    const float dist = sqrtf(d2);
+    const v3 n = dist <= 0.00001f ? v3{1, 0, 0} : vmul(delta, 1.0f / dist);
+    const v3 p = vadd(b, vmul(n, r1));
+    o.p[0] = p.x; o.p[1] = p.y; o.p[2] = p.z;
+    o.n[0] = n.x; o.n[1] = n.y; o.n[2] = n.z;
+    o.sep = dist - rs;
+    return 1;
+}
+__device__ int sphere_plane(v3 c, float r, float ph, float cd, ContactPt& o) {
+    const float sep = c.y - ph - r;
+    if (!(cd >= sep)) return 0;
+    o.p[0] = c.x; o.p[1] = c.y - r; o.p[2] = c.z;
+    o.n[0] = 0.f; o.n[1] = 1.f; o.n[2] = 0.f;   // two flips cancel (scene.cpp:4474-4482, 4670)
+    o.sep = sep;
+    return 1;
+}
+__device__ int sphere_box(v3 center, float r, v3 h, v3 bc, qt bq, float cd, ContactPt& o) {
+    const v3 local = rotinv_gu(bq, vsub(center, bc));
+    const v3 cl = {sclamp(local.x, -h.x, h.x), sclamp(local.y, -h.y, h.y), sclamp(local.z, -h.z, h.z)};
+    const v3 gap = vsub(local, cl);
+    const float l2 = vdot(gap, gap);
+    const float infl = r + cd;
+    if (!(infl * infl > l2)) return 0;
+    const bool inside = fabsf(local.x) <= h.x && fabsf(local.y) <= h.y && fabsf(local.z) <= h.z;
+    v3 p, n;
+    float sep;
+    if (inside) {
+        const v3 d = {h.x - fabsf(cl.x), h.y - fabsf(cl.y), h.z - fabsf(cl.z)};
+        v3 nl;
+        float depth;
+        if (d.z <= d.x && d.z <= d.y) { nl = {0, 0, cl.z >= 0.f ? 1.f : -1.f}; depth = d.z; }
+        else if (d.x <= d.y && d.x <= d.z) { nl = {cl.x >= 0.f ? 1.f : -1.f, 0, 0}; depth = d.x; }
+        else { nl = {0, cl.y >= 0.f ? 1.f : -1.f, 0}; depth = d.y; }
+        n = rot_gu(bq, nl);
+        p = vadd(center, vmul(n, depth));
+        sep = -depth - r;
+    } else {
+        const float len = sqrtf(l2);
+        n = rot_gu(bq, vmul(gap, 1.f / len));
+        p = vadd(bc, rot_gu(bq, cl));
+        sep = len - r;
+    }
+    o.p[0] = p.x; o.p[1] = p.y; o.p[2] = p.z;
+    o.n[0] = n.x; o.n[1] = n.y; o.n[2] = n.z;
+    o.sep = sep;
+    return 1;
+}
+
+__global__ void __launch_bounds__(128) k_narrowphase(DevState s) {
+    const uint32_t n = *s.cur.n;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+        const uint64_t key = s.cur.key[k];
+        const uint32_t sa = uint32_t(key >> 32), sb = uint32_t(key);
+        const int32_t pj = s.prev_idx[k];
+        PcmCache cache;
+        if (pj >= 0) cache = s.prev.cache[pj];
+        else cache.meta = 0u;
+        const uint32_t ta = s.s_type[sa], tb = s.s_type[sb];
+        const uint32_t ba = s.s_body[sa], bb = s.s_body[sb];
+        const bool da = s.b_flags[ba] & kBodyDynamic, db = s.b_flags[bb] & kBodyDynamic;
+        // ScNPhaseCore::shouldSwapBodies orientation (scene.cpp:3275-3283)
+        const bool reversed = !da || (da && db && ba < bb);
+        const bool plane = ta == kPlane || tb == kPlane;
+        const bool sphere = ta == kSphere || tb == kSphere;
+        const uint32_t first = plane ? (ta == kPlane ? sa : sb) : (reversed ? sb : sa);
+        const uint32_t second = plane ? (ta == kPlane ? sb : sa) : (reversed ? sa : sb);
+        const float cd = s.s_lp[sa].w + s.s_lp[sb].w;
+        ContactPt out[4];
+        int count = 0;
+        const v3 p0 = ld3(s.s_wp[first]), p1 = ld3(s.s_wp[second]);
+        const qt q0 = ldq(s.s_wq[first]), q1 = ldq(s.s_wq[second]);
+        const float4 g0 = s.s_geom[first], g1 = s.s_geom[second];
+        if (plane && !sphere) {
+            count = generate_plane_box(p0, {g1.x, g1.y, g1.z}, p1, q1, cd, cache, out);
+        } else if (!plane && !sphere) {
+            count = generate_box_box({g0.x, g0.y, g0.z}, p0, q0, {g1.x, g1.y, g1.z}, p1, q1, cd, cache, out);
+        } else {
+            const uint32_t sp = ta == kSphere ? sa : sb;
+            const v3 c = ld3(s.s_wp[sp]);
+            const float r = s.s_geom[sp].w;
+            if (plane) {
+                count = sphere_plane(c, r, p0.y, cd, out[0]);
+            } else if (ta == kSphere && tb == kSphere) {
+                count = sphere_sphere(p0, g0.w, p1, g1.w, cd, out[0]);
+            } else {
+                const uint32_t bx = ta == kBox ? sa : sb;
+                const float4 gb = s.s_geom[bx];
+                count = sphere_box(c, r, {gb.x, gb.y, gb.z}, ld3(s.s_wp[bx]), ldq(s.s_wq[bx]), cd, out[0]);
+                if (count && s.s_type[first] == kBox) {
+                    out[0].n[0] = -out[0].n[0]; out[0].n[1] = -out[0].n[1]; out[0].n[2] = -out[0].n[2];
+                }
+            }
+        }
+        if (count < 0) {
+            atomicOr(s.err, kErrContactOverflow);
+            count = 0;
+        }
+        s.cur.cache[k] = cache;
+        s.cur.count[k] = uint32_t(count);
+        for (int i = 0; i < count; ++i) s.pts[4 * size_t(k) + i] = out[i];
+        // friction history follows its manager
+        if (pj >= 0) s.cur.fric[k] = s.prev.fric[pj];
+        else s.cur.fric[k].epoch = 0u;
+    }
+}
+
+}  // namespace
+
+void enqueue_narrowphase(const DevState& s, cudaStream_t st) {
+    const int T = 128;
+    const uint32_t blocks = (s.pair_cap + T - 1) / T;
+    k_narrowphase<<<blocks < 148u * 16u ? blocks : 148u * 16u, T, 0, st>>>(s);
+}
+
+}  // namespace fyzz::b200

@@ -1,0 +1,787 @@
+// Dy: unconstrained velocities, solver bodies, islands, conflict-free
+// partitions, contact / friction / distance row preparation, PGS and pose
+// integration.
+//
+// Reference routines (src/native/scene.cpp):
+//   prepare_unconstrained_velocities  10383-10507
+//   prepare_solver_bodies             6940-7110 (sqrt inverse inertia in world)
+//   partition_constraints             7113-7488 (greedy first-fit 32-bit masks,
+//                                       overflow waves, statics after the body's
+//                                       last dynamic partition)
+//   prepare_constraints               7490-8510 (distance rows, material
+//                                       combine, friction correlation and anchor
+//                                       growth, contact and tangent rows)
+//   solve_constraint_task             8853-9148 (4 biased + 1 velocity pass,
+//                                       friction on the last three position passes)
+//   publish_solver_bodies / integrate 9509-9548, 10508-10707
+//
+// B200 mapping.  Descriptors are the distance joints (constraint slot
+// descending) followed by the touching managers in pair order.  A lock-free
+// union-find groups them into islands; a stable radix sort by island root
+// keeps each island's descriptors in that order, so the per-island greedy
+// partition is exactly the reference's per-task greedy (islands share no
+// dynamic body).  PGS runs one warp (small islands) or one CTA (large
+// islands) per island, sweeping its partitions in order with warp / block
+// barriers only: no grid-wide synchronisation and no host round trip.
+#include "state.h"
+#include <cfloat>
+
+namespace fyzz::b200 {
+
+namespace {
+constexpr uint32_t kInvalid = 0xffffffffu;
+constexpr int kMaxLevels = 256;
+constexpr uint32_t kSmallIsland = 96;
+
+__device__ __forceinline__ bool is_dyn(const DevState& s, uint32_t b) { return s.b_flags[b] & kBodyDynamic; }
+
+__device__ __forceinline__ v3 mass_position(const DevState& s, uint32_t b) {
+    return vadd(ld3(s.b_p[b]), rot_sc(ldq(s.b_q[b]), ld3(s.b_ml_p[b])));
+}
+__device__ __forceinline__ qt mass_orientation(const DevState& s, uint32_t b) {
+    return qmul(ldq(s.b_q[b]), ldq(s.b_ml_q[b]));
+}
+
+__global__ void k_frame_begin(DevState s) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) s.counters[kCntFrame] += 1u;
+}
+
+// Unconstrained velocity + solver-body data for every dynamic body.
+__global__ void k_bodies_begin(DevState s) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= s.n_bodies) return;
+    s.uf_parent[b] = b;
+    s.sb_mask[b] = 0u;
+    s.sb_maxdyn[b] = 0u;
+    s.sb_static[b] = 0u;
+    const float4 z = make_float4(0, 0, 0, 0);
+    s.sb_dv[b] = z; s.sb_dw[b] = z; s.sb_mdv[b] = z; s.sb_mdw[b] = z;
+    if (!is_dyn(s, b)) return;
+    const float dt = s.dt;
+    const float gravity = -9.81f;
+    const float4 d0 = s.b_dyn0[b];
+    v3 v = ld3(s.b_v[b]);
+    float vx = v.x, vy = v.y + gravity * dt, vz = v.z;
+    const float lm = smax(1.0f - d0.x * dt, 0.0f);
+    vx *= lm; vy *= lm; vz *= lm;
+    v3 w = ld3(s.b_w[b]);
+    const float am = smax(1.0f - d0.y * dt, 0.0f);
+    w.x *= am; w.y *= am; w.z *= am;
+    const float s2 = vx * vx + vy * vy + vz * vz;
+    const float ml2 = d0.z * d0.z, ma2 = d0.w * d0.w;
+    if (s2 > ml2) {
+        const float f = sqrtf(ml2 / s2);
+        vx *= f; vy *= f; vz *= f;
+    }
+    const float w2 = w.x * w.x + w.y * w.y + w.z * w.z;
+    if (w2 > ma2) {
+        const float f = sqrtf(ma2 / w2);
+        w.x *= f; w.y *= f; w.z *= f;
+    }
+    if (!(isfinite(vx) && isfinite(vy) && isfinite(vz) && vfinite(w))) atomicOr(s.err, kErrNonFinite);
+    s.b_v[b] = make_float4(vx, vy, vz, 0.0f);
+    s.b_w[b] = st4(w, 0.0f);
+    s.sb_v[b] = make_float4(vx, vy, vz, 0.0f);
+    s.sb_w[b] = st4(w, 0.0f);
+    const float4 inv = s.b_inv[b];
+    const v3 l = {sqrtf(inv.x), sqrtf(inv.y), sqrtf(inv.z)};
+    const qt q = mass_orientation(s, b);
+    float4* si = s.sb_sqrt_i + 3 * size_t(b);
+    if (q.x == 0.0f && q.y == 0.0f && q.z == 0.0f && q.w == 1.0f) {
+        si[0] = make_float4(l.x, 0, 0, 0); si[1] = make_float4(0, l.y, 0, 0); si[2] = make_float4(0, 0, l.z, 0);
+        return;
+    }
+    const v3 rx = rot_sc(q, {1, 0, 0}), ry = rot_sc(q, {0, 1, 0}), rz = rot_sc(q, {0, 0, 1});
+    const float xx = l.x * rx.x * rx.x + l.y * ry.x * ry.x + l.z * rz.x * rz.x;
+    const float yy = l.x * rx.y * rx.y + l.y * ry.y * ry.y + l.z * rz.y * rz.y;
+    const float zz = l.x * rx.z * rx.z + l.y * ry.z * ry.z + l.z * rz.z * rz.z;
+    const float xy = l.x * rx.x * rx.y + l.y * ry.x * ry.y + l.z * rz.x * rz.y;
+    const float xz = l.x * rx.x * rx.z + l.y * ry.x * ry.z + l.z * rz.x * rz.z;
+    const float yz = l.x * rx.y * rx.z + l.y * ry.y * ry.z + l.z * rz.y * rz.z;
+    si[0] = make_float4(xx, xy, xz, 0); si[1] = make_float4(xy, yy, yz, 0); si[2] = make_float4(xz, yz, zz, 0);
+}
+
+__global__ void k_touch_flags(DevState s, uint32_t* flags) {
+    const uint32_t n = *s.cur.n;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
+        flags[k] = s.cur.count[k] > 0u ? 1u : 0u;
+}
+__global__ void k_touch_scatter(DevState s, const uint32_t* flags, const uint32_t* pos) {
+    const uint32_t n = *s.cur.n;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
+        if (flags[k]) s.man_list[pos[k]] = k;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        s.counters[kCntDesc] = s.n_joints + s.counters[kCntMan];
+}
+
+// Gu-ordered bodies of a touching manager: shape0 (dynamic first) / shape1.
+__device__ __forceinline__ void manager_bodies(const DevState& s, uint32_t pair, uint32_t& sh0, uint32_t& sh1) {
+    const uint64_t key = s.cur.key[pair];
+    const uint32_t sa = uint32_t(key >> 32), sb = uint32_t(key);
+    const uint32_t ba = s.s_body[sa], bb = s.s_body[sb];
+    const bool da = is_dyn(s, ba), db = is_dyn(s, bb);
+    const bool reversed = !da || (da && db && ba < bb);
+    sh0 = reversed ? sb : sa;
+    sh1 = reversed ? sa : sb;
+}
+
+__device__ uint32_t uf_find(uint32_t* parent, uint32_t x) {
+    volatile uint32_t* vp = parent;
+    for (int it = 0; it < 1 << 20; ++it) {
+        const uint32_t p = vp[x];
+        if (p == x) return x;
+        const uint32_t gp = vp[p];
+        if (gp != p) atomicCAS(&parent[x], p, gp);
+        x = gp;
+    }
+    return x;
+}
+__device__ void uf_union(const DevState& s, uint32_t a, uint32_t b) {
+    for (int it = 0; it < 4096; ++it) {
+        const uint32_t ra = uf_find(s.uf_parent, a), rb = uf_find(s.uf_parent, b);
+        if (ra == rb) return;
+        const uint32_t hi = max(ra, rb), lo = min(ra, rb);
+        if (atomicCAS(&s.uf_parent[hi], hi, lo) == hi) return;
+    }
+    atomicOr(s.err, kErrUnionFind);
+}
+// Descriptor endpoints: joints use the ordered edge pair (scene.cpp:3154),
+// managers the Gu order.  -1 marks the static world body.
+__device__ __forceinline__ void desc_bodies(const DevState& s, uint32_t d, int32_t& b0, int32_t& b1) {
+    if (d < s.n_joints) {
+        b0 = int32_t(s.j_a[d]);
+        b1 = int32_t(s.j_b[d]);
+    } else {
+        uint32_t sh0, sh1;
+        manager_bodies(s, s.man_list[d - s.n_joints], sh0, sh1);
+        b0 = int32_t(s.s_body[sh0]);
+        b1 = int32_t(s.s_body[sh1]);
+    }
+    if (!is_dyn(s, uint32_t(b0))) b0 = -1;
+    if (!is_dyn(s, uint32_t(b1))) b1 = -1;
+}
+__global__ void k_union(DevState s) {
+    const uint32_t n = s.counters[kCntDesc];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += stride) {
+        int32_t b0, b1;
+        desc_bodies(s, d, b0, b1);
+        if (b0 >= 0 && b1 >= 0) uf_union(s, uint32_t(b0), uint32_t(b1));
+    }
+}
+__global__ void k_desc_keys(DevState s) {
+    const uint32_t n = s.counters[kCntDesc];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += stride) {
+        int32_t b0, b1;
+        desc_bodies(s, d, b0, b1);
+        const uint32_t body = b0 >= 0 ? uint32_t(b0) : uint32_t(b1);
+        s.d_key[d] = uf_find(s.uf_parent, body);
+        s.d_val[d] = d;
+        s.d_level[d] = kInvalid;
+    }
+}
+__global__ void k_island_flags(DevState s) {
+    const uint32_t n = s.counters[kCntDesc];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        s.isl_flag[i] = (i == 0 || s.d_key[i] != s.d_key[i - 1]) ? 1u : 0u;
+}
+__global__ void k_island_scatter(DevState s, const uint32_t* pos) {
+    const uint32_t n = s.counters[kCntDesc];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        if (s.isl_flag[i]) s.isl_begin[pos[i]] = i;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const uint32_t ni = *s.n_isl;
+        s.isl_begin[ni] = n;
+    }
+}
+
+// One thread per island: the reference's sequential greedy partition over
+// the island's descriptors (scene.cpp:7367-7437), then a counting sort of the
+// island's descriptors by partition into d_key2/d_val2 and the partition
+// boundaries into isl_end-based storage.
+__global__ void k_partition(DevState s, uint32_t* lvl_bound) {
+    const uint32_t ni = *s.n_isl;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < ni; isl += stride) {
+        const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
+        uint32_t nlev = 0;
+        bool pending = true;
+        for (uint32_t wave = 0; pending; wave += 32) {
+            if (wave >= kMaxLevels) { atomicOr(s.err, kErrLevelRange); break; }
+            pending = false;
+            if (wave)
+                for (uint32_t i = begin; i < end; ++i) {
+                    const uint32_t d = s.d_val[i];
+                    if (s.d_level[d] != kInvalid) continue;
+                    int32_t b0, b1;
+                    desc_bodies(s, d, b0, b1);
+                    if (b0 < 0 || b1 < 0) continue;
+                    s.sb_mask[b0] = 0u;
+                    s.sb_mask[b1] = 0u;
+                }
+            bool progress = false;
+            for (uint32_t i = begin; i < end; ++i) {
+                const uint32_t d = s.d_val[i];
+                if (s.d_level[d] != kInvalid) continue;
+                int32_t b0, b1;
+                desc_bodies(s, d, b0, b1);
+                if (b0 < 0 || b1 < 0) continue;
+                const uint32_t avail = ~(s.sb_mask[b0] | s.sb_mask[b1]);
+                if (!avail) { pending = true; continue; }
+                const uint32_t bit = __ffs(avail) - 1;
+                s.sb_mask[b0] |= 1u << bit;
+                s.sb_mask[b1] |= 1u << bit;
+                const uint32_t lp = wave + bit;
+                s.sb_maxdyn[b0] = max(s.sb_maxdyn[b0], lp + 1);
+                s.sb_maxdyn[b1] = max(s.sb_maxdyn[b1], lp + 1);
+                s.d_level[d] = lp;
+                nlev = max(nlev, lp + 1);
+                progress = true;
+            }
+            if (pending && !progress) { atomicOr(s.err, kErrPartition); break; }
+        }
+        for (uint32_t i = begin; i < end; ++i) {
+            const uint32_t d = s.d_val[i];
+            if (s.d_level[d] != kInvalid) continue;
+            int32_t b0, b1;
+            desc_bodies(s, d, b0, b1);
+            const int32_t act = b0 >= 0 ? b0 : b1;
+            if (act < 0) continue;
+            const uint32_t lp = s.sb_maxdyn[act] + s.sb_static[act]++;
+            s.d_level[d] = lp;
+            nlev = max(nlev, lp + 1);
+        }
+        if (nlev > kMaxLevels) { atomicOr(s.err, kErrLevelRange); nlev = kMaxLevels; }
+        if (nlev > end - begin) { atomicOr(s.err, kErrLevelRange); nlev = end - begin; }
+        // counting sort by level inside [begin, end), stable in descriptor order
+        uint32_t* bound = lvl_bound + begin + isl;   // nlev + 1 entries
+        for (uint32_t l = 0; l <= nlev; ++l) bound[l] = 0u;
+        for (uint32_t i = begin; i < end; ++i) {
+            const uint32_t l = min(s.d_level[s.d_val[i]], uint32_t(kMaxLevels - 1));
+            ++bound[l + 1];
+        }
+        uint32_t run = begin;
+        for (uint32_t l = 0; l <= nlev; ++l) { run += bound[l]; bound[l] = run; }
+        // bound[l] is now the start of level l; place descriptors
+        for (uint32_t i = begin; i < end; ++i) {
+            const uint32_t d = s.d_val[i];
+            const uint32_t l = min(s.d_level[d], uint32_t(kMaxLevels - 1));
+            s.d_val2[bound[l]++] = d;
+        }
+        // restore level starts: after placement bound[l] = start of level l+1
+        for (uint32_t l = nlev; l > 0; --l) bound[l] = bound[l - 1];
+        bound[0] = begin;
+        s.isl_end[isl] = nlev;
+    }
+}
+
+// ---------------- row preparation ----------------
+struct SBody { v3 v, w, p; float inv_mass; v3 c0, c1, c2; };
+__device__ __forceinline__ SBody load_sbody(const DevState& s, int32_t b) {
+    SBody r;
+    if (b < 0) {
+        r.v = r.w = r.p = {0, 0, 0};
+        r.inv_mass = 0.0f;
+        r.c0 = r.c1 = r.c2 = {0, 0, 0};
+        return r;
+    }
+    r.v = ld3(s.sb_v[b]);
+    r.w = ld3(s.sb_w[b]);
+    r.p = mass_position(s, uint32_t(b));
+    r.inv_mass = s.b_inv[b].w;
+    const float4* si = s.sb_sqrt_i + 3 * size_t(b);
+    r.c0 = ld3(si[0]); r.c1 = ld3(si[1]); r.c2 = ld3(si[2]);
+    return r;
+}
+__device__ __forceinline__ v3 xform(const SBody& d, v3 v) {
+    return {d.c0.x * v.x + d.c1.x * v.y + d.c2.x * v.z,
+            d.c0.y * v.x + d.c1.y * v.y + d.c2.y * v.z,
+            d.c0.z * v.x + d.c1.z * v.y + d.c2.z * v.z};
+}
+
+__global__ void k_prep_joints(DevState s) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= s.n_joints) return;
+    const uint32_t a = s.j_a[j], b = s.j_b[j];
+    const bool da = is_dyn(s, a), db = is_dyn(s, b);
+    const float inv_dt = 1.0f / s.dt;
+    const v3 world0 = ld3(s.b_p[a]), world1 = ld3(s.b_p[b]);   // centre anchors
+    const v3 c0 = mass_position(s, a), c1 = mass_position(s, b);
+    const v3 ra = vsub(world0, c0), rb = vsub(world1, c1);
+    const float m0 = da ? s.b_inv[a].w : 0.0f, m1 = db ? s.b_inv[b].w : 0.0f;
+    const v3 rel = vsub(ld3(s.b_v[a]), ld3(s.b_v[b]));
+    const v3 off = {c0.x + ra.x - c1.x - rb.x, c0.y + ra.y - c1.y - rb.y, c0.z + ra.z - c1.z - rb.z};
+    const float dist = sqrtf(vdot(off, off));
+    const v3 axis = dist < 1.192092896e-07f ? v3{1, 0, 0} : v3{off.x / dist, off.y / dist, off.z / dist};
+    const v3 an0 = vcross(ra, axis), an1 = vcross(rb, axis);
+    const v3 ja = da ? xform(load_sbody(s, int32_t(a)), an0) : v3{0, 0, 0};
+    const v3 jb = db ? xform(load_sbody(s, int32_t(b)), an1) : v3{0, 0, 0};
+    const float response = m0 + m1 + vdot(ja, ja) + vdot(jb, jb);
+    if (!(response > 0.0f) || !isfinite(response)) atomicOr(s.err, kErrLogic);
+    const float rcp = 1.0f / response;
+    JointRow r;
+    r.axis[0] = axis.x; r.axis[1] = axis.y; r.axis[2] = axis.z;
+    r.ang_a[0] = ja.x; r.ang_a[1] = ja.y; r.ang_a[2] = ja.z;
+    r.ang_b[0] = jb.x; r.ang_b[1] = jb.y; r.ang_b[2] = jb.z;
+    r.ima = m0; r.imb = m1;
+    r.vel_mult = -rcp;
+    const float speed = vdot(axis, rel) + vdot(an0, ld3(s.b_w[a])) - vdot(an1, ld3(s.b_w[b]));
+    const float err = dist - s.j_len[j];
+    r.constant = -rcp * (err * inv_dt + speed);
+    r.unbiased = -rcp * speed;
+    r.applied = 0.0f;
+    r.pad = 0.0f;
+    s.jrow[j] = r;
+}
+
+__device__ __forceinline__ v3 lv(const float* f) { return {f[0], f[1], f[2]}; }
+__device__ __forceinline__ void sv(float* f, v3 v) { f[0] = v.x; f[1] = v.y; f[2] = v.z; }
+
+__global__ void k_prep_contacts(DevState s) {
+    const uint32_t nm = s.counters[kCntMan];
+    const uint32_t frame = s.counters[kCntFrame];
+    const float inv_dt = 1.0f / s.dt;
+    const float bias_coeff = 0.8f, bounce = -2.0f, same_normal = 0.999f, fr_thr = 0.04f;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < nm; m += stride) {
+        const uint32_t pair = s.man_list[m];
+        uint32_t sh0, sh1;
+        manager_bodies(s, pair, sh0, sh1);
+        const uint32_t a0 = s.s_body[sh0], a1 = s.s_body[sh1];
+        const int32_t b0 = is_dyn(s, a0) ? int32_t(a0) : -1;
+        const int32_t b1 = is_dyn(s, a1) ? int32_t(a1) : -1;
+        const SBody A = load_sbody(s, b0), B = load_sbody(s, b1);
+        const float4 m0 = s.s_mat[sh0], m1 = s.s_mat[sh1];
+        const float4 d0 = s.b_dyn1[a0], d1 = s.b_dyn1[a1];
+        const float rest_d = m0.w + m1.w;
+        const float maximp = smin(d0.y, d1.y);
+        const float maxpen = -smin(d0.x, d1.x);
+        const float restitution = 0.5f * (m0.z + m1.z);
+        const float damping = 0.0f;
+        const float dfr = smax(0.0f, 0.5f * (m0.y + m1.y));
+        const float sfr = smax(dfr, 0.5f * (m0.x + m1.x));
+        const uint32_t count = s.cur.count[pair];
+        const ContactPt* pts = s.pts + 4 * size_t(pair);
+        const v3 n = lv(pts[0].n);
+        v3 bmin = lv(pts[0].p), bmax = bmin;
+        for (uint32_t j = 1; j < count; ++j) {
+            const v3 p = lv(pts[j].p);
+            bmin = {smin(bmin.x, p.x), smin(bmin.y, p.y), smin(bmin.z, p.z)};
+            bmax = {smax(bmax.x, p.x), smax(bmax.y, p.y), smax(bmax.z, p.z)};
+        }
+        const qt q0 = mass_orientation(s, a0), q1 = mass_orientation(s, a1);
+        const v3 p0 = mass_position(s, a0), p1 = mass_position(s, a1);
+        // correlatePatches: a valid previous anchor patch comes first
+        // (cached_friction_patch_valid, scene.cpp:3981-4011).
+        FrictionHist h = s.cur.fric[pair];
+        bool have_old = false;
+        if (h.epoch != 0u && h.epoch + 1u == frame && (h.meta & 512u)) {
+            bool valid = !((h.meta >> 8) & 1u) && (h.meta & 255u) != 0u;
+            if (valid) {
+                const v3 on = rotinv_sc(q0, rot_sc(q1, lv(h.n1)));
+                if (vdot(lv(h.n0), on) <= same_normal) valid = false;
+                for (uint32_t k = 0; valid && k < (h.meta & 255u); ++k) {
+                    const v3 lc = rot_sc(q1, lv(h.a1[k]));
+                    const v3 wld = {lc.x + p1.x, lc.y + p1.y, lc.z + p1.z};
+                    const v3 in0 = rotinv_sc(q0, {wld.x - p0.x, wld.y - p0.y, wld.z - p0.z});
+                    const v3 dl = {h.a0[k][0] - in0.x, h.a0[k][1] - in0.y, h.a0[k][2] - in0.z};
+                    if (fabsf(vdot(dl, lv(h.n0))) >= 0.025f) valid = false;
+                }
+            }
+            if (valid) {
+                const v3 pn = rot_sc(q0, lv(h.n0));
+                have_old = vdot(pn, n) >= same_normal && h.rest == restitution && h.damping == damping &&
+                           h.sf == sfr && h.df == dfr;
+            }
+        }
+        uint32_t anchors = 0;
+        v3 a0l[2], a1l[2];
+        v3 patch_n0, patch_n1;
+        if (have_old) {
+            anchors = h.meta & 255u;
+            a0l[0] = lv(h.a0[0]); a0l[1] = lv(h.a0[1]);
+            a1l[0] = lv(h.a1[0]); a1l[1] = lv(h.a1[1]);
+            patch_n0 = lv(h.n0);
+            patch_n1 = lv(h.n1);
+        } else {
+            a0l[0] = a0l[1] = a1l[0] = a1l[1] = {0, 0, 0};
+            patch_n0 = rotinv_sc(q0, n);
+            patch_n1 = rotinv_sc(q1, n);
+        }
+        // contact rows in Gu point order (one patch, one run)
+        NormalRow* rows = s.nrow + 4 * size_t(m);
+        for (uint32_t j = 0; j < count; ++j) {
+            const v3 pos = lv(pts[j].p);
+            const v3 raxn = vcross(vsub(pos, A.p), n);
+            const v3 rbxn = vcross(vsub(pos, B.p), n);
+            const float lin_vrel = vdot(n, vsub(A.v, B.v));
+            const v3 ra = xform(A, raxn), rb = xform(B, rbxn);
+            const float ang_vrel = vdot(raxn, A.w) - vdot(rbxn, B.w);
+            const float vrel = lin_vrel + ang_vrel;
+            const float response = (A.inv_mass + vdot(ra, ra)) + (B.inv_mass + vdot(rb, rb));
+            const float vm = response > 0.0f ? 1.0f / response : 0.0f;
+            const float pen = pts[j].sep - rest_d;
+            const float pen_dt = pen * inv_dt;
+            const bool separated = pen >= 0.0f;
+            const bool closing = -vrel > pen_dt;
+            const bool bouncing = restitution > 0.0f && bounce > vrel && closing;
+            const float tv = bouncing ? -vrel * restitution : 0.0f;
+            NormalRow r;
+            sv(r.n, n); sv(r.ra, ra); sv(r.rb, rb);
+            r.max_impulse = maximp;
+            r.applied = 0.0f;
+            r.pad = 0.0f;
+            const float target = tv - vrel;
+            if (restitution < 0.0f) {
+                // compliant spring (scene.cpp:8251-8272)
+                const float en_damp = separated && !closing ? 0.0f : damping;
+                const float nrdt = s.dt * restitution;
+                const float a_coeff = s.dt * (en_damp - nrdt);
+                const float x = 1.0f / (1.0f + a_coeff * response);
+                const float bias = x * (-nrdt * pen);
+                r.vel_mult = x * a_coeff;
+                r.imp_mult = 1.0f - x;
+                r.biased = target * r.vel_mult - bias;
+                r.unbiased = r.biased;
+            } else {
+                const float pds = separated ? pen_dt : pen * (inv_dt * bias_coeff);
+                const float sb_ = bouncing ? 0.0f : vm * smax(maxpen, pds);
+                r.vel_mult = vm;
+                r.imp_mult = 1.0f;
+                r.biased = target * vm - sb_;
+                r.unbiased = target * vm - (bouncing ? 0.0f : smax(sb_, 0.0f));
+            }
+            if (!isfinite(response) || !isfinite(r.biased) || !isfinite(r.unbiased)) atomicOr(s.err, kErrNonFinite);
+            rows[j] = r;
+        }
+        // growPatches (scene.cpp:8296-8380)
+        const v3 ext = vsub(bmax, bmin);
+        const float dsq = vlen2(ext);
+        bool keep_pair = false;
+        if (anchors == 2) {
+            keep_pair = vlen2(vsub(a0l[0], a0l[1])) * 4.0f >= dsq;
+            if (!keep_pair) anchors = 0;
+        }
+        if (!keep_pair) {
+            v3 anch[2] = {{0, 0, 0}, {0, 0, 0}};
+            bool changed[2] = {false, false};
+            uint32_t cnt = anchors;
+            if (cnt == 1) anch[0] = vadd(rot_sc(q0, a0l[0]), p0);
+            float pd2 = 0.0f;
+            for (uint32_t j = 0; j < count; ++j) {
+                if (pts[j].sep >= fr_thr + rest_d) continue;
+                const v3 w = lv(pts[j].p);
+                if (cnt == 0) { anch[0] = w; changed[0] = true; ++cnt; }
+                else if (cnt == 1) {
+                    const float dd = vlen2(vsub(w, anch[0]));
+                    if (dd > 1.0e-8f) { anch[1] = w; changed[1] = true; pd2 = dd; ++cnt; }
+                } else {
+                    const float e0 = vlen2(vsub(w, anch[0]));
+                    const float e1 = vlen2(vsub(w, anch[1]));
+                    if (e0 > e1 && e0 > pd2) { anch[1] = w; changed[1] = true; pd2 = e0; }
+                    else if (e1 >= e0 && e1 > pd2) { anch[0] = w; changed[0] = true; pd2 = e1; }
+                }
+            }
+            for (uint32_t k = 0; k < cnt; ++k) {
+                if (!changed[k]) continue;
+                a0l[k] = rotinv_sc(q0, {anch[k].x - p0.x, anch[k].y - p0.y, anch[k].z - p0.z});
+                a1l[k] = rotinv_sc(q1, {anch[k].x - p1.x, anch[k].y - p1.y, anch[k].z - p1.z});
+            }
+            if (cnt == 0) { a0l[0] = {0, 0, 0}; a1l[0] = {0, 0, 0}; }
+            anchors = cnt;
+        }
+        // tangent rows (scene.cpp:8400-8450)
+        FrictionRow* fr = s.frow + 4 * size_t(m);
+        if (anchors) {
+            const v3 rel = vsub(A.v, B.v);
+            v3 t0 = vsub(rel, {n.x * vdot(rel, n), n.y * vdot(rel, n), n.z * vdot(rel, n)});
+            if (vlen2(t0) <= 0.0001f) t0 = fabsf(n.x) < 0.70710678f ? v3{0.0f, -n.z, n.y} : v3{-n.y, n.x, 0.0f};
+            const float il = 1.0f / sqrtf(vlen2(t0));
+            t0 = {t0.x * il, t0.y * il, t0.z * il};
+            const v3 t1 = vcross(n, t0);
+            for (uint32_t k = 0; k < anchors; ++k) {
+                const v3 ra = rot_sc(q0, a0l[k]);
+                const v3 rb = rot_sc(q1, a1l[k]);
+                const v3 err = vsub({ra.x + p0.x, ra.y + p0.y, ra.z + p0.z}, {rb.x + p1.x, rb.y + p1.y, rb.z + p1.z});
+                for (int t = 0; t < 2; ++t) {
+                    const v3 tg = t == 0 ? t0 : t1;
+                    const v3 ax0 = vcross(ra, tg), ax1 = vcross(rb, tg);
+                    const v3 j0 = xform(A, ax0), j1 = xform(B, ax1);
+                    const float resp = (A.inv_mass + vdot(j0, j0)) + (B.inv_mass + vdot(j1, j1));
+                    FrictionRow f;
+                    sv(f.t, tg); sv(f.ra, j0); sv(f.rb, j1);
+                    f.vel_mult = resp > 0.0f ? bias_coeff / resp : 0.0f;
+                    f.bias = vdot(tg, err) * inv_dt;
+                    f.target = -(vdot(tg, rel) + vdot(ax0, A.w) - vdot(ax1, B.w));
+                    f.applied = 0.0f;
+                    f.pad[0] = f.pad[1] = f.pad[2] = 0.0f;
+                    fr[2 * k + t] = f;
+                }
+            }
+        }
+        ManagerHeader hd;
+        hd.b0 = b0; hd.b1 = b1; hd.count = count; hd.anchors = anchors;
+        hd.sf = sfr; hd.df = dfr; hd.pad0 = hd.pad1 = 0.0f;
+        s.mh[m] = hd;
+        // the new history replaces the old one (friction_by_edge_ swap)
+        FrictionHist nh;
+        sv(nh.n0, patch_n0); sv(nh.n1, patch_n1);
+        sv(nh.a0[0], a0l[0]); sv(nh.a0[1], a0l[1]);
+        sv(nh.a1[0], a1l[0]); sv(nh.a1[1], a1l[1]);
+        nh.sf = sfr; nh.df = dfr; nh.rest = restitution; nh.damping = damping;
+        nh.meta = anchors | 512u;   // broken bit written by the last PGS pass
+        nh.epoch = frame;
+        s.cur.fric[pair] = nh;
+    }
+}
+
+// ---------------- PGS ----------------
+__device__ __forceinline__ void load_delta(const DevState& s, int32_t b, v3& dv, v3& dw) {
+    if (b < 0) { dv = dw = {0, 0, 0}; return; }
+    dv = ld3(s.sb_dv[b]);
+    dw = ld3(s.sb_dw[b]);
+}
+__device__ __forceinline__ void store_delta(const DevState& s, int32_t b, v3 dv, v3 dw) {
+    if (b < 0) return;
+    s.sb_dv[b] = st4(dv, 0.0f);
+    s.sb_dw[b] = st4(dw, 0.0f);
+}
+
+__device__ void solve_desc(const DevState& s, uint32_t d, int it, int pos, int vel) {
+    if (d < s.n_joints) {
+        JointRow& r = s.jrow[d];
+        const int32_t b0 = is_dyn(s, s.j_a[d]) ? int32_t(s.j_a[d]) : -1;
+        const int32_t b1 = is_dyn(s, s.j_b[d]) ? int32_t(s.j_b[d]) : -1;
+        v3 av, aw, bv, bw;
+        load_delta(s, b0, av, aw);
+        load_delta(s, b1, bv, bw);
+        const v3 ax = lv(r.axis), ja = lv(r.ang_a), jb = lv(r.ang_b);
+        const float nd = ax.x * (av.x - bv.x) + ax.y * (av.y - bv.y) + ax.z * (av.z - bv.z) + vdot(ja, aw) - vdot(jb, bw);
+        const float cst = it < pos ? r.constant : r.unbiased;
+        const float nx = sclamp(r.applied + nd * r.vel_mult + cst, -FLT_MAX, FLT_MAX);
+        const float imp = nx - r.applied;
+        const float ia = imp * r.ima, ib = imp * r.imb;
+        av = {av.x + ia * ax.x, av.y + ia * ax.y, av.z + ia * ax.z};
+        bv = {bv.x - ib * ax.x, bv.y - ib * ax.y, bv.z - ib * ax.z};
+        aw = {aw.x + imp * ja.x, aw.y + imp * ja.y, aw.z + imp * ja.z};
+        bw = {bw.x - imp * jb.x, bw.y - imp * jb.y, bw.z - imp * jb.z};
+        store_delta(s, b0, av, aw);
+        store_delta(s, b1, bv, bw);
+        r.applied = nx;
+        return;
+    }
+    const uint32_t m = d - s.n_joints;
+    const ManagerHeader hd = s.mh[m];
+    v3 av, aw, bv, bw;
+    load_delta(s, hd.b0, av, aw);
+    load_delta(s, hd.b1, bv, bw);
+    const float ima = hd.b0 >= 0 ? s.b_inv[hd.b0].w : 0.0f;
+    const float imb = hd.b1 >= 0 ? s.b_inv[hd.b1].w : 0.0f;
+    NormalRow* rows = s.nrow + 4 * size_t(m);
+    float nsum = 0.0f;
+    for (uint32_t j = 0; j < hd.count; ++j) {
+        NormalRow& r = rows[j];
+        const v3 n = lv(r.n), ra = lv(r.ra), rb = lv(r.rb);
+        const float nvel = vdot(n, av) - vdot(n, bv) + vdot(aw, ra) - vdot(bw, rb);
+        const float err = it < pos ? r.biased : r.unbiased;
+        const float dc = smax(-nvel * r.vel_mult + err, -r.applied);
+        const float ni = smin(r.max_impulse, r.imp_mult * r.applied + dc);
+        const float dl = ni - r.applied;
+        const float da = dl * ima, db = dl * imb;
+        av = {av.x + n.x * da, av.y + n.y * da, av.z + n.z * da};
+        bv = {bv.x - n.x * db, bv.y - n.y * db, bv.z - n.z * db};
+        aw = {aw.x + ra.x * dl, aw.y + ra.y * dl, aw.z + ra.z * dl};
+        bw = {bw.x - rb.x * dl, bw.y - rb.y * dl, bw.z - rb.z * dl};
+        r.applied = ni;
+        nsum += ni;
+    }
+    if ((it >= pos || pos - it <= 3) && hd.anchors) {
+        const float coeff = hd.anchors == 2 ? 0.5f : 1.0f;
+        const float ms = hd.sf * coeff * nsum;
+        const float md = hd.df * coeff * nsum;
+        bool broken = false;
+        FrictionRow* fr = s.frow + 4 * size_t(m);
+        for (uint32_t k = 0; k < 2 * hd.anchors; ++k) {
+            FrictionRow& f = fr[k];
+            const v3 n = lv(f.t), ra = lv(f.ra), rb = lv(f.rb);
+            const float td = vdot(n, av) - vdot(n, bv) + vdot(aw, ra) - vdot(bw, rb);
+            const float bias = it < pos ? f.bias : 0.0f;
+            const float cand = f.applied + (f.target - bias - td) * f.vel_mult;
+            const bool clamped = fabsf(cand) > ms;
+            const float nx = clamped ? smin(md, smax(-md, cand)) : cand;
+            const float dl = nx - f.applied;
+            const float da = dl * ima, db = dl * imb;
+            av = {av.x + n.x * da, av.y + n.y * da, av.z + n.z * da};
+            bv = {bv.x - n.x * db, bv.y - n.y * db, bv.z - n.z * db};
+            aw = {aw.x + ra.x * dl, aw.y + ra.y * dl, aw.z + ra.z * dl};
+            bw = {bw.x - rb.x * dl, bw.y - rb.y * dl, bw.z - rb.z * dl};
+            f.applied = nx;
+            broken |= clamped;
+        }
+        if (it + 1 == pos + vel) {
+            FrictionHist& h = s.cur.fric[s.man_list[m]];
+            h.meta = (h.meta & ~256u) | (broken ? 256u : 0u);
+        }
+    }
+    store_delta(s, hd.b0, av, aw);
+    store_delta(s, hd.b1, bv, bw);
+}
+__device__ __forceinline__ void save_motion(const DevState& s, uint32_t d) {
+    int32_t b0, b1;
+    if (d < s.n_joints) {
+        b0 = is_dyn(s, s.j_a[d]) ? int32_t(s.j_a[d]) : -1;
+        b1 = is_dyn(s, s.j_b[d]) ? int32_t(s.j_b[d]) : -1;
+    } else {
+        const ManagerHeader hd = s.mh[d - s.n_joints];
+        b0 = hd.b0; b1 = hd.b1;
+    }
+    if (b0 >= 0) { s.sb_mdv[b0] = s.sb_dv[b0]; s.sb_mdw[b0] = s.sb_dw[b0]; }
+    if (b1 >= 0) { s.sb_mdv[b1] = s.sb_dv[b1]; s.sb_mdw[b1] = s.sb_dw[b1]; }
+}
+
+// One warp per small island.
+__global__ void k_pgs_warp(DevState s, const uint32_t* lvl_bound) {
+    const uint32_t ni = *s.n_isl;
+    const int lane = threadIdx.x & 31;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int pos = s.pos_iters, vel = s.vel_iters < 1 ? 1 : s.vel_iters;
+    for (uint32_t isl = warp; isl < ni; isl += nwarps) {
+        const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
+        if (end - begin > kSmallIsland) continue;
+        const uint32_t nlev = s.isl_end[isl];
+        const uint32_t* bound = lvl_bound + begin + isl;
+        for (int it = 0; it < pos + vel; ++it) {
+            for (uint32_t l = 0; l < nlev; ++l) {
+                const uint32_t lb = bound[l], le = bound[l + 1];
+                for (uint32_t i = lb + lane; i < le; i += 32) solve_desc(s, s.d_val2[i], it, pos, vel);
+                __syncwarp();
+            }
+            if (it + 1 == pos) {
+                for (uint32_t i = begin + lane; i < end; i += 32) save_motion(s, s.d_val2[i]);
+                __syncwarp();
+            }
+        }
+    }
+}
+// One CTA per large island.
+__global__ void __launch_bounds__(256) k_pgs_block(DevState s, const uint32_t* lvl_bound) {
+    const uint32_t ni = *s.n_isl;
+    const int pos = s.pos_iters, vel = s.vel_iters < 1 ? 1 : s.vel_iters;
+    for (uint32_t isl = blockIdx.x; isl < ni; isl += gridDim.x) {
+        const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
+        if (end - begin <= kSmallIsland) continue;
+        const uint32_t nlev = s.isl_end[isl];
+        const uint32_t* bound = lvl_bound + begin + isl;
+        for (int it = 0; it < pos + vel; ++it) {
+            for (uint32_t l = 0; l < nlev; ++l) {
+                const uint32_t lb = bound[l], le = bound[l + 1];
+                for (uint32_t i = lb + threadIdx.x; i < le; i += blockDim.x) solve_desc(s, s.d_val2[i], it, pos, vel);
+                __syncthreads();
+            }
+            if (it + 1 == pos) {
+                for (uint32_t i = begin + threadIdx.x; i < end; i += blockDim.x) save_motion(s, s.d_val2[i]);
+                __syncthreads();
+            }
+        }
+    }
+}
+
+// scene.cpp:114-143
+__device__ qt integrate_q(qt pose, v3 w, float dt) {
+    float m = w.x * w.x + w.y * w.y + w.z * w.z;
+    if (m != 0.0f) {
+        m = sqrtf(m);
+        if (m > 1.0e7f) {
+            const float sc = 1.0e7f / m;
+            w = {w.x * sc, w.y * sc, w.z * sc};
+            m = 1.0e7f;
+        }
+        const float v = dt * m * 0.5f;
+        const float sn = sinf(v) / m;
+        const float cs = cosf(v);
+        const qt dq = qmul({w.x * sn, w.y * sn, w.z * sn, 0.0f}, pose);
+        const qt nx = {dq.x + pose.x * cs, dq.y + pose.y * cs, dq.z + pose.z * cs, dq.w + pose.w * cs};
+        const float len = sqrtf(nx.x * nx.x + nx.y * nx.y + nx.z * nx.z + nx.w * nx.w);
+        pose = {nx.x / len, nx.y / len, nx.z / len, nx.w / len};
+    }
+    return pose;
+}
+
+__global__ void k_integrate(DevState s) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= s.n_bodies || !is_dyn(s, b)) return;
+    const float dt = s.dt;
+    const v3 v = ld3(s.sb_v[b]), w = ld3(s.sb_w[b]);
+    const float4* si = s.sb_sqrt_i + 3 * size_t(b);
+    const v3 c0 = ld3(si[0]), c1 = ld3(si[1]), c2 = ld3(si[2]);
+    const v3 mdv = ld3(s.sb_mdv[b]), mdw = ld3(s.sb_mdw[b]);
+    const v3 fdv = ld3(s.sb_dv[b]), fdw = ld3(s.sb_dw[b]);
+    const v3 ml = {v.x + mdv.x, v.y + mdv.y, v.z + mdv.z};
+    const v3 mw = {w.x + c0.x * mdw.x + c1.x * mdw.y + c2.x * mdw.z,
+                   w.y + c0.y * mdw.x + c1.y * mdw.y + c2.y * mdw.z,
+                   w.z + c0.z * mdw.x + c1.z * mdw.y + c2.z * mdw.z};
+    const v3 fv = {v.x + fdv.x, v.y + fdv.y, v.z + fdv.z};
+    const v3 fw = {w.x + c0.x * fdw.x + c1.x * fdw.y + c2.x * fdw.z,
+                   w.y + c0.y * fdw.x + c1.y * fdw.y + c2.y * fdw.z,
+                   w.z + c0.z * fdw.x + c1.z * fdw.y + c2.z * fdw.z};
+    const v3 center = mass_position(s, b);
+    v3 p = {center.x + ml.x * dt, center.y + ml.y * dt, center.z + ml.z * dt};
+    const qt mlq = ldq(s.b_ml_q[b]);
+    qt q = integrate_q(mass_orientation(s, b), mw, dt);
+    q = qmul(q, qconj(mlq));
+    const v3 off = rot_sc(q, ld3(s.b_ml_p[b]));
+    p = {p.x - off.x, p.y - off.y, p.z - off.z};
+    if (!(vfinite(p) && isfinite(q.x) && isfinite(q.y) && isfinite(q.z) && isfinite(q.w) && vfinite(fv) && vfinite(fw)))
+        atomicOr(s.err, kErrNonFinite);
+    s.b_p[b] = make_float4(p.x, p.y, p.z, s.b_p[b].w);
+    s.b_q[b] = stq(q);
+    s.b_v[b] = st4(fv, 0.0f);
+    s.b_w[b] = st4(fw, 0.0f);
+}
+
+inline uint32_t grid_for(uint32_t n, uint32_t t, uint32_t cap) {
+    const uint32_t g = (n + t - 1) / t;
+    return g == 0 ? 1 : (g < cap ? g : cap);
+}
+
+}  // namespace
+
+void enqueue_solver(const DevState& s, cudaStream_t st) {
+    uint32_t* flags = s.tmp_flags;
+    uint32_t* pos = s.tmp_pos;
+    uint32_t* lvl_bound = s.lvl_bound;
+    const uint32_t T = 256;
+    const uint32_t cap_blocks = 148u * 8u;
+    k_frame_begin<<<1, 32, 0, st>>>(s);
+    k_bodies_begin<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
+    // touching managers in canonical pair order
+    k_touch_flags<<<grid_for(s.pair_cap, T, cap_blocks), T, 0, st>>>(s, flags);
+    scan_exclusive(flags, pos, s.pair_cap, s.cur.n, s.counters + kCntMan, s.scan_tmp, s.scan_tmp_words, st);
+    k_touch_scatter<<<grid_for(s.pair_cap, T, cap_blocks), T, 0, st>>>(s, flags, pos);
+    // islands and partitions
+    k_union<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
+    k_desc_keys<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
+    int bits = 1;
+    while ((1ull << bits) < s.n_bodies) ++bits;
+    radix_sort_pairs(s.d_key, s.d_val, s.d_key2, s.d_val2, s.desc_cap, s.counters + kCntDesc, 0,
+                     (bits + 7) / 8 * 8, s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st);
+    k_island_flags<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
+    scan_exclusive(s.isl_flag, pos, s.desc_cap, s.counters + kCntDesc, s.n_isl, s.scan_tmp, s.scan_tmp_words, st);
+    k_island_scatter<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s, pos);
+    k_partition<<<grid_for(s.desc_cap, 128, cap_blocks), 128, 0, st>>>(s, lvl_bound);
+    // rows
+    if (s.n_joints) k_prep_joints<<<grid_for(s.n_joints, T, 1u << 30), T, 0, st>>>(s);
+    k_prep_contacts<<<grid_for(s.desc_cap, 128, cap_blocks), 128, 0, st>>>(s);
+    // PGS
+    k_pgs_warp<<<grid_for(s.desc_cap * 32u, T, cap_blocks), T, 0, st>>>(s, lvl_bound);
+    k_pgs_block<<<grid_for(s.desc_cap, 1, 148u * 4u), 256, 0, st>>>(s, lvl_bound);
+    k_integrate<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
+}
+
+}  // namespace fyzz::b200

@@ -1,0 +1,139 @@
+// Device-resident state of a batched rigid-body world and the host entry
+// points that enqueue the step's kernels on a stream.
+//
+// Layout (HBM, structure of arrays, 16-byte records for 128-bit loads):
+//   bodies   b_*  one record per actor of every scene (floors included)
+//   shapes   s_*  one record per attached shape
+//   pairs    two ping-pong generations of sorted broadphase pair keys and
+//            the persistent contact-manager records keyed by them
+//   solver   per-step rows, island/level ordering and body deltas
+// Scenes are contiguous ranges of bodies and shapes; every shape of a scene
+// has a larger global index than every shape of the previous scene, so the
+// global (shape a, shape b) order equals the per-scene canonical pair order.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+namespace fyzz::b200 {
+
+struct ManagerSet {
+    uint64_t* key = nullptr;       // sorted pair keys (a << 32 | b)
+    PcmCache* cache = nullptr;
+    FrictionHist* fric = nullptr;
+    uint32_t* count = nullptr;     // published contact count (touch state)
+    uint32_t* n = nullptr;         // device-side pair count of this generation
+};
+
+struct DevState {
+    // static topology sizes (host-known)
+    uint32_t n_scenes = 0, n_bodies = 0, n_shapes = 0, n_finite = 0, n_joints = 0;
+    uint32_t pair_cap = 0, desc_cap = 0;
+    uint32_t max_small_scene = 2048;   // finite shapes sorted inside one CTA
+    int pos_iters = 4, vel_iters = 1;
+    float dt = 1.0f / 120.0f;
+    uint32_t frame = 0;
+
+    // scenes
+    uint32_t* sc_fbegin = nullptr;     // S+1, finite-shape ranges (finite-rank space)
+    int32_t* sc_plane = nullptr;       // plane shape of each scene or -1
+    uint32_t* small_scenes = nullptr;  // scenes sorted inside one CTA
+    uint32_t n_small = 0;
+
+    // bodies
+    float4 *b_p = nullptr, *b_q = nullptr, *b_v = nullptr, *b_w = nullptr;
+    float4 *b_inv = nullptr;           // inverse inertia xyz, w = inverse mass
+    float4 *b_ml_p = nullptr, *b_ml_q = nullptr;
+    float4 *b_dyn0 = nullptr;          // linear damping, angular damping, max linear, max angular
+    float4 *b_dyn1 = nullptr;          // max depenetration, max contact impulse, slop, unused
+    uint32_t* b_flags = nullptr;
+    uint32_t* b_scene = nullptr;
+
+    // shapes
+    uint32_t *s_body = nullptr, *s_type = nullptr, *s_scene = nullptr;
+    float4 *s_geom = nullptr;          // half extents xyz, radius
+    float4 *s_lp = nullptr;            // local position, w = contact offset
+    float4 *s_lq = nullptr;
+    float4 *s_mat = nullptr;           // static f, dynamic f, restitution, rest offset
+    float4 *s_wp = nullptr, *s_wq = nullptr;
+    uint4 *s_lo = nullptr, *s_hi = nullptr;   // encoded bounds (x,y,z,-)
+    int32_t* s_frank = nullptr;        // finite rank, -1 for planes
+    int32_t* s_dynrank = nullptr;      // rank among the scene's dynamic finite shapes
+    uint32_t* s_static_pairs = nullptr;// plane pairs owned by this shape
+
+    // broadphase scratch
+    uint32_t *srt_key = nullptr, *srt_id = nullptr;      // sorted min-x endpoints
+    uint32_t *srt_key2 = nullptr, *srt_id2 = nullptr;
+    uint32_t *own_cnt = nullptr, *own_off = nullptr, *own_cur = nullptr;
+    ManagerSet cur, prev;
+    int32_t* prev_idx = nullptr;
+    uint32_t* found_flag = nullptr;    // per current pair
+    uint32_t* lost_flag = nullptr;     // per previous pair
+    ContactPt* pts = nullptr;          // 4 per current pair
+
+    // touching managers
+    uint32_t* man_list = nullptr;      // current-pair indices, canonical order
+    uint32_t* n_man = nullptr;
+    ManagerHeader* mh = nullptr;       // per touching manager
+    NormalRow* nrow = nullptr;         // 4 per touching manager
+    FrictionRow* frow = nullptr;       // 4 per touching manager
+
+    // joints (static, sorted by scene then constraint slot descending)
+    uint32_t *j_a = nullptr, *j_b = nullptr;
+    float* j_len = nullptr;
+    JointRow* jrow = nullptr;
+
+    // solver bodies
+    float4 *sb_dv = nullptr, *sb_dw = nullptr, *sb_mdv = nullptr, *sb_mdw = nullptr;
+    float4 *sb_v = nullptr, *sb_w = nullptr;
+    float4 *sb_sqrt_i = nullptr;       // 3 per body: columns of R sqrt(I^-1) R^T
+    uint32_t* uf_parent = nullptr;
+
+    // descriptors: [0, n_joints) joints, then touching managers
+    uint32_t *d_key = nullptr, *d_val = nullptr, *d_key2 = nullptr, *d_val2 = nullptr;
+    uint32_t* d_level = nullptr;
+    uint32_t *isl_begin = nullptr, *isl_end = nullptr, *n_isl = nullptr;
+    uint32_t* isl_flag = nullptr;
+    uint32_t* sb_mask = nullptr;       // partition masks per body
+    uint32_t* sb_maxdyn = nullptr;
+    uint32_t* sb_static = nullptr;
+
+    // step scratch
+    uint4* sw_rec = nullptr;           // sweep y/z bounds in sorted order
+    uint2* sw_meta = nullptr;          // sweep max x and body | dynamic bit
+    uint32_t* tmp_flags = nullptr;     // pair_cap
+    uint32_t* tmp_pos = nullptr;       // max(pair_cap, desc_cap)
+    uint32_t* lvl_bound = nullptr;     // 2 * desc_cap + 2: per-island partition starts
+    // scenes too large for one CTA: sorted with the device-wide radix sort
+    static constexpr int kMaxLarge = 64;
+    uint32_t n_large = 0;
+    uint32_t large_begin[kMaxLarge] = {}, large_n[kMaxLarge] = {};
+
+    // scratch for scans / sorts
+    uint32_t* scan_tmp = nullptr;
+    size_t scan_tmp_words = 0;
+    uint32_t* sort_hist = nullptr;
+    size_t sort_hist_words = 0;
+    uint32_t* counters = nullptr;      // small device counters
+    uint32_t* err = nullptr;           // error bits
+};
+
+// primitives.cu
+void scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, const uint32_t* n_dev,
+                    uint32_t* total, uint32_t* tmp, size_t tmp_words, cudaStream_t st);
+void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
+                      uint32_t n_cap, const uint32_t* n_dev, int begin_bit, int end_bit,
+                      uint32_t* hist, size_t hist_words, uint32_t* scan_tmp, size_t scan_words,
+                      cudaStream_t st);
+size_t radix_hist_words(uint32_t n_cap);
+size_t scan_tmp_words_for(uint32_t n_cap);
+
+// broadphase.cu / narrowphase.cu / solver.cu
+void enqueue_broadphase(const DevState& s, cudaStream_t st);
+void enqueue_narrowphase(const DevState& s, cudaStream_t st);
+void enqueue_solver(const DevState& s, cudaStream_t st);
+// counters[] slots
+enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels = 4, kCntSlots = 8 };
+
+}  // namespace fyzz::b200

@@ -1,0 +1,1128 @@
+// Host side of the B200 rigid-body world: authoring tables that mirror the
+// reference's fyzz::World / WorldBackend semantics, mass properties, the
+// device upload, CUDA-graph stepping and the C ABI (include/fyzz_b200.h).
+//
+// Authoring follows the reference NativeCpu scene:
+//   transforms are validated and normalised twice, once by World
+//   (src/world.cpp:38-55) and once by Scene::validated_pose
+//   (src/native/compound.cpp:9-18);
+//   create_body gives unit inverse mass / inertia until
+//   update_mass_properties (scene.cpp:254-265, compound.cpp:113-203);
+//   shapes default to contact offset 0.02, rest offset 0 and the default
+//   Material (world.h:78-90, scene.h:1189).
+// Stepping is failure-atomic like Scene::step (scene.cpp:10725-11016): body
+// state is checkpointed before a launch and restored when the device
+// reports an error; a pair-capacity overflow grows the pair arrays, drops the
+// contact-manager history (the reference's invalidate_after_rollback,
+// source_sc_owned_gpu_broadphase_native.h:479-484) and replays the steps.
+#include "state.h"
+#include "../../include/fyzz_b200.h"
+
+#include <algorithm>
+#include <array>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace fyzz::b200 {
+namespace {
+
+struct HostBody {
+    uint32_t scene = 0;
+    bool dynamic = false;
+    std::array<float, 3> p{}, v{}, w{};
+    std::array<float, 4> q{0, 0, 0, 1};
+    float inv_mass = 0.0f;
+    std::array<float, 3> inv_inertia{0, 0, 0};
+    std::array<float, 3> ml_p{0, 0, 0};
+    std::array<float, 4> ml_q{0, 0, 0, 1};
+    std::vector<uint32_t> shapes;   // attachment order
+};
+struct HostShape {
+    uint32_t body = 0, scene = 0, type = kBox;
+    std::array<float, 3> half{0, 0, 0};
+    float radius = 0.0f;
+    std::array<float, 3> lp{0, 0, 0};
+    std::array<float, 4> lq{0, 0, 0, 1};
+    std::array<float, 4> mat{0.5f, 0.5f, 0.2f, 0.0f};   // static, dynamic, restitution, rest offset
+    float contact_offset = 0.02f;
+};
+struct HostJoint { uint32_t a = 0, b = 0; float len = 0.0f; uint32_t scene = 0; uint32_t slot = 0; };
+
+void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess)
+        throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+std::array<float, 4> normalize_once(std::array<float, 4> q) {
+    const float len = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    return {q[0] / len, q[1] / len, q[2] / len, q[3] / len};
+}
+// World::validated_transform then Scene::validated_pose.
+std::array<float, 4> validated_orientation(const float* q4) {
+    std::array<float, 4> q{q4[0], q4[1], q4[2], q4[3]};
+    for (int pass = 0; pass < 2; ++pass) {
+        const float len = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+        if (!std::isfinite(q[0]) || !std::isfinite(q[1]) || !std::isfinite(q[2]) || !std::isfinite(q[3]) ||
+            !std::isfinite(len) || std::abs(len - 1.0f) >= 1.0e-2f)
+            throw std::invalid_argument("Rigid pose orientation is not sane");
+        q = normalize_once(q);
+    }
+    return q;
+}
+void validate_position(const float* p) {
+    if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2]))
+        throw std::invalid_argument("Position must be finite");
+}
+
+// ---- mass properties (compound.cpp:113-203) ----
+struct M3 { v3 c[3]; };
+M3 m_from_q(qt q) {
+    const float x = q.x, y = q.y, z = q.z, w = q.w;
+    const float x2 = x + x, y2 = y + y, z2 = z + z;
+    const float xx = x2 * x, yy = y2 * y, zz = z2 * z;
+    const float xy = x2 * y, xz = x2 * z, xw = x2 * w;
+    const float yz = y2 * z, yw = y2 * w, zw = z2 * w;
+    M3 m;
+    m.c[0] = {1.0f - yy - zz, xy + zw, xz - yw};
+    m.c[1] = {xy - zw, 1.0f - xx - zz, yz + xw};
+    m.c[2] = {xz + yw, yz - xw, 1.0f - xx - yy};
+    return m;
+}
+float mel(const M3& m, int row, int col) { return vcomp(m.c[col], row); }
+M3 m_mul(const M3& a, const M3& b) {
+    M3 r;
+    for (int c = 0; c < 3; ++c) {
+        const v3 bc = b.c[c];
+        r.c[c] = vadd(vadd(vmul(a.c[0], bc.x), vmul(a.c[1], bc.y)), vmul(a.c[2], bc.z));
+    }
+    return r;
+}
+M3 m_t(const M3& a) {
+    M3 r;
+    r.c[0] = {a.c[0].x, a.c[1].x, a.c[2].x};
+    r.c[1] = {a.c[0].y, a.c[1].y, a.c[2].y};
+    r.c[2] = {a.c[0].z, a.c[1].z, a.c[2].z};
+    return r;
+}
+// Jacobi diagonalisation with quaternion rotations (S. Melax): at most 24
+// sweeps, each rotating away the largest off-diagonal element.
+v3 diagonalize(const M3& m, qt& frame) {
+    qt q = {0, 0, 0, 1};
+    M3 d = m;
+    for (int it = 0; it < 24; ++it) {
+        const M3 axes = m_from_q(q);
+        d = m_mul(m_mul(m_t(axes), m), axes);
+        const float d0 = std::abs(mel(d, 2, 1)), d1 = std::abs(mel(d, 2, 0)), d2 = std::abs(mel(d, 1, 0));
+        const int a = (d0 > d1 && d0 > d2) ? 0 : (d1 > d2 ? 1 : 2);
+        const int a1 = (a + 1) % 3, a2 = (a1 + 1) % 3;
+        const float off = mel(d, a2, a1);
+        if (off == 0.0f || std::abs(mel(d, a1, a1) - mel(d, a2, a2)) > 2e6f * std::abs(2.0f * off)) break;
+        const float w = (mel(d, a1, a1) - mel(d, a2, a2)) / (2.0f * off);
+        const float absw = std::abs(w);
+        float v[3] = {0, 0, 0};
+        float c;
+        if (absw > 1000) {
+            v[a] = 1.0f / (4.0f * w);
+            c = 1.0f;
+        } else {
+            const float t = 1.0f / (absw + std::sqrt(w * w + 1.0f));
+            const float h = 1.0f / std::sqrt(t * t + 1.0f);
+            v[a] = std::sqrt((1.0f - h) / 2.0f) * (w < 0 ? -1.0f : 1.0f);
+            c = std::sqrt((1.0f + h) / 2.0f);
+        }
+        const qt r = qmul(q, {v[0], v[1], v[2], c});
+        const float mag = std::sqrt(r.x * r.x + r.y * r.y + r.z * r.z + r.w * r.w);
+        const float sc = 1.0f / mag;
+        q = {r.x * sc, r.y * sc, r.z * sc, r.w * sc};
+    }
+    frame = q;
+    return {d.c[0].x, d.c[1].y, d.c[2].z};
+}
+
+template <class T> void dalloc(T*& p, size_t n, std::vector<void*>& owned) {
+    if (n == 0) n = 1;
+    check_cuda(cudaMalloc(reinterpret_cast<void**>(&p), n * sizeof(T)), "cudaMalloc");
+    owned.push_back(p);
+}
+template <class T> void upload(T* dst, const std::vector<T>& src, cudaStream_t st) {
+    if (!src.empty())
+        check_cuda(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, st), "upload");
+}
+
+}  // namespace
+
+class World {
+public:
+    explicit World(int device) : device_(device) {
+        check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+        check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+        check_cuda(cudaMallocHost(reinterpret_cast<void**>(&host_err_), 64), "cudaMallocHost");
+        scene_body_begin_.push_back(0);
+        scene_shape_begin_.push_back(0);
+        scene_has_floor_.push_back(false);
+    }
+    ~World() {
+        cudaSetDevice(device_);
+        release_device();
+        if (host_err_) cudaFreeHost(host_err_);
+        if (stream_) cudaStreamDestroy(stream_);
+    }
+    std::string error;
+
+    // ---------------- authoring ----------------
+    uint32_t begin_scene() {
+        pull_state();
+        if (bodies_.size() == scene_body_begin_.back() && shapes_.size() == scene_shape_begin_.back())
+            return uint32_t(scene_body_begin_.size() - 1);
+        scene_body_begin_.push_back(uint32_t(bodies_.size()));
+        scene_shape_begin_.push_back(uint32_t(shapes_.size()));
+        scene_has_floor_.push_back(false);
+        topology_dirty_ = true;
+        return uint32_t(scene_body_begin_.size() - 1);
+    }
+    uint32_t current_scene() const { return uint32_t(scene_body_begin_.size() - 1); }
+    uint32_t add_static_floor(float height) {
+        if (!std::isfinite(height)) throw std::invalid_argument("Native scene floor must be finite");
+        if (scene_has_floor_.back()) throw std::logic_error("One static floor per scene is supported");
+        pull_state();
+        HostBody b;
+        b.scene = current_scene();
+        b.dynamic = false;
+        b.p = {0.0f, height, 0.0f};
+        bodies_.push_back(b);
+        HostShape s;
+        s.body = uint32_t(bodies_.size() - 1);
+        s.scene = b.scene;
+        s.type = kPlane;
+        bodies_.back().shapes.push_back(uint32_t(shapes_.size()));
+        shapes_.push_back(s);
+        scene_has_floor_.back() = true;
+        topology_dirty_ = true;
+        return uint32_t(bodies_.size() - 1);
+    }
+    uint32_t create_dynamic_body(const float* pose) {
+        validate_position(pose);
+        const auto q = validated_orientation(pose + 3);
+        pull_state();
+        HostBody b;
+        b.scene = current_scene();
+        b.dynamic = true;
+        b.p = {pose[0], pose[1], pose[2]};
+        b.q = q;
+        b.inv_mass = 1.0f;
+        b.inv_inertia = {1.0f, 1.0f, 1.0f};
+        bodies_.push_back(b);
+        topology_dirty_ = true;
+        return uint32_t(bodies_.size() - 1);
+    }
+    HostBody& require_body(uint32_t id) {
+        if (id >= bodies_.size()) throw std::out_of_range("Unknown rigid body");
+        return bodies_[id];
+    }
+    const HostBody& require_body(uint32_t id) const {
+        if (id >= bodies_.size()) throw std::out_of_range("Unknown rigid body");
+        return bodies_[id];
+    }
+    uint32_t attach(uint32_t body, uint32_t type, const float* half, float radius, const float* local) {
+        HostBody& b = require_body(body);
+        if (!b.dynamic) throw std::logic_error("Shapes attach to dynamic bodies on this backend");
+        if (b.scene != current_scene()) throw std::logic_error("Bodies of a closed scene cannot gain shapes");
+        validate_position(local);
+        const auto lq = validated_orientation(local + 3);
+        if (type == kBox) {
+            if (!std::isfinite(half[0]) || !std::isfinite(half[1]) || !std::isfinite(half[2]) ||
+                half[0] <= 0.0f || half[1] <= 0.0f || half[2] <= 0.0f)
+                throw std::invalid_argument("Box half-extents must be finite and positive");
+        } else if (!std::isfinite(radius) || radius <= 0.0f) {
+            throw std::invalid_argument("Sphere radius must be finite and positive");
+        }
+        if (b.shapes.size() >= 8) throw std::logic_error("At most 8 shapes per body are supported");
+        pull_state();
+        HostShape s;
+        s.body = body;
+        s.scene = b.scene;
+        s.type = type;
+        if (type == kBox) s.half = {half[0], half[1], half[2]};
+        s.radius = radius;
+        s.lp = {local[0], local[1], local[2]};
+        s.lq = lq;
+        b.shapes.push_back(uint32_t(shapes_.size()));
+        shapes_.push_back(s);
+        topology_dirty_ = true;
+        return uint32_t(shapes_.size() - 1);
+    }
+    void update_mass_properties(uint32_t body, float density) {
+        HostBody& b = require_body(body);
+        if (!b.dynamic) throw std::logic_error("Static body has no mass properties");
+        if (!std::isfinite(density) || density <= 0.0f)
+            throw std::invalid_argument("Mass density must be positive and finite");
+        pull_state();
+        const float pi = 3.14159265358979323846f;
+        // Shapes are visited in list order: most recently attached first.
+        std::vector<uint32_t> order(b.shapes.rbegin(), b.shapes.rend());
+        std::vector<float> um(order.size());
+        float mass = 0.0f;
+        v3 center = {0, 0, 0};
+        for (size_t i = 0; i < order.size(); ++i) {
+            const HostShape& s = shapes_[order[i]];
+            um[i] = s.type == kBox ? s.half[0] * s.half[1] * s.half[2] * 8.0f
+                                   : (4.0f / 3.0f) * pi * s.radius * s.radius * s.radius;
+            const float m = um[i] * density;
+            mass += m;
+            center = vadd(center, vmul({s.lp[0], s.lp[1], s.lp[2]}, m));
+        }
+        if (!std::isfinite(mass) || !(mass > 0.0f)) throw std::invalid_argument("Compound mass outside supported range");
+        center = vmul(center, 1.0f / mass);
+        M3 tensor{};
+        for (size_t i = 0; i < order.size(); ++i) {
+            const HostShape& s = shapes_[order[i]];
+            const float m = um[i] * density;
+            v3 diag;
+            if (s.type == kBox) {
+                const v3 h = {s.half[0], s.half[1], s.half[2]};
+                diag = vmul({h.y * h.y + h.z * h.z, h.x * h.x + h.z * h.z, h.x * h.x + h.y * h.y}, m / 3.0f);
+            } else {
+                const float v = (2.0f / 5.0f) * m * s.radius * s.radius;
+                diag = {v, v, v};
+            }
+            M3 local{};
+            local.c[0].x = diag.x; local.c[1].y = diag.y; local.c[2].z = diag.z;
+            const M3 rot = m_from_q({s.lq[0], s.lq[1], s.lq[2], s.lq[3]});
+            const M3 rt = m_mul(m_mul(rot, local), m_t(rot));
+            const v3 d = vsub({s.lp[0], s.lp[1], s.lp[2]}, center);
+            const float dd = vdot(d, d);
+            for (int c = 0; c < 3; ++c) {
+                tensor.c[c] = vadd(tensor.c[c], rt.c[c]);
+                const float dc = vcomp(d, c);
+                v3 pc = {-d.x * dc, -d.y * dc, -d.z * dc};
+                if (c == 0) pc.x += dd; else if (c == 1) pc.y += dd; else pc.z += dd;
+                tensor.c[c] = vadd(tensor.c[c], vmul(pc, m));
+            }
+        }
+        qt axes;
+        const v3 inertia = diagonalize(tensor, axes);
+        const v3 inv = {1.0f / inertia.x, 1.0f / inertia.y, 1.0f / inertia.z};
+        const float inv_mass = 1.0f / mass;
+        if (!std::isfinite(inv.x) || !std::isfinite(inv.y) || !std::isfinite(inv.z) ||
+            std::min({inv.x, inv.y, inv.z}) <= 0.0f || !std::isfinite(inv_mass) || inv_mass <= 0.0f)
+            throw std::invalid_argument("Compound inverse mass/inertia outside supported range");
+        b.inv_mass = inv_mass;
+        b.inv_inertia = {inv.x, inv.y, inv.z};
+        b.ml_p = {center.x, center.y, center.z};
+        b.ml_q = {axes.x, axes.y, axes.z, axes.w};
+        mass_dirty_ = true;
+    }
+    void set_shape_material(uint32_t shape, const fyzz_b200_material& m) {
+        if (shape >= shapes_.size()) throw std::out_of_range("Unknown shape");
+        if (!std::isfinite(m.static_friction) || !std::isfinite(m.dynamic_friction) ||
+            !std::isfinite(m.restitution) || m.static_friction < 0.0f || m.dynamic_friction < 0.0f ||
+            m.restitution > 1.0f)
+            throw std::invalid_argument("PhysX contact material coefficients/modes invalid");
+        pull_state();
+        shapes_[shape].mat[0] = m.static_friction;
+        shapes_[shape].mat[1] = m.dynamic_friction;
+        shapes_[shape].mat[2] = m.restitution;
+        mass_dirty_ = true;
+    }
+    void set_velocity(uint32_t body, const float* v, bool angular) {
+        HostBody& b = require_body(body);
+        if (!std::isfinite(v[0]) || !std::isfinite(v[1]) || !std::isfinite(v[2]))
+            throw std::invalid_argument("Velocity must be finite");
+        if (!b.dynamic) throw std::logic_error("Static actors have no velocity");
+        pull_state();
+        (angular ? b.w : b.v) = {v[0], v[1], v[2]};
+        mass_dirty_ = true;
+    }
+    uint64_t add_distance(uint32_t a, uint32_t b, float len) {
+        const HostBody& A = require_body(a);
+        const HostBody& B = require_body(b);
+        if (a == b || (!A.dynamic && !B.dynamic))
+            throw std::invalid_argument("Constraint requires two distinct actors and a rigid node");
+        if (A.scene != B.scene) throw std::invalid_argument("Constraint endpoints must share a scene");
+        if (!std::isfinite(len) || len < 0.0f)
+            throw std::invalid_argument("Rigid 1D distance must be finite and nonnegative");
+        pull_state();
+        HostJoint j;
+        j.a = std::min(a, b);
+        j.b = std::max(a, b);
+        j.len = len;
+        j.scene = A.scene;
+        uint32_t slot = 0;
+        for (const auto& o : joints_) if (o.scene == j.scene) ++slot;
+        j.slot = slot;
+        joints_.push_back(j);
+        topology_dirty_ = true;
+        return (uint64_t(1) << 32) | slot;   // generation 1, slot (scene.cpp:3042-3045)
+    }
+    void mass_props(uint32_t body, float* out) const {
+        const HostBody& b = require_body(body);
+        if (!b.dynamic) throw std::logic_error("Static body has no mass properties");
+        out[0] = b.inv_mass;
+        for (int i = 0; i < 3; ++i) out[1 + i] = b.inv_inertia[i];
+        for (int i = 0; i < 3; ++i) out[4 + i] = b.ml_p[i];
+        for (int i = 0; i < 4; ++i) out[7 + i] = b.ml_q[i];
+    }
+
+    // ---------------- device state ----------------
+    void ensure_device() {
+        if (topology_dirty_ || !uploaded_) {
+            build_device();
+        } else if (mass_dirty_) {
+            upload_bodies();
+        }
+        mass_dirty_ = false;
+    }
+    // Device -> host body state, before any host authoring edit.
+    void pull_state() {
+        if (!uploaded_ || host_authoritative_) return;
+        check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+        const size_t n = bodies_.size() < d_.n_bodies ? bodies_.size() : d_.n_bodies;
+        std::vector<float4> p(n), q(n), v(n), w(n);
+        if (n) {
+            check_cuda(cudaMemcpyAsync(p.data(), d_.b_p, n * 16, cudaMemcpyDeviceToHost, stream_), "pull");
+            check_cuda(cudaMemcpyAsync(q.data(), d_.b_q, n * 16, cudaMemcpyDeviceToHost, stream_), "pull");
+            check_cuda(cudaMemcpyAsync(v.data(), d_.b_v, n * 16, cudaMemcpyDeviceToHost, stream_), "pull");
+            check_cuda(cudaMemcpyAsync(w.data(), d_.b_w, n * 16, cudaMemcpyDeviceToHost, stream_), "pull");
+            check_cuda(cudaStreamSynchronize(stream_), "pull sync");
+        }
+        for (size_t i = 0; i < n; ++i) {
+            auto& b = bodies_[i];
+            if (!b.dynamic) continue;
+            b.p = {p[i].x, p[i].y, p[i].z};
+            b.q = {q[i].x, q[i].y, q[i].z, q[i].w};
+            b.v = {v[i].x, v[i].y, v[i].z};
+            b.w = {w[i].x, w[i].y, w[i].z};
+        }
+        host_authoritative_ = true;
+    }
+
+    void step(float dt, uint32_t steps) {
+        if (!std::isfinite(dt) || dt <= 0.0f) throw std::invalid_argument("Native CPU timestep must be finite and positive");
+        check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+        ensure_device();
+        if (steps == 0) return;
+        for (int attempt = 0; attempt < 8; ++attempt) {
+            snapshot();
+            run_steps(dt, steps);
+            const uint32_t err = read_err();
+            if (!err) {
+                steps_done_ += steps;
+                return;
+            }
+            restore();
+            if (err & kErrPairCapacity) {
+                grow_pairs(d_.pair_cap * 2u);
+                continue;
+            }
+            throw std::overflow_error("Device step reported error bits " + std::to_string(err));
+        }
+        throw std::overflow_error("Pair capacity could not be satisfied");
+    }
+    void collide() {
+        check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+        ensure_device();
+        for (int attempt = 0; attempt < 8; ++attempt) {
+            snapshot();
+            check_cuda(cudaMemsetAsync(d_.err, 0, 4, stream_), "memset");
+            const DevState s = view(parity_);
+            enqueue_broadphase(s, stream_);
+            enqueue_narrowphase(s, stream_);
+            check_cuda(cudaGetLastError(), "collide launch");
+            const uint32_t err = read_err();
+            if (!err) {
+                last_cur_ = parity_;
+                parity_ ^= 1;
+                return;
+            }
+            restore();
+            if (err & kErrPairCapacity) { grow_pairs(d_.pair_cap * 2u); continue; }
+            throw std::overflow_error("Device collision reported error bits " + std::to_string(err));
+        }
+    }
+    void synchronize() { check_cuda(cudaStreamSynchronize(stream_), "synchronize"); }
+
+    void read_bodies(float* out, uint32_t n) {
+        if (n != bodies_.size()) throw std::invalid_argument("Body count mismatch");
+        if (!uploaded_ || host_authoritative_) {
+            for (uint32_t i = 0; i < n; ++i) pack_host(i, out + 14 * size_t(i));
+            return;
+        }
+        stage_.resize(size_t(n) * 4);
+        check_cuda(cudaMemcpyAsync(stage_.data(), d_.b_p, size_t(n) * 16, cudaMemcpyDeviceToHost, stream_), "read");
+        check_cuda(cudaMemcpyAsync(stage_.data() + n, d_.b_v, size_t(n) * 16, cudaMemcpyDeviceToHost, stream_), "read");
+        check_cuda(cudaMemcpyAsync(stage_.data() + 2 * size_t(n), d_.b_q, size_t(n) * 16, cudaMemcpyDeviceToHost, stream_), "read");
+        check_cuda(cudaMemcpyAsync(stage_.data() + 3 * size_t(n), d_.b_w, size_t(n) * 16, cudaMemcpyDeviceToHost, stream_), "read");
+        check_cuda(cudaStreamSynchronize(stream_), "read sync");
+        for (uint32_t i = 0; i < n; ++i) {
+            float* o = out + 14 * size_t(i);
+            const float4 p = stage_[i], v = stage_[n + i], q = stage_[2 * size_t(n) + i], w = stage_[3 * size_t(n) + i];
+            o[0] = p.x; o[1] = p.y; o[2] = p.z;
+            o[3] = v.x; o[4] = v.y; o[5] = v.z;
+            o[6] = q.x; o[7] = q.y; o[8] = q.z; o[9] = q.w;
+            o[10] = w.x; o[11] = w.y; o[12] = w.z; o[13] = 0.0f;
+        }
+    }
+    void body_state(uint32_t id, fyzz_b200_body_state_t* out) {
+        require_body(id);
+        float rec[14];
+        if (!uploaded_ || host_authoritative_) {
+            pack_host(id, rec);
+        } else {
+            float4 t[4];
+            check_cuda(cudaMemcpyAsync(&t[0], d_.b_p + id, 16, cudaMemcpyDeviceToHost, stream_), "read");
+            check_cuda(cudaMemcpyAsync(&t[1], d_.b_v + id, 16, cudaMemcpyDeviceToHost, stream_), "read");
+            check_cuda(cudaMemcpyAsync(&t[2], d_.b_q + id, 16, cudaMemcpyDeviceToHost, stream_), "read");
+            check_cuda(cudaMemcpyAsync(&t[3], d_.b_w + id, 16, cudaMemcpyDeviceToHost, stream_), "read");
+            check_cuda(cudaStreamSynchronize(stream_), "read sync");
+            const float r[14] = {t[0].x, t[0].y, t[0].z, t[1].x, t[1].y, t[1].z, t[2].x, t[2].y, t[2].z, t[2].w,
+                                 t[3].x, t[3].y, t[3].z, 0.0f};
+            std::memcpy(rec, r, sizeof rec);
+        }
+        std::memcpy(out->position, rec, 12);
+        std::memcpy(out->velocity, rec + 3, 12);
+        std::memcpy(out->orientation, rec + 6, 16);
+        std::memcpy(out->angular_velocity, rec + 10, 12);
+        out->sleeping = 0;
+    }
+    void write_velocities(const float* v6, uint32_t n) {
+        if (n != bodies_.size()) throw std::invalid_argument("Body count mismatch");
+        ensure_device();
+        stage_.resize(size_t(n) * 2);
+        for (uint32_t i = 0; i < n; ++i) {
+            const float* r = v6 + 6 * size_t(i);
+            const bool dyn = bodies_[i].dynamic;
+            stage_[i] = dyn ? make_float4(r[0], r[1], r[2], 0.0f) : make_float4(0, 0, 0, 0);
+            stage_[n + i] = dyn ? make_float4(r[3], r[4], r[5], 0.0f) : make_float4(0, 0, 0, 0);
+        }
+        check_cuda(cudaMemcpyAsync(d_.b_v, stage_.data(), size_t(n) * 16, cudaMemcpyHostToDevice, stream_), "write");
+        check_cuda(cudaMemcpyAsync(d_.b_w, stage_.data() + n, size_t(n) * 16, cudaMemcpyHostToDevice, stream_), "write");
+        check_cuda(cudaStreamSynchronize(stream_), "write sync");
+    }
+    void counts(uint64_t* out) {
+        out[0] = bodies_.size(); out[1] = shapes_.size(); out[2] = scene_body_begin_.size();
+        out[3] = out[4] = out[5] = out[6] = out[7] = 0;
+        out[8] = joints_.size(); out[9] = steps_done_;
+        if (!uploaded_) return;
+        const auto c = read_counters();
+        out[3] = c.pairs; out[4] = c.man; out[6] = c.desc; out[7] = c.isl;
+        std::vector<uint32_t> cnt(c.pairs);
+        if (c.pairs)
+            check_cuda(cudaMemcpy(cnt.data(), sets_[last_cur_].count, size_t(c.pairs) * 4, cudaMemcpyDeviceToHost), "read");
+        uint64_t pts = 0;
+        for (auto x : cnt) pts += x;
+        out[5] = pts;
+    }
+    void device_view(fyzz_b200_device_view_t* v) {
+        ensure_device();
+        v->position = d_.b_p; v->orientation = d_.b_q; v->velocity = d_.b_v; v->angular_velocity = d_.b_w;
+        v->n_bodies = d_.n_bodies; v->n_shapes = d_.n_shapes; v->stream = stream_;
+    }
+    uint64_t read_pairs(int which, uint32_t* out, uint64_t cap) {
+        if (!uploaded_) return 0;
+        const auto c = read_counters();
+        const ManagerSet& cur = sets_[last_cur_];
+        const ManagerSet& prev = sets_[last_cur_ ^ 1];
+        const uint32_t n = which == 2 ? c.prev_pairs : c.pairs;
+        std::vector<uint64_t> keys(n);
+        std::vector<uint32_t> flag(n, 1u);
+        if (n) {
+            check_cuda(cudaMemcpy(keys.data(), which == 2 ? prev.key : cur.key, size_t(n) * 8, cudaMemcpyDeviceToHost), "read");
+            if (which == 1) check_cuda(cudaMemcpy(flag.data(), d_.found_flag, size_t(n) * 4, cudaMemcpyDeviceToHost), "read");
+            if (which == 2) check_cuda(cudaMemcpy(flag.data(), d_.lost_flag, size_t(n) * 4, cudaMemcpyDeviceToHost), "read");
+        }
+        uint64_t k = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (!flag[i]) continue;
+            if (out && k < cap) { out[2 * k] = uint32_t(keys[i] >> 32); out[2 * k + 1] = uint32_t(keys[i]); }
+            ++k;
+        }
+        return k;
+    }
+    uint64_t read_manifolds(uint32_t* pairs, uint32_t* counts, float* points, uint64_t cap) {
+        if (!uploaded_) return 0;
+        const auto c = read_counters();
+        const ManagerSet& cur = sets_[last_cur_];
+        std::vector<uint64_t> keys(c.pairs);
+        std::vector<uint32_t> cnt(c.pairs);
+        std::vector<ContactPt> pts(size_t(c.pairs) * 4);
+        if (c.pairs) {
+            check_cuda(cudaMemcpy(keys.data(), cur.key, size_t(c.pairs) * 8, cudaMemcpyDeviceToHost), "read");
+            check_cuda(cudaMemcpy(cnt.data(), cur.count, size_t(c.pairs) * 4, cudaMemcpyDeviceToHost), "read");
+            check_cuda(cudaMemcpy(pts.data(), d_.pts, size_t(c.pairs) * 4 * sizeof(ContactPt), cudaMemcpyDeviceToHost), "read");
+        }
+        uint64_t k = 0;
+        for (uint32_t i = 0; i < c.pairs; ++i) {
+            if (!cnt[i]) continue;
+            if (pairs && k < cap) {
+                pairs[2 * k] = uint32_t(keys[i] >> 32);
+                pairs[2 * k + 1] = uint32_t(keys[i]);
+                counts[k] = cnt[i];
+                for (uint32_t j = 0; j < 4; ++j) {
+                    float* o = points + 28 * k + 7 * j;
+                    if (j < cnt[i]) {
+                        const ContactPt& p = pts[4 * size_t(i) + j];
+                        std::memcpy(o, p.p, 12); std::memcpy(o + 3, p.n, 12); o[6] = p.sep;
+                    } else {
+                        std::memset(o, 0, 28);
+                    }
+                }
+            }
+            ++k;
+        }
+        return k;
+    }
+    void read_bounds(uint32_t* out, uint32_t n) {
+        if (n != shapes_.size()) throw std::invalid_argument("Shape count mismatch");
+        ensure_device();
+        std::vector<uint4> lo(n), hi(n);
+        check_cuda(cudaMemcpy(lo.data(), d_.s_lo, size_t(n) * 16, cudaMemcpyDeviceToHost), "read");
+        check_cuda(cudaMemcpy(hi.data(), d_.s_hi, size_t(n) * 16, cudaMemcpyDeviceToHost), "read");
+        for (uint32_t i = 0; i < n; ++i) {
+            uint32_t* o = out + 6 * size_t(i);
+            o[0] = lo[i].x; o[1] = lo[i].y; o[2] = lo[i].z; o[3] = hi[i].x; o[4] = hi[i].y; o[5] = hi[i].z;
+        }
+    }
+    uint64_t read_sorted_min_x(uint32_t scene, uint32_t* values, uint32_t* ids, uint64_t cap) {
+        if (scene >= scene_body_begin_.size()) throw std::out_of_range("Unknown scene");
+        ensure_device();
+        const uint32_t b = h_fbegin_[scene], e = h_fbegin_[scene + 1];
+        const uint64_t n = e - b;
+        if (values && n) {
+            const uint64_t m = std::min<uint64_t>(n, cap);
+            check_cuda(cudaMemcpy(values, d_.srt_key + b, m * 4, cudaMemcpyDeviceToHost), "read");
+            check_cuda(cudaMemcpy(ids, d_.srt_id + b, m * 4, cudaMemcpyDeviceToHost), "read");
+        }
+        return n;
+    }
+    uint64_t read_levels(uint32_t* levels, uint64_t cap) {
+        if (!uploaded_) return 0;
+        const auto c = read_counters();
+        if (levels && c.desc)
+            check_cuda(cudaMemcpy(levels, d_.d_level, std::min<uint64_t>(c.desc, cap) * 4, cudaMemcpyDeviceToHost), "read");
+        return c.desc;
+    }
+    uint32_t error_bits() const { return last_err_; }
+    uint32_t last_shape() const { return uint32_t(shapes_.size() - 1); }
+    size_t n_bodies() const { return bodies_.size(); }
+
+private:
+    struct Counters { uint32_t pairs, prev_pairs, man, desc, isl; };
+    Counters read_counters() {
+        uint32_t h[8] = {};
+        check_cuda(cudaStreamSynchronize(stream_), "sync");
+        check_cuda(cudaMemcpy(h, d_.counters, sizeof h, cudaMemcpyDeviceToHost), "read");
+        uint32_t np = 0, npp = 0, ni = 0;
+        check_cuda(cudaMemcpy(&np, sets_[last_cur_].n, 4, cudaMemcpyDeviceToHost), "read");
+        check_cuda(cudaMemcpy(&npp, sets_[last_cur_ ^ 1].n, 4, cudaMemcpyDeviceToHost), "read");
+        check_cuda(cudaMemcpy(&ni, d_.n_isl, 4, cudaMemcpyDeviceToHost), "read");
+        return {np, npp, h[kCntMan], h[kCntDesc], ni};
+    }
+    void pack_host(uint32_t i, float* o) const {
+        const HostBody& b = bodies_[i];
+        o[0] = b.p[0]; o[1] = b.p[1]; o[2] = b.p[2];
+        o[3] = b.v[0]; o[4] = b.v[1]; o[5] = b.v[2];
+        o[6] = b.q[0]; o[7] = b.q[1]; o[8] = b.q[2]; o[9] = b.q[3];
+        o[10] = b.w[0]; o[11] = b.w[1]; o[12] = b.w[2]; o[13] = 0.0f;
+    }
+    DevState view(int parity) const {
+        DevState s = d_;
+        s.cur = sets_[parity];
+        s.prev = sets_[parity ^ 1];
+        return s;
+    }
+    uint32_t read_err() {
+        check_cuda(cudaMemcpyAsync(host_err_, d_.err, 4, cudaMemcpyDeviceToHost, stream_), "err");
+        check_cuda(cudaStreamSynchronize(stream_), "step sync");
+        last_err_ = host_err_[0];
+        return last_err_;
+    }
+    void run_steps(float dt, uint32_t steps) {
+        if (dt != graph_dt_) {
+            for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+            graph_dt_ = dt;
+        }
+        d_.dt = dt;
+        check_cuda(cudaMemsetAsync(d_.err, 0, 4, stream_), "memset");
+        for (uint32_t i = 0; i < steps; ++i) {
+            if (!graphs_[parity_]) {
+                cudaGraph_t g;
+                check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
+                const DevState s = view(parity_);
+                enqueue_broadphase(s, stream_);
+                enqueue_narrowphase(s, stream_);
+                enqueue_solver(s, stream_);
+                check_cuda(cudaStreamEndCapture(stream_, &g), "end capture");
+                check_cuda(cudaGraphInstantiate(&graphs_[parity_], g, 0), "instantiate");
+                cudaGraphDestroy(g);
+            }
+            check_cuda(cudaGraphLaunch(graphs_[parity_], stream_), "graph launch");
+            last_cur_ = parity_;
+            parity_ ^= 1;
+        }
+    }
+    void snapshot() {
+        const size_t n = size_t(d_.n_bodies) * 16;
+        check_cuda(cudaMemcpyAsync(bk_p_, d_.b_p, n, cudaMemcpyDeviceToDevice, stream_), "snapshot");
+        check_cuda(cudaMemcpyAsync(bk_q_, d_.b_q, n, cudaMemcpyDeviceToDevice, stream_), "snapshot");
+        check_cuda(cudaMemcpyAsync(bk_v_, d_.b_v, n, cudaMemcpyDeviceToDevice, stream_), "snapshot");
+        check_cuda(cudaMemcpyAsync(bk_w_, d_.b_w, n, cudaMemcpyDeviceToDevice, stream_), "snapshot");
+        snap_parity_ = parity_;
+        snap_last_ = last_cur_;
+    }
+    void restore() {
+        const size_t n = size_t(d_.n_bodies) * 16;
+        check_cuda(cudaMemcpyAsync(d_.b_p, bk_p_, n, cudaMemcpyDeviceToDevice, stream_), "restore");
+        check_cuda(cudaMemcpyAsync(d_.b_q, bk_q_, n, cudaMemcpyDeviceToDevice, stream_), "restore");
+        check_cuda(cudaMemcpyAsync(d_.b_v, bk_v_, n, cudaMemcpyDeviceToDevice, stream_), "restore");
+        check_cuda(cudaMemcpyAsync(d_.b_w, bk_w_, n, cudaMemcpyDeviceToDevice, stream_), "restore");
+        // contact-manager history is discarded, as after a reference rollback
+        check_cuda(cudaMemsetAsync(sets_[0].n, 0, 4, stream_), "restore");
+        check_cuda(cudaMemsetAsync(sets_[1].n, 0, 4, stream_), "restore");
+        check_cuda(cudaMemsetAsync(d_.err, 0, 4, stream_), "restore");
+        check_cuda(cudaStreamSynchronize(stream_), "restore sync");
+        parity_ = snap_parity_;
+        last_cur_ = snap_last_;
+    }
+
+    void release_device() {
+        for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        for (void* p : owned_) cudaFree(p);
+        owned_.clear();
+        for (void* p : pair_owned_) cudaFree(p);
+        pair_owned_.clear();
+        uploaded_ = false;
+    }
+
+    void alloc_pairs(uint32_t cap) {
+        for (void* p : pair_owned_) cudaFree(p);
+        pair_owned_.clear();
+        for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        d_.pair_cap = cap;
+        d_.desc_cap = cap + d_.n_joints;
+        for (int k = 0; k < 2; ++k) {
+            dalloc(sets_[k].key, cap, pair_owned_);
+            dalloc(sets_[k].cache, cap, pair_owned_);
+            dalloc(sets_[k].fric, cap, pair_owned_);
+            dalloc(sets_[k].count, cap, pair_owned_);
+            dalloc(sets_[k].n, 1, pair_owned_);
+            check_cuda(cudaMemsetAsync(sets_[k].n, 0, 4, stream_), "memset");
+        }
+        dalloc(d_.prev_idx, cap, pair_owned_);
+        dalloc(d_.found_flag, cap, pair_owned_);
+        dalloc(d_.lost_flag, cap, pair_owned_);
+        dalloc(d_.pts, size_t(cap) * 4, pair_owned_);
+        dalloc(d_.man_list, cap, pair_owned_);
+        dalloc(d_.mh, cap, pair_owned_);
+        dalloc(d_.nrow, size_t(cap) * 4, pair_owned_);
+        dalloc(d_.frow, size_t(cap) * 4, pair_owned_);
+        const uint32_t dc = d_.desc_cap;
+        dalloc(d_.d_key, dc, pair_owned_); dalloc(d_.d_val, dc, pair_owned_);
+        dalloc(d_.d_key2, dc, pair_owned_); dalloc(d_.d_val2, dc, pair_owned_);
+        dalloc(d_.d_level, dc, pair_owned_);
+        dalloc(d_.isl_begin, size_t(dc) + 1, pair_owned_);
+        dalloc(d_.isl_end, size_t(dc) + 1, pair_owned_);
+        dalloc(d_.isl_flag, dc, pair_owned_);
+        dalloc(d_.tmp_flags, cap, pair_owned_);
+        dalloc(d_.tmp_pos, std::max(cap, dc), pair_owned_);
+        dalloc(d_.lvl_bound, 2 * size_t(dc) + 2, pair_owned_);
+        const uint32_t big = std::max({cap, dc, d_.n_shapes, d_.n_finite, 256u * 64u});
+        d_.scan_tmp_words = scan_tmp_words_for(std::max<uint32_t>(big, uint32_t(radix_hist_words(big))));
+        dalloc(d_.scan_tmp, d_.scan_tmp_words, pair_owned_);
+        d_.sort_hist_words = radix_hist_words(big);
+        dalloc(d_.sort_hist, d_.sort_hist_words, pair_owned_);
+    }
+    void grow_pairs(uint32_t cap) {
+        alloc_pairs(cap);
+        parity_ = 0;
+        last_cur_ = 1;
+    }
+
+    void upload_bodies() {
+        const uint32_t nb = uint32_t(bodies_.size());
+        std::vector<float4> p(nb), q(nb), v(nb), w(nb), inv(nb), mlp(nb), mlq(nb);
+        for (uint32_t i = 0; i < nb; ++i) {
+            const HostBody& b = bodies_[i];
+            p[i] = make_float4(b.p[0], b.p[1], b.p[2], b.inv_mass);
+            q[i] = make_float4(b.q[0], b.q[1], b.q[2], b.q[3]);
+            v[i] = make_float4(b.v[0], b.v[1], b.v[2], 0);
+            w[i] = make_float4(b.w[0], b.w[1], b.w[2], 0);
+            inv[i] = make_float4(b.inv_inertia[0], b.inv_inertia[1], b.inv_inertia[2], b.dynamic ? b.inv_mass : 0.0f);
+            mlp[i] = make_float4(b.ml_p[0], b.ml_p[1], b.ml_p[2], 0);
+            mlq[i] = make_float4(b.ml_q[0], b.ml_q[1], b.ml_q[2], b.ml_q[3]);
+        }
+        upload(d_.b_p, p, stream_); upload(d_.b_q, q, stream_); upload(d_.b_v, v, stream_);
+        upload(d_.b_w, w, stream_); upload(d_.b_inv, inv, stream_);
+        upload(d_.b_ml_p, mlp, stream_); upload(d_.b_ml_q, mlq, stream_);
+        std::vector<float4> mat(shapes_.size());
+        for (size_t i = 0; i < shapes_.size(); ++i)
+            mat[i] = make_float4(shapes_[i].mat[0], shapes_[i].mat[1], shapes_[i].mat[2], shapes_[i].mat[3]);
+        upload(d_.s_mat, mat, stream_);
+        check_cuda(cudaStreamSynchronize(stream_), "upload sync");
+        host_authoritative_ = false;
+    }
+
+    void build_device() {
+        release_device();
+        DevState d;
+        const uint32_t nb = uint32_t(bodies_.size()), ns = uint32_t(shapes_.size());
+        const uint32_t nsc = uint32_t(scene_body_begin_.size());
+        d.n_scenes = nsc;
+        d.n_bodies = nb;
+        d.n_shapes = ns;
+        d.n_joints = uint32_t(joints_.size());
+        // finite ranks, scene ranges, plane pairs
+        std::vector<int32_t> frank(ns, -1), dynrank(ns, -1);
+        std::vector<uint32_t> sscene(ns), sbody(ns), stype(ns), static_pairs(ns, 0);
+        std::vector<uint32_t> fbegin(nsc + 1, 0);
+        std::vector<int32_t> plane(nsc, -1);
+        uint32_t nf = 0, n_dyn_finite = 0;
+        for (uint32_t sc = 0; sc < nsc; ++sc) {
+            fbegin[sc] = nf;
+            const uint32_t s0 = scene_shape_begin_[sc];
+            const uint32_t s1 = sc + 1 < nsc ? scene_shape_begin_[sc + 1] : ns;
+            for (uint32_t i = s0; i < s1; ++i)
+                if (shapes_[i].type == kPlane) plane[sc] = int32_t(i);
+            uint32_t owned_by_plane = 0;
+            for (uint32_t i = s0; i < s1; ++i) {
+                const HostShape& s = shapes_[i];
+                sscene[i] = sc; sbody[i] = s.body; stype[i] = s.type;
+                if (s.type == kPlane) continue;
+                frank[i] = int32_t(nf++);
+                if (!bodies_[s.body].dynamic || plane[sc] < 0) continue;
+                ++n_dyn_finite;
+                if (uint32_t(plane[sc]) < i) {
+                    dynrank[i] = int32_t(owned_by_plane++);
+                    ++static_pairs[uint32_t(plane[sc])];
+                } else {
+                    ++static_pairs[i];
+                }
+            }
+        }
+        fbegin[nsc] = nf;
+        d.n_finite = nf;
+        h_fbegin_ = fbegin;
+        std::vector<uint32_t> small;
+        d.n_large = 0;
+        for (uint32_t sc = 0; sc < nsc; ++sc) {
+            const uint32_t n = fbegin[sc + 1] - fbegin[sc];
+            if (n == 0) continue;
+            if (n <= d.max_small_scene) small.push_back(sc);
+            else {
+                if (d.n_large >= DevState::kMaxLarge) throw std::logic_error("Too many scenes above the per-CTA sort size");
+                d.large_begin[d.n_large] = fbegin[sc];
+                d.large_n[d.n_large] = n;
+                ++d.n_large;
+            }
+        }
+        d.n_small = uint32_t(small.size());
+        d_ = d;
+        // allocations
+        dalloc(d_.sc_fbegin, nsc + 1, owned_); dalloc(d_.sc_plane, nsc, owned_);
+        dalloc(d_.small_scenes, small.size(), owned_);
+        dalloc(d_.b_p, nb, owned_); dalloc(d_.b_q, nb, owned_); dalloc(d_.b_v, nb, owned_); dalloc(d_.b_w, nb, owned_);
+        dalloc(d_.b_inv, nb, owned_); dalloc(d_.b_ml_p, nb, owned_); dalloc(d_.b_ml_q, nb, owned_);
+        dalloc(d_.b_dyn0, nb, owned_); dalloc(d_.b_dyn1, nb, owned_);
+        dalloc(d_.b_flags, nb, owned_); dalloc(d_.b_scene, nb, owned_);
+        dalloc(bk_p_, nb, owned_); dalloc(bk_q_, nb, owned_); dalloc(bk_v_, nb, owned_); dalloc(bk_w_, nb, owned_);
+        dalloc(d_.s_body, ns, owned_); dalloc(d_.s_type, ns, owned_); dalloc(d_.s_scene, ns, owned_);
+        dalloc(d_.s_geom, ns, owned_); dalloc(d_.s_lp, ns, owned_); dalloc(d_.s_lq, ns, owned_);
+        dalloc(d_.s_mat, ns, owned_); dalloc(d_.s_wp, ns, owned_); dalloc(d_.s_wq, ns, owned_);
+        dalloc(d_.s_lo, ns, owned_); dalloc(d_.s_hi, ns, owned_);
+        dalloc(d_.s_frank, ns, owned_); dalloc(d_.s_dynrank, ns, owned_); dalloc(d_.s_static_pairs, ns, owned_);
+        dalloc(d_.srt_key, nf, owned_); dalloc(d_.srt_id, nf, owned_);
+        dalloc(d_.srt_key2, nf, owned_); dalloc(d_.srt_id2, nf, owned_);
+        dalloc(d_.sw_rec, nf, owned_); dalloc(d_.sw_meta, nf, owned_);
+        dalloc(d_.own_cnt, ns, owned_); dalloc(d_.own_off, ns, owned_); dalloc(d_.own_cur, ns, owned_);
+        dalloc(d_.j_a, joints_.size(), owned_); dalloc(d_.j_b, joints_.size(), owned_);
+        dalloc(d_.j_len, joints_.size(), owned_); dalloc(d_.jrow, joints_.size(), owned_);
+        dalloc(d_.sb_dv, nb, owned_); dalloc(d_.sb_dw, nb, owned_); dalloc(d_.sb_mdv, nb, owned_);
+        dalloc(d_.sb_mdw, nb, owned_); dalloc(d_.sb_v, nb, owned_); dalloc(d_.sb_w, nb, owned_);
+        dalloc(d_.sb_sqrt_i, size_t(nb) * 3, owned_);
+        dalloc(d_.uf_parent, nb, owned_);
+        dalloc(d_.sb_mask, nb, owned_); dalloc(d_.sb_maxdyn, nb, owned_); dalloc(d_.sb_static, nb, owned_);
+        dalloc(d_.n_isl, 1, owned_);
+        dalloc(d_.n_man, 1, owned_);
+        dalloc(d_.counters, kCntSlots, owned_);
+        dalloc(d_.err, 1, owned_);
+        check_cuda(cudaMemsetAsync(d_.counters, 0, kCntSlots * 4, stream_), "memset");
+        check_cuda(cudaMemsetAsync(d_.err, 0, 4, stream_), "memset");
+        check_cuda(cudaMemsetAsync(d_.s_lo, 0, size_t(ns) * 16, stream_), "memset");
+        check_cuda(cudaMemsetAsync(d_.s_hi, 0, size_t(ns) * 16, stream_), "memset");
+        check_cuda(cudaMemsetAsync(d_.n_isl, 0, 4, stream_), "memset");
+        // host tables
+        std::vector<float4> dyn0(nb, make_float4(0.0f, 0.05f, 1.0e16f, 100.0f));
+        std::vector<float4> dyn1(nb, make_float4(1.0e32f, FLT_MAX, 0.0f, 0.0f));
+        std::vector<uint32_t> flags(nb), bscene(nb);
+        for (uint32_t i = 0; i < nb; ++i) {
+            flags[i] = bodies_[i].dynamic ? kBodyDynamic : 0u;
+            bscene[i] = bodies_[i].scene;
+        }
+        std::vector<float4> geom(ns), lp(ns), lq(ns);
+        for (uint32_t i = 0; i < ns; ++i) {
+            const HostShape& s = shapes_[i];
+            geom[i] = make_float4(s.half[0], s.half[1], s.half[2], s.radius);
+            lp[i] = make_float4(s.lp[0], s.lp[1], s.lp[2], s.contact_offset);
+            lq[i] = make_float4(s.lq[0], s.lq[1], s.lq[2], s.lq[3]);
+        }
+        // joints: per scene, constraint slot descending (scene.cpp:7153-7162)
+        std::vector<HostJoint> js = joints_;
+        std::stable_sort(js.begin(), js.end(), [](const HostJoint& a, const HostJoint& b) {
+            return a.scene != b.scene ? a.scene < b.scene : a.slot > b.slot;
+        });
+        std::vector<uint32_t> ja(js.size()), jb(js.size());
+        std::vector<float> jl(js.size());
+        for (size_t i = 0; i < js.size(); ++i) { ja[i] = js[i].a; jb[i] = js[i].b; jl[i] = js[i].len; }
+        upload(d_.sc_fbegin, fbegin, stream_); upload(d_.sc_plane, plane, stream_);
+        upload(d_.small_scenes, small, stream_);
+        upload(d_.b_dyn0, dyn0, stream_); upload(d_.b_dyn1, dyn1, stream_);
+        upload(d_.b_flags, flags, stream_); upload(d_.b_scene, bscene, stream_);
+        upload(d_.s_body, sbody, stream_); upload(d_.s_type, stype, stream_); upload(d_.s_scene, sscene, stream_);
+        upload(d_.s_geom, geom, stream_); upload(d_.s_lp, lp, stream_); upload(d_.s_lq, lq, stream_);
+        upload(d_.s_frank, frank, stream_); upload(d_.s_dynrank, dynrank, stream_);
+        upload(d_.s_static_pairs, static_pairs, stream_);
+        upload(d_.j_a, ja, stream_); upload(d_.j_b, jb, stream_); upload(d_.j_len, jl, stream_);
+        uploaded_ = true;
+        upload_bodies();
+        // pair capacity: every plane pair plus a generous overlap budget
+        const uint64_t cap = uint64_t(n_dyn_finite) + 8ull * nf + 4096ull;
+        alloc_pairs(uint32_t(std::min<uint64_t>(cap, 0x7fffffffull)));
+        parity_ = 0;
+        last_cur_ = 1;
+        topology_dirty_ = false;
+        check_cuda(cudaStreamSynchronize(stream_), "build sync");
+    }
+
+    int device_ = 0;
+    cudaStream_t stream_ = nullptr;
+    std::vector<HostBody> bodies_;
+    std::vector<HostShape> shapes_;
+    std::vector<HostJoint> joints_;
+    std::vector<uint32_t> scene_body_begin_, scene_shape_begin_;
+    std::vector<bool> scene_has_floor_;
+    std::vector<uint32_t> h_fbegin_;
+    bool topology_dirty_ = true, mass_dirty_ = false, uploaded_ = false, host_authoritative_ = true;
+    DevState d_;
+    ManagerSet sets_[2];
+    std::vector<void*> owned_, pair_owned_;
+    float4 *bk_p_ = nullptr, *bk_q_ = nullptr, *bk_v_ = nullptr, *bk_w_ = nullptr;
+    cudaGraphExec_t graphs_[2] = {nullptr, nullptr};
+    float graph_dt_ = -1.0f;
+    int parity_ = 0, last_cur_ = 1, snap_parity_ = 0, snap_last_ = 1;
+    uint64_t steps_done_ = 0;
+    uint32_t last_err_ = 0;
+    uint32_t* host_err_ = nullptr;
+    std::vector<float4> stage_;
+};
+
+}  // namespace fyzz::b200
+
+// ------------------------------------------------------------------ C ABI
+struct fyzz_b200_world {
+    fyzz::b200::World* impl = nullptr;
+    std::string error;
+};
+
+namespace {
+template <class F> int guarded(fyzz_b200_world* w, F&& f) {
+    if (!w || !w->impl) return FYZZ_B200_INVALID_ARGUMENT;
+    try {
+        f(*w->impl);
+        w->error.clear();
+        return FYZZ_B200_OK;
+    } catch (const std::invalid_argument& e) {
+        w->error = e.what(); return FYZZ_B200_INVALID_ARGUMENT;
+    } catch (const std::out_of_range& e) {
+        w->error = e.what(); return FYZZ_B200_INVALID_ARGUMENT;
+    } catch (const std::overflow_error& e) {
+        w->error = e.what(); return FYZZ_B200_OVERFLOW;
+    } catch (const std::logic_error& e) {
+        w->error = e.what(); return FYZZ_B200_LOGIC_ERROR;
+    } catch (const std::exception& e) {
+        w->error = e.what(); return FYZZ_B200_RUNTIME_ERROR;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int fyzz_b200_create(int device, fyzz_b200_world** out) {
+    if (!out) return FYZZ_B200_INVALID_ARGUMENT;
+    try {
+        auto* w = new fyzz_b200_world;
+        w->impl = new fyzz::b200::World(device);
+        *out = w;
+        return FYZZ_B200_OK;
+    } catch (const std::exception&) {
+        *out = nullptr;
+        return FYZZ_B200_RUNTIME_ERROR;
+    }
+}
+int fyzz_b200_destroy(fyzz_b200_world* w) {
+    if (!w) return FYZZ_B200_INVALID_ARGUMENT;
+    delete w->impl;
+    delete w;
+    return FYZZ_B200_OK;
+}
+const char* fyzz_b200_last_error(const fyzz_b200_world* w) { return w ? w->error.c_str() : "null world"; }
+int fyzz_b200_error_bits(const fyzz_b200_world* w, uint32_t* bits) {
+    if (!w || !w->impl || !bits) return FYZZ_B200_INVALID_ARGUMENT;
+    *bits = w->impl->error_bits();
+    return FYZZ_B200_OK;
+}
+int fyzz_b200_begin_scene(fyzz_b200_world* w, uint32_t* out) {
+    return guarded(w, [&](auto& W) { const uint32_t s = W.begin_scene(); if (out) *out = s; });
+}
+int fyzz_b200_add_static_floor(fyzz_b200_world* w, float h, uint32_t* out) {
+    return guarded(w, [&](auto& W) { const uint32_t b = W.add_static_floor(h); if (out) *out = b; });
+}
+int fyzz_b200_create_dynamic_body(fyzz_b200_world* w, const float pose[7], uint32_t* out) {
+    if (!pose) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) { const uint32_t b = W.create_dynamic_body(pose); if (out) *out = b; });
+}
+int fyzz_b200_attach_box_shape(fyzz_b200_world* w, uint32_t body, const float half[3], const float local[7], uint32_t* out) {
+    if (!half) return FYZZ_B200_INVALID_ARGUMENT;
+    static const float identity[7] = {0, 0, 0, 0, 0, 0, 1};
+    return guarded(w, [&](auto& W) {
+        const uint32_t s = W.attach(body, fyzz::b200::kBox, half, 0.0f, local ? local : identity);
+        if (out) *out = s;
+    });
+}
+int fyzz_b200_attach_sphere_shape(fyzz_b200_world* w, uint32_t body, float r, const float local[7], uint32_t* out) {
+    static const float identity[7] = {0, 0, 0, 0, 0, 0, 1};
+    static const float none[3] = {0, 0, 0};
+    return guarded(w, [&](auto& W) {
+        const uint32_t s = W.attach(body, fyzz::b200::kSphere, none, r, local ? local : identity);
+        if (out) *out = s;
+    });
+}
+int fyzz_b200_update_mass_properties(fyzz_b200_world* w, uint32_t body, float density) {
+    return guarded(w, [&](auto& W) { W.update_mass_properties(body, density); });
+}
+int fyzz_b200_body_mass_properties(const fyzz_b200_world* w, uint32_t body, float out[11]) {
+    if (!out) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(const_cast<fyzz_b200_world*>(w), [&](auto& W) { W.mass_props(body, out); });
+}
+int fyzz_b200_set_shape_material(fyzz_b200_world* w, uint32_t shape, const fyzz_b200_material* m) {
+    if (!m) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) { W.set_shape_material(shape, *m); });
+}
+int fyzz_b200_set_body_velocity(fyzz_b200_world* w, uint32_t body, const float v[3]) {
+    if (!v) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) { W.set_velocity(body, v, false); });
+}
+int fyzz_b200_set_body_angular_velocity(fyzz_b200_world* w, uint32_t body, const float v[3]) {
+    if (!v) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) { W.set_velocity(body, v, true); });
+}
+int fyzz_b200_add_center_distance_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b, float d, uint64_t* out) {
+    return guarded(w, [&](auto& W) { const uint64_t id = W.add_distance(a, b, d); if (out) *out = id; });
+}
+int fyzz_b200_add_scene(fyzz_b200_world* w, uint32_t nb, const float* bodies, uint32_t ns,
+                        const uint32_t* shape_body, const uint32_t* shape_type, const float* shape_geom,
+                        const float* shape_local, const float* shape_mat, uint32_t nj,
+                        const uint32_t* joint_bodies, const float* joint_dist, int has_floor,
+                        float floor_height, const float* floor_mat, uint32_t* first_body_out) {
+    if ((nb && !bodies) || (ns && (!shape_body || !shape_type || !shape_geom || !shape_local || !shape_mat)) ||
+        (nj && (!joint_bodies || !joint_dist)))
+        return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) {
+        W.begin_scene();
+        if (has_floor) {
+            W.add_static_floor(floor_height);
+            if (floor_mat) {
+                const fyzz_b200_material m{floor_mat[0], floor_mat[1], floor_mat[2]};
+                W.set_shape_material(W.last_shape(), m);
+            }
+        }
+        std::vector<uint32_t> body_id(nb), shape_id(ns);
+        uint32_t si = 0;
+        for (uint32_t b = 0; b < nb; ++b) {
+            const float* r = bodies + 14 * size_t(b);
+            body_id[b] = W.create_dynamic_body(r);
+            if (b == 0 && first_body_out) *first_body_out = body_id[b];
+            while (si < ns && shape_body[si] == b) {
+                const float* g = shape_geom + 4 * size_t(si);
+                shape_id[si] = shape_type[si] == 0
+                    ? W.attach(body_id[b], fyzz::b200::kBox, g, 0.0f, shape_local + 7 * size_t(si))
+                    : W.attach(body_id[b], fyzz::b200::kSphere, g, g[0], shape_local + 7 * size_t(si));
+                ++si;
+            }
+            W.update_mass_properties(body_id[b], r[13]);
+        }
+        if (si != ns) throw std::invalid_argument("shape_body must be grouped and ascending");
+        for (uint32_t i = 0; i < ns; ++i) {
+            const fyzz_b200_material m{shape_mat[3 * i], shape_mat[3 * i + 1], shape_mat[3 * i + 2]};
+            W.set_shape_material(shape_id[i], m);
+        }
+        for (uint32_t b = 0; b < nb; ++b) {
+            const float* r = bodies + 14 * size_t(b);
+            W.set_velocity(body_id[b], r + 7, false);
+            W.set_velocity(body_id[b], r + 10, true);
+        }
+        for (uint32_t j = 0; j < nj; ++j)
+            W.add_distance(body_id[joint_bodies[2 * j]], body_id[joint_bodies[2 * j + 1]], joint_dist[j]);
+    });
+}
+int fyzz_b200_step(fyzz_b200_world* w, float dt) {
+    return guarded(w, [&](auto& W) { W.step(dt, 1); });
+}
+int fyzz_b200_step_n(fyzz_b200_world* w, float dt, uint32_t steps) {
+    return guarded(w, [&](auto& W) { W.step(dt, steps); });
+}
+int fyzz_b200_collide(fyzz_b200_world* w) {
+    return guarded(w, [&](auto& W) { W.collide(); });
+}
+int fyzz_b200_synchronize(fyzz_b200_world* w) {
+    return guarded(w, [&](auto& W) { W.synchronize(); });
+}
+int fyzz_b200_body_state(const fyzz_b200_world* w, uint32_t body, fyzz_b200_body_state_t* out) {
+    if (!out) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(const_cast<fyzz_b200_world*>(w), [&](auto& W) { W.body_state(body, out); });
+}
+int fyzz_b200_read_bodies(fyzz_b200_world* w, float* out, uint32_t n) {
+    if (!out) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) { W.read_bodies(out, n); });
+}
+int fyzz_b200_write_velocities(fyzz_b200_world* w, const float* v6, uint32_t n) {
+    if (!v6) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) { W.write_velocities(v6, n); });
+}
+int fyzz_b200_counts(fyzz_b200_world* w, uint64_t out[10]) {
+    if (!out) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) { W.counts(out); });
+}
+int fyzz_b200_device_view(fyzz_b200_world* w, fyzz_b200_device_view_t* out) {
+    if (!out) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) { W.device_view(out); });
+}
+uint64_t fyzz_b200_read_pairs(fyzz_b200_world* w, int which, uint32_t* out, uint64_t cap) {
+    uint64_t n = 0;
+    if (guarded(w, [&](auto& W) { n = W.read_pairs(which, out, cap); })) return 0;
+    return n;
+}
+uint64_t fyzz_b200_read_manifolds(fyzz_b200_world* w, uint32_t* pairs, uint32_t* counts, float* points, uint64_t cap) {
+    uint64_t n = 0;
+    if (guarded(w, [&](auto& W) { n = W.read_manifolds(pairs, counts, points, cap); })) return 0;
+    return n;
+}
+int fyzz_b200_read_encoded_bounds(fyzz_b200_world* w, uint32_t* out, uint32_t n) {
+    if (!out) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) { W.read_bounds(out, n); });
+}
+uint64_t fyzz_b200_read_sorted_min_x(fyzz_b200_world* w, uint32_t scene, uint32_t* values, uint32_t* ids, uint64_t cap) {
+    uint64_t n = 0;
+    if (guarded(w, [&](auto& W) { n = W.read_sorted_min_x(scene, values, ids, cap); })) return 0;
+    return n;
+}
+uint64_t fyzz_b200_read_levels(fyzz_b200_world* w, uint32_t* levels, uint64_t cap) {
+    uint64_t n = 0;
+    if (guarded(w, [&](auto& W) { n = W.read_levels(levels, cap); })) return 0;
+    return n;
+}
+
+}  // extern "C"

@@ -1,0 +1,163 @@
+/* fyzz_b200.h - C ABI of the B200 rigid-body step.
+ *
+ * A drop-in for the FyzzXYZZY NativePortableGpu step: the entry points mirror
+ * fyzz::World / fyzz::WorldBackend (include/fyzzxyzzy/world.h:226-510 of the
+ * reference) and its GPU factory create_native_gpu_world
+ * (include/fyzzxyzzy/native_gpu_world.h:90-138).  Plain pointers and sizes
+ * only; no C++ or torch types cross this boundary.
+ *
+ * Status codes map 1:1 to the reference's exception types
+ * (world.h, src/native/scene.cpp): 1 std::invalid_argument,
+ * 2 std::logic_error, 3 std::overflow_error, 4 std::runtime_error.
+ *
+ * Identifiers.  Body and shape ids are world-global, allocated in creation
+ * order like the reference's BodyId / ShapeId (scene.cpp:192-252).  A world
+ * holds one scene unless fyzz_b200_begin_scene is called; scenes are
+ * independent (no pairs across scenes) and are stepped together.
+ *
+ * Threading: a world is not thread-safe (reference compute.h:265).
+ */
+#ifndef FYZZ_B200_H
+#define FYZZ_B200_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    FYZZ_B200_OK = 0,
+    FYZZ_B200_INVALID_ARGUMENT = 1,
+    FYZZ_B200_LOGIC_ERROR = 2,
+    FYZZ_B200_OVERFLOW = 3,
+    FYZZ_B200_RUNTIME_ERROR = 4
+};
+
+typedef struct fyzz_b200_world fyzz_b200_world;
+
+/* fyzz::Material (world.h:78-90): friction / restitution used by the step. */
+typedef struct {
+    float static_friction;
+    float dynamic_friction;
+    float restitution;
+} fyzz_b200_material;
+
+/* fyzz::BodyState (world.h:201-212). */
+typedef struct {
+    float position[3];
+    float velocity[3];
+    float orientation[4]; /* x, y, z, w */
+    float angular_velocity[3];
+    uint32_t sleeping;
+} fyzz_b200_body_state_t;
+
+/* Device pointers of the resident state, for callers that keep their
+ * inputs in HBM (float4 records: xyz + pad; see fyzz_b200_read_bodies for
+ * the host layout). */
+typedef struct {
+    void* position;         /* float4 per body, w = inverse mass */
+    void* orientation;      /* float4 per body */
+    void* velocity;         /* float4 per body */
+    void* angular_velocity; /* float4 per body */
+    uint32_t n_bodies;
+    uint32_t n_shapes;
+    void* stream;           /* cudaStream_t the world launches on */
+} fyzz_b200_device_view_t;
+
+/* ---- lifecycle: create_native_gpu_world (native_gpu_world.h:90-138) ---- */
+int fyzz_b200_create(int device, fyzz_b200_world** out);
+int fyzz_b200_destroy(fyzz_b200_world* w);
+/* Message of the last failed call on this world (valid until the next call). */
+const char* fyzz_b200_last_error(const fyzz_b200_world* w);
+/* Device error bits of the last step (source_dy_distance_native.h:1336-1345). */
+int fyzz_b200_error_bits(const fyzz_b200_world* w, uint32_t* bits);
+
+/* ---- authoring: WorldBackend (world.h:226-394) ---- */
+/* New independent scene; later bodies belong to it.  (No reference
+ * counterpart: the reference World holds exactly one scene.) */
+int fyzz_b200_begin_scene(fyzz_b200_world* w, uint32_t* scene_out);
+/* World::add_static_floor (world.h:424) */
+int fyzz_b200_add_static_floor(fyzz_b200_world* w, float height, uint32_t* body_out);
+/* World::create_dynamic_body (world.h:409); pose = position(3) + quaternion xyzw(4) */
+int fyzz_b200_create_dynamic_body(fyzz_b200_world* w, const float pose[7], uint32_t* body_out);
+/* World::attach_box_shape (world.h:410) */
+int fyzz_b200_attach_box_shape(fyzz_b200_world* w, uint32_t body, const float half_extents[3],
+                               const float local_pose[7], uint32_t* shape_out);
+/* World::attach_sphere_shape (world.h:411) */
+int fyzz_b200_attach_sphere_shape(fyzz_b200_world* w, uint32_t body, float radius,
+                                  const float local_pose[7], uint32_t* shape_out);
+/* World::update_mass_properties (world.h:420, compound.cpp:113-203) */
+int fyzz_b200_update_mass_properties(fyzz_b200_world* w, uint32_t body, float density);
+/* World::body_mass_properties (world.h:421): inverse mass, inverse inertia(3),
+ * mass-local position(3), mass-local orientation(4). */
+int fyzz_b200_body_mass_properties(const fyzz_b200_world* w, uint32_t body, float out[11]);
+/* World::set_shape_material (world.h:416) */
+int fyzz_b200_set_shape_material(fyzz_b200_world* w, uint32_t shape, const fyzz_b200_material* m);
+/* World::set_body_velocity / set_body_angular_velocity (world.h:477-478) */
+int fyzz_b200_set_body_velocity(fyzz_b200_world* w, uint32_t body, const float v[3]);
+int fyzz_b200_set_body_angular_velocity(fyzz_b200_world* w, uint32_t body, const float v[3]);
+/* World::add_center_distance_constraint (world.h:438) */
+int fyzz_b200_add_center_distance_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b,
+                                             float distance, uint64_t* id_out);
+
+/* Bulk authoring of one scene with the seeded-workload record layout:
+ * bodies(14 floats: position 3, orientation 4, velocity 3, angular 3,
+ * density), per-shape owner / type (0 box, 1 sphere) / geometry(4) /
+ * local pose(7) / material(3), distance joints, optional floor (created
+ * first, with material floor_mat).  Equivalent to the per-call sequence
+ * add_static_floor, create_dynamic_body, attach_*_shape,
+ * update_mass_properties, set_shape_material, set_body_velocity,
+ * set_body_angular_velocity, add_center_distance_constraint. */
+int fyzz_b200_add_scene(fyzz_b200_world* w, uint32_t n_bodies, const float* bodies,
+                        uint32_t n_shapes, const uint32_t* shape_body, const uint32_t* shape_type,
+                        const float* shape_geom, const float* shape_local, const float* shape_mat,
+                        uint32_t n_joints, const uint32_t* joint_bodies, const float* joint_dist,
+                        int has_floor, float floor_height, const float* floor_mat,
+                        uint32_t* first_body_out);
+
+/* ---- stepping: World::step (world.h:459, scene.cpp:10725) ---- */
+int fyzz_b200_step(fyzz_b200_world* w, float seconds);
+/* `steps` consecutive steps launched as one captured CUDA graph per step,
+ * with a single error check at the end. */
+int fyzz_b200_step_n(fyzz_b200_world* w, float seconds, uint32_t steps);
+/* Scene::advance_collision (scene.h:819): bounds, pairs and manifolds only. */
+int fyzz_b200_collide(fyzz_b200_world* w);
+int fyzz_b200_synchronize(fyzz_b200_world* w);
+
+/* ---- results ---- */
+/* World::body_state (world.h:460) */
+int fyzz_b200_body_state(const fyzz_b200_world* w, uint32_t body, fyzz_b200_body_state_t* out);
+/* All bodies, 14 floats each: position(3) velocity(3) orientation(4)
+ * angular velocity(3) sleeping(1).  Host buffer. */
+int fyzz_b200_read_bodies(fyzz_b200_world* w, float* out, uint32_t n_bodies);
+/* Overwrite linear(3) + angular(3) velocities of all bodies from a host
+ * buffer (6 floats per body; statics ignored). */
+int fyzz_b200_write_velocities(fyzz_b200_world* w, const float* v6, uint32_t n_bodies);
+/* Counts: [bodies, shapes, scenes, pairs, touching managers, contact points,
+ * descriptors, islands, joints, steps] */
+int fyzz_b200_counts(fyzz_b200_world* w, uint64_t out[10]);
+int fyzz_b200_device_view(fyzz_b200_world* w, fyzz_b200_device_view_t* out);
+
+/* ---- broadphase / narrowphase views (Scene::pairs, found_pairs,
+ *      lost_pairs, contacts: scene.h:827-833) ---- */
+/* which: 0 current pairs, 1 found, 2 lost; 2 u32 (shape a < shape b) each.
+ * Returns the count; writes at most cap pairs. */
+uint64_t fyzz_b200_read_pairs(fyzz_b200_world* w, int which, uint32_t* out, uint64_t cap);
+/* Touching managers in pair order: pair(2), count, and 4 points of
+ * position(3) normal(3) separation(1). */
+uint64_t fyzz_b200_read_manifolds(fyzz_b200_world* w, uint32_t* pairs, uint32_t* counts,
+                                  float* points, uint64_t cap);
+/* Encoded AABBs (Shape::encoded_bounds, scene.h:1194): 6 u32 per shape. */
+int fyzz_b200_read_encoded_bounds(fyzz_b200_world* w, uint32_t* out, uint32_t n_shapes);
+/* Sorted min-x endpoints of one scene (value, shape id), i.e. the minimum
+ * endpoints of the reference's axis-0 endpoint order (scene.cpp:1341-1345). */
+uint64_t fyzz_b200_read_sorted_min_x(fyzz_b200_world* w, uint32_t scene, uint32_t* values,
+                                     uint32_t* ids, uint64_t cap);
+/* Partition level of every descriptor of the last step, in canonical
+ * descriptor order (joints then touching managers). */
+uint64_t fyzz_b200_read_levels(fyzz_b200_world* w, uint32_t* levels, uint64_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
