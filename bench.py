@@ -1,0 +1,418 @@
+#!/usr/bin/env python3
+"""Rigid-body step benchmark: body-steps/s of the B200 step.
+
+Headline workload (one scene, all steps on the GPU): 131,072 dynamic bodies
+(70% boxes, 20% spheres, 10% box+sphere compounds, 2% in distance-joined
+pairs) in a 200 x 50 x 200 m region above a floor; dt = 1/120 s, 4 position
++ 1 velocity iteration; 600 steps.  Also measured on the same line: the
+batched forward (4,096 independent scenes, 16-512 bodies each, one launch
+per stage) and the batched / plain throughput ratio.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+For N > 1 (torchrun, one rank per GPU) every rank steps its own replica of
+the plain scene and its own shard of 4,096 batched scenes (weak scaling, no
+data-path collective); times are the maximum over ranks.  --impl reference
+times the reference SDK's NativeCpu scene (built from the reference sources
+by oracle/Makefile) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+PKG = "fyzzxyzzy-sdk_b200"
+DT = 1.0 / 120.0
+METRIC = "body-steps/s on 1 B200: batched vs plain GPU step; backward/forward ratio"
+UNIT = "body-steps/s"
+PLAIN_WORKLOAD = ("plain method at scale, one scene: 131,072 bodies (70% boxes, 20% spheres, "
+                  "10% box+sphere compounds, 2% distance-joined pairs), 200x50x200 m above a floor, "
+                  "dt=1/120 s, 4 position + 1 velocity iterations")
+BATCHED_WORKLOAD = ("batched forward: 4,096 independent scenes, body count log-uniform in [16,512] "
+                    "(random piles and 5-20 high unit-cube stacks), own floor each, one launch per stage, "
+                    "step captured as a CUDA graph")
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=600)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--batched-steps", type=int, default=256)
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=60)
+    ap.add_argument("--profile-steps", type=int, default=6)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--bodies", type=int, default=131072, help="plain-scene body count")
+    ap.add_argument("--scenes", type=int, default=4096, help="batched scene count per rank")
+    return ap.parse_args()
+
+
+def scenes_mod():
+    return importlib.import_module(PKG + ".scenes")
+
+
+def plain_spec(n):
+    return scenes_mod().mixed_scale(n, seed=1)
+
+
+def batched_specs(n, rank):
+    return scenes_mod().batched_scenes(n, base_seed=rank * n)
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, local_rank: int):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        idx = vis.split(",")[local_rank] if vis else str(local_rank)
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", idx, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def clocks_bad(c: dict) -> bool:
+    bad = {"hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown"}
+    if bad & set(c.get("reasons", [])):
+        return True
+    sm, smax = c.get("sm_mhz"), c.get("sm_max_mhz")
+    return bool(sm and smax and sm < 0.5 * smax and not c.get("reasons"))
+
+
+# --------------------------------------------------------------- roofline
+def algorithmic_bytes(stage: str, c: dict, iters: int = 5) -> float:
+    """Per-step algorithmic bytes of each stage: the fixed per-unit
+    accounting constants of the hot-path scope (bytes per body / shape /
+    pair / contact / friction row), independent of tuning."""
+    nb, ns, npair = c["bodies"], c["shapes"], c["pairs"]
+    nc, nf, nj = c["points"], c["friction_rows"], c["joints"]
+    return {
+        "bounds": 68.0 * ns,
+        "sort": 384.0 * ns,
+        "pairs": 48.0 * ns + 8.0 * c["found_lost"],
+        "narrowphase": 212.0 * npair,
+        "islands": 16.0 * (c["managers"] + nj) * 3,
+        "prep": 92.0 * nc + 56.0 * nf + 64.0 * nj,
+        "pgs": iters * (68.0 * nc + 60.0 * nf + 68.0 * nj + 48.0 * nb),
+        "integrate": 120.0 * nb,
+    }[stage]
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(stage: str):
+    """Per-unit DRAM traffic of the dominant kernel from the committed ncu
+    summary (profiles/ncu_traffic.json), or None."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        t = json.load(f)
+    return t.get(stage)
+
+
+# --------------------------------------------------------------- b200 arm
+def timed_steps(torch, w, steps, stream):
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    w.synchronize()
+    start.record(stream)
+    w.step(DT, steps)
+    end.record(stream)
+    end.synchronize()
+    return start.elapsed_time(end)
+
+
+def run_b200(args, rank, world, local_rank):
+    import torch
+    pkg = importlib.import_module(PKG)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    # ---- plain scene (replica per rank) ----
+    spec = plain_spec(args.bodies)
+    w = pkg.World(local_rank)
+    w.add_scene(spec)
+    n_dyn = spec.n_bodies
+    if args.warmup:
+        w.step(DT, args.warmup)
+    stream = torch.cuda.ExternalStream(w.device_view().stream)
+    barrier()
+    torch.cuda.synchronize()
+    for attempt in range(2):
+        sampler = ClockSampler(local_rank)
+        ms = timed_steps(torch, w, args.steps, stream)
+        clocks = sampler.stop()
+        if not clocks_bad(clocks):
+            break
+        if attempt == 0:
+            w = pkg.World(local_rank)
+            w.add_scene(spec)
+            w.step(DT, args.warmup)
+            stream = torch.cuda.ExternalStream(w.device_view().stream)
+    barrier()
+    ms_max = max_over_ranks(ms)
+    value = sum_over_ranks(n_dyn * args.steps) / (ms_max / 1e3)
+    counts = w.counts()
+    kernels = w.kernels_per_step()
+
+    # ---- roofline of the dominant stage (CUDA events per stage) ----
+    prof = {}
+    for _ in range(max(1, args.profile_steps)):
+        st = w.profile_step(DT)
+        for k, v in st.items():
+            prof[k] = prof.get(k, 0.0) + v / max(1, args.profile_steps)
+    counts = w.counts()
+    dom = max(prof, key=prof.get)
+    alg = algorithmic_bytes(dom, counts)
+    peak, peak_kind = measured_peaks()
+    achieved = alg / (prof[dom] / 1e3) / 1e9
+    per_unit = ncu_traffic(dom)
+    units = {"narrowphase": counts["pairs"], "pgs": counts["managers"], "pairs": counts["shapes"],
+             "sort": counts["shapes"], "bounds": counts["shapes"], "integrate": counts["bodies"],
+             "prep": counts["managers"], "islands": counts["managers"]}[dom]
+    roofline = {"bound": "hbm", "kernel_stage": dom, "achieved": round(achieved, 2), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                "traffic": (per_unit * units if per_unit is not None else None),
+                "algorithmic_bytes": alg, "stage_ms": round(prof[dom], 4)}
+
+    # ---- end to end through the C ABI with host buffers ----
+    e2e_steps = max(1, min(args.e2e_steps, args.steps))
+    buf = np.zeros((spec.n_actors, 14), np.float32)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        w.read_bodies(buf)
+        v6 = np.ascontiguousarray(buf[:, [3, 4, 5, 10, 11, 12]])
+        w.write_velocities(v6)
+        w.step(DT)
+    w.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = {"value": sum_over_ranks(n_dyn * e2e_steps) / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": 32 * spec.n_actors, "d2h_bytes_per_step": 64 * spec.n_actors,
+           "steps": e2e_steps,
+           "loop": "read_bodies (D2H) -> write_velocities (H2D) -> step, host buffers, pinned staging"}
+
+    # ---- batched forward ----
+    batched = None
+    if not args.no_batched:
+        specs = batched_specs(args.scenes, rank)
+        wb = pkg.World(local_rank)
+        for s in specs:
+            wb.add_scene(s)
+        nb_dyn = sum(s.n_bodies for s in specs)
+        if args.warmup:
+            wb.step(DT, args.warmup)
+        bstream = torch.cuda.ExternalStream(wb.device_view().stream)
+        barrier()
+        sampler = ClockSampler(local_rank)
+        bms = timed_steps(torch, wb, args.batched_steps, bstream)
+        bclocks = sampler.stop()
+        bms_max = max_over_ranks(bms)
+        bvalue = sum_over_ranks(nb_dyn * args.batched_steps) / (bms_max / 1e3)
+        bprof = wb.profile_step(DT)
+        batched = {"workload": BATCHED_WORKLOAD, "scenes": len(specs) * world, "bodies": nb_dyn * world,
+                   "steps": args.batched_steps, "value": bvalue, "unit": UNIT,
+                   "ms_per_step": bms_max / args.batched_steps, "clocks": bclocks,
+                   "stages_ms": {k: round(v, 4) for k, v in bprof.items()},
+                   "counts": wb.counts(), "gpu_launches": wb.kernels_per_step() * args.batched_steps}
+        wb.close()
+
+    # ---- CPU baseline: the reference NativeCpu scene on this host ----
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu = cpu_baseline(spec, args.cpu_seconds)
+
+    if rank == 0:
+        ws_mb = (counts["pairs"] * (2 * 332 + 112 + 16) + counts["bodies"] * 400 + counts["shapes"] * 250) / 2**20
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded generator with the workload's distributions (no dataset)",
+            "config": {"workload": PLAIN_WORKLOAD, "bodies": n_dyn, "shapes": spec.n_shapes,
+                       "joints": int(spec.joints.shape[0]), "dt": DT, "position_iterations": 4,
+                       "velocity_iterations": 1,
+                       "l2": f"resident working set ~{ws_mb:.0f} MB > 126 MB L2 (not flushed)",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "batched": batched,
+            "batched_vs_plain": (batched["value"] / value) if batched else None,
+            "e2e": e2e,
+            "gpu_launches": kernels * args.steps,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "stages_ms": {k: round(v, 4) for k, v in prof.items()},
+            "counts": counts,
+        }
+        print(json.dumps(line), flush=True)
+    w.close()
+
+
+def cpu_baseline(spec, seconds):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refscene
+    if not refscene.available():
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": "reference harness not built"}
+    r = refscene.RefScene(spec)
+    r.step(DT, 1)   # first step rebuilds the SAP endpoint lists; not timed
+    n = 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds and n < 200:
+        r.step(DT, 1)
+        n += 1
+    el = time.perf_counter() - t0
+    r.close()
+    return {"value": spec.n_bodies * n / el, "unit": UNIT, "cores": 2, "kind": "reference",
+            "sample": f"steps 2..{n + 1} of the same {spec.n_bodies}-body scene "
+                      f"({el:.1f} s; NativeCpu uses the caller plus one worker thread)"}
+
+
+# --------------------------------------------------------------- reference arm
+def run_reference(args):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refscene
+    if not refscene.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference NativeCpu harness not built (oracle/_ref)"}))
+        return
+    spec = plain_spec(args.bodies)
+    r = refscene.RefScene(spec)
+    r.step(DT, max(1, min(args.warmup, 2)))
+    budget = 120.0
+    n = 0
+    t0 = time.perf_counter()
+    while n < args.steps and time.perf_counter() - t0 < budget:
+        r.step(DT, 1)
+        n += 1
+    el = time.perf_counter() - t0
+    r.close()
+    value = spec.n_bodies * n / el
+    cores = os.cpu_count() or 1
+    batched = None
+    if not args.no_batched:
+        specs = batched_specs(args.scenes, 0)[:512]
+        refs = [refscene.RefScene(s) for s in specs]
+        refscene.step_many(refs, DT, 1, cores)
+        bsteps = 16
+        t0 = time.perf_counter()
+        refscene.step_many(refs, DT, bsteps, cores)
+        bel = time.perf_counter() - t0
+        nb = sum(s.n_bodies for s in specs)
+        batched = {"value": nb * bsteps / bel, "unit": UNIT, "scenes": len(specs),
+                   "sample": f"{len(specs)} of the 4,096 batched scenes x {bsteps} steps, "
+                             f"one NativeCpu scene per batched scene over {cores} host threads"}
+    sample = (f"steps {2 if args.warmup else 1}..{n + 1} of the {spec.n_bodies}-body scene "
+              f"({el:.1f} s; {n} of the requested {args.steps} steps within a {budget:.0f} s budget)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+            "steps": n, "requested_steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": el / max(n, 1) * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded generator with the workload's distributions (no dataset)",
+            "config": {"workload": PLAIN_WORKLOAD, "bodies": spec.n_bodies, "shapes": spec.n_shapes},
+            "cpu_baseline": {"value": value, "unit": UNIT, "kind": "reference", "cores": 2,
+                             "sample": sample},
+            "batched": batched,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
+    try:
+        run_b200(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

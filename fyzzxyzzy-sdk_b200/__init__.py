@@ -31,8 +31,10 @@ EXPORTS = (
     "fyzz_b200_synchronize", "fyzz_b200_body_state", "fyzz_b200_read_bodies",
     "fyzz_b200_write_velocities", "fyzz_b200_counts", "fyzz_b200_device_view",
     "fyzz_b200_read_pairs", "fyzz_b200_read_manifolds", "fyzz_b200_read_encoded_bounds",
-    "fyzz_b200_read_sorted_min_x", "fyzz_b200_read_levels",
+    "fyzz_b200_read_sorted_min_x", "fyzz_b200_read_levels", "fyzz_b200_profile_step",
+    "fyzz_b200_kernels_per_step",
 )
+STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 
 
 def build() -> str:
@@ -101,6 +103,8 @@ def lib():
         L.fyzz_b200_read_sorted_min_x.restype = u64
         L.fyzz_b200_read_levels.argtypes = [vp, vp, u64]
         L.fyzz_b200_read_levels.restype = u64
+        L.fyzz_b200_profile_step.argtypes = [vp, f32, vp, u32]
+        L.fyzz_b200_kernels_per_step.argtypes = [vp, P(u32)]
         _lib = L
     return _lib
 
@@ -228,15 +232,27 @@ class World:
     def collide(self):
         self._check(lib().fyzz_b200_collide(self.h))
 
+    def profile_step(self, seconds: float = 1.0 / 120.0) -> dict:
+        """One eagerly launched step; per-stage device milliseconds from CUDA
+        events the library records on its stream."""
+        out = np.zeros(len(STAGES), np.float32)
+        self._check(lib().fyzz_b200_profile_step(self.h, seconds, _p(out), out.size))
+        return dict(zip(STAGES, out.tolist()))
+
+    def kernels_per_step(self) -> int:
+        out = C.c_uint32()
+        self._check(lib().fyzz_b200_kernels_per_step(self.h, C.byref(out)))
+        return out.value
+
     def synchronize(self):
         self._check(lib().fyzz_b200_synchronize(self.h))
 
     # ---- results ----
     def counts(self) -> dict:
-        out = np.zeros(10, np.uint64)
+        out = np.zeros(12, np.uint64)
         self._check(lib().fyzz_b200_counts(self.h, _p(out)))
         keys = ["bodies", "shapes", "scenes", "pairs", "managers", "points",
-                "descriptors", "islands", "joints", "steps"]
+                "descriptors", "islands", "joints", "steps", "friction_rows", "found_lost"]
         return {k: int(v) for k, v in zip(keys, out)}
 
     def body_state(self, body: int) -> BodyState:

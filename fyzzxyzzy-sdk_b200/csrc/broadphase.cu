@@ -207,11 +207,13 @@ __global__ void k_pair_match(DevState s) {
 
 }  // namespace
 
-void enqueue_broadphase(const DevState& s, cudaStream_t st) {
+void enqueue_broadphase(const DevState& s, cudaStream_t st, const StageHook& hook) {
     uint4* rec = s.sw_rec;
     uint2* meta = s.sw_meta;
     const int T = 256;
+    hook(kStBounds, st);
     k_shape_bounds<<<(s.n_shapes + T - 1) / T, T, 0, st>>>(s);
+    hook(kStSort, st);
     if (s.n_small) {
         uint32_t m = 1;
         while (m < s.max_small_scene) m <<= 1;
@@ -221,6 +223,7 @@ void enqueue_broadphase(const DevState& s, cudaStream_t st) {
         radix_sort_pairs(s.srt_key + s.large_begin[i], s.srt_id + s.large_begin[i],
                          s.srt_key2, s.srt_id2, s.large_n[i], nullptr, 0, 32,
                          s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st);
+    hook(kStPairs, st);
     if (s.n_finite) {
         k_sweep_gather<<<(s.n_finite + T - 1) / T, T, 0, st>>>(s, rec, meta);
     }

@@ -1044,8 +1044,9 @@ __global__ void __launch_bounds__(128) k_narrowphase(DevState s) {
 
 }  // namespace
 
-void enqueue_narrowphase(const DevState& s, cudaStream_t st) {
+void enqueue_narrowphase(const DevState& s, cudaStream_t st, const StageHook& hook) {
     const int T = 128;
+    hook(kStNarrow, st);
     const uint32_t blocks = (s.pair_cap + T - 1) / T;
     k_narrowphase<<<blocks < 148u * 16u ? blocks : 148u * 16u, T, 0, st>>>(s);
 }

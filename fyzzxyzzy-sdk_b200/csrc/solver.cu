@@ -752,12 +752,13 @@ inline uint32_t grid_for(uint32_t n, uint32_t t, uint32_t cap) {
 
 }  // namespace
 
-void enqueue_solver(const DevState& s, cudaStream_t st) {
+void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook) {
     uint32_t* flags = s.tmp_flags;
     uint32_t* pos = s.tmp_pos;
     uint32_t* lvl_bound = s.lvl_bound;
     const uint32_t T = 256;
     const uint32_t cap_blocks = 148u * 8u;
+    hook(kStIslands, st);
     k_frame_begin<<<1, 32, 0, st>>>(s);
     k_bodies_begin<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
     // touching managers in canonical pair order
@@ -776,12 +777,16 @@ void enqueue_solver(const DevState& s, cudaStream_t st) {
     k_island_scatter<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s, pos);
     k_partition<<<grid_for(s.desc_cap, 128, cap_blocks), 128, 0, st>>>(s, lvl_bound);
     // rows
+    hook(kStPrep, st);
     if (s.n_joints) k_prep_joints<<<grid_for(s.n_joints, T, 1u << 30), T, 0, st>>>(s);
     k_prep_contacts<<<grid_for(s.desc_cap, 128, cap_blocks), 128, 0, st>>>(s);
     // PGS
+    hook(kStPgs, st);
     k_pgs_warp<<<grid_for(s.desc_cap * 32u, T, cap_blocks), T, 0, st>>>(s, lvl_bound);
     k_pgs_block<<<grid_for(s.desc_cap, 1, 148u * 4u), 256, 0, st>>>(s, lvl_bound);
+    hook(kStIntegrate, st);
     k_integrate<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
+    hook(kStEnd, st);
 }
 
 }  // namespace fyzz::b200

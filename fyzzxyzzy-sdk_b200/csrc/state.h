@@ -129,10 +129,21 @@ void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32
 size_t radix_hist_words(uint32_t n_cap);
 size_t scan_tmp_words_for(uint32_t n_cap);
 
+// Stage boundaries of one step, reported to an optional hook (the world uses
+// it to bracket stages with CUDA events when profiling).
+enum Stage : int {
+    kStBounds = 0, kStSort, kStPairs, kStNarrow, kStIslands, kStPrep, kStPgs, kStIntegrate, kStEnd
+};
+struct StageHook {
+    void (*fn)(void* ctx, int stage, cudaStream_t st) = nullptr;
+    void* ctx = nullptr;
+    void operator()(int stage, cudaStream_t st) const { if (fn) fn(ctx, stage, st); }
+};
+
 // broadphase.cu / narrowphase.cu / solver.cu
-void enqueue_broadphase(const DevState& s, cudaStream_t st);
-void enqueue_narrowphase(const DevState& s, cudaStream_t st);
-void enqueue_solver(const DevState& s, cudaStream_t st);
+void enqueue_broadphase(const DevState& s, cudaStream_t st, const StageHook& hook = {});
+void enqueue_narrowphase(const DevState& s, cudaStream_t st, const StageHook& hook = {});
+void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook = {});
 // counters[] slots
 enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels = 4, kCntSlots = 8 };
 

@@ -446,6 +446,47 @@ public:
     }
     void synchronize() { check_cuda(cudaStreamSynchronize(stream_), "synchronize"); }
 
+    // One step launched eagerly (not from the graph) with a CUDA event on the
+    // world's stream at every stage boundary; returns per-stage milliseconds
+    // in Stage order.
+    void profile_step(float dt, float* ms, uint32_t n) {
+        if (!std::isfinite(dt) || dt <= 0.0f) throw std::invalid_argument("timestep must be finite and positive");
+        check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+        ensure_device();
+        struct Ctx { cudaEvent_t ev[kStEnd + 1]; bool seen[kStEnd + 1]; } ctx{};
+        for (int i = 0; i <= kStEnd; ++i) check_cuda(cudaEventCreate(&ctx.ev[i]), "event");
+        StageHook hook;
+        hook.ctx = &ctx;
+        hook.fn = [](void* c, int stage, cudaStream_t st) {
+            auto* x = static_cast<Ctx*>(c);
+            cudaEventRecord(x->ev[stage], st);
+            x->seen[stage] = true;
+        };
+        snapshot();
+        d_.dt = dt;
+        check_cuda(cudaMemsetAsync(d_.err, 0, 4, stream_), "memset");
+        const DevState s = view(parity_);
+        enqueue_broadphase(s, stream_, hook);
+        enqueue_narrowphase(s, stream_, hook);
+        enqueue_solver(s, stream_, hook);
+        check_cuda(cudaGetLastError(), "profile launch");
+        const uint32_t err = read_err();
+        last_cur_ = parity_;
+        parity_ ^= 1;
+        for (uint32_t i = 0; i < n && i < uint32_t(kStEnd); ++i) {
+            float t = 0.0f;
+            if (ctx.seen[i] && ctx.seen[i + 1]) cudaEventElapsedTime(&t, ctx.ev[i], ctx.ev[i + 1]);
+            ms[i] = t;
+        }
+        for (int i = 0; i <= kStEnd; ++i) cudaEventDestroy(ctx.ev[i]);
+        if (err) {
+            restore();
+            throw std::overflow_error("Device step reported error bits " + std::to_string(err));
+        }
+        ++steps_done_;
+    }
+    uint32_t kernels_per_step() const { return kernels_per_step_; }
+
     void read_bodies(float* out, uint32_t n) {
         if (n != bodies_.size()) throw std::invalid_argument("Body count mismatch");
         if (!uploaded_ || host_authoritative_) {
@@ -505,17 +546,29 @@ public:
     }
     void counts(uint64_t* out) {
         out[0] = bodies_.size(); out[1] = shapes_.size(); out[2] = scene_body_begin_.size();
-        out[3] = out[4] = out[5] = out[6] = out[7] = 0;
+        out[3] = out[4] = out[5] = out[6] = out[7] = out[10] = out[11] = 0;
         out[8] = joints_.size(); out[9] = steps_done_;
         if (!uploaded_) return;
         const auto c = read_counters();
         out[3] = c.pairs; out[4] = c.man; out[6] = c.desc; out[7] = c.isl;
-        std::vector<uint32_t> cnt(c.pairs);
-        if (c.pairs)
+        std::vector<uint32_t> cnt(c.pairs), found(c.pairs), lost(c.prev_pairs);
+        std::vector<ManagerHeader> mh(c.man);
+        if (c.pairs) {
             check_cuda(cudaMemcpy(cnt.data(), sets_[last_cur_].count, size_t(c.pairs) * 4, cudaMemcpyDeviceToHost), "read");
-        uint64_t pts = 0;
+            check_cuda(cudaMemcpy(found.data(), d_.found_flag, size_t(c.pairs) * 4, cudaMemcpyDeviceToHost), "read");
+        }
+        if (c.prev_pairs)
+            check_cuda(cudaMemcpy(lost.data(), d_.lost_flag, size_t(c.prev_pairs) * 4, cudaMemcpyDeviceToHost), "read");
+        if (c.man && steps_done_)
+            check_cuda(cudaMemcpy(mh.data(), d_.mh, size_t(c.man) * sizeof(ManagerHeader), cudaMemcpyDeviceToHost), "read");
+        uint64_t pts = 0, fl = 0, frows = 0;
         for (auto x : cnt) pts += x;
+        for (auto x : found) fl += x;
+        for (auto x : lost) fl += x;
+        for (const auto& h : mh) frows += 2u * h.anchors;
         out[5] = pts;
+        out[10] = frows;
+        out[11] = fl;
     }
     void device_view(fyzz_b200_device_view_t* v) {
         ensure_device();
@@ -657,6 +710,16 @@ private:
                 enqueue_narrowphase(s, stream_);
                 enqueue_solver(s, stream_);
                 check_cuda(cudaStreamEndCapture(stream_, &g), "end capture");
+                size_t nn = 0;
+                check_cuda(cudaGraphGetNodes(g, nullptr, &nn), "graph nodes");
+                std::vector<cudaGraphNode_t> nodes(nn);
+                check_cuda(cudaGraphGetNodes(g, nodes.data(), &nn), "graph nodes");
+                uint32_t kernels = 0;
+                for (auto nd : nodes) {
+                    cudaGraphNodeType t;
+                    if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++kernels;
+                }
+                kernels_per_step_ = kernels;
                 check_cuda(cudaGraphInstantiate(&graphs_[parity_], g, 0), "instantiate");
                 cudaGraphDestroy(g);
             }
@@ -916,7 +979,21 @@ private:
     uint64_t steps_done_ = 0;
     uint32_t last_err_ = 0;
     uint32_t* host_err_ = nullptr;
-    std::vector<float4> stage_;
+    uint32_t kernels_per_step_ = 0;
+    // Pinned staging for the host-buffer API (read_bodies, write_velocities).
+    struct PinnedStage {
+        float4* p = nullptr;
+        size_t n = 0;
+        void resize(size_t m) {
+            if (m <= n) return;
+            if (p) cudaFreeHost(p);
+            check_cuda(cudaMallocHost(reinterpret_cast<void**>(&p), m * sizeof(float4)), "cudaMallocHost");
+            n = m;
+        }
+        float4* data() { return p; }
+        float4& operator[](size_t i) { return p[i]; }
+        ~PinnedStage() { if (p) cudaFreeHost(p); }
+    } stage_;
 };
 
 }  // namespace fyzz::b200
@@ -994,9 +1071,9 @@ int fyzz_b200_attach_box_shape(fyzz_b200_world* w, uint32_t body, const float ha
 }
 int fyzz_b200_attach_sphere_shape(fyzz_b200_world* w, uint32_t body, float r, const float local[7], uint32_t* out) {
     static const float identity[7] = {0, 0, 0, 0, 0, 0, 1};
-    static const float none[3] = {0, 0, 0};
     return guarded(w, [&](auto& W) {
-        const uint32_t s = W.attach(body, fyzz::b200::kSphere, none, r, local ? local : identity);
+        const float no_half[3] = {0.0f, 0.0f, 0.0f};
+        const uint32_t s = W.attach(body, fyzz::b200::kSphere, no_half, r, local ? local : identity);
         if (out) *out = s;
     });
 }
@@ -1080,6 +1157,14 @@ int fyzz_b200_collide(fyzz_b200_world* w) {
 int fyzz_b200_synchronize(fyzz_b200_world* w) {
     return guarded(w, [&](auto& W) { W.synchronize(); });
 }
+int fyzz_b200_profile_step(fyzz_b200_world* w, float dt, float* ms, uint32_t n) {
+    if (!ms && n) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) { W.profile_step(dt, ms, n); });
+}
+int fyzz_b200_kernels_per_step(fyzz_b200_world* w, uint32_t* out) {
+    if (!out) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) { *out = W.kernels_per_step(); });
+}
 int fyzz_b200_body_state(const fyzz_b200_world* w, uint32_t body, fyzz_b200_body_state_t* out) {
     if (!out) return FYZZ_B200_INVALID_ARGUMENT;
     return guarded(const_cast<fyzz_b200_world*>(w), [&](auto& W) { W.body_state(body, out); });
@@ -1092,7 +1177,7 @@ int fyzz_b200_write_velocities(fyzz_b200_world* w, const float* v6, uint32_t n) 
     if (!v6) return FYZZ_B200_INVALID_ARGUMENT;
     return guarded(w, [&](auto& W) { W.write_velocities(v6, n); });
 }
-int fyzz_b200_counts(fyzz_b200_world* w, uint64_t out[10]) {
+int fyzz_b200_counts(fyzz_b200_world* w, uint64_t out[12]) {
     if (!out) return FYZZ_B200_INVALID_ARGUMENT;
     return guarded(w, [&](auto& W) { W.counts(out); });
 }

@@ -123,6 +123,14 @@ int fyzz_b200_step_n(fyzz_b200_world* w, float seconds, uint32_t steps);
 /* Scene::advance_collision (scene.h:819): bounds, pairs and manifolds only. */
 int fyzz_b200_collide(fyzz_b200_world* w);
 int fyzz_b200_synchronize(fyzz_b200_world* w);
+/* One step launched without the graph, with CUDA events on the world's
+ * stream at each stage boundary.  stage_ms receives up to n stage times:
+ * 0 bounds, 1 endpoint sort, 2 pairs, 3 narrowphase, 4 islands+partitions,
+ * 5 row preparation, 6 PGS, 7 integration.  (Counterpart of the reference's
+ * Context::profile_batch_gpu_nanoseconds, compute.h:299.) */
+int fyzz_b200_profile_step(fyzz_b200_world* w, float seconds, float* stage_ms, uint32_t n);
+/* Kernel launches in one captured step graph (0 before the first step). */
+int fyzz_b200_kernels_per_step(fyzz_b200_world* w, uint32_t* out);
 
 /* ---- results ---- */
 /* World::body_state (world.h:460) */
@@ -134,8 +142,8 @@ int fyzz_b200_read_bodies(fyzz_b200_world* w, float* out, uint32_t n_bodies);
  * buffer (6 floats per body; statics ignored). */
 int fyzz_b200_write_velocities(fyzz_b200_world* w, const float* v6, uint32_t n_bodies);
 /* Counts: [bodies, shapes, scenes, pairs, touching managers, contact points,
- * descriptors, islands, joints, steps] */
-int fyzz_b200_counts(fyzz_b200_world* w, uint64_t out[10]);
+ * descriptors, islands, joints, steps, friction rows, found + lost pairs] */
+int fyzz_b200_counts(fyzz_b200_world* w, uint64_t out[12]);
 int fyzz_b200_device_view(fyzz_b200_world* w, fyzz_b200_device_view_t* out);
 
 /* ---- broadphase / narrowphase views (Scene::pairs, found_pairs,
