@@ -148,8 +148,9 @@ __device__ void uf_union(const DevState& s, uint32_t a, uint32_t b) {
     atomicOr(s.err, kErrUnionFind);
 }
 // Descriptor endpoints: joints use the ordered edge pair (scene.cpp:3154),
-// managers the Gu order.  -1 marks the static world body.
-__device__ __forceinline__ void desc_bodies(const DevState& s, uint32_t d, int32_t& b0, int32_t& b1) {
+// managers the Gu order.  -1 marks the static world body.  Resolved once per
+// step into d_bod by k_desc_bodies; every later stage reads that array.
+__device__ __forceinline__ void resolve_desc_bodies(const DevState& s, uint32_t d, int32_t& b0, int32_t& b1) {
     if (d < s.n_joints) {
         b0 = int32_t(s.j_a[d]);
         b1 = int32_t(s.j_b[d]);
@@ -161,6 +162,20 @@ __device__ __forceinline__ void desc_bodies(const DevState& s, uint32_t d, int32
     }
     if (!is_dyn(s, uint32_t(b0))) b0 = -1;
     if (!is_dyn(s, uint32_t(b1))) b1 = -1;
+}
+__device__ __forceinline__ void desc_bodies(const DevState& s, uint32_t d, int32_t& b0, int32_t& b1) {
+    const int2 b = s.d_bod[d];
+    b0 = b.x;
+    b1 = b.y;
+}
+__global__ void k_desc_bodies(DevState s) {
+    const uint32_t n = s.counters[kCntDesc];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += stride) {
+        int32_t b0, b1;
+        resolve_desc_bodies(s, d, b0, b1);
+        s.d_bod[d] = make_int2(b0, b1);
+    }
 }
 __global__ void k_union(DevState s) {
     const uint32_t n = s.counters[kCntDesc];
@@ -200,15 +215,187 @@ __global__ void k_island_scatter(DevState s, const uint32_t* pos) {
     }
 }
 
-// One thread per island: the reference's sequential greedy partition over
-// the island's descriptors (scene.cpp:7367-7437), then a counting sort of the
-// island's descriptors by partition into d_key2/d_val2 and the partition
-// boundaries into isl_end-based storage.
+// Partitioning.  The reference assigns each dynamic/dynamic descriptor, in
+// order, the lowest partition bit free on both bodies (32-bit masks, overflow
+// waves), then gives each static descriptor the partition after its body's
+// last dynamic one plus the number of earlier statics on that body
+// (scene.cpp:7367-7437).
+//
+// Small islands: one thread replays that sequential loop.
+// Large islands: one CTA reproduces it exactly in rounds.  A descriptor that
+// is the earliest undecided one on both of its bodies has every earlier
+// descriptor touching those bodies already decided, so it sees exactly the
+// masks the sequential loop would; all such descriptors share no body and are
+// decided together.  Each round decides at least the earliest undecided
+// descriptor of the island.  Waves and the static pass use the same rule.
+constexpr uint32_t kSerialIsland = 32;
+constexpr uint32_t kDeferred = 0xfffffffeu;
+
+__device__ void place_by_level(const DevState& s, uint32_t isl, uint32_t begin, uint32_t end,
+                               uint32_t nlev, uint32_t* lvl_bound) {
+    uint32_t* bound = lvl_bound + begin + isl;   // nlev + 1 entries
+    for (uint32_t l = 0; l <= nlev; ++l) bound[l] = 0u;
+    for (uint32_t i = begin; i < end; ++i) {
+        const uint32_t l = min(s.d_level[s.d_val[i]], uint32_t(kMaxLevels - 1));
+        ++bound[l + 1];
+    }
+    uint32_t run = begin;
+    for (uint32_t l = 0; l <= nlev; ++l) { run += bound[l]; bound[l] = run; }
+    for (uint32_t i = begin; i < end; ++i) {
+        const uint32_t d = s.d_val[i];
+        const uint32_t l = min(s.d_level[d], uint32_t(kMaxLevels - 1));
+        s.d_val2[bound[l]++] = d;
+    }
+    for (uint32_t l = nlev; l > 0; --l) bound[l] = bound[l - 1];
+    bound[0] = begin;
+    s.isl_end[isl] = nlev;
+}
+
+__global__ void __launch_bounds__(256) k_partition_large(DevState s, uint32_t* lvl_bound) {
+    __shared__ uint32_t cursor[kMaxLevels + 1];
+    __shared__ uint32_t nlev_s;
+    const uint32_t ni = *s.n_isl;
+    const uint32_t tid = threadIdx.x, nt = blockDim.x;
+    for (uint32_t isl = blockIdx.x; isl < ni; isl += gridDim.x) {
+        const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
+        if (end - begin <= kSerialIsland) continue;
+        if (tid == 0) nlev_s = 0;
+        uint32_t nlev = 0;
+        bool ok = true;
+        for (uint32_t wave = 0; ok; wave += 32) {
+            if (wave) {
+                for (uint32_t i = begin + tid; i < end; i += nt) {
+                    const uint32_t d = s.d_val[i];
+                    if (s.d_level[d] != kDeferred) continue;
+                    const int2 b = s.d_bod[d];
+                    s.sb_mask[b.x] = 0u;
+                    s.sb_mask[b.y] = 0u;
+                }
+                __syncthreads();
+                for (uint32_t i = begin + tid; i < end; i += nt) {
+                    const uint32_t d = s.d_val[i];
+                    if (s.d_level[d] == kDeferred) s.d_level[d] = kInvalid;
+                }
+                __syncthreads();
+            }
+            for (uint32_t round = 0; round <= end - begin; ++round) {
+                bool any = false;
+                for (uint32_t i = begin + tid; i < end; i += nt) {
+                    const uint32_t d = s.d_val[i];
+                    const int2 b = s.d_bod[d];
+                    if (b.x < 0 || b.y < 0 || s.d_level[d] != kInvalid) continue;
+                    s.sb_earliest[b.x] = kInvalid;
+                    s.sb_earliest[b.y] = kInvalid;
+                    any = true;
+                }
+                if (!__syncthreads_or(any)) break;
+                for (uint32_t i = begin + tid; i < end; i += nt) {
+                    const uint32_t d = s.d_val[i];
+                    const int2 b = s.d_bod[d];
+                    if (b.x < 0 || b.y < 0 || s.d_level[d] != kInvalid) continue;
+                    atomicMin(&s.sb_earliest[b.x], i);
+                    atomicMin(&s.sb_earliest[b.y], i);
+                }
+                __syncthreads();
+                for (uint32_t i = begin + tid; i < end; i += nt) {
+                    const uint32_t d = s.d_val[i];
+                    const int2 b = s.d_bod[d];
+                    if (b.x < 0 || b.y < 0 || s.d_level[d] != kInvalid) continue;
+                    if (s.sb_earliest[b.x] != i || s.sb_earliest[b.y] != i) continue;
+                    const uint32_t avail = ~(s.sb_mask[b.x] | s.sb_mask[b.y]);
+                    if (!avail) { s.d_level[d] = kDeferred; continue; }
+                    const uint32_t bit = __ffs(avail) - 1;
+                    s.sb_mask[b.x] |= 1u << bit;
+                    s.sb_mask[b.y] |= 1u << bit;
+                    const uint32_t lp = wave + bit;
+                    s.sb_maxdyn[b.x] = max(s.sb_maxdyn[b.x], lp + 1);
+                    s.sb_maxdyn[b.y] = max(s.sb_maxdyn[b.y], lp + 1);
+                    s.d_level[d] = lp;
+                    nlev = max(nlev, lp + 1);
+                }
+                __syncthreads();
+            }
+            bool deferred = false;
+            for (uint32_t i = begin + tid; i < end; i += nt)
+                deferred |= s.d_level[s.d_val[i]] == kDeferred;
+            if (!__syncthreads_or(deferred)) break;
+            if (wave + 32 >= kMaxLevels) {
+                if (tid == 0) atomicOr(s.err, kErrLevelRange);
+                ok = false;
+            }
+        }
+        // statics, in descriptor order per body
+        for (uint32_t round = 0; round <= end - begin; ++round) {
+            bool any = false;
+            for (uint32_t i = begin + tid; i < end; i += nt) {
+                const uint32_t d = s.d_val[i];
+                const int2 b = s.d_bod[d];
+                if ((b.x < 0) == (b.y < 0) || s.d_level[d] != kInvalid) continue;
+                s.sb_earliest[b.x >= 0 ? b.x : b.y] = kInvalid;
+                any = true;
+            }
+            if (!__syncthreads_or(any)) break;
+            for (uint32_t i = begin + tid; i < end; i += nt) {
+                const uint32_t d = s.d_val[i];
+                const int2 b = s.d_bod[d];
+                if ((b.x < 0) == (b.y < 0) || s.d_level[d] != kInvalid) continue;
+                atomicMin(&s.sb_earliest[b.x >= 0 ? b.x : b.y], i);
+            }
+            __syncthreads();
+            for (uint32_t i = begin + tid; i < end; i += nt) {
+                const uint32_t d = s.d_val[i];
+                const int2 b = s.d_bod[d];
+                if ((b.x < 0) == (b.y < 0) || s.d_level[d] != kInvalid) continue;
+                const int32_t act = b.x >= 0 ? b.x : b.y;
+                if (s.sb_earliest[act] != i) continue;
+                const uint32_t lp = s.sb_maxdyn[act] + s.sb_static[act]++;
+                s.d_level[d] = lp;
+                nlev = max(nlev, lp + 1);
+            }
+            __syncthreads();
+        }
+        atomicMax(&nlev_s, nlev);
+        __syncthreads();
+        nlev = max(nlev_s, 1u);
+        if (nlev > kMaxLevels || nlev > end - begin) {
+            if (tid == 0) atomicOr(s.err, kErrLevelRange);
+            nlev = min(min(nlev, uint32_t(kMaxLevels)), end - begin);
+        }
+        // partition starts and placement (order inside a partition is free:
+        // its descriptors share no dynamic body)
+        for (uint32_t l = tid; l <= nlev; l += nt) cursor[l] = 0u;
+        __syncthreads();
+        for (uint32_t i = begin + tid; i < end; i += nt)
+            atomicAdd(&cursor[min(s.d_level[s.d_val[i]], nlev - 1)], 1u);
+        __syncthreads();
+        if (tid == 0) {
+            uint32_t* bound = lvl_bound + begin + isl;
+            uint32_t run = begin;
+            for (uint32_t l = 0; l < nlev; ++l) {
+                const uint32_t c = cursor[l];
+                bound[l] = run;
+                cursor[l] = run;
+                run += c;
+            }
+            bound[nlev] = end;
+            s.isl_end[isl] = nlev;
+        }
+        __syncthreads();
+        for (uint32_t i = begin + tid; i < end; i += nt) {
+            const uint32_t d = s.d_val[i];
+            s.d_val2[atomicAdd(&cursor[min(s.d_level[d], nlev - 1)], 1u)] = d;
+        }
+        __syncthreads();
+    }
+}
+
+// One thread per small island: the sequential loop itself.
 __global__ void k_partition(DevState s, uint32_t* lvl_bound) {
     const uint32_t ni = *s.n_isl;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < ni; isl += stride) {
         const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
+        if (end - begin > kSerialIsland) continue;
         uint32_t nlev = 0;
         bool pending = true;
         for (uint32_t wave = 0; pending; wave += 32) {
@@ -258,25 +445,7 @@ __global__ void k_partition(DevState s, uint32_t* lvl_bound) {
         }
         if (nlev > kMaxLevels) { atomicOr(s.err, kErrLevelRange); nlev = kMaxLevels; }
         if (nlev > end - begin) { atomicOr(s.err, kErrLevelRange); nlev = end - begin; }
-        // counting sort by level inside [begin, end), stable in descriptor order
-        uint32_t* bound = lvl_bound + begin + isl;   // nlev + 1 entries
-        for (uint32_t l = 0; l <= nlev; ++l) bound[l] = 0u;
-        for (uint32_t i = begin; i < end; ++i) {
-            const uint32_t l = min(s.d_level[s.d_val[i]], uint32_t(kMaxLevels - 1));
-            ++bound[l + 1];
-        }
-        uint32_t run = begin;
-        for (uint32_t l = 0; l <= nlev; ++l) { run += bound[l]; bound[l] = run; }
-        // bound[l] is now the start of level l; place descriptors
-        for (uint32_t i = begin; i < end; ++i) {
-            const uint32_t d = s.d_val[i];
-            const uint32_t l = min(s.d_level[d], uint32_t(kMaxLevels - 1));
-            s.d_val2[bound[l]++] = d;
-        }
-        // restore level starts: after placement bound[l] = start of level l+1
-        for (uint32_t l = nlev; l > 0; --l) bound[l] = bound[l - 1];
-        bound[0] = begin;
-        s.isl_end[isl] = nlev;
+        place_by_level(s, isl, begin, end, nlev, lvl_bound);
     }
 }
 
@@ -766,6 +935,7 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook) {
     scan_exclusive(flags, pos, s.pair_cap, s.cur.n, s.counters + kCntMan, s.scan_tmp, s.scan_tmp_words, st);
     k_touch_scatter<<<grid_for(s.pair_cap, T, cap_blocks), T, 0, st>>>(s, flags, pos);
     // islands and partitions
+    k_desc_bodies<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     k_union<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     k_desc_keys<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     int bits = 1;
@@ -776,6 +946,7 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook) {
     scan_exclusive(s.isl_flag, pos, s.desc_cap, s.counters + kCntDesc, s.n_isl, s.scan_tmp, s.scan_tmp_words, st);
     k_island_scatter<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s, pos);
     k_partition<<<grid_for(s.desc_cap, 128, cap_blocks), 128, 0, st>>>(s, lvl_bound);
+    k_partition_large<<<grid_for(s.desc_cap, 1, 148u * 4u), 256, 0, st>>>(s, lvl_bound);
     // rows
     hook(kStPrep, st);
     if (s.n_joints) k_prep_joints<<<grid_for(s.n_joints, T, 1u << 30), T, 0, st>>>(s);

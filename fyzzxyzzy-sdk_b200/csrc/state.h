@@ -98,6 +98,8 @@ struct DevState {
     uint32_t* sb_mask = nullptr;       // partition masks per body
     uint32_t* sb_maxdyn = nullptr;
     uint32_t* sb_static = nullptr;
+    uint32_t* sb_earliest = nullptr;   // per-body earliest undecided descriptor (partition rounds)
+    int2* d_bod = nullptr;             // per descriptor: dynamic solver bodies (-1 = static world)
 
     // step scratch
     uint4* sw_rec = nullptr;           // sweep y/z bounds in sorted order

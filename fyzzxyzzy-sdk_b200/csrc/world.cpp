@@ -787,6 +787,7 @@ private:
         dalloc(d_.d_key, dc, pair_owned_); dalloc(d_.d_val, dc, pair_owned_);
         dalloc(d_.d_key2, dc, pair_owned_); dalloc(d_.d_val2, dc, pair_owned_);
         dalloc(d_.d_level, dc, pair_owned_);
+        dalloc(d_.d_bod, dc, pair_owned_);
         dalloc(d_.isl_begin, size_t(dc) + 1, pair_owned_);
         dalloc(d_.isl_end, size_t(dc) + 1, pair_owned_);
         dalloc(d_.isl_flag, dc, pair_owned_);
@@ -908,6 +909,7 @@ private:
         dalloc(d_.sb_sqrt_i, size_t(nb) * 3, owned_);
         dalloc(d_.uf_parent, nb, owned_);
         dalloc(d_.sb_mask, nb, owned_); dalloc(d_.sb_maxdyn, nb, owned_); dalloc(d_.sb_static, nb, owned_);
+        dalloc(d_.sb_earliest, nb, owned_);
         dalloc(d_.n_isl, 1, owned_);
         dalloc(d_.n_man, 1, owned_);
         dalloc(d_.counters, kCntSlots, owned_);

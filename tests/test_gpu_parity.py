@@ -83,6 +83,57 @@ def test_one_step_matches_oracle(pkg, oracle, cases, name):
     assert rel_err(ws[:, 0:3], os_[:, 0:3]) <= VEL_RTOL
 
 
+def oracle_levels(o, n_joints):
+    """Per-descriptor partition in canonical order (joints, then managers)."""
+    desc, ends = o.partitions()
+    man = o.counts()["manifolds"]
+    levels = np.zeros(n_joints + man, np.uint32)
+    start = 0
+    for p, e in enumerate(ends):
+        for d in desc[start:int(e)]:
+            idx = int(d[0]) if d[3] else n_joints + int(d[0])
+            levels[idx] = p
+        start = int(e)
+    return levels
+
+
+def wave_scene(scenes):
+    # One 10 x 0.2 x 10 m slab carrying 40 small boxes: the slab's 40
+    # dynamic contacts overflow the 32-bit partition mask into a second wave.
+    n_small = 40
+    nb = 1 + n_small
+    bodies = np.zeros((nb, 14), np.float32)
+    bodies[:, 6] = 1.0
+    bodies[:, 13] = 1000.0
+    bodies[0, :3] = (0.0, 0.1, 0.0)
+    geom = np.zeros((nb, 4), np.float32)
+    geom[0, :3] = (5.0, 0.1, 5.0)
+    for i in range(n_small):
+        gx, gz = divmod(i, 7)
+        bodies[1 + i, :3] = (-4.0 + 1.3 * gx, 0.2 + 0.25, -4.0 + 1.3 * gz)
+        geom[1 + i, :3] = (0.25, 0.25, 0.25)
+    local = np.tile(np.array([0, 0, 0, 0, 0, 0, 1], np.float32), (nb, 1))
+    mat = np.tile(np.array([0.5, 0.5, 0.0], np.float32), (nb, 1))
+    return scenes.SceneSpec(bodies=bodies, shape_body=np.arange(nb, dtype=np.uint32),
+                            shape_type=np.zeros(nb, np.uint32), shape_geom=geom,
+                            shape_local=local, shape_mat=mat, floor=0.0)
+
+
+@pytest.mark.parametrize("name", ["dense", "wave", "mixed"])
+def test_partition_levels_match_oracle(pkg, oracle, scenes, cases, name):
+    spec = {"dense": scenes.random_boxes(1200, seed=4, xz=3.0, y=(0.3, 9.0)),
+            "wave": wave_scene(scenes), "mixed": cases["mixed"]}[name]
+    w, _ = make_world(pkg, [spec])
+    o = oracle.OracleScene(spec)
+    w.step(DT)
+    o.step(DT)
+    want = oracle_levels(o, spec.joints.shape[0])
+    got = w.levels()
+    np.testing.assert_array_equal(got, want)
+    if name == "wave":
+        assert want.max() >= 32, "scene must exercise a second partition wave"
+
+
 def test_one_step_matches_reference_sparse(pkg, ref, scenes):
     # Bodies touch only the floor or one partner, so every island's
     # descriptor order is forced and the reference's order coincides.
