@@ -131,7 +131,7 @@ static_assert(sizeof(JointRow) == 64, "JointRow layout");
 struct ManagerHeader {
     int32_t b0, b1;
     uint32_t count, anchors;
-    float sf, df, pad0, pad1;
+    float sf, df, ima, imb;    // friction coefficients, inverse masses
 };
 
 }  // namespace fyzz::b200

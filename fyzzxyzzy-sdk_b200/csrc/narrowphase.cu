@@ -25,6 +25,9 @@ namespace fyzz::b200 {
 namespace {
 
 struct Cand { v3 la, lb, nb; float sep; };
+// Incident-face clipping emits at most 4 vertices + 4 reference corners +
+// 2 points per edge of the 4-edge incident polygon.
+constexpr int kMaxBoxCandidates = 16;
 
 // ---------------- box/box face contacts ----------------
 struct GBox { v3 half, pos; qt rot; v3 axis[3]; };
@@ -80,7 +83,7 @@ __device__ bool seg_aabb(v3 p, v3 delta, v3 high, v3 low, float& enter, float& e
 struct Gen {
     const GBox* a; const GBox* b; Cand* out; int count; bool overflow;
     __device__ void emit(const Frame& f, v3 reference, v3 incident, v3 normal, float sep, bool flipped) {
-        if (count >= 64) { overflow = true; return; }
+        if (count >= kMaxBoxCandidates) { overflow = true; return; }
         const v3 w0 = fr_unproject(f, flipped ? incident : reference);
         const v3 w1 = fr_unproject(f, flipped ? reference : incident);
         Cand& c = out[count++];
@@ -715,9 +718,14 @@ __device__ void reduce_five(PcmCache& c, const PcmPoint& nw) {
 }
 __device__ __forceinline__ float pcm_box_margin(v3 h) { return smin(0.15f * smin(smin(h.x, h.y), h.z), 0.15f); }
 
+__device__ int emit_box_box(qt q1, v3 p1, float cd, const PcmCache& cache, bool direct, bool gjk, v3 gjk_n,
+                            ContactPt* out);
+
 // Returns the emitted count, or -1 on an invalid manifold normal / overflow.
+// Sets gjk_pending (and emits nothing) when the zero-face GJK/EPA
+// continuation must complete the manifold.
 __device__ int generate_box_box(v3 h0, v3 p0, qt q0, v3 h1, v3 p1, qt q1, float cd, PcmCache& cache,
-                                ContactPt* out) {
+                                ContactPt* out, bool& gjk_pending) {
     const v3 delta = {p0.x - p1.x, p0.y - p1.y, p0.z - p1.z};
     const v3 relative = rotinv_sc(q1, delta);
     const qt rotation = qmul(qconj(q1), q0);
@@ -743,15 +751,16 @@ __device__ int generate_box_box(v3 h0, v3 p0, qt q0, v3 h1, v3 p1, qt q1, float 
         regen = a0 * sqrtf(h0.x * h0.x + h0.y * h0.y + h0.z * h0.z) > tp ||
                 a1 * sqrtf(h1.x * h1.x + h1.y * h1.y + h1.z * h1.z) > tp;
     }
-    bool direct = false, gjk = false;
-    v3 gjk_n = {0, 0, 0};
+    bool direct = false;
+    const bool gjk = false;
+    const v3 gjk_n = {0, 0, 0};
     if (regen) {
         sv(cache.rel_p, relative);
         cache.rel_q[0] = rotation.x; cache.rel_q[1] = rotation.y; cache.rel_q[2] = rotation.z; cache.rel_q[3] = rotation.w;
         cache.qa[0] = q0.x; cache.qa[1] = q0.y; cache.qa[2] = q0.z; cache.qa[3] = q0.w;
         cache.qb[0] = q1.x; cache.qb[1] = q1.y; cache.qb[2] = q1.z; cache.qb[3] = q1.w;
         set_meta(cache, cache_count(cache), true);
-        Cand cands[64];
+        Cand cands[kMaxBoxCandidates];
         int count = 0;
         const int ov = box_box_candidates(h0, p0, q0, h1, p1, q1, cd, cands, count);
         if (ov < 0) return -1;
@@ -760,33 +769,11 @@ __device__ int generate_box_box(v3 h0, v3 p0, qt q0, v3 h1, v3 p1, qt q1, float 
             return 0;
         }
         if (count == 0) {
-            Cand w;
-            if (!box_box_gjk_epa(h0, p0, q0, h1, p1, q1, cd, w)) {
-                set_meta(cache, 0, true);
-                return 0;
-            }
-            gjk = true;
-            gjk_n = w.nb;
-            const float rb = mm * 0.05f;
-            const float rsq = rb * rb;
-            bool replaced = false;
-            const uint32_t n0 = cache_count(cache);
-            for (uint32_t i = 0; i < n0; ++i) {
-                const PcmPoint& o = cache.pts[i];
-                if (smin(vlen2(vsub(lv(o.la), w.la)), vlen2(vsub(lv(o.lb), w.lb))) < rsq) {
-                    cache.pts[i] = to_pt(w);
-                    replaced = true;
-                    break;
-                }
-            }
-            if (!replaced) {
-                if (n0 < 4) {
-                    cache.pts[n0] = to_pt(w);
-                    set_meta(cache, n0 + 1, true);
-                } else {
-                    reduce_five(cache, to_pt(w));
-                }
-            }
+            // Zero face contacts: the GJK/EPA continuation runs in its own
+            // kernel (k_narrowphase_gjk) over the pairs that need it, so its
+            // polytope working set stays out of this kernel.
+            gjk_pending = true;
+            return 0;
         } else if (count <= 4) {
             for (int i = 0; i < count; ++i) cache.pts[i] = to_pt(cands[i]);
             set_meta(cache, uint32_t(count), true);
@@ -798,6 +785,44 @@ __device__ int generate_box_box(v3 h0, v3 p0, qt q0, v3 h1, v3 p1, qt q1, float 
         }
         direct = count > 0;
     }
+    return emit_box_box(q1, p1, cd, cache, direct, gjk, gjk_n, out);
+}
+
+// Second half of the zero-face case (scene.cpp:3545-3590): GJK/EPA witness,
+// replacement or append into the refreshed cache, then emission.
+__device__ int finish_box_box_gjk(v3 h0, v3 p0, qt q0, v3 h1, v3 p1, qt q1, float cd, PcmCache& cache,
+                                  ContactPt* out) {
+    const float mm = smin(pcm_box_margin(h0), pcm_box_margin(h1));
+    Cand w;
+    if (!box_box_gjk_epa(h0, p0, q0, h1, p1, q1, cd, w)) {
+        set_meta(cache, 0, true);
+        return 0;
+    }
+    const float rb = mm * 0.05f;
+    const float rsq = rb * rb;
+    bool replaced = false;
+    const uint32_t n0 = cache_count(cache);
+    for (uint32_t i = 0; i < n0; ++i) {
+        const PcmPoint& o = cache.pts[i];
+        if (smin(vlen2(vsub(lv(o.la), w.la)), vlen2(vsub(lv(o.lb), w.lb))) < rsq) {
+            cache.pts[i] = to_pt(w);
+            replaced = true;
+            break;
+        }
+    }
+    if (!replaced) {
+        if (n0 < 4) {
+            cache.pts[n0] = to_pt(w);
+            set_meta(cache, n0 + 1, true);
+        } else {
+            reduce_five(cache, to_pt(w));
+        }
+    }
+    return emit_box_box(q1, p1, cd, cache, false, true, w.nb, out);
+}
+
+__device__ int emit_box_box(qt q1, v3 p1, float cd, const PcmCache& cache, bool direct, bool gjk, v3 gjk_n,
+                            ContactPt* out) {
     const uint32_t n = cache_count(cache);
     if (n == 0) return 0;
     v3 nb = {0, 0, 0};
@@ -983,26 +1008,42 @@ __device__ int sphere_box(v3 center, float r, v3 h, v3 bc, qt bq, float cd, Cont
     return 1;
 }
 
+// Gu order of a pair (scene.cpp:4298-4310): planes first, otherwise the
+// ScNPhaseCore::shouldSwapBodies orientation (scene.cpp:3275-3283).
+struct PairShapes {
+    uint32_t sa, sb, ta, tb, first, second;
+    bool plane, sphere;
+    float cd;
+};
+__device__ __forceinline__ PairShapes pair_shapes(const DevState& s, uint64_t key) {
+    PairShapes p;
+    p.sa = uint32_t(key >> 32);
+    p.sb = uint32_t(key);
+    p.ta = s.s_type[p.sa];
+    p.tb = s.s_type[p.sb];
+    const uint32_t ba = s.s_body[p.sa], bb = s.s_body[p.sb];
+    const bool da = s.b_flags[ba] & kBodyDynamic, db = s.b_flags[bb] & kBodyDynamic;
+    const bool reversed = !da || (da && db && ba < bb);
+    p.plane = p.ta == kPlane || p.tb == kPlane;
+    p.sphere = p.ta == kSphere || p.tb == kSphere;
+    p.first = p.plane ? (p.ta == kPlane ? p.sa : p.sb) : (reversed ? p.sb : p.sa);
+    p.second = p.plane ? (p.ta == kPlane ? p.sb : p.sa) : (reversed ? p.sa : p.sb);
+    p.cd = s.s_lp[p.sa].w + s.s_lp[p.sb].w;
+    return p;
+}
+
 __global__ void __launch_bounds__(128) k_narrowphase(DevState s) {
     const uint32_t n = *s.cur.n;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-        const uint64_t key = s.cur.key[k];
-        const uint32_t sa = uint32_t(key >> 32), sb = uint32_t(key);
         const int32_t pj = s.prev_idx[k];
         PcmCache cache;
         if (pj >= 0) cache = s.prev.cache[pj];
         else cache.meta = 0u;
-        const uint32_t ta = s.s_type[sa], tb = s.s_type[sb];
-        const uint32_t ba = s.s_body[sa], bb = s.s_body[sb];
-        const bool da = s.b_flags[ba] & kBodyDynamic, db = s.b_flags[bb] & kBodyDynamic;
-        // ScNPhaseCore::shouldSwapBodies orientation (scene.cpp:3275-3283)
-        const bool reversed = !da || (da && db && ba < bb);
-        const bool plane = ta == kPlane || tb == kPlane;
-        const bool sphere = ta == kSphere || tb == kSphere;
-        const uint32_t first = plane ? (ta == kPlane ? sa : sb) : (reversed ? sb : sa);
-        const uint32_t second = plane ? (ta == kPlane ? sb : sa) : (reversed ? sa : sb);
-        const float cd = s.s_lp[sa].w + s.s_lp[sb].w;
+        const PairShapes ps = pair_shapes(s, s.cur.key[k]);
+        const uint32_t sa = ps.sa, sb = ps.sb, ta = ps.ta, tb = ps.tb, first = ps.first, second = ps.second;
+        const bool plane = ps.plane, sphere = ps.sphere;
+        const float cd = ps.cd;
         ContactPt out[4];
         int count = 0;
         const v3 p0 = ld3(s.s_wp[first]), p1 = ld3(s.s_wp[second]);
@@ -1011,7 +1052,10 @@ __global__ void __launch_bounds__(128) k_narrowphase(DevState s) {
         if (plane && !sphere) {
             count = generate_plane_box(p0, {g1.x, g1.y, g1.z}, p1, q1, cd, cache, out);
         } else if (!plane && !sphere) {
-            count = generate_box_box({g0.x, g0.y, g0.z}, p0, q0, {g1.x, g1.y, g1.z}, p1, q1, cd, cache, out);
+            bool gjk_pending = false;
+            count = generate_box_box({g0.x, g0.y, g0.z}, p0, q0, {g1.x, g1.y, g1.z}, p1, q1, cd, cache, out,
+                                     gjk_pending);
+            if (gjk_pending) s.gjk_list[atomicAdd(&s.counters[kCntGjk], 1u)] = k;
         } else {
             const uint32_t sp = ta == kSphere ? sa : sb;
             const v3 c = ld3(s.s_wp[sp]);
@@ -1042,13 +1086,40 @@ __global__ void __launch_bounds__(128) k_narrowphase(DevState s) {
     }
 }
 
+// Box/box pairs whose regenerated manifold had no face contact: GJK/EPA
+// witness and emission from the cache the first kernel left behind.
+__global__ void __launch_bounds__(64) k_narrowphase_gjk(DevState s) {
+    const uint32_t n = s.counters[kCntGjk];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t k = s.gjk_list[i];
+        const PairShapes ps = pair_shapes(s, s.cur.key[k]);
+        PcmCache cache = s.cur.cache[k];
+        const float4 g0 = s.s_geom[ps.first], g1 = s.s_geom[ps.second];
+        ContactPt out[4];
+        int count = finish_box_box_gjk({g0.x, g0.y, g0.z}, ld3(s.s_wp[ps.first]), ldq(s.s_wq[ps.first]),
+                                       {g1.x, g1.y, g1.z}, ld3(s.s_wp[ps.second]), ldq(s.s_wq[ps.second]),
+                                       ps.cd, cache, out);
+        if (count < 0) {
+            atomicOr(s.err, kErrContactOverflow);
+            count = 0;
+        }
+        s.cur.cache[k] = cache;
+        s.cur.count[k] = uint32_t(count);
+        for (int j = 0; j < count; ++j) s.pts[4 * size_t(k) + j] = out[j];
+    }
+}
+
 }  // namespace
 
 void enqueue_narrowphase(const DevState& s, cudaStream_t st, const StageHook& hook) {
     const int T = 128;
     hook(kStNarrow, st);
+    cudaMemsetAsync(s.counters + kCntGjk, 0, 4, st);
     const uint32_t blocks = (s.pair_cap + T - 1) / T;
     k_narrowphase<<<blocks < 148u * 16u ? blocks : 148u * 16u, T, 0, st>>>(s);
+    const uint32_t gb = (s.pair_cap + 63) / 64;
+    k_narrowphase_gjk<<<gb < 148u * 4u ? gb : 148u * 4u, 64, 0, st>>>(s);
 }
 
 }  // namespace fyzz::b200

@@ -695,7 +695,7 @@ __global__ void k_prep_contacts(DevState s) {
         }
         ManagerHeader hd;
         hd.b0 = b0; hd.b1 = b1; hd.count = count; hd.anchors = anchors;
-        hd.sf = sfr; hd.df = dfr; hd.pad0 = hd.pad1 = 0.0f;
+        hd.sf = sfr; hd.df = dfr; hd.ima = A.inv_mass; hd.imb = B.inv_mass;
         s.mh[m] = hd;
         // the new history replaces the old one (friction_by_edge_ swap)
         FrictionHist nh;
@@ -745,51 +745,77 @@ __device__ void solve_desc(const DevState& s, uint32_t d, int it, int pos, int v
         return;
     }
     const uint32_t m = d - s.n_joints;
+    // All of a manager's rows are loaded up front (128-bit loads, issued
+    // together) before the sequential Gauss-Seidel updates run on registers.
+    // NormalRow float4s: {n.xyz, ra.x} {ra.yz, rb.xy} {rb.z, vel_mult,
+    // imp_mult, biased} {unbiased, applied, max_impulse, -}; FrictionRow:
+    // {t.xyz, ra.x} {ra.yz, rb.xy} {rb.z, vel_mult, bias, target} {applied}.
     const ManagerHeader hd = s.mh[m];
+    const float ima = hd.ima, imb = hd.imb;   // 0 for the static world
+    const bool friction = (it >= pos || pos - it <= 3) && hd.anchors;
+    const float4* nr = reinterpret_cast<const float4*>(s.nrow + 4 * size_t(m));
+    const float4* fq = reinterpret_cast<const float4*>(s.frow + 4 * size_t(m));
+    float4 n0[4], n1[4], n2[4], n3[4], f0[4], f1[4], f2[4];
+    float fa[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (uint32_t(j) < hd.count) {
+            n0[j] = nr[4 * j]; n1[j] = nr[4 * j + 1]; n2[j] = nr[4 * j + 2]; n3[j] = nr[4 * j + 3];
+        }
+        if (friction && uint32_t(j) < 2 * hd.anchors) {
+            f0[j] = fq[4 * j]; f1[j] = fq[4 * j + 1]; f2[j] = fq[4 * j + 2];
+            fa[j] = reinterpret_cast<const float*>(fq + 4 * j + 3)[0];
+        }
+    }
     v3 av, aw, bv, bw;
     load_delta(s, hd.b0, av, aw);
     load_delta(s, hd.b1, bv, bw);
-    const float ima = hd.b0 >= 0 ? s.b_inv[hd.b0].w : 0.0f;
-    const float imb = hd.b1 >= 0 ? s.b_inv[hd.b1].w : 0.0f;
-    NormalRow* rows = s.nrow + 4 * size_t(m);
     float nsum = 0.0f;
-    for (uint32_t j = 0; j < hd.count; ++j) {
-        NormalRow& r = rows[j];
-        const v3 n = lv(r.n), ra = lv(r.ra), rb = lv(r.rb);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (uint32_t(j) >= hd.count) break;
+        const v3 n = {n0[j].x, n0[j].y, n0[j].z};
+        const v3 ra = {n0[j].w, n1[j].x, n1[j].y};
+        const v3 rb = {n1[j].z, n1[j].w, n2[j].x};
+        const float vel_mult = n2[j].y, imp_mult = n2[j].z;
+        const float applied = n3[j].y, max_impulse = n3[j].z;
         const float nvel = vdot(n, av) - vdot(n, bv) + vdot(aw, ra) - vdot(bw, rb);
-        const float err = it < pos ? r.biased : r.unbiased;
-        const float dc = smax(-nvel * r.vel_mult + err, -r.applied);
-        const float ni = smin(r.max_impulse, r.imp_mult * r.applied + dc);
-        const float dl = ni - r.applied;
+        const float err = it < pos ? n2[j].w : n3[j].x;
+        const float dc = smax(-nvel * vel_mult + err, -applied);
+        const float ni = smin(max_impulse, imp_mult * applied + dc);
+        const float dl = ni - applied;
         const float da = dl * ima, db = dl * imb;
         av = {av.x + n.x * da, av.y + n.y * da, av.z + n.z * da};
         bv = {bv.x - n.x * db, bv.y - n.y * db, bv.z - n.z * db};
         aw = {aw.x + ra.x * dl, aw.y + ra.y * dl, aw.z + ra.z * dl};
         bw = {bw.x - rb.x * dl, bw.y - rb.y * dl, bw.z - rb.z * dl};
-        r.applied = ni;
+        s.nrow[4 * size_t(m) + j].applied = ni;
         nsum += ni;
     }
-    if ((it >= pos || pos - it <= 3) && hd.anchors) {
+    if (friction) {
         const float coeff = hd.anchors == 2 ? 0.5f : 1.0f;
         const float ms = hd.sf * coeff * nsum;
         const float md = hd.df * coeff * nsum;
         bool broken = false;
-        FrictionRow* fr = s.frow + 4 * size_t(m);
-        for (uint32_t k = 0; k < 2 * hd.anchors; ++k) {
-            FrictionRow& f = fr[k];
-            const v3 n = lv(f.t), ra = lv(f.ra), rb = lv(f.rb);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (uint32_t(k) >= 2 * hd.anchors) break;
+            const v3 n = {f0[k].x, f0[k].y, f0[k].z};
+            const v3 ra = {f0[k].w, f1[k].x, f1[k].y};
+            const v3 rb = {f1[k].z, f1[k].w, f2[k].x};
+            const float vel_mult = f2[k].y, target = f2[k].w, applied = fa[k];
             const float td = vdot(n, av) - vdot(n, bv) + vdot(aw, ra) - vdot(bw, rb);
-            const float bias = it < pos ? f.bias : 0.0f;
-            const float cand = f.applied + (f.target - bias - td) * f.vel_mult;
+            const float bias = it < pos ? f2[k].z : 0.0f;
+            const float cand = applied + (target - bias - td) * vel_mult;
             const bool clamped = fabsf(cand) > ms;
             const float nx = clamped ? smin(md, smax(-md, cand)) : cand;
-            const float dl = nx - f.applied;
+            const float dl = nx - applied;
             const float da = dl * ima, db = dl * imb;
             av = {av.x + n.x * da, av.y + n.y * da, av.z + n.z * da};
             bv = {bv.x - n.x * db, bv.y - n.y * db, bv.z - n.z * db};
             aw = {aw.x + ra.x * dl, aw.y + ra.y * dl, aw.z + ra.z * dl};
             bw = {bw.x - rb.x * dl, bw.y - rb.y * dl, bw.z - rb.z * dl};
-            f.applied = nx;
+            s.frow[4 * size_t(m) + k].applied = nx;
             broken |= clamped;
         }
         if (it + 1 == pos + vel) {

@@ -71,6 +71,7 @@ struct DevState {
     uint32_t* found_flag = nullptr;    // per current pair
     uint32_t* lost_flag = nullptr;     // per previous pair
     ContactPt* pts = nullptr;          // 4 per current pair
+    uint32_t* gjk_list = nullptr;      // pairs awaiting the GJK/EPA continuation
 
     // touching managers
     uint32_t* man_list = nullptr;      // current-pair indices, canonical order
@@ -147,6 +148,6 @@ void enqueue_broadphase(const DevState& s, cudaStream_t st, const StageHook& hoo
 void enqueue_narrowphase(const DevState& s, cudaStream_t st, const StageHook& hook = {});
 void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook = {});
 // counters[] slots
-enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels = 4, kCntSlots = 8 };
+enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels = 4, kCntGjk = 5, kCntSlots = 8 };
 
 }  // namespace fyzz::b200

@@ -779,6 +779,7 @@ private:
         dalloc(d_.found_flag, cap, pair_owned_);
         dalloc(d_.lost_flag, cap, pair_owned_);
         dalloc(d_.pts, size_t(cap) * 4, pair_owned_);
+        dalloc(d_.gjk_list, cap, pair_owned_);
         dalloc(d_.man_list, cap, pair_owned_);
         dalloc(d_.mh, cap, pair_owned_);
         dalloc(d_.nrow, size_t(cap) * 4, pair_owned_);
