@@ -32,7 +32,7 @@ EXPORTS = (
     "fyzz_b200_write_velocities", "fyzz_b200_counts", "fyzz_b200_device_view",
     "fyzz_b200_read_pairs", "fyzz_b200_read_manifolds", "fyzz_b200_read_encoded_bounds",
     "fyzz_b200_read_sorted_min_x", "fyzz_b200_read_levels", "fyzz_b200_profile_step",
-    "fyzz_b200_kernels_per_step",
+    "fyzz_b200_kernels_per_step", "fyzz_b200_sap_pairs_static_scratch",
 )
 STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 
@@ -105,6 +105,8 @@ def lib():
         L.fyzz_b200_read_levels.restype = u64
         L.fyzz_b200_profile_step.argtypes = [vp, f32, vp, u32]
         L.fyzz_b200_kernels_per_step.argtypes = [vp, P(u32)]
+        L.fyzz_b200_sap_pairs_static_scratch.argtypes = [vp, vp, u32, vp, u32, vp, vp, C.c_char_p,
+                                                         C.c_size_t]
         _lib = L
     return _lib
 

@@ -165,6 +165,36 @@ uint64_t fyzz_b200_read_sorted_min_x(fyzz_b200_world* w, uint32_t scene, uint32_
  * descriptor order (joints then touching managers). */
 uint64_t fyzz_b200_read_levels(fyzz_b200_world* w, uint32_t* levels, uint64_t cap);
 
+/* ---- allocation-free sweep-and-prune (no counterpart in the reference) ----
+ * The overlap-pair set of one scene's finite shapes, computed on the device
+ * without allocating any memory: for callers that cannot allocate where they
+ * need a pair set (a frame loop sharing the GPU that must not take the
+ * device-wide synchronisation of cudaMalloc / cudaFree, or a process held to
+ * a device memory budget fixed up front).  The working set lives in one
+ * fixed device array of this library (256 KiB), so:
+ *  - n_shapes is at most FYZZ_B200_STATIC_SAP_MAX_SHAPES; larger inputs
+ *    return FYZZ_B200_INVALID_ARGUMENT and launch nothing;
+ *  - all calls on a device share that array: calls whose work may overlap
+ *    in time (other streams, other threads) race; order them on one stream;
+ *  - the first call on a device (with that device current) resolves the
+ *    array's address and the kernel's shared-memory limit; make it before
+ *    any stream capture on that device.
+ * Inputs (device pointers): bounds_dev n_shapes x 6 encoded values (min x,
+ * y, z, max x, y, z: the layout of fyzz_b200_read_encoded_bounds), body_dev
+ * n_shapes values of body id | (1 << 31 if the body is dynamic).  Pairs
+ * follow the reference's full sweep (scene.cpp:2635-2704: 3-axis overlap,
+ * different bodies, at least one dynamic), are written as (a, b) with a < b
+ * in ascending order to pairs_dev (at most pair_cap pairs), and their total
+ * to *count_dev; when the total exceeds pair_cap the list is incomplete.
+ * Enqueued on stream (a cudaStream_t, NULL = legacy default stream); the
+ * results are ready when that stream reaches this point.  message (may be
+ * NULL) receives the reason for a non-zero status. */
+#define FYZZ_B200_STATIC_SAP_MAX_SHAPES 8192u
+int fyzz_b200_sap_pairs_static_scratch(const uint32_t* bounds_dev, const uint32_t* body_dev,
+                                       uint32_t n_shapes, uint32_t* pairs_dev, uint32_t pair_cap,
+                                       uint32_t* count_dev, void* stream, char* message,
+                                       size_t message_len);
+
 #ifdef __cplusplus
 }
 #endif
