@@ -58,6 +58,13 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--bodies", type=int, default=131072, help="plain-scene body count")
     ap.add_argument("--scenes", type=int, default=4096, help="batched scene count per rank")
+    ap.add_argument("--same-scenes", type=int, default=64,
+                    help="batched scenes sampled for the plain-path-on-the-same-bodies comparison")
+    ap.add_argument("--same-steps", type=int, default=32)
+    ap.add_argument("--settle", type=int, default=0,
+                    help="untimed steps of the plain scene before warm-up (profiling a settled pile)")
+    ap.add_argument("--plain-only", action="store_true",
+                    help="time the plain scene only (no e2e, batched or CPU legs; for profiler runs)")
     return ap.parse_args()
 
 
@@ -66,7 +73,10 @@ def scenes_mod():
 
 
 def plain_spec(n):
-    return scenes_mod().mixed_scale(n, seed=1)
+    """The plain at-scale scene; a smaller body count keeps the scene's
+    density (the 200 x 200 m footprint shrinks with sqrt(n / 131,072))."""
+    side = 200.0 * (n / 131072.0) ** 0.5
+    return scenes_mod().mixed_scale(n, seed=1, region=(side, 50.0, side))
 
 
 def batched_specs(n, rank):
@@ -167,6 +177,29 @@ def ncu_traffic(stage: str):
 
 
 # --------------------------------------------------------------- b200 arm
+def plain_same_bodies(torch, pkg, specs, local_rank, n_sample, steps):
+    """The plain single-scene path on the batched workload's own bodies: a
+    sample of the scenes (evenly spaced over the list, so over the size
+    distribution), each stepped as its own one-scene world, timed with CUDA
+    events on that world's stream.  Returns body-steps/s over the sample."""
+    if n_sample <= 0:
+        return None
+    idx = np.unique(np.linspace(0, len(specs) - 1, min(n_sample, len(specs))).astype(int))
+    total_ms, total_bs = 0.0, 0
+    for i in idx:
+        w = pkg.World(local_rank)
+        w.add_scene(specs[i])
+        w.step(DT, 3)
+        st = torch.cuda.ExternalStream(w.device_view().stream)
+        total_ms += timed_steps(torch, w, steps, st)
+        total_bs += specs[i].n_bodies * steps
+        w.close()
+    return {"value": total_bs / (total_ms / 1e3), "unit": UNIT, "scenes_sampled": int(len(idx)),
+            "bodies_sampled": int(sum(specs[i].n_bodies for i in idx)), "steps": steps,
+            "how": "each sampled scene stepped alone as a one-scene world (the plain path), "
+                   "device time summed over scenes"}
+
+
 def timed_steps(torch, w, steps, stream):
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
@@ -209,6 +242,8 @@ def run_b200(args, rank, world, local_rank):
     w = pkg.World(local_rank)
     w.add_scene(spec)
     n_dyn = spec.n_bodies
+    if args.settle:
+        w.step(DT, args.settle)
     if args.warmup:
         w.step(DT, args.warmup)
     stream = torch.cuda.ExternalStream(w.device_view().stream)
@@ -216,13 +251,17 @@ def run_b200(args, rank, world, local_rank):
     torch.cuda.synchronize()
     for attempt in range(2):
         sampler = ClockSampler(local_rank)
+        torch.cuda.nvtx.range_push("timed")
         ms = timed_steps(torch, w, args.steps, stream)
+        torch.cuda.nvtx.range_pop()
         clocks = sampler.stop()
         if not clocks_bad(clocks):
             break
         if attempt == 0:
             w = pkg.World(local_rank)
             w.add_scene(spec)
+            if args.settle:
+                w.step(DT, args.settle)
             w.step(DT, args.warmup)
             stream = torch.cuda.ExternalStream(w.device_view().stream)
     barrier()
@@ -252,25 +291,27 @@ def run_b200(args, rank, world, local_rank):
                 "algorithmic_bytes": alg, "stage_ms": round(prof[dom], 4)}
 
     # ---- end to end through the C ABI with host buffers ----
-    e2e_steps = max(1, min(args.e2e_steps, args.steps))
-    buf = np.zeros((spec.n_actors, 14), np.float32)
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        w.read_bodies(buf)
-        v6 = np.ascontiguousarray(buf[:, [3, 4, 5, 10, 11, 12]])
-        w.write_velocities(v6)
-        w.step(DT)
-    w.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e = {"value": sum_over_ranks(n_dyn * e2e_steps) / e2e_s, "unit": UNIT,
-           "h2d_bytes_per_step": 32 * spec.n_actors, "d2h_bytes_per_step": 64 * spec.n_actors,
-           "steps": e2e_steps,
-           "loop": "read_bodies (D2H) -> write_velocities (H2D) -> step, host buffers, pinned staging"}
+    e2e = None
+    if not args.plain_only:
+        e2e_steps = max(1, min(args.e2e_steps, args.steps))
+        buf = np.zeros((spec.n_actors, 14), np.float32)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            w.read_bodies(buf)
+            v6 = np.ascontiguousarray(buf[:, [3, 4, 5, 10, 11, 12]])
+            w.write_velocities(v6)
+            w.step(DT)
+        w.synchronize()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        e2e = {"value": sum_over_ranks(n_dyn * e2e_steps) / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": 32 * spec.n_actors, "d2h_bytes_per_step": 64 * spec.n_actors,
+               "steps": e2e_steps,
+               "loop": "read_bodies (D2H) -> write_velocities (H2D) -> step, host buffers, pinned staging"}
 
     # ---- batched forward ----
     batched = None
-    if not args.no_batched:
+    if not args.no_batched and not args.plain_only:
         specs = batched_specs(args.scenes, rank)
         wb = pkg.World(local_rank)
         for s in specs:
@@ -286,16 +327,19 @@ def run_b200(args, rank, world, local_rank):
         bms_max = max_over_ranks(bms)
         bvalue = sum_over_ranks(nb_dyn * args.batched_steps) / (bms_max / 1e3)
         bprof = wb.profile_step(DT)
+        same = plain_same_bodies(torch, pkg, specs, local_rank, args.same_scenes, args.same_steps)
         batched = {"workload": BATCHED_WORKLOAD, "scenes": len(specs) * world, "bodies": nb_dyn * world,
                    "steps": args.batched_steps, "value": bvalue, "unit": UNIT,
                    "ms_per_step": bms_max / args.batched_steps, "clocks": bclocks,
                    "stages_ms": {k: round(v, 4) for k, v in bprof.items()},
-                   "counts": wb.counts(), "gpu_launches": wb.kernels_per_step() * args.batched_steps}
+                   "counts": wb.counts(), "gpu_launches": wb.kernels_per_step() * args.batched_steps,
+                   "plain_same_bodies": same,
+                   "vs_plain_same_bodies": bvalue / world / same["value"] if same else None}
         wb.close()
 
     # ---- CPU baseline: the reference NativeCpu scene on this host ----
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.plain_only:
         cpu = cpu_baseline(spec, args.cpu_seconds)
 
     if rank == 0:
@@ -311,7 +355,8 @@ def run_b200(args, rank, world, local_rank):
                        "l2": f"resident working set ~{ws_mb:.0f} MB > 126 MB L2 (not flushed)",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "batched": batched,
-            "batched_vs_plain": (batched["value"] / value) if batched else None,
+            "batched_vs_plain": batched["vs_plain_same_bodies"] if batched else None,
+            "batched_vs_plain_scene": (batched["value"] / value) if batched else None,
             "e2e": e2e,
             "gpu_launches": kernels * args.steps,
             "roofline": roofline,

@@ -31,7 +31,6 @@ namespace fyzz::b200 {
 namespace {
 constexpr uint32_t kInvalid = 0xffffffffu;
 constexpr int kMaxLevels = 256;
-constexpr uint32_t kSmallIsland = 96;
 
 __device__ __forceinline__ bool is_dyn(const DevState& s, uint32_t b) { return s.b_flags[b] & kBodyDynamic; }
 
@@ -222,7 +221,7 @@ __global__ void k_island_scatter(DevState s, const uint32_t* pos) {
 // (scene.cpp:7367-7437).
 //
 // Small islands: one thread replays that sequential loop.
-// Large islands: one CTA reproduces it exactly in rounds.  A descriptor that
+// Larger islands: one CTA reproduces it exactly in rounds.  A descriptor that
 // is the earliest undecided one on both of its bodies has every earlier
 // descriptor touching those bodies already decided, so it sees exactly the
 // masks the sequential loop would; all such descriptors share no body and are
@@ -230,6 +229,16 @@ __global__ void k_island_scatter(DevState s, const uint32_t* pos) {
 // descriptor of the island.  Waves and the static pass use the same rule.
 constexpr uint32_t kSerialIsland = 32;
 constexpr uint32_t kDeferred = 0xfffffffeu;
+
+// Island-local number of a body (0xffff for the static world), appending
+// unseen bodies to the island's body list.
+__device__ __forceinline__ uint32_t local_slot_serial(int32_t* ib, uint32_t& nb, int32_t b) {
+    if (b < 0) return 0xffffu;
+    for (uint32_t k = 0; k < nb; ++k)
+        if (ib[k] == b) return k;
+    ib[nb] = b;
+    return nb++;
+}
 
 __device__ void place_by_level(const DevState& s, uint32_t isl, uint32_t begin, uint32_t end,
                                uint32_t nlev, uint32_t* lvl_bound) {
@@ -258,7 +267,7 @@ __global__ void __launch_bounds__(256) k_partition_large(DevState s, uint32_t* l
     const uint32_t tid = threadIdx.x, nt = blockDim.x;
     for (uint32_t isl = blockIdx.x; isl < ni; isl += gridDim.x) {
         const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
-        if (end - begin <= kSerialIsland) continue;
+        if (end - begin <= kBigIsland) continue;
         if (tid == 0) nlev_s = 0;
         uint32_t nlev = 0;
         bool ok = true;
@@ -446,6 +455,251 @@ __global__ void k_partition(DevState s, uint32_t* lvl_bound) {
         if (nlev > kMaxLevels) { atomicOr(s.err, kErrLevelRange); nlev = kMaxLevels; }
         if (nlev > end - begin) { atomicOr(s.err, kErrLevelRange); nlev = end - begin; }
         place_by_level(s, isl, begin, end, nlev, lvl_bound);
+        // island-local body numbering, in placed order
+        int32_t* ib = s.isl_bod + begin + isl;
+        uint32_t nb = 0;
+        for (uint32_t i = begin; i < end; ++i) {
+            const int2 b = s.d_bod[s.d_val2[i]];
+            const uint32_t la = local_slot_serial(ib, nb, b.x);
+            const uint32_t lb = local_slot_serial(ib, nb, b.y);
+            s.d_lbod[i] = la | (lb << 16);
+        }
+        s.isl_nbod[isl] = nb;
+    }
+}
+
+// Block-wide exclusive scan of one value per thread; *total receives the sum.
+__device__ uint32_t block_excl_scan(uint32_t v, uint32_t* warp_tot, uint32_t* total) {
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t incl = v;
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= uint32_t(d)) incl += t;
+    }
+    if (lane == 31) warp_tot[w] = incl;
+    __syncthreads();
+    uint32_t pre = 0, tot = 0;
+    for (uint32_t k = 0; k < nw; ++k) {
+        const uint32_t t = warp_tot[k];
+        if (k < w) pre += t;
+        tot += t;
+    }
+    if (threadIdx.x == 0) *total = tot;
+    __syncthreads();
+    return pre + incl - v;
+}
+
+__host__ __device__ constexpr uint32_t pow2_at_least(uint32_t x) {
+    uint32_t p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+// Shared memory of k_partition_smem<MAXN>: a body hash table of at least
+// 1.5x the island's bodies (<= descriptors + 1) with its dense numbering,
+// and per-descriptor local bodies and partitions.
+template <uint32_t MAXN> struct PartSmem {
+    static constexpr uint32_t kTable = pow2_at_least(3 * (MAXN + 1) / 2 + 1);
+    static constexpr size_t kBytes = (2 * size_t(kTable) + 2 * size_t(MAXN)) * 4;
+};
+
+__device__ __forceinline__ uint32_t body_hash(int32_t b, uint32_t lg) {
+    return (uint32_t(b) * 0x9E3779B1u) >> (32u - lg);
+}
+__device__ __forceinline__ uint32_t find_local(const uint32_t* key, const uint32_t* slot, uint32_t T,
+                                               uint32_t lg, int32_t b) {
+    if (b < 0) return 0xffffu;
+    uint32_t h = body_hash(b, lg);
+    for (uint32_t probe = 0; probe < T; ++probe) {
+        if (key[h] == uint32_t(b)) return slot[h];
+        h = (h + 1) & (T - 1);
+    }
+    return 0xffffu;   // unreachable: every body was inserted
+}
+
+// Islands of (min_n, MAXN] descriptors: the rounds of k_partition_large on
+// island-local body slots in shared memory.  The island's dynamic bodies
+// are numbered through a shared-memory hash (open addressing), compacted to
+// 0..nb-1 (written to isl_bod for the solver), and the per-body partition
+// state lives in shared memory.  A round needs two passes: every undecided
+// descriptor offers its index to its bodies (atomicMin), then the ones that
+// won on both bodies are decided and clear their bodies' minimum.  Islands
+// larger than list_min are appended to list for the CTA solver.
+template <uint32_t MAXN>
+__global__ void __launch_bounds__(256) k_partition_smem(DevState s, uint32_t* lvl_bound, uint32_t min_n,
+                                                        uint32_t* list, uint32_t* list_n,
+                                                        uint32_t list_min) {
+    constexpr uint32_t TMAX = PartSmem<MAXN>::kTable;
+    extern __shared__ uint32_t sm[];
+    uint32_t* key = sm;              // [T] hashed body ids
+    uint32_t* slot = sm + TMAX;      // [T] dense number of an occupied entry
+    uint32_t* lid = sm + 2 * TMAX;   // [n] local a | local b << 16
+    uint32_t* lvl = lid + MAXN;      // [n] partition, kInvalid undecided, kDeferred
+    // After numbering, the body state reuses the table (3 nb <= 2 T):
+    uint32_t* mask = sm;             // [nb] partition bits of the current wave
+    uint32_t* mds = sm;              // [nb] last dynamic partition + 1 | statics << 16 (set below)
+    uint32_t* earliest = sm;         // [nb]
+    __shared__ uint32_t cursor[kMaxLevels + 1];
+    __shared__ uint32_t warp_tot[32];
+    __shared__ uint32_t nb_s, nlev_s;
+    const uint32_t tid = threadIdx.x, nt = blockDim.x;
+    const uint32_t ni = *s.n_isl;
+    for (uint32_t isl = blockIdx.x; isl < ni; isl += gridDim.x) {
+        const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
+        const uint32_t n = end - begin;
+        if (n <= min_n || n > MAXN) continue;
+        const uint32_t T = pow2_at_least(3 * (n + 1) / 2 + 1);
+        uint32_t lg = 0;
+        while ((1u << lg) < T) ++lg;
+        for (uint32_t h = tid; h < T; h += nt) key[h] = kInvalid;
+        __syncthreads();
+        for (uint32_t i = tid; i < n; i += nt) {
+            const int2 b = s.d_bod[s.d_val[begin + i]];
+            for (int k = 0; k < 2; ++k) {
+                const int32_t body = k ? b.y : b.x;
+                if (body < 0) continue;
+                uint32_t h = body_hash(body, lg);
+                for (uint32_t probe = 0; probe < T; ++probe) {
+                    const uint32_t prev = atomicCAS(&key[h], kInvalid, uint32_t(body));
+                    if (prev == kInvalid || prev == uint32_t(body)) break;
+                    h = (h + 1) & (T - 1);
+                }
+            }
+        }
+        __syncthreads();
+        {
+            const uint32_t per = (T + nt - 1) / nt;
+            const uint32_t h0 = min(tid * per, T), h1 = min(h0 + per, T);
+            uint32_t c = 0;
+            for (uint32_t h = h0; h < h1; ++h) c += key[h] != kInvalid ? 1u : 0u;
+            uint32_t at = block_excl_scan(c, warp_tot, &nb_s);
+            for (uint32_t h = h0; h < h1; ++h)
+                if (key[h] != kInvalid) {
+                    slot[h] = at;
+                    s.isl_bod[begin + isl + at] = int32_t(key[h]);
+                    ++at;
+                }
+        }
+        __syncthreads();
+        const uint32_t nb = nb_s;
+        for (uint32_t i = tid; i < n; i += nt) {
+            const int2 b = s.d_bod[s.d_val[begin + i]];
+            lid[i] = find_local(key, slot, T, lg, b.x) | (find_local(key, slot, T, lg, b.y) << 16);
+            lvl[i] = kInvalid;
+        }
+        __syncthreads();
+        mask = sm;
+        mds = sm + nb;
+        earliest = sm + 2 * nb;
+        for (uint32_t l = tid; l < nb; l += nt) { mask[l] = 0u; mds[l] = 0u; }
+        __syncthreads();
+        uint32_t nlev = 0;
+        for (uint32_t wave = 0;; wave += 32) {
+            if (wave) {
+                for (uint32_t i = tid; i < n; i += nt)
+                    if (lvl[i] == kDeferred) { mask[lid[i] & 0xffffu] = 0u; mask[lid[i] >> 16] = 0u; }
+                __syncthreads();
+                for (uint32_t i = tid; i < n; i += nt)
+                    if (lvl[i] == kDeferred) lvl[i] = kInvalid;
+            }
+            for (uint32_t l = tid; l < nb; l += nt) earliest[l] = kInvalid;
+            __syncthreads();
+            for (uint32_t round = 0; round <= n; ++round) {
+                for (uint32_t i = tid; i < n; i += nt) {
+                    const uint32_t la = lid[i] & 0xffffu, lb = lid[i] >> 16;
+                    if (la == 0xffffu || lb == 0xffffu || lvl[i] != kInvalid) continue;
+                    atomicMin(&earliest[la], i);
+                    atomicMin(&earliest[lb], i);
+                }
+                __syncthreads();
+                bool left = false;
+                for (uint32_t i = tid; i < n; i += nt) {
+                    const uint32_t la = lid[i] & 0xffffu, lb = lid[i] >> 16;
+                    if (la == 0xffffu || lb == 0xffffu || lvl[i] != kInvalid) continue;
+                    if (earliest[la] != i || earliest[lb] != i) { left = true; continue; }
+                    earliest[la] = kInvalid;
+                    earliest[lb] = kInvalid;
+                    const uint32_t avail = ~(mask[la] | mask[lb]);
+                    if (!avail) { lvl[i] = kDeferred; continue; }
+                    const uint32_t bit = __ffs(avail) - 1;
+                    mask[la] |= 1u << bit;
+                    mask[lb] |= 1u << bit;
+                    const uint32_t lp = wave + bit;
+                    mds[la] = max(mds[la], lp + 1);
+                    mds[lb] = max(mds[lb], lp + 1);
+                    lvl[i] = lp;
+                    nlev = max(nlev, lp + 1);
+                }
+                if (!__syncthreads_or(left)) break;
+            }
+            bool deferred = false;
+            for (uint32_t i = tid; i < n; i += nt) deferred |= lvl[i] == kDeferred;
+            if (!__syncthreads_or(deferred)) break;
+            if (wave + 32 >= kMaxLevels) {
+                if (tid == 0) atomicOr(s.err, kErrLevelRange);
+                break;
+            }
+        }
+        // statics, in descriptor order per body, after its last dynamic partition
+        for (uint32_t l = tid; l < nb; l += nt) earliest[l] = kInvalid;
+        __syncthreads();
+        for (uint32_t round = 0; round <= n; ++round) {
+            for (uint32_t i = tid; i < n; i += nt) {
+                const uint32_t la = lid[i] & 0xffffu, lb = lid[i] >> 16;
+                if ((la == 0xffffu) == (lb == 0xffffu) || lvl[i] != kInvalid) continue;
+                atomicMin(&earliest[la != 0xffffu ? la : lb], i);
+            }
+            __syncthreads();
+            bool left = false;
+            for (uint32_t i = tid; i < n; i += nt) {
+                const uint32_t la = lid[i] & 0xffffu, lb = lid[i] >> 16;
+                if ((la == 0xffffu) == (lb == 0xffffu) || lvl[i] != kInvalid) continue;
+                const uint32_t act = la != 0xffffu ? la : lb;
+                if (earliest[act] != i) { left = true; continue; }
+                earliest[act] = kInvalid;
+                const uint32_t m = mds[act];
+                const uint32_t lp = (m & 0xffffu) + (m >> 16);
+                mds[act] = m + 0x10000u;
+                lvl[i] = lp;
+                nlev = max(nlev, lp + 1);
+            }
+            if (!__syncthreads_or(left)) break;
+        }
+        if (tid == 0) nlev_s = 0;
+        __syncthreads();
+        atomicMax(&nlev_s, nlev);
+        __syncthreads();
+        nlev = max(nlev_s, 1u);
+        if (nlev > uint32_t(kMaxLevels) || nlev > n) {
+            if (tid == 0) atomicOr(s.err, kErrLevelRange);
+            nlev = min(min(nlev, uint32_t(kMaxLevels)), n);
+        }
+        for (uint32_t l = tid; l <= nlev; l += nt) cursor[l] = 0u;
+        __syncthreads();
+        for (uint32_t i = tid; i < n; i += nt) atomicAdd(&cursor[min(lvl[i], nlev - 1)], 1u);
+        __syncthreads();
+        if (tid == 0) {
+            uint32_t* bound = lvl_bound + begin + isl;
+            uint32_t run = begin;
+            for (uint32_t l = 0; l < nlev; ++l) {
+                const uint32_t c = cursor[l];
+                bound[l] = run;
+                cursor[l] = run;
+                run += c;
+            }
+            bound[nlev] = end;
+            s.isl_end[isl] = nlev;
+            s.isl_nbod[isl] = nb;
+            if (n > list_min) list[atomicAdd(list_n, 1u)] = isl;
+        }
+        __syncthreads();
+        for (uint32_t i = tid; i < n; i += nt) {
+            const uint32_t d = s.d_val[begin + i];
+            const uint32_t at = atomicAdd(&cursor[min(lvl[i], nlev - 1)], 1u);
+            s.d_val2[at] = d;
+            s.d_lbod[at] = lid[i];
+            s.d_level[d] = lvl[i];
+        }
+        __syncthreads();
     }
 }
 
@@ -710,25 +964,60 @@ __global__ void k_prep_contacts(DevState s) {
 }
 
 // ---------------- PGS ----------------
-__device__ __forceinline__ void load_delta(const DevState& s, int32_t b, v3& dv, v3& dw) {
-    if (b < 0) { dv = dw = {0, 0, 0}; return; }
-    dv = ld3(s.sb_dv[b]);
-    dw = ld3(s.sb_dw[b]);
-}
-__device__ __forceinline__ void store_delta(const DevState& s, int32_t b, v3 dv, v3 dw) {
-    if (b < 0) return;
-    s.sb_dv[b] = st4(dv, 0.0f);
-    s.sb_dw[b] = st4(dw, 0.0f);
-}
+// Velocity deltas of the solver bodies, addressed either by global body
+// (islands too large for shared memory) or by island-local slot in shared
+// memory.  Handle -1 is the static world (zero delta, never written).
+struct GlobalDeltas {
+    static constexpr bool kLocal = false;
+    const DevState& s;
+    __device__ __forceinline__ void load(int32_t b, v3& dv, v3& dw) const {
+        if (b < 0) { dv = dw = {0, 0, 0}; return; }
+        dv = ld3(s.sb_dv[b]);
+        dw = ld3(s.sb_dw[b]);
+    }
+    __device__ __forceinline__ void store(int32_t b, v3 dv, v3 dw) const {
+        if (b < 0) return;
+        s.sb_dv[b] = st4(dv, 0.0f);
+        s.sb_dw[b] = st4(dw, 0.0f);
+    }
+};
+struct LocalDeltas {
+    static constexpr bool kLocal = true;
+    float4* dv_;
+    float4* dw_;
+    __device__ __forceinline__ void load(int32_t l, v3& dv, v3& dw) const {
+        if (l < 0) { dv = dw = {0, 0, 0}; return; }
+        dv = ld3(dv_[l]);
+        dw = ld3(dw_[l]);
+    }
+    __device__ __forceinline__ void store(int32_t l, v3 dv, v3 dw) const {
+        if (l < 0) return;
+        dv_[l] = st4(dv, 0.0f);
+        dw_[l] = st4(dw, 0.0f);
+    }
+};
+__device__ __forceinline__ int32_t unpack_local(uint32_t v) { return v == 0xffffu ? -1 : int32_t(v); }
 
-__device__ void solve_desc(const DevState& s, uint32_t d, int it, int pos, int vel) {
+// One descriptor's rows for pass `it` (scene.cpp:8853-9148).  lid carries
+// the island-local bodies when D addresses shared memory.
+// kEagerFriction issues the friction-row loads together with the normal
+// rows (lowest latency, for the CTA solvers); otherwise they are issued
+// after the normal rows are solved (fewer registers, for the warp solver).
+template <class D, bool kEagerFriction = true>
+__device__ void solve_desc(const DevState& s, uint32_t d, uint32_t lid, int it, int pos, int vel, const D& D_) {
     if (d < s.n_joints) {
         JointRow& r = s.jrow[d];
-        const int32_t b0 = is_dyn(s, s.j_a[d]) ? int32_t(s.j_a[d]) : -1;
-        const int32_t b1 = is_dyn(s, s.j_b[d]) ? int32_t(s.j_b[d]) : -1;
+        int32_t b0, b1;
+        if constexpr (D::kLocal) {
+            b0 = unpack_local(lid & 0xffffu);
+            b1 = unpack_local(lid >> 16);
+        } else {
+            b0 = is_dyn(s, s.j_a[d]) ? int32_t(s.j_a[d]) : -1;
+            b1 = is_dyn(s, s.j_b[d]) ? int32_t(s.j_b[d]) : -1;
+        }
         v3 av, aw, bv, bw;
-        load_delta(s, b0, av, aw);
-        load_delta(s, b1, bv, bw);
+        D_.load(b0, av, aw);
+        D_.load(b1, bv, bw);
         const v3 ax = lv(r.axis), ja = lv(r.ang_a), jb = lv(r.ang_b);
         const float nd = ax.x * (av.x - bv.x) + ax.y * (av.y - bv.y) + ax.z * (av.z - bv.z) + vdot(ja, aw) - vdot(jb, bw);
         const float cst = it < pos ? r.constant : r.unbiased;
@@ -739,8 +1028,8 @@ __device__ void solve_desc(const DevState& s, uint32_t d, int it, int pos, int v
         bv = {bv.x - ib * ax.x, bv.y - ib * ax.y, bv.z - ib * ax.z};
         aw = {aw.x + imp * ja.x, aw.y + imp * ja.y, aw.z + imp * ja.z};
         bw = {bw.x - imp * jb.x, bw.y - imp * jb.y, bw.z - imp * jb.z};
-        store_delta(s, b0, av, aw);
-        store_delta(s, b1, bv, bw);
+        D_.store(b0, av, aw);
+        D_.store(b1, bv, bw);
         r.applied = nx;
         return;
     }
@@ -762,14 +1051,22 @@ __device__ void solve_desc(const DevState& s, uint32_t d, int it, int pos, int v
         if (uint32_t(j) < hd.count) {
             n0[j] = nr[4 * j]; n1[j] = nr[4 * j + 1]; n2[j] = nr[4 * j + 2]; n3[j] = nr[4 * j + 3];
         }
-        if (friction && uint32_t(j) < 2 * hd.anchors) {
+        if (kEagerFriction && friction && uint32_t(j) < 2 * hd.anchors) {
             f0[j] = fq[4 * j]; f1[j] = fq[4 * j + 1]; f2[j] = fq[4 * j + 2];
             fa[j] = reinterpret_cast<const float*>(fq + 4 * j + 3)[0];
         }
     }
+    int32_t h0, h1;
+    if constexpr (D::kLocal) {
+        h0 = unpack_local(lid & 0xffffu);
+        h1 = unpack_local(lid >> 16);
+    } else {
+        h0 = hd.b0;
+        h1 = hd.b1;
+    }
     v3 av, aw, bv, bw;
-    load_delta(s, hd.b0, av, aw);
-    load_delta(s, hd.b1, bv, bw);
+    D_.load(h0, av, aw);
+    D_.load(h1, bv, bw);
     float nsum = 0.0f;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -793,6 +1090,14 @@ __device__ void solve_desc(const DevState& s, uint32_t d, int it, int pos, int v
         nsum += ni;
     }
     if (friction) {
+        if constexpr (!kEagerFriction) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (uint32_t(j) < 2 * hd.anchors) {
+                    f0[j] = fq[4 * j]; f1[j] = fq[4 * j + 1]; f2[j] = fq[4 * j + 2];
+                    fa[j] = reinterpret_cast<const float*>(fq + 4 * j + 3)[0];
+                }
+        }
         const float coeff = hd.anchors == 2 ? 0.5f : 1.0f;
         const float ms = hd.sf * coeff * nsum;
         const float md = hd.df * coeff * nsum;
@@ -823,8 +1128,8 @@ __device__ void solve_desc(const DevState& s, uint32_t d, int it, int pos, int v
             h.meta = (h.meta & ~256u) | (broken ? 256u : 0u);
         }
     }
-    store_delta(s, hd.b0, av, aw);
-    store_delta(s, hd.b1, bv, bw);
+    D_.store(h0, av, aw);
+    D_.store(h1, bv, bw);
 }
 __device__ __forceinline__ void save_motion(const DevState& s, uint32_t d) {
     int32_t b0, b1;
@@ -839,44 +1144,112 @@ __device__ __forceinline__ void save_motion(const DevState& s, uint32_t d) {
     if (b1 >= 0) { s.sb_mdv[b1] = s.sb_dv[b1]; s.sb_mdw[b1] = s.sb_dw[b1]; }
 }
 
-// One warp per small island.
-__global__ void k_pgs_warp(DevState s, const uint32_t* lvl_bound) {
+// Copies of an island's shared-memory deltas to the solver bodies.
+__device__ __forceinline__ void island_deltas_out(float4* dst_v, float4* dst_w, const int32_t* ib, uint32_t nb,
+                                                  const float4* sdv, const float4* sdw, uint32_t t0,
+                                                  uint32_t nt) {
+    for (uint32_t l = t0; l < nb; l += nt) {
+        const int32_t g = ib[l];
+        dst_v[g] = sdv[l];
+        dst_w[g] = sdw[l];
+    }
+}
+
+// One warp per small island (<= kSmallIsland descriptors, so <= 97 bodies):
+// the island's deltas live in this warp's slice of shared memory.
+constexpr uint32_t kWarpBodies = kSmallIsland + 1;
+constexpr uint32_t kPgsWarpsPerBlock = 4;
+__global__ void __launch_bounds__(kPgsWarpsPerBlock * 32, 3) k_pgs_warp(DevState s, const uint32_t* lvl_bound) {
+    __shared__ float4 sh[kPgsWarpsPerBlock][2][kWarpBodies];
     const uint32_t ni = *s.n_isl;
-    const int lane = threadIdx.x & 31;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t wib = threadIdx.x >> 5;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const int pos = s.pos_iters, vel = s.vel_iters < 1 ? 1 : s.vel_iters;
+    float4* sdv = sh[wib][0];
+    float4* sdw = sh[wib][1];
+    const LocalDeltas D{sdv, sdw};
+    const float4 zero = make_float4(0, 0, 0, 0);
     for (uint32_t isl = warp; isl < ni; isl += nwarps) {
         const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
         if (end - begin > kSmallIsland) continue;
         const uint32_t nlev = s.isl_end[isl];
+        const uint32_t nb = s.isl_nbod[isl];
+        const int32_t* ib = s.isl_bod + begin + isl;
         const uint32_t* bound = lvl_bound + begin + isl;
+        for (uint32_t l = lane; l < nb; l += 32) { sdv[l] = zero; sdw[l] = zero; }
+        __syncwarp();
         for (int it = 0; it < pos + vel; ++it) {
             for (uint32_t l = 0; l < nlev; ++l) {
                 const uint32_t lb = bound[l], le = bound[l + 1];
-                for (uint32_t i = lb + lane; i < le; i += 32) solve_desc(s, s.d_val2[i], it, pos, vel);
+                for (uint32_t i = lb + lane; i < le; i += 32)
+                    solve_desc<LocalDeltas, false>(s, s.d_val2[i], s.d_lbod[i], it, pos, vel, D);
                 __syncwarp();
             }
             if (it + 1 == pos) {
-                for (uint32_t i = begin + lane; i < end; i += 32) save_motion(s, s.d_val2[i]);
+                island_deltas_out(s.sb_mdv, s.sb_mdw, ib, nb, sdv, sdw, lane, 32);
                 __syncwarp();
             }
         }
+        island_deltas_out(s.sb_dv, s.sb_dw, ib, nb, sdv, sdw, lane, 32);
+        __syncwarp();
     }
 }
-// One CTA per large island.
+
+// One CTA per island of (kSmallIsland, MAXN] descriptors from list, with
+// the island's deltas in shared memory (2 x (MAXN + 1) float4).
+template <uint32_t MAXN>
+__global__ void __launch_bounds__(256) k_pgs_block_smem(DevState s, const uint32_t* lvl_bound,
+                                                        const uint32_t* list, const uint32_t* list_n) {
+    extern __shared__ float4 shb[];
+    float4* sdv = shb;
+    float4* sdw = shb + (MAXN + 1);
+    const LocalDeltas D{sdv, sdw};
+    const uint32_t n_list = *list_n;
+    const int pos = s.pos_iters, vel = s.vel_iters < 1 ? 1 : s.vel_iters;
+    const float4 zero = make_float4(0, 0, 0, 0);
+    for (uint32_t k = blockIdx.x; k < n_list; k += gridDim.x) {
+        const uint32_t isl = list[k];
+        const uint32_t begin = s.isl_begin[isl];
+        const uint32_t nlev = s.isl_end[isl];
+        const uint32_t nb = s.isl_nbod[isl];
+        const int32_t* ib = s.isl_bod + begin + isl;
+        const uint32_t* bound = lvl_bound + begin + isl;
+        for (uint32_t l = threadIdx.x; l < nb; l += blockDim.x) { sdv[l] = zero; sdw[l] = zero; }
+        __syncthreads();
+        for (int it = 0; it < pos + vel; ++it) {
+            for (uint32_t l = 0; l < nlev; ++l) {
+                const uint32_t lb = bound[l], le = bound[l + 1];
+                for (uint32_t i = lb + threadIdx.x; i < le; i += blockDim.x)
+                    solve_desc(s, s.d_val2[i], s.d_lbod[i], it, pos, vel, D);
+                __syncthreads();
+            }
+            if (it + 1 == pos) {
+                island_deltas_out(s.sb_mdv, s.sb_mdw, ib, nb, sdv, sdw, threadIdx.x, blockDim.x);
+                __syncthreads();
+            }
+        }
+        island_deltas_out(s.sb_dv, s.sb_dw, ib, nb, sdv, sdw, threadIdx.x, blockDim.x);
+        __syncthreads();
+    }
+}
+
+// One CTA per island beyond kBigIsland descriptors: deltas in global memory.
 __global__ void __launch_bounds__(256) k_pgs_block(DevState s, const uint32_t* lvl_bound) {
     const uint32_t ni = *s.n_isl;
     const int pos = s.pos_iters, vel = s.vel_iters < 1 ? 1 : s.vel_iters;
+    const GlobalDeltas D{s};
     for (uint32_t isl = blockIdx.x; isl < ni; isl += gridDim.x) {
         const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
-        if (end - begin <= kSmallIsland) continue;
+        if (end - begin <= kBigIsland) continue;
         const uint32_t nlev = s.isl_end[isl];
         const uint32_t* bound = lvl_bound + begin + isl;
         for (int it = 0; it < pos + vel; ++it) {
             for (uint32_t l = 0; l < nlev; ++l) {
                 const uint32_t lb = bound[l], le = bound[l + 1];
-                for (uint32_t i = lb + threadIdx.x; i < le; i += blockDim.x) solve_desc(s, s.d_val2[i], it, pos, vel);
+                for (uint32_t i = lb + threadIdx.x; i < le; i += blockDim.x)
+                    solve_desc(s, s.d_val2[i], 0u, it, pos, vel, D);
                 __syncthreads();
             }
             if (it + 1 == pos) {
@@ -947,12 +1320,34 @@ inline uint32_t grid_for(uint32_t n, uint32_t t, uint32_t cap) {
 
 }  // namespace
 
-void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook) {
+// Fork n side branches off st (or run everything on st without branches).
+static void fork_branches(const Branches* br, cudaStream_t st, int n) {
+    if (!br) return;
+    cudaEventRecord(br->fork, st);
+    for (int i = 0; i < n; ++i) cudaStreamWaitEvent(br->st[i], br->fork, 0);
+}
+static void join_branches(const Branches* br, cudaStream_t st, int n) {
+    if (!br) return;
+    for (int i = 0; i < n; ++i) {
+        cudaEventRecord(br->join[i], br->st[i]);
+        cudaStreamWaitEvent(st, br->join[i], 0);
+    }
+}
+
+void init_solver_kernels() {
+    cudaFuncSetAttribute(k_partition_smem<kBigIsland>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(PartSmem<kBigIsland>::kBytes));
+    cudaFuncSetAttribute(k_pgs_block_smem<kBigIsland>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(2 * (kBigIsland + 1) * sizeof(float4)));
+}
+
+void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, const Branches* br) {
     uint32_t* flags = s.tmp_flags;
     uint32_t* pos = s.tmp_pos;
     uint32_t* lvl_bound = s.lvl_bound;
     const uint32_t T = 256;
     const uint32_t cap_blocks = 148u * 8u;
+    auto side = [&](int i) { return br ? br->st[i] : st; };
     hook(kStIslands, st);
     k_frame_begin<<<1, 32, 0, st>>>(s);
     k_bodies_begin<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
@@ -960,7 +1355,7 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook) {
     k_touch_flags<<<grid_for(s.pair_cap, T, cap_blocks), T, 0, st>>>(s, flags);
     scan_exclusive(flags, pos, s.pair_cap, s.cur.n, s.counters + kCntMan, s.scan_tmp, s.scan_tmp_words, st);
     k_touch_scatter<<<grid_for(s.pair_cap, T, cap_blocks), T, 0, st>>>(s, flags, pos);
-    // islands and partitions
+    // islands
     k_desc_bodies<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     k_union<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     k_desc_keys<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
@@ -971,16 +1366,34 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook) {
     k_island_flags<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     scan_exclusive(s.isl_flag, pos, s.desc_cap, s.counters + kCntDesc, s.n_isl, s.scan_tmp, s.scan_tmp_words, st);
     k_island_scatter<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s, pos);
-    k_partition<<<grid_for(s.desc_cap, 128, cap_blocks), 128, 0, st>>>(s, lvl_bound);
-    k_partition_large<<<grid_for(s.desc_cap, 1, 148u * 4u), 256, 0, st>>>(s, lvl_bound);
-    // rows
+    cudaMemsetAsync(s.counters + kCntMid, 0, 2 * sizeof(uint32_t), st);
+    // partitions by island size class, and row preparation: independent
     hook(kStPrep, st);
-    if (s.n_joints) k_prep_joints<<<grid_for(s.n_joints, T, 1u << 30), T, 0, st>>>(s);
-    k_prep_contacts<<<grid_for(s.desc_cap, 128, cap_blocks), 128, 0, st>>>(s);
-    // PGS
+    fork_branches(br, st, 3);
+    k_partition<<<grid_for(s.desc_cap, 128, cap_blocks), 128, 0, st>>>(s, lvl_bound);
+    k_partition_smem<kMidIsland><<<grid_for(s.desc_cap, kSerialIsland + 1, 148u * 8u), 256,
+                                   PartSmem<kMidIsland>::kBytes, side(0)>>>(
+        s, lvl_bound, kSerialIsland, s.isl_mid, s.counters + kCntMid, kSmallIsland);
+    k_partition_smem<kBigIsland><<<grid_for(s.desc_cap, kMidIsland + 1, 148u * 2u), 256,
+                                   PartSmem<kBigIsland>::kBytes, side(1)>>>(
+        s, lvl_bound, kMidIsland, s.isl_big, s.counters + kCntBig, kMidIsland);
+    k_partition_large<<<grid_for(s.desc_cap, kBigIsland + 1, 148u), 256, 0, side(1)>>>(s, lvl_bound);
+    if (s.n_joints) k_prep_joints<<<grid_for(s.n_joints, T, 1u << 30), T, 0, side(2)>>>(s);
+    k_prep_contacts<<<grid_for(s.desc_cap, 128, cap_blocks), 128, 0, side(2)>>>(s);
+    join_branches(br, st, 3);
+    // PGS: islands by size class, independent
     hook(kStPgs, st);
-    k_pgs_warp<<<grid_for(s.desc_cap * 32u, T, cap_blocks), T, 0, st>>>(s, lvl_bound);
-    k_pgs_block<<<grid_for(s.desc_cap, 1, 148u * 4u), 256, 0, st>>>(s, lvl_bound);
+    fork_branches(br, st, 2);
+    k_pgs_warp<<<grid_for(s.desc_cap * 32u, kPgsWarpsPerBlock * 32u, 148u * 3u), kPgsWarpsPerBlock * 32u, 0, st>>>(
+        s, lvl_bound);
+    k_pgs_block_smem<kMidIsland><<<grid_for(s.desc_cap, kSmallIsland + 1, 148u * 4u), 256,
+                                   2 * (kMidIsland + 1) * sizeof(float4), side(0)>>>(
+        s, lvl_bound, s.isl_mid, s.counters + kCntMid);
+    k_pgs_block_smem<kBigIsland><<<grid_for(s.desc_cap, kMidIsland + 1, 148u), 256,
+                                   2 * (kBigIsland + 1) * sizeof(float4), side(1)>>>(
+        s, lvl_bound, s.isl_big, s.counters + kCntBig);
+    k_pgs_block<<<grid_for(s.desc_cap, kBigIsland + 1, 148u), 256, 0, side(1)>>>(s, lvl_bound);
+    join_branches(br, st, 2);
     hook(kStIntegrate, st);
     k_integrate<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
     hook(kStEnd, st);

@@ -101,6 +101,14 @@ struct DevState {
     uint32_t* sb_static = nullptr;
     uint32_t* sb_earliest = nullptr;   // per-body earliest undecided descriptor (partition rounds)
     int2* d_bod = nullptr;             // per descriptor: dynamic solver bodies (-1 = static world)
+    // Island-local body slots (islands up to kBigIsland descriptors): the
+    // island's dynamic bodies are numbered 0..n-1 so PGS can keep their
+    // velocity deltas in shared memory.
+    uint32_t* d_lbod = nullptr;        // per placed descriptor: local a | local b << 16 (0xffff static)
+    int32_t* isl_bod = nullptr;        // island isl's bodies at [isl_begin + isl, + isl_nbod)
+    uint32_t* isl_nbod = nullptr;      // per island
+    uint32_t* isl_mid = nullptr;       // islands solved by one CTA with shared-memory deltas
+    uint32_t* isl_big = nullptr;
 
     // step scratch
     uint4* sw_rec = nullptr;           // sweep y/z bounds in sorted order
@@ -143,11 +151,30 @@ struct StageHook {
     void operator()(int stage, cudaStream_t st) const { if (fn) fn(ctx, stage, st); }
 };
 
+// Side streams for independent branches of a step.  They fork from and join
+// back into the main stream through events, so inside a stream capture they
+// become parallel branches of the step's graph.
+struct Branches {
+    static constexpr int kN = 3;
+    cudaStream_t st[kN] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[kN] = {};
+};
+
 // broadphase.cu / narrowphase.cu / solver.cu
 void enqueue_broadphase(const DevState& s, cudaStream_t st, const StageHook& hook = {});
 void enqueue_narrowphase(const DevState& s, cudaStream_t st, const StageHook& hook = {});
-void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook = {});
+void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook = {},
+                    const Branches* br = nullptr);
+// Per-device kernel attributes (shared-memory limits); call with the device
+// current before the first step or capture.
+void init_solver_kernels();
+// Island size classes (descriptors per island).
+constexpr uint32_t kSmallIsland = 96;     // one warp
+constexpr uint32_t kMidIsland = 512;      // one CTA, shared-memory deltas
+constexpr uint32_t kBigIsland = 4096;     // one CTA, shared-memory deltas (1 CTA / SM)
 // counters[] slots
-enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels = 4, kCntGjk = 5, kCntSlots = 8 };
+enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels = 4, kCntGjk = 5,
+             kCntMid = 6, kCntBig = 7, kCntSlots = 8 };
 
 }  // namespace fyzz::b200

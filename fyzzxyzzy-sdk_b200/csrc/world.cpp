@@ -161,6 +161,13 @@ public:
     explicit World(int device) : device_(device) {
         check_cuda(cudaSetDevice(device_), "cudaSetDevice");
         check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+        for (int i = 0; i < Branches::kN; ++i) {
+            check_cuda(cudaStreamCreateWithFlags(&br_.st[i], cudaStreamNonBlocking), "cudaStreamCreate");
+            check_cuda(cudaEventCreateWithFlags(&br_.join[i], cudaEventDisableTiming), "cudaEventCreate");
+        }
+        check_cuda(cudaEventCreateWithFlags(&br_.fork, cudaEventDisableTiming), "cudaEventCreate");
+        init_solver_kernels();
+        check_cuda(cudaGetLastError(), "kernel attributes");
         check_cuda(cudaMallocHost(reinterpret_cast<void**>(&host_err_), 64), "cudaMallocHost");
         scene_body_begin_.push_back(0);
         scene_shape_begin_.push_back(0);
@@ -170,6 +177,11 @@ public:
         cudaSetDevice(device_);
         release_device();
         if (host_err_) cudaFreeHost(host_err_);
+        for (int i = 0; i < Branches::kN; ++i) {
+            if (br_.st[i]) cudaStreamDestroy(br_.st[i]);
+            if (br_.join[i]) cudaEventDestroy(br_.join[i]);
+        }
+        if (br_.fork) cudaEventDestroy(br_.fork);
         if (stream_) cudaStreamDestroy(stream_);
     }
     std::string error;
@@ -468,7 +480,7 @@ public:
         const DevState s = view(parity_);
         enqueue_broadphase(s, stream_, hook);
         enqueue_narrowphase(s, stream_, hook);
-        enqueue_solver(s, stream_, hook);
+        enqueue_solver(s, stream_, hook, &br_);
         check_cuda(cudaGetLastError(), "profile launch");
         const uint32_t err = read_err();
         last_cur_ = parity_;
@@ -708,7 +720,7 @@ private:
                 const DevState s = view(parity_);
                 enqueue_broadphase(s, stream_);
                 enqueue_narrowphase(s, stream_);
-                enqueue_solver(s, stream_);
+                enqueue_solver(s, stream_, {}, &br_);
                 check_cuda(cudaStreamEndCapture(stream_, &g), "end capture");
                 size_t nn = 0;
                 check_cuda(cudaGraphGetNodes(g, nullptr, &nn), "graph nodes");
@@ -789,6 +801,11 @@ private:
         dalloc(d_.d_key2, dc, pair_owned_); dalloc(d_.d_val2, dc, pair_owned_);
         dalloc(d_.d_level, dc, pair_owned_);
         dalloc(d_.d_bod, dc, pair_owned_);
+        dalloc(d_.d_lbod, dc, pair_owned_);
+        dalloc(d_.isl_bod, 2 * size_t(dc) + 2, pair_owned_);
+        dalloc(d_.isl_nbod, size_t(dc) + 1, pair_owned_);
+        dalloc(d_.isl_mid, size_t(dc) / (kSmallIsland + 1) + 2, pair_owned_);
+        dalloc(d_.isl_big, size_t(dc) / (kMidIsland + 1) + 2, pair_owned_);
         dalloc(d_.isl_begin, size_t(dc) + 1, pair_owned_);
         dalloc(d_.isl_end, size_t(dc) + 1, pair_owned_);
         dalloc(d_.isl_flag, dc, pair_owned_);
@@ -965,6 +982,7 @@ private:
 
     int device_ = 0;
     cudaStream_t stream_ = nullptr;
+    Branches br_;
     std::vector<HostBody> bodies_;
     std::vector<HostShape> shapes_;
     std::vector<HostJoint> joints_;
