@@ -33,6 +33,7 @@ EXPORTS = (
     "fyzz_b200_read_pairs", "fyzz_b200_read_manifolds", "fyzz_b200_read_encoded_bounds",
     "fyzz_b200_read_sorted_min_x", "fyzz_b200_read_levels", "fyzz_b200_profile_step",
     "fyzz_b200_kernels_per_step", "fyzz_b200_sap_pairs_static_scratch",
+    "fyzz_b200_read_step_counters",
 )
 STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 
@@ -105,6 +106,7 @@ def lib():
         L.fyzz_b200_read_levels.restype = u64
         L.fyzz_b200_profile_step.argtypes = [vp, f32, vp, u32]
         L.fyzz_b200_kernels_per_step.argtypes = [vp, P(u32)]
+        L.fyzz_b200_read_step_counters.argtypes = [vp, vp, u32]
         L.fyzz_b200_sap_pairs_static_scratch.argtypes = [vp, vp, u32, vp, u32, vp, vp, C.c_char_p,
                                                          C.c_size_t]
         _lib = L
@@ -310,6 +312,14 @@ class World:
         out = np.zeros(n, np.uint32)
         lib().fyzz_b200_read_levels(self.h, _p(out), n)
         return out
+
+    def step_counters(self) -> dict:
+        """Device counters of the last step (see fyzz_b200_read_step_counters)."""
+        out = np.zeros(16, np.uint32)
+        self._check(lib().fyzz_b200_read_step_counters(self.h, _p(out), 16))
+        return {"managers": int(out[0]), "descriptors": int(out[1]), "gjk_pairs": int(out[5]),
+                "islands_32_512": int(out[8]), "islands_96_512": int(out[9]),
+                "islands_512_4096": int(out[10]), "islands_4096_up": int(out[11])}
 
     def error_bits(self) -> int:
         out = C.c_uint32()

@@ -113,43 +113,102 @@ __global__ void k_sweep_gather(DevState s, uint4* rec, uint2* meta) {
     meta[i] = make_uint2(hi.x, body | (dyn << 31));
 }
 
-__global__ void k_sweep(DevState s, const uint4* __restrict__ rec, const uint2* __restrict__ meta,
-                        int fill) {
-    const uint32_t stride = gridDim.x * blockDim.x;
-    uint64_t* keys = s.cur.key;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n_finite; i += stride) {
-        const uint32_t id = s.srt_id[i];
-        const uint32_t scene = s.s_scene[id];
-        const uint32_t end = s.sc_fbegin[scene + 1];
-        const uint4 a = rec[i];
-        const uint2 am = meta[i];
-        const uint32_t abody = am.y & 0x7fffffffu;
-        const bool adyn = (am.y >> 31) != 0u;
-        for (uint32_t j = i + 1; j < end; ++j) {
-            if (s.srt_key[j] > am.x) break;
-            const uint2 bm = meta[j];
-            const uint32_t bbody = bm.y & 0x7fffffffu;
-            if (bbody == abody) continue;
-            if (!adyn && (bm.y >> 31) == 0u) continue;
-            const uint4 b = rec[j];
-            if (a.x > b.y || b.x > a.y || a.z > b.w || b.z > a.w) continue;
-            const uint32_t other = s.srt_id[j];
-            const uint32_t owner = min(id, other), partner = max(id, other);
-            if (!fill) {
-                atomicAdd(&s.own_cnt[owner], 1u);
-            } else {
-                const uint32_t pos = s.own_off[owner] + s.s_static_pairs[owner] + atomicAdd(&s.own_cur[owner], 1u);
-                if (pos < s.pair_cap) keys[pos] = (uint64_t(owner) << 32) | partner;
-                else atomicOr(s.err, kErrPairCapacity);
+__device__ __forceinline__ void emit_pair(const DevState& s, uint32_t id, uint32_t other) {
+    const uint32_t owner = min(id, other), partner = max(id, other);
+    const uint32_t pos = s.own_off[owner] + s.s_static_pairs[owner] + atomicAdd(&s.own_cur[owner], 1u);
+    if (pos < s.pair_cap) s.cur.key[pos] = (uint64_t(owner) << 32) | partner;
+    else atomicOr(s.err, kErrPairCapacity);
+}
+
+// Warp-cooperative sweep.  Lane l owns sorted shape i = base + l; the warp
+// walks the candidates after base in chunks of 32 loaded once (coalesced)
+// into shared memory, and every lane tests its own shape against each
+// staged candidate (j > i, same scene, min x <= its max x, different body,
+// one dynamic, y/z overlap) until all lanes have passed their max x.
+// fill = 0: count each pair for its owner and keep up to kSweepCache
+// partners per shape.  fill = 1: write the kept partners into the owner
+// buckets; lanes that found more rescan (the warp walks again only if one
+// of its lanes needs it).
+constexpr int kSweepWarps = 8;
+struct SweepCand { uint32_t key, id, body, pad; uint4 yz; };
+
+__global__ void __launch_bounds__(kSweepWarps * 32) k_sweep(DevState s, const uint4* __restrict__ rec,
+                                                           const uint2* __restrict__ meta, int fill) {
+    constexpr uint32_t C = DevState::kSweepCache;
+    __shared__ SweepCand stage[kSweepWarps][32];
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    SweepCand* st = stage[wib];
+    const uint32_t nwarps = gridDim.x * kSweepWarps;
+    const uint32_t n = s.n_finite;
+    for (uint32_t base = (blockIdx.x * kSweepWarps + wib) * 32u; base < n; base += nwarps * 32u) {
+        const uint32_t i = base + lane;
+        const bool valid = i < n;
+        uint32_t id = 0, scene_end = 0, abody = 0;
+        uint2 am = make_uint2(0, 0);
+        uint4 a = make_uint4(0, 0, 0, 0);
+        bool adyn = false;
+        uint32_t nfound = 0;
+        if (valid) {
+            id = s.srt_id[i];
+            scene_end = s.sc_fbegin[s.s_scene[id] + 1];
+            am = meta[i];
+            a = rec[i];
+            abody = am.y & 0x7fffffffu;
+            adyn = (am.y >> 31) != 0u;
+        }
+        uint32_t* cache = s.sw_cache + size_t(i) * C;
+        bool scan = valid;
+        if (fill && valid) {
+            nfound = s.sw_found[i];
+            if (nfound <= C) {
+                for (uint32_t c = 0; c < nfound; ++c) emit_pair(s, id, cache[c]);
+                scan = false;
             }
         }
-        if (fill && adyn) {
-            const int32_t p = s.sc_plane[scene];
+        uint32_t found = 0;
+        bool active = scan;
+        for (uint32_t j0 = base + 1; __any_sync(0xffffffffu, active); j0 += 32) {
+            const uint32_t jl = j0 + lane;
+            if (jl < n) {
+                SweepCand c;
+                c.key = s.srt_key[jl];
+                c.id = s.srt_id[jl];
+                c.body = meta[jl].y;
+                c.pad = 0u;
+                c.yz = rec[jl];
+                st[lane] = c;
+            }
+            __syncwarp();
+            if (active) {
+                for (uint32_t t = 0; t < 32; ++t) {
+                    const uint32_t j = j0 + t;
+                    if (j >= scene_end || j >= n) { active = false; break; }
+                    if (j <= i) continue;
+                    const SweepCand& c = st[t];
+                    if (c.key > am.x) { active = false; break; }
+                    if ((c.body & 0x7fffffffu) == abody) continue;
+                    if (!adyn && (c.body >> 31) == 0u) continue;
+                    const uint4 b = c.yz;
+                    if (a.x > b.y || b.x > a.y || a.z > b.w || b.z > a.w) continue;
+                    if (!fill) {
+                        atomicAdd(&s.own_cnt[min(id, c.id)], 1u);
+                        if (found < C) cache[found] = c.id;
+                        ++found;
+                    } else {
+                        emit_pair(s, id, c.id);
+                    }
+                }
+            }
+            __syncwarp();
+        }
+        if (!fill && valid) s.sw_found[i] = found;
+        if (fill && valid && adyn) {
+            const int32_t p = s.sc_plane[s.s_scene[id]];
             if (p >= 0) {
                 const uint32_t pp = uint32_t(p);
                 const uint32_t pos = pp < id ? s.own_off[pp] + uint32_t(s.s_dynrank[id]) : s.own_off[id];
                 const uint32_t owner = min(pp, id), partner = max(pp, id);
-                if (pos < s.pair_cap) keys[pos] = (uint64_t(owner) << 32) | partner;
+                if (pos < s.pair_cap) s.cur.key[pos] = (uint64_t(owner) << 32) | partner;
                 else atomicOr(s.err, kErrPairCapacity);
             }
         }
@@ -229,11 +288,12 @@ void enqueue_broadphase(const DevState& s, cudaStream_t st, const StageHook& hoo
     }
     cudaMemcpyAsync(s.own_cnt, s.s_static_pairs, size_t(s.n_shapes) * 4, cudaMemcpyDeviceToDevice, st);
     cudaMemsetAsync(s.own_cur, 0, size_t(s.n_shapes) * 4, st);
-    const uint32_t sweep_blocks = s.n_finite ? (s.n_finite + T - 1) / T : 0;
-    if (sweep_blocks) k_sweep<<<sweep_blocks, T, 0, st>>>(s, rec, meta, 0);
+    const uint32_t sweep_threads = kSweepWarps * 32;
+    const uint32_t sweep_blocks = s.n_finite ? (s.n_finite + sweep_threads - 1) / sweep_threads : 0;
+    if (sweep_blocks) k_sweep<<<sweep_blocks, sweep_threads, 0, st>>>(s, rec, meta, 0);
     scan_exclusive(s.own_cnt, s.own_off, s.n_shapes, nullptr, s.cur.n, s.scan_tmp, s.scan_tmp_words, st);
     k_pair_total<<<1, 32, 0, st>>>(s);
-    if (sweep_blocks) k_sweep<<<sweep_blocks, T, 0, st>>>(s, rec, meta, 1);
+    if (sweep_blocks) k_sweep<<<sweep_blocks, sweep_threads, 0, st>>>(s, rec, meta, 1);
     k_owner_sort<<<(s.n_shapes + T - 1) / T, T, 0, st>>>(s);
     const uint32_t mb = (s.pair_cap + T - 1) / T;
     k_pair_match<<<mb < 1184 ? mb : 1184, T, 0, st>>>(s);

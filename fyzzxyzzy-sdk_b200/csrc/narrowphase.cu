@@ -1087,8 +1087,12 @@ __global__ void __launch_bounds__(128) k_narrowphase(DevState s) {
 }
 
 // Box/box pairs whose regenerated manifold had no face contact: GJK/EPA
-// witness and emission from the cache the first kernel left behind.
-__global__ void __launch_bounds__(64) k_narrowphase_gjk(DevState s) {
+// witness and emission from the cache the first kernel left behind.  These
+// are few (hundreds to a few thousand per step) and each is a long serial
+// search, so the kernel runs one warp per SM: every thread's polytope
+// working set then stays in that SM's L1 instead of spilling to L2.
+constexpr int kGjkThreads = 32;
+__global__ void __launch_bounds__(kGjkThreads) k_narrowphase_gjk(DevState s) {
     const uint32_t n = s.counters[kCntGjk];
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -1118,8 +1122,8 @@ void enqueue_narrowphase(const DevState& s, cudaStream_t st, const StageHook& ho
     cudaMemsetAsync(s.counters + kCntGjk, 0, 4, st);
     const uint32_t blocks = (s.pair_cap + T - 1) / T;
     k_narrowphase<<<blocks < 148u * 16u ? blocks : 148u * 16u, T, 0, st>>>(s);
-    const uint32_t gb = (s.pair_cap + 63) / 64;
-    k_narrowphase_gjk<<<gb < 148u * 4u ? gb : 148u * 4u, 64, 0, st>>>(s);
+    const uint32_t gb = (s.pair_cap + kGjkThreads - 1) / kGjkThreads;
+    k_narrowphase_gjk<<<gb < 148u ? gb : 148u, kGjkThreads, 0, st>>>(s);
 }
 
 }  // namespace fyzz::b200

@@ -31,6 +31,7 @@ namespace fyzz::b200 {
 namespace {
 constexpr uint32_t kInvalid = 0xffffffffu;
 constexpr int kMaxLevels = 256;
+constexpr uint32_t kSerialIsland = 32;   // partitioned by one thread
 
 __device__ __forceinline__ bool is_dyn(const DevState& s, uint32_t b) { return s.b_flags[b] & kBodyDynamic; }
 
@@ -214,6 +215,21 @@ __global__ void k_island_scatter(DevState s, const uint32_t* pos) {
     }
 }
 
+// Size classes of the islands (lists consumed by the partition and PGS
+// kernels of each class).
+__global__ void k_island_classes(DevState s) {
+    const uint32_t ni = *s.n_isl;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < ni; isl += stride) {
+        const uint32_t n = s.isl_begin[isl + 1] - s.isl_begin[isl];
+        auto push = [&](int c) { s.isl_list[c][atomicAdd(&s.counters[kCntList + c], 1u)] = isl; };
+        if (n > kSerialIsland && n <= kMidIsland) push(0);
+        if (n > kSmallIsland && n <= kMidIsland) push(1);
+        else if (n > kMidIsland && n <= kBigIsland) push(2);
+        else if (n > kBigIsland) push(3);
+    }
+}
+
 // Partitioning.  The reference assigns each dynamic/dynamic descriptor, in
 // order, the lowest partition bit free on both bodies (32-bit masks, overflow
 // waves), then gives each static descriptor the partition after its body's
@@ -227,7 +243,6 @@ __global__ void k_island_scatter(DevState s, const uint32_t* pos) {
 // masks the sequential loop would; all such descriptors share no body and are
 // decided together.  Each round decides at least the earliest undecided
 // descriptor of the island.  Waves and the static pass use the same rule.
-constexpr uint32_t kSerialIsland = 32;
 constexpr uint32_t kDeferred = 0xfffffffeu;
 
 // Island-local number of a body (0xffff for the static world), appending
@@ -263,11 +278,11 @@ __device__ void place_by_level(const DevState& s, uint32_t isl, uint32_t begin, 
 __global__ void __launch_bounds__(256) k_partition_large(DevState s, uint32_t* lvl_bound) {
     __shared__ uint32_t cursor[kMaxLevels + 1];
     __shared__ uint32_t nlev_s;
-    const uint32_t ni = *s.n_isl;
+    const uint32_t n_list = s.counters[kCntList + 3];
     const uint32_t tid = threadIdx.x, nt = blockDim.x;
-    for (uint32_t isl = blockIdx.x; isl < ni; isl += gridDim.x) {
+    for (uint32_t k = blockIdx.x; k < n_list; k += gridDim.x) {
+        const uint32_t isl = s.isl_list[3][k];
         const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
-        if (end - begin <= kBigIsland) continue;
         if (tid == 0) nlev_s = 0;
         uint32_t nlev = 0;
         bool ok = true;
@@ -516,18 +531,15 @@ __device__ __forceinline__ uint32_t find_local(const uint32_t* key, const uint32
     return 0xffffu;   // unreachable: every body was inserted
 }
 
-// Islands of (min_n, MAXN] descriptors: the rounds of k_partition_large on
+// Islands of one size class (at most MAXN descriptors): the rounds of k_partition_large on
 // island-local body slots in shared memory.  The island's dynamic bodies
 // are numbered through a shared-memory hash (open addressing), compacted to
 // 0..nb-1 (written to isl_bod for the solver), and the per-body partition
 // state lives in shared memory.  A round needs two passes: every undecided
 // descriptor offers its index to its bodies (atomicMin), then the ones that
-// won on both bodies are decided and clear their bodies' minimum.  Islands
-// larger than list_min are appended to list for the CTA solver.
+// won on both bodies are decided and clear their bodies' minimum.
 template <uint32_t MAXN>
-__global__ void __launch_bounds__(256) k_partition_smem(DevState s, uint32_t* lvl_bound, uint32_t min_n,
-                                                        uint32_t* list, uint32_t* list_n,
-                                                        uint32_t list_min) {
+__global__ void __launch_bounds__(256) k_partition_smem(DevState s, uint32_t* lvl_bound, int list_class) {
     constexpr uint32_t TMAX = PartSmem<MAXN>::kTable;
     extern __shared__ uint32_t sm[];
     uint32_t* key = sm;              // [T] hashed body ids
@@ -542,11 +554,12 @@ __global__ void __launch_bounds__(256) k_partition_smem(DevState s, uint32_t* lv
     __shared__ uint32_t warp_tot[32];
     __shared__ uint32_t nb_s, nlev_s;
     const uint32_t tid = threadIdx.x, nt = blockDim.x;
-    const uint32_t ni = *s.n_isl;
-    for (uint32_t isl = blockIdx.x; isl < ni; isl += gridDim.x) {
+    const uint32_t n_list = s.counters[kCntList + list_class];
+    const uint32_t* list = s.isl_list[list_class];
+    for (uint32_t k = blockIdx.x; k < n_list; k += gridDim.x) {
+        const uint32_t isl = list[k];
         const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
         const uint32_t n = end - begin;
-        if (n <= min_n || n > MAXN) continue;
         const uint32_t T = pow2_at_least(3 * (n + 1) / 2 + 1);
         uint32_t lg = 0;
         while ((1u << lg) < T) ++lg;
@@ -689,7 +702,6 @@ __global__ void __launch_bounds__(256) k_partition_smem(DevState s, uint32_t* lv
             bound[nlev] = end;
             s.isl_end[isl] = nlev;
             s.isl_nbod[isl] = nb;
-            if (n > list_min) list[atomicAdd(list_n, 1u)] = isl;
         }
         __syncthreads();
         for (uint32_t i = tid; i < n; i += nt) {
@@ -1046,15 +1058,25 @@ __device__ void solve_desc(const DevState& s, uint32_t d, uint32_t lid, int it, 
     const float4* fq = reinterpret_cast<const float4*>(s.frow + 4 * size_t(m));
     float4 n0[4], n1[4], n2[4], n3[4], f0[4], f1[4], f2[4];
     float fa[4];
+    if constexpr (kEagerFriction) {
+        // All four row slots of the manager are read without waiting for
+        // the header (unused slots are never consumed), so the row loads and
+        // the header load are in flight together.
+        const bool friction_pass = it >= pos || pos - it <= 3;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        if (uint32_t(j) < hd.count) {
+        for (int j = 0; j < 4; ++j) {
             n0[j] = nr[4 * j]; n1[j] = nr[4 * j + 1]; n2[j] = nr[4 * j + 2]; n3[j] = nr[4 * j + 3];
+            if (friction_pass) {
+                f0[j] = fq[4 * j]; f1[j] = fq[4 * j + 1]; f2[j] = fq[4 * j + 2];
+                fa[j] = reinterpret_cast<const float*>(fq + 4 * j + 3)[0];
+            }
         }
-        if (kEagerFriction && friction && uint32_t(j) < 2 * hd.anchors) {
-            f0[j] = fq[4 * j]; f1[j] = fq[4 * j + 1]; f2[j] = fq[4 * j + 2];
-            fa[j] = reinterpret_cast<const float*>(fq + 4 * j + 3)[0];
-        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (uint32_t(j) < hd.count) {
+                n0[j] = nr[4 * j]; n1[j] = nr[4 * j + 1]; n2[j] = nr[4 * j + 2]; n3[j] = nr[4 * j + 3];
+            }
     }
     int32_t h0, h1;
     if constexpr (D::kLocal) {
@@ -1197,16 +1219,17 @@ __global__ void __launch_bounds__(kPgsWarpsPerBlock * 32, 3) k_pgs_warp(DevState
     }
 }
 
-// One CTA per island of (kSmallIsland, MAXN] descriptors from list, with
-// the island's deltas in shared memory (2 x (MAXN + 1) float4).
-template <uint32_t MAXN>
-__global__ void __launch_bounds__(256) k_pgs_block_smem(DevState s, const uint32_t* lvl_bound,
-                                                        const uint32_t* list, const uint32_t* list_n) {
+// One CTA of NT threads per island of a size class (at most MAXN
+// descriptors), with the island's deltas in shared memory
+// (2 x (MAXN + 1) float4).
+template <uint32_t MAXN, uint32_t NT>
+__global__ void __launch_bounds__(NT) k_pgs_block_smem(DevState s, const uint32_t* lvl_bound, int list_class) {
     extern __shared__ float4 shb[];
     float4* sdv = shb;
     float4* sdw = shb + (MAXN + 1);
     const LocalDeltas D{sdv, sdw};
-    const uint32_t n_list = *list_n;
+    const uint32_t n_list = s.counters[kCntList + list_class];
+    const uint32_t* list = s.isl_list[list_class];
     const int pos = s.pos_iters, vel = s.vel_iters < 1 ? 1 : s.vel_iters;
     const float4 zero = make_float4(0, 0, 0, 0);
     for (uint32_t k = blockIdx.x; k < n_list; k += gridDim.x) {
@@ -1237,12 +1260,12 @@ __global__ void __launch_bounds__(256) k_pgs_block_smem(DevState s, const uint32
 
 // One CTA per island beyond kBigIsland descriptors: deltas in global memory.
 __global__ void __launch_bounds__(256) k_pgs_block(DevState s, const uint32_t* lvl_bound) {
-    const uint32_t ni = *s.n_isl;
+    const uint32_t n_list = s.counters[kCntList + 3];
     const int pos = s.pos_iters, vel = s.vel_iters < 1 ? 1 : s.vel_iters;
     const GlobalDeltas D{s};
-    for (uint32_t isl = blockIdx.x; isl < ni; isl += gridDim.x) {
+    for (uint32_t k = blockIdx.x; k < n_list; k += gridDim.x) {
+        const uint32_t isl = s.isl_list[3][k];
         const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
-        if (end - begin <= kBigIsland) continue;
         const uint32_t nlev = s.isl_end[isl];
         const uint32_t* bound = lvl_bound + begin + isl;
         for (int it = 0; it < pos + vel; ++it) {
@@ -1337,7 +1360,7 @@ static void join_branches(const Branches* br, cudaStream_t st, int n) {
 void init_solver_kernels() {
     cudaFuncSetAttribute(k_partition_smem<kBigIsland>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          int(PartSmem<kBigIsland>::kBytes));
-    cudaFuncSetAttribute(k_pgs_block_smem<kBigIsland>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_pgs_block_smem<kBigIsland, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          int(2 * (kBigIsland + 1) * sizeof(float4)));
 }
 
@@ -1366,17 +1389,16 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     k_island_flags<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     scan_exclusive(s.isl_flag, pos, s.desc_cap, s.counters + kCntDesc, s.n_isl, s.scan_tmp, s.scan_tmp_words, st);
     k_island_scatter<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s, pos);
-    cudaMemsetAsync(s.counters + kCntMid, 0, 2 * sizeof(uint32_t), st);
+    cudaMemsetAsync(s.counters + kCntList, 0, 4 * sizeof(uint32_t), st);
+    k_island_classes<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     // partitions by island size class, and row preparation: independent
     hook(kStPrep, st);
     fork_branches(br, st, 3);
     k_partition<<<grid_for(s.desc_cap, 128, cap_blocks), 128, 0, st>>>(s, lvl_bound);
     k_partition_smem<kMidIsland><<<grid_for(s.desc_cap, kSerialIsland + 1, 148u * 8u), 256,
-                                   PartSmem<kMidIsland>::kBytes, side(0)>>>(
-        s, lvl_bound, kSerialIsland, s.isl_mid, s.counters + kCntMid, kSmallIsland);
+                                   PartSmem<kMidIsland>::kBytes, side(0)>>>(s, lvl_bound, 0);
     k_partition_smem<kBigIsland><<<grid_for(s.desc_cap, kMidIsland + 1, 148u * 2u), 256,
-                                   PartSmem<kBigIsland>::kBytes, side(1)>>>(
-        s, lvl_bound, kMidIsland, s.isl_big, s.counters + kCntBig, kMidIsland);
+                                   PartSmem<kBigIsland>::kBytes, side(1)>>>(s, lvl_bound, 2);
     k_partition_large<<<grid_for(s.desc_cap, kBigIsland + 1, 148u), 256, 0, side(1)>>>(s, lvl_bound);
     if (s.n_joints) k_prep_joints<<<grid_for(s.n_joints, T, 1u << 30), T, 0, side(2)>>>(s);
     k_prep_contacts<<<grid_for(s.desc_cap, 128, cap_blocks), 128, 0, side(2)>>>(s);
@@ -1386,12 +1408,10 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     fork_branches(br, st, 2);
     k_pgs_warp<<<grid_for(s.desc_cap * 32u, kPgsWarpsPerBlock * 32u, 148u * 3u), kPgsWarpsPerBlock * 32u, 0, st>>>(
         s, lvl_bound);
-    k_pgs_block_smem<kMidIsland><<<grid_for(s.desc_cap, kSmallIsland + 1, 148u * 4u), 256,
-                                   2 * (kMidIsland + 1) * sizeof(float4), side(0)>>>(
-        s, lvl_bound, s.isl_mid, s.counters + kCntMid);
-    k_pgs_block_smem<kBigIsland><<<grid_for(s.desc_cap, kMidIsland + 1, 148u), 256,
-                                   2 * (kBigIsland + 1) * sizeof(float4), side(1)>>>(
-        s, lvl_bound, s.isl_big, s.counters + kCntBig);
+    k_pgs_block_smem<kMidIsland, 128><<<grid_for(s.desc_cap, kSmallIsland + 1, 148u * 3u), 128,
+                                        2 * (kMidIsland + 1) * sizeof(float4), side(0)>>>(s, lvl_bound, 1);
+    k_pgs_block_smem<kBigIsland, 256><<<grid_for(s.desc_cap, kMidIsland + 1, 148u), 256,
+                                        2 * (kBigIsland + 1) * sizeof(float4), side(1)>>>(s, lvl_bound, 2);
     k_pgs_block<<<grid_for(s.desc_cap, kBigIsland + 1, 148u), 256, 0, side(1)>>>(s, lvl_bound);
     join_branches(br, st, 2);
     hook(kStIntegrate, st);

@@ -107,12 +107,20 @@ struct DevState {
     uint32_t* d_lbod = nullptr;        // per placed descriptor: local a | local b << 16 (0xffff static)
     int32_t* isl_bod = nullptr;        // island isl's bodies at [isl_begin + isl, + isl_nbod)
     uint32_t* isl_nbod = nullptr;      // per island
-    uint32_t* isl_mid = nullptr;       // islands solved by one CTA with shared-memory deltas
-    uint32_t* isl_big = nullptr;
+    // Islands by size class (descriptors), listed each step by
+    // k_island_classes: 0 (32, 512] shared-memory partition, 1 (96, 512]
+    // CTA solver, 2 (512, 4096] both, 3 beyond 4096 global-memory paths.
+    uint32_t* isl_list[4] = {};
 
     // step scratch
     uint4* sw_rec = nullptr;           // sweep y/z bounds in sorted order
     uint2* sw_meta = nullptr;          // sweep max x and body | dynamic bit
+    // Partners found by the counting sweep (kSweepCache per sorted shape) and
+    // how many each shape found; the filling sweep reuses them instead of
+    // scanning the candidates again (it rescans only shapes that overflowed).
+    uint32_t* sw_cache = nullptr;
+    uint32_t* sw_found = nullptr;
+    static constexpr uint32_t kSweepCache = 16;
     uint32_t* tmp_flags = nullptr;     // pair_cap
     uint32_t* tmp_pos = nullptr;       // max(pair_cap, desc_cap)
     uint32_t* lvl_bound = nullptr;     // 2 * desc_cap + 2: per-island partition starts
@@ -175,6 +183,6 @@ constexpr uint32_t kMidIsland = 512;      // one CTA, shared-memory deltas
 constexpr uint32_t kBigIsland = 4096;     // one CTA, shared-memory deltas (1 CTA / SM)
 // counters[] slots
 enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels = 4, kCntGjk = 5,
-             kCntMid = 6, kCntBig = 7, kCntSlots = 8 };
+             kCntList = 8 /* 4 island-class list lengths */, kCntSlots = 16 };
 
 }  // namespace fyzz::b200

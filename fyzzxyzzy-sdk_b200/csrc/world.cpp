@@ -671,6 +671,12 @@ public:
             check_cuda(cudaMemcpy(levels, d_.d_level, std::min<uint64_t>(c.desc, cap) * 4, cudaMemcpyDeviceToHost), "read");
         return c.desc;
     }
+    void read_step_counters(uint32_t* out, uint32_t n) {
+        if (n > uint32_t(kCntSlots)) throw std::invalid_argument("At most 16 counters");
+        if (!uploaded_) { for (uint32_t i = 0; i < n; ++i) out[i] = 0; return; }
+        check_cuda(cudaStreamSynchronize(stream_), "sync");
+        check_cuda(cudaMemcpy(out, d_.counters, size_t(n) * 4, cudaMemcpyDeviceToHost), "read");
+    }
     uint32_t error_bits() const { return last_err_; }
     uint32_t last_shape() const { return uint32_t(shapes_.size() - 1); }
     size_t n_bodies() const { return bodies_.size(); }
@@ -804,8 +810,10 @@ private:
         dalloc(d_.d_lbod, dc, pair_owned_);
         dalloc(d_.isl_bod, 2 * size_t(dc) + 2, pair_owned_);
         dalloc(d_.isl_nbod, size_t(dc) + 1, pair_owned_);
-        dalloc(d_.isl_mid, size_t(dc) / (kSmallIsland + 1) + 2, pair_owned_);
-        dalloc(d_.isl_big, size_t(dc) / (kMidIsland + 1) + 2, pair_owned_);
+        dalloc(d_.isl_list[0], size_t(dc) / 33 + 2, pair_owned_);
+        dalloc(d_.isl_list[1], size_t(dc) / (kSmallIsland + 1) + 2, pair_owned_);
+        dalloc(d_.isl_list[2], size_t(dc) / (kMidIsland + 1) + 2, pair_owned_);
+        dalloc(d_.isl_list[3], size_t(dc) / (kBigIsland + 1) + 2, pair_owned_);
         dalloc(d_.isl_begin, size_t(dc) + 1, pair_owned_);
         dalloc(d_.isl_end, size_t(dc) + 1, pair_owned_);
         dalloc(d_.isl_flag, dc, pair_owned_);
@@ -919,6 +927,8 @@ private:
         dalloc(d_.srt_key, nf, owned_); dalloc(d_.srt_id, nf, owned_);
         dalloc(d_.srt_key2, nf, owned_); dalloc(d_.srt_id2, nf, owned_);
         dalloc(d_.sw_rec, nf, owned_); dalloc(d_.sw_meta, nf, owned_);
+        dalloc(d_.sw_cache, size_t(nf) * DevState::kSweepCache, owned_);
+        dalloc(d_.sw_found, nf, owned_);
         dalloc(d_.own_cnt, ns, owned_); dalloc(d_.own_off, ns, owned_); dalloc(d_.own_cur, ns, owned_);
         dalloc(d_.j_a, joints_.size(), owned_); dalloc(d_.j_b, joints_.size(), owned_);
         dalloc(d_.j_len, joints_.size(), owned_); dalloc(d_.jrow, joints_.size(), owned_);
@@ -1224,6 +1234,10 @@ uint64_t fyzz_b200_read_sorted_min_x(fyzz_b200_world* w, uint32_t scene, uint32_
     uint64_t n = 0;
     if (guarded(w, [&](auto& W) { n = W.read_sorted_min_x(scene, values, ids, cap); })) return 0;
     return n;
+}
+int fyzz_b200_read_step_counters(fyzz_b200_world* w, uint32_t* out, uint32_t n) {
+    if (!out) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) { W.read_step_counters(out, n); });
 }
 uint64_t fyzz_b200_read_levels(fyzz_b200_world* w, uint32_t* levels, uint64_t cap) {
     uint64_t n = 0;

@@ -125,8 +125,9 @@ int fyzz_b200_collide(fyzz_b200_world* w);
 int fyzz_b200_synchronize(fyzz_b200_world* w);
 /* One step launched without the graph, with CUDA events on the world's
  * stream at each stage boundary.  stage_ms receives up to n stage times:
- * 0 bounds, 1 endpoint sort, 2 pairs, 3 narrowphase, 4 islands+partitions,
- * 5 row preparation, 6 PGS, 7 integration.  (Counterpart of the reference's
+ * 0 bounds, 1 endpoint sort, 2 pairs, 3 narrowphase, 4 islands,
+ * 5 partitions and row preparation (concurrent graph branches), 6 PGS,
+ * 7 integration.  (Counterpart of the reference's
  * Context::profile_batch_gpu_nanoseconds, compute.h:299.) */
 int fyzz_b200_profile_step(fyzz_b200_world* w, float seconds, float* stage_ms, uint32_t n);
 /* Kernel launches in one captured step graph (0 before the first step). */
@@ -164,6 +165,10 @@ uint64_t fyzz_b200_read_sorted_min_x(fyzz_b200_world* w, uint32_t scene, uint32_
 /* Partition level of every descriptor of the last step, in canonical
  * descriptor order (joints then touching managers). */
 uint64_t fyzz_b200_read_levels(fyzz_b200_world* w, uint32_t* levels, uint64_t cap);
+/* Device counters of the last step, n <= 16: 0 touching managers,
+ * 1 descriptors, 5 box pairs finished by GJK/EPA, 8-11 islands per size
+ * class ((32,512], (96,512], (512,4096], >4096 descriptors). */
+int fyzz_b200_read_step_counters(fyzz_b200_world* w, uint32_t* out, uint32_t n);
 
 /* ---- allocation-free sweep-and-prune (no counterpart in the reference) ----
  * The overlap-pair set of one scene's finite shapes, computed on the device
