@@ -481,124 +481,184 @@ __device__ bool contact_from_facet(const BPair& p, const Sup* vtx, const Facet& 
     out = {bp_local_a(p, pa), pb, vneg(f.normal), -depth};
     return sqrtf(vlen2(vsub(pa, pb))) <= depth + 1.0e-3f;
 }
-__device__ bool run_epa(const BPair& p, const Sup* simplex, int sc, Cand& out) {
-    Sup vtx[64];
-    int vc = sc;
-    for (int i = 0; i < sc; ++i) vtx[i] = simplex[i];
-    Facet facets[64];
-    int fc = 0;
-    if (!init_epa(p, vtx, vc, facets, fc)) return false;
-    const float eps = 0.1f * smin(box_min_margin(p.ha), box_min_margin(p.hb));
-    int bfrom[32], bto[32];
-    float upper = FLT_MAX;
-    for (int it = 0; it < 60; ++it) {
-        int closest = -1;
-        float dist = FLT_MAX;
-        for (int i = 0; i < fc; ++i)
-            if (facets[i].valid && facets[i].in_heap && facets[i].distance < dist) {
-                closest = i;
-                dist = facets[i].distance;
-            }
-        if (closest < 0) return false;
-        const Facet sel = facets[closest];
-        const Sup np = bp_support(p, sel.normal);
-        const float proj = vdot(np.q, sel.normal);
-        if (fabsf(proj - dist) <= eps) return contact_from_facet(p, vtx, sel, out);
-        if (vc == 64) return false;
-        upper = smin(upper, proj);
-        for (int i = 0; i < vc; ++i)
-            if (vtx[i].ai == np.ai && vtx[i].bi == np.bi) return contact_from_facet(p, vtx, sel, out);
-        const int ni = vc++;
-        vtx[ni] = np;
-        int bc = 0;
-        for (int i = 0; i < fc; ++i) {
-            Facet& f = facets[i];
-            if (!f.valid) continue;
-            if (vdot(f.normal, vsub(np.q, vtx[f.i].q)) < 0.0f) continue;
-            f.valid = false;
-            const int ef[3] = {f.i, f.j, f.k}, et[3] = {f.j, f.k, f.i};
-            for (int e = 0; e < 3; ++e) {
-                int rev = -1;
-                for (int j = 0; j < bc; ++j)
-                    if (bfrom[j] == et[e] && bto[j] == ef[e]) { rev = j; break; }
-                if (rev >= 0) {
-                    --bc;
-                    bfrom[rev] = bfrom[bc];
-                    bto[rev] = bto[bc];
-                } else {
-                    if (bc == 32) return false;
-                    bfrom[bc] = ef[e];
-                    bto[bc] = et[e];
-                    ++bc;
-                }
-            }
-        }
-        if (bc == 0) return false;
-        int avail = 64 - fc;
-        for (int i = 0; i < fc; ++i) avail += !facets[i].valid;
-        if (bc > avail) return false;
-        for (int i = 0; i < bc; ++i) {
-            Facet f = make_facet(vtx, bfrom[i], bto[i], ni);
-            if (!f.valid) return false;
-            f.in_heap = f.distance <= upper;
-            int slot = -1;
-            for (int j = 0; j < fc; ++j)
-                if (!facets[j].valid) { slot = j; break; }
-            if (slot < 0) slot = fc++;
-            facets[slot] = f;
-        }
-    }
-    return false;
-}
-__device__ bool gjk_epa(const BPair& p, float cd, Cand& out) {
+// GJK (GuPCMGjkEpa.cpp) up to the point where EPA starts: returns 0 (no
+// witness), 1 (witness in out) or 2 (EPA needed from simplex[0, sc)).
+__device__ int gjk_phase(const BPair& p, float cd, Cand& out, Sup* simplex, int& count) {
     const float eps = 0.1f * smin(box_min_margin(p.ha), box_min_margin(p.hb));
     const float progress = 1.0f - 0.000225f;
-    Sup simplex[4];
-    int count = 0;
+    count = 0;
     v3 closest = vlen2(p.a_in_b) > 0.0f ? p.a_in_b : v3{1, 0, 0};
     float previous = FLT_MAX;
     for (int it = 0; it < 32; ++it) {
         const float dist = sqrtf(vlen2(closest));
-        if (count > 0 && dist <= eps) return run_epa(p, simplex, count, out);
-        if (dist <= 0.0f) return false;
+        if (count > 0 && dist <= eps) return 2;
+        if (dist <= 0.0f) return 0;
         const v3 normal = vmul(closest, 1.0f / dist);
         const Sup s = bp_support(p, vneg(closest));
         const float proj = vdot(normal, s.q);
-        if (proj > cd) return false;
+        if (proj > cd) return 0;
         if (count > 0 && proj > dist * progress) {
             const Closest cur = closest_simplex(simplex, count);
-            return cur.mask && contact_from_gjk(p, cur, out);
+            return cur.mask && contact_from_gjk(p, cur, out) ? 1 : 0;
         }
         for (int i = 0; i < count; ++i)
             if (s.ai == simplex[i].ai && s.bi == simplex[i].bi) {
                 if (proj > 0.f) {
                     const Closest cur = closest_simplex(simplex, count);
-                    return cur.mask && contact_from_gjk(p, cur, out) && out.sep <= cd;
+                    return cur.mask && contact_from_gjk(p, cur, out) && out.sep <= cd ? 1 : 0;
                 }
-                return false;
+                return 0;
             }
-        if (count == 4) return run_epa(p, simplex, count, out);
+        if (count == 4) return 2;
         simplex[count++] = s;
         const Closest nx = closest_simplex(simplex, count);
-        if (!nx.mask) return false;
+        if (!nx.mask) return 0;
         closest = nx.point;
         const float nd = sqrtf(nx.dist2);
         compact_simplex(simplex, count, nx);
-        if (nd >= previous) return false;
+        if (nd >= previous) return 0;
         previous = nd;
+    }
+    return 0;
+}
+
+// EPA (GuPCMGjkEpa.cpp) with one warp: the polytope lives in shared memory; the closest
+// facet search, the duplicate-vertex test, the visibility marking, the free
+// slot count and the new facets are spread over the lanes, while the
+// horizon walk (whose order decides where new facets land) stays on lane 0
+// and visits the visible facets in index order, as the sequential search does.  Every
+// lane returns the same result; out is valid on every lane.
+struct EpaShared {
+    Sup vtx[64];
+    Facet facets[64];
+    int bfrom[32], bto[32];
+    int bc;
+    int status;
+};
+__device__ bool run_epa_warp(const BPair& p, const Sup* simplex, int sc, Cand& out, EpaShared& E) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t full = 0xffffffffu;
+    if (lane == 0) {
+        int vc0 = sc;
+        for (int i = 0; i < sc; ++i) E.vtx[i] = simplex[i];
+        int fc0 = 0;
+        E.status = init_epa(p, E.vtx, vc0, E.facets, fc0) ? fc0 : -1;
+        E.bc = vc0;
+    }
+    __syncwarp();
+    if (E.status < 0) return false;
+    int fc = E.status, vc = E.bc;
+    __syncwarp();
+    const float eps = 0.1f * smin(box_min_margin(p.ha), box_min_margin(p.hb));
+    float upper = FLT_MAX;
+    for (int it = 0; it < 60; ++it) {
+        // closest facet: smallest distance, lowest index on ties
+        float dist = FLT_MAX;
+        int closest = -1;
+        for (int i = int(lane); i < fc; i += 32) {
+            const Facet& f = E.facets[i];
+            if (f.valid && f.in_heap && f.distance < dist) { dist = f.distance; closest = i; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const float od = __shfl_xor_sync(full, dist, o);
+            const int oc = __shfl_xor_sync(full, closest, o);
+            if (oc >= 0 && (closest < 0 || od < dist || (od == dist && oc < closest))) { dist = od; closest = oc; }
+        }
+        if (closest < 0) return false;
+        const Facet sel = E.facets[closest];
+        const Sup np = bp_support(p, sel.normal);
+        const float proj = vdot(np.q, sel.normal);
+        if (fabsf(proj - dist) <= eps) return contact_from_facet(p, E.vtx, sel, out);
+        if (vc == 64) return false;
+        upper = smin(upper, proj);
+        bool dup = false;
+        for (int i = int(lane); i < vc; i += 32) dup |= E.vtx[i].ai == np.ai && E.vtx[i].bi == np.bi;
+        if (__any_sync(full, dup)) return contact_from_facet(p, E.vtx, sel, out);
+        const int ni = vc++;
+        // visibility (independent per facet)
+        bool vis0 = false, vis1 = false;
+        for (int r = 0; r < 2; ++r) {
+            const int i = int(lane) + 32 * r;
+            bool vis = false;
+            if (i < fc) {
+                const Facet& f = E.facets[i];
+                vis = f.valid && !(vdot(f.normal, vsub(np.q, E.vtx[f.i].q)) < 0.0f);
+            }
+            (r ? vis1 : vis0) = vis;
+        }
+        const uint32_t vmask0 = __ballot_sync(full, vis0), vmask1 = __ballot_sync(full, vis1);
+        __syncwarp();
+        if (lane == 0) {
+            E.vtx[ni] = np;
+            // horizon edges in the order the sequential search finds them
+            int bc = 0;
+            bool fail = false;
+            for (int r = 0; r < 2 && !fail; ++r) {
+                uint32_t m = r ? vmask1 : vmask0;
+                while (m && !fail) {
+                    const int i = __ffs(m) - 1 + 32 * r;
+                    m &= m - 1;
+                    Facet& f = E.facets[i];
+                    f.valid = false;
+                    const int ef[3] = {f.i, f.j, f.k}, et[3] = {f.j, f.k, f.i};
+                    for (int e = 0; e < 3; ++e) {
+                        int rev = -1;
+                        for (int j = 0; j < bc; ++j)
+                            if (E.bfrom[j] == et[e] && E.bto[j] == ef[e]) { rev = j; break; }
+                        if (rev >= 0) {
+                            --bc;
+                            E.bfrom[rev] = E.bfrom[bc];
+                            E.bto[rev] = E.bto[bc];
+                        } else {
+                            if (bc == 32) { fail = true; break; }
+                            E.bfrom[bc] = ef[e];
+                            E.bto[bc] = et[e];
+                            ++bc;
+                        }
+                    }
+                }
+            }
+            E.bc = fail ? -1 : bc;
+        }
+        __syncwarp();
+        const int bc = E.bc;
+        if (bc <= 0) return false;
+        // free slots among [0, fc): invalid facets, in index order
+        bool inv0 = int(lane) < fc && !E.facets[lane].valid;
+        bool inv1 = int(lane) + 32 < fc && !E.facets[lane + 32].valid;
+        const uint32_t fmask0 = __ballot_sync(full, inv0), fmask1 = __ballot_sync(full, inv1);
+        const int nfree = __popc(fmask0) + __popc(fmask1);
+        if (bc > 64 - fc + nfree) return false;
+        // new facet for horizon edge `lane`, placed in the lane-th free slot
+        Facet nf;
+        bool ok = true;
+        int slot = -1;
+        if (int(lane) < bc) {
+            nf = make_facet(E.vtx, E.bfrom[lane], E.bto[lane], ni);
+            ok = nf.valid;
+            nf.in_heap = nf.distance <= upper;
+            const int k = int(lane);
+            if (k < __popc(fmask0)) {
+                uint32_t m = fmask0;
+                for (int t = 0; t < k; ++t) m &= m - 1;
+                slot = __ffs(m) - 1;
+            } else if (k < nfree) {
+                uint32_t m = fmask1;
+                for (int t = __popc(fmask0); t < k; ++t) m &= m - 1;
+                slot = 32 + __ffs(m) - 1;
+            } else {
+                slot = fc + (k - nfree);
+            }
+        }
+        if (!__all_sync(full, ok)) return false;
+        __syncwarp();
+        if (int(lane) < bc) E.facets[slot] = nf;
+        fc = bc > nfree ? fc + (bc - nfree) : fc;
+        __syncwarp();
     }
     return false;
 }
-__device__ bool box_box_gjk_epa(v3 h0, v3 p0, qt q0, v3 h1, v3 p1, qt q1, float cd, Cand& out) {
-    BPair p;
-    p.ha = h0;
-    p.hb = h1;
-    p.a_in_b = rotinv_gu(q1, vsub(p0, p1));
-    p.rel = qmul(qconj(q1), q0);
-    out = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0.0f};
-    if (!gjk_epa(p, cd, out)) return false;
-    return out.sep <= cd;
-}
+
 
 // ---------------- persistent manifolds ----------------
 __device__ __forceinline__ v3 lv(const float* f) { return {f[0], f[1], f[2]}; }
@@ -790,11 +850,10 @@ __device__ int generate_box_box(v3 h0, v3 p0, qt q0, v3 h1, v3 p1, qt q1, float 
 
 // Second half of the zero-face case (scene.cpp:3545-3590): GJK/EPA witness,
 // replacement or append into the refreshed cache, then emission.
-__device__ int finish_box_box_gjk(v3 h0, v3 p0, qt q0, v3 h1, v3 p1, qt q1, float cd, PcmCache& cache,
-                                  ContactPt* out) {
+__device__ int finish_box_box_gjk(v3 h0, v3 h1, v3 p1, qt q1, float cd, PcmCache& cache, bool have,
+                                  const Cand& w, ContactPt* out) {
     const float mm = smin(pcm_box_margin(h0), pcm_box_margin(h1));
-    Cand w;
-    if (!box_box_gjk_epa(h0, p0, q0, h1, p1, q1, cd, w)) {
+    if (!have) {
         set_meta(cache, 0, true);
         return 0;
     }
@@ -1088,29 +1147,53 @@ __global__ void __launch_bounds__(128) k_narrowphase(DevState s) {
 
 // Box/box pairs whose regenerated manifold had no face contact: GJK/EPA
 // witness and emission from the cache the first kernel left behind.  These
-// are few (hundreds to a few thousand per step) and each is a long serial
-// search, so the kernel runs one warp per SM: every thread's polytope
-// working set then stays in that SM's L1 instead of spilling to L2.
-constexpr int kGjkThreads = 32;
-__global__ void __launch_bounds__(kGjkThreads) k_narrowphase_gjk(DevState s) {
+// are few (hundreds to a few thousand per step) and each is a long search,
+// so one warp takes a pair: lane 0 runs GJK, the warp runs EPA together
+// (run_epa_warp) with the polytope in shared memory.
+constexpr int kGjkWarps = 4;
+__global__ void __launch_bounds__(kGjkWarps * 32, 1) k_narrowphase_gjk(DevState s) {
+    __shared__ EpaShared epa[kGjkWarps];
+    __shared__ Sup simplex_s[kGjkWarps][4];
+    __shared__ int mode_s[kGjkWarps], sc_s[kGjkWarps];
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     const uint32_t n = s.counters[kCntGjk];
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t nwarps = gridDim.x * kGjkWarps;
+    for (uint32_t i = blockIdx.x * kGjkWarps + wib; i < n; i += nwarps) {
         const uint32_t k = s.gjk_list[i];
         const PairShapes ps = pair_shapes(s, s.cur.key[k]);
-        PcmCache cache = s.cur.cache[k];
         const float4 g0 = s.s_geom[ps.first], g1 = s.s_geom[ps.second];
-        ContactPt out[4];
-        int count = finish_box_box_gjk({g0.x, g0.y, g0.z}, ld3(s.s_wp[ps.first]), ldq(s.s_wq[ps.first]),
-                                       {g1.x, g1.y, g1.z}, ld3(s.s_wp[ps.second]), ldq(s.s_wq[ps.second]),
-                                       ps.cd, cache, out);
-        if (count < 0) {
-            atomicOr(s.err, kErrContactOverflow);
-            count = 0;
+        const v3 h0 = {g0.x, g0.y, g0.z}, h1 = {g1.x, g1.y, g1.z};
+        const v3 p0 = ld3(s.s_wp[ps.first]), p1 = ld3(s.s_wp[ps.second]);
+        const qt q0 = ldq(s.s_wq[ps.first]), q1 = ldq(s.s_wq[ps.second]);
+        BPair bp;
+        bp.ha = h0;
+        bp.hb = h1;
+        bp.a_in_b = rotinv_gu(q1, vsub(p0, p1));
+        bp.rel = qmul(qconj(q1), q0);
+        Cand w = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0.0f};
+        if (lane == 0) {
+            int sc = 0;
+            mode_s[wib] = gjk_phase(bp, ps.cd, w, simplex_s[wib], sc);
+            sc_s[wib] = sc;
         }
-        s.cur.cache[k] = cache;
-        s.cur.count[k] = uint32_t(count);
-        for (int j = 0; j < count; ++j) s.pts[4 * size_t(k) + j] = out[j];
+        __syncwarp();
+        const int mode = mode_s[wib];
+        bool have = mode == 1;
+        if (mode == 2) have = run_epa_warp(bp, simplex_s[wib], sc_s[wib], w, epa[wib]);
+        if (lane == 0) {
+            have = have && w.sep <= ps.cd;
+            PcmCache cache = s.cur.cache[k];
+            ContactPt out[4];
+            int count = finish_box_box_gjk(h0, h1, p1, q1, ps.cd, cache, have, w, out);
+            if (count < 0) {
+                atomicOr(s.err, kErrContactOverflow);
+                count = 0;
+            }
+            s.cur.cache[k] = cache;
+            s.cur.count[k] = uint32_t(count);
+            for (int j = 0; j < count; ++j) s.pts[4 * size_t(k) + j] = out[j];
+        }
+        __syncwarp();
     }
 }
 
@@ -1122,8 +1205,8 @@ void enqueue_narrowphase(const DevState& s, cudaStream_t st, const StageHook& ho
     cudaMemsetAsync(s.counters + kCntGjk, 0, 4, st);
     const uint32_t blocks = (s.pair_cap + T - 1) / T;
     k_narrowphase<<<blocks < 148u * 16u ? blocks : 148u * 16u, T, 0, st>>>(s);
-    const uint32_t gb = (s.pair_cap + kGjkThreads - 1) / kGjkThreads;
-    k_narrowphase_gjk<<<gb < 148u ? gb : 148u, kGjkThreads, 0, st>>>(s);
+    const uint32_t gb = (s.pair_cap + kGjkWarps - 1) / kGjkWarps;
+    k_narrowphase_gjk<<<gb < 148u * 8u ? gb : 148u * 8u, kGjkWarps * 32, 0, st>>>(s);
 }
 
 }  // namespace fyzz::b200

@@ -1183,6 +1183,8 @@ constexpr uint32_t kWarpBodies = kSmallIsland + 1;
 constexpr uint32_t kPgsWarpsPerBlock = 4;
 __global__ void __launch_bounds__(kPgsWarpsPerBlock * 32, 3) k_pgs_warp(DevState s, const uint32_t* lvl_bound) {
     __shared__ float4 sh[kPgsWarpsPerBlock][2][kWarpBodies];
+    __shared__ uint32_t sdesc[kPgsWarpsPerBlock][2][kSmallIsland];   // descriptor, local bodies per slot
+    __shared__ uint32_t sbound[kPgsWarpsPerBlock][kSmallIsland + 1];
     const uint32_t ni = *s.n_isl;
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t wib = threadIdx.x >> 5;
@@ -1200,13 +1202,21 @@ __global__ void __launch_bounds__(kPgsWarpsPerBlock * 32, 3) k_pgs_warp(DevState
         const uint32_t nb = s.isl_nbod[isl];
         const int32_t* ib = s.isl_bod + begin + isl;
         const uint32_t* bound = lvl_bound + begin + isl;
+        uint32_t* sd = sdesc[wib][0];
+        uint32_t* sl = sdesc[wib][1];
+        uint32_t* sb = sbound[wib];
         for (uint32_t l = lane; l < nb; l += 32) { sdv[l] = zero; sdw[l] = zero; }
+        for (uint32_t i = lane; i < end - begin; i += 32) {
+            sd[i] = s.d_val2[begin + i];
+            sl[i] = s.d_lbod[begin + i];
+        }
+        for (uint32_t l = lane; l <= nlev; l += 32) sb[l] = bound[l] - begin;
         __syncwarp();
         for (int it = 0; it < pos + vel; ++it) {
             for (uint32_t l = 0; l < nlev; ++l) {
-                const uint32_t lb = bound[l], le = bound[l + 1];
+                const uint32_t lb = sb[l], le = sb[l + 1];
                 for (uint32_t i = lb + lane; i < le; i += 32)
-                    solve_desc<LocalDeltas, false>(s, s.d_val2[i], s.d_lbod[i], it, pos, vel, D);
+                    solve_desc<LocalDeltas, false>(s, sd[i], sl[i], it, pos, vel, D);
                 __syncwarp();
             }
             if (it + 1 == pos) {
@@ -1222,11 +1232,20 @@ __global__ void __launch_bounds__(kPgsWarpsPerBlock * 32, 3) k_pgs_warp(DevState
 // One CTA of NT threads per island of a size class (at most MAXN
 // descriptors), with the island's deltas in shared memory
 // (2 x (MAXN + 1) float4).
+// Shared memory of k_pgs_block_smem<MAXN>: deltas, then the island's
+// placed descriptors and local bodies, then its partition bounds.
+template <uint32_t MAXN> struct PgsSmem {
+    static constexpr size_t kBytes = 2 * size_t(MAXN + 1) * sizeof(float4) + 2 * size_t(MAXN) * 4 +
+                                     size_t(kMaxLevels + 1) * 4;
+};
 template <uint32_t MAXN, uint32_t NT>
 __global__ void __launch_bounds__(NT) k_pgs_block_smem(DevState s, const uint32_t* lvl_bound, int list_class) {
     extern __shared__ float4 shb[];
     float4* sdv = shb;
     float4* sdw = shb + (MAXN + 1);
+    uint32_t* sd = reinterpret_cast<uint32_t*>(shb + 2 * (MAXN + 1));   // descriptor per placed slot
+    uint32_t* sl = sd + MAXN;                                             // local bodies per placed slot
+    uint32_t* sb = sl + MAXN;                                             // partition bounds (island-relative)
     const LocalDeltas D{sdv, sdw};
     const uint32_t n_list = s.counters[kCntList + list_class];
     const uint32_t* list = s.isl_list[list_class];
@@ -1239,13 +1258,19 @@ __global__ void __launch_bounds__(NT) k_pgs_block_smem(DevState s, const uint32_
         const uint32_t nb = s.isl_nbod[isl];
         const int32_t* ib = s.isl_bod + begin + isl;
         const uint32_t* bound = lvl_bound + begin + isl;
+        const uint32_t n = s.isl_begin[isl + 1] - begin;
         for (uint32_t l = threadIdx.x; l < nb; l += blockDim.x) { sdv[l] = zero; sdw[l] = zero; }
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            sd[i] = s.d_val2[begin + i];
+            sl[i] = s.d_lbod[begin + i];
+        }
+        for (uint32_t l = threadIdx.x; l <= nlev; l += blockDim.x) sb[l] = bound[l] - begin;
         __syncthreads();
         for (int it = 0; it < pos + vel; ++it) {
             for (uint32_t l = 0; l < nlev; ++l) {
-                const uint32_t lb = bound[l], le = bound[l + 1];
+                const uint32_t lb = sb[l], le = sb[l + 1];
                 for (uint32_t i = lb + threadIdx.x; i < le; i += blockDim.x)
-                    solve_desc(s, s.d_val2[i], s.d_lbod[i], it, pos, vel, D);
+                    solve_desc(s, sd[i], sl[i], it, pos, vel, D);
                 __syncthreads();
             }
             if (it + 1 == pos) {
@@ -1361,7 +1386,7 @@ void init_solver_kernels() {
     cudaFuncSetAttribute(k_partition_smem<kBigIsland>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          int(PartSmem<kBigIsland>::kBytes));
     cudaFuncSetAttribute(k_pgs_block_smem<kBigIsland, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         int(2 * (kBigIsland + 1) * sizeof(float4)));
+                         int(PgsSmem<kBigIsland>::kBytes));
 }
 
 void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, const Branches* br) {
@@ -1409,9 +1434,9 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     k_pgs_warp<<<grid_for(s.desc_cap * 32u, kPgsWarpsPerBlock * 32u, 148u * 3u), kPgsWarpsPerBlock * 32u, 0, st>>>(
         s, lvl_bound);
     k_pgs_block_smem<kMidIsland, 128><<<grid_for(s.desc_cap, kSmallIsland + 1, 148u * 3u), 128,
-                                        2 * (kMidIsland + 1) * sizeof(float4), side(0)>>>(s, lvl_bound, 1);
+                                        PgsSmem<kMidIsland>::kBytes, side(0)>>>(s, lvl_bound, 1);
     k_pgs_block_smem<kBigIsland, 256><<<grid_for(s.desc_cap, kMidIsland + 1, 148u), 256,
-                                        2 * (kBigIsland + 1) * sizeof(float4), side(1)>>>(s, lvl_bound, 2);
+                                        PgsSmem<kBigIsland>::kBytes, side(1)>>>(s, lvl_bound, 2);
     k_pgs_block<<<grid_for(s.desc_cap, kBigIsland + 1, 148u), 256, 0, side(1)>>>(s, lvl_bound);
     join_branches(br, st, 2);
     hook(kStIntegrate, st);

@@ -247,3 +247,19 @@ def test_long_run_statistics_vs_reference(pkg, ref, scenes):
     _, _, pts = w.manifolds()
     assert -pts[..., 6].min() < 0.25
     assert np.all(np.isfinite(ws))
+
+
+def test_gjk_epa_manifolds_match_reference(pkg, ref, scenes):
+    # Densely overlapping rotated boxes: many pairs have no face contact and
+    # finish through GJK/EPA (the warp-cooperative continuation).
+    spec = scenes.random_boxes(500, seed=9, xz=2.5, y=(0.3, 3.0))
+    w, _ = make_world(pkg, [spec])
+    w.collide()
+    assert w.step_counters()["gjk_pairs"] > 0
+    r = ref.RefScene(spec)
+    r.advance_collision()
+    wp, wc, wpts = w.manifolds()
+    rp, rc, _, rpts = r.manifolds()
+    np.testing.assert_array_equal(wp, rp)
+    np.testing.assert_array_equal(wc, rc)
+    assert rel_err(wpts, rpts) <= CONTACT_RTOL
