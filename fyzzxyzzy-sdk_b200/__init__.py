@@ -33,7 +33,8 @@ EXPORTS = (
     "fyzz_b200_read_pairs", "fyzz_b200_read_manifolds", "fyzz_b200_read_encoded_bounds",
     "fyzz_b200_read_sorted_min_x", "fyzz_b200_read_levels", "fyzz_b200_profile_step",
     "fyzz_b200_kernels_per_step", "fyzz_b200_sap_pairs_static_scratch",
-    "fyzz_b200_read_step_counters",
+    "fyzz_b200_read_step_counters", "fyzz_b200_set_contact_notifications",
+    "fyzz_b200_contact_events",
 )
 STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 
@@ -52,6 +53,27 @@ class BodyState(C.Structure):
 class Material(C.Structure):
     _fields_ = [("static_friction", C.c_float), ("dynamic_friction", C.c_float),
                 ("restitution", C.c_float)]
+
+
+class ContactEvent(C.Structure):
+    """fyzz_b200_contact_event_t (reference ContactEvent, world.h:176-190)."""
+    _fields_ = [("body0", C.c_uint32), ("body1", C.c_uint32), ("shape0", C.c_uint32),
+                ("shape1", C.c_uint32), ("kind", C.c_uint32), ("contact_count", C.c_uint32),
+                ("point_offset", C.c_uint64), ("normal_impulse", C.c_double)]
+
+
+class ContactEventPoint(C.Structure):
+    """fyzz_b200_contact_event_point_t (reference ContactEventPoint, world.h:194-199)."""
+    _fields_ = [("position", C.c_float * 3), ("normal", C.c_float * 3), ("separation", C.c_float),
+                ("reserved", C.c_uint32), ("normal_impulse", C.c_double)]
+
+
+EVENT_DTYPE = np.dtype([("body0", "<u4"), ("body1", "<u4"), ("shape0", "<u4"), ("shape1", "<u4"),
+                        ("kind", "<u4"), ("contact_count", "<u4"), ("point_offset", "<u8"),
+                        ("normal_impulse", "<f8")])
+EVENT_POINT_DTYPE = np.dtype([("position", "<f4", 3), ("normal", "<f4", 3), ("separation", "<f4"),
+                              ("reserved", "<u4"), ("normal_impulse", "<f8")])
+FOUND, PERSISTS, LOST = 0, 1, 2
 
 
 class DeviceView(C.Structure):
@@ -107,6 +129,9 @@ def lib():
         L.fyzz_b200_profile_step.argtypes = [vp, f32, vp, u32]
         L.fyzz_b200_kernels_per_step.argtypes = [vp, P(u32)]
         L.fyzz_b200_read_step_counters.argtypes = [vp, vp, u32]
+        L.fyzz_b200_set_contact_notifications.argtypes = [vp, i32]
+        L.fyzz_b200_contact_events.argtypes = [vp, P(P(ContactEvent)), P(u64), P(P(ContactEventPoint)),
+                                               P(u64)]
         L.fyzz_b200_sap_pairs_static_scratch.argtypes = [vp, vp, u32, vp, u32, vp, vp, C.c_char_p,
                                                          C.c_size_t]
         _lib = L
@@ -312,6 +337,25 @@ class World:
         out = np.zeros(n, np.uint32)
         lib().fyzz_b200_read_levels(self.h, _p(out), n)
         return out
+
+    def set_contact_notifications(self, enabled: bool = True):
+        """WorldOptions::contact_notifications (reference world.h:61)."""
+        self._check(lib().fyzz_b200_set_contact_notifications(self.h, 1 if enabled else 0))
+
+    def contact_events(self):
+        """Events and points of the last step as numpy structured arrays
+        (EVENT_DTYPE, EVENT_POINT_DTYPE), copied out of the world's buffers."""
+        ev, pt = C.POINTER(ContactEvent)(), C.POINTER(ContactEventPoint)()
+        nev, npt = C.c_uint64(), C.c_uint64()
+        self._check(lib().fyzz_b200_contact_events(self.h, C.byref(ev), C.byref(nev), C.byref(pt),
+                                                   C.byref(npt)))
+        events = np.zeros(nev.value, EVENT_DTYPE)
+        points = np.zeros(npt.value, EVENT_POINT_DTYPE)
+        if nev.value:
+            C.memmove(events.ctypes.data, ev, nev.value * EVENT_DTYPE.itemsize)
+        if npt.value:
+            C.memmove(points.ctypes.data, pt, npt.value * EVENT_POINT_DTYPE.itemsize)
+        return events, points
 
     def step_counters(self) -> dict:
         """Device counters of the last step (see fyzz_b200_read_step_counters)."""

@@ -1441,6 +1441,7 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     join_branches(br, st, 2);
     hook(kStIntegrate, st);
     k_integrate<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
+    if (s.events) enqueue_events(s, st);
     hook(kStEnd, st);
 }
 

@@ -134,6 +134,13 @@ struct DevState {
     size_t scan_tmp_words = 0;
     uint32_t* sort_hist = nullptr;
     size_t sort_hist_words = 0;
+    // contact events (allocated while notifications are enabled)
+    bool events = false;
+    void* ev = nullptr;                // EventRecord, 2 per pair
+    void* ev_pts = nullptr;            // EventPoint, 4 per pair
+    uint64_t* ev_lost_key = nullptr;   // lost touches, pair order
+    uint32_t* ev_cnt = nullptr;        // contact count per touching manager
+    uint32_t* ev_pt_off = nullptr;     // first event point per touching manager
     uint32_t* counters = nullptr;      // small device counters
     uint32_t* err = nullptr;           // error bits
 };
@@ -174,6 +181,8 @@ void enqueue_broadphase(const DevState& s, cudaStream_t st, const StageHook& hoo
 void enqueue_narrowphase(const DevState& s, cudaStream_t st, const StageHook& hook = {});
 void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook = {},
                     const Branches* br = nullptr);
+// events.cu: the step's contact events into s.ev / s.ev_pts (after PGS).
+void enqueue_events(const DevState& s, cudaStream_t st);
 // Per-device kernel attributes (shared-memory limits); call with the device
 // current before the first step or capture.
 void init_solver_kernels();
@@ -183,6 +192,22 @@ constexpr uint32_t kMidIsland = 512;      // one CTA, shared-memory deltas
 constexpr uint32_t kBigIsland = 4096;     // one CTA, shared-memory deltas (1 CTA / SM)
 // counters[] slots
 enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels = 4, kCntGjk = 5,
-             kCntList = 8 /* 4 island-class list lengths */, kCntSlots = 16 };
+             kCntList = 8 /* 4 island-class list lengths */, kCntLost = 12, kCntEvPts = 13,
+             kCntSlots = 16 };
+
+// Contact event records in device memory; the layouts of
+// fyzz_b200_contact_event_t and fyzz_b200_contact_event_point_t.
+struct EventRecord {
+    uint32_t body0, body1, shape0, shape1, kind, count;
+    uint64_t point_offset;
+    double normal_impulse;
+};
+static_assert(sizeof(EventRecord) == 40, "EventRecord layout");
+struct EventPoint {
+    float position[3], normal[3], separation;
+    uint32_t pad;
+    double normal_impulse;
+};
+static_assert(sizeof(EventPoint) == 40, "EventPoint layout");
 
 }  // namespace fyzz::b200

@@ -424,6 +424,7 @@ public:
             const uint32_t err = read_err();
             if (!err) {
                 steps_done_ += steps;
+                ev_device_valid_ = true;
                 return;
             }
             restore();
@@ -431,9 +432,45 @@ public:
                 grow_pairs(d_.pair_cap * 2u);
                 continue;
             }
+            ev_device_valid_ = false;
             throw std::overflow_error("Device step reported error bits " + std::to_string(err));
         }
+        ev_device_valid_ = false;
         throw std::overflow_error("Pair capacity could not be satisfied");
+    }
+
+    // ---------------- contact events ----------------
+    // WorldOptions::contact_notifications (world.h:61).  Event buffers are
+    // allocated only while notifications are on; the step graph is rebuilt.
+    void set_contact_notifications(bool on) {
+        if (on == notify_) return;
+        notify_ = on;
+        d_.events = on;
+        if (uploaded_ && on) alloc_events();
+        for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    }
+    // World::contact_events / contact_event_points (world.h:466-468): the
+    // last completed step's events, copied from the device on the first
+    // request after the step and valid until the next step.
+    void contact_events(const EventRecord** ev, uint64_t* nev, const EventPoint** pts, uint64_t* npts) {
+        if (notify_ && uploaded_ && steps_done_ && ev_device_valid_ && ev_fetched_ != steps_done_) {
+            check_cuda(cudaStreamSynchronize(stream_), "sync");
+            uint32_t h[kCntSlots] = {};
+            check_cuda(cudaMemcpy(h, d_.counters, sizeof h, cudaMemcpyDeviceToHost), "read");
+            const uint64_t n_ev = uint64_t(h[kCntMan]) + h[kCntLost], n_pts = h[kCntEvPts];
+            h_ev_.resize(n_ev);
+            h_ev_pts_.resize(n_pts);
+            if (n_ev)
+                check_cuda(cudaMemcpy(h_ev_.data(), d_.ev, n_ev * sizeof(EventRecord), cudaMemcpyDeviceToHost), "read");
+            if (n_pts)
+                check_cuda(cudaMemcpy(h_ev_pts_.data(), d_.ev_pts, n_pts * sizeof(EventPoint), cudaMemcpyDeviceToHost), "read");
+            ev_fetched_ = steps_done_;
+        }
+        const bool have = notify_ && ev_fetched_ == steps_done_ && steps_done_;
+        *ev = have ? h_ev_.data() : nullptr;
+        *nev = have ? h_ev_.size() : 0;
+        *pts = have ? h_ev_pts_.data() : nullptr;
+        *npts = have ? h_ev_pts_.size() : 0;
     }
     void collide() {
         check_cuda(cudaSetDevice(device_), "cudaSetDevice");
@@ -825,6 +862,15 @@ private:
         dalloc(d_.scan_tmp, d_.scan_tmp_words, pair_owned_);
         d_.sort_hist_words = radix_hist_words(big);
         dalloc(d_.sort_hist, d_.sort_hist_words, pair_owned_);
+        if (notify_) alloc_events();
+    }
+    void alloc_events() {
+        const size_t cap = d_.pair_cap;
+        dalloc(reinterpret_cast<EventRecord*&>(d_.ev), 2 * cap, pair_owned_);
+        dalloc(reinterpret_cast<EventPoint*&>(d_.ev_pts), 4 * cap, pair_owned_);
+        dalloc(d_.ev_lost_key, cap, pair_owned_);
+        dalloc(d_.ev_cnt, cap, pair_owned_);
+        dalloc(d_.ev_pt_off, cap + 1, pair_owned_);
     }
     void grow_pairs(uint32_t cap) {
         alloc_pairs(cap);
@@ -910,6 +956,7 @@ private:
             }
         }
         d.n_small = uint32_t(small.size());
+        d.events = notify_;
         d_ = d;
         // allocations
         dalloc(d_.sc_fbegin, nsc + 1, owned_); dalloc(d_.sc_plane, nsc, owned_);
@@ -1008,6 +1055,11 @@ private:
     float graph_dt_ = -1.0f;
     int parity_ = 0, last_cur_ = 1, snap_parity_ = 0, snap_last_ = 1;
     uint64_t steps_done_ = 0;
+    bool notify_ = false;
+    bool ev_device_valid_ = false;
+    uint64_t ev_fetched_ = ~0ull;
+    std::vector<EventRecord> h_ev_;
+    std::vector<EventPoint> h_ev_pts_;
     uint32_t last_err_ = 0;
     uint32_t* host_err_ = nullptr;
     uint32_t kernels_per_step_ = 0;
@@ -1234,6 +1286,22 @@ uint64_t fyzz_b200_read_sorted_min_x(fyzz_b200_world* w, uint32_t scene, uint32_
     uint64_t n = 0;
     if (guarded(w, [&](auto& W) { n = W.read_sorted_min_x(scene, values, ids, cap); })) return 0;
     return n;
+}
+int fyzz_b200_set_contact_notifications(fyzz_b200_world* w, int enabled) {
+    return guarded(w, [&](auto& W) { W.set_contact_notifications(enabled != 0); });
+}
+int fyzz_b200_contact_events(fyzz_b200_world* w, const fyzz_b200_contact_event_t** events, uint64_t* n_events,
+                             const fyzz_b200_contact_event_point_t** points, uint64_t* n_points) {
+    static_assert(sizeof(fyzz_b200_contact_event_t) == sizeof(fyzz::b200::EventRecord), "event layout");
+    static_assert(sizeof(fyzz_b200_contact_event_point_t) == sizeof(fyzz::b200::EventPoint), "point layout");
+    if (!events || !n_events || !points || !n_points) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) {
+        const fyzz::b200::EventRecord* e = nullptr;
+        const fyzz::b200::EventPoint* p = nullptr;
+        W.contact_events(&e, n_events, &p, n_points);
+        *events = reinterpret_cast<const fyzz_b200_contact_event_t*>(e);
+        *points = reinterpret_cast<const fyzz_b200_contact_event_point_t*>(p);
+    });
 }
 int fyzz_b200_read_step_counters(fyzz_b200_world* w, uint32_t* out, uint32_t n) {
     if (!out) return FYZZ_B200_INVALID_ARGUMENT;

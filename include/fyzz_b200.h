@@ -147,6 +147,40 @@ int fyzz_b200_write_velocities(fyzz_b200_world* w, const float* v6, uint32_t n_b
 int fyzz_b200_counts(fyzz_b200_world* w, uint64_t out[12]);
 int fyzz_b200_device_view(fyzz_b200_world* w, fyzz_b200_device_view_t* out);
 
+/* ---- contact events: World::contact_events / contact_event_points
+ *      (world.h:176-199, 466-468; Scene::publish_contact_events,
+ *      scene.cpp:9149-9264) ---- */
+/* ContactEvent.  kind: 0 Found, 1 Persists, 2 Lost (ContactEventKind).
+ * body0 < body1; shape0 belongs to body0.  point_offset indexes the points
+ * span; lost events carry no points and zero impulse. */
+typedef struct {
+    uint32_t body0, body1;
+    uint32_t shape0, shape1;
+    uint32_t kind;
+    uint32_t contact_count;
+    uint64_t point_offset;
+    double normal_impulse;  /* sum of the points' impulses */
+} fyzz_b200_contact_event_t;
+/* ContactEventPoint: manifold point with its normal oriented from body0's
+ * solver side, and the final normal impulse of its solver row. */
+typedef struct {
+    float position[3];
+    float normal[3];
+    float separation;
+    uint32_t reserved;
+    double normal_impulse;
+} fyzz_b200_contact_event_point_t;
+/* WorldOptions::contact_notifications (world.h:61); off by default. */
+int fyzz_b200_set_contact_notifications(fyzz_b200_world* w, int enabled);
+/* Events of the last completed step, in the reference's order (touching
+ * contact managers in shape-pair order merged with lost touches).  The
+ * first call after a step copies them from the device; the returned arrays
+ * are owned by the world and valid until the next step.  Empty while
+ * notifications are off or after a step that failed. */
+int fyzz_b200_contact_events(fyzz_b200_world* w, const fyzz_b200_contact_event_t** events,
+                             uint64_t* n_events, const fyzz_b200_contact_event_point_t** points,
+                             uint64_t* n_points);
+
 /* ---- broadphase / narrowphase views (Scene::pairs, found_pairs,
  *      lost_pairs, contacts: scene.h:827-833) ---- */
 /* which: 0 current pairs, 1 found, 2 lost; 2 u32 (shape a < shape b) each.

@@ -352,6 +352,22 @@ uint64_t fz_ref_contact_events(void* p, uint32_t* ev, double* impulse) {
     return e.size();
 }
 
+// Contact event points: position(3) normal(3) separation as floats plus the
+// normal impulse (ContactEventPoint, world.h:194-199).
+uint64_t fz_ref_contact_event_points(void* p, float* pts, double* impulse) {
+    const Scene& s = *static_cast<Handle*>(p)->scene;
+    const auto e = s.contact_event_points();
+    if (pts)
+        for (std::size_t i = 0; i < e.size(); ++i) {
+            float* o = pts + 7 * i;
+            o[0] = e[i].position.x; o[1] = e[i].position.y; o[2] = e[i].position.z;
+            o[3] = e[i].normal.x; o[4] = e[i].normal.y; o[5] = e[i].normal.z;
+            o[6] = e[i].separation;
+            impulse[i] = e[i].normal_impulse;
+        }
+    return e.size();
+}
+
 // ---- stateless Gu generators (public free functions of the reference) ----
 // Shape records: half extents(3) position(3) orientation xyzw(4).
 // Candidate records: local_a(3) local_b(3) normal_b(3) separation(1).

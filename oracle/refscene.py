@@ -55,6 +55,8 @@ def lib():
         L.fz_ref_normal_impulses.argtypes = [vp, vp]
         L.fz_ref_contact_events.restype = u64
         L.fz_ref_contact_events.argtypes = [vp, vp, vp]
+        L.fz_ref_contact_event_points.restype = u64
+        L.fz_ref_contact_event_points.argtypes = [vp, vp, vp]
         L.fz_ref_pcm_box_box_candidates.argtypes = [vp, vp, f32, vp, vp]
         L.fz_ref_pcm_batch_selection.argtypes = [vp, u32, vp]
         L.fz_ref_pcm_box_box_gjk_epa.argtypes = [vp, vp, f32, vp]
@@ -178,11 +180,21 @@ class RefScene:
         return out
 
     def contact_events(self):
+        """Events as (n, 7) u32: body0, body1, kind, count, point offset,
+        shape0, shape1; and their summed normal impulses."""
         n = lib().fz_ref_contact_events(self.h, None, None)
         ev = np.zeros((n, 7), np.uint32)
         imp = np.zeros(n, np.float64)
         lib().fz_ref_contact_events(self.h, _p(ev), _p(imp))
         return ev, imp
+
+    def contact_event_points(self):
+        """Points as (n, 7) f32: position, normal, separation; and impulses."""
+        n = lib().fz_ref_contact_event_points(self.h, None, None)
+        pts = np.zeros((n, 7), np.float32)
+        imp = np.zeros(n, np.float64)
+        lib().fz_ref_contact_event_points(self.h, _p(pts), _p(imp))
+        return pts, imp
 
 
 def step_many(scenes, dt: float, steps: int, threads: int) -> None:
