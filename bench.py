@@ -176,6 +176,35 @@ def ncu_traffic(stage: str):
     return t.get(stage)
 
 
+# --------------------------------------------------------------- ranks
+class RankReducer:
+    """Cross-rank reductions of the timing (max of device times, sum of
+    work units).  Single process: identity.  Under torch.distributed the
+    reductions run on `device` ("cuda" with NCCL, "cpu" with gloo)."""
+
+    def __init__(self, dist=None, device: str = "cuda"):
+        self.dist = dist
+        self.device = device
+
+    def _reduce(self, x: float, op) -> float:
+        if self.dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max(self, x: float) -> float:
+        return self._reduce(x, self.dist.ReduceOp.MAX if self.dist else None)
+
+    def sum(self, x: float) -> float:
+        return self._reduce(x, self.dist.ReduceOp.SUM if self.dist else None)
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+
 # --------------------------------------------------------------- b200 arm
 def plain_same_bodies(torch, pkg, specs, local_rank, n_sample, steps):
     """The plain single-scene path on the batched workload's own bodies: a
@@ -219,23 +248,8 @@ def run_b200(args, rank, world, local_rank):
         import torch.distributed as dist
     torch.cuda.set_device(local_rank)
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    red = RankReducer(dist, "cuda")
+    barrier, max_over_ranks, sum_over_ranks = red.barrier, red.max, red.sum
 
     # ---- plain scene (replica per rank) ----
     spec = plain_spec(args.bodies)
