@@ -34,7 +34,8 @@ EXPORTS = (
     "fyzz_b200_read_sorted_min_x", "fyzz_b200_read_levels", "fyzz_b200_profile_step",
     "fyzz_b200_kernels_per_step", "fyzz_b200_sap_pairs_static_scratch",
     "fyzz_b200_read_step_counters", "fyzz_b200_set_contact_notifications",
-    "fyzz_b200_contact_events",
+    "fyzz_b200_contact_events", "fyzz_b200_rollout_begin", "fyzz_b200_rollout_forward",
+    "fyzz_b200_rollout_backward", "fyzz_b200_read_mass_frames", "fyzz_b200_read_friction_anchors",
 )
 STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 
@@ -130,6 +131,12 @@ def lib():
         L.fyzz_b200_kernels_per_step.argtypes = [vp, P(u32)]
         L.fyzz_b200_read_step_counters.argtypes = [vp, vp, u32]
         L.fyzz_b200_set_contact_notifications.argtypes = [vp, i32]
+        L.fyzz_b200_rollout_begin.argtypes = [vp, u32, u32]
+        L.fyzz_b200_rollout_forward.argtypes = [vp, f32]
+        L.fyzz_b200_rollout_backward.argtypes = [vp] + [vp] * 9
+        L.fyzz_b200_read_mass_frames.argtypes = [vp, vp, vp]
+        L.fyzz_b200_read_friction_anchors.argtypes = [vp, vp, vp, vp, u64]
+        L.fyzz_b200_read_friction_anchors.restype = u64
         L.fyzz_b200_contact_events.argtypes = [vp, P(P(ContactEvent)), P(u64), P(P(ContactEventPoint)),
                                                P(u64)]
         L.fyzz_b200_sap_pairs_static_scratch.argtypes = [vp, vp, u32, vp, u32, vp, vp, C.c_char_p,
@@ -356,6 +363,48 @@ class World:
         if npt.value:
             C.memmove(points.ctypes.data, pt, npt.value * EVENT_POINT_DTYPE.itemsize)
         return events, points
+
+    # ---- differentiable rollouts ----
+    def rollout_begin(self, steps: int, checkpoint_every: int):
+        self._check(lib().fyzz_b200_rollout_begin(self.h, steps, checkpoint_every))
+
+    def rollout_forward(self, seconds: float = 1.0 / 120.0):
+        self._check(lib().fyzz_b200_rollout_forward(self.h, seconds))
+
+    def rollout_backward(self, grad_center, grad_orientation=None, grad_velocity=None, grad_angular=None):
+        """Gradients of a loss on the final state with respect to the initial
+        velocities, body masses and shape friction coefficients."""
+        nb, ns = self.counts()["bodies"], self.counts()["shapes"]
+
+        def arr(x, k):
+            return None if x is None else np.ascontiguousarray(np.asarray(x, np.float32).reshape(nb, k))
+        gc, gq, gv, gw = arr(grad_center, 3), arr(grad_orientation, 4), arr(grad_velocity, 3), arr(grad_angular, 3)
+        out = {"v0": np.zeros((nb, 3), np.float32), "w0": np.zeros((nb, 3), np.float32),
+               "mass": np.zeros(nb, np.float32), "static_friction": np.zeros(ns, np.float32),
+               "dynamic_friction": np.zeros(ns, np.float32)}
+        self._check(lib().fyzz_b200_rollout_backward(
+            self.h, _p(gc), _p(gq), _p(gv), _p(gw), _p(out["v0"]), _p(out["w0"]), _p(out["mass"]),
+            _p(out["static_friction"]), _p(out["dynamic_friction"])))
+        return out
+
+    def friction_anchors(self):
+        """Per touching manager (pair order): anchor word (count in bits 0-7,
+        bit 10 + k: anchor k taken from this step's contact point, whose
+        index is in bits 12 + 2k..13 + 2k) and the anchors in the shape0 /
+        shape1 bodies' mass frames, (n, 2, 3) each."""
+        n = lib().fyzz_b200_read_friction_anchors(self.h, None, None, None, 0)
+        cnt = np.zeros(n, np.uint32)
+        a0 = np.zeros((n, 2, 3), np.float32)
+        a1 = np.zeros((n, 2, 3), np.float32)
+        lib().fyzz_b200_read_friction_anchors(self.h, _p(cnt), _p(a0), _p(a1), n)
+        return cnt, a0, a1
+
+    def read_mass_frames(self):
+        nb = self.counts()["bodies"]
+        c = np.zeros((nb, 3), np.float32)
+        q = np.zeros((nb, 4), np.float32)
+        self._check(lib().fyzz_b200_read_mass_frames(self.h, _p(c), _p(q)))
+        return c, q
 
     def step_counters(self) -> dict:
         """Device counters of the last step (see fyzz_b200_read_step_counters)."""

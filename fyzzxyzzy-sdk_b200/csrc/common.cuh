@@ -100,7 +100,9 @@ struct FrictionHist {
     float n0[3], n1[3];
     float a0[2][3], a1[2][3];
     float sf, df, rest, damping;
-    uint32_t meta;   // bits 0-7 anchor count, bit 8 broken, bit 9 valid patch
+    uint32_t meta;   // bits 0-7 anchor count, bit 8 broken, bit 9 valid patch,
+                     // bits 10-11 anchor k taken from this step's contact point
+                     // (bits 12-13 / 14-15: that point's index)
     uint32_t epoch;
 };
 static_assert(sizeof(FrictionHist) == 96, "FrictionHist layout");

@@ -23,7 +23,7 @@
 // dynamic body).  PGS runs one warp (small islands) or one CTA (large
 // islands) per island, sweeping its partitions in order with warp / block
 // barriers only: no grid-wide synchronisation and no host round trip.
-#include "state.h"
+#include "solver_common.cuh"
 #include <cfloat>
 
 namespace fyzz::b200 {
@@ -32,15 +32,6 @@ namespace {
 constexpr uint32_t kInvalid = 0xffffffffu;
 constexpr int kMaxLevels = 256;
 constexpr uint32_t kSerialIsland = 32;   // partitioned by one thread
-
-__device__ __forceinline__ bool is_dyn(const DevState& s, uint32_t b) { return s.b_flags[b] & kBodyDynamic; }
-
-__device__ __forceinline__ v3 mass_position(const DevState& s, uint32_t b) {
-    return vadd(ld3(s.b_p[b]), rot_sc(ldq(s.b_q[b]), ld3(s.b_ml_p[b])));
-}
-__device__ __forceinline__ qt mass_orientation(const DevState& s, uint32_t b) {
-    return qmul(ldq(s.b_q[b]), ldq(s.b_ml_q[b]));
-}
 
 __global__ void k_frame_begin(DevState s) {
     if (threadIdx.x == 0 && blockIdx.x == 0) s.counters[kCntFrame] += 1u;
@@ -114,17 +105,6 @@ __global__ void k_touch_scatter(DevState s, const uint32_t* flags, const uint32_
         if (flags[k]) s.man_list[pos[k]] = k;
     if (blockIdx.x == 0 && threadIdx.x == 0)
         s.counters[kCntDesc] = s.n_joints + s.counters[kCntMan];
-}
-
-// Gu-ordered bodies of a touching manager: shape0 (dynamic first) / shape1.
-__device__ __forceinline__ void manager_bodies(const DevState& s, uint32_t pair, uint32_t& sh0, uint32_t& sh1) {
-    const uint64_t key = s.cur.key[pair];
-    const uint32_t sa = uint32_t(key >> 32), sb = uint32_t(key);
-    const uint32_t ba = s.s_body[sa], bb = s.s_body[sb];
-    const bool da = is_dyn(s, ba), db = is_dyn(s, bb);
-    const bool reversed = !da || (da && db && ba < bb);
-    sh0 = reversed ? sb : sa;
-    sh1 = reversed ? sa : sb;
 }
 
 __device__ uint32_t uf_find(uint32_t* parent, uint32_t x) {
@@ -716,29 +696,6 @@ __global__ void __launch_bounds__(256) k_partition_smem(DevState s, uint32_t* lv
 }
 
 // ---------------- row preparation ----------------
-struct SBody { v3 v, w, p; float inv_mass; v3 c0, c1, c2; };
-__device__ __forceinline__ SBody load_sbody(const DevState& s, int32_t b) {
-    SBody r;
-    if (b < 0) {
-        r.v = r.w = r.p = {0, 0, 0};
-        r.inv_mass = 0.0f;
-        r.c0 = r.c1 = r.c2 = {0, 0, 0};
-        return r;
-    }
-    r.v = ld3(s.sb_v[b]);
-    r.w = ld3(s.sb_w[b]);
-    r.p = mass_position(s, uint32_t(b));
-    r.inv_mass = s.b_inv[b].w;
-    const float4* si = s.sb_sqrt_i + 3 * size_t(b);
-    r.c0 = ld3(si[0]); r.c1 = ld3(si[1]); r.c2 = ld3(si[2]);
-    return r;
-}
-__device__ __forceinline__ v3 xform(const SBody& d, v3 v) {
-    return {d.c0.x * v.x + d.c1.x * v.y + d.c2.x * v.z,
-            d.c0.y * v.x + d.c1.y * v.y + d.c2.y * v.z,
-            d.c0.z * v.x + d.c1.z * v.y + d.c2.z * v.z};
-}
-
 __global__ void k_prep_joints(DevState s) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= s.n_joints) return;
@@ -773,9 +730,6 @@ __global__ void k_prep_joints(DevState s) {
     r.pad = 0.0f;
     s.jrow[j] = r;
 }
-
-__device__ __forceinline__ v3 lv(const float* f) { return {f[0], f[1], f[2]}; }
-__device__ __forceinline__ void sv(float* f, v3 v) { f[0] = v.x; f[1] = v.y; f[2] = v.z; }
 
 __global__ void k_prep_contacts(DevState s) {
     const uint32_t nm = s.counters[kCntMan];
@@ -898,6 +852,7 @@ __global__ void k_prep_contacts(DevState s) {
         const v3 ext = vsub(bmax, bmin);
         const float dsq = vlen2(ext);
         bool keep_pair = false;
+        uint32_t fresh_bits = 0;   // anchors taken from this step's points: bit k, source point at 2 + 2k
         if (anchors == 2) {
             keep_pair = vlen2(vsub(a0l[0], a0l[1])) * 4.0f >= dsq;
             if (!keep_pair) anchors = 0;
@@ -905,23 +860,26 @@ __global__ void k_prep_contacts(DevState s) {
         if (!keep_pair) {
             v3 anch[2] = {{0, 0, 0}, {0, 0, 0}};
             bool changed[2] = {false, false};
+            uint32_t src[2] = {0, 0};
             uint32_t cnt = anchors;
             if (cnt == 1) anch[0] = vadd(rot_sc(q0, a0l[0]), p0);
             float pd2 = 0.0f;
             for (uint32_t j = 0; j < count; ++j) {
                 if (pts[j].sep >= fr_thr + rest_d) continue;
                 const v3 w = lv(pts[j].p);
-                if (cnt == 0) { anch[0] = w; changed[0] = true; ++cnt; }
+                if (cnt == 0) { anch[0] = w; changed[0] = true; src[0] = j; ++cnt; }
                 else if (cnt == 1) {
                     const float dd = vlen2(vsub(w, anch[0]));
-                    if (dd > 1.0e-8f) { anch[1] = w; changed[1] = true; pd2 = dd; ++cnt; }
+                    if (dd > 1.0e-8f) { anch[1] = w; changed[1] = true; src[1] = j; pd2 = dd; ++cnt; }
                 } else {
                     const float e0 = vlen2(vsub(w, anch[0]));
                     const float e1 = vlen2(vsub(w, anch[1]));
-                    if (e0 > e1 && e0 > pd2) { anch[1] = w; changed[1] = true; pd2 = e0; }
-                    else if (e1 >= e0 && e1 > pd2) { anch[0] = w; changed[0] = true; pd2 = e1; }
+                    if (e0 > e1 && e0 > pd2) { anch[1] = w; changed[1] = true; src[1] = j; pd2 = e0; }
+                    else if (e1 >= e0 && e1 > pd2) { anch[0] = w; changed[0] = true; src[0] = j; pd2 = e1; }
                 }
             }
+            for (uint32_t k = 0; k < 2; ++k)
+                if (changed[k]) fresh_bits |= (1u << k) | (src[k] << (2 + 2 * k));
             for (uint32_t k = 0; k < cnt; ++k) {
                 if (!changed[k]) continue;
                 a0l[k] = rotinv_sc(q0, {anch[k].x - p0.x, anch[k].y - p0.y, anch[k].z - p0.z});
@@ -969,7 +927,7 @@ __global__ void k_prep_contacts(DevState s) {
         sv(nh.a0[0], a0l[0]); sv(nh.a0[1], a0l[1]);
         sv(nh.a1[0], a1l[0]); sv(nh.a1[1], a1l[1]);
         nh.sf = sfr; nh.df = dfr; nh.rest = restitution; nh.damping = damping;
-        nh.meta = anchors | 512u;   // broken bit written by the last PGS pass
+        nh.meta = anchors | 512u | (fresh_bits << 10);   // broken bit written by the last PGS pass
         nh.epoch = frame;
         s.cur.fric[pair] = nh;
     }
@@ -1043,6 +1001,7 @@ __device__ void solve_desc(const DevState& s, uint32_t d, uint32_t lid, int it, 
         D_.store(b0, av, aw);
         D_.store(b1, bv, bw);
         r.applied = nx;
+        if (s.tape_j) s.tape_j[size_t(it) * s.n_joints + d] = nx;
         return;
     }
     const uint32_t m = d - s.n_joints;
@@ -1109,6 +1068,7 @@ __device__ void solve_desc(const DevState& s, uint32_t d, uint32_t lid, int it, 
         aw = {aw.x + ra.x * dl, aw.y + ra.y * dl, aw.z + ra.z * dl};
         bw = {bw.x - rb.x * dl, bw.y - rb.y * dl, bw.z - rb.z * dl};
         s.nrow[4 * size_t(m) + j].applied = ni;
+        if (s.tape_n) s.tape_n[(size_t(it) * s.pair_cap + m) * 4 + j] = ni;
         nsum += ni;
     }
     if (friction) {
@@ -1143,6 +1103,7 @@ __device__ void solve_desc(const DevState& s, uint32_t d, uint32_t lid, int it, 
             aw = {aw.x + ra.x * dl, aw.y + ra.y * dl, aw.z + ra.z * dl};
             bw = {bw.x - rb.x * dl, bw.y - rb.y * dl, bw.z - rb.z * dl};
             s.frow[4 * size_t(m) + k].applied = nx;
+            if (s.tape_f) s.tape_f[(size_t(it) * s.pair_cap + m) * 4 + k] = nx;
             broken |= clamped;
         }
         if (it + 1 == pos + vel) {
@@ -1306,27 +1267,6 @@ __global__ void __launch_bounds__(256) k_pgs_block(DevState s, const uint32_t* l
             }
         }
     }
-}
-
-// scene.cpp:114-143
-__device__ qt integrate_q(qt pose, v3 w, float dt) {
-    float m = w.x * w.x + w.y * w.y + w.z * w.z;
-    if (m != 0.0f) {
-        m = sqrtf(m);
-        if (m > 1.0e7f) {
-            const float sc = 1.0e7f / m;
-            w = {w.x * sc, w.y * sc, w.z * sc};
-            m = 1.0e7f;
-        }
-        const float v = dt * m * 0.5f;
-        const float sn = sinf(v) / m;
-        const float cs = cosf(v);
-        const qt dq = qmul({w.x * sn, w.y * sn, w.z * sn, 0.0f}, pose);
-        const qt nx = {dq.x + pose.x * cs, dq.y + pose.y * cs, dq.z + pose.z * cs, dq.w + pose.w * cs};
-        const float len = sqrtf(nx.x * nx.x + nx.y * nx.y + nx.z * nx.z + nx.w * nx.w);
-        pose = {nx.x / len, nx.y / len, nx.z / len, nx.w / len};
-    }
-    return pose;
 }
 
 __global__ void k_integrate(DevState s) {

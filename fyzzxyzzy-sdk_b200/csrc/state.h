@@ -134,6 +134,13 @@ struct DevState {
     size_t scan_tmp_words = 0;
     uint32_t* sort_hist = nullptr;
     size_t sort_hist_words = 0;
+    // Impulse tape of a differentiated step (null otherwise): the applied
+    // impulse of every row after each PGS pass, [pass][manager][4] for the
+    // normal and friction rows and [pass][joint] for the joints.
+    float* tape_n = nullptr;
+    float* tape_f = nullptr;
+    float* tape_j = nullptr;
+
     // contact events (allocated while notifications are enabled)
     bool events = false;
     void* ev = nullptr;                // EventRecord, 2 per pair
@@ -175,6 +182,34 @@ struct Branches {
     cudaEvent_t fork = nullptr;
     cudaEvent_t join[kN] = {};
 };
+
+// Reverse-mode state of a differentiated rollout (adjoint.cu).  Per body,
+// the adjoint of the mass-frame state (centre c, orientation Q) and the
+// velocities: on entry to a step's reverse pass it refers to the end of
+// the step, on exit to its start.  The rest is per-step scratch and the
+// parameter gradients accumulated over the rollout.
+struct AdjState {
+    float4 *c = nullptr, *q = nullptr, *v = nullptr, *w = nullptr;
+    float4 *x_c = nullptr, *x_q = nullptr;        // the step's start state (mass frame)
+    float4 *dvm = nullptr, *dwm = nullptr;        // adjoints of the position-pass deltas
+    float4 *dv = nullptr, *dw = nullptr;          // adjoints of the final deltas (reverse sweep)
+    float4 *rdv = nullptr, *rdw = nullptr;        // deltas rebuilt during the reverse sweep
+    float4 *v1 = nullptr, *w1 = nullptr;          // adjoints of the pre-integrated velocities
+    float4 *C = nullptr;                          // 3 rows per body: sqrt inverse inertia tensor
+    float *im = nullptr;                          // inverse mass (this step)
+    float *g_im = nullptr;                        // inverse mass, whole rollout
+    float4 *iI = nullptr, *g_iI = nullptr;        // inverse principal inertia (step, rollout)
+    float *g_fs = nullptr, *g_fd = nullptr;       // per shape: static / dynamic friction
+    NormalRow* nrow = nullptr;                    // row adjoints
+    FrictionRow* frow = nullptr;
+    JointRow* jrow = nullptr;
+    float4* hd = nullptr;                         // per manager: ima, imb, sf, df
+    float *yn = nullptr, *yf = nullptr, *yj = nullptr;   // applied-impulse adjoints
+    uint32_t* mark = nullptr;                     // per body (island body lists)
+};
+// adjoint.cu
+void enqueue_adjoint_save_start(const DevState& s, const AdjState& a, cudaStream_t st);
+void enqueue_adjoint_step(const DevState& s, const AdjState& a, cudaStream_t st);
 
 // broadphase.cu / narrowphase.cu / solver.cu
 void enqueue_broadphase(const DevState& s, cudaStream_t st, const StageHook& hook = {});

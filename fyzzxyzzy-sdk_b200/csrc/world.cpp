@@ -439,6 +439,236 @@ public:
         throw std::overflow_error("Pair capacity could not be satisfied");
     }
 
+    // ---------------- differentiable rollouts ----------------
+    // A rollout of `steps` steps keeps a full-state checkpoint every `every`
+    // steps.  The backward pass walks the segments in reverse: it restores
+    // the segment's checkpoint, re-runs the segment forward saving each step's
+    // start state, then for each step in reverse re-runs it with the impulse
+    // tape and applies the step's adjoint (enqueue_adjoint_step).  The
+    // persistent state of a step is the bodies, both contact-manager
+    // generations (keys, PCM caches, friction histories, touch counts), the
+    // device counters and the ping-pong parity.
+    struct Slot {
+        float4 *p = nullptr, *q = nullptr, *v = nullptr, *w = nullptr;
+        uint64_t* key[2] = {};
+        PcmCache* cache[2] = {};
+        FrictionHist* fric[2] = {};
+        uint32_t* count[2] = {};
+        uint32_t* n[2] = {};
+        uint32_t* counters = nullptr;
+        int parity = 0, last = 1;
+        uint64_t steps = 0;
+    };
+    void alloc_slot(Slot& sl) {
+        const size_t nb = d_.n_bodies, cap = d_.pair_cap;
+        dalloc(sl.p, nb, roll_owned_); dalloc(sl.q, nb, roll_owned_);
+        dalloc(sl.v, nb, roll_owned_); dalloc(sl.w, nb, roll_owned_);
+        for (int k = 0; k < 2; ++k) {
+            dalloc(sl.key[k], cap, roll_owned_); dalloc(sl.cache[k], cap, roll_owned_);
+            dalloc(sl.fric[k], cap, roll_owned_); dalloc(sl.count[k], cap, roll_owned_);
+            dalloc(sl.n[k], 1, roll_owned_);
+        }
+        dalloc(sl.counters, kCntSlots, roll_owned_);
+    }
+    template <class T> void d2d(T* dst, const T* src, size_t n) {
+        if (n) check_cuda(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToDevice, stream_), "state copy");
+    }
+    void save_slot(Slot& sl) {
+        const size_t nb = d_.n_bodies, cap = d_.pair_cap;
+        d2d(sl.p, d_.b_p, nb); d2d(sl.q, d_.b_q, nb); d2d(sl.v, d_.b_v, nb); d2d(sl.w, d_.b_w, nb);
+        for (int k = 0; k < 2; ++k) {
+            d2d(sl.key[k], sets_[k].key, cap); d2d(sl.cache[k], sets_[k].cache, cap);
+            d2d(sl.fric[k], sets_[k].fric, cap); d2d(sl.count[k], sets_[k].count, cap);
+            d2d(sl.n[k], sets_[k].n, 1);
+        }
+        d2d(sl.counters, d_.counters, size_t(kCntSlots));
+        sl.parity = parity_; sl.last = last_cur_; sl.steps = steps_done_;
+    }
+    void load_slot(const Slot& sl) {
+        const size_t nb = d_.n_bodies, cap = d_.pair_cap;
+        d2d(d_.b_p, sl.p, nb); d2d(d_.b_q, sl.q, nb); d2d(d_.b_v, sl.v, nb); d2d(d_.b_w, sl.w, nb);
+        for (int k = 0; k < 2; ++k) {
+            d2d(sets_[k].key, sl.key[k], cap); d2d(sets_[k].cache, sl.cache[k], cap);
+            d2d(sets_[k].fric, sl.fric[k], cap); d2d(sets_[k].count, sl.count[k], cap);
+            d2d(sets_[k].n, sl.n[k], 1);
+        }
+        d2d(d_.counters, sl.counters, size_t(kCntSlots));
+        parity_ = sl.parity; last_cur_ = sl.last; steps_done_ = sl.steps;
+        host_authoritative_ = false;
+    }
+    void release_rollout() {
+        for (void* p : roll_owned_) cudaFree(p);
+        roll_owned_.clear();
+        ckpt_.clear();
+        seg_.clear();
+        roll_steps_ = 0;
+        roll_done_ = false;
+    }
+    void rollout_begin(uint32_t steps, uint32_t every) {
+        if (steps == 0 || every == 0) throw std::invalid_argument("Rollout needs steps and a checkpoint interval");
+        check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+        ensure_device();
+        pull_state();
+        check_cuda(cudaStreamSynchronize(stream_), "sync");
+        release_rollout();
+        roll_steps_ = steps;
+        roll_every_ = every;
+        roll_cap_ = d_.pair_cap;
+        ckpt_.resize((steps + every - 1) / every + 1);   // last one: the final state
+        seg_.resize(std::min(every, steps));
+        for (auto& sl : ckpt_) alloc_slot(sl);
+        for (auto& sl : seg_) alloc_slot(sl);
+        const size_t cap = d_.pair_cap, nb = d_.n_bodies, passes = size_t(d_.pos_iters + std::max(d_.vel_iters, 1));
+        dalloc(tape_n_, passes * cap * 4, roll_owned_);
+        dalloc(tape_f_, passes * cap * 4, roll_owned_);
+        dalloc(tape_j_, passes * std::max<size_t>(d_.n_joints, 1), roll_owned_);
+        AdjState& A = adj_;
+        A = AdjState{};
+        for (float4** f : {&A.c, &A.q, &A.v, &A.w, &A.x_c, &A.x_q, &A.dvm, &A.dwm, &A.dv, &A.dw, &A.rdv,
+                           &A.rdw, &A.v1, &A.w1, &A.iI, &A.g_iI})
+            dalloc(*f, nb, roll_owned_);
+        dalloc(A.C, 3 * nb, roll_owned_);
+        dalloc(A.im, nb, roll_owned_); dalloc(A.g_im, nb, roll_owned_);
+        dalloc(A.g_fs, d_.n_shapes, roll_owned_); dalloc(A.g_fd, d_.n_shapes, roll_owned_);
+        dalloc(A.nrow, 4 * cap, roll_owned_); dalloc(A.frow, 4 * cap, roll_owned_);
+        dalloc(A.jrow, std::max<size_t>(d_.n_joints, 1), roll_owned_);
+        dalloc(A.hd, cap, roll_owned_);
+        dalloc(A.yn, 4 * cap, roll_owned_); dalloc(A.yf, 4 * cap, roll_owned_);
+        dalloc(A.yj, std::max<size_t>(d_.n_joints, 1), roll_owned_);
+        dalloc(A.mark, nb, roll_owned_);
+        check_cuda(cudaMemsetAsync(A.mark, 0, nb * 4, stream_), "memset");
+        check_cuda(cudaStreamSynchronize(stream_), "sync");
+    }
+    void require_rollout_capacity() {
+        if (d_.pair_cap != roll_cap_)
+            throw std::logic_error("Pair capacity grew during a differentiable rollout; step the scene once "
+                                   "before rollout_begin so the pair budget is settled");
+    }
+    void rollout_forward(float dt) {
+        if (!roll_steps_) throw std::logic_error("rollout_begin must come first");
+        roll_dt_ = dt;
+        for (uint32_t t0 = 0; t0 < roll_steps_; t0 += roll_every_) {
+            save_slot(ckpt_[t0 / roll_every_]);
+            step(dt, std::min(roll_every_, roll_steps_ - t0));
+            require_rollout_capacity();
+        }
+        save_slot(ckpt_.back());
+        check_cuda(cudaStreamSynchronize(stream_), "sync");
+        roll_done_ = true;
+    }
+    // One step re-run eagerly with the impulse tape, then its adjoint.
+    void taped_step_and_adjoint() {
+        DevState s = view(parity_);
+        s.dt = roll_dt_;
+        s.tape_n = tape_n_; s.tape_f = tape_f_; s.tape_j = n_joints_tape();
+        enqueue_adjoint_save_start(s, adj_, stream_);
+        check_cuda(cudaMemsetAsync(d_.err, 0, 4, stream_), "memset");
+        enqueue_broadphase(s, stream_);
+        enqueue_narrowphase(s, stream_);
+        enqueue_solver(s, stream_, {}, &br_);
+        enqueue_adjoint_step(s, adj_, stream_);
+        check_cuda(cudaGetLastError(), "adjoint launch");
+        last_cur_ = parity_;
+        parity_ ^= 1;
+    }
+    float* n_joints_tape() const { return d_.n_joints ? tape_j_ : nullptr; }
+    void rollout_backward(const float* gc, const float* gq, const float* gv, const float* gw,
+                          float* gv0, float* gw0, float* gmass, float* gfs, float* gfd) {
+        if (!roll_done_) throw std::logic_error("rollout_forward must come first");
+        const uint32_t nb = d_.n_bodies, ns = d_.n_shapes;
+        auto up3 = [&](float4* dst, const float* src) {
+            std::vector<float4> h(nb, make_float4(0, 0, 0, 0));
+            if (src) for (uint32_t i = 0; i < nb; ++i) h[i] = make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0);
+            upload(dst, h, stream_);
+            check_cuda(cudaStreamSynchronize(stream_), "sync");
+        };
+        up3(adj_.c, gc); up3(adj_.v, gv); up3(adj_.w, gw);
+        {
+            std::vector<float4> h(nb, make_float4(0, 0, 0, 0));
+            if (gq) for (uint32_t i = 0; i < nb; ++i) h[i] = make_float4(gq[4 * i], gq[4 * i + 1], gq[4 * i + 2], gq[4 * i + 3]);
+            upload(adj_.q, h, stream_);
+        }
+        check_cuda(cudaMemsetAsync(adj_.g_im, 0, nb * 4, stream_), "memset");
+        check_cuda(cudaMemsetAsync(adj_.g_iI, 0, nb * 16, stream_), "memset");
+        check_cuda(cudaMemsetAsync(adj_.g_fs, 0, ns * 4, stream_), "memset");
+        check_cuda(cudaMemsetAsync(adj_.g_fd, 0, ns * 4, stream_), "memset");
+        const uint32_t nseg = uint32_t(ckpt_.size() - 1);
+        for (int seg = int(nseg) - 1; seg >= 0; --seg) {
+            const uint32_t t0 = uint32_t(seg) * roll_every_, t1 = std::min(roll_steps_, t0 + roll_every_);
+            load_slot(ckpt_[seg]);
+            for (uint32_t t = t0; t < t1; ++t) {
+                save_slot(seg_[t - t0]);
+                if (t + 1 < t1) { d_.dt = roll_dt_; run_steps(roll_dt_, 1); }
+            }
+            for (int t = int(t1) - 1; t >= int(t0); --t) {
+                load_slot(seg_[t - t0]);
+                taped_step_and_adjoint();
+            }
+        }
+        check_cuda(cudaStreamSynchronize(stream_), "backward sync");
+        if (read_err()) throw std::overflow_error("Device error during the backward pass");
+        // outputs
+        std::vector<float4> v(nb), w(nb), iI(nb), inv(nb);
+        std::vector<float> im(nb);
+        check_cuda(cudaMemcpy(v.data(), adj_.v, nb * 16, cudaMemcpyDeviceToHost), "read");
+        check_cuda(cudaMemcpy(w.data(), adj_.w, nb * 16, cudaMemcpyDeviceToHost), "read");
+        check_cuda(cudaMemcpy(iI.data(), adj_.g_iI, nb * 16, cudaMemcpyDeviceToHost), "read");
+        check_cuda(cudaMemcpy(im.data(), adj_.g_im, nb * 4, cudaMemcpyDeviceToHost), "read");
+        check_cuda(cudaMemcpy(inv.data(), d_.b_inv, nb * 16, cudaMemcpyDeviceToHost), "read");
+        for (uint32_t i = 0; i < nb; ++i) {
+            if (gv0) { gv0[3 * i] = v[i].x; gv0[3 * i + 1] = v[i].y; gv0[3 * i + 2] = v[i].z; }
+            if (gw0) { gw0[3 * i] = w[i].x; gw0[3 * i + 1] = w[i].y; gw0[3 * i + 2] = w[i].z; }
+            // inverse mass and inertia scale as 1/m: dm = -im (im g_im + iI . g_iI)
+            if (gmass) gmass[i] = -inv[i].w * (inv[i].w * im[i] + inv[i].x * iI[i].x + inv[i].y * iI[i].y + inv[i].z * iI[i].z);
+        }
+        if (gfs) check_cuda(cudaMemcpy(gfs, adj_.g_fs, ns * 4, cudaMemcpyDeviceToHost), "read");
+        if (gfd) check_cuda(cudaMemcpy(gfd, adj_.g_fd, ns * 4, cudaMemcpyDeviceToHost), "read");
+        // leave the world at the end of the rollout
+        load_slot(ckpt_.back());
+        check_cuda(cudaStreamSynchronize(stream_), "sync");
+    }
+    // Friction patches of the touching managers (pair order) after the last
+    // step: anchor count and the anchors in both bodies' mass frames.
+    uint64_t read_friction_anchors(uint32_t* anchors, float* a0, float* a1, uint64_t cap) {
+        if (!uploaded_) return 0;
+        const auto c = read_counters();
+        if (!anchors || !c.man) return c.man;
+        const uint64_t n = std::min<uint64_t>(c.man, cap);
+        std::vector<uint32_t> ml(n);
+        check_cuda(cudaMemcpy(ml.data(), d_.man_list, n * 4, cudaMemcpyDeviceToHost), "read");
+        std::vector<FrictionHist> h(d_.pair_cap);
+        check_cuda(cudaMemcpy(h.data(), sets_[last_cur_].fric, size_t(d_.pair_cap) * sizeof(FrictionHist),
+                              cudaMemcpyDeviceToHost), "read");
+        for (uint64_t m = 0; m < n; ++m) {
+            const FrictionHist& f = h[ml[m]];
+            anchors[m] = (f.meta & 255u) | (f.meta & 0xfc00u);
+            for (int k = 0; k < 2; ++k)
+                for (int i = 0; i < 3; ++i) {
+                    a0[6 * m + 3 * k + i] = f.a0[k][i];
+                    a1[6 * m + 3 * k + i] = f.a1[k][i];
+                }
+        }
+        return c.man;
+    }
+    // Mass-frame centres and orientations of all bodies (loss inputs).
+    void read_mass_frames(float* c3, float* q4) {
+        ensure_device();
+        const uint32_t nb = d_.n_bodies;
+        std::vector<float4> p(nb), q(nb), mlp(nb), mlq(nb);
+        check_cuda(cudaStreamSynchronize(stream_), "sync");
+        check_cuda(cudaMemcpy(p.data(), d_.b_p, nb * 16, cudaMemcpyDeviceToHost), "read");
+        check_cuda(cudaMemcpy(q.data(), d_.b_q, nb * 16, cudaMemcpyDeviceToHost), "read");
+        check_cuda(cudaMemcpy(mlp.data(), d_.b_ml_p, nb * 16, cudaMemcpyDeviceToHost), "read");
+        check_cuda(cudaMemcpy(mlq.data(), d_.b_ml_q, nb * 16, cudaMemcpyDeviceToHost), "read");
+        for (uint32_t i = 0; i < nb; ++i) {
+            const qt bq = {q[i].x, q[i].y, q[i].z, q[i].w};
+            const v3 off = rot_sc(bq, {mlp[i].x, mlp[i].y, mlp[i].z});
+            const qt mq = qmul(bq, {mlq[i].x, mlq[i].y, mlq[i].z, mlq[i].w});
+            if (c3) { c3[3 * i] = p[i].x + off.x; c3[3 * i + 1] = p[i].y + off.y; c3[3 * i + 2] = p[i].z + off.z; }
+            if (q4) { q4[4 * i] = mq.x; q4[4 * i + 1] = mq.y; q4[4 * i + 2] = mq.z; q4[4 * i + 3] = mq.w; }
+        }
+    }
+
     // ---------------- contact events ----------------
     // WorldOptions::contact_notifications (world.h:61).  Event buffers are
     // allocated only while notifications are on; the step graph is rebuilt.
@@ -808,6 +1038,7 @@ private:
     }
 
     void release_device() {
+        release_rollout();
         for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
         for (void* p : owned_) cudaFree(p);
         owned_.clear();
@@ -1055,6 +1286,13 @@ private:
     float graph_dt_ = -1.0f;
     int parity_ = 0, last_cur_ = 1, snap_parity_ = 0, snap_last_ = 1;
     uint64_t steps_done_ = 0;
+    std::vector<void*> roll_owned_;
+    std::vector<Slot> ckpt_, seg_;
+    uint32_t roll_steps_ = 0, roll_every_ = 1, roll_cap_ = 0;
+    float roll_dt_ = 1.0f / 120.0f;
+    bool roll_done_ = false;
+    float *tape_n_ = nullptr, *tape_f_ = nullptr, *tape_j_ = nullptr;
+    AdjState adj_;
     bool notify_ = false;
     bool ev_device_valid_ = false;
     uint64_t ev_fetched_ = ~0ull;
@@ -1302,6 +1540,30 @@ int fyzz_b200_contact_events(fyzz_b200_world* w, const fyzz_b200_contact_event_t
         *events = reinterpret_cast<const fyzz_b200_contact_event_t*>(e);
         *points = reinterpret_cast<const fyzz_b200_contact_event_point_t*>(p);
     });
+}
+int fyzz_b200_rollout_begin(fyzz_b200_world* w, uint32_t steps, uint32_t checkpoint_every) {
+    return guarded(w, [&](auto& W) { W.rollout_begin(steps, checkpoint_every); });
+}
+int fyzz_b200_rollout_forward(fyzz_b200_world* w, float seconds) {
+    return guarded(w, [&](auto& W) { W.rollout_forward(seconds); });
+}
+int fyzz_b200_rollout_backward(fyzz_b200_world* w, const float* grad_center, const float* grad_orientation,
+                               const float* grad_velocity, const float* grad_angular, float* grad_v0,
+                               float* grad_w0, float* grad_mass, float* grad_static_friction,
+                               float* grad_dynamic_friction) {
+    return guarded(w, [&](auto& W) {
+        W.rollout_backward(grad_center, grad_orientation, grad_velocity, grad_angular, grad_v0, grad_w0,
+                           grad_mass, grad_static_friction, grad_dynamic_friction);
+    });
+}
+uint64_t fyzz_b200_read_friction_anchors(fyzz_b200_world* w, uint32_t* anchors, float* anchors0,
+                                         float* anchors1, uint64_t cap) {
+    uint64_t n = 0;
+    if (guarded(w, [&](auto& W) { n = W.read_friction_anchors(anchors, anchors0, anchors1, cap); })) return 0;
+    return n;
+}
+int fyzz_b200_read_mass_frames(fyzz_b200_world* w, float* centers, float* orientations) {
+    return guarded(w, [&](auto& W) { W.read_mass_frames(centers, orientations); });
 }
 int fyzz_b200_read_step_counters(fyzz_b200_world* w, uint32_t* out, uint32_t n) {
     if (!out) return FYZZ_B200_INVALID_ARGUMENT;

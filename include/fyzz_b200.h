@@ -181,6 +181,34 @@ int fyzz_b200_contact_events(fyzz_b200_world* w, const fyzz_b200_contact_event_t
                              uint64_t* n_events, const fyzz_b200_contact_event_point_t** points,
                              uint64_t* n_points);
 
+/* ---- differentiable rollouts (no counterpart in the reference, which has
+ *      no adjoint) ----
+ * A rollout of `steps` steps of the current state with a full-state
+ * checkpoint every `checkpoint_every` steps; the backward pass re-runs each
+ * segment forward from its checkpoint and applies the step adjoints in
+ * reverse.  Differentiated model: the step with its discrete structure
+ * (pairs, manifolds, partitions, clamp and branch decisions) frozen from
+ * the forward run and contact points moving rigidly with their bodies.
+ * Gradients are with respect to the initial linear / angular velocities,
+ * the body masses (inverse inertia scaling as the inverse mass) and the
+ * shapes' static / dynamic friction coefficients.  Step the scene once
+ * before rollout_begin so the pair budget is settled. */
+int fyzz_b200_rollout_begin(fyzz_b200_world* w, uint32_t steps, uint32_t checkpoint_every);
+int fyzz_b200_rollout_forward(fyzz_b200_world* w, float seconds);
+/* Loss gradients with respect to the final mass-frame centres (3 per body),
+ * orientations (4 per body, may be NULL), linear and angular velocities
+ * (3 per body; NULL = zero).  Outputs (NULL to skip): per body grad_v0,
+ * grad_w0 (3 floats), grad_mass (1); per shape the two friction gradients.
+ * Leaves the world at the end of the rollout. */
+int fyzz_b200_rollout_backward(fyzz_b200_world* w, const float* grad_center,
+                               const float* grad_orientation, const float* grad_velocity,
+                               const float* grad_angular, float* grad_v0, float* grad_w0,
+                               float* grad_mass, float* grad_static_friction,
+                               float* grad_dynamic_friction);
+/* Mass-frame centres (3 per body) and orientations (4 per body) of all
+ * bodies (either may be NULL). */
+int fyzz_b200_read_mass_frames(fyzz_b200_world* w, float* centers, float* orientations);
+
 /* ---- broadphase / narrowphase views (Scene::pairs, found_pairs,
  *      lost_pairs, contacts: scene.h:827-833) ---- */
 /* which: 0 current pairs, 1 found, 2 lost; 2 u32 (shape a < shape b) each.
@@ -196,6 +224,13 @@ int fyzz_b200_read_encoded_bounds(fyzz_b200_world* w, uint32_t* out, uint32_t n_
  * endpoints of the reference's axis-0 endpoint order (scene.cpp:1341-1345). */
 uint64_t fyzz_b200_read_sorted_min_x(fyzz_b200_world* w, uint32_t scene, uint32_t* values,
                                      uint32_t* ids, uint64_t cap);
+/* Friction patch of every touching manager of the last step (pair order):
+ * anchor count (bits 0-7; bit 10 + k: anchor k was taken from this step's
+ * contact point with index in bits 12 + 2k .. 13 + 2k) and the anchors in
+ * the shape0 / shape1 bodies' mass frames (2 x 3 floats each).  Returns the
+ * manager count; writes at most cap. */
+uint64_t fyzz_b200_read_friction_anchors(fyzz_b200_world* w, uint32_t* anchors, float* anchors0,
+                                         float* anchors1, uint64_t cap);
 /* Partition level of every descriptor of the last step, in canonical
  * descriptor order (joints then touching managers). */
 uint64_t fyzz_b200_read_levels(fyzz_b200_world* w, uint32_t* levels, uint64_t cap);
