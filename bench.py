@@ -61,6 +61,13 @@ def parse_args():
     ap.add_argument("--same-scenes", type=int, default=64,
                     help="batched scenes sampled for the plain-path-on-the-same-bodies comparison")
     ap.add_argument("--same-steps", type=int, default=32)
+    ap.add_argument("--no-diff", action="store_true", help="skip the differentiable rollout leg")
+    ap.add_argument("--diff-only", action="store_true", help="time the differentiable rollout leg only")
+    ap.add_argument("--diff-scenes", type=int, default=1024)
+    ap.add_argument("--diff-boxes", type=int, default=64)
+    ap.add_argument("--diff-steps", type=int, default=128)
+    ap.add_argument("--diff-every", type=int, default=16)
+    ap.add_argument("--diff-settle", type=int, default=120)
     ap.add_argument("--settle", type=int, default=0,
                     help="untimed steps of the plain scene before warm-up (profiling a settled pile)")
     ap.add_argument("--plain-only", action="store_true",
@@ -206,6 +213,62 @@ class RankReducer:
 
 
 # --------------------------------------------------------------- b200 arm
+DIFF_WORKLOAD = ("differentiable batched rollout: 1,024 scenes of 64 boxes (half extents U[0.1,0.3]) settled "
+                 "into loose piles, v0 and w0 ~ N(0, 0.5), masses log-uniform [0.5,5] kg, per-scene friction "
+                 "U[0.2,1.0]; 128-step horizon, checkpoint every 16 steps; loss = mean squared distance of "
+                 "the final centres to targets uniform within 2 m; gradients w.r.t. v0, w0, masses, friction")
+
+
+def differentiable_leg(torch, pkg, local_rank, args):
+    """Forward and backward time of the differentiable rollout; the forward
+    includes its checkpoints, the backward the segment recompute, the taped
+    re-run of each step and its adjoint."""
+    specs = scenes_mod().loose_piles(args.diff_scenes, args.diff_boxes)
+    w = pkg.World(local_rank)
+    for s in specs:
+        w.add_scene(s)
+    w.step(DT, args.diff_settle)                      # settled piles: the shared input state
+    nb = w.counts()["bodies"]
+    v6 = np.zeros((nb, 6), np.float32)
+    dyn = np.zeros(nb, bool)
+    at = 0
+    for s in specs:
+        n = s.n_bodies
+        v6[at + 1: at + 1 + n, 0:3] = s.bodies[:, 7:10]
+        v6[at + 1: at + 1 + n, 3:6] = s.bodies[:, 10:13]
+        dyn[at + 1: at + 1 + n] = True
+        at += s.n_actors
+    w.write_velocities(v6)
+    c_start, _ = w.read_mass_frames()
+    rng = np.random.default_rng(0)
+    d = rng.normal(size=(nb, 3))
+    d *= (2.0 * rng.uniform(0, 1, (nb, 1)) ** (1.0 / 3.0)) / np.linalg.norm(d, axis=1, keepdims=True)
+    target = c_start + d
+    w.rollout_begin(args.diff_steps, args.diff_every)
+    w.synchronize()
+    t0 = time.perf_counter()
+    w.rollout_forward(DT)
+    w.synchronize()
+    fwd = time.perf_counter() - t0
+    c, _ = w.read_mass_frames()
+    n_dyn = int(dyn.sum())
+    loss = float(np.sum((c - target)[dyn] ** 2) / n_dyn)
+    grad = (2.0 * (c - target) / n_dyn) * dyn[:, None]
+    t0 = time.perf_counter()
+    torch.cuda.nvtx.range_push("diff_backward")
+    g = w.rollout_backward(grad_center=grad)
+    w.synchronize()
+    torch.cuda.nvtx.range_pop()
+    bwd = time.perf_counter() - t0
+    w.close()
+    return {"workload": DIFF_WORKLOAD, "scenes": len(specs), "bodies": n_dyn, "steps": args.diff_steps,
+            "checkpoint_every": args.diff_every, "forward_ms": fwd * 1e3, "backward_ms": bwd * 1e3,
+            "backward_forward_ratio": bwd / fwd,
+            "forward_value": n_dyn * args.diff_steps / fwd, "unit": UNIT, "loss": loss,
+            "grad_norm_v0": float(np.linalg.norm(g["v0"])),
+            "timing": "host clock around the synchronised rollout_forward / rollout_backward calls"}
+
+
 def plain_same_bodies(torch, pkg, specs, local_rank, n_sample, steps):
     """The plain single-scene path on the batched workload's own bodies: a
     sample of the scenes (evenly spaced over the list, so over the size
@@ -242,6 +305,12 @@ def timed_steps(torch, w, steps, stream):
 
 def run_b200(args, rank, world, local_rank):
     import torch
+    if args.diff_only:
+        torch.cuda.set_device(local_rank)
+        diff = differentiable_leg(torch, importlib.import_module(PKG), local_rank, args)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "differentiable": diff}), flush=True)
+        return
     pkg = importlib.import_module(PKG)
     dist = None
     if world > 1:
@@ -351,6 +420,11 @@ def run_b200(args, rank, world, local_rank):
                    "vs_plain_same_bodies": bvalue / world / same["value"] if same else None}
         wb.close()
 
+    # ---- differentiable rollout (forward + adjoint) ----
+    diff = None
+    if not args.no_diff and not args.plain_only:
+        diff = differentiable_leg(torch, pkg, local_rank, args)
+
     # ---- CPU baseline: the reference NativeCpu scene on this host ----
     cpu = None
     if rank == 0 and world == 1 and not args.plain_only:
@@ -372,6 +446,8 @@ def run_b200(args, rank, world, local_rank):
             "batched_vs_plain": batched["vs_plain_same_bodies"] if batched else None,
             "batched_vs_plain_scene": (batched["value"] / value) if batched else None,
             "e2e": e2e,
+            "differentiable": diff,
+            "backward_forward_ratio": diff["backward_forward_ratio"] if diff else None,
             "gpu_launches": kernels * args.steps,
             "roofline": roofline,
             "cpu_baseline": cpu,

@@ -188,14 +188,34 @@ __global__ void k_adj_integrate(DevState s, AdjState A) {
 __device__ __forceinline__ int32_t joint_body(const DevState& s, uint32_t b) {
     return is_dyn(s, b) ? int32_t(b) : -1;
 }
-__device__ __forceinline__ void load_d(const AdjState& A, int32_t b, v3& v, v3& w, v3& vb, v3& wb) {
-    if (b < 0) { v = w = vb = wb = {0, 0, 0}; return; }
-    v = ld3(A.rdv[b]); w = ld3(A.rdw[b]); vb = ld3(A.dv[b]); wb = ld3(A.dw[b]);
-}
-__device__ __forceinline__ void store_d(const AdjState& A, int32_t b, v3 v, v3 w, v3 vb, v3 wb) {
-    if (b < 0) return;
-    A.rdv[b] = f4(v); A.rdw[b] = f4(w); A.dv[b] = f4(vb); A.dw[b] = f4(wb);
-}
+// Deltas (rebuilt backwards) and their adjoints, addressed by global body
+// (RevGlobal) or by island-local slot in shared memory (RevLocal); handle -1
+// is the static world.
+struct RevGlobal {
+    static constexpr bool kLocal = false;
+    const AdjState& A;
+    __device__ __forceinline__ void load(int32_t b, v3& v, v3& w, v3& vb, v3& wb) const {
+        if (b < 0) { v = w = vb = wb = {0, 0, 0}; return; }
+        v = ld3(A.rdv[b]); w = ld3(A.rdw[b]); vb = ld3(A.dv[b]); wb = ld3(A.dw[b]);
+    }
+    __device__ __forceinline__ void store(int32_t b, v3 v, v3 w, v3 vb, v3 wb) const {
+        if (b < 0) return;
+        A.rdv[b] = f4(v); A.rdw[b] = f4(w); A.dv[b] = f4(vb); A.dw[b] = f4(wb);
+    }
+};
+struct RevLocal {
+    static constexpr bool kLocal = true;
+    float4* d;   // 4 per slot: delta v, delta w, their adjoints
+    __device__ __forceinline__ void load(int32_t b, v3& v, v3& w, v3& vb, v3& wb) const {
+        if (b < 0) { v = w = vb = wb = {0, 0, 0}; return; }
+        v = ld3(d[4 * b]); w = ld3(d[4 * b + 1]); vb = ld3(d[4 * b + 2]); wb = ld3(d[4 * b + 3]);
+    }
+    __device__ __forceinline__ void store(int32_t b, v3 v, v3 w, v3 vb, v3 wb) const {
+        if (b < 0) return;
+        d[4 * b] = f4(v); d[4 * b + 1] = f4(w); d[4 * b + 2] = f4(vb); d[4 * b + 3] = f4(wb);
+    }
+};
+__device__ __forceinline__ int32_t local_handle(uint32_t v) { return v == 0xffffu ? -1 : int32_t(v); }
 
 // One row update in reverse.  Forward: y' = y + dl, av += n dl ima,
 // bv -= n dl imb, aw += ra dl, bw -= rb dl, with dl from the row rule.
@@ -231,14 +251,21 @@ __device__ __forceinline__ void rel_adj(v3 n, v3 ra, v3 rb, v3 av, v3 aw, v3 bv,
     g.rb = vsub(g.rb, vmul(bw, gb));
 }
 
-__device__ void reverse_desc(const DevState& s, const AdjState& A, uint32_t d, int it, int pos) {
+template <class R>
+__device__ void reverse_desc(const DevState& s, const AdjState& A, uint32_t d, uint32_t lid, int it, int pos,
+                             const R& D) {
     const size_t cap = s.pair_cap;
     if (d < s.n_joints) {
         const JointRow& r = s.jrow[d];
-        const int32_t b0 = joint_body(s, s.j_a[d]), b1 = joint_body(s, s.j_b[d]);
+        int32_t b0, b1;
+        if constexpr (R::kLocal) {
+            b0 = local_handle(lid & 0xffffu); b1 = local_handle(lid >> 16);
+        } else {
+            b0 = joint_body(s, s.j_a[d]); b1 = joint_body(s, s.j_b[d]);
+        }
         v3 av, aw, bv, bw, avb, awb, bvb, bwb;
-        load_d(A, b0, av, aw, avb, awb);
-        load_d(A, b1, bv, bw, bvb, bwb);
+        D.load(b0, av, aw, avb, awb);
+        D.load(b1, bv, bw, bvb, bwb);
         const v3 ax = lv(r.axis), ja = lv(r.ang_a), jb = lv(r.ang_b);
         const float yn = s.tape_j[size_t(it) * s.n_joints + d];
         const float yo = it > 0 ? s.tape_j[size_t(it - 1) * s.n_joints + d] : 0.0f;
@@ -257,16 +284,22 @@ __device__ void reverse_desc(const DevState& s, const AdjState& A, uint32_t d, i
         o.vel_mult += nd * ynb;
         if (it < pos) o.constant += ynb; else o.unbiased += ynb;
         A.yj[d] = ynb - dlb;
-        store_d(A, b0, av, aw, avb, awb);
-        store_d(A, b1, bv, bw, bvb, bwb);
+        D.store(b0, av, aw, avb, awb);
+        D.store(b1, bv, bw, bvb, bwb);
         return;
     }
     const uint32_t m = d - s.n_joints;
     const ManagerHeader hd = s.mh[m];
     const float ima = hd.ima, imb = hd.imb;
+    int32_t h0, h1;
+    if constexpr (R::kLocal) {
+        h0 = local_handle(lid & 0xffffu); h1 = local_handle(lid >> 16);
+    } else {
+        h0 = hd.b0; h1 = hd.b1;
+    }
     v3 av, aw, bv, bw, avb, awb, bvb, bwb;
-    load_d(A, hd.b0, av, aw, avb, awb);
-    load_d(A, hd.b1, bv, bw, bvb, bwb);
+    D.load(h0, av, aw, avb, awb);
+    D.load(h1, bv, bw, bvb, bwb);
     RowAdj hg = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0.0f, 0.0f};
     float nsumb = 0.0f, dfb = 0.0f;
     const bool friction = (it >= pos || pos - it <= 3) && hd.anchors;
@@ -340,8 +373,8 @@ __device__ void reverse_desc(const DevState& s, const AdjState& A, uint32_t d, i
     float4 h = A.hd[m];
     h.x += hg.ima; h.y += hg.imb; h.w += dfb;
     A.hd[m] = h;
-    store_d(A, hd.b0, av, aw, avb, awb);
-    store_d(A, hd.b1, bv, bw, bvb, bwb);
+    D.store(h0, av, aw, avb, awb);
+    D.store(h1, bv, bw, bvb, bwb);
 }
 
 // Adds the position-pass delta adjoints of an island's bodies (once each).
@@ -364,39 +397,103 @@ __device__ __forceinline__ void inject_motion(const DevState& s, const AdjState&
     }
 }
 
-// Reverse PGS sweep: one warp per island of <= kSmallIsland descriptors.
-__global__ void k_adj_pgs_warp(DevState s, AdjState A, const uint32_t* lvl_bound, uint32_t epoch) {
+// Reverse PGS sweep over island-local slots in shared memory: one warp per
+// island of <= kSmallIsland descriptors (4 warps per block).
+constexpr uint32_t kRevWarps = 4;
+__global__ void __launch_bounds__(kRevWarps * 32) k_adj_pgs_warp_smem(DevState s, AdjState A,
+                                                                     const uint32_t* lvl_bound) {
+    __shared__ float4 sh[kRevWarps][4 * (kSmallIsland + 1)];
     const uint32_t ni = *s.n_isl;
-    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const int pos = s.pos_iters, vel = s.vel_iters < 1 ? 1 : s.vel_iters;
+    const RevLocal D{sh[wib]};
     for (uint32_t isl = warp; isl < ni; isl += nwarps) {
         const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
         if (end - begin > kSmallIsland) continue;
         const uint32_t nlev = s.isl_end[isl];
+        const uint32_t nb = s.isl_nbod[isl];
+        const int32_t* ib = s.isl_bod + begin + isl;
         const uint32_t* bound = lvl_bound + begin + isl;
+        for (uint32_t l = lane; l < nb; l += 32) {
+            const int32_t g = ib[l];
+            sh[wib][4 * l] = s.sb_dv[g]; sh[wib][4 * l + 1] = s.sb_dw[g];
+            sh[wib][4 * l + 2] = A.dv[g]; sh[wib][4 * l + 3] = A.dw[g];
+        }
+        __syncwarp();
         for (int it = pos + vel - 1; it >= 0; --it) {
             if (it == pos - 1) {
-                for (uint32_t i = begin + lane; i < end; i += 32) inject_motion(s, A, s.d_val2[i], epoch);
+                for (uint32_t l = lane; l < nb; l += 32) {
+                    const int32_t g = ib[l];
+                    float4 v = sh[wib][4 * l + 2], w = sh[wib][4 * l + 3];
+                    const float4 mv = A.dvm[g], mw = A.dwm[g];
+                    v.x += mv.x; v.y += mv.y; v.z += mv.z;
+                    w.x += mw.x; w.y += mw.y; w.z += mw.z;
+                    sh[wib][4 * l + 2] = v; sh[wib][4 * l + 3] = w;
+                }
                 __syncwarp();
             }
             for (int l = int(nlev) - 1; l >= 0; --l) {
                 const uint32_t lb = bound[l], le = bound[l + 1];
-                for (uint32_t i = lb + lane; i < le; i += 32) reverse_desc(s, A, s.d_val2[i], it, pos);
+                for (uint32_t i = lb + lane; i < le; i += 32) reverse_desc(s, A, s.d_val2[i], s.d_lbod[i], it, pos, D);
                 __syncwarp();
             }
         }
+        __syncwarp();
     }
 }
-// Reverse PGS sweep: one CTA per larger island.
-__global__ void __launch_bounds__(256) k_adj_pgs_block(DevState s, AdjState A, const uint32_t* lvl_bound,
-                                                       uint32_t epoch) {
+// The same with one CTA per island of (kSmallIsland, kMidIsland] descriptors.
+__global__ void __launch_bounds__(128) k_adj_pgs_mid_smem(DevState s, AdjState A, const uint32_t* lvl_bound) {
+    extern __shared__ float4 shm[];
+    const uint32_t n_list = s.counters[kCntList + 1];
+    const uint32_t* list = s.isl_list[1];
+    const int pos = s.pos_iters, vel = s.vel_iters < 1 ? 1 : s.vel_iters;
+    const RevLocal D{shm};
+    for (uint32_t k = blockIdx.x; k < n_list; k += gridDim.x) {
+        const uint32_t isl = list[k];
+        const uint32_t begin = s.isl_begin[isl];
+        const uint32_t nlev = s.isl_end[isl];
+        const uint32_t nb = s.isl_nbod[isl];
+        const int32_t* ib = s.isl_bod + begin + isl;
+        const uint32_t* bound = lvl_bound + begin + isl;
+        for (uint32_t l = threadIdx.x; l < nb; l += blockDim.x) {
+            const int32_t g = ib[l];
+            shm[4 * l] = s.sb_dv[g]; shm[4 * l + 1] = s.sb_dw[g];
+            shm[4 * l + 2] = A.dv[g]; shm[4 * l + 3] = A.dw[g];
+        }
+        __syncthreads();
+        for (int it = pos + vel - 1; it >= 0; --it) {
+            if (it == pos - 1) {
+                for (uint32_t l = threadIdx.x; l < nb; l += blockDim.x) {
+                    const int32_t g = ib[l];
+                    float4 v = shm[4 * l + 2], w = shm[4 * l + 3];
+                    const float4 mv = A.dvm[g], mw = A.dwm[g];
+                    v.x += mv.x; v.y += mv.y; v.z += mv.z;
+                    w.x += mw.x; w.y += mw.y; w.z += mw.z;
+                    shm[4 * l + 2] = v; shm[4 * l + 3] = w;
+                }
+                __syncthreads();
+            }
+            for (int l = int(nlev) - 1; l >= 0; --l) {
+                const uint32_t lb = bound[l], le = bound[l + 1];
+                for (uint32_t i = lb + threadIdx.x; i < le; i += blockDim.x)
+                    reverse_desc(s, A, s.d_val2[i], s.d_lbod[i], it, pos, D);
+                __syncthreads();
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Reverse PGS sweep on global memory: one CTA per island beyond kMidIsland.
+__global__ void __launch_bounds__(256) k_adj_pgs_block(DevState s, AdjState A, const uint32_t* lvl_bound) {
     const uint32_t ni = *s.n_isl;
+    const uint32_t epoch = *A.epoch;
     const int pos = s.pos_iters, vel = s.vel_iters < 1 ? 1 : s.vel_iters;
     for (uint32_t isl = blockIdx.x; isl < ni; isl += gridDim.x) {
         const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
-        if (end - begin <= kSmallIsland) continue;
+        if (end - begin <= kMidIsland) continue;
         const uint32_t nlev = s.isl_end[isl];
         const uint32_t* bound = lvl_bound + begin + isl;
         for (int it = pos + vel - 1; it >= 0; --it) {
@@ -407,7 +504,8 @@ __global__ void __launch_bounds__(256) k_adj_pgs_block(DevState s, AdjState A, c
             }
             for (int l = int(nlev) - 1; l >= 0; --l) {
                 const uint32_t lb = bound[l], le = bound[l + 1];
-                for (uint32_t i = lb + threadIdx.x; i < le; i += blockDim.x) reverse_desc(s, A, s.d_val2[i], it, pos);
+                for (uint32_t i = lb + threadIdx.x; i < le; i += blockDim.x)
+                    reverse_desc(s, A, s.d_val2[i], 0u, it, pos, RevGlobal{A});
                 __syncthreads();
             }
         }
@@ -772,21 +870,45 @@ inline uint32_t grid_n(uint32_t n, uint32_t t, uint32_t cap) {
     return g == 0 ? 1 : (g < cap ? g : cap);
 }
 
+__global__ void k_adj_next_epoch(AdjState A) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *A.epoch += 1u;
+}
+
+// Copies the live part of a contact-manager generation (its device count;
+// the PCM caches only when dst has them).
+__global__ void k_copy_set(ManagerSet dst, ManagerSet src, uint32_t cap) {
+    const uint32_t n = min(*src.n, cap);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        dst.key[i] = src.key[i];
+        if (dst.cache) dst.cache[i] = src.cache[i];
+        dst.fric[i] = src.fric[i];
+        dst.count[i] = src.count[i];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *dst.n = *src.n;
+}
+
 }  // namespace
 
 void enqueue_adjoint_save_start(const DevState& s, const AdjState& a, cudaStream_t st) {
     k_adj_save_start<<<grid_n(s.n_bodies, 256, 1u << 30), 256, 0, st>>>(s, a);
 }
 
+void enqueue_copy_set(const ManagerSet& dst, const ManagerSet& src, uint32_t cap, cudaStream_t st) {
+    k_copy_set<<<grid_n(cap, 256, 148u * 8u), 256, 0, st>>>(dst, src, cap);
+}
+
 void enqueue_adjoint_step(const DevState& s, const AdjState& a, cudaStream_t st) {
-    static uint32_t epoch = 0;
-    ++epoch;
     const uint32_t T = 256;
+    k_adj_next_epoch<<<1, 32, 0, st>>>(a);
     k_adj_clear_bodies<<<grid_n(s.n_bodies, T, 1u << 30), T, 0, st>>>(s, a);
     k_adj_clear_rows<<<grid_n(s.pair_cap, T, 148u * 8u), T, 0, st>>>(s, a);
     k_adj_integrate<<<grid_n(s.n_bodies, T, 1u << 30), T, 0, st>>>(s, a);
-    k_adj_pgs_warp<<<grid_n(s.desc_cap * 32u, T, 148u * 8u), T, 0, st>>>(s, a, s.lvl_bound, epoch);
-    k_adj_pgs_block<<<grid_n(s.desc_cap, 1, 148u * 4u), 256, 0, st>>>(s, a, s.lvl_bound, epoch);
+    k_adj_pgs_warp_smem<<<grid_n(s.desc_cap * 32u, kRevWarps * 32u, 148u * 8u), kRevWarps * 32u, 0, st>>>(
+        s, a, s.lvl_bound);
+    k_adj_pgs_mid_smem<<<grid_n(s.desc_cap, kSmallIsland + 1, 148u * 4u), 128,
+                         4 * (kMidIsland + 1) * sizeof(float4), st>>>(s, a, s.lvl_bound);
+    k_adj_pgs_block<<<grid_n(s.desc_cap, 1, 148u * 4u), 256, 0, st>>>(s, a, s.lvl_bound);
     k_adj_prep_contacts<<<grid_n(s.pair_cap, 128, 148u * 8u), 128, 0, st>>>(s, a);
     if (s.n_joints) k_adj_prep_joints<<<grid_n(s.n_joints, T, 1u << 30), T, 0, st>>>(s, a);
     k_adj_bodies<<<grid_n(s.n_bodies, T, 1u << 30), T, 0, st>>>(s, a);

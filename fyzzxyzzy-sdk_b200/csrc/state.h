@@ -205,8 +205,11 @@ struct AdjState {
     JointRow* jrow = nullptr;
     float4* hd = nullptr;                         // per manager: ima, imb, sf, df
     float *yn = nullptr, *yf = nullptr, *yj = nullptr;   // applied-impulse adjoints
-    uint32_t* mark = nullptr;                     // per body (island body lists)
+    uint32_t* mark = nullptr;                     // per body: last step it was visited
+    uint32_t* epoch = nullptr;                    // step counter of the reverse pass
 };
+// Copies the live pairs of a contact-manager generation.
+void enqueue_copy_set(const ManagerSet& dst, const ManagerSet& src, uint32_t cap, cudaStream_t st);
 // adjoint.cu
 void enqueue_adjoint_save_start(const DevState& s, const AdjState& a, cudaStream_t st);
 void enqueue_adjoint_step(const DevState& s, const AdjState& a, cudaStream_t st);

@@ -442,19 +442,18 @@ public:
     // ---------------- differentiable rollouts ----------------
     // A rollout of `steps` steps keeps a full-state checkpoint every `every`
     // steps.  The backward pass walks the segments in reverse: it restores
-    // the segment's checkpoint, re-runs the segment forward saving each step's
-    // start state, then for each step in reverse re-runs it with the impulse
-    // tape and applies the step's adjoint (enqueue_adjoint_step).  The
-    // persistent state of a step is the bodies, both contact-manager
-    // generations (keys, PCM caches, friction histories, touch counts), the
-    // device counters and the ping-pong parity.
+    // the segment's checkpoint and re-runs the segment forward with each
+    // step writing its per-step solver data (solver bodies, manager rows and
+    // headers, contact points, island and partition structure, impulse tape)
+    // straight into its own frame, plus a copy of the step's pair keys,
+    // touch counts and friction histories; then it applies the step adjoints
+    // over the frames in reverse (enqueue_adjoint_step).  The persistent state
+    // of a step (checkpoints) is the bodies, both contact-manager generations
+    // (keys, PCM caches, friction histories, touch counts), the device
+    // counters and the ping-pong parity.
     struct Slot {
         float4 *p = nullptr, *q = nullptr, *v = nullptr, *w = nullptr;
-        uint64_t* key[2] = {};
-        PcmCache* cache[2] = {};
-        FrictionHist* fric[2] = {};
-        uint32_t* count[2] = {};
-        uint32_t* n[2] = {};
+        ManagerSet sets[2];
         uint32_t* counters = nullptr;
         int parity = 0, last = 1;
         uint64_t steps = 0;
@@ -463,44 +462,91 @@ public:
         const size_t nb = d_.n_bodies, cap = d_.pair_cap;
         dalloc(sl.p, nb, roll_owned_); dalloc(sl.q, nb, roll_owned_);
         dalloc(sl.v, nb, roll_owned_); dalloc(sl.w, nb, roll_owned_);
-        for (int k = 0; k < 2; ++k) {
-            dalloc(sl.key[k], cap, roll_owned_); dalloc(sl.cache[k], cap, roll_owned_);
-            dalloc(sl.fric[k], cap, roll_owned_); dalloc(sl.count[k], cap, roll_owned_);
-            dalloc(sl.n[k], 1, roll_owned_);
+        for (auto& m : sl.sets) {
+            dalloc(m.key, cap, roll_owned_); dalloc(m.cache, cap, roll_owned_);
+            dalloc(m.fric, cap, roll_owned_); dalloc(m.count, cap, roll_owned_);
+            dalloc(m.n, 1, roll_owned_);
         }
         dalloc(sl.counters, kCntSlots, roll_owned_);
     }
     template <class T> void d2d(T* dst, const T* src, size_t n) {
         if (n) check_cuda(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToDevice, stream_), "state copy");
     }
+    // Bodies, the live pairs of both generations, counters and parity.
     void save_slot(Slot& sl) {
-        const size_t nb = d_.n_bodies, cap = d_.pair_cap;
+        const size_t nb = d_.n_bodies;
         d2d(sl.p, d_.b_p, nb); d2d(sl.q, d_.b_q, nb); d2d(sl.v, d_.b_v, nb); d2d(sl.w, d_.b_w, nb);
-        for (int k = 0; k < 2; ++k) {
-            d2d(sl.key[k], sets_[k].key, cap); d2d(sl.cache[k], sets_[k].cache, cap);
-            d2d(sl.fric[k], sets_[k].fric, cap); d2d(sl.count[k], sets_[k].count, cap);
-            d2d(sl.n[k], sets_[k].n, 1);
-        }
+        for (int k = 0; k < 2; ++k) enqueue_copy_set(sl.sets[k], sets_[k], d_.pair_cap, stream_);
         d2d(sl.counters, d_.counters, size_t(kCntSlots));
         sl.parity = parity_; sl.last = last_cur_; sl.steps = steps_done_;
     }
     void load_slot(const Slot& sl) {
-        const size_t nb = d_.n_bodies, cap = d_.pair_cap;
+        const size_t nb = d_.n_bodies;
         d2d(d_.b_p, sl.p, nb); d2d(d_.b_q, sl.q, nb); d2d(d_.b_v, sl.v, nb); d2d(d_.b_w, sl.w, nb);
-        for (int k = 0; k < 2; ++k) {
-            d2d(sets_[k].key, sl.key[k], cap); d2d(sets_[k].cache, sl.cache[k], cap);
-            d2d(sets_[k].fric, sl.fric[k], cap); d2d(sets_[k].count, sl.count[k], cap);
-            d2d(sets_[k].n, sl.n[k], 1);
-        }
+        for (int k = 0; k < 2; ++k) enqueue_copy_set(sets_[k], sl.sets[k], d_.pair_cap, stream_);
         d2d(d_.counters, sl.counters, size_t(kCntSlots));
         parity_ = sl.parity; last_cur_ = sl.last; steps_done_ = sl.steps;
         host_authoritative_ = false;
+    }
+    struct Frame {
+        float4 *sb_v = nullptr, *sb_w = nullptr, *sb_dv = nullptr, *sb_dw = nullptr, *sb_mdv = nullptr,
+               *sb_mdw = nullptr, *sb_sqrt_i = nullptr, *x_c = nullptr, *x_q = nullptr;
+        uint32_t* man_list = nullptr;
+        ManagerHeader* mh = nullptr;
+        NormalRow* nrow = nullptr;
+        FrictionRow* frow = nullptr;
+        JointRow* jrow = nullptr;
+        ContactPt* pts = nullptr;
+        ManagerSet cur;                 // keys, friction histories and touch counts of the step
+        float *tn = nullptr, *tf = nullptr, *tj = nullptr;
+        uint32_t *d_val2 = nullptr, *d_lbod = nullptr, *lvl_bound = nullptr, *isl_begin = nullptr,
+                 *isl_end = nullptr, *isl_nbod = nullptr, *n_isl = nullptr, *counters = nullptr;
+        uint32_t* lists[4] = {};
+        int32_t* isl_bod = nullptr;
+        int parity = 0;
+    };
+    void alloc_frame(Frame& f) {
+        const size_t nb = d_.n_bodies, cap = d_.pair_cap, dc = d_.desc_cap;
+        const size_t passes = size_t(d_.pos_iters + std::max(d_.vel_iters, 1));
+        auto& o = roll_owned_;
+        for (float4** b : {&f.sb_v, &f.sb_w, &f.sb_dv, &f.sb_dw, &f.sb_mdv, &f.sb_mdw, &f.x_c, &f.x_q})
+            dalloc(*b, nb, o);
+        dalloc(f.sb_sqrt_i, 3 * nb, o);
+        dalloc(f.man_list, cap, o); dalloc(f.mh, cap, o);
+        dalloc(f.nrow, 4 * cap, o); dalloc(f.frow, 4 * cap, o);
+        dalloc(f.jrow, std::max<size_t>(d_.n_joints, 1), o);
+        dalloc(f.pts, 4 * cap, o);
+        dalloc(f.cur.key, cap, o); dalloc(f.cur.fric, cap, o); dalloc(f.cur.count, cap, o); dalloc(f.cur.n, 1, o);
+        dalloc(f.tn, passes * cap * 4, o); dalloc(f.tf, passes * cap * 4, o);
+        dalloc(f.tj, passes * std::max<size_t>(d_.n_joints, 1), o);
+        dalloc(f.d_val2, dc, o); dalloc(f.d_lbod, dc, o);
+        dalloc(f.lvl_bound, 2 * dc + 2, o); dalloc(f.isl_bod, 2 * dc + 2, o);
+        dalloc(f.isl_begin, dc + 1, o); dalloc(f.isl_end, dc + 1, o); dalloc(f.isl_nbod, dc + 1, o);
+        dalloc(f.n_isl, 1, o); dalloc(f.counters, kCntSlots, o);
+        dalloc(f.lists[0], dc / 33 + 2, o);
+        dalloc(f.lists[1], dc / (kSmallIsland + 1) + 2, o);
+        dalloc(f.lists[2], dc / (kMidIsland + 1) + 2, o);
+        dalloc(f.lists[3], dc / (kBigIsland + 1) + 2, o);
+    }
+    // The step's DevState with its per-step arrays in frame f.
+    DevState framed(const Frame& f, int parity) const {
+        DevState s = view(parity);
+        s.dt = roll_dt_;
+        s.sb_v = f.sb_v; s.sb_w = f.sb_w; s.sb_dv = f.sb_dv; s.sb_dw = f.sb_dw;
+        s.sb_mdv = f.sb_mdv; s.sb_mdw = f.sb_mdw; s.sb_sqrt_i = f.sb_sqrt_i;
+        s.man_list = f.man_list; s.mh = f.mh; s.nrow = f.nrow; s.frow = f.frow; s.jrow = f.jrow;
+        s.pts = f.pts;
+        s.tape_n = f.tn; s.tape_f = f.tf; s.tape_j = d_.n_joints ? f.tj : nullptr;
+        s.d_val2 = f.d_val2; s.d_lbod = f.d_lbod; s.lvl_bound = f.lvl_bound; s.isl_bod = f.isl_bod;
+        s.isl_begin = f.isl_begin; s.isl_end = f.isl_end; s.isl_nbod = f.isl_nbod; s.n_isl = f.n_isl;
+        for (int k = 0; k < 4; ++k) s.isl_list[k] = f.lists[k];
+        return s;
     }
     void release_rollout() {
         for (void* p : roll_owned_) cudaFree(p);
         roll_owned_.clear();
         ckpt_.clear();
-        seg_.clear();
+        frames_.clear();
         roll_steps_ = 0;
         roll_done_ = false;
     }
@@ -515,13 +561,10 @@ public:
         roll_every_ = every;
         roll_cap_ = d_.pair_cap;
         ckpt_.resize((steps + every - 1) / every + 1);   // last one: the final state
-        seg_.resize(std::min(every, steps));
+        frames_.resize(std::min(every, steps));
         for (auto& sl : ckpt_) alloc_slot(sl);
-        for (auto& sl : seg_) alloc_slot(sl);
-        const size_t cap = d_.pair_cap, nb = d_.n_bodies, passes = size_t(d_.pos_iters + std::max(d_.vel_iters, 1));
-        dalloc(tape_n_, passes * cap * 4, roll_owned_);
-        dalloc(tape_f_, passes * cap * 4, roll_owned_);
-        dalloc(tape_j_, passes * std::max<size_t>(d_.n_joints, 1), roll_owned_);
+        for (auto& f : frames_) alloc_frame(f);
+        const size_t cap = d_.pair_cap, nb = d_.n_bodies;
         AdjState& A = adj_;
         A = AdjState{};
         for (float4** f : {&A.c, &A.q, &A.v, &A.w, &A.x_c, &A.x_q, &A.dvm, &A.dwm, &A.dv, &A.dw, &A.rdv,
@@ -536,7 +579,9 @@ public:
         dalloc(A.yn, 4 * cap, roll_owned_); dalloc(A.yf, 4 * cap, roll_owned_);
         dalloc(A.yj, std::max<size_t>(d_.n_joints, 1), roll_owned_);
         dalloc(A.mark, nb, roll_owned_);
+        dalloc(A.epoch, 1, roll_owned_);
         check_cuda(cudaMemsetAsync(A.mark, 0, nb * 4, stream_), "memset");
+        check_cuda(cudaMemsetAsync(A.epoch, 0, 4, stream_), "memset");
         check_cuda(cudaStreamSynchronize(stream_), "sync");
     }
     void require_rollout_capacity() {
@@ -556,22 +601,30 @@ public:
         check_cuda(cudaStreamSynchronize(stream_), "sync");
         roll_done_ = true;
     }
-    // One step re-run eagerly with the impulse tape, then its adjoint.
-    void taped_step_and_adjoint() {
-        DevState s = view(parity_);
-        s.dt = roll_dt_;
-        s.tape_n = tape_n_; s.tape_f = tape_f_; s.tape_j = n_joints_tape();
-        enqueue_adjoint_save_start(s, adj_, stream_);
-        check_cuda(cudaMemsetAsync(d_.err, 0, 4, stream_), "memset");
+    // One step of the segment recompute, its per-step data written to frame f.
+    void framed_step(Frame& f) {
+        f.parity = parity_;
+        const DevState s = framed(f, parity_);
+        AdjState a = adj_;
+        a.x_c = f.x_c; a.x_q = f.x_q;
+        enqueue_adjoint_save_start(s, a, stream_);
         enqueue_broadphase(s, stream_);
         enqueue_narrowphase(s, stream_);
         enqueue_solver(s, stream_, {}, &br_);
-        enqueue_adjoint_step(s, adj_, stream_);
-        check_cuda(cudaGetLastError(), "adjoint launch");
+        enqueue_copy_set(f.cur, sets_[parity_], d_.pair_cap, stream_);
+        d2d(f.counters, d_.counters, size_t(kCntSlots));
         last_cur_ = parity_;
         parity_ ^= 1;
     }
-    float* n_joints_tape() const { return d_.n_joints ? tape_j_ : nullptr; }
+    // The step's adjoint over frame f.
+    void frame_adjoint(const Frame& f) {
+        DevState s = framed(f, f.parity);
+        s.cur = f.cur;
+        s.counters = f.counters;
+        AdjState a = adj_;
+        a.x_c = f.x_c; a.x_q = f.x_q;
+        enqueue_adjoint_step(s, a, stream_);
+    }
     void rollout_backward(const float* gc, const float* gq, const float* gv, const float* gw,
                           float* gv0, float* gw0, float* gmass, float* gfs, float* gfd) {
         if (!roll_done_) throw std::logic_error("rollout_forward must come first");
@@ -592,18 +645,15 @@ public:
         check_cuda(cudaMemsetAsync(adj_.g_iI, 0, nb * 16, stream_), "memset");
         check_cuda(cudaMemsetAsync(adj_.g_fs, 0, ns * 4, stream_), "memset");
         check_cuda(cudaMemsetAsync(adj_.g_fd, 0, ns * 4, stream_), "memset");
+        check_cuda(cudaMemsetAsync(d_.err, 0, 4, stream_), "memset");
         const uint32_t nseg = uint32_t(ckpt_.size() - 1);
         for (int seg = int(nseg) - 1; seg >= 0; --seg) {
             const uint32_t t0 = uint32_t(seg) * roll_every_, t1 = std::min(roll_steps_, t0 + roll_every_);
             load_slot(ckpt_[seg]);
-            for (uint32_t t = t0; t < t1; ++t) {
-                save_slot(seg_[t - t0]);
-                if (t + 1 < t1) { d_.dt = roll_dt_; run_steps(roll_dt_, 1); }
-            }
-            for (int t = int(t1) - 1; t >= int(t0); --t) {
-                load_slot(seg_[t - t0]);
-                taped_step_and_adjoint();
-            }
+            for (uint32_t t = t0; t < t1; ++t) framed_step(frames_[t - t0]);
+            check_cuda(cudaGetLastError(), "recompute launch");
+            for (int t = int(t1) - 1; t >= int(t0); --t) frame_adjoint(frames_[t - t0]);
+            check_cuda(cudaGetLastError(), "adjoint launch");
         }
         check_cuda(cudaStreamSynchronize(stream_), "backward sync");
         if (read_err()) throw std::overflow_error("Device error during the backward pass");
@@ -1287,11 +1337,11 @@ private:
     int parity_ = 0, last_cur_ = 1, snap_parity_ = 0, snap_last_ = 1;
     uint64_t steps_done_ = 0;
     std::vector<void*> roll_owned_;
-    std::vector<Slot> ckpt_, seg_;
+    std::vector<Slot> ckpt_;
+    std::vector<Frame> frames_;
     uint32_t roll_steps_ = 0, roll_every_ = 1, roll_cap_ = 0;
     float roll_dt_ = 1.0f / 120.0f;
     bool roll_done_ = false;
-    float *tape_n_ = nullptr, *tape_f_ = nullptr, *tape_j_ = nullptr;
     AdjState adj_;
     bool notify_ = false;
     bool ev_device_valid_ = false;
