@@ -68,6 +68,11 @@ def parse_args():
     ap.add_argument("--diff-steps", type=int, default=128)
     ap.add_argument("--diff-every", type=int, default=16)
     ap.add_argument("--diff-settle", type=int, default=120)
+    ap.add_argument("--diff4", action="store_true",
+                    help="also run the differentiable rollout at scale (16,384 mixed scenes, 64 steps)")
+    ap.add_argument("--diff4-scenes", type=int, default=16384)
+    ap.add_argument("--diff4-steps", type=int, default=64)
+    ap.add_argument("--diff4-every", type=int, default=8)
     ap.add_argument("--settle", type=int, default=0,
                     help="untimed steps of the plain scene before warm-up (profiling a settled pile)")
     ap.add_argument("--plain-only", action="store_true",
@@ -228,6 +233,7 @@ def differentiable_leg(torch, pkg, local_rank, args):
     for s in specs:
         w.add_scene(s)
     w.step(DT, args.diff_settle)                      # settled piles: the shared input state
+    w.fit_pair_budget(1.5)                            # checkpoints and frames sized by the live pairs
     nb = w.counts()["bodies"]
     v6 = np.zeros((nb, 6), np.float32)
     dyn = np.zeros(nb, bool)
@@ -269,6 +275,58 @@ def differentiable_leg(torch, pkg, local_rank, args):
             "timing": "host clock around the synchronised rollout_forward / rollout_backward calls"}
 
 
+DIFF4_WORKLOAD = ("batched and differentiable at scale: 16,384 scenes, body count log-uniform in [8,256] (60% "
+                  "boxes, 25% spheres, 15% box+sphere compounds, 5% distance-joined pairs), friction U[0.2,1.0]; "
+                  "64-step horizon, checkpoint every 8 steps; loss = mean over scenes of the final centre-of-mass "
+                  "height plus translational kinetic energy; gradients w.r.t. initial velocities and masses")
+
+
+def differentiable_leg_at_scale(torch, pkg, local_rank, args):
+    specs = scenes_mod().mixed_batched(args.diff4_scenes)
+    w = pkg.World(local_rank)
+    first = [w.add_scene(s) for s in specs]
+    w.step(DT, 1)
+    budget = w.fit_pair_budget(1.5)
+    nb = w.counts()["bodies"]
+    mass = np.zeros(nb)
+    scene_of = np.full(nb, -1)
+    for k, (s, f) in enumerate(zip(specs, first)):
+        for i in range(s.n_bodies):
+            mass[f + i] = 1.0 / w.body_mass_properties(f + i)[0]
+            scene_of[f + i] = k
+    dyn = scene_of >= 0
+    free0, total = torch.cuda.mem_get_info()
+    w.rollout_begin(args.diff4_steps, args.diff4_every)
+    free1, _ = torch.cuda.mem_get_info()
+    w.synchronize()
+    t0 = time.perf_counter()
+    w.rollout_forward(DT)
+    w.synchronize()
+    fwd = time.perf_counter() - t0
+    c, _ = w.read_mass_frames()
+    v = w.read_bodies()[:, 3:6].astype(np.float64)
+    S = len(specs)
+    M = np.bincount(scene_of[dyn], weights=mass[dyn], minlength=S)
+    gc = np.zeros((nb, 3))
+    gc[dyn, 1] = mass[dyn] / M[scene_of[dyn]] / S
+    gv = np.zeros((nb, 3))
+    gv[dyn] = mass[dyn, None] * v[dyn] / S
+    height = np.bincount(scene_of[dyn], weights=mass[dyn] * c[dyn, 1], minlength=S) / M
+    ke = np.bincount(scene_of[dyn], weights=0.5 * mass[dyn] * (v[dyn] ** 2).sum(1), minlength=S)
+    t0 = time.perf_counter()
+    g = w.rollout_backward(grad_center=gc, grad_velocity=gv)
+    w.synchronize()
+    bwd = time.perf_counter() - t0
+    w.close()
+    return {"workload": DIFF4_WORKLOAD, "scenes": S, "bodies": int(dyn.sum()), "steps": args.diff4_steps,
+            "checkpoint_every": args.diff4_every, "pair_budget": budget,
+            "rollout_device_bytes": int(free0 - free1), "device_bytes_total": int(total),
+            "forward_ms": fwd * 1e3, "backward_ms": bwd * 1e3, "backward_forward_ratio": bwd / fwd,
+            "forward_value": int(dyn.sum()) * args.diff4_steps / fwd, "unit": UNIT,
+            "loss": float(np.mean(height + ke)), "grad_norm_mass": float(np.linalg.norm(g["mass"])),
+            "timing": "host clock around the synchronised rollout_forward / rollout_backward calls"}
+
+
 def plain_same_bodies(torch, pkg, specs, local_rank, n_sample, steps):
     """The plain single-scene path on the batched workload's own bodies: a
     sample of the scenes (evenly spaced over the list, so over the size
@@ -307,9 +365,12 @@ def run_b200(args, rank, world, local_rank):
     import torch
     if args.diff_only:
         torch.cuda.set_device(local_rank)
-        diff = differentiable_leg(torch, importlib.import_module(PKG), local_rank, args)
+        pkg = importlib.import_module(PKG)
+        out = {"metric": METRIC, "differentiable": differentiable_leg(torch, pkg, local_rank, args)}
+        if args.diff4:
+            out["differentiable_at_scale"] = differentiable_leg_at_scale(torch, pkg, local_rank, args)
         if rank == 0:
-            print(json.dumps({"metric": METRIC, "differentiable": diff}), flush=True)
+            print(json.dumps(out), flush=True)
         return
     pkg = importlib.import_module(PKG)
     dist = None
@@ -424,6 +485,7 @@ def run_b200(args, rank, world, local_rank):
     diff = None
     if not args.no_diff and not args.plain_only:
         diff = differentiable_leg(torch, pkg, local_rank, args)
+    diff4 = differentiable_leg_at_scale(torch, pkg, local_rank, args) if args.diff4 and not args.plain_only else None
 
     # ---- CPU baseline: the reference NativeCpu scene on this host ----
     cpu = None
@@ -447,6 +509,7 @@ def run_b200(args, rank, world, local_rank):
             "batched_vs_plain_scene": (batched["value"] / value) if batched else None,
             "e2e": e2e,
             "differentiable": diff,
+            "differentiable_at_scale": diff4,
             "backward_forward_ratio": diff["backward_forward_ratio"] if diff else None,
             "gpu_launches": kernels * args.steps,
             "roofline": roofline,

@@ -36,6 +36,7 @@ EXPORTS = (
     "fyzz_b200_read_step_counters", "fyzz_b200_set_contact_notifications",
     "fyzz_b200_contact_events", "fyzz_b200_rollout_begin", "fyzz_b200_rollout_forward",
     "fyzz_b200_rollout_backward", "fyzz_b200_read_mass_frames", "fyzz_b200_read_friction_anchors",
+    "fyzz_b200_fit_pair_budget",
 )
 STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 
@@ -132,6 +133,7 @@ def lib():
         L.fyzz_b200_read_step_counters.argtypes = [vp, vp, u32]
         L.fyzz_b200_set_contact_notifications.argtypes = [vp, i32]
         L.fyzz_b200_rollout_begin.argtypes = [vp, u32, u32]
+        L.fyzz_b200_fit_pair_budget.argtypes = [vp, f32, P(u32)]
         L.fyzz_b200_rollout_forward.argtypes = [vp, f32]
         L.fyzz_b200_rollout_backward.argtypes = [vp] + [vp] * 9
         L.fyzz_b200_read_mass_frames.argtypes = [vp, vp, vp]
@@ -365,6 +367,12 @@ class World:
         return events, points
 
     # ---- differentiable rollouts ----
+    def fit_pair_budget(self, headroom: float = 1.5) -> int:
+        """Shrinks the pair budget to the live pairs x headroom (history kept)."""
+        out = C.c_uint32()
+        self._check(lib().fyzz_b200_fit_pair_budget(self.h, headroom, C.byref(out)))
+        return out.value
+
     def rollout_begin(self, steps: int, checkpoint_every: int):
         self._check(lib().fyzz_b200_rollout_begin(self.h, steps, checkpoint_every))
 

@@ -439,6 +439,39 @@ public:
         throw std::overflow_error("Pair capacity could not be satisfied");
     }
 
+    // Re-sizes the pair budget to the live pairs times `headroom`, keeping
+    // both contact-manager generations (keys, PCM caches, friction
+    // histories, touch counts): the next step continues exactly as it would
+    // have.  Per-step buffers are reallocated; the step graphs re-captured.
+    void fit_pair_budget(float headroom) {
+        if (!(headroom >= 1.0f)) throw std::invalid_argument("Pair budget headroom must be at least 1");
+        check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+        ensure_device();
+        release_rollout();
+        uint32_t live[2] = {0, 0};
+        for (int k = 0; k < 2; ++k)
+            check_cuda(cudaMemcpy(&live[k], sets_[k].n, 4, cudaMemcpyDeviceToHost), "read");
+        const uint64_t want = uint64_t(double(std::max(live[0], live[1])) * headroom) + 4096;
+        const uint32_t cap = uint32_t(std::min<uint64_t>(want, 0x7fffffffull));
+        if (cap < std::max(live[0], live[1])) throw std::overflow_error("Pair budget below the live pairs");
+        std::vector<void*> tmp;
+        ManagerSet keep[2];
+        for (int k = 0; k < 2; ++k) {
+            dalloc(keep[k].key, std::max(live[k], 1u), tmp); dalloc(keep[k].cache, std::max(live[k], 1u), tmp);
+            dalloc(keep[k].fric, std::max(live[k], 1u), tmp); dalloc(keep[k].count, std::max(live[k], 1u), tmp);
+            dalloc(keep[k].n, 1, tmp);
+            enqueue_copy_set(keep[k], sets_[k], live[k], stream_);
+        }
+        check_cuda(cudaStreamSynchronize(stream_), "sync");
+        const int parity = parity_, last = last_cur_;
+        alloc_pairs(cap);
+        for (int k = 0; k < 2; ++k) enqueue_copy_set(sets_[k], keep[k], live[k], stream_);
+        check_cuda(cudaStreamSynchronize(stream_), "sync");
+        for (void* p : tmp) cudaFree(p);
+        parity_ = parity;
+        last_cur_ = last;
+    }
+    uint32_t pair_budget() const { return d_.pair_cap; }
     // ---------------- differentiable rollouts ----------------
     // A rollout of `steps` steps keeps a full-state checkpoint every `every`
     // steps.  The backward pass walks the segments in reverse: it restores
@@ -1589,6 +1622,12 @@ int fyzz_b200_contact_events(fyzz_b200_world* w, const fyzz_b200_contact_event_t
         W.contact_events(&e, n_events, &p, n_points);
         *events = reinterpret_cast<const fyzz_b200_contact_event_t*>(e);
         *points = reinterpret_cast<const fyzz_b200_contact_event_point_t*>(p);
+    });
+}
+int fyzz_b200_fit_pair_budget(fyzz_b200_world* w, float headroom, uint32_t* budget_out) {
+    return guarded(w, [&](auto& W) {
+        W.fit_pair_budget(headroom);
+        if (budget_out) *budget_out = W.pair_budget();
     });
 }
 int fyzz_b200_rollout_begin(fyzz_b200_world* w, uint32_t steps, uint32_t checkpoint_every) {

@@ -194,6 +194,12 @@ int fyzz_b200_contact_events(fyzz_b200_world* w, const fyzz_b200_contact_event_t
  * shapes' static / dynamic friction coefficients.  Step the scene once
  * before rollout_begin so the pair budget is settled. */
 int fyzz_b200_rollout_begin(fyzz_b200_world* w, uint32_t steps, uint32_t checkpoint_every);
+/* Re-sizes the pair budget (initially 8 per shape) to the live pairs times
+ * headroom (>= 1), keeping the contact-manager history so the trajectory is
+ * unchanged; rollouts size their checkpoints and frames by this budget.
+ * A later step that needs more pairs grows it again (and a rollout that
+ * sees it grow fails with FYZZ_B200_LOGIC_ERROR). */
+int fyzz_b200_fit_pair_budget(fyzz_b200_world* w, float headroom, uint32_t* budget_out);
 int fyzz_b200_rollout_forward(fyzz_b200_world* w, float seconds);
 /* Loss gradients with respect to the final mass-frame centres (3 per body),
  * orientations (4 per body, may be NULL), linear and angular velocities

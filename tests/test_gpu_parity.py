@@ -263,3 +263,21 @@ def test_gjk_epa_manifolds_match_reference(pkg, ref, scenes):
     np.testing.assert_array_equal(wp, rp)
     np.testing.assert_array_equal(wc, rc)
     assert rel_err(wpts, rpts) <= CONTACT_RTOL
+
+
+def test_fit_pair_budget_keeps_the_trajectory(pkg, scenes):
+    # Shrinking the pair budget keeps the contact-manager history: the run
+    # continues bit for bit as without it.
+    spec = scenes.random_boxes(300, seed=12, xz=2.0, y=(0.3, 4.0))
+    wa, _ = make_world(pkg, [spec])
+    wb, _ = make_world(pkg, [spec])
+    wa.step(DT, steps=20)
+    wb.step(DT, steps=20)
+    before = wa.counts()["pairs"]
+    budget = wa.fit_pair_budget(1.2)
+    # both generations stay: the budget covers the larger one
+    assert before <= budget <= int(1.5 * before) + 4097
+    wa.step(DT, steps=20)
+    wb.step(DT, steps=20)
+    np.testing.assert_array_equal(wa.read_bodies(), wb.read_bodies())
+    np.testing.assert_array_equal(wa.pairs(0), wb.pairs(0))
