@@ -14,8 +14,33 @@ pytestmark = pytest.mark.gpu
 DT = 1.0 / 120.0
 
 
-def settled_piles(pkg, scenes, n_scenes=2, n_boxes=10, settle=90, seed=3):
-    specs = scenes.loose_piles(n_scenes, n_boxes, base_seed=seed)
+def slab_scene(scenes, n_side=10):
+    """A dynamic 10 x 0.2 x 10 m slab carrying n_side^2 boxes: all boxes touch
+    the slab, so the island holds more than 96 descriptors."""
+    n = n_side * n_side
+    nb = 1 + n
+    bodies = np.zeros((nb, 14), np.float32)
+    bodies[:, 6] = 1.0
+    bodies[:, 13] = 500.0
+    bodies[0, :3] = (0.0, 0.1, 0.0)
+    geom = np.zeros((nb, 4), np.float32)
+    geom[0, :3] = (5.0, 0.1, 5.0)
+    for i in range(n):
+        gx, gz = divmod(i, n_side)
+        bodies[1 + i, :3] = (-4.5 + 0.95 * gx, 0.4, -4.5 + 0.95 * gz)
+        geom[1 + i, :3] = (0.2, 0.2, 0.2)
+    local = np.tile(np.array([0, 0, 0, 0, 0, 0, 1], np.float32), (nb, 1))
+    mat = np.tile(np.array([0.6, 0.6, 0.0], np.float32), (nb, 1))
+    return scenes.SceneSpec(bodies=bodies, shape_body=np.arange(nb, dtype=np.uint32),
+                            shape_type=np.zeros(nb, np.uint32), shape_geom=geom, shape_local=local,
+                            shape_mat=mat, floor=0.0, floor_mat=(0.6, 0.6, 0.0))
+
+
+def settled_piles(pkg, scenes, n_scenes=2, n_boxes=10, settle=90, seed=3, dense=False):
+    if dense:
+        specs = [slab_scene(scenes)]
+    else:
+        specs = scenes.loose_piles(n_scenes, n_boxes, base_seed=seed)
     w = pkg.World(0)
     for s in specs:
         w.add_scene(s)
@@ -88,12 +113,17 @@ def shape_friction(specs):
     return np.concatenate(fs).astype(np.float64), np.concatenate(fd).astype(np.float64)
 
 
-@pytest.mark.parametrize("steps,every", [(12, 4), (16, 16)])
-def test_gradients_match_fp64_model(pkg, scenes, steps, every):
+@pytest.mark.parametrize("steps,every,pile", [(12, 4, "small"), (16, 16, "small"), (10, 5, "dense")])
+def test_gradients_match_fp64_model(pkg, scenes, steps, every, pile):
     import torch
     import diff_model as dm
-    wa, specs = settled_piles(pkg, scenes)
-    wb, _ = settled_piles(pkg, scenes)
+    kw = {} if pile == "small" else dict(settle=30, dense=True)
+    wa, specs = settled_piles(pkg, scenes, **kw)
+    wb, _ = settled_piles(pkg, scenes, **kw)
+    if pile == "dense":
+        wa.step(DT)
+        wb.step(DT)
+        assert wa.step_counters()["islands_96_512"] > 0, "the dense pile must reach the CTA island class"
     nb = wa.counts()["bodies"]
     dyn = dynamic_mask(wa)
     v0, w0 = initial_velocities(nb, dyn)
