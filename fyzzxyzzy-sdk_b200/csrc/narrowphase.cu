@@ -349,13 +349,23 @@ __device__ bool solve_small(int n, float a[3][4], float r[3]) {
     return true;
 }
 struct Closest { v3 point, a, b; float w[4]; unsigned mask; float dist2; };
-__device__ Closest closest_simplex(const Sup* s, int count) {
-    Closest best;
-    best.point = best.a = best.b = {0, 0, 0};
-    best.w[0] = best.w[1] = best.w[2] = best.w[3] = 0.0f;
-    best.mask = 0;
-    best.dist2 = FLT_MAX;
-    for (unsigned mask = 1; mask < (1u << count); ++mask) {
+// Closest point of the simplex to the origin (GuPCMGjkEpa.cpp's sub-simplex
+// search): every non-empty vertex subset is solved as an affine system and
+// the nearest feasible one wins.  One lane takes one subset (mask = lane + 1,
+// at most 15); the warp then keeps the smallest distance, and among equal
+// distances the lowest mask, which is the subset the sequential search in
+// mask order keeps (it replaces the best only on a strictly smaller
+// distance).  Each lane's arithmetic is that of one iteration of the
+// sequential search, so the winner is bit for bit the same.  Every lane of
+// the warp calls this with the same simplex and gets the same result.
+__device__ Closest closest_simplex_warp(const Sup* s, int count) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const unsigned mask = lane + 1u;
+    Closest mine;
+    mine.point = mine.a = mine.b = {0, 0, 0};
+    mine.w[0] = mine.w[1] = mine.w[2] = mine.w[3] = 0.0f;
+    bool ok = mask < (1u << count);
+    if (ok) {
         int ids[4] = {0, 0, 0, 0}, n = 0;
         for (int i = 0; i < count; ++i)
             if (mask & (1u << i)) ids[n++] = i;
@@ -371,29 +381,50 @@ __device__ Closest closest_simplex(const Sup* s, int count) {
                 m[i - 1][n - 1] = -vdot(dirs[i - 1], base);
             }
             float coef[3] = {0, 0, 0};
-            if (!solve_small(n - 1, m, coef)) continue;
+            if (!solve_small(n - 1, m, coef)) ok = false;
             for (int i = 1; i < n; ++i) {
                 w[ids[i]] = coef[i - 1];
                 w[ids[0]] -= coef[i - 1];
             }
         }
-        bool feasible = true;
         for (int i = 0; i < n; ++i)
-            if (w[ids[i]] < -1.0e-5f) feasible = false;
-        if (!feasible) continue;
-        v3 q = {0, 0, 0}, pa = {0, 0, 0}, pb = {0, 0, 0};
-        for (int i = 0; i < count; ++i) {
-            q = vadd(q, vmul(s[i].q, w[i]));
-            pa = vadd(pa, vmul(s[i].a, w[i]));
-            pb = vadd(pb, vmul(s[i].b, w[i]));
-        }
-        const float d = vlen2(q);
-        if (d < best.dist2) {
-            best.point = q; best.a = pa; best.b = pb;
-            for (int i = 0; i < 4; ++i) best.w[i] = w[i];
-            best.mask = mask; best.dist2 = d;
+            if (w[ids[i]] < -1.0e-5f) ok = false;
+        if (ok) {
+            v3 q = {0, 0, 0}, pa = {0, 0, 0}, pb = {0, 0, 0};
+            for (int i = 0; i < count; ++i) {
+                q = vadd(q, vmul(s[i].q, w[i]));
+                pa = vadd(pa, vmul(s[i].a, w[i]));
+                pb = vadd(pb, vmul(s[i].b, w[i]));
+            }
+            mine.point = q; mine.a = pa; mine.b = pb;
+            for (int i = 0; i < 4; ++i) mine.w[i] = w[i];
+            mine.dist2 = vlen2(q);
+            ok = mine.dist2 < FLT_MAX;
         }
     }
+    float d = ok ? mine.dist2 : FLT_MAX;
+    unsigned m = ok ? mask : 0xffffffffu;
+    for (int off = 16; off > 0; off >>= 1) {
+        const float od = __shfl_xor_sync(0xffffffffu, d, off);
+        const unsigned om = __shfl_xor_sync(0xffffffffu, m, off);
+        if (od < d || (od == d && om < m)) { d = od; m = om; }
+    }
+    Closest best;
+    if (m == 0xffffffffu) {
+        best.point = best.a = best.b = {0, 0, 0};
+        best.w[0] = best.w[1] = best.w[2] = best.w[3] = 0.0f;
+        best.mask = 0;
+        best.dist2 = FLT_MAX;
+        return best;
+    }
+    const int src = int(m - 1u);
+    const auto bc = [src](float x) { return __shfl_sync(0xffffffffu, x, src); };
+    best.point = {bc(mine.point.x), bc(mine.point.y), bc(mine.point.z)};
+    best.a = {bc(mine.a.x), bc(mine.a.y), bc(mine.a.z)};
+    best.b = {bc(mine.b.x), bc(mine.b.y), bc(mine.b.z)};
+    for (int i = 0; i < 4; ++i) best.w[i] = bc(mine.w[i]);
+    best.mask = m;
+    best.dist2 = d;
     return best;
 }
 __device__ void compact_simplex(Sup* s, int& count, const Closest& c) {
@@ -482,7 +513,10 @@ __device__ bool contact_from_facet(const BPair& p, const Sup* vtx, const Facet& 
     return sqrtf(vlen2(vsub(pa, pb))) <= depth + 1.0e-3f;
 }
 // GJK (GuPCMGjkEpa.cpp) up to the point where EPA starts: returns 0 (no
-// witness), 1 (witness in out) or 2 (EPA needed from simplex[0, sc)).
+// witness), 1 (witness in out) or 2 (EPA needed from simplex[0, sc)).  The
+// whole warp runs it in step on the same pair (every lane holds the same
+// simplex; the sub-simplex search is spread over the lanes), so every lane
+// returns the same mode, witness and simplex.
 __device__ int gjk_phase(const BPair& p, float cd, Cand& out, Sup* simplex, int& count) {
     const float eps = 0.1f * smin(box_min_margin(p.ha), box_min_margin(p.hb));
     const float progress = 1.0f - 0.000225f;
@@ -498,20 +532,20 @@ __device__ int gjk_phase(const BPair& p, float cd, Cand& out, Sup* simplex, int&
         const float proj = vdot(normal, s.q);
         if (proj > cd) return 0;
         if (count > 0 && proj > dist * progress) {
-            const Closest cur = closest_simplex(simplex, count);
+            const Closest cur = closest_simplex_warp(simplex, count);
             return cur.mask && contact_from_gjk(p, cur, out) ? 1 : 0;
         }
         for (int i = 0; i < count; ++i)
             if (s.ai == simplex[i].ai && s.bi == simplex[i].bi) {
                 if (proj > 0.f) {
-                    const Closest cur = closest_simplex(simplex, count);
+                    const Closest cur = closest_simplex_warp(simplex, count);
                     return cur.mask && contact_from_gjk(p, cur, out) && out.sep <= cd ? 1 : 0;
                 }
                 return 0;
             }
         if (count == 4) return 2;
         simplex[count++] = s;
-        const Closest nx = closest_simplex(simplex, count);
+        const Closest nx = closest_simplex_warp(simplex, count);
         if (!nx.mask) return 0;
         closest = nx.point;
         const float nd = sqrtf(nx.dist2);
@@ -1148,13 +1182,12 @@ __global__ void __launch_bounds__(128) k_narrowphase(DevState s) {
 // Box/box pairs whose regenerated manifold had no face contact: GJK/EPA
 // witness and emission from the cache the first kernel left behind.  These
 // are few (hundreds to a few thousand per step) and each is a long search,
-// so one warp takes a pair: lane 0 runs GJK, the warp runs EPA together
-// (run_epa_warp) with the polytope in shared memory.
+// so one warp takes a pair: the warp runs GJK in step (the sub-simplex
+// search one subset per lane) and EPA together (run_epa_warp) with the
+// polytope in shared memory.
 constexpr int kGjkWarps = 4;
 __global__ void __launch_bounds__(kGjkWarps * 32, 1) k_narrowphase_gjk(DevState s) {
     __shared__ EpaShared epa[kGjkWarps];
-    __shared__ Sup simplex_s[kGjkWarps][4];
-    __shared__ int mode_s[kGjkWarps], sc_s[kGjkWarps];
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     const uint32_t n = s.counters[kCntGjk];
     const uint32_t nwarps = gridDim.x * kGjkWarps;
@@ -1171,15 +1204,11 @@ __global__ void __launch_bounds__(kGjkWarps * 32, 1) k_narrowphase_gjk(DevState 
         bp.a_in_b = rotinv_gu(q1, vsub(p0, p1));
         bp.rel = qmul(qconj(q1), q0);
         Cand w = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0.0f};
-        if (lane == 0) {
-            int sc = 0;
-            mode_s[wib] = gjk_phase(bp, ps.cd, w, simplex_s[wib], sc);
-            sc_s[wib] = sc;
-        }
-        __syncwarp();
-        const int mode = mode_s[wib];
+        Sup simplex[4];
+        int sc = 0;
+        const int mode = gjk_phase(bp, ps.cd, w, simplex, sc);
         bool have = mode == 1;
-        if (mode == 2) have = run_epa_warp(bp, simplex_s[wib], sc_s[wib], w, epa[wib]);
+        if (mode == 2) have = run_epa_warp(bp, simplex, sc, w, epa[wib]);
         if (lane == 0) {
             have = have && w.sep <= ps.cd;
             PcmCache cache = s.cur.cache[k];

@@ -216,7 +216,7 @@ __global__ void k_island_classes(DevState s) {
 // last dynamic one plus the number of earlier statics on that body
 // (scene.cpp:7367-7437).
 //
-// Small islands: one thread replays that sequential loop.
+// Small islands: one warp, whose lane 0 replays that sequential loop.
 // Larger islands: one CTA reproduces it exactly in rounds.  A descriptor that
 // is the earliest undecided one on both of its bodies has every earlier
 // descriptor touching those bodies already decided, so it sees exactly the
@@ -224,36 +224,6 @@ __global__ void k_island_classes(DevState s) {
 // decided together.  Each round decides at least the earliest undecided
 // descriptor of the island.  Waves and the static pass use the same rule.
 constexpr uint32_t kDeferred = 0xfffffffeu;
-
-// Island-local number of a body (0xffff for the static world), appending
-// unseen bodies to the island's body list.
-__device__ __forceinline__ uint32_t local_slot_serial(int32_t* ib, uint32_t& nb, int32_t b) {
-    if (b < 0) return 0xffffu;
-    for (uint32_t k = 0; k < nb; ++k)
-        if (ib[k] == b) return k;
-    ib[nb] = b;
-    return nb++;
-}
-
-__device__ void place_by_level(const DevState& s, uint32_t isl, uint32_t begin, uint32_t end,
-                               uint32_t nlev, uint32_t* lvl_bound) {
-    uint32_t* bound = lvl_bound + begin + isl;   // nlev + 1 entries
-    for (uint32_t l = 0; l <= nlev; ++l) bound[l] = 0u;
-    for (uint32_t i = begin; i < end; ++i) {
-        const uint32_t l = min(s.d_level[s.d_val[i]], uint32_t(kMaxLevels - 1));
-        ++bound[l + 1];
-    }
-    uint32_t run = begin;
-    for (uint32_t l = 0; l <= nlev; ++l) { run += bound[l]; bound[l] = run; }
-    for (uint32_t i = begin; i < end; ++i) {
-        const uint32_t d = s.d_val[i];
-        const uint32_t l = min(s.d_level[d], uint32_t(kMaxLevels - 1));
-        s.d_val2[bound[l]++] = d;
-    }
-    for (uint32_t l = nlev; l > 0; --l) bound[l] = bound[l - 1];
-    bound[0] = begin;
-    s.isl_end[isl] = nlev;
-}
 
 __global__ void __launch_bounds__(256) k_partition_large(DevState s, uint32_t* lvl_bound) {
     __shared__ uint32_t cursor[kMaxLevels + 1];
@@ -393,73 +363,148 @@ __global__ void __launch_bounds__(256) k_partition_large(DevState s, uint32_t* l
     }
 }
 
-// One thread per small island: the sequential loop itself.
-__global__ void k_partition(DevState s, uint32_t* lvl_bound) {
+// Island-local numbers of the bodies of up to 32 descriptors held one per
+// lane (bx, by; -1 for the static world): bodies are numbered in the order
+// of their first appearance in x0, y0, x1, y1, ..., so an entry's number is
+// the count of first appearances before the entry's own first appearance.  lx / ly
+// receive the numbers (0xffff for the static world), nb the body count and
+// fx / fy the entry index of the body's first appearance.
+__device__ __forceinline__ void warp_local_slots(int32_t bx, int32_t by, uint32_t n, uint32_t& lx, uint32_t& ly,
+                                                 uint32_t& nb, uint32_t& fx, uint32_t& fy) {
+    const uint32_t full = 0xffffffffu, lane = threadIdx.x & 31u;
+    fx = 2u * lane;
+    fy = 2u * lane + 1u;
+    for (uint32_t j = 0; j < n; ++j) {
+        const int32_t ox = __shfl_sync(full, bx, int(j)), oy = __shfl_sync(full, by, int(j));
+        const uint32_t ex = 2u * j, ey = ex + 1u;
+        if (ox == bx && ex < fx) fx = ex;
+        if (oy == bx && ey < fx) fx = ey;
+        if (ox == by && ex < fy) fy = ex;
+        if (oy == by && ey < fy) fy = ey;
+    }
+    const bool on = lane < n;
+    const uint32_t mx = __ballot_sync(full, on && bx >= 0 && fx == 2u * lane);
+    const uint32_t my = __ballot_sync(full, on && by >= 0 && fy == 2u * lane + 1u);
+    auto number = [&](uint32_t f) {
+        const uint32_t j = f >> 1, below = (1u << j) - 1u;
+        return uint32_t(__popc(mx & below) + __popc(my & below)) + ((f & 1u) ? ((mx >> j) & 1u) : 0u);
+    };
+    lx = bx >= 0 ? number(fx) : 0xffffu;
+    ly = by >= 0 ? number(fy) : 0xffffu;
+    nb = uint32_t(__popc(mx) + __popc(my));
+}
+
+// One warp per small island: lane i holds the island's i-th descriptor.
+// Lane 0 replays the sequential loop over island-local body masks kept in
+// shared memory; the placement by level and the island-local body numbering
+// of the placed order are spread over the lanes.
+constexpr int kPartWarps = 4;
+__global__ void __launch_bounds__(kPartWarps * 32) k_partition(DevState s, uint32_t* lvl_bound) {
+    __shared__ uint32_t smask[kPartWarps][2 * kSerialIsland], smaxd[kPartWarps][2 * kSerialIsland];
+    __shared__ uint32_t sstat[kPartWarps][2 * kSerialIsland], spair[kPartWarps][kSerialIsland];
+    __shared__ uint32_t slev[kPartWarps][kSerialIsland], snlev[kPartWarps];
+    __shared__ int2 sbod[kPartWarps][kSerialIsland];
+    const uint32_t full = 0xffffffffu, lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    uint32_t* mask = smask[wib];
+    uint32_t* maxd = smaxd[wib];
+    uint32_t* stat = sstat[wib];
+    uint32_t* pr = spair[wib];
+    uint32_t* lv = slev[wib];
     const uint32_t ni = *s.n_isl;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < ni; isl += stride) {
+    for (uint32_t isl = blockIdx.x * kPartWarps + wib; isl < ni; isl += gridDim.x * kPartWarps) {
         const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
-        if (end - begin > kSerialIsland) continue;
-        uint32_t nlev = 0;
-        bool pending = true;
-        for (uint32_t wave = 0; pending; wave += 32) {
-            if (wave >= kMaxLevels) { atomicOr(s.err, kErrLevelRange); break; }
-            pending = false;
-            if (wave)
-                for (uint32_t i = begin; i < end; ++i) {
-                    const uint32_t d = s.d_val[i];
-                    if (s.d_level[d] != kInvalid) continue;
-                    int32_t b0, b1;
-                    desc_bodies(s, d, b0, b1);
-                    if (b0 < 0 || b1 < 0) continue;
-                    s.sb_mask[b0] = 0u;
-                    s.sb_mask[b1] = 0u;
+        const uint32_t n = end - begin;
+        if (n > kSerialIsland) continue;
+        const bool on = lane < n;
+        const uint32_t d = on ? s.d_val[begin + lane] : 0u;
+        const int2 b = on ? s.d_bod[d] : make_int2(-1, -1);
+        uint32_t lx, ly, nb, fx, fy;
+        warp_local_slots(b.x, b.y, n, lx, ly, nb, fx, fy);
+        mask[lane] = mask[lane + 32] = 0u;
+        maxd[lane] = maxd[lane + 32] = 0u;
+        stat[lane] = stat[lane + 32] = 0u;
+        pr[lane] = lx | (ly << 16);
+        lv[lane] = kInvalid;
+        __syncwarp();
+        if (lane == 0) {
+            uint32_t nlev = 0;
+            bool pending = true;
+            for (uint32_t wave = 0; pending; wave += 32) {
+                if (wave >= kMaxLevels) { atomicOr(s.err, kErrLevelRange); break; }
+                pending = false;
+                if (wave)
+                    for (uint32_t i = 0; i < n; ++i) {
+                        const uint32_t x = pr[i] & 0xffffu, y = pr[i] >> 16;
+                        if (lv[i] != kInvalid || x == 0xffffu || y == 0xffffu) continue;
+                        mask[x] = 0u;
+                        mask[y] = 0u;
+                    }
+                bool progress = false;
+                for (uint32_t i = 0; i < n; ++i) {
+                    const uint32_t x = pr[i] & 0xffffu, y = pr[i] >> 16;
+                    if (lv[i] != kInvalid || x == 0xffffu || y == 0xffffu) continue;
+                    const uint32_t avail = ~(mask[x] | mask[y]);
+                    if (!avail) { pending = true; continue; }
+                    const uint32_t bit = __ffs(avail) - 1;
+                    mask[x] |= 1u << bit;
+                    mask[y] |= 1u << bit;
+                    const uint32_t lp = wave + bit;
+                    maxd[x] = max(maxd[x], lp + 1);
+                    maxd[y] = max(maxd[y], lp + 1);
+                    lv[i] = lp;
+                    nlev = max(nlev, lp + 1);
+                    progress = true;
                 }
-            bool progress = false;
-            for (uint32_t i = begin; i < end; ++i) {
-                const uint32_t d = s.d_val[i];
-                if (s.d_level[d] != kInvalid) continue;
-                int32_t b0, b1;
-                desc_bodies(s, d, b0, b1);
-                if (b0 < 0 || b1 < 0) continue;
-                const uint32_t avail = ~(s.sb_mask[b0] | s.sb_mask[b1]);
-                if (!avail) { pending = true; continue; }
-                const uint32_t bit = __ffs(avail) - 1;
-                s.sb_mask[b0] |= 1u << bit;
-                s.sb_mask[b1] |= 1u << bit;
-                const uint32_t lp = wave + bit;
-                s.sb_maxdyn[b0] = max(s.sb_maxdyn[b0], lp + 1);
-                s.sb_maxdyn[b1] = max(s.sb_maxdyn[b1], lp + 1);
-                s.d_level[d] = lp;
-                nlev = max(nlev, lp + 1);
-                progress = true;
+                if (pending && !progress) { atomicOr(s.err, kErrPartition); break; }
             }
-            if (pending && !progress) { atomicOr(s.err, kErrPartition); break; }
+            for (uint32_t i = 0; i < n; ++i) {
+                if (lv[i] != kInvalid) continue;
+                const uint32_t x = pr[i] & 0xffffu, y = pr[i] >> 16;
+                const uint32_t act = x != 0xffffu ? x : y;
+                if (act == 0xffffu) continue;
+                const uint32_t lp = maxd[act] + stat[act]++;
+                lv[i] = lp;
+                nlev = max(nlev, lp + 1);
+            }
+            if (nlev > kMaxLevels) { atomicOr(s.err, kErrLevelRange); nlev = kMaxLevels; }
+            if (nlev > n) { atomicOr(s.err, kErrLevelRange); nlev = n; }
+            snlev[wib] = nlev;
         }
-        for (uint32_t i = begin; i < end; ++i) {
-            const uint32_t d = s.d_val[i];
-            if (s.d_level[d] != kInvalid) continue;
-            int32_t b0, b1;
-            desc_bodies(s, d, b0, b1);
-            const int32_t act = b0 >= 0 ? b0 : b1;
-            if (act < 0) continue;
-            const uint32_t lp = s.sb_maxdyn[act] + s.sb_static[act]++;
-            s.d_level[d] = lp;
-            nlev = max(nlev, lp + 1);
+        __syncwarp();
+        const uint32_t nlev = snlev[wib];
+        const uint32_t level = lv[lane];
+        if (on) s.d_level[d] = level;
+        // placement by level, stable in island order
+        const uint32_t l = on ? min(level, nlev ? nlev - 1u : 0u) : 0xffffffffu;
+        uint32_t before = 0, rank = 0;
+        for (uint32_t j = 0; j < n; ++j) {
+            const uint32_t o = __shfl_sync(full, l, int(j));
+            before += o < lane ? 1u : 0u;
+            rank += (o < l || (o == l && j < lane)) ? 1u : 0u;
         }
-        if (nlev > kMaxLevels) { atomicOr(s.err, kErrLevelRange); nlev = kMaxLevels; }
-        if (nlev > end - begin) { atomicOr(s.err, kErrLevelRange); nlev = end - begin; }
-        place_by_level(s, isl, begin, end, nlev, lvl_bound);
+        uint32_t* bound = lvl_bound + begin + isl;   // nlev + 1 entries
+        if (lane < nlev) bound[lane] = begin + before;
+        if (lane == 0) {
+            bound[nlev] = end;
+            s.isl_end[isl] = nlev;
+        }
+        if (on) {
+            s.d_val2[begin + rank] = d;
+            sbod[wib][rank] = b;
+        }
+        __syncwarp();
         // island-local body numbering, in placed order
-        int32_t* ib = s.isl_bod + begin + isl;
-        uint32_t nb = 0;
-        for (uint32_t i = begin; i < end; ++i) {
-            const int2 b = s.d_bod[s.d_val2[i]];
-            const uint32_t la = local_slot_serial(ib, nb, b.x);
-            const uint32_t lb = local_slot_serial(ib, nb, b.y);
-            s.d_lbod[i] = la | (lb << 16);
+        const int2 pb = on ? sbod[wib][lane] : make_int2(-1, -1);
+        __syncwarp();
+        warp_local_slots(pb.x, pb.y, n, lx, ly, nb, fx, fy);
+        if (on) {
+            s.d_lbod[begin + lane] = lx | (ly << 16);
+            int32_t* ib = s.isl_bod + begin + isl;
+            if (pb.x >= 0 && fx == 2u * lane) ib[lx] = pb.x;
+            if (pb.y >= 0 && fy == 2u * lane + 1u) ib[ly] = pb.y;
         }
-        s.isl_nbod[isl] = nb;
+        if (lane == 0) s.isl_nbod[isl] = nb;
+        __syncwarp();
     }
 }
 
@@ -1359,7 +1404,7 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     // partitions by island size class, and row preparation: independent
     hook(kStPrep, st);
     fork_branches(br, st, 3);
-    k_partition<<<grid_for(s.desc_cap, 128, cap_blocks), 128, 0, st>>>(s, lvl_bound);
+    k_partition<<<grid_for(s.desc_cap, kPartWarps, 148u * 16u), kPartWarps * 32, 0, st>>>(s, lvl_bound);
     k_partition_smem<kMidIsland><<<grid_for(s.desc_cap, kSerialIsland + 1, 148u * 8u), 256,
                                    PartSmem<kMidIsland>::kBytes, side(0)>>>(s, lvl_bound, 0);
     k_partition_smem<kBigIsland><<<grid_for(s.desc_cap, kMidIsland + 1, 148u * 2u), 256,
