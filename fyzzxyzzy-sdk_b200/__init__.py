@@ -36,7 +36,7 @@ EXPORTS = (
     "fyzz_b200_read_step_counters", "fyzz_b200_set_contact_notifications",
     "fyzz_b200_contact_events", "fyzz_b200_rollout_begin", "fyzz_b200_rollout_forward",
     "fyzz_b200_rollout_backward", "fyzz_b200_read_mass_frames", "fyzz_b200_read_friction_anchors",
-    "fyzz_b200_fit_pair_budget",
+    "fyzz_b200_fit_pair_budget", "fyzz_b200_set_sleeping", "fyzz_b200_read_sleep_state",
 )
 STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 
@@ -132,6 +132,8 @@ def lib():
         L.fyzz_b200_kernels_per_step.argtypes = [vp, P(u32)]
         L.fyzz_b200_read_step_counters.argtypes = [vp, vp, u32]
         L.fyzz_b200_set_contact_notifications.argtypes = [vp, i32]
+        L.fyzz_b200_set_sleeping.argtypes = [vp, i32]
+        L.fyzz_b200_read_sleep_state.argtypes = [vp, vp, vp, vp, vp, u32]
         L.fyzz_b200_rollout_begin.argtypes = [vp, u32, u32]
         L.fyzz_b200_fit_pair_budget.argtypes = [vp, f32, P(u32)]
         L.fyzz_b200_rollout_forward.argtypes = [vp, f32]
@@ -346,6 +348,21 @@ class World:
         out = np.zeros(n, np.uint32)
         lib().fyzz_b200_read_levels(self.h, _p(out), n)
         return out
+
+    def set_sleeping(self, enabled: bool = True):
+        """Sleeping on (default, as in the reference scene) or off (wakes every body)."""
+        self._check(lib().fyzz_b200_set_sleeping(self.h, 1 if enabled else 0))
+
+    def sleep_state(self) -> dict:
+        """Per body: wake counter, flags (1 asleep, 2 ready), sleep-filter motion
+        (accumulated linear, body-local angular) and counted interactions."""
+        n = self.counts()["bodies"]
+        wake = np.zeros(n, np.float32)
+        flags = np.zeros(n, np.uint32)
+        motion = np.zeros((n, 6), np.float32)
+        counted = np.zeros(n, np.uint32)
+        self._check(lib().fyzz_b200_read_sleep_state(self.h, _p(wake), _p(flags), _p(motion), _p(counted), n))
+        return {"wake": wake, "flags": flags, "motion": motion, "counted": counted}
 
     def set_contact_notifications(self, enabled: bool = True):
         """WorldOptions::contact_notifications (reference world.h:61)."""

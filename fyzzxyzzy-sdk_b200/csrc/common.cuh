@@ -16,6 +16,8 @@ using std::isfinite;
 
 enum : uint32_t { kBox = 0, kSphere = 1, kPlane = 2 };
 enum : uint32_t { kBodyDynamic = 1u };
+// b_sleep bits
+enum : uint32_t { kSleeping = 1u, kReady = 2u };
 
 // Device error bits (published to the host after each step; the C ABI maps
 // them to status codes like the reference's task error words,

@@ -14,8 +14,9 @@
 //                            orientation (gu_order_reversed, 3276-3287)
 //                            disagrees with body order; impulses are the final
 //                            normal impulses of the solver rows, summed in
-//                            double precision
-// (Sleeping is not modelled, so every touching manager has an active body.)
+//                            double precision; a persisting touch is
+//                            reported only while one of its bodies is an
+//                            awake dynamic body (9201-9216)
 //
 // B200 mapping: both streams are already sorted by pair key, so each event
 // finds its slot in the merged list with one binary search in the other
@@ -72,21 +73,39 @@ __global__ void k_ev_lost_scatter(DevState s, const uint32_t* flags, const uint3
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < np; j += stride)
         if (flags[j]) s.ev_lost_key[pos[j]] = s.prev.key[j];
 }
-__global__ void k_ev_counts(DevState s) {
+__device__ __forceinline__ bool awake_dynamic(const DevState& s, uint32_t body) {
+    return (s.b_flags[body] & kBodyDynamic) && !(s.sleep && (s.b_sleep[body] & kSleeping));
+}
+// Touching managers with an event (rep, scanned into rep_pos) and their
+// point counts.
+__global__ void k_ev_counts(DevState s, uint32_t* rep) {
     const uint32_t nm = s.counters[kCntMan];
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < s.pair_cap; m += stride)
-        s.ev_cnt[m] = m < nm ? s.cur.count[s.man_list[m]] : 0u;
+    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < s.pair_cap; m += stride) {
+        bool on = false;
+        uint32_t count = 0u;
+        if (m < nm) {
+            const uint32_t k = s.man_list[m];
+            const uint64_t key = s.cur.key[k];
+            const int32_t pj = s.prev_idx[k];
+            const bool fresh = pj < 0 || s.prev.count[pj] == 0u;
+            on = fresh || awake_dynamic(s, s.s_body[uint32_t(key >> 32)]) || awake_dynamic(s, s.s_body[uint32_t(key)]);
+            count = on ? s.cur.count[k] : 0u;
+        }
+        rep[m] = on ? 1u : 0u;
+        s.ev_cnt[m] = count;
+    }
 }
-__global__ void k_ev_managers(DevState s) {
+__global__ void k_ev_managers(DevState s, const uint32_t* rep, const uint32_t* rep_pos) {
     const uint32_t nm = s.counters[kCntMan], nl = s.counters[kCntLost];
     EventRecord* ev = static_cast<EventRecord*>(s.ev);
     EventPoint* pts = static_cast<EventPoint*>(s.ev_pts);
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < nm; m += stride) {
+        if (!rep[m]) continue;
         const uint32_t k = s.man_list[m];
         const uint64_t key = s.cur.key[k];
-        const uint32_t slot = m + rank_below([&](uint32_t i) { return s.ev_lost_key[i]; }, nl, key);
+        const uint32_t slot = rep_pos[m] + rank_below([&](uint32_t i) { return s.ev_lost_key[i]; }, nl, key);
         const int32_t pj = s.prev_idx[k];
         EventRecord e;
         fill_bodies(s, key, e);
@@ -117,9 +136,9 @@ __global__ void k_ev_managers(DevState s) {
         ev[slot] = e;
     }
 }
-__global__ void k_ev_lost(DevState s) {
+__global__ void k_ev_lost(DevState s, const uint32_t* rep_pos) {
     const uint32_t nm = s.counters[kCntMan], nl = s.counters[kCntLost];
-    const uint32_t total_pts = s.counters[kCntEvPts];
+    const uint32_t total_pts = s.counters[kCntEvPts], total_rep = s.counters[kCntReported];
     EventRecord* ev = static_cast<EventRecord*>(s.ev);
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nl; l += stride) {
@@ -131,7 +150,7 @@ __global__ void k_ev_lost(DevState s) {
         e.count = 0u;
         e.point_offset = before < nm ? s.ev_pt_off[before] : total_pts;
         e.normal_impulse = 0.0;
-        ev[l + before] = e;
+        ev[l + (before < nm ? rep_pos[before] : total_rep)] = e;
     }
 }
 
@@ -148,11 +167,15 @@ void enqueue_events(const DevState& s, cudaStream_t st) {
     scan_exclusive(s.tmp_flags, s.tmp_pos, s.pair_cap, s.prev.n, s.counters + kCntLost, s.scan_tmp,
                    s.scan_tmp_words, st);
     k_ev_lost_scatter<<<blocks_for(s.pair_cap, T), T, 0, st>>>(s, s.tmp_flags, s.tmp_pos);
-    k_ev_counts<<<blocks_for(s.pair_cap, T), T, 0, st>>>(s);
+    // the lost-touch flags are consumed: tmp_flags / tmp_pos now hold the
+    // reported managers
+    k_ev_counts<<<blocks_for(s.pair_cap, T), T, 0, st>>>(s, s.tmp_flags);
+    scan_exclusive(s.tmp_flags, s.tmp_pos, s.pair_cap, s.counters + kCntMan, s.counters + kCntReported,
+                   s.scan_tmp, s.scan_tmp_words, st);
     scan_exclusive(s.ev_cnt, s.ev_pt_off, s.pair_cap, s.counters + kCntMan, s.counters + kCntEvPts,
                    s.scan_tmp, s.scan_tmp_words, st);
-    k_ev_managers<<<blocks_for(s.pair_cap, T), T, 0, st>>>(s);
-    k_ev_lost<<<blocks_for(s.pair_cap, T), T, 0, st>>>(s);
+    k_ev_managers<<<blocks_for(s.pair_cap, T), T, 0, st>>>(s, s.tmp_flags, s.tmp_pos);
+    k_ev_lost<<<blocks_for(s.pair_cap, T), T, 0, st>>>(s, s.tmp_pos);
 }
 
 }  // namespace fyzz::b200

@@ -37,17 +37,45 @@ __global__ void k_frame_begin(DevState s) {
     if (threadIdx.x == 0 && blockIdx.x == 0) s.counters[kCntFrame] += 1u;
 }
 
-// Unconstrained velocity + solver-body data for every dynamic body.
+__device__ __forceinline__ bool is_asleep(const DevState& s, uint32_t b) {
+    return s.sleep && (s.b_sleep[b] & kSleeping);
+}
+
+// Per-step resets of the body tables; counts the bodies asleep at the start
+// of the step.
 __global__ void k_bodies_begin(DevState s) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= s.n_bodies) return;
+    const bool on = b < s.n_bodies;
+    const bool asleep = on && is_dyn(s, b) && is_asleep(s, b);
+    const uint32_t am = __activemask();
+    const uint32_t votes = __ballot_sync(am, asleep);
+    if (votes && (threadIdx.x & 31u) == uint32_t(__ffs(am) - 1)) atomicAdd(&s.counters[kCntSleeping], __popc(votes));
+    if (!on) return;
     s.uf_parent[b] = b;
     s.sb_mask[b] = 0u;
     s.sb_maxdyn[b] = 0u;
     s.sb_static[b] = 0u;
     const float4 z = make_float4(0, 0, 0, 0);
     s.sb_dv[b] = z; s.sb_dw[b] = z; s.sb_mdv[b] = z; s.sb_mdw[b] = z;
-    if (!is_dyn(s, b)) return;
+    if (s.sleep) {
+        s.sl_act[b] = 0u;
+        s.sl_spec[b] = b;
+        s.sl_root[b] = 0u;
+        s.b_counted[b] = s.b_jcount[b];
+    }
+}
+
+// Unconstrained velocity + solver-body data for every awake dynamic body
+// (scene.cpp:10383 prepare_unconstrained_velocities skips sleeping actors).
+__global__ void k_bodies_velocity(DevState s) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= s.n_bodies || !is_dyn(s, b)) return;
+    if (is_asleep(s, b)) {
+        const float4 z = make_float4(0, 0, 0, 0);
+        s.sb_v[b] = z;
+        s.sb_w[b] = z;
+        return;
+    }
     const float dt = s.dt;
     const float gravity = -9.81f;
     const float4 d0 = s.b_dyn0[b];
@@ -118,12 +146,12 @@ __device__ uint32_t uf_find(uint32_t* parent, uint32_t x) {
     }
     return x;
 }
-__device__ void uf_union(const DevState& s, uint32_t a, uint32_t b) {
+__device__ void uf_union(const DevState& s, uint32_t* parent, uint32_t a, uint32_t b) {
     for (int it = 0; it < 4096; ++it) {
-        const uint32_t ra = uf_find(s.uf_parent, a), rb = uf_find(s.uf_parent, b);
+        const uint32_t ra = uf_find(parent, a), rb = uf_find(parent, b);
         if (ra == rb) return;
         const uint32_t hi = max(ra, rb), lo = min(ra, rb);
-        if (atomicCAS(&s.uf_parent[hi], hi, lo) == hi) return;
+        if (atomicCAS(&parent[hi], hi, lo) == hi) return;
     }
     atomicOr(s.err, kErrUnionFind);
 }
@@ -163,9 +191,13 @@ __global__ void k_union(DevState s) {
     for (uint32_t d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += stride) {
         int32_t b0, b1;
         desc_bodies(s, d, b0, b1);
-        if (b0 >= 0 && b1 >= 0) uf_union(s, uint32_t(b0), uint32_t(b1));
+        if (b0 >= 0 && b1 >= 0) uf_union(s, s.uf_parent, uint32_t(b0), uint32_t(b1));
     }
 }
+// Island key of every descriptor: the union-find root of its bodies.  The
+// descriptors of sleeping islands (every island is either awake or asleep
+// once the step's sleep decisions are made) take the key n_bodies, which
+// sorts them after every awake island; kCntAwake counts the others.
 __global__ void k_desc_keys(DevState s) {
     const uint32_t n = s.counters[kCntDesc];
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -173,19 +205,122 @@ __global__ void k_desc_keys(DevState s) {
         int32_t b0, b1;
         desc_bodies(s, d, b0, b1);
         const uint32_t body = b0 >= 0 ? uint32_t(b0) : uint32_t(b1);
-        s.d_key[d] = uf_find(s.uf_parent, body);
+        const bool asleep = is_asleep(s, body);
+        s.d_key[d] = asleep ? s.n_bodies : uf_find(s.uf_parent, body);
         s.d_val[d] = d;
         s.d_level[d] = kInvalid;
+        const uint32_t am = __activemask();
+        const uint32_t votes = __ballot_sync(am, !asleep);
+        if ((threadIdx.x & 31u) == uint32_t(__ffs(am) - 1)) atomicAdd(&s.counters[kCntAwake], __popc(votes));
     }
 }
+
+// ---------------- sleep ----------------
+// Reference behaviour (src/native/scene.cpp), per step:
+//   activate_published_islands 6148-6250: a newly found overlap pair of two
+//     dynamic bodies, at least one awake, marks both activating; a newly
+//     found touch marks its dynamic bodies activating and not ready for
+//     sleep; every sleeping body in the overlap-graph island of an
+//     activating body wakes (wake counter >= 0.4 s, sleep filters cleared)
+//   deactivate_ready_accurate_islands 6465-6530: an island of the touch and
+//     constraint graph whose bodies are all ready for sleep and not all
+//     asleep falls asleep (velocities and filters cleared, counter 0)
+//   integrate_solver_task 10640-10705: sleepCheck of every awake body after
+//     integration sets its wake counter and readiness for the next step
+//   change_counted_interactions 2728-2749: a body's counted interactions are
+//     its overlap pairs plus its constraints
+// Activation sees the overlap graph's islands as the previous step left
+// them (this step's lost pairs split them only afterwards, in the third
+// pass; this step's new pairs activate both of their bodies instead), so
+// they are rebuilt here, only when some body is asleep, as connected
+// components of the previous step's pairs and the constraints.  The touch
+// graph's islands are the solver's.
+
+// Counted interactions and activations.
+__global__ void k_sleep_pairs(DevState s) {
+    const uint32_t n = *s.cur.n;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+        const uint64_t key = s.cur.key[k];
+        const uint32_t ba = s.s_body[uint32_t(key >> 32)], bb = s.s_body[uint32_t(key)];
+        const bool da = is_dyn(s, ba), db = is_dyn(s, bb);
+        if (da) atomicAdd(&s.b_counted[ba], 1u);
+        if (db) atomicAdd(&s.b_counted[bb], 1u);
+        const int32_t pj = s.prev_idx[k];
+        const bool found = pj < 0;
+        const bool touch = s.cur.count[k] > 0u;
+        const bool touched = !found && s.prev.count[pj] > 0u;
+        if (found && da && db && (!is_asleep(s, ba) || !is_asleep(s, bb))) {
+            s.sl_act[ba] = 1u;
+            s.sl_act[bb] = 1u;
+        }
+        if (touch && !touched) {
+            if (da) { s.sl_act[ba] = 1u; atomicAnd(&s.b_sleep[ba], ~kReady); }
+            if (db) { s.sl_act[bb] = 1u; atomicAnd(&s.b_sleep[bb], ~kReady); }
+        }
+    }
+}
+// The overlap-graph union over the previous step's pairs.
+__global__ void k_sleep_spec(DevState s) {
+    if (s.counters[kCntSleeping] == 0u) return;
+    const uint32_t n = *s.prev.n;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        const uint64_t key = s.prev.key[j];
+        const uint32_t ba = s.s_body[uint32_t(key >> 32)], bb = s.s_body[uint32_t(key)];
+        if (is_dyn(s, ba) && is_dyn(s, bb)) uf_union(s, s.sl_spec, ba, bb);
+    }
+}
+__global__ void k_sleep_joints(DevState s) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= s.n_joints || s.counters[kCntSleeping] == 0u) return;
+    const uint32_t a = s.j_a[j], b = s.j_b[j];
+    if (is_dyn(s, a) && is_dyn(s, b)) uf_union(s, s.sl_spec, a, b);
+}
+constexpr uint32_t kRootWake = 1u, kRootUnready = 2u, kRootAwake = 4u;
+__global__ void k_sleep_wake_roots(DevState s) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= s.n_bodies || s.counters[kCntSleeping] == 0u || !s.sl_act[b]) return;
+    atomicOr(&s.sl_root[uf_find(s.sl_spec, b)], kRootWake);
+}
+__global__ void k_sleep_wake(DevState s) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= s.n_bodies || s.counters[kCntSleeping] == 0u || !is_dyn(s, b) || !is_asleep(s, b)) return;
+    if (!(s.sl_root[uf_find(s.sl_spec, b)] & kRootWake)) return;
+    s.b_sleep[b] = 0u;
+    s.b_wake[b] = smax(s.b_wake[b], 0.4f);
+    const float4 z = make_float4(0, 0, 0, 0);
+    s.b_sacc[2 * size_t(b)] = z;
+    s.b_sacc[2 * size_t(b) + 1] = z;
+}
+__global__ void k_sleep_island_flags(DevState s) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= s.n_bodies || !is_dyn(s, b)) return;
+    const uint32_t f = s.b_sleep[b];
+    const uint32_t bits = ((f & kReady) ? 0u : kRootUnready) | ((f & kSleeping) ? 0u : kRootAwake);
+    if (bits) atomicOr(&s.sl_root[uf_find(s.uf_parent, b)], bits);
+}
+__global__ void k_sleep_decide(DevState s) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= s.n_bodies || !is_dyn(s, b) || (s.b_sleep[b] & kSleeping)) return;
+    const uint32_t f = s.sl_root[uf_find(s.uf_parent, b)];
+    if ((f & kRootUnready) || !(f & kRootAwake)) return;
+    s.b_sleep[b] = kSleeping | kReady;
+    s.b_wake[b] = 0.0f;
+    const float4 z = make_float4(0, 0, 0, 0);
+    s.b_v[b] = z;
+    s.b_w[b] = z;
+    s.b_sacc[2 * size_t(b)] = z;
+    s.b_sacc[2 * size_t(b) + 1] = z;
+}
 __global__ void k_island_flags(DevState s) {
-    const uint32_t n = s.counters[kCntDesc];
+    const uint32_t n = s.counters[kCntAwake];
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
         s.isl_flag[i] = (i == 0 || s.d_key[i] != s.d_key[i - 1]) ? 1u : 0u;
 }
 __global__ void k_island_scatter(DevState s, const uint32_t* pos) {
-    const uint32_t n = s.counters[kCntDesc];
+    const uint32_t n = s.counters[kCntAwake];
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
         if (s.isl_flag[i]) s.isl_begin[pos[i]] = i;
@@ -789,6 +924,8 @@ __global__ void k_prep_contacts(DevState s) {
         const uint32_t a0 = s.s_body[sh0], a1 = s.s_body[sh1];
         const int32_t b0 = is_dyn(s, a0) ? int32_t(a0) : -1;
         const int32_t b1 = is_dyn(s, a1) ? int32_t(a1) : -1;
+        // managers of sleeping islands are not solved (their history stays)
+        if (is_asleep(s, uint32_t(b0 >= 0 ? b0 : b1))) continue;
         const SBody A = load_sbody(s, b0), B = load_sbody(s, b1);
         const float4 m0 = s.s_mat[sh0], m1 = s.s_mat[sh1];
         const float4 d0 = s.b_dyn1[a0], d1 = s.b_dyn1[a1];
@@ -1314,9 +1451,56 @@ __global__ void __launch_bounds__(256) k_pgs_block(DevState s, const uint32_t* l
     }
 }
 
+// Dy sleepCheck without stabilization (DySleep.cpp updateWakeCounter as the
+// reference restates it, scene.cpp:10640-10705): the motion velocities of
+// the step accumulate while the wake counter is low; enough accumulated
+// energy (scaled by the body's counted interactions) resets the counter,
+// otherwise it runs down; a body whose counter reached 0 is ready to sleep.
+__device__ void sleep_check(const DevState& s, uint32_t b, qt q, v3 ml, v3 mw) {
+    constexpr float kWakeReset = 20.0f * 0.02f;
+    constexpr float kEnergy = 5.0e-5f * 10.0f * 10.0f;
+    const float dt = s.dt;
+    float wc = s.b_wake[b];
+    float4* acc = s.b_sacc + 2 * size_t(b);
+    v3 lin = ld3(acc[0]), ang = ld3(acc[1]);
+    if (wc < kWakeReset * 0.5f || wc < dt) {
+        const v3 la = rotinv_sc(q, mw);
+        const v3 lacc = {lin.x + ml.x, lin.y + ml.y, lin.z + ml.z};
+        const v3 aacc = {ang.x + la.x, ang.y + la.y, ang.z + la.z};
+        if (!(vfinite(lacc) && vfinite(aacc))) atomicOr(s.err, kErrNonFinite);
+        const float4 inv = s.b_inv[b];
+        const v3 inertia = {inv.x > 0.0f ? 1.0f / inv.x : 1.0f, inv.y > 0.0f ? 1.0f / inv.y : 1.0f,
+                            inv.z > 0.0f ? 1.0f / inv.z : 1.0f};
+        const float angular = (aacc.x * aacc.x * inertia.x + aacc.y * aacc.y * inertia.y +
+                               aacc.z * aacc.z * inertia.z) * inv.w;
+        const float linear = lacc.x * lacc.x + lacc.y * lacc.y + lacc.z * lacc.z;
+        const float energy = 0.5f * (angular + linear);
+        const float cluster = 1.0f + float(s.b_counted[b]);
+        const float threshold = cluster * kEnergy;
+        if (energy >= threshold) {
+            lin = {0, 0, 0};
+            ang = {0, 0, 0};
+            const float factor = threshold == 0.0f ? 2.0f : smin(energy / threshold, 2.0f);
+            wc = factor * 0.5f * kWakeReset + dt * (cluster - 1.0f);
+        } else {
+            lin = lacc;
+            ang = aacc;
+            wc = smax(wc - dt, 0.0f);
+        }
+    } else {
+        wc = smax(wc - dt, 0.0f);
+    }
+    const bool ready = wc == 0.0f;
+    if (ready) { lin = {0, 0, 0}; ang = {0, 0, 0}; }
+    s.b_wake[b] = wc;
+    s.b_sleep[b] = ready ? kReady : 0u;
+    acc[0] = st4(lin, 0.0f);
+    acc[1] = st4(ang, 0.0f);
+}
+
 __global__ void k_integrate(DevState s) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= s.n_bodies || !is_dyn(s, b)) return;
+    if (b >= s.n_bodies || !is_dyn(s, b) || is_asleep(s, b)) return;
     const float dt = s.dt;
     const v3 v = ld3(s.sb_v[b]), w = ld3(s.sb_w[b]);
     const float4* si = s.sb_sqrt_i + 3 * size_t(b);
@@ -1344,6 +1528,21 @@ __global__ void k_integrate(DevState s) {
     s.b_q[b] = stq(q);
     s.b_v[b] = st4(fv, 0.0f);
     s.b_w[b] = st4(fw, 0.0f);
+    if (s.sleep) sleep_check(s, b, q, ml, mw);
+}
+
+// An authored velocity wakes every dynamic body it is written to
+// (scene.cpp:728-783): a sleeping body restarts with cleared filters.
+__global__ void k_wake_bodies(DevState s) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= s.n_bodies || !is_dyn(s, b)) return;
+    if (s.b_sleep[b] & kSleeping) {
+        const float4 z = make_float4(0, 0, 0, 0);
+        s.b_sacc[2 * size_t(b)] = z;
+        s.b_sacc[2 * size_t(b) + 1] = z;
+    }
+    s.b_wake[b] = smax(s.b_wake[b], 0.4f);
+    s.b_sleep[b] = 0u;
 }
 
 inline uint32_t grid_for(uint32_t n, uint32_t t, uint32_t cap) {
@@ -1367,6 +1566,10 @@ static void join_branches(const Branches* br, cudaStream_t st, int n) {
     }
 }
 
+void enqueue_wake_bodies(const DevState& s, cudaStream_t st) {
+    if (s.n_bodies) k_wake_bodies<<<grid_for(s.n_bodies, 256, 1u << 30), 256, 0, st>>>(s);
+}
+
 void init_solver_kernels() {
     cudaFuncSetAttribute(k_partition_smem<kBigIsland>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          int(PartSmem<kBigIsland>::kBytes));
@@ -1383,6 +1586,7 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     auto side = [&](int i) { return br ? br->st[i] : st; };
     hook(kStIslands, st);
     k_frame_begin<<<1, 32, 0, st>>>(s);
+    cudaMemsetAsync(s.counters + kCntAwake, 0, 2 * sizeof(uint32_t), st);
     k_bodies_begin<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
     // touching managers in canonical pair order
     k_touch_flags<<<grid_for(s.pair_cap, T, cap_blocks), T, 0, st>>>(s, flags);
@@ -1391,13 +1595,25 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     // islands
     k_desc_bodies<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     k_union<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
+    if (s.sleep) {
+        const uint32_t bb = grid_for(s.n_bodies, T, 1u << 30);
+        k_sleep_pairs<<<grid_for(s.pair_cap, T, cap_blocks), T, 0, st>>>(s);
+        k_sleep_spec<<<grid_for(s.pair_cap, T, cap_blocks), T, 0, st>>>(s);
+        if (s.n_joints) k_sleep_joints<<<grid_for(s.n_joints, T, 1u << 30), T, 0, st>>>(s);
+        k_sleep_wake_roots<<<bb, T, 0, st>>>(s);
+        k_sleep_wake<<<bb, T, 0, st>>>(s);
+        k_sleep_island_flags<<<bb, T, 0, st>>>(s);
+        k_sleep_decide<<<bb, T, 0, st>>>(s);
+    }
+    k_bodies_velocity<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
     k_desc_keys<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
+    // keys are island roots < n_bodies, or n_bodies for sleeping islands
     int bits = 1;
-    while ((1ull << bits) < s.n_bodies) ++bits;
+    while ((1ull << bits) < uint64_t(s.n_bodies) + 1u) ++bits;
     radix_sort_pairs(s.d_key, s.d_val, s.d_key2, s.d_val2, s.desc_cap, s.counters + kCntDesc, 0,
                      (bits + 7) / 8 * 8, s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st);
     k_island_flags<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
-    scan_exclusive(s.isl_flag, pos, s.desc_cap, s.counters + kCntDesc, s.n_isl, s.scan_tmp, s.scan_tmp_words, st);
+    scan_exclusive(s.isl_flag, pos, s.desc_cap, s.counters + kCntAwake, s.n_isl, s.scan_tmp, s.scan_tmp_words, st);
     k_island_scatter<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s, pos);
     cudaMemsetAsync(s.counters + kCntList, 0, 4 * sizeof(uint32_t), st);
     k_island_classes<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);

@@ -49,6 +49,16 @@ struct DevState {
     float4 *b_dyn1 = nullptr;          // max depenetration, max contact impulse, slop, unused
     uint32_t* b_flags = nullptr;
     uint32_t* b_scene = nullptr;
+    // sleep (Dy sleepCheck and the accurate island's deactivation)
+    float* b_wake = nullptr;           // wake counter, seconds
+    float4* b_sacc = nullptr;          // 2 per body: accumulated linear, local angular motion
+    uint32_t* b_sleep = nullptr;       // kSleeping | kReady
+    uint32_t* b_jcount = nullptr;      // distance constraints attached (counted interactions)
+    uint32_t* b_counted = nullptr;     // per step: overlap pairs + constraints
+    uint32_t* sl_act = nullptr;        // per step: activating this step
+    uint32_t* sl_spec = nullptr;       // per step: overlap-graph union-find parent
+    uint32_t* sl_root = nullptr;       // per step: flags of the union-find roots
+    bool sleep = true;                 // sleeping enabled for this step
 
     // shapes
     uint32_t *s_body = nullptr, *s_type = nullptr, *s_scene = nullptr;
@@ -223,6 +233,8 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook = 
 void enqueue_events(const DevState& s, cudaStream_t st);
 // Per-device kernel attributes (shared-memory limits); call with the device
 // current before the first step or capture.
+// Wakes every dynamic body (as an authored velocity on each would).
+void enqueue_wake_bodies(const DevState& s, cudaStream_t st);
 void init_solver_kernels();
 // Island size classes (descriptors per island).
 constexpr uint32_t kSmallIsland = 96;     // one warp
@@ -230,8 +242,9 @@ constexpr uint32_t kMidIsland = 512;      // one CTA, shared-memory deltas
 constexpr uint32_t kBigIsland = 4096;     // one CTA, shared-memory deltas (1 CTA / SM)
 // counters[] slots
 enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels = 4, kCntGjk = 5,
+             kCntAwake = 6 /* descriptors of awake islands */, kCntSleeping = 7 /* asleep at step start */,
              kCntList = 8 /* 4 island-class list lengths */, kCntLost = 12, kCntEvPts = 13,
-             kCntSlots = 16 };
+             kCntReported = 14 /* touching managers with an event */, kCntSlots = 16 };
 
 // Contact event records in device memory; the layouts of
 // fyzz_b200_contact_event_t and fyzz_b200_contact_event_point_t.

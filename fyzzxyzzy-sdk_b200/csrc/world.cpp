@@ -41,6 +41,17 @@ struct HostBody {
     std::array<float, 3> ml_p{0, 0, 0};
     std::array<float, 4> ml_q{0, 0, 0, 1};
     std::vector<uint32_t> shapes;   // attachment order
+    // sleep state (scene.h:1147-1153 Actor defaults)
+    float wake = 0.4f;
+    uint32_t sleep = 0;              // kSleeping | kReady
+    std::array<float, 6> sacc{};     // accumulated linear, local angular motion
+    // NpRigidDynamic wake on an authored velocity (scene.cpp:728-783): a
+    // sleeping body starts with cleared sleep filters.
+    void wake_up() {
+        if (sleep & kSleeping) sacc = {};
+        wake = std::max(wake, 0.4f);
+        sleep = 0;
+    }
 };
 struct HostShape {
     uint32_t body = 0, scene = 0, type = kBox;
@@ -348,6 +359,7 @@ public:
         if (!b.dynamic) throw std::logic_error("Static actors have no velocity");
         pull_state();
         (angular ? b.w : b.v) = {v[0], v[1], v[2]};
+        b.wake_up();
         mass_dirty_ = true;
     }
     uint64_t add_distance(uint32_t a, uint32_t b, float len) {
@@ -394,12 +406,17 @@ public:
         if (!uploaded_ || host_authoritative_) return;
         check_cuda(cudaSetDevice(device_), "cudaSetDevice");
         const size_t n = bodies_.size() < d_.n_bodies ? bodies_.size() : d_.n_bodies;
-        std::vector<float4> p(n), q(n), v(n), w(n);
+        std::vector<float4> p(n), q(n), v(n), w(n), acc(2 * n);
+        std::vector<float> wake(n);
+        std::vector<uint32_t> sl(n);
         if (n) {
             check_cuda(cudaMemcpyAsync(p.data(), d_.b_p, n * 16, cudaMemcpyDeviceToHost, stream_), "pull");
             check_cuda(cudaMemcpyAsync(q.data(), d_.b_q, n * 16, cudaMemcpyDeviceToHost, stream_), "pull");
             check_cuda(cudaMemcpyAsync(v.data(), d_.b_v, n * 16, cudaMemcpyDeviceToHost, stream_), "pull");
             check_cuda(cudaMemcpyAsync(w.data(), d_.b_w, n * 16, cudaMemcpyDeviceToHost, stream_), "pull");
+            check_cuda(cudaMemcpyAsync(wake.data(), d_.b_wake, n * 4, cudaMemcpyDeviceToHost, stream_), "pull");
+            check_cuda(cudaMemcpyAsync(sl.data(), d_.b_sleep, n * 4, cudaMemcpyDeviceToHost, stream_), "pull");
+            check_cuda(cudaMemcpyAsync(acc.data(), d_.b_sacc, n * 32, cudaMemcpyDeviceToHost, stream_), "pull");
             check_cuda(cudaStreamSynchronize(stream_), "pull sync");
         }
         for (size_t i = 0; i < n; ++i) {
@@ -409,6 +426,9 @@ public:
             b.q = {q[i].x, q[i].y, q[i].z, q[i].w};
             b.v = {v[i].x, v[i].y, v[i].z};
             b.w = {w[i].x, w[i].y, w[i].z};
+            b.wake = wake[i];
+            b.sleep = sl[i];
+            b.sacc = {acc[2 * i].x, acc[2 * i].y, acc[2 * i].z, acc[2 * i + 1].x, acc[2 * i + 1].y, acc[2 * i + 1].z};
         }
         host_authoritative_ = true;
     }
@@ -565,6 +585,7 @@ public:
     DevState framed(const Frame& f, int parity) const {
         DevState s = view(parity);
         s.dt = roll_dt_;
+        s.sleep = false;
         s.sb_v = f.sb_v; s.sb_w = f.sb_w; s.sb_dv = f.sb_dv; s.sb_dw = f.sb_dw;
         s.sb_mdv = f.sb_mdv; s.sb_mdw = f.sb_mdw; s.sb_sqrt_i = f.sb_sqrt_i;
         s.man_list = f.man_list; s.mh = f.mh; s.nrow = f.nrow; s.frow = f.frow; s.jrow = f.jrow;
@@ -590,6 +611,9 @@ public:
         pull_state();
         check_cuda(cudaStreamSynchronize(stream_), "sync");
         release_rollout();
+        // a differentiable rollout simulates every body: wake them all
+        enqueue_wake_bodies(d_, stream_);
+        check_cuda(cudaStreamSynchronize(stream_), "sync");
         roll_steps_ = steps;
         roll_every_ = every;
         roll_cap_ = d_.pair_cap;
@@ -625,6 +649,17 @@ public:
     void rollout_forward(float dt) {
         if (!roll_steps_) throw std::logic_error("rollout_begin must come first");
         roll_dt_ = dt;
+        // the forward runs without sleeping, like its recompute (framed())
+        struct SleepOff {
+            World& w;
+            explicit SleepOff(World& x) : w(x) { flip(false); }
+            ~SleepOff() { flip(w.sleep_enabled_); }
+            void flip(bool on) {
+                if (w.d_.sleep == on) return;
+                w.d_.sleep = on;
+                for (auto& g : w.graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+            }
+        } off(*this);
         for (uint32_t t0 = 0; t0 < roll_steps_; t0 += roll_every_) {
             save_slot(ckpt_[t0 / roll_every_]);
             step(dt, std::min(roll_every_, roll_steps_ - t0));
@@ -755,6 +790,50 @@ public:
     // ---------------- contact events ----------------
     // WorldOptions::contact_notifications (world.h:61).  Event buffers are
     // allocated only while notifications are on; the step graph is rebuilt.
+    // Sleeping (on by default, as in the reference scene).  Turning it off
+    // wakes every body.
+    void set_sleeping(bool on) {
+        check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+        if (on == sleep_enabled_) return;
+        if (uploaded_ && !host_authoritative_) {
+            if (!on) {
+                enqueue_wake_bodies(d_, stream_);
+                check_cuda(cudaStreamSynchronize(stream_), "sync");
+            }
+        } else {
+            for (auto& b : bodies_) if (!on && b.dynamic) b.wake_up();
+            mass_dirty_ = true;
+        }
+        sleep_enabled_ = on;
+        d_.sleep = on;
+        for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    }
+    bool sleeping_enabled() const { return sleep_enabled_; }
+    void read_sleep_state(float* wake, uint32_t* flags, float* motion6, uint32_t* counted, uint32_t n) {
+        if (n != bodies_.size()) throw std::invalid_argument("Body count mismatch");
+        if (!uploaded_ || host_authoritative_) {
+            for (uint32_t i = 0; i < n; ++i) {
+                const HostBody& b = bodies_[i];
+                if (wake) wake[i] = b.dynamic ? b.wake : 0.0f;
+                if (flags) flags[i] = b.dynamic ? b.sleep : 0u;
+                if (motion6) for (int k = 0; k < 6; ++k) motion6[6 * size_t(i) + k] = b.dynamic ? b.sacc[k] : 0.0f;
+                if (counted) counted[i] = 0u;
+            }
+            return;
+        }
+        std::vector<float4> acc(motion6 ? 2 * size_t(n) : 0);
+        if (wake) check_cuda(cudaMemcpyAsync(wake, d_.b_wake, size_t(n) * 4, cudaMemcpyDeviceToHost, stream_), "read");
+        if (flags) check_cuda(cudaMemcpyAsync(flags, d_.b_sleep, size_t(n) * 4, cudaMemcpyDeviceToHost, stream_), "read");
+        if (counted) check_cuda(cudaMemcpyAsync(counted, d_.b_counted, size_t(n) * 4, cudaMemcpyDeviceToHost, stream_), "read");
+        if (motion6) check_cuda(cudaMemcpyAsync(acc.data(), d_.b_sacc, size_t(n) * 32, cudaMemcpyDeviceToHost, stream_), "read");
+        check_cuda(cudaStreamSynchronize(stream_), "read sync");
+        if (motion6)
+            for (uint32_t i = 0; i < n; ++i) {
+                const float4 l = acc[2 * size_t(i)], a = acc[2 * size_t(i) + 1];
+                const float r[6] = {l.x, l.y, l.z, a.x, a.y, a.z};
+                std::memcpy(motion6 + 6 * size_t(i), r, sizeof r);
+            }
+    }
     void set_contact_notifications(bool on) {
         if (on == notify_) return;
         notify_ = on;
@@ -770,7 +849,7 @@ public:
             check_cuda(cudaStreamSynchronize(stream_), "sync");
             uint32_t h[kCntSlots] = {};
             check_cuda(cudaMemcpy(h, d_.counters, sizeof h, cudaMemcpyDeviceToHost), "read");
-            const uint64_t n_ev = uint64_t(h[kCntMan]) + h[kCntLost], n_pts = h[kCntEvPts];
+            const uint64_t n_ev = uint64_t(h[kCntReported]) + h[kCntLost], n_pts = h[kCntEvPts];
             h_ev_.resize(n_ev);
             h_ev_pts_.resize(n_pts);
             if (n_ev)
@@ -860,6 +939,8 @@ public:
         check_cuda(cudaMemcpyAsync(stage_.data() + n, d_.b_v, size_t(n) * 16, cudaMemcpyDeviceToHost, stream_), "read");
         check_cuda(cudaMemcpyAsync(stage_.data() + 2 * size_t(n), d_.b_q, size_t(n) * 16, cudaMemcpyDeviceToHost, stream_), "read");
         check_cuda(cudaMemcpyAsync(stage_.data() + 3 * size_t(n), d_.b_w, size_t(n) * 16, cudaMemcpyDeviceToHost, stream_), "read");
+        sleep_stage_.resize(n);
+        check_cuda(cudaMemcpyAsync(sleep_stage_.data(), d_.b_sleep, size_t(n) * 4, cudaMemcpyDeviceToHost, stream_), "read");
         check_cuda(cudaStreamSynchronize(stream_), "read sync");
         for (uint32_t i = 0; i < n; ++i) {
             float* o = out + 14 * size_t(i);
@@ -867,7 +948,8 @@ public:
             o[0] = p.x; o[1] = p.y; o[2] = p.z;
             o[3] = v.x; o[4] = v.y; o[5] = v.z;
             o[6] = q.x; o[7] = q.y; o[8] = q.z; o[9] = q.w;
-            o[10] = w.x; o[11] = w.y; o[12] = w.z; o[13] = 0.0f;
+            o[10] = w.x; o[11] = w.y; o[12] = w.z;
+            o[13] = (sleep_stage_[i] & kSleeping) ? 1.0f : 0.0f;
         }
     }
     void body_state(uint32_t id, fyzz_b200_body_state_t* out) {
@@ -877,20 +959,22 @@ public:
             pack_host(id, rec);
         } else {
             float4 t[4];
+            uint32_t sl = 0;
             check_cuda(cudaMemcpyAsync(&t[0], d_.b_p + id, 16, cudaMemcpyDeviceToHost, stream_), "read");
             check_cuda(cudaMemcpyAsync(&t[1], d_.b_v + id, 16, cudaMemcpyDeviceToHost, stream_), "read");
             check_cuda(cudaMemcpyAsync(&t[2], d_.b_q + id, 16, cudaMemcpyDeviceToHost, stream_), "read");
             check_cuda(cudaMemcpyAsync(&t[3], d_.b_w + id, 16, cudaMemcpyDeviceToHost, stream_), "read");
+            check_cuda(cudaMemcpyAsync(&sl, d_.b_sleep + id, 4, cudaMemcpyDeviceToHost, stream_), "read");
             check_cuda(cudaStreamSynchronize(stream_), "read sync");
             const float r[14] = {t[0].x, t[0].y, t[0].z, t[1].x, t[1].y, t[1].z, t[2].x, t[2].y, t[2].z, t[2].w,
-                                 t[3].x, t[3].y, t[3].z, 0.0f};
+                                 t[3].x, t[3].y, t[3].z, (sl & kSleeping) ? 1.0f : 0.0f};
             std::memcpy(rec, r, sizeof rec);
         }
         std::memcpy(out->position, rec, 12);
         std::memcpy(out->velocity, rec + 3, 12);
         std::memcpy(out->orientation, rec + 6, 16);
         std::memcpy(out->angular_velocity, rec + 10, 12);
-        out->sleeping = 0;
+        out->sleeping = rec[13] != 0.0f ? 1 : 0;
     }
     void write_velocities(const float* v6, uint32_t n) {
         if (n != bodies_.size()) throw std::invalid_argument("Body count mismatch");
@@ -904,6 +988,8 @@ public:
         }
         check_cuda(cudaMemcpyAsync(d_.b_v, stage_.data(), size_t(n) * 16, cudaMemcpyHostToDevice, stream_), "write");
         check_cuda(cudaMemcpyAsync(d_.b_w, stage_.data() + n, size_t(n) * 16, cudaMemcpyHostToDevice, stream_), "write");
+        enqueue_wake_bodies(d_, stream_);
+        check_cuda(cudaGetLastError(), "wake");
         check_cuda(cudaStreamSynchronize(stream_), "write sync");
     }
     void counts(uint64_t* out) {
@@ -1048,7 +1134,8 @@ private:
         o[0] = b.p[0]; o[1] = b.p[1]; o[2] = b.p[2];
         o[3] = b.v[0]; o[4] = b.v[1]; o[5] = b.v[2];
         o[6] = b.q[0]; o[7] = b.q[1]; o[8] = b.q[2]; o[9] = b.q[3];
-        o[10] = b.w[0]; o[11] = b.w[1]; o[12] = b.w[2]; o[13] = 0.0f;
+        o[10] = b.w[0]; o[11] = b.w[1]; o[12] = b.w[2];
+        o[13] = (b.dynamic && (b.sleep & kSleeping)) ? 1.0f : 0.0f;
     }
     DevState view(int parity) const {
         DevState s = d_;
@@ -1102,6 +1189,9 @@ private:
         check_cuda(cudaMemcpyAsync(bk_q_, d_.b_q, n, cudaMemcpyDeviceToDevice, stream_), "snapshot");
         check_cuda(cudaMemcpyAsync(bk_v_, d_.b_v, n, cudaMemcpyDeviceToDevice, stream_), "snapshot");
         check_cuda(cudaMemcpyAsync(bk_w_, d_.b_w, n, cudaMemcpyDeviceToDevice, stream_), "snapshot");
+        check_cuda(cudaMemcpyAsync(bk_wake_, d_.b_wake, n / 4, cudaMemcpyDeviceToDevice, stream_), "snapshot");
+        check_cuda(cudaMemcpyAsync(bk_sleep_, d_.b_sleep, n / 4, cudaMemcpyDeviceToDevice, stream_), "snapshot");
+        check_cuda(cudaMemcpyAsync(bk_sacc_, d_.b_sacc, 2 * n, cudaMemcpyDeviceToDevice, stream_), "snapshot");
         snap_parity_ = parity_;
         snap_last_ = last_cur_;
     }
@@ -1111,6 +1201,9 @@ private:
         check_cuda(cudaMemcpyAsync(d_.b_q, bk_q_, n, cudaMemcpyDeviceToDevice, stream_), "restore");
         check_cuda(cudaMemcpyAsync(d_.b_v, bk_v_, n, cudaMemcpyDeviceToDevice, stream_), "restore");
         check_cuda(cudaMemcpyAsync(d_.b_w, bk_w_, n, cudaMemcpyDeviceToDevice, stream_), "restore");
+        check_cuda(cudaMemcpyAsync(d_.b_wake, bk_wake_, n / 4, cudaMemcpyDeviceToDevice, stream_), "restore");
+        check_cuda(cudaMemcpyAsync(d_.b_sleep, bk_sleep_, n / 4, cudaMemcpyDeviceToDevice, stream_), "restore");
+        check_cuda(cudaMemcpyAsync(d_.b_sacc, bk_sacc_, 2 * n, cudaMemcpyDeviceToDevice, stream_), "restore");
         // contact-manager history is discarded, as after a reference rollback
         check_cuda(cudaMemsetAsync(sets_[0].n, 0, 4, stream_), "restore");
         check_cuda(cudaMemsetAsync(sets_[1].n, 0, 4, stream_), "restore");
@@ -1194,9 +1287,15 @@ private:
 
     void upload_bodies() {
         const uint32_t nb = uint32_t(bodies_.size());
-        std::vector<float4> p(nb), q(nb), v(nb), w(nb), inv(nb), mlp(nb), mlq(nb);
+        std::vector<float4> p(nb), q(nb), v(nb), w(nb), inv(nb), mlp(nb), mlq(nb), acc(2 * size_t(nb));
+        std::vector<float> wake(nb);
+        std::vector<uint32_t> sl(nb);
         for (uint32_t i = 0; i < nb; ++i) {
             const HostBody& b = bodies_[i];
+            wake[i] = b.wake;
+            sl[i] = b.dynamic ? b.sleep : 0u;
+            acc[2 * i] = make_float4(b.sacc[0], b.sacc[1], b.sacc[2], 0);
+            acc[2 * i + 1] = make_float4(b.sacc[3], b.sacc[4], b.sacc[5], 0);
             p[i] = make_float4(b.p[0], b.p[1], b.p[2], b.inv_mass);
             q[i] = make_float4(b.q[0], b.q[1], b.q[2], b.q[3]);
             v[i] = make_float4(b.v[0], b.v[1], b.v[2], 0);
@@ -1208,6 +1307,7 @@ private:
         upload(d_.b_p, p, stream_); upload(d_.b_q, q, stream_); upload(d_.b_v, v, stream_);
         upload(d_.b_w, w, stream_); upload(d_.b_inv, inv, stream_);
         upload(d_.b_ml_p, mlp, stream_); upload(d_.b_ml_q, mlq, stream_);
+        upload(d_.b_wake, wake, stream_); upload(d_.b_sleep, sl, stream_); upload(d_.b_sacc, acc, stream_);
         std::vector<float4> mat(shapes_.size());
         for (size_t i = 0; i < shapes_.size(); ++i)
             mat[i] = make_float4(shapes_[i].mat[0], shapes_[i].mat[1], shapes_[i].mat[2], shapes_[i].mat[3]);
@@ -1271,6 +1371,7 @@ private:
         }
         d.n_small = uint32_t(small.size());
         d.events = notify_;
+        d.sleep = sleep_enabled_;
         d_ = d;
         // allocations
         dalloc(d_.sc_fbegin, nsc + 1, owned_); dalloc(d_.sc_plane, nsc, owned_);
@@ -1279,7 +1380,11 @@ private:
         dalloc(d_.b_inv, nb, owned_); dalloc(d_.b_ml_p, nb, owned_); dalloc(d_.b_ml_q, nb, owned_);
         dalloc(d_.b_dyn0, nb, owned_); dalloc(d_.b_dyn1, nb, owned_);
         dalloc(d_.b_flags, nb, owned_); dalloc(d_.b_scene, nb, owned_);
+        dalloc(d_.b_wake, nb, owned_); dalloc(d_.b_sacc, 2 * size_t(nb), owned_); dalloc(d_.b_sleep, nb, owned_);
+        dalloc(d_.b_jcount, nb, owned_); dalloc(d_.b_counted, nb, owned_);
+        dalloc(d_.sl_act, nb, owned_); dalloc(d_.sl_spec, nb, owned_); dalloc(d_.sl_root, nb, owned_);
         dalloc(bk_p_, nb, owned_); dalloc(bk_q_, nb, owned_); dalloc(bk_v_, nb, owned_); dalloc(bk_w_, nb, owned_);
+        dalloc(bk_wake_, nb, owned_); dalloc(bk_sleep_, nb, owned_); dalloc(bk_sacc_, 2 * size_t(nb), owned_);
         dalloc(d_.s_body, ns, owned_); dalloc(d_.s_type, ns, owned_); dalloc(d_.s_scene, ns, owned_);
         dalloc(d_.s_geom, ns, owned_); dalloc(d_.s_lp, ns, owned_); dalloc(d_.s_lq, ns, owned_);
         dalloc(d_.s_mat, ns, owned_); dalloc(d_.s_wp, ns, owned_); dalloc(d_.s_wq, ns, owned_);
@@ -1331,6 +1436,13 @@ private:
         std::vector<uint32_t> ja(js.size()), jb(js.size());
         std::vector<float> jl(js.size());
         for (size_t i = 0; i < js.size(); ++i) { ja[i] = js[i].a; jb[i] = js[i].b; jl[i] = js[i].len; }
+        // constraints counted on their dynamic endpoints (scene.cpp:2728-2749)
+        std::vector<uint32_t> jcount(nb, 0u);
+        for (const auto& j : js) {
+            if (bodies_[j.a].dynamic) ++jcount[j.a];
+            if (bodies_[j.b].dynamic) ++jcount[j.b];
+        }
+        upload(d_.b_jcount, jcount, stream_);
         upload(d_.sc_fbegin, fbegin, stream_); upload(d_.sc_plane, plane, stream_);
         upload(d_.small_scenes, small, stream_);
         upload(d_.b_dyn0, dyn0, stream_); upload(d_.b_dyn1, dyn1, stream_);
@@ -1364,7 +1476,10 @@ private:
     DevState d_;
     ManagerSet sets_[2];
     std::vector<void*> owned_, pair_owned_;
-    float4 *bk_p_ = nullptr, *bk_q_ = nullptr, *bk_v_ = nullptr, *bk_w_ = nullptr;
+    float4 *bk_p_ = nullptr, *bk_q_ = nullptr, *bk_v_ = nullptr, *bk_w_ = nullptr, *bk_sacc_ = nullptr;
+    float* bk_wake_ = nullptr;
+    uint32_t* bk_sleep_ = nullptr;
+    bool sleep_enabled_ = true;
     cudaGraphExec_t graphs_[2] = {nullptr, nullptr};
     float graph_dt_ = -1.0f;
     int parity_ = 0, last_cur_ = 1, snap_parity_ = 0, snap_last_ = 1;
@@ -1398,6 +1513,7 @@ private:
         float4& operator[](size_t i) { return p[i]; }
         ~PinnedStage() { if (p) cudaFreeHost(p); }
     } stage_;
+    std::vector<uint32_t> sleep_stage_;
 };
 
 }  // namespace fyzz::b200
@@ -1607,6 +1723,13 @@ uint64_t fyzz_b200_read_sorted_min_x(fyzz_b200_world* w, uint32_t scene, uint32_
     uint64_t n = 0;
     if (guarded(w, [&](auto& W) { n = W.read_sorted_min_x(scene, values, ids, cap); })) return 0;
     return n;
+}
+int fyzz_b200_set_sleeping(fyzz_b200_world* w, int enabled) {
+    return guarded(w, [&](auto& W) { W.set_sleeping(enabled != 0); });
+}
+int fyzz_b200_read_sleep_state(fyzz_b200_world* w, float* wake, uint32_t* flags, float* motion6,
+                               uint32_t* counted, uint32_t n) {
+    return guarded(w, [&](auto& W) { W.read_sleep_state(wake, flags, motion6, counted, n); });
 }
 int fyzz_b200_set_contact_notifications(fyzz_b200_world* w, int enabled) {
     return guarded(w, [&](auto& W) { W.set_contact_notifications(enabled != 0); });

@@ -181,6 +181,26 @@ int fyzz_b200_contact_events(fyzz_b200_world* w, const fyzz_b200_contact_event_t
                              uint64_t* n_events, const fyzz_b200_contact_event_point_t** points,
                              uint64_t* n_points);
 
+/* ---- sleeping ----
+ * Bodies fall asleep and wake as in the reference scene: the sleep check
+ * after integration (scene.cpp:10640-10705), deactivation of touch-graph
+ * islands whose bodies are all ready (scene.cpp:6465-6530), waking on new
+ * overlaps and touches (scene.cpp:6148-6250) and on authored velocities
+ * (World::set_body_velocity / set_body_angular_velocity, world.h:459-460).
+ * A sleeping body keeps its pose, reports zero velocity and sleeping = 1 in
+ * its body state. */
+/* On by default, as in the reference, which has no switch (no counterpart).
+ * Turning it off wakes every body; differentiable rollouts always run with
+ * it off. */
+int fyzz_b200_set_sleeping(fyzz_b200_world* w, int enabled);
+/* Per body (n = body count), any pointer may be null: wake counter in
+ * seconds, flags (bit 0 asleep, bit 1 ready for sleep), the sleep filter's
+ * accumulated linear and body-local angular motion (6 floats) and the
+ * counted interactions (overlap pairs plus constraints) of the last step.
+ * No reference counterpart (Scene keeps these in its actors). */
+int fyzz_b200_read_sleep_state(fyzz_b200_world* w, float* wake, uint32_t* flags, float* motion6,
+                               uint32_t* counted, uint32_t n);
+
 /* ---- differentiable rollouts (no counterpart in the reference, which has
  *      no adjoint) ----
  * A rollout of `steps` steps of the current state with a full-state

@@ -34,6 +34,11 @@ typedef struct {
     float max_contact_impulse, max_depenetration, slop;
     float lin_damp, ang_damp, max_lin, max_ang;
     int pos_iters, vel_iters;
+    /* sleep state (scene.h:1147-1156) */
+    float wake;
+    v3 lin_acc, ang_acc;
+    int sleeping, ready;
+    uint32_t counted, joints;
 } actor_t;
 typedef struct {
     uint32_t body, type;
@@ -58,6 +63,8 @@ typedef struct {
     int reversed;              /* gu_order_reversed (scene.cpp:3275-3283) */
     fo_pcm_cache cache;
     int touching;              /* published manifold count > 0 */
+    uint8_t found_now;         /* overlap found this step */
+    uint8_t new_touch;         /* touching now, not the step before */
     uint8_t count;
     fo_point pts[4];
     /* friction history (prepared in the previous step) */
@@ -102,6 +109,7 @@ struct fo_scene {
     uint64_t* pend; uint64_t npend;
     double* impulses; uint64_t nimp;
     uint32_t* sorted_minx_val; uint32_t* sorted_minx_id; uint64_t nsorted;
+    int sleep;                 /* sleeping enabled */
 };
 
 /* ------------------------- setup ------------------------- */
@@ -261,7 +269,9 @@ fo_scene* fo_scene_create(uint32_t nb, const float* bodies, uint32_t ns,
         a->max_depenetration = 1.0e32f;
         a->lin_damp = 0.0f; a->ang_damp = 0.05f; a->max_lin = 1.0e16f; a->max_ang = 100.0f;
         a->pos_iters = 4; a->vel_iters = 1;
+        a->wake = 0.4f;
     }
+    s->sleep = 1;
     if (has_floor) {
         s->actors[0].p = V3(0, floor_height, 0);
         shape_t* f = &s->shapes[0];
@@ -311,6 +321,8 @@ fo_scene* fo_scene_create(uint32_t nb, const float* bodies, uint32_t ns,
         s->joint_a[j] = a < b ? a : b;   /* edge pair is ordered (scene.cpp:3154) */
         s->joint_b[j] = a < b ? b : a;
         s->joint_len[j] = joint_dist[j];
+        if (s->actors[a].dynamic) ++s->actors[a].joints;
+        if (s->actors[b].dynamic) ++s->actors[b].joints;
     }
     return s;
 }
@@ -434,10 +446,12 @@ static int collide(fo_scene* s) {
             const int a_static = !s->actors[A->body].dynamic;
             const int both = s->actors[A->body].dynamic && s->actors[B->body].dynamic;
             m->reversed = a_static || (both && A->body < B->body);
+            m->found_now = 1;
             s->found[s->nfound++] = pairs[k];
             ++k;
         } else {
             nm[k] = s->mgr[o];
+            nm[k].found_now = 0;
             ++o; ++k;
         }
     }
@@ -496,6 +510,7 @@ static int collide(fo_scene* s) {
             }
         m->count = (uint8_t)count;
         memcpy(m->pts, pts, sizeof(fo_point) * (size_t)count);
+        m->new_touch = count > 0 && !m->touching;
         m->touching = count > 0;
         if (count > 0) s->man[s->nman++] = i;
     }
@@ -511,7 +526,7 @@ static void pre_integrate(fo_scene* s, float dt) {
     const float gravity = -9.81f;
     for (uint32_t i = 0; i < s->na; ++i) {
         actor_t* a = &s->actors[i];
-        if (!a->dynamic) continue;
+        if (!a->dynamic || a->sleeping) continue;
         float vx = a->v.x, vy = a->v.y + gravity * dt, vz = a->v.z;
         const float lm = fmaxf_(1.0f - a->lin_damp * dt, 0.0f);
         vx *= lm; vy *= lm; vz *= lm;
@@ -587,23 +602,170 @@ typedef struct {
     uint32_t b0, b1;                /* actor ids of shape0 / shape1 */
 } mprep_t;
 
+/* ------------------------- sleep ------------------------- */
+/* Union-find with path halving; the smaller index becomes the root. */
+static uint32_t uf_root(uint32_t* p, uint32_t x) {
+    while (p[x] != x) { p[x] = p[p[x]]; x = p[x]; }
+    return x;
+}
+static void uf_join(uint32_t* p, uint32_t a, uint32_t b) {
+    a = uf_root(p, a); b = uf_root(p, b);
+    if (a < b) p[b] = a; else if (b < a) p[a] = b;
+}
+static void clear_sleep_filter(actor_t* a) { a->lin_acc = V3(0, 0, 0); a->ang_acc = V3(0, 0, 0); }
+/* Counted interactions (scene.cpp:2728-2749: overlap pairs and constraints
+ * on their dynamic bodies), activation (scene.cpp:6148-6250: a newly found
+ * overlap of two dynamic bodies, one awake, or a newly found touch marks its
+ * bodies activating -- the touch also clears readiness -- and every sleeping
+ * body in the overlap-graph island of an activating body wakes, the islands
+ * being those of the previous step's pairs) and
+ * deactivation (scene.cpp:6465-6530: an island of the touch and constraint
+ * graph whose bodies are all ready and not all asleep falls asleep). */
+static void sleep_islands(fo_scene* s) {
+    const uint32_t na = s->na;
+    for (uint32_t i = 0; i < na; ++i) s->actors[i].counted = s->actors[i].joints;
+    int any_asleep = 0;
+    for (uint32_t i = 0; i < na; ++i) any_asleep |= s->actors[i].dynamic && s->actors[i].sleeping;
+    uint8_t* act = (uint8_t*)calloc(na + 1, 1);
+    for (uint64_t i = 0; i < s->nmgr; ++i) {
+        const mgr_t* m = &s->mgr[i];
+        const uint32_t a = s->shapes[(uint32_t)(m->key >> 32)].body, b = s->shapes[(uint32_t)m->key].body;
+        actor_t* A = &s->actors[a];
+        actor_t* B = &s->actors[b];
+        if (A->dynamic) ++A->counted;
+        if (B->dynamic) ++B->counted;
+        if (m->found_now && A->dynamic && B->dynamic && (!A->sleeping || !B->sleeping)) act[a] = act[b] = 1;
+        if (m->new_touch) {
+            if (A->dynamic) { act[a] = 1; A->ready = 0; }
+            if (B->dynamic) { act[b] = 1; B->ready = 0; }
+        }
+    }
+    uint32_t* par = (uint32_t*)malloc(4 * (na + 1));
+    uint8_t* flag = (uint8_t*)calloc(na + 1, 1);
+    if (any_asleep) {
+        /* The overlap graph's islands as the previous step left them: its
+         * pairs (the kept and the lost ones of this step) and constraints.
+         * This step's lost pairs split them only after activation; its new
+         * pairs activate both of their bodies instead. */
+        for (uint32_t i = 0; i < na; ++i) par[i] = i;
+        for (uint64_t i = 0; i < s->nmgr + s->nlost; ++i) {
+            uint64_t key;
+            if (i < s->nmgr) {
+                if (s->mgr[i].found_now) continue;
+                key = s->mgr[i].key;
+            } else {
+                key = s->lost[i - s->nmgr];
+            }
+            const uint32_t a = s->shapes[(uint32_t)(key >> 32)].body, b = s->shapes[(uint32_t)key].body;
+            if (s->actors[a].dynamic && s->actors[b].dynamic) uf_join(par, a, b);
+        }
+        for (uint32_t j = 0; j < s->nj; ++j)
+            if (s->actors[s->joint_a[j]].dynamic && s->actors[s->joint_b[j]].dynamic)
+                uf_join(par, s->joint_a[j], s->joint_b[j]);
+        for (uint32_t i = 0; i < na; ++i)
+            if (act[i]) flag[uf_root(par, i)] = 1;
+        for (uint32_t i = 0; i < na; ++i) {
+            actor_t* a = &s->actors[i];
+            if (!a->dynamic || !a->sleeping || !flag[uf_root(par, i)]) continue;
+            a->sleeping = 0;
+            a->ready = 0;
+            a->wake = fmaxf_(a->wake, 0.4f);
+            clear_sleep_filter(a);
+        }
+    }
+    for (uint32_t i = 0; i < na; ++i) { par[i] = i; flag[i] = 0; }
+    for (uint64_t i = 0; i < s->nmgr; ++i) {
+        const mgr_t* m = &s->mgr[i];
+        if (!m->touching) continue;
+        const uint32_t a = s->shapes[(uint32_t)(m->key >> 32)].body, b = s->shapes[(uint32_t)m->key].body;
+        if (s->actors[a].dynamic && s->actors[b].dynamic) uf_join(par, a, b);
+    }
+    for (uint32_t j = 0; j < s->nj; ++j)
+        if (s->actors[s->joint_a[j]].dynamic && s->actors[s->joint_b[j]].dynamic)
+            uf_join(par, s->joint_a[j], s->joint_b[j]);
+    for (uint32_t i = 0; i < na; ++i) {
+        const actor_t* a = &s->actors[i];
+        if (!a->dynamic) continue;
+        const uint32_t r = uf_root(par, i);
+        if (!a->ready) flag[r] |= 1;
+        if (!a->sleeping) flag[r] |= 2;
+    }
+    for (uint32_t i = 0; i < na; ++i) {
+        actor_t* a = &s->actors[i];
+        if (!a->dynamic || a->sleeping || flag[uf_root(par, i)] != 2) continue;
+        a->sleeping = 1;
+        a->wake = 0.0f;
+        a->v = V3(0, 0, 0);
+        a->w = V3(0, 0, 0);
+        clear_sleep_filter(a);
+    }
+    free(act); free(par); free(flag);
+}
+/* Dy sleepCheck without stabilization (scene.cpp:10640-10705). */
+static void sleep_check(actor_t* a, qt q, v3 ml, v3 mw, float dt) {
+    const float wake_reset = 20.0f * 0.02f;
+    const float energy_threshold = 5.0e-5f * 10.0f * 10.0f;
+    float wc = a->wake;
+    if (wc < wake_reset * 0.5f || wc < dt) {
+        const v3 la = rotinv_sc(q, mw);
+        const v3 lacc = V3(a->lin_acc.x + ml.x, a->lin_acc.y + ml.y, a->lin_acc.z + ml.z);
+        const v3 aacc = V3(a->ang_acc.x + la.x, a->ang_acc.y + la.y, a->ang_acc.z + la.z);
+        const v3 ii = a->inv_inertia;
+        const v3 inertia = V3(ii.x > 0.0f ? 1.0f / ii.x : 1.0f, ii.y > 0.0f ? 1.0f / ii.y : 1.0f,
+                              ii.z > 0.0f ? 1.0f / ii.z : 1.0f);
+        const float angular = (aacc.x * aacc.x * inertia.x + aacc.y * aacc.y * inertia.y +
+                               aacc.z * aacc.z * inertia.z) * a->inv_mass;
+        const float linear = lacc.x * lacc.x + lacc.y * lacc.y + lacc.z * lacc.z;
+        const float energy = 0.5f * (angular + linear);
+        const float cluster = 1.0f + (float)a->counted;
+        const float threshold = cluster * energy_threshold;
+        if (energy >= threshold) {
+            clear_sleep_filter(a);
+            const float factor = threshold == 0.0f ? 2.0f : fminf_(energy / threshold, 2.0f);
+            wc = factor * 0.5f * wake_reset + dt * (cluster - 1.0f);
+        } else {
+            a->lin_acc = lacc;
+            a->ang_acc = aacc;
+            wc = fmaxf_(wc - dt, 0.0f);
+        }
+    } else {
+        wc = fmaxf_(wc - dt, 0.0f);
+    }
+    a->wake = wc;
+    a->ready = wc == 0.0f;
+    if (a->ready) clear_sleep_filter(a);
+}
+
 int fo_scene_step(fo_scene* s, float dt, const uint64_t* manager_order, uint64_t n_mgr,
                   const uint64_t* joint_order, uint64_t n_joint) {
     if (!isfinite(dt) || dt <= 0.0f) FAIL(FO_INVALID, "Native CPU timestep must be finite and positive");
     int rc = collide(s);
     if (rc) return rc;
+    if (s->sleep) sleep_islands(s);
     pre_integrate(s, dt);
     const float inv_dt = 1.0f / dt;
     /* ---- descriptor order (scene.cpp:7174-7216) ---- */
-    uint64_t nmo = manager_order ? n_mgr : s->nman;
-    uint64_t* mo = (uint64_t*)malloc(8 * (nmo + 1));
-    for (uint64_t i = 0; i < nmo; ++i) {
-        mo[i] = manager_order ? manager_order[i] : i;
-        if (mo[i] >= s->nman) { free(mo); FAIL(FO_LOGIC, "manager order out of range"); }
+    /* managers and joints of sleeping islands are not solved */
+#define ASLEEP(b) (s->actors[b].dynamic && s->actors[b].sleeping)
+    const uint64_t nmo_in = manager_order ? n_mgr : s->nman;
+    uint64_t nmo = 0;
+    uint64_t* mo = (uint64_t*)malloc(8 * (nmo_in + 1));
+    for (uint64_t i = 0; i < nmo_in; ++i) {
+        const uint64_t mi = manager_order ? manager_order[i] : i;
+        if (mi >= s->nman) { free(mo); FAIL(FO_LOGIC, "manager order out of range"); }
+        const uint64_t key = s->mgr[s->man[mi]].key;
+        if (ASLEEP(s->shapes[(uint32_t)(key >> 32)].body) || ASLEEP(s->shapes[(uint32_t)key].body)) continue;
+        mo[nmo++] = mi;
     }
-    uint64_t njo = joint_order ? n_joint : s->nj;
-    uint64_t* jo = (uint64_t*)malloc(8 * (njo + 1));
-    for (uint64_t i = 0; i < njo; ++i) jo[i] = joint_order ? joint_order[i] : (s->nj - 1 - i);
+    const uint64_t njo_in = joint_order ? n_joint : s->nj;
+    uint64_t njo = 0;
+    uint64_t* jo = (uint64_t*)malloc(8 * (njo_in + 1));
+    for (uint64_t i = 0; i < njo_in; ++i) {
+        const uint64_t ji = joint_order ? joint_order[i] : (s->nj - 1 - i);
+        if (ASLEEP(s->joint_a[ji]) || ASLEEP(s->joint_b[ji])) continue;
+        jo[njo++] = ji;
+    }
+#undef ASLEEP
     /* ---- solver body admission (scene.cpp:6940-7040) ---- */
     srow_t* rows = (srow_t*)calloc(s->na + 1, sizeof(srow_t));
     srow_t world;
@@ -1081,7 +1243,7 @@ int fo_scene_step(fo_scene* s, float dt, const uint64_t* manager_order, uint64_t
     }
     for (uint32_t i = 0; i < s->na; ++i) {
         actor_t* a = &s->actors[i];
-        if (!a->dynamic) continue;
+        if (!a->dynamic || a->sleeping) continue;
         v3 ml = a->v, mw = a->w;
         if (rows[i].admitted) {
             const srow_t* r = &rows[i];
@@ -1105,6 +1267,7 @@ int fo_scene_step(fo_scene* s, float dt, const uint64_t* manager_order, uint64_t
         p = V3(p.x - offv.x, p.y - offv.y, p.z - offv.z);
         a->p = p;
         a->q = q;
+        if (s->sleep) sleep_check(a, q, ml, mw, dt);
     }
 #undef ROW
     free(mo); free(jo); free(rows); free(d); free(part); free(pending); free(ordered);
@@ -1127,7 +1290,30 @@ void fo_scene_body_states(const fo_scene* s, float* out) {
         o[0] = a->p.x; o[1] = a->p.y; o[2] = a->p.z;
         o[3] = a->v.x; o[4] = a->v.y; o[5] = a->v.z;
         o[6] = a->q.x; o[7] = a->q.y; o[8] = a->q.z; o[9] = a->q.w;
-        o[10] = a->w.x; o[11] = a->w.y; o[12] = a->w.z; o[13] = 0.0f;
+        o[10] = a->w.x; o[11] = a->w.y; o[12] = a->w.z;
+        o[13] = a->dynamic && a->sleeping ? 1.0f : 0.0f;
+    }
+}
+void fo_scene_set_sleeping(fo_scene* s, int on) {
+    if (!on)
+        for (uint32_t i = 0; i < s->na; ++i) {
+            actor_t* a = &s->actors[i];
+            if (!a->dynamic) continue;
+            if (a->sleeping) clear_sleep_filter(a);
+            a->wake = fmaxf_(a->wake, 0.4f);
+            a->sleeping = a->ready = 0;
+        }
+    s->sleep = on;
+}
+/* Per actor: wake counter, sleeping, ready, counted interactions, linear and
+ * local angular filter motion = 10 floats. */
+void fo_scene_sleep_state(const fo_scene* s, float* out) {
+    for (uint32_t i = 0; i < s->na; ++i) {
+        const actor_t* a = &s->actors[i];
+        float* o = out + 10 * i;
+        o[0] = a->wake; o[1] = (float)a->sleeping; o[2] = (float)a->ready; o[3] = (float)a->counted;
+        o[4] = a->lin_acc.x; o[5] = a->lin_acc.y; o[6] = a->lin_acc.z;
+        o[7] = a->ang_acc.x; o[8] = a->ang_acc.y; o[9] = a->ang_acc.z;
     }
 }
 void fo_scene_set_body_states(fo_scene* s, const float* in) {

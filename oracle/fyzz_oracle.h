@@ -77,6 +77,11 @@ uint64_t fo_scene_manifolds(const fo_scene* s, uint32_t* pairs, uint32_t* counts
 uint64_t fo_scene_partitions(const fo_scene* s, uint32_t* desc4, uint64_t* ends);
 uint64_t fo_scene_normal_impulses(const fo_scene* s, double* out);
 uint64_t fo_scene_sorted_min_x(const fo_scene* s, uint32_t* values, uint32_t* ids);
+/* Sleeping on (default) or off (wakes every body). */
+void fo_scene_set_sleeping(fo_scene* s, int on);
+/* Per actor: wake counter, sleeping, ready, counted interactions, linear
+ * and local angular sleep-filter motion (10 floats). */
+void fo_scene_sleep_state(const fo_scene* s, float* out10);
 
 #ifdef __cplusplus
 }

@@ -43,6 +43,8 @@ def lib():
         L.fo_scene_partitions.argtypes = [vp, vp, vp]
         L.fo_scene_normal_impulses.restype = u64
         L.fo_scene_normal_impulses.argtypes = [vp, vp]
+        L.fo_scene_set_sleeping.argtypes = [vp, i32]
+        L.fo_scene_sleep_state.argtypes = [vp, vp]
         L.fo_scene_sorted_min_x.restype = u64
         L.fo_scene_sorted_min_x.argtypes = [vp, vp, vp]
         L.fo_encode_min.restype = u32
@@ -115,6 +117,17 @@ class OracleScene:
         out = np.zeros((self.counts()["actors"], 14), np.float32)
         lib().fo_scene_body_states(self.h, _p(out))
         return out
+
+    def set_sleeping(self, on: bool):
+        lib().fo_scene_set_sleeping(self.h, 1 if on else 0)
+
+    def sleep_state(self) -> dict:
+        """Per actor: wake counter, sleeping, ready, counted interactions and
+        the sleep filter's linear / local angular motion."""
+        out = np.zeros((self.counts()["actors"], 10), np.float32)
+        lib().fo_scene_sleep_state(self.h, _p(out))
+        return {"wake": out[:, 0], "sleeping": out[:, 1].astype(bool), "ready": out[:, 2].astype(bool),
+                "counted": out[:, 3].astype(np.uint32), "motion": out[:, 4:10]}
 
     def set_body_states(self, st: np.ndarray):
         st = np.ascontiguousarray(st, np.float32)

@@ -216,6 +216,24 @@ void fz_ref_body_states(void* p, float* out) {
     }
 }
 
+// Per actor: wake counter, sleeping, ready for sleep, counted interactions,
+// sleep-filter linear and local angular motion (scene.h:1147-1156) = 10
+// floats.
+void fz_ref_sleep_state(void* p, float* out) {
+    const Scene& s = *static_cast<Handle*>(p)->scene;
+    const auto& actors = Fix::actors(s);
+    for (std::size_t i = 0; i < actors.size(); ++i) {
+        const auto& a = actors[i];
+        float* o = out + 10 * i;
+        o[0] = a.wake_counter;
+        o[1] = a.sleeping ? 1.0f : 0.0f;
+        o[2] = a.ready_for_sleep ? 1.0f : 0.0f;
+        o[3] = static_cast<float>(a.num_counted_interactions);
+        o[4] = a.sleep_linear_acc.x; o[5] = a.sleep_linear_acc.y; o[6] = a.sleep_linear_acc.z;
+        o[7] = a.sleep_angular_acc.x; o[8] = a.sleep_angular_acc.y; o[9] = a.sleep_angular_acc.z;
+    }
+}
+
 // Per actor: inverse mass, inverse inertia(3), mass-local position(3),
 // mass-local orientation(4) = 11 floats.  Statics are zero-filled.
 void fz_ref_mass_props(void* p, float* out) {

@@ -37,6 +37,7 @@ def lib():
         L.fz_ref_counts.argtypes = [vp, vp]
         L.fz_ref_body_states.argtypes = [vp, vp]
         L.fz_ref_mass_props.argtypes = [vp, vp]
+        L.fz_ref_sleep_state.argtypes = [vp, vp]
         L.fz_ref_encoded_bounds.argtypes = [vp, vp]
         for name in ("fz_ref_endpoints",):
             getattr(L, name).restype = u64
@@ -120,6 +121,14 @@ class RefScene:
         out = np.zeros((n, 14), np.float32)
         lib().fz_ref_body_states(self.h, _p(out))
         return out
+
+    def sleep_state(self) -> dict:
+        """Per actor: wake counter, sleeping, ready, counted interactions and
+        the sleep filter's linear / local angular motion."""
+        out = np.zeros((self.counts()["actors"], 10), np.float32)
+        lib().fz_ref_sleep_state(self.h, _p(out))
+        return {"wake": out[:, 0], "sleeping": out[:, 1].astype(bool), "ready": out[:, 2].astype(bool),
+                "counted": out[:, 3].astype(np.uint32), "motion": out[:, 4:10]}
 
     def mass_props(self) -> np.ndarray:
         n = self.counts()["actors"]
