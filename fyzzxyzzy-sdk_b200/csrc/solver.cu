@@ -46,10 +46,15 @@ __device__ __forceinline__ bool is_asleep(const DevState& s, uint32_t b) {
 __global__ void k_bodies_begin(DevState s) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     const bool on = b < s.n_bodies;
-    const bool asleep = on && is_dyn(s, b) && is_asleep(s, b);
+    const bool dyn = on && is_dyn(s, b);
+    const bool asleep = dyn && is_asleep(s, b);
+    const bool ready = dyn && s.sleep && (s.b_sleep[b] & kReady);
     const uint32_t am = __activemask();
-    const uint32_t votes = __ballot_sync(am, asleep);
-    if (votes && (threadIdx.x & 31u) == uint32_t(__ffs(am) - 1)) atomicAdd(&s.counters[kCntSleeping], __popc(votes));
+    const uint32_t votes = __ballot_sync(am, asleep), ready_votes = __ballot_sync(am, ready);
+    if ((threadIdx.x & 31u) == uint32_t(__ffs(am) - 1)) {
+        if (votes) atomicAdd(&s.counters[kCntSleeping], __popc(votes));
+        if (ready_votes) atomicAdd(&s.counters[kCntReady], __popc(ready_votes));
+    }
     if (!on) return;
     s.uf_parent[b] = b;
     s.sb_mask[b] = 0u;
@@ -120,11 +125,17 @@ __global__ void k_bodies_velocity(DevState s) {
     si[0] = make_float4(xx, xy, xz, 0); si[1] = make_float4(xy, yy, yz, 0); si[2] = make_float4(xz, yz, zz, 0);
 }
 
+__device__ void sleep_pair(const DevState& s, uint32_t k, bool touch);
+// Touch flags of the current pairs; with sleeping on, also each pair's
+// counted interactions and activations (sleep_pair).
 __global__ void k_touch_flags(DevState s, uint32_t* flags) {
     const uint32_t n = *s.cur.n;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
-        flags[k] = s.cur.count[k] > 0u ? 1u : 0u;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+        const bool touch = s.cur.count[k] > 0u;
+        flags[k] = touch ? 1u : 0u;
+        if (s.sleep) sleep_pair(s, k, touch);
+    }
 }
 __global__ void k_touch_scatter(DevState s, const uint32_t* flags, const uint32_t* pos) {
     const uint32_t n = *s.cur.n;
@@ -135,23 +146,42 @@ __global__ void k_touch_scatter(DevState s, const uint32_t* flags, const uint32_
         s.counters[kCntDesc] = s.n_joints + s.counters[kCntMan];
 }
 
+// Lock-free union-find after ECL-CC (Jaiganesh and Burtscher, "A
+// high-performance connected components implementation for GPUs", HPDC
+// 2018): a root is hooked under the smaller root, so every parent index is
+// at most its child's and the root of a set is its smallest member; finds
+// shorten the path they walk (intermediate pointer jumping, plain stores:
+// a node that is not a root only ever gets an ancestor written); a failed
+// hook continues from the value it found instead of finding both roots
+// again.  Loads go through L1: a stale parent is still an ancestor (sets
+// only merge), a stale root fails its hook and the hook continues from the
+// value the atomic returns, and the root of a large set is then read from
+// each SM's L1 instead of by every thread from one L2 line.
 __device__ uint32_t uf_find(uint32_t* parent, uint32_t x) {
-    volatile uint32_t* vp = parent;
-    for (int it = 0; it < 1 << 20; ++it) {
-        const uint32_t p = vp[x];
-        if (p == x) return x;
-        const uint32_t gp = vp[p];
-        if (gp != p) atomicCAS(&parent[x], p, gp);
-        x = gp;
+    uint32_t cur = parent[x];
+    if (cur == x) return x;
+    uint32_t prev = x, next;
+    for (int it = 0; it < (1 << 24) && cur > (next = parent[cur]); ++it) {
+        parent[prev] = next;
+        prev = cur;
+        cur = next;
     }
-    return x;
+    return cur;
 }
 __device__ void uf_union(const DevState& s, uint32_t* parent, uint32_t a, uint32_t b) {
-    for (int it = 0; it < 4096; ++it) {
-        const uint32_t ra = uf_find(parent, a), rb = uf_find(parent, b);
+    uint32_t ra = uf_find(parent, a), rb = uf_find(parent, b);
+    // every failed hook moves one root strictly down, so this ends
+    for (int it = 0; it < (1 << 24); ++it) {
         if (ra == rb) return;
-        const uint32_t hi = max(ra, rb), lo = min(ra, rb);
-        if (atomicCAS(&parent[hi], hi, lo) == hi) return;
+        if (ra < rb) {
+            const uint32_t r = atomicCAS(&parent[rb], rb, ra);
+            if (r == rb) return;
+            rb = r;
+        } else {
+            const uint32_t r = atomicCAS(&parent[ra], ra, rb);
+            if (r == ra) return;
+            ra = r;
+        }
     }
     atomicOr(s.err, kErrUnionFind);
 }
@@ -230,79 +260,94 @@ __global__ void k_desc_keys(DevState s) {
 //   change_counted_interactions 2728-2749: a body's counted interactions are
 //     its overlap pairs plus its constraints
 // Activation sees the overlap graph's islands as the previous step left
-// them (this step's lost pairs split them only afterwards, in the third
-// pass; this step's new pairs activate both of their bodies instead), so
-// they are rebuilt here, only when some body is asleep, as connected
-// components of the previous step's pairs and the constraints.  The touch
-// graph's islands are the solver's.
+// them: the previous step's pairs and the constraints (this step's lost
+// pairs split them only afterwards, in the third pass).  They are rebuilt
+// here only when some body is asleep, on top of the touch graph's islands
+// of this step (its touching pairs and constraints): the touching pairs
+// that are new this step join two activating bodies, whose islands wake
+// either way, so adding them changes no wake.  What remains to join are the
+// previous step's pairs that do not touch now: the kept ones and the lost
+// ones, each joining the two touch-graph roots of its bodies.
 
-// Counted interactions and activations.
-__global__ void k_sleep_pairs(DevState s) {
-    const uint32_t n = *s.cur.n;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-        const uint64_t key = s.cur.key[k];
-        const uint32_t ba = s.s_body[uint32_t(key >> 32)], bb = s.s_body[uint32_t(key)];
-        const bool da = is_dyn(s, ba), db = is_dyn(s, bb);
-        if (da) atomicAdd(&s.b_counted[ba], 1u);
-        if (db) atomicAdd(&s.b_counted[bb], 1u);
-        const int32_t pj = s.prev_idx[k];
-        const bool found = pj < 0;
-        const bool touch = s.cur.count[k] > 0u;
-        const bool touched = !found && s.prev.count[pj] > 0u;
-        if (found && da && db && (!is_asleep(s, ba) || !is_asleep(s, bb))) {
-            s.sl_act[ba] = 1u;
-            s.sl_act[bb] = 1u;
-        }
-        if (touch && !touched) {
-            if (da) { s.sl_act[ba] = 1u; atomicAnd(&s.b_sleep[ba], ~kReady); }
-            if (db) { s.sl_act[bb] = 1u; atomicAnd(&s.b_sleep[bb], ~kReady); }
-        }
+// Counted interactions and activations of current pair k.
+__device__ void sleep_pair(const DevState& s, uint32_t k, bool touch) {
+    const uint64_t key = s.cur.key[k];
+    const uint32_t ba = s.s_body[uint32_t(key >> 32)], bb = s.s_body[uint32_t(key)];
+    const bool da = is_dyn(s, ba), db = is_dyn(s, bb);
+    if (da) atomicAdd(&s.b_counted[ba], 1u);
+    if (db) atomicAdd(&s.b_counted[bb], 1u);
+    const int32_t pj = s.prev_idx[k];
+    const bool found = pj < 0;
+    const bool touched = !found && s.prev.count[pj] > 0u;
+    if (found && da && db && (!is_asleep(s, ba) || !is_asleep(s, bb))) {
+        s.sl_act[ba] = 1u;
+        s.sl_act[bb] = 1u;
+    }
+    if (touch && !touched) {
+        if (da) { s.sl_act[ba] = 1u; atomicAnd(&s.b_sleep[ba], ~kReady); }
+        if (db) { s.sl_act[bb] = 1u; atomicAnd(&s.b_sleep[bb], ~kReady); }
     }
 }
-// The overlap-graph union over the previous step's pairs.
+// The overlap graph's union-find runs over touch-graph island roots: a
+// body's overlap-graph island is that of its touch-graph root.
+// Remaining pair i of the previous step (kept and not touching, or lost):
+// the touch-graph roots of its two dynamic bodies, or false.
+__device__ __forceinline__ bool spec_pair(const DevState& s, uint32_t i, uint32_t n, uint32_t& ra, uint32_t& rb) {
+    uint64_t key;
+    if (i < n) {
+        if (s.prev_idx[i] < 0 || s.cur.count[i] > 0u) return false;   // new, or joined already
+        key = s.cur.key[i];
+    } else {
+        if (!s.lost_flag[i - n]) return false;
+        key = s.prev.key[i - n];
+    }
+    const uint32_t ba = s.s_body[uint32_t(key >> 32)], bb = s.s_body[uint32_t(key)];
+    if (!is_dyn(s, ba) || !is_dyn(s, bb)) return false;
+    ra = uf_find(s.uf_parent, ba);
+    rb = uf_find(s.uf_parent, bb);
+    return ra != rb;
+}
 __global__ void k_sleep_spec(DevState s) {
     if (s.counters[kCntSleeping] == 0u) return;
-    const uint32_t n = *s.prev.n;
+    const uint32_t n = *s.cur.n, np = *s.prev.n;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
-        const uint64_t key = s.prev.key[j];
-        const uint32_t ba = s.s_body[uint32_t(key >> 32)], bb = s.s_body[uint32_t(key)];
-        if (is_dyn(s, ba) && is_dyn(s, bb)) uf_union(s, s.sl_spec, ba, bb);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n + np; i += stride) {
+        uint32_t ra, rb;
+        if (spec_pair(s, i, n, ra, rb)) uf_union(s, s.sl_spec, ra, rb);
     }
 }
-__global__ void k_sleep_joints(DevState s) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= s.n_joints || s.counters[kCntSleeping] == 0u) return;
-    const uint32_t a = s.j_a[j], b = s.j_b[j];
-    if (is_dyn(s, a) && is_dyn(s, b)) uf_union(s, s.sl_spec, a, b);
+__device__ __forceinline__ uint32_t spec_root(const DevState& s, uint32_t acc_root) {
+    return uf_find(s.sl_spec, acc_root);
 }
 constexpr uint32_t kRootWake = 1u, kRootUnready = 2u, kRootAwake = 4u;
 __global__ void k_sleep_wake_roots(DevState s) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= s.n_bodies || s.counters[kCntSleeping] == 0u || !s.sl_act[b]) return;
-    atomicOr(&s.sl_root[uf_find(s.sl_spec, b)], kRootWake);
+    atomicOr(&s.sl_root[spec_root(s, uf_find(s.uf_parent, b))], kRootWake);
 }
-__global__ void k_sleep_wake(DevState s) {
-    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= s.n_bodies || s.counters[kCntSleeping] == 0u || !is_dyn(s, b) || !is_asleep(s, b)) return;
-    if (!(s.sl_root[uf_find(s.sl_spec, b)] & kRootWake)) return;
-    s.b_sleep[b] = 0u;
-    s.b_wake[b] = smax(s.b_wake[b], 0.4f);
-    const float4 z = make_float4(0, 0, 0, 0);
-    s.b_sacc[2 * size_t(b)] = z;
-    s.b_sacc[2 * size_t(b) + 1] = z;
-}
-__global__ void k_sleep_island_flags(DevState s) {
+// Wakes the sleeping bodies of marked overlap-graph islands, then adds each
+// body's readiness and wakefulness to its touch-graph island's root (only
+// when some body could fall asleep: a body was ready at the step's start).
+__global__ void k_sleep_wake_flags(DevState s) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= s.n_bodies || !is_dyn(s, b)) return;
-    const uint32_t f = s.b_sleep[b];
+    uint32_t f = s.b_sleep[b];
+    const uint32_t root = uf_find(s.uf_parent, b);
+    if ((f & kSleeping) && s.counters[kCntSleeping] != 0u && (s.sl_root[spec_root(s, root)] & kRootWake)) {
+        f = 0u;
+        s.b_sleep[b] = 0u;
+        s.b_wake[b] = smax(s.b_wake[b], 0.4f);
+        const float4 z = make_float4(0, 0, 0, 0);
+        s.b_sacc[2 * size_t(b)] = z;
+        s.b_sacc[2 * size_t(b) + 1] = z;
+    }
+    if (s.counters[kCntReady] == 0u) return;
     const uint32_t bits = ((f & kReady) ? 0u : kRootUnready) | ((f & kSleeping) ? 0u : kRootAwake);
-    if (bits) atomicOr(&s.sl_root[uf_find(s.uf_parent, b)], bits);
+    if (bits) atomicOr(&s.sl_root[root], bits);
 }
 __global__ void k_sleep_decide(DevState s) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= s.n_bodies || !is_dyn(s, b) || (s.b_sleep[b] & kSleeping)) return;
+    if (b >= s.n_bodies || s.counters[kCntReady] == 0u || !is_dyn(s, b) || (s.b_sleep[b] & kSleeping)) return;
     const uint32_t f = s.sl_root[uf_find(s.uf_parent, b)];
     if ((f & kRootUnready) || !(f & kRootAwake)) return;
     s.b_sleep[b] = kSleeping | kReady;
@@ -1587,6 +1632,7 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     hook(kStIslands, st);
     k_frame_begin<<<1, 32, 0, st>>>(s);
     cudaMemsetAsync(s.counters + kCntAwake, 0, 2 * sizeof(uint32_t), st);
+    cudaMemsetAsync(s.counters + kCntReady, 0, sizeof(uint32_t), st);
     k_bodies_begin<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
     // touching managers in canonical pair order
     k_touch_flags<<<grid_for(s.pair_cap, T, cap_blocks), T, 0, st>>>(s, flags);
@@ -1597,12 +1643,9 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     k_union<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     if (s.sleep) {
         const uint32_t bb = grid_for(s.n_bodies, T, 1u << 30);
-        k_sleep_pairs<<<grid_for(s.pair_cap, T, cap_blocks), T, 0, st>>>(s);
-        k_sleep_spec<<<grid_for(s.pair_cap, T, cap_blocks), T, 0, st>>>(s);
-        if (s.n_joints) k_sleep_joints<<<grid_for(s.n_joints, T, 1u << 30), T, 0, st>>>(s);
+        k_sleep_spec<<<grid_for(2u * s.pair_cap, T, cap_blocks), T, 0, st>>>(s);
         k_sleep_wake_roots<<<bb, T, 0, st>>>(s);
-        k_sleep_wake<<<bb, T, 0, st>>>(s);
-        k_sleep_island_flags<<<bb, T, 0, st>>>(s);
+        k_sleep_wake_flags<<<bb, T, 0, st>>>(s);
         k_sleep_decide<<<bb, T, 0, st>>>(s);
     }
     k_bodies_velocity<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);

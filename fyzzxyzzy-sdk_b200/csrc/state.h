@@ -56,7 +56,7 @@ struct DevState {
     uint32_t* b_jcount = nullptr;      // distance constraints attached (counted interactions)
     uint32_t* b_counted = nullptr;     // per step: overlap pairs + constraints
     uint32_t* sl_act = nullptr;        // per step: activating this step
-    uint32_t* sl_spec = nullptr;       // per step: overlap-graph union-find parent
+    uint32_t* sl_spec = nullptr;       // per step: overlap-graph union-find parent (over touch-graph roots)
     uint32_t* sl_root = nullptr;       // per step: flags of the union-find roots
     bool sleep = true;                 // sleeping enabled for this step
 
@@ -244,7 +244,8 @@ constexpr uint32_t kBigIsland = 4096;     // one CTA, shared-memory deltas (1 CT
 enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels = 4, kCntGjk = 5,
              kCntAwake = 6 /* descriptors of awake islands */, kCntSleeping = 7 /* asleep at step start */,
              kCntList = 8 /* 4 island-class list lengths */, kCntLost = 12, kCntEvPts = 13,
-             kCntReported = 14 /* touching managers with an event */, kCntSlots = 16 };
+             kCntReported = 14 /* touching managers with an event */,
+             kCntReady = 15 /* ready for sleep at step start */, kCntSlots = 16 };
 
 // Contact event records in device memory; the layouts of
 // fyzz_b200_contact_event_t and fyzz_b200_contact_event_point_t.

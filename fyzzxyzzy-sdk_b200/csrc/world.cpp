@@ -1108,7 +1108,7 @@ public:
         return c.desc;
     }
     void read_step_counters(uint32_t* out, uint32_t n) {
-        if (n > uint32_t(kCntSlots)) throw std::invalid_argument("At most 16 counters");
+        if (n > uint32_t(kCntSlots)) throw std::invalid_argument("At most kCntSlots counters");
         if (!uploaded_) { for (uint32_t i = 0; i < n; ++i) out[i] = 0; return; }
         check_cuda(cudaStreamSynchronize(stream_), "sync");
         check_cuda(cudaMemcpy(out, d_.counters, size_t(n) * 4, cudaMemcpyDeviceToHost), "read");
