@@ -1597,6 +1597,27 @@ inline uint32_t grid_for(uint32_t n, uint32_t t, uint32_t cap) {
 
 }  // namespace
 
+// The largest islands set the critical path of the partition and PGS
+// stages: their one-CTA-per-island kernels launch with the device's highest
+// priority so their CTAs take SMs before the many small-island blocks of
+// the concurrent branches (graphs are instantiated with node priorities).
+static int g_high_priority = 0;
+template <class... KArgs, class... Args>
+static void launch_high(void (*kernel)(KArgs...), uint32_t grid, uint32_t block, size_t smem, cudaStream_t st,
+                        Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributePriority;
+    attr[0].val.priority = g_high_priority;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // Fork n side branches off st (or run everything on st without branches).
 static void fork_branches(const Branches* br, cudaStream_t st, int n) {
     if (!br) return;
@@ -1616,6 +1637,8 @@ void enqueue_wake_bodies(const DevState& s, cudaStream_t st) {
 }
 
 void init_solver_kernels() {
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess) g_high_priority = greatest;
     cudaFuncSetAttribute(k_partition_smem<kBigIsland>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          int(PartSmem<kBigIsland>::kBytes));
     cudaFuncSetAttribute(k_pgs_block_smem<kBigIsland, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1663,25 +1686,26 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     // partitions by island size class, and row preparation: independent
     hook(kStPrep, st);
     fork_branches(br, st, 3);
+    launch_high(k_partition_smem<kBigIsland>, grid_for(s.desc_cap, kMidIsland + 1, 148u * 2u), 256u,
+                PartSmem<kBigIsland>::kBytes, side(1), s, lvl_bound, 2);
+    launch_high(k_partition_large, grid_for(s.desc_cap, kBigIsland + 1, 148u), 256u, size_t(0), side(1), s,
+                lvl_bound);
     k_partition<<<grid_for(s.desc_cap, kPartWarps, 148u * 16u), kPartWarps * 32, 0, st>>>(s, lvl_bound);
     k_partition_smem<kMidIsland><<<grid_for(s.desc_cap, kSerialIsland + 1, 148u * 8u), 256,
                                    PartSmem<kMidIsland>::kBytes, side(0)>>>(s, lvl_bound, 0);
-    k_partition_smem<kBigIsland><<<grid_for(s.desc_cap, kMidIsland + 1, 148u * 2u), 256,
-                                   PartSmem<kBigIsland>::kBytes, side(1)>>>(s, lvl_bound, 2);
-    k_partition_large<<<grid_for(s.desc_cap, kBigIsland + 1, 148u), 256, 0, side(1)>>>(s, lvl_bound);
     if (s.n_joints) k_prep_joints<<<grid_for(s.n_joints, T, 1u << 30), T, 0, side(2)>>>(s);
     k_prep_contacts<<<grid_for(s.desc_cap, 128, cap_blocks), 128, 0, side(2)>>>(s);
     join_branches(br, st, 3);
     // PGS: islands by size class, independent
     hook(kStPgs, st);
     fork_branches(br, st, 2);
+    launch_high(k_pgs_block_smem<kBigIsland, 256>, grid_for(s.desc_cap, kMidIsland + 1, 148u), 256u,
+                PgsSmem<kBigIsland>::kBytes, side(1), s, lvl_bound, 2);
+    launch_high(k_pgs_block, grid_for(s.desc_cap, kBigIsland + 1, 148u), 256u, size_t(0), side(1), s, lvl_bound);
     k_pgs_warp<<<grid_for(s.desc_cap * 32u, kPgsWarpsPerBlock * 32u, 148u * 3u), kPgsWarpsPerBlock * 32u, 0, st>>>(
         s, lvl_bound);
     k_pgs_block_smem<kMidIsland, 128><<<grid_for(s.desc_cap, kSmallIsland + 1, 148u * 3u), 128,
                                         PgsSmem<kMidIsland>::kBytes, side(0)>>>(s, lvl_bound, 1);
-    k_pgs_block_smem<kBigIsland, 256><<<grid_for(s.desc_cap, kMidIsland + 1, 148u), 256,
-                                        PgsSmem<kBigIsland>::kBytes, side(1)>>>(s, lvl_bound, 2);
-    k_pgs_block<<<grid_for(s.desc_cap, kBigIsland + 1, 148u), 256, 0, side(1)>>>(s, lvl_bound);
     join_branches(br, st, 2);
     hook(kStIntegrate, st);
     k_integrate<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);

@@ -1175,7 +1175,9 @@ private:
                     if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++kernels;
                 }
                 kernels_per_step_ = kernels;
-                check_cuda(cudaGraphInstantiate(&graphs_[parity_], g, 0), "instantiate");
+                // kernel-node priorities (the largest islands' kernels) are honoured
+                check_cuda(cudaGraphInstantiateWithFlags(&graphs_[parity_], g, cudaGraphInstantiateFlagUseNodePriority),
+                           "instantiate");
                 cudaGraphDestroy(g);
             }
             check_cuda(cudaGraphLaunch(graphs_[parity_], stream_), "graph launch");
