@@ -1365,8 +1365,41 @@ __device__ __forceinline__ void island_deltas_out(float4* dst_v, float4* dst_w, 
     }
 }
 
-// One warp per small island (<= kSmallIsland descriptors, so <= 97 bodies):
-// the island's deltas live in this warp's slice of shared memory.
+// One thread per tiny island (<= kTinyIsland descriptors): the island's
+// placed descriptors are solved in order (level by level, the order the
+// wider kernels use, since a level's descriptors share no body) with the
+// deltas in the thread's slice of shared memory.  Tiny islands (a body
+// resting alone, a short chain) are most islands of a spread-out scene; a
+// warp each would leave 31 lanes idle for all five passes.
+constexpr uint32_t kTinyIsland = 4;
+constexpr uint32_t kPgsThreadBlock = 128;
+__global__ void __launch_bounds__(kPgsThreadBlock) k_pgs_thread(DevState s) {
+    __shared__ float4 sh[kPgsThreadBlock][2][kTinyIsland + 1];
+    const uint32_t ni = *s.n_isl;
+    const int pos = s.pos_iters, vel = s.vel_iters < 1 ? 1 : s.vel_iters;
+    float4* sdv = sh[threadIdx.x][0];
+    float4* sdw = sh[threadIdx.x][1];
+    const LocalDeltas D{sdv, sdw};
+    const float4 zero = make_float4(0, 0, 0, 0);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < ni; isl += stride) {
+        const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
+        if (end - begin > kTinyIsland) continue;
+        const uint32_t nb = s.isl_nbod[isl];
+        const int32_t* ib = s.isl_bod + begin + isl;
+        for (uint32_t l = 0; l < nb; ++l) { sdv[l] = zero; sdw[l] = zero; }
+        for (int it = 0; it < pos + vel; ++it) {
+            for (uint32_t i = begin; i < end; ++i)
+                solve_desc<LocalDeltas, false>(s, s.d_val2[i], s.d_lbod[i], it, pos, vel, D);
+            if (it + 1 == pos) island_deltas_out(s.sb_mdv, s.sb_mdw, ib, nb, sdv, sdw, 0u, 1u);
+        }
+        island_deltas_out(s.sb_dv, s.sb_dw, ib, nb, sdv, sdw, 0u, 1u);
+    }
+}
+
+// One warp per small island (kTinyIsland < descriptors <= kSmallIsland, so
+// <= 97 bodies): the island's deltas live in this warp's slice of shared
+// memory.
 constexpr uint32_t kWarpBodies = kSmallIsland + 1;
 constexpr uint32_t kPgsWarpsPerBlock = 4;
 __global__ void __launch_bounds__(kPgsWarpsPerBlock * 32, 3) k_pgs_warp(DevState s, const uint32_t* lvl_bound) {
@@ -1385,7 +1418,7 @@ __global__ void __launch_bounds__(kPgsWarpsPerBlock * 32, 3) k_pgs_warp(DevState
     const float4 zero = make_float4(0, 0, 0, 0);
     for (uint32_t isl = warp; isl < ni; isl += nwarps) {
         const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
-        if (end - begin > kSmallIsland) continue;
+        if (end - begin > kSmallIsland || end - begin <= kTinyIsland) continue;
         const uint32_t nlev = s.isl_end[isl];
         const uint32_t nb = s.isl_nbod[isl];
         const int32_t* ib = s.isl_bod + begin + isl;
@@ -1698,7 +1731,7 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     join_branches(br, st, 3);
     // PGS: islands by size class, independent
     hook(kStPgs, st);
-    fork_branches(br, st, 2);
+    fork_branches(br, st, 3);
     launch_high(k_pgs_block_smem<kBigIsland, 256>, grid_for(s.desc_cap, kMidIsland + 1, 148u), 256u,
                 PgsSmem<kBigIsland>::kBytes, side(1), s, lvl_bound, 2);
     launch_high(k_pgs_block, grid_for(s.desc_cap, kBigIsland + 1, 148u), 256u, size_t(0), side(1), s, lvl_bound);
@@ -1706,7 +1739,8 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
         s, lvl_bound);
     k_pgs_block_smem<kMidIsland, 128><<<grid_for(s.desc_cap, kSmallIsland + 1, 148u * 3u), 128,
                                         PgsSmem<kMidIsland>::kBytes, side(0)>>>(s, lvl_bound, 1);
-    join_branches(br, st, 2);
+    k_pgs_thread<<<grid_for(s.desc_cap, kPgsThreadBlock, 148u * 8u), kPgsThreadBlock, 0, side(2)>>>(s);
+    join_branches(br, st, 3);
     hook(kStIntegrate, st);
     k_integrate<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
     if (s.events) enqueue_events(s, st);
