@@ -1371,7 +1371,7 @@ __device__ __forceinline__ void island_deltas_out(float4* dst_v, float4* dst_w, 
 // deltas in the thread's slice of shared memory.  Tiny islands (a body
 // resting alone, a short chain) are most islands of a spread-out scene; a
 // warp each would leave 31 lanes idle for all five passes.
-constexpr uint32_t kTinyIsland = 4;
+constexpr uint32_t kTinyIsland = 8;
 constexpr uint32_t kPgsThreadBlock = 128;
 __global__ void __launch_bounds__(kPgsThreadBlock) k_pgs_thread(DevState s) {
     __shared__ float4 sh[kPgsThreadBlock][2][kTinyIsland + 1];
