@@ -90,7 +90,7 @@ __device__ __forceinline__ float4 stq(qt q) { return make_float4(q.x, q.y, q.z, 
 // carried from frame to frame by pair identity.
 // PcmPersistentContact / PcmManifoldCache (scene.h:1444-1459).
 struct PcmPoint { float la[3], lb[3], nb[3], sep; };
-struct PcmCache {
+struct alignas(16) PcmCache {
     PcmPoint pts[4];
     float rel_p[3], rel_q[4], qa[4], qb[4];
     uint32_t meta;  // bits 0-7 count, bit 8 initialized
@@ -98,7 +98,7 @@ struct PcmCache {
 static_assert(sizeof(PcmCache) == 224, "PcmCache layout");
 // One retained friction patch (FrictionPatch, scene.h:1588-1614) plus the
 // epoch of the step that prepared it (friction_by_edge_, scene.cpp:8082).
-struct FrictionHist {
+struct alignas(16) FrictionHist {
     float n0[3], n1[3];
     float a0[2][3], a1[2][3];
     float sf, df, rest, damping;
@@ -109,30 +109,32 @@ struct FrictionHist {
 };
 static_assert(sizeof(FrictionHist) == 96, "FrictionHist layout");
 // ContactPoint (scene.h:510-514), four slots per manager.
-struct ContactPt { float p[3], n[3], sep; };
+struct alignas(16) ContactPt { float p[3], n[3], sep; };
 
+// Records are 16-byte aligned so that whole-record copies move as 128-bit
+// loads and stores.
 // Solver rows.  SolverContactPoint (scene.h:1561-1576) without the
 // per-point patch index (one patch per manager for the supported shapes).
-struct NormalRow {
+struct alignas(16) NormalRow {
     float n[3], ra[3], rb[3];
     float vel_mult, imp_mult, biased, unbiased, applied, max_impulse, pad;
 };
 static_assert(sizeof(NormalRow) == 64, "NormalRow layout");
 // SolverContactFriction (scene.h:1622-1630)
-struct FrictionRow {
+struct alignas(16) FrictionRow {
     float t[3], ra[3], rb[3];
     float vel_mult, bias, target, applied, pad[3];
 };
 static_assert(sizeof(FrictionRow) == 64, "FrictionRow layout");
 // JointRow (scene.h:1983-1990)
-struct JointRow {
+struct alignas(16) JointRow {
     float axis[3], ang_a[3], ang_b[3];
     float ima, imb, constant, unbiased, vel_mult, applied, pad;
 };
 static_assert(sizeof(JointRow) == 64, "JointRow layout");
 // Per-manager solver header: bodies (-1 = static world), counts and the
 // combined friction coefficients.
-struct ManagerHeader {
+struct alignas(16) ManagerHeader {
     int32_t b0, b1;
     uint32_t count, anchors;
     float sf, df, ima, imb;    // friction coefficients, inverse masses
