@@ -251,12 +251,27 @@ __device__ __forceinline__ void rel_adj(v3 n, v3 ra, v3 rb, v3 av, v3 aw, v3 bv,
     g.rb = vsub(g.rb, vmul(bw, gb));
 }
 
+// Adds a row-gradient increment to its accumulator with 128-bit accesses
+// (the row records are 16-byte aligned; fields the increment leaves at 0
+// are unchanged).
+template <class T> __device__ __forceinline__ void add_row(T& dst, const T& inc) {
+    static_assert(sizeof(T) % 16 == 0 && alignof(T) == 16, "16-byte row record");
+    float4* d = reinterpret_cast<float4*>(&dst);
+    const float4* a = reinterpret_cast<const float4*>(&inc);
+#pragma unroll
+    for (int k = 0; k < int(sizeof(T) / 16); ++k) {
+        float4 x = d[k];
+        const float4 y = a[k];
+        x.x += y.x; x.y += y.y; x.z += y.z; x.w += y.w;
+        d[k] = x;
+    }
+}
 template <class R>
 __device__ void reverse_desc(const DevState& s, const AdjState& A, uint32_t d, uint32_t lid, int it, int pos,
                              const R& D) {
     const size_t cap = s.pair_cap;
     if (d < s.n_joints) {
-        const JointRow& r = s.jrow[d];
+        const JointRow r = s.jrow[d];
         int32_t b0, b1;
         if constexpr (R::kLocal) {
             b0 = local_handle(lid & 0xffffu); b1 = local_handle(lid >> 16);
@@ -276,13 +291,14 @@ __device__ void reverse_desc(const DevState& s, const AdjState& A, uint32_t d, u
         const float nd = vdot(ax, vsub(av, bv)) + vdot(ja, aw) - vdot(jb, bw);
         const float ndb = r.vel_mult * ynb;
         rel_adj(ax, ja, jb, av, aw, bv, bw, ndb, avb, awb, bvb, bwb, g);
-        JointRow& o = A.jrow[d];
-        o.axis[0] += g.n.x; o.axis[1] += g.n.y; o.axis[2] += g.n.z;
-        o.ang_a[0] += g.ra.x; o.ang_a[1] += g.ra.y; o.ang_a[2] += g.ra.z;
-        o.ang_b[0] += g.rb.x; o.ang_b[1] += g.rb.y; o.ang_b[2] += g.rb.z;
-        o.ima += g.ima; o.imb += g.imb;
-        o.vel_mult += nd * ynb;
-        if (it < pos) o.constant += ynb; else o.unbiased += ynb;
+        JointRow o = {};
+        o.axis[0] = g.n.x; o.axis[1] = g.n.y; o.axis[2] = g.n.z;
+        o.ang_a[0] = g.ra.x; o.ang_a[1] = g.ra.y; o.ang_a[2] = g.ra.z;
+        o.ang_b[0] = g.rb.x; o.ang_b[1] = g.rb.y; o.ang_b[2] = g.rb.z;
+        o.ima = g.ima; o.imb = g.imb;
+        o.vel_mult = nd * ynb;
+        if (it < pos) o.constant = ynb; else o.unbiased = ynb;
+        add_row(A.jrow[d], o);
         A.yj[d] = ynb - dlb;
         D.store(b0, av, aw, avb, awb);
         D.store(b1, bv, bw, bvb, bwb);
@@ -300,26 +316,43 @@ __device__ void reverse_desc(const DevState& s, const AdjState& A, uint32_t d, u
     v3 av, aw, bv, bw, avb, awb, bvb, bwb;
     D.load(h0, av, aw, avb, awb);
     D.load(h1, bv, bw, bvb, bwb);
+    // the manager's four tape slots of this pass and the previous one, and
+    // its four running row adjoints, as 128-bit loads
+    const float4 zero4 = make_float4(0, 0, 0, 0);
+    const size_t slot = size_t(it) * cap + m;
+    const float4* tn4 = reinterpret_cast<const float4*>(s.tape_n);
+    const float4* tf4 = reinterpret_cast<const float4*>(s.tape_f);
+    const float tn[4] = {tn4[slot].x, tn4[slot].y, tn4[slot].z, tn4[slot].w};
+    float4 y4 = reinterpret_cast<float4*>(A.yn)[m];
+    float yv[4] = {y4.x, y4.y, y4.z, y4.w};
     RowAdj hg = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0.0f, 0.0f};
     float nsumb = 0.0f, dfb = 0.0f;
     const bool friction = (it >= pos || pos - it <= 3) && hd.anchors;
     if (friction) {
         const bool prev_friction = it > 0 && (it - 1 >= pos || pos - (it - 1) <= 3);
+        const float4 x4 = tf4[slot], xo4 = prev_friction ? tf4[slot - cap] : zero4;
+        const float xt[4] = {x4.x, x4.y, x4.z, x4.w}, xto[4] = {xo4.x, xo4.y, xo4.z, xo4.w};
+        float4 f4 = reinterpret_cast<float4*>(A.yf)[m];
+        float fv[4] = {f4.x, f4.y, f4.z, f4.w};
         float nsum = 0.0f;
-        for (uint32_t j = 0; j < hd.count; ++j) nsum += s.tape_n[(size_t(it) * cap + m) * 4 + j];
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j)
+            if (j < hd.count) nsum += tn[j];
         const float coeff = hd.anchors == 2 ? 0.5f : 1.0f;
         const float md = hd.df * coeff * nsum;
         float mdb = 0.0f;
-        for (int k = int(2 * hd.anchors) - 1; k >= 0; --k) {
-            const FrictionRow& f = s.frow[4 * size_t(m) + k];
+#pragma unroll
+        for (int k = 3; k >= 0; --k) {
+            if (k >= int(2 * hd.anchors)) continue;
+            const FrictionRow f = s.frow[4 * size_t(m) + k];
             const v3 t = lv(f.t), ra = lv(f.ra), rb = lv(f.rb);
-            const float xn = s.tape_f[(size_t(it) * cap + m) * 4 + k];
-            const float xo = prev_friction ? s.tape_f[(size_t(it - 1) * cap + m) * 4 + k] : 0.0f;
+            const float xn = xt[k];
+            const float xo = xto[k];
             RowAdj g = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0.0f, 0.0f};
             const float dlb = undo_update(t, ra, rb, ima, imb, xn - xo, av, aw, bv, bw, avb, awb, bvb, bwb, g);
-            const float xnb = A.yf[4 * size_t(m) + k] + dlb;
+            const float xnb = fv[k] + dlb;
             float xob = -dlb;
-            FrictionRow& o = A.frow[4 * size_t(m) + k];
+            FrictionRow o = {};
             if (xn == md && md != 0.0f) {
                 mdb += xnb;
             } else if (xn == -md && md != 0.0f) {
@@ -329,47 +362,55 @@ __device__ void reverse_desc(const DevState& s, const AdjState& A, uint32_t d, u
                 const float bias = it < pos ? f.bias : 0.0f;
                 const float td = vdot(t, vsub(av, bv)) + vdot(aw, ra) - vdot(bw, rb);
                 xob += xnb;
-                o.target += f.vel_mult * xnb;
-                if (it < pos) o.bias -= f.vel_mult * xnb;
-                o.vel_mult += (f.target - bias - td) * xnb;
+                o.target = f.vel_mult * xnb;
+                if (it < pos) o.bias = -(f.vel_mult * xnb);
+                o.vel_mult = (f.target - bias - td) * xnb;
                 rel_adj(t, ra, rb, av, aw, bv, bw, -f.vel_mult * xnb, avb, awb, bvb, bwb, g);
             } else {
                 mdb += xnb;   // clamped to a zero bound
             }
-            o.t[0] += g.n.x; o.t[1] += g.n.y; o.t[2] += g.n.z;
-            o.ra[0] += g.ra.x; o.ra[1] += g.ra.y; o.ra[2] += g.ra.z;
-            o.rb[0] += g.rb.x; o.rb[1] += g.rb.y; o.rb[2] += g.rb.z;
+            o.t[0] = g.n.x; o.t[1] = g.n.y; o.t[2] = g.n.z;
+            o.ra[0] = g.ra.x; o.ra[1] = g.ra.y; o.ra[2] = g.ra.z;
+            o.rb[0] = g.rb.x; o.rb[1] = g.rb.y; o.rb[2] = g.rb.z;
+            add_row(A.frow[4 * size_t(m) + k], o);
             hg.ima += g.ima; hg.imb += g.imb;
-            A.yf[4 * size_t(m) + k] = xob;
+            fv[k] = xob;
         }
+        reinterpret_cast<float4*>(A.yf)[m] = make_float4(fv[0], fv[1], fv[2], fv[3]);
         dfb += coeff * nsum * mdb;
         nsumb += hd.df * coeff * mdb;
     }
-    for (int j = int(hd.count) - 1; j >= 0; --j) {
-        const NormalRow& r = s.nrow[4 * size_t(m) + j];
+    const float4 yo4 = it > 0 ? tn4[slot - cap] : zero4;
+    const float tno[4] = {yo4.x, yo4.y, yo4.z, yo4.w};
+#pragma unroll
+    for (int j = 3; j >= 0; --j) {
+        if (j >= int(hd.count)) continue;
+        const NormalRow r = s.nrow[4 * size_t(m) + j];
         const v3 n = lv(r.n), ra = lv(r.ra), rb = lv(r.rb);
-        const float yn = s.tape_n[(size_t(it) * cap + m) * 4 + j];
-        const float yo = it > 0 ? s.tape_n[(size_t(it - 1) * cap + m) * 4 + j] : 0.0f;
+        const float yn = tn[j];
+        const float yo = tno[j];
         RowAdj g = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0.0f, 0.0f};
         const float dlb = undo_update(n, ra, rb, ima, imb, yn - yo, av, aw, bv, bw, avb, awb, bvb, bwb, g);
-        const float ynb = A.yn[4 * size_t(m) + j] + dlb + nsumb;
+        const float ynb = yv[j] + dlb + nsumb;
         float yob = -dlb;
-        NormalRow& o = A.nrow[4 * size_t(m) + j];
+        NormalRow o = {};
         if (yn != 0.0f) {
             // y' = imp y + (-nvel vm + err)
             const float nvel = vdot(n, vsub(av, bv)) + vdot(aw, ra) - vdot(bw, rb);
             yob += r.imp_mult * ynb;
-            o.imp_mult += yo * ynb;
-            o.vel_mult += -nvel * ynb;
-            if (it < pos) o.biased += ynb; else o.unbiased += ynb;
+            o.imp_mult = yo * ynb;
+            o.vel_mult = -nvel * ynb;
+            if (it < pos) o.biased = ynb; else o.unbiased = ynb;
             rel_adj(n, ra, rb, av, aw, bv, bw, -r.vel_mult * ynb, avb, awb, bvb, bwb, g);
         }
-        o.n[0] += g.n.x; o.n[1] += g.n.y; o.n[2] += g.n.z;
-        o.ra[0] += g.ra.x; o.ra[1] += g.ra.y; o.ra[2] += g.ra.z;
-        o.rb[0] += g.rb.x; o.rb[1] += g.rb.y; o.rb[2] += g.rb.z;
+        o.n[0] = g.n.x; o.n[1] = g.n.y; o.n[2] = g.n.z;
+        o.ra[0] = g.ra.x; o.ra[1] = g.ra.y; o.ra[2] = g.ra.z;
+        o.rb[0] = g.rb.x; o.rb[1] = g.rb.y; o.rb[2] = g.rb.z;
+        add_row(A.nrow[4 * size_t(m) + j], o);
         hg.ima += g.ima; hg.imb += g.imb;
-        A.yn[4 * size_t(m) + j] = yob;
+        yv[j] = yob;
     }
+    reinterpret_cast<float4*>(A.yn)[m] = make_float4(yv[0], yv[1], yv[2], yv[3]);
     float4 h = A.hd[m];
     h.x += hg.ima; h.y += hg.imb; h.w += dfb;
     A.hd[m] = h;
@@ -399,6 +440,44 @@ __device__ __forceinline__ void inject_motion(const DevState& s, const AdjState&
 
 // Reverse PGS sweep over island-local slots in shared memory: one warp per
 // island of <= kSmallIsland descriptors (4 warps per block).
+// One thread per tiny island (<= kRevTiny descriptors): its descriptors in
+// reverse placed order (levels in reverse; a level's descriptors share no
+// body), with the deltas and their adjoints in the thread's slice of shared
+// memory.  Most islands of a loose pile are a box resting alone.
+constexpr uint32_t kRevTiny = 8;
+constexpr uint32_t kRevThreadBlock = 64;
+__global__ void __launch_bounds__(kRevThreadBlock) k_adj_pgs_thread(DevState s, AdjState A) {
+    __shared__ float4 sh[kRevThreadBlock][4 * (kRevTiny + 1)];
+    const uint32_t ni = *s.n_isl;
+    const int pos = s.pos_iters, vel = s.vel_iters < 1 ? 1 : s.vel_iters;
+    float4* my = sh[threadIdx.x];
+    const RevLocal D{my};
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < ni; isl += stride) {
+        const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
+        if (end - begin > kRevTiny) continue;
+        const uint32_t nb = s.isl_nbod[isl];
+        const int32_t* ib = s.isl_bod + begin + isl;
+        for (uint32_t l = 0; l < nb; ++l) {
+            const int32_t g = ib[l];
+            my[4 * l] = s.sb_dv[g]; my[4 * l + 1] = s.sb_dw[g];
+            my[4 * l + 2] = A.dv[g]; my[4 * l + 3] = A.dw[g];
+        }
+        for (int it = pos + vel - 1; it >= 0; --it) {
+            if (it == pos - 1)
+                for (uint32_t l = 0; l < nb; ++l) {
+                    const int32_t g = ib[l];
+                    float4 v = my[4 * l + 2], w = my[4 * l + 3];
+                    const float4 mv = A.dvm[g], mw = A.dwm[g];
+                    v.x += mv.x; v.y += mv.y; v.z += mv.z;
+                    w.x += mw.x; w.y += mw.y; w.z += mw.z;
+                    my[4 * l + 2] = v; my[4 * l + 3] = w;
+                }
+            for (uint32_t i = end; i-- > begin;) reverse_desc(s, A, s.d_val2[i], s.d_lbod[i], it, pos, D);
+        }
+    }
+}
+
 constexpr uint32_t kRevWarps = 4;
 __global__ void __launch_bounds__(kRevWarps * 32) k_adj_pgs_warp_smem(DevState s, AdjState A,
                                                                      const uint32_t* lvl_bound) {
@@ -411,7 +490,7 @@ __global__ void __launch_bounds__(kRevWarps * 32) k_adj_pgs_warp_smem(DevState s
     const RevLocal D{sh[wib]};
     for (uint32_t isl = warp; isl < ni; isl += nwarps) {
         const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
-        if (end - begin > kSmallIsland) continue;
+        if (end - begin > kSmallIsland || end - begin <= kRevTiny) continue;
         const uint32_t nlev = s.isl_end[isl];
         const uint32_t nb = s.isl_nbod[isl];
         const int32_t* ib = s.isl_bod + begin + isl;
@@ -904,6 +983,7 @@ void enqueue_adjoint_step(const DevState& s, const AdjState& a, cudaStream_t st)
     k_adj_clear_bodies<<<grid_n(s.n_bodies, T, 1u << 30), T, 0, st>>>(s, a);
     k_adj_clear_rows<<<grid_n(s.pair_cap, T, 148u * 8u), T, 0, st>>>(s, a);
     k_adj_integrate<<<grid_n(s.n_bodies, T, 1u << 30), T, 0, st>>>(s, a);
+    k_adj_pgs_thread<<<grid_n(s.desc_cap, kRevThreadBlock, 148u * 16u), kRevThreadBlock, 0, st>>>(s, a);
     k_adj_pgs_warp_smem<<<grid_n(s.desc_cap * 32u, kRevWarps * 32u, 148u * 8u), kRevWarps * 32u, 0, st>>>(
         s, a, s.lvl_bound);
     k_adj_pgs_mid_smem<<<grid_n(s.desc_cap, kSmallIsland + 1, 148u * 4u), 128,

@@ -596,7 +596,12 @@ public:
         for (int k = 0; k < 4; ++k) s.isl_list[k] = f.lists[k];
         return s;
     }
+    void release_segment_graphs() {
+        for (auto& g : seg_graphs_) if (g.exec) cudaGraphExecDestroy(g.exec);
+        seg_graphs_.clear();
+    }
     void release_rollout() {
+        release_segment_graphs();
         for (void* p : roll_owned_) cudaFree(p);
         roll_owned_.clear();
         ckpt_.clear();
@@ -684,6 +689,39 @@ public:
         last_cur_ = parity_;
         parity_ ^= 1;
     }
+    // One segment of the backward pass: its recompute into frames [0, len)
+    // and the step adjoints in reverse, as one CUDA graph per (start parity,
+    // length), captured on first use and replayed for the other segments
+    // (the frames and the live buffers they read are the same each time;
+    // the checkpoint is loaded before the launch).
+    void segment_backward(uint32_t len) {
+        if (seg_dt_ != roll_dt_) { release_segment_graphs(); seg_dt_ = roll_dt_; }
+        const int p0 = parity_;
+        SegGraph* g = nullptr;
+        for (auto& x : seg_graphs_) if (x.parity == p0 && x.len == len) g = &x;
+        if (!g) {
+            cudaGraph_t graph;
+            check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
+            for (uint32_t t = 0; t < len; ++t) framed_step(frames_[t]);
+            for (int t = int(len) - 1; t >= 0; --t) frame_adjoint(frames_[t]);
+            check_cuda(cudaStreamEndCapture(stream_, &graph), "end capture");
+            SegGraph ng;
+            ng.parity = p0;
+            ng.len = len;
+            check_cuda(cudaGraphInstantiateWithFlags(&ng.exec, graph, cudaGraphInstantiateFlagUseNodePriority),
+                       "instantiate");
+            cudaGraphDestroy(graph);
+            seg_graphs_.push_back(ng);
+            g = &seg_graphs_.back();
+            parity_ = p0;   // the capture advanced the host-side parities; replay below does it again
+        }
+        for (uint32_t t = 0; t < len; ++t) {
+            frames_[t].parity = parity_;
+            last_cur_ = parity_;
+            parity_ ^= 1;
+        }
+        check_cuda(cudaGraphLaunch(g->exec, stream_), "segment launch");
+    }
     // The step's adjoint over frame f.
     void frame_adjoint(const Frame& f) {
         DevState s = framed(f, f.parity);
@@ -718,10 +756,7 @@ public:
         for (int seg = int(nseg) - 1; seg >= 0; --seg) {
             const uint32_t t0 = uint32_t(seg) * roll_every_, t1 = std::min(roll_steps_, t0 + roll_every_);
             load_slot(ckpt_[seg]);
-            for (uint32_t t = t0; t < t1; ++t) framed_step(frames_[t - t0]);
-            check_cuda(cudaGetLastError(), "recompute launch");
-            for (int t = int(t1) - 1; t >= int(t0); --t) frame_adjoint(frames_[t - t0]);
-            check_cuda(cudaGetLastError(), "adjoint launch");
+            segment_backward(t1 - t0);
         }
         check_cuda(cudaStreamSynchronize(stream_), "backward sync");
         if (read_err()) throw std::overflow_error("Device error during the backward pass");
@@ -807,6 +842,7 @@ public:
         sleep_enabled_ = on;
         d_.sleep = on;
         for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        release_segment_graphs();
     }
     bool sleeping_enabled() const { return sleep_enabled_; }
     void read_sleep_state(float* wake, uint32_t* flags, float* motion6, uint32_t* counted, uint32_t n) {
@@ -840,6 +876,7 @@ public:
         d_.events = on;
         if (uploaded_ && on) alloc_events();
         for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        release_segment_graphs();
     }
     // World::contact_events / contact_event_points (world.h:466-468): the
     // last completed step's events, copied from the device on the first
@@ -1152,6 +1189,7 @@ private:
     void run_steps(float dt, uint32_t steps) {
         if (dt != graph_dt_) {
             for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        release_segment_graphs();
             graph_dt_ = dt;
         }
         d_.dt = dt;
@@ -1218,6 +1256,7 @@ private:
     void release_device() {
         release_rollout();
         for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        release_segment_graphs();
         for (void* p : owned_) cudaFree(p);
         owned_.clear();
         for (void* p : pair_owned_) cudaFree(p);
@@ -1229,6 +1268,7 @@ private:
         for (void* p : pair_owned_) cudaFree(p);
         pair_owned_.clear();
         for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        release_segment_graphs();
         d_.pair_cap = cap;
         d_.desc_cap = cap + d_.n_joints;
         for (int k = 0; k < 2; ++k) {
@@ -1493,6 +1533,9 @@ private:
     float roll_dt_ = 1.0f / 120.0f;
     bool roll_done_ = false;
     AdjState adj_;
+    struct SegGraph { int parity = 0; uint32_t len = 0; cudaGraphExec_t exec = nullptr; };
+    std::vector<SegGraph> seg_graphs_;
+    float seg_dt_ = -1.0f;
     bool notify_ = false;
     bool ev_device_valid_ = false;
     uint64_t ev_fetched_ = ~0ull;
