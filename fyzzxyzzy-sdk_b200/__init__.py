@@ -36,7 +36,7 @@ EXPORTS = (
     "fyzz_b200_read_step_counters", "fyzz_b200_set_contact_notifications",
     "fyzz_b200_contact_events", "fyzz_b200_rollout_begin", "fyzz_b200_rollout_forward",
     "fyzz_b200_rollout_backward", "fyzz_b200_read_mass_frames", "fyzz_b200_read_friction_anchors",
-    "fyzz_b200_fit_pair_budget", "fyzz_b200_set_sleeping", "fyzz_b200_read_sleep_state",
+    "fyzz_b200_fit_pair_budget", "fyzz_b200_set_sleeping", "fyzz_b200_read_sleep_state", "fyzz_b200_rollout_rewind",
 )
 STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 
@@ -135,6 +135,7 @@ def lib():
         L.fyzz_b200_set_sleeping.argtypes = [vp, i32]
         L.fyzz_b200_read_sleep_state.argtypes = [vp, vp, vp, vp, vp, u32]
         L.fyzz_b200_rollout_begin.argtypes = [vp, u32, u32]
+        L.fyzz_b200_rollout_rewind.argtypes = [vp]
         L.fyzz_b200_fit_pair_budget.argtypes = [vp, f32, P(u32)]
         L.fyzz_b200_rollout_forward.argtypes = [vp, f32]
         L.fyzz_b200_rollout_backward.argtypes = [vp] + [vp] * 9
@@ -392,6 +393,10 @@ class World:
 
     def rollout_begin(self, steps: int, checkpoint_every: int):
         self._check(lib().fyzz_b200_rollout_begin(self.h, steps, checkpoint_every))
+
+    def rollout_rewind(self):
+        """Back to the state the last rollout_forward started from."""
+        self._check(lib().fyzz_b200_rollout_rewind(self.h))
 
     def rollout_forward(self, seconds: float = 1.0 / 120.0):
         self._check(lib().fyzz_b200_rollout_forward(self.h, seconds))

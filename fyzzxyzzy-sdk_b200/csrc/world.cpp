@@ -615,10 +615,19 @@ public:
         ensure_device();
         pull_state();
         check_cuda(cudaStreamSynchronize(stream_), "sync");
-        release_rollout();
         // a differentiable rollout simulates every body: wake them all
         enqueue_wake_bodies(d_, stream_);
         check_cuda(cudaStreamSynchronize(stream_), "sync");
+        if (roll_steps_ == steps && roll_every_ == every && roll_cap_ == d_.pair_cap && !ckpt_.empty()) {
+            // same shape as the previous rollout: checkpoints, frames and the
+            // captured segment graphs are reused
+            roll_done_ = false;
+            check_cuda(cudaMemsetAsync(adj_.mark, 0, size_t(d_.n_bodies) * 4, stream_), "memset");
+            check_cuda(cudaMemsetAsync(adj_.epoch, 0, 4, stream_), "memset");
+            check_cuda(cudaStreamSynchronize(stream_), "sync");
+            return;
+        }
+        release_rollout();
         roll_steps_ = steps;
         roll_every_ = every;
         roll_cap_ = d_.pair_cap;
@@ -646,6 +655,14 @@ public:
         check_cuda(cudaMemsetAsync(A.epoch, 0, 4, stream_), "memset");
         check_cuda(cudaStreamSynchronize(stream_), "sync");
     }
+    // Back to the state the last rollout_forward started from (its first
+    // checkpoint), e.g. to run the rollout again with new parameters.
+    void rollout_rewind() {
+        if (!roll_done_) throw std::logic_error("rollout_forward must come first");
+        load_slot(ckpt_.front());
+        check_cuda(cudaStreamSynchronize(stream_), "sync");
+        host_authoritative_ = false;
+    }
     void require_rollout_capacity() {
         if (d_.pair_cap != roll_cap_)
             throw std::logic_error("Pair capacity grew during a differentiable rollout; step the scene once "
@@ -659,11 +676,7 @@ public:
             World& w;
             explicit SleepOff(World& x) : w(x) { flip(false); }
             ~SleepOff() { flip(w.sleep_enabled_); }
-            void flip(bool on) {
-                if (w.d_.sleep == on) return;
-                w.d_.sleep = on;
-                for (auto& g : w.graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
-            }
+            void flip(bool on) { w.d_.sleep = on; }   // the step graphs are cached per sleep mode
         } off(*this);
         for (uint32_t t0 = 0; t0 < roll_steps_; t0 += roll_every_) {
             save_slot(ckpt_[t0 / roll_every_]);
@@ -1195,7 +1208,8 @@ private:
         d_.dt = dt;
         check_cuda(cudaMemsetAsync(d_.err, 0, 4, stream_), "memset");
         for (uint32_t i = 0; i < steps; ++i) {
-            if (!graphs_[parity_]) {
+            cudaGraphExec_t& exec = graphs_[parity_ + (d_.sleep ? 2 : 0)];
+            if (!exec) {
                 cudaGraph_t g;
                 check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
                 const DevState s = view(parity_);
@@ -1214,11 +1228,11 @@ private:
                 }
                 kernels_per_step_ = kernels;
                 // kernel-node priorities (the largest islands' kernels) are honoured
-                check_cuda(cudaGraphInstantiateWithFlags(&graphs_[parity_], g, cudaGraphInstantiateFlagUseNodePriority),
+                check_cuda(cudaGraphInstantiateWithFlags(&exec, g, cudaGraphInstantiateFlagUseNodePriority),
                            "instantiate");
                 cudaGraphDestroy(g);
             }
-            check_cuda(cudaGraphLaunch(graphs_[parity_], stream_), "graph launch");
+            check_cuda(cudaGraphLaunch(exec, stream_), "graph launch");
             last_cur_ = parity_;
             parity_ ^= 1;
         }
@@ -1522,7 +1536,7 @@ private:
     float* bk_wake_ = nullptr;
     uint32_t* bk_sleep_ = nullptr;
     bool sleep_enabled_ = true;
-    cudaGraphExec_t graphs_[2] = {nullptr, nullptr};
+    cudaGraphExec_t graphs_[4] = {nullptr, nullptr, nullptr, nullptr};   // [parity + 2 * sleeping]
     float graph_dt_ = -1.0f;
     int parity_ = 0, last_cur_ = 1, snap_parity_ = 0, snap_last_ = 1;
     uint64_t steps_done_ = 0;
@@ -1800,6 +1814,9 @@ int fyzz_b200_fit_pair_budget(fyzz_b200_world* w, float headroom, uint32_t* budg
 }
 int fyzz_b200_rollout_begin(fyzz_b200_world* w, uint32_t steps, uint32_t checkpoint_every) {
     return guarded(w, [&](auto& W) { W.rollout_begin(steps, checkpoint_every); });
+}
+int fyzz_b200_rollout_rewind(fyzz_b200_world* w) {
+    return guarded(w, [&](auto& W) { W.rollout_rewind(); });
 }
 int fyzz_b200_rollout_forward(fyzz_b200_world* w, float seconds) {
     return guarded(w, [&](auto& W) { W.rollout_forward(seconds); });

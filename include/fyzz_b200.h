@@ -214,6 +214,11 @@ int fyzz_b200_read_sleep_state(fyzz_b200_world* w, float* wake, uint32_t* flags,
  * shapes' static / dynamic friction coefficients.  Step the scene once
  * before rollout_begin so the pair budget is settled. */
 int fyzz_b200_rollout_begin(fyzz_b200_world* w, uint32_t steps, uint32_t checkpoint_every);
+/* Restores the state the last rollout_forward started from (no reference
+ * counterpart), so the rollout can be run again, e.g. with new initial
+ * velocities; a rollout_begin with the same steps and interval then reuses
+ * its checkpoints, frames and captured graphs. */
+int fyzz_b200_rollout_rewind(fyzz_b200_world* w);
 /* Re-sizes the pair budget (initially 8 per shape) to the live pairs times
  * headroom (>= 1), keeping the contact-manager history so the trajectory is
  * unchanged; rollouts size their checkpoints and frames by this budget.
