@@ -28,6 +28,10 @@ from dataclasses import dataclass, field
 import numpy as np
 
 BOX, SPHERE = 0, 1
+# Joint kinds: World::add_center_distance_constraint, add_anchored_distance_
+# constraint, add_fixed / spherical / revolute / prismatic_constraint.
+JOINT_CENTER, JOINT_ANCHORED, JOINT_FIXED, JOINT_SPHERICAL, JOINT_REVOLUTE, JOINT_PRISMATIC = range(6)
+FLOOR_BODY = 0xFFFFFFFF
 
 
 @dataclass
@@ -40,6 +44,11 @@ class SceneSpec:
     shape_mat: np.ndarray
     joints: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.uint32))
     joint_dist: np.ndarray = field(default_factory=lambda: np.zeros((0,), np.float32))
+    # Per joint: kind (JOINT_* below; default center distance) and the local
+    # frames of its two bodies (position 3 + quaternion xyzw 4 each).  A
+    # joint endpoint of FLOOR_BODY is the scene's static floor.
+    joint_kind: np.ndarray | None = None
+    joint_local: np.ndarray | None = None
     floor: float | None = 0.0
     floor_mat: tuple = (0.5, 0.5, 0.0)
 
@@ -54,6 +63,23 @@ class SceneSpec:
     @property
     def n_actors(self) -> int:
         return self.n_bodies + (1 if self.floor is not None else 0)
+
+    def joint_kinds(self) -> np.ndarray:
+        n = self.joints.shape[0]
+        return np.zeros(n, np.uint32) if self.joint_kind is None else np.asarray(self.joint_kind, np.uint32)
+
+    def joint_locals(self) -> np.ndarray:
+        n = self.joints.shape[0]
+        if self.joint_local is not None:
+            return np.ascontiguousarray(self.joint_local, np.float32).reshape(n, 14)
+        out = np.zeros((n, 14), np.float32)
+        out[:, 6] = out[:, 13] = 1.0
+        return out
+
+    def has_joint_kinds(self) -> bool:
+        """True when some joint is not a plain center distance joint."""
+        return bool(self.joints.shape[0]) and (bool(np.any(self.joint_kinds() != JOINT_CENTER)) or
+                                               bool(np.any(self.joints == FLOOR_BODY)))
 
     def validate(self) -> "SceneSpec":
         assert self.bodies.dtype == np.float32 and self.bodies.shape[1] == 14
@@ -255,3 +281,78 @@ def mixed_batched(n_scenes: int = 16384, low: int = 8, high: int = 256,
                                frac_box=0.6, frac_sphere=0.25, joint_frac=0.05,
                                size=(0.05, 0.3)))
     return out
+
+
+def _qmul(a, b):
+    ax, ay, az, aw = a
+    bx, by, bz, bw = b
+    return np.array([aw * bx + bw * ax + ay * bz - az * by, aw * by + bw * ay + az * bx - ax * bz,
+                     aw * bz + bw * az + ax * by - ay * bx, aw * bw - ax * bx - ay * by - az * bz])
+
+
+def _qrot(q, v):
+    u = np.asarray(q[:3], np.float64)
+    t = 2.0 * np.cross(u, v)
+    return v + q[3] * t + np.cross(u, t)
+
+
+def joint_mechanisms(n_chains: int = 24, seed: int = 0, links: int = 4, kinds=None, floor_every: int = 3,
+                     spacing: float = 4.0, height: float = 2.5, density: float = 500.0,
+                     speed: float = 1.0) -> SceneSpec:
+    """Chains of boxes joined end to end by the joint kinds in `kinds`
+    (cycled over the chains; default: every kind), at rest or moving with
+    N(0, speed) velocities.  Each joint's two local frames coincide in the
+    world at creation: the joint sits halfway between the linked boxes with
+    a random orientation (the hinge / slider axis is its local X).  Every
+    `floor_every`-th chain hangs its first box from the floor by a joint of
+    the same kind."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    kinds = list(range(6)) if kinds is None else list(kinds)
+    side = int(np.ceil(np.sqrt(n_chains)))
+    pos, quat, vel, ang, shapes, joints, dist, jk, jl = [], [], [], [], [], [], [], [], []
+    body = 0
+    for c in range(n_chains):
+        kind = kinds[c % len(kinds)]
+        gx, gz = divmod(c, side)
+        origin = np.array([spacing * gx, height, spacing * gz])
+        direction = rng.normal(size=3)
+        direction[1] = abs(direction[1]) * 0.3
+        direction /= np.linalg.norm(direction)
+        half = rng.uniform(0.1, 0.25, (links, 3))
+        step = 2.0 * half[:, 0].max() + 0.1
+        first = body
+        for k in range(links):
+            p = origin + direction * step * k
+            q = random_quaternions(rng, 1)[0].astype(np.float64)
+            pos.append(p); quat.append(q)
+            vel.append(rng.normal(0.0, speed, 3)); ang.append(rng.normal(0.0, speed, 3))
+            shapes.append([_box(half[k])])
+            body += 1
+        def frames(pa, qa, pb, qb, mid):
+            qj = random_quaternions(rng, 1)[0].astype(np.float64)
+            ca, cb = qa * np.array([-1, -1, -1, 1]), qb * np.array([-1, -1, -1, 1])
+            la = np.concatenate([_qrot(ca, mid - pa), _qmul(ca, qj)])
+            lb = np.concatenate([_qrot(cb, mid - pb), _qmul(cb, qj)])
+            return np.concatenate([la, lb])
+        def length(kind, pa, pb):
+            # center distance: the centres' separation; anchored: a short rope
+            return float(np.linalg.norm(pa - pb)) if kind == JOINT_CENTER else 0.05
+        for k in range(1, links):
+            a, b = first + k - 1, first + k
+            joints.append((a, b)); dist.append(length(kind, pos[a], pos[b])); jk.append(kind)
+            jl.append(frames(pos[a], quat[a], pos[b], quat[b], 0.5 * (pos[a] + pos[b])))
+        if floor_every and c % floor_every == 0:
+            # hung from the floor actor (at the origin: floor height 0)
+            anchor = pos[first] - direction * step * 0.5
+            floor_p, floor_q = np.zeros(3), np.array([0, 0, 0, 1.0])
+            joints.append((FLOOR_BODY, first)); jk.append(kind)
+            dist.append(float(np.linalg.norm(floor_p - pos[first])) if kind == JOINT_CENTER else 0.05)
+            jl.append(frames(floor_p, floor_q, pos[first], quat[first], anchor))
+    n = len(pos)
+    mats = np.tile(np.array([0.5, 0.5, 0.0], np.float32), (n, 1))
+    spec = _assemble(np.asarray(pos, np.float32), np.asarray(quat, np.float32), np.asarray(vel, np.float32),
+                     np.asarray(ang, np.float32), density, shapes, mats,
+                     joints=np.asarray(joints, np.uint32).reshape(-1, 2), joint_dist=np.asarray(dist, np.float32))
+    spec.joint_kind = np.asarray(jk, np.uint32)
+    spec.joint_local = np.asarray(jl, np.float32).reshape(-1, 14)
+    return spec

@@ -95,6 +95,9 @@ struct fo_scene {
     actor_t* actors;
     shape_t* shapes;
     uint32_t* joint_a; uint32_t* joint_b; float* joint_len;
+    /* joint kind, authored endpoints and local frames (ConstraintRecord,
+     * scene.h:1529-1545) */
+    uint8_t* joint_kind; uint32_t* joint_auth; v3* joint_lp; qt* joint_lq;
     int has_floor;
     uint32_t plane_shape;
     /* pair state */
@@ -316,20 +319,70 @@ fo_scene* fo_scene_create(uint32_t nb, const float* bodies, uint32_t ns,
     s->joint_a = (uint32_t*)calloc(nj + 1, 4);
     s->joint_b = (uint32_t*)calloc(nj + 1, 4);
     s->joint_len = (float*)calloc(nj + 1, 4);
+    s->joint_kind = (uint8_t*)calloc(nj + 1, 1);
+    s->joint_auth = (uint32_t*)calloc(2 * nj + 2, 4);
+    s->joint_lp = (v3*)calloc(2 * nj + 2, sizeof(v3));
+    s->joint_lq = (qt*)calloc(2 * nj + 2, sizeof(qt));
     for (uint32_t j = 0; j < nj; ++j) {
-        const uint32_t a = joint_bodies[2 * j] + off, b = joint_bodies[2 * j + 1] + off;
+        /* 0xffffffff names the floor (actor 0) */
+        const uint32_t a = joint_bodies[2 * j] == 0xffffffffu ? 0u : joint_bodies[2 * j] + off;
+        const uint32_t b = joint_bodies[2 * j + 1] == 0xffffffffu ? 0u : joint_bodies[2 * j + 1] + off;
         s->joint_a[j] = a < b ? a : b;   /* edge pair is ordered (scene.cpp:3154) */
         s->joint_b[j] = a < b ? b : a;
         s->joint_len[j] = joint_dist[j];
+        s->joint_auth[2 * j] = a;
+        s->joint_auth[2 * j + 1] = b;
+        s->joint_lq[2 * j] = s->joint_lq[2 * j + 1] = Q4(0, 0, 0, 1);
         if (s->actors[a].dynamic) ++s->actors[a].joints;
         if (s->actors[b].dynamic) ++s->actors[b].joints;
     }
     return s;
 }
 
+/* World::add_*_constraint (src/world.cpp:231-276) and Scene::create_*
+ * (scene.cpp:3046-3120): local frames validated and normalised twice; the
+ * distance kinds keep the ordered body pair with the authored anchors
+ * (scene.cpp:3097-3108); the other kinds keep the authored endpoint order
+ * (record.swapped, scene.cpp:3050-3060). */
+static int validated_q(const float* q4, qt* out) {
+    qt q = Q4(q4[0], q4[1], q4[2], q4[3]);
+    for (int pass = 0; pass < 2; ++pass) {
+        const float len = sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+        if (!isfinite(q.x) || !isfinite(q.y) || !isfinite(q.z) || !isfinite(q.w) || !isfinite(len) ||
+            fabsf(len - 1.0f) >= 1.0e-2f)
+            return 0;
+        q = Q4(q.x / len, q.y / len, q.z / len, q.w / len);
+    }
+    *out = q;
+    return 1;
+}
+int fo_scene_set_joint(fo_scene* s, uint32_t j, uint32_t kind, const float* la, const float* lb) {
+    if (j >= s->nj || kind > FO_JOINT_PRISMATIC) FAIL(FO_INVALID, "joint index or kind out of range");
+    const float* l[2] = {la, lb};
+    for (int k = 0; k < 2; ++k) {
+        if (!isfinite(l[k][0]) || !isfinite(l[k][1]) || !isfinite(l[k][2])) FAIL(FO_INVALID, "Position must be finite");
+        s->joint_lp[2 * j + k] = V3(l[k][0], l[k][1], l[k][2]);
+        s->joint_lq[2 * j + k] = Q4(0, 0, 0, 1);
+        if (kind >= FO_JOINT_FIXED && !validated_q(l[k] + 3, &s->joint_lq[2 * j + k]))
+            FAIL(FO_INVALID, "Rigid pose orientation is not sane");
+    }
+    if (kind == FO_JOINT_CENTER) s->joint_lp[2 * j] = s->joint_lp[2 * j + 1] = V3(0, 0, 0);
+    s->joint_kind[j] = (uint8_t)kind;
+    const uint32_t a = s->joint_auth[2 * j], b = s->joint_auth[2 * j + 1];
+    if (kind >= FO_JOINT_FIXED) {
+        s->joint_a[j] = a;
+        s->joint_b[j] = b;
+    }
+    return 0;
+}
+static uint32_t joint_rows(uint8_t kind) {
+    return kind <= FO_JOINT_ANCHORED ? 1u : kind == FO_JOINT_SPHERICAL ? 3u : kind == FO_JOINT_FIXED ? 6u : 5u;
+}
+
 void fo_scene_destroy(fo_scene* s) {
     if (!s) return;
     free(s->actors); free(s->shapes); free(s->joint_a); free(s->joint_b); free(s->joint_len);
+    free(s->joint_kind); free(s->joint_auth); free(s->joint_lp); free(s->joint_lq);
     free(s->mgr); free(s->found); free(s->lost); free(s->man); free(s->desc); free(s->pend);
     free(s->impulses); free(s->sorted_minx_val); free(s->sorted_minx_id);
     free(s);
@@ -797,10 +850,13 @@ int fo_scene_step(fo_scene* s, float dt, const uint64_t* manager_order, uint64_t
 #define ROW(b) (s->actors[b].dynamic ? &rows[b] : &world)
     /* ---- partition (scene.cpp:7113-7488, one task) ---- */
     const uint64_t nd = njo + nmo;
+    uint32_t jrow_n = 0;
     desc_t* d = (desc_t*)calloc(nd + 1, sizeof(desc_t));
     for (uint64_t i = 0; i < njo; ++i) {
-        d[i].index = (uint32_t)i;   /* joint row index == position in joint order */
-        d[i].b0 = s->joint_a[jo[i]]; d[i].b1 = s->joint_b[jo[i]]; d[i].rows = 1; d[i].joint = 1;
+        d[i].index = jrow_n;   /* first row of the joint, rows in joint order */
+        jrow_n += joint_rows(s->joint_kind[jo[i]]);
+        d[i].b0 = s->joint_a[jo[i]]; d[i].b1 = s->joint_b[jo[i]]; d[i].joint = 1;
+        d[i].rows = joint_rows(s->joint_kind[jo[i]]);
     }
     for (uint64_t i = 0; i < nmo; ++i) {
         const mgr_t* m = &s->mgr[s->man[mo[i]]];
@@ -875,33 +931,107 @@ int fo_scene_step(fo_scene* s, float dt, const uint64_t* manager_order, uint64_t
         s->desc[4 * i + 2] = e->b1;
         s->desc[4 * i + 3] = e->rows;
     }
-    /* ---- joint rows (scene.cpp:7547-7630, distance joints) ---- */
-    jrow_t* jr = (jrow_t*)calloc(njo + 1, sizeof(jrow_t));
+    /* ---- joint rows (scene.cpp:7615-7767) ---- */
+    jrow_t* jr = (jrow_t*)calloc(jrow_n + 1, sizeof(jrow_t));
     for (uint64_t i = 0; i < njo; ++i) {
-        const actor_t* b0 = &s->actors[s->joint_a[jo[i]]];
-        const actor_t* b1 = &s->actors[s->joint_b[jo[i]]];
-        const v3 world0 = b0->p, world1 = b1->p;    /* zero local anchors */
+        const uint32_t j = (uint32_t)jo[i];
+        const uint32_t id0 = s->joint_a[j], id1 = s->joint_b[j];
+        const actor_t* b0 = &s->actors[id0];
+        const actor_t* b1 = &s->actors[id1];
+        const uint8_t kind = s->joint_kind[j];
+        const v3 an0 = rot_sc(b0->q, s->joint_lp[2 * j]), an1 = rot_sc(b1->q, s->joint_lp[2 * j + 1]);
+        const v3 world0 = vadd(b0->p, an0), world1 = vadd(b1->p, an1);
         const v3 c0 = mass_position(b0), c1 = mass_position(b1);
         const v3 ra = vsub(world0, c0), rb = vsub(world1, c1);
         const float m0 = b0->dynamic ? b0->inv_mass : 0.0f;
         const float m1 = b1->dynamic ? b1->inv_mass : 0.0f;
         const v3 rel = vsub(b0->v, b1->v);
-        const v3 off = V3(c0.x + ra.x - c1.x - rb.x, c0.y + ra.y - c1.y - rb.y, c0.z + ra.z - c1.z - rb.z);
-        const float dist = sqrtf(vdot(off, off));
-        const v3 axis = dist < 1.192092896e-07f ? V3(1, 0, 0) : V3(off.x / dist, off.y / dist, off.z / dist);
-        const v3 an0 = vcross(ra, axis), an1 = vcross(rb, axis);
-        const v3 ja = b0->dynamic ? xform(&rows[s->joint_a[jo[i]]], an0) : V3(0, 0, 0);
-        const v3 jb = b1->dynamic ? xform(&rows[s->joint_b[jo[i]]], an1) : V3(0, 0, 0);
-        const float response = m0 + m1 + vdot(ja, ja) + vdot(jb, jb);
-        if (!(response > 0.0f) || !isfinite(response)) FAIL(FO_LOGIC, "joint response");
-        const float rcp = 1.0f / response;
-        jrow_t* r = &jr[i];
-        r->axis = axis; r->ang_a = ja; r->ang_b = jb; r->ima = m0; r->imb = m1;
-        r->vel_mult = -rcp;
-        const float speed = vdot(axis, rel) + vdot(an0, b0->w) - vdot(an1, b1->w);
-        const float err = dist - s->joint_len[jo[i]];
-        r->constant = -rcp * (err * inv_dt + speed);
-        r->unbiased = -rcp * speed;
+        jrow_t* out = &jr[d[i].index];
+        uint32_t emitted = 0;
+#define RESP0(v) (b0->dynamic ? xform(&rows[id0], (v)) : V3(0, 0, 0))
+#define RESP1(v) (b1->dynamic ? xform(&rows[id1], (v)) : V3(0, 0, 0))
+#define EMIT(AX, A0, A1, JA, JB, ERR, RESP)                                                          \
+        do {                                                                                         \
+            const float resp_ = (RESP);                                                              \
+            if (!(resp_ > 0.0f) || !isfinite(resp_)) FAIL(FO_LOGIC, "joint response");               \
+            const float rcp_ = 1.0f / resp_;                                                         \
+            jrow_t* r_ = &out[emitted++];                                                            \
+            r_->axis = (AX); r_->ang_a = (JA); r_->ang_b = (JB); r_->ima = m0; r_->imb = m1;          \
+            r_->vel_mult = -rcp_;                                                                    \
+            const float speed_ = vdot((AX), rel) + vdot((A0), b0->w) - vdot((A1), b1->w);            \
+            r_->constant = -rcp_ * ((ERR) * inv_dt + speed_);                                        \
+            r_->unbiased = -rcp_ * speed_;                                                           \
+        } while (0)
+        if (kind <= FO_JOINT_ANCHORED) {
+            const v3 off = V3(c0.x + ra.x - c1.x - rb.x, c0.y + ra.y - c1.y - rb.y, c0.z + ra.z - c1.z - rb.z);
+            const float dist = sqrtf(vdot(off, off));
+            const v3 axis = dist < 1.192092896e-07f ? V3(1, 0, 0) : V3(off.x / dist, off.y / dist, off.z / dist);
+            const v3 a0 = vcross(ra, axis), a1 = vcross(rb, axis);
+            const v3 ja = RESP0(a0), jb = RESP1(a1);
+            EMIT(axis, a0, a1, ja, jb, dist - s->joint_len[j], m0 + m1 + vdot(ja, ja) + vdot(jb, jb));
+            continue;
+        }
+        /* locked axes in frame A; rotation errors from the relative
+         * quaternion, rows orthogonalised in the inverse-mass metric */
+        const qt qa = qmul(b0->q, s->joint_lq[2 * j]);
+        const v3 error_p = rotinv_sc(qa, vsub(world0, world1));
+        v3 error_angle = V3(0, 0, 0), va = V3(0, 0, 0), vb = V3(0, 0, 0), c = V3(0, 0, 0);
+        float dd = 0.0f, overlap = 0.0f;
+        if (kind != FO_JOINT_SPHERICAL) {
+            qt qb = qmul(b1->q, s->joint_lq[2 * j + 1]);
+            if (qa.x * qb.x + qa.y * qb.y + qa.z * qb.z + qa.w * qb.w < 0.0f) qb = Q4(-qb.x, -qb.y, -qb.z, -qb.w);
+            const qt eq = qmul(qconj(qa), qb);
+            error_angle = V3(eq.x, eq.y, eq.z);
+            va = V3(qa.x, qa.y, qa.z);
+            vb = V3(qb.x, qb.y, qb.z);
+            dd = qa.w * qb.w - vdot(va, vb);
+            overlap = qa.w * qb.w + vdot(va, vb);
+            c = V3(qa.w * vb.x + qb.w * va.x, qa.w * vb.y + qb.w * va.y, qa.w * vb.z + qb.w * va.z);
+        }
+        const float errors[6] = {error_p.x, error_p.y, error_p.z, -error_angle.x, -error_angle.y, -error_angle.z};
+        const v3 basis[3] = {V3(1, 0, 0), V3(0, 1, 0), V3(0, 0, 1)};
+        const float avc[3] = {va.x, va.y, va.z}, bvc[3] = {vb.x, vb.y, vb.z};
+        const v3 diag[3] = {V3(dd, c.z, -c.y), V3(-c.z, dd, c.x), V3(c.y, -c.x, dd)};
+        struct { v3 lin, a0, a1, ja, jb; float err, inv; } er[6];
+        memset(er, 0, sizeof er);
+        const uint32_t count = joint_rows(kind);
+        for (uint32_t k = 0; k < count; ++k) {
+            const uint32_t comp = k + (kind == FO_JOINT_PRISMATIC ? 1u : 0u) +
+                                  (kind == FO_JOINT_REVOLUTE && k >= 3u ? 1u : 0u);
+            er[k].err = errors[comp];
+            if (comp < 3u) {
+                er[k].lin = rot_sc(qa, basis[comp]);
+                const v3 arm = kind == FO_JOINT_PRISMATIC ? vsub(world1, c0) : ra;
+                er[k].a0 = vcross(arm, er[k].lin);
+                er[k].a1 = vcross(rb, er[k].lin);
+            } else {
+                const uint32_t q = comp - 3u;
+                const v3 v = diag[q];
+                er[k].a0 = V3(0.5f * (va.x * bvc[q] + vb.x * avc[q] + v.x), 0.5f * (va.y * bvc[q] + vb.y * avc[q] + v.y),
+                              0.5f * (va.z * bvc[q] + vb.z * avc[q] + v.z));
+                if (overlap == 0.0f) {
+                    const float t = -FLT_EPSILON;
+                    er[k].a0 = V3(er[k].a0.x - basis[q].x * t, er[k].a0.y - basis[q].y * t, er[k].a0.z - basis[q].z * t);
+                }
+                er[k].a1 = er[k].a0;
+            }
+            er[k].ja = RESP0(er[k].a0);
+            er[k].jb = RESP1(er[k].a1);
+            for (uint32_t p = 0; p < k; ++p) {
+                const float w = (m0 + m1) * vdot(er[k].lin, er[p].lin) + vdot(er[k].ja, er[p].ja) + vdot(er[k].jb, er[p].jb);
+                const float t = w * er[p].inv;
+#define PROJ(F) er[k].F = V3(er[k].F.x - er[p].F.x * t, er[k].F.y - er[p].F.y * t, er[k].F.z - er[p].F.z * t)
+                PROJ(lin); PROJ(a0); PROJ(a1); PROJ(ja); PROJ(jb);
+#undef PROJ
+                er[k].err -= er[p].err * t;
+            }
+            const float resp = (m0 + m1) * vdot(er[k].lin, er[k].lin) + vdot(er[k].ja, er[k].ja) + vdot(er[k].jb, er[k].jb);
+            er[k].inv = resp > 0.0f ? 1.0f / resp : 0.0f;
+            EMIT(er[k].lin, er[k].a0, er[k].a1, er[k].ja, er[k].jb, er[k].err, resp);
+        }
+#undef EMIT
+#undef RESP0
+#undef RESP1
     }
     /* ---- contact and friction rows (scene.cpp:7631-8510, CPU path) ---- */
     const float bias_coeff = 0.8f, bounce = -2.0f, same_normal = 0.999f, fr_thr = 0.04f;
@@ -1159,18 +1289,20 @@ int fo_scene_step(fo_scene* s, float dt, const uint64_t* manager_order, uint64_t
             srow_t* a = s->actors[e->b0].dynamic ? &rows[e->b0] : &wl;
             srow_t* b = s->actors[e->b1].dynamic ? &rows[e->b1] : &wl;
             if (e->joint) {
-                jrow_t* r = &jr[e->index];
-                const float nd_ = r->axis.x * (a->dv.x - b->dv.x) + r->axis.y * (a->dv.y - b->dv.y) +
-                                  r->axis.z * (a->dv.z - b->dv.z) + vdot(r->ang_a, a->dw) - vdot(r->ang_b, b->dw);
-                const float cst = it < pos ? r->constant : r->unbiased;
-                const float nx = fclamp(r->applied + nd_ * r->vel_mult + cst, -maxf, maxf);
-                const float imp = nx - r->applied;
-                const float ia = imp * r->ima, ib = imp * r->imb;
-                a->dv = V3(a->dv.x + ia * r->axis.x, a->dv.y + ia * r->axis.y, a->dv.z + ia * r->axis.z);
-                b->dv = V3(b->dv.x - ib * r->axis.x, b->dv.y - ib * r->axis.y, b->dv.z - ib * r->axis.z);
-                a->dw = V3(a->dw.x + imp * r->ang_a.x, a->dw.y + imp * r->ang_a.y, a->dw.z + imp * r->ang_a.z);
-                b->dw = V3(b->dw.x - imp * r->ang_b.x, b->dw.y - imp * r->ang_b.y, b->dw.z - imp * r->ang_b.z);
-                r->applied = nx;
+                for (uint32_t q = 0; q < e->rows; ++q) {
+                    jrow_t* r = &jr[e->index + q];
+                    const float nd_ = r->axis.x * (a->dv.x - b->dv.x) + r->axis.y * (a->dv.y - b->dv.y) +
+                                      r->axis.z * (a->dv.z - b->dv.z) + vdot(r->ang_a, a->dw) - vdot(r->ang_b, b->dw);
+                    const float cst = it < pos ? r->constant : r->unbiased;
+                    const float nx = fclamp(r->applied + nd_ * r->vel_mult + cst, -maxf, maxf);
+                    const float imp = nx - r->applied;
+                    const float ia = imp * r->ima, ib = imp * r->imb;
+                    a->dv = V3(a->dv.x + ia * r->axis.x, a->dv.y + ia * r->axis.y, a->dv.z + ia * r->axis.z);
+                    b->dv = V3(b->dv.x - ib * r->axis.x, b->dv.y - ib * r->axis.y, b->dv.z - ib * r->axis.z);
+                    a->dw = V3(a->dw.x + imp * r->ang_a.x, a->dw.y + imp * r->ang_a.y, a->dw.z + imp * r->ang_a.z);
+                    b->dw = V3(b->dw.x - imp * r->ang_b.x, b->dw.y - imp * r->ang_b.y, b->dw.z - imp * r->ang_b.z);
+                    r->applied = nx;
+                }
                 continue;
             }
             const mprep_t* P = &mp[e->index];

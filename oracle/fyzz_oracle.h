@@ -15,6 +15,9 @@ extern "C" {
 
 enum { FO_BOX = 0, FO_SPHERE = 1, FO_PLANE = 2 };
 enum { FO_OK = 0, FO_INVALID = 1, FO_LOGIC = 2, FO_OVERFLOW = 3 };
+/* Joint kinds (scene.h:1528 JointKind, plus the two distance authorings). */
+enum { FO_JOINT_CENTER = 0, FO_JOINT_ANCHORED = 1, FO_JOINT_FIXED = 2, FO_JOINT_SPHERICAL = 3,
+       FO_JOINT_REVOLUTE = 4, FO_JOINT_PRISMATIC = 5 };
 #define FO_OVERFLOW_NEG (-3)
 #define FO_LOGIC_NEG (-2)
 
@@ -77,6 +80,10 @@ uint64_t fo_scene_manifolds(const fo_scene* s, uint32_t* pairs, uint32_t* counts
 uint64_t fo_scene_partitions(const fo_scene* s, uint32_t* desc4, uint64_t* ends);
 uint64_t fo_scene_normal_impulses(const fo_scene* s, double* out);
 uint64_t fo_scene_sorted_min_x(const fo_scene* s, uint32_t* values, uint32_t* ids);
+/* Sets joint j's kind and local frames (position 3 + orientation xyzw 4
+ * each; orientations are validated and normalised as World and Scene do;
+ * the distance kinds use the positions only).  Call before stepping. */
+int fo_scene_set_joint(fo_scene* s, uint32_t j, uint32_t kind, const float* local_a7, const float* local_b7);
 /* Sleeping on (default) or off (wakes every body). */
 void fo_scene_set_sleeping(fo_scene* s, int on);
 /* Per actor: wake counter, sleeping, ready, counted interactions, linear

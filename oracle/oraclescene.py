@@ -44,6 +44,7 @@ def lib():
         L.fo_scene_normal_impulses.restype = u64
         L.fo_scene_normal_impulses.argtypes = [vp, vp]
         L.fo_scene_set_sleeping.argtypes = [vp, i32]
+        L.fo_scene_set_joint.argtypes = [vp, u32, u32, vp, vp]
         L.fo_scene_sleep_state.argtypes = [vp, vp]
         L.fo_scene_sorted_min_x.restype = u64
         L.fo_scene_sorted_min_x.argtypes = [vp, vp, vp]
@@ -82,6 +83,11 @@ class OracleScene:
                                    _p(self._floor_mat))
         if not self.h:
             raise RuntimeError(L.fo_error().decode())
+        if spec.has_joint_kinds():
+            kinds, local = spec.joint_kinds(), spec.joint_locals()
+            for j in range(spec.joints.shape[0]):
+                la, lb = np.ascontiguousarray(local[j, :7]), np.ascontiguousarray(local[j, 7:])
+                self._check(L.fo_scene_set_joint(self.h, j, int(kinds[j]), _p(la), _p(lb)))
 
     def close(self):
         if getattr(self, "h", None):

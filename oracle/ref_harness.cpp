@@ -169,6 +169,39 @@ int fz_ref_build(void* p, uint32_t nb, const float* bodies, uint32_t ns,
     });
 }
 
+// One joint after fz_ref_build, through the Scene members World forwards to
+// (scene.cpp:11236-11260) with World's validation applied first
+// (src/world.cpp:231-276).  kind: 0 center distance, 1 anchored distance,
+// 2 fixed, 3 spherical, 4 revolute, 5 prismatic.  a / b are 0-based dynamic
+// body indices, 0xffffffff for the floor; local poses are 7 floats.
+int fz_ref_add_joint(void* p, int kind, uint32_t a, uint32_t b, const float* la, const float* lb,
+                     float distance) {
+    auto* h = static_cast<Handle*>(p);
+    return guarded([&] {
+        auto body = [&](uint32_t i) -> fyzz::BodyId {
+            if (i == 0xffffffffu) {
+                if (!h->has_floor) throw std::invalid_argument("no floor");
+                return 0;
+            }
+            return h->bodies.at(i);
+        };
+        Scene& s = *h->scene;
+        const fyzz::BodyId A = body(a), B = body(b);
+        if (kind == 0) {
+            s.create_center_distance_constraint(A, B, distance);
+        } else if (kind == 1) {
+            s.create_anchored_distance_constraint(A, B, {la[0], la[1], la[2]}, {lb[0], lb[1], lb[2]}, distance);
+        } else {
+            const fyzz::Transform ta = transform_of(la), tb = transform_of(lb);
+            if (kind == 2) s.create_fixed_constraint(A, B, ta, tb);
+            else if (kind == 3) s.create_spherical_constraint(A, B, ta, tb);
+            else if (kind == 4) s.create_revolute_constraint(A, B, ta, tb);
+            else if (kind == 5) s.create_prismatic_constraint(A, B, ta, tb);
+            else throw std::invalid_argument("joint kind");
+        }
+    });
+}
+
 int fz_ref_step(void* p, float dt, int steps) {
     auto* h = static_cast<Handle*>(p);
     return guarded([&] {

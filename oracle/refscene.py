@@ -38,6 +38,7 @@ def lib():
         L.fz_ref_body_states.argtypes = [vp, vp]
         L.fz_ref_mass_props.argtypes = [vp, vp]
         L.fz_ref_sleep_state.argtypes = [vp, vp]
+        L.fz_ref_add_joint.argtypes = [vp, i32, u32, u32, vp, vp, f32]
         L.fz_ref_encoded_bounds.argtypes = [vp, vp]
         for name in ("fz_ref_endpoints",):
             getattr(L, name).restype = u64
@@ -84,13 +85,20 @@ class RefScene:
             spec.shape_local, spec.shape_mat, spec.joints, spec.joint_dist)]
         self._keep = arrs
         self._floor_mat = np.asarray(spec.floor_mat, np.float32)
+        kinds = spec.has_joint_kinds()
         rc = L.fz_ref_build(self.h, spec.n_bodies, _p(arrs[0]), spec.n_shapes,
                             _p(arrs[1]), _p(arrs[2]), _p(arrs[3]), _p(arrs[4]),
-                            _p(arrs[5]), arrs[6].shape[0], _p(arrs[6]), _p(arrs[7]),
+                            _p(arrs[5]), 0 if kinds else arrs[6].shape[0], _p(arrs[6]), _p(arrs[7]),
                             0 if spec.floor is None else 1,
                             0.0 if spec.floor is None else float(spec.floor),
                             _p(self._floor_mat))
         self._check(rc)
+        if kinds:   # every joint in authoring order, each with its kind
+            jk, local = spec.joint_kinds(), spec.joint_locals()
+            for j in range(spec.joints.shape[0]):
+                la, lb = np.ascontiguousarray(local[j, :7]), np.ascontiguousarray(local[j, 7:])
+                self._check(L.fz_ref_add_joint(self.h, int(jk[j]), int(spec.joints[j, 0]), int(spec.joints[j, 1]),
+                                               _p(la), _p(lb), float(spec.joint_dist[j])))
 
     def _check(self, rc):
         if rc:
