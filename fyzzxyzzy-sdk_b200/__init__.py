@@ -27,6 +27,9 @@ EXPORTS = (
     "fyzz_b200_update_mass_properties", "fyzz_b200_body_mass_properties",
     "fyzz_b200_set_shape_material", "fyzz_b200_set_body_velocity",
     "fyzz_b200_set_body_angular_velocity", "fyzz_b200_add_center_distance_constraint",
+    "fyzz_b200_add_anchored_distance_constraint", "fyzz_b200_add_fixed_constraint",
+    "fyzz_b200_add_spherical_constraint", "fyzz_b200_add_revolute_constraint",
+    "fyzz_b200_add_prismatic_constraint",
     "fyzz_b200_add_scene", "fyzz_b200_step", "fyzz_b200_step_n", "fyzz_b200_collide",
     "fyzz_b200_synchronize", "fyzz_b200_body_state", "fyzz_b200_read_bodies",
     "fyzz_b200_write_velocities", "fyzz_b200_counts", "fyzz_b200_device_view",
@@ -109,6 +112,9 @@ def lib():
         L.fyzz_b200_set_body_velocity.argtypes = [vp, u32, vp]
         L.fyzz_b200_set_body_angular_velocity.argtypes = [vp, u32, vp]
         L.fyzz_b200_add_center_distance_constraint.argtypes = [vp, u32, u32, f32, P(u64)]
+        L.fyzz_b200_add_anchored_distance_constraint.argtypes = [vp, u32, u32, vp, vp, f32, P(u64)]
+        for name in ("fixed", "spherical", "revolute", "prismatic"):
+            getattr(L, f"fyzz_b200_add_{name}_constraint").argtypes = [vp, u32, u32, vp, vp, P(u64)]
         L.fyzz_b200_add_scene.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, vp, u32, vp, vp, i32, f32, vp, P(u32)]
         L.fyzz_b200_step.argtypes = [vp, f32]
         L.fyzz_b200_step_n.argtypes = [vp, f32, u32]
@@ -248,6 +254,33 @@ class World:
         self._check(lib().fyzz_b200_add_center_distance_constraint(self.h, a, b, distance, C.byref(out)))
         return out.value
 
+    def add_anchored_distance_constraint(self, a: int, b: int, local_a, local_b, distance: float) -> int:
+        """World::add_anchored_distance_constraint (reference world.h:441)."""
+        la, lb = np.asarray(local_a, np.float32)[:3].copy(), np.asarray(local_b, np.float32)[:3].copy()
+        out = C.c_uint64()
+        self._check(lib().fyzz_b200_add_anchored_distance_constraint(self.h, a, b, _p(la), _p(lb), distance,
+                                                                     C.byref(out)))
+        return out.value
+
+    def _frame_joint(self, name: str, a: int, b: int, local_a, local_b) -> int:
+        la, lb = np.asarray(local_a, np.float32).reshape(7).copy(), np.asarray(local_b, np.float32).reshape(7).copy()
+        out = C.c_uint64()
+        self._check(getattr(lib(), f"fyzz_b200_add_{name}_constraint")(self.h, a, b, _p(la), _p(lb), C.byref(out)))
+        return out.value
+
+    def add_fixed_constraint(self, a: int, b: int, local_a, local_b) -> int:
+        """World::add_fixed_constraint: local frames are position(3) + xyzw(4)."""
+        return self._frame_joint("fixed", a, b, local_a, local_b)
+
+    def add_spherical_constraint(self, a: int, b: int, local_a, local_b) -> int:
+        return self._frame_joint("spherical", a, b, local_a, local_b)
+
+    def add_revolute_constraint(self, a: int, b: int, local_a, local_b) -> int:
+        return self._frame_joint("revolute", a, b, local_a, local_b)
+
+    def add_prismatic_constraint(self, a: int, b: int, local_a, local_b) -> int:
+        return self._frame_joint("prismatic", a, b, local_a, local_b)
+
     def add_scene(self, spec) -> int:
         """Author one seeded scene (fyzzxyzzy-sdk_b200.scenes.SceneSpec);
         returns the BodyId of its first dynamic body."""
@@ -256,12 +289,28 @@ class World:
             spec.shape_local, spec.shape_mat, spec.joints, spec.joint_dist)]
         fm = np.asarray(spec.floor_mat, np.float32)
         out = C.c_uint32()
+        kinds = spec.has_joint_kinds()
         self._check(lib().fyzz_b200_add_scene(
             self.h, spec.n_bodies, _p(arrs[0]), spec.n_shapes, _p(arrs[1]), _p(arrs[2]),
-            _p(arrs[3]), _p(arrs[4]), _p(arrs[5]), arrs[6].shape[0], _p(arrs[6]), _p(arrs[7]),
+            _p(arrs[3]), _p(arrs[4]), _p(arrs[5]), 0 if kinds else arrs[6].shape[0], _p(arrs[6]), _p(arrs[7]),
             0 if spec.floor is None else 1, 0.0 if spec.floor is None else float(spec.floor),
             _p(fm), C.byref(out)))
-        return out.value
+        first = out.value
+        if kinds:   # every joint in authoring order, each with its kind
+            from .scenes import FLOOR_BODY
+            jk, local = spec.joint_kinds(), spec.joint_locals()
+            body = lambda i: first - 1 if int(i) == FLOOR_BODY else first + int(i)
+            names = {2: "fixed", 3: "spherical", 4: "revolute", 5: "prismatic"}
+            for j in range(spec.joints.shape[0]):
+                a, b, k = body(spec.joints[j, 0]), body(spec.joints[j, 1]), int(jk[j])
+                if k == 0:
+                    self.add_center_distance_constraint(a, b, float(spec.joint_dist[j]))
+                elif k == 1:
+                    self.add_anchored_distance_constraint(a, b, local[j, :3], local[j, 7:10],
+                                                          float(spec.joint_dist[j]))
+                else:
+                    self._frame_joint(names[k], a, b, local[j, :7], local[j, 7:])
+        return first
 
     # ---- stepping ----
     def step(self, seconds: float = 1.0 / 120.0, steps: int = 1):

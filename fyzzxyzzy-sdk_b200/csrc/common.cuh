@@ -18,6 +18,9 @@ enum : uint32_t { kBox = 0, kSphere = 1, kPlane = 2 };
 enum : uint32_t { kBodyDynamic = 1u };
 // b_sleep bits
 enum : uint32_t { kSleeping = 1u, kReady = 2u };
+// joint kinds: the two distance authorings, then JointKind (scene.h:1528)
+enum : uint32_t { kJointCenter = 0u, kJointAnchored = 1u, kJointFixed = 2u, kJointSpherical = 3u,
+                  kJointRevolute = 4u, kJointPrismatic = 5u };
 
 // Device error bits (published to the host after each step; the C ABI maps
 // them to status codes like the reference's task error words,

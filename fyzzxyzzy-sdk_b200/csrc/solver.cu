@@ -921,39 +921,121 @@ __global__ void __launch_bounds__(256) k_partition_smem(DevState s, uint32_t* lv
 }
 
 // ---------------- row preparation ----------------
+// Joint rows (scene.cpp:7615-7767): one thread per joint.  Distance kinds
+// give one row along the anchor separation; the others lock translation
+// along frame A's axes (prismatic: not X) and rotation through the relative
+// quaternion's vector part (spherical: none; revolute: not X), the rows
+// orthogonalised in the inverse-mass metric in order.
+__device__ __forceinline__ uint32_t joint_row_count(uint32_t kind) {
+    return kind <= kJointAnchored ? 1u : kind == kJointSpherical ? 3u : kind == kJointFixed ? 6u : 5u;
+}
 __global__ void k_prep_joints(DevState s) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= s.n_joints) return;
-    const uint32_t a = s.j_a[j], b = s.j_b[j];
+    const uint32_t a = s.j_a[j], b = s.j_b[j], kind = s.j_kind[j];
     const bool da = is_dyn(s, a), db = is_dyn(s, b);
+    if (s.sleep && ((da && (s.b_sleep[a] & kSleeping)) || (db && (s.b_sleep[b] & kSleeping)))) return;
     const float inv_dt = 1.0f / s.dt;
-    const v3 world0 = ld3(s.b_p[a]), world1 = ld3(s.b_p[b]);   // centre anchors
+    const qt qa0 = ldq(s.b_q[a]), qb0 = ldq(s.b_q[b]);
+    const v3 world0 = vadd(ld3(s.b_p[a]), rot_sc(qa0, ld3(s.j_la[j])));
+    const v3 world1 = vadd(ld3(s.b_p[b]), rot_sc(qb0, ld3(s.j_lb[j])));
     const v3 c0 = mass_position(s, a), c1 = mass_position(s, b);
     const v3 ra = vsub(world0, c0), rb = vsub(world1, c1);
     const float m0 = da ? s.b_inv[a].w : 0.0f, m1 = db ? s.b_inv[b].w : 0.0f;
     const v3 rel = vsub(ld3(s.b_v[a]), ld3(s.b_v[b]));
-    const v3 off = {c0.x + ra.x - c1.x - rb.x, c0.y + ra.y - c1.y - rb.y, c0.z + ra.z - c1.z - rb.z};
-    const float dist = sqrtf(vdot(off, off));
-    const v3 axis = dist < 1.192092896e-07f ? v3{1, 0, 0} : v3{off.x / dist, off.y / dist, off.z / dist};
-    const v3 an0 = vcross(ra, axis), an1 = vcross(rb, axis);
-    const v3 ja = da ? xform(load_sbody(s, int32_t(a)), an0) : v3{0, 0, 0};
-    const v3 jb = db ? xform(load_sbody(s, int32_t(b)), an1) : v3{0, 0, 0};
-    const float response = m0 + m1 + vdot(ja, ja) + vdot(jb, jb);
-    if (!(response > 0.0f) || !isfinite(response)) atomicOr(s.err, kErrLogic);
-    const float rcp = 1.0f / response;
-    JointRow r;
-    r.axis[0] = axis.x; r.axis[1] = axis.y; r.axis[2] = axis.z;
-    r.ang_a[0] = ja.x; r.ang_a[1] = ja.y; r.ang_a[2] = ja.z;
-    r.ang_b[0] = jb.x; r.ang_b[1] = jb.y; r.ang_b[2] = jb.z;
-    r.ima = m0; r.imb = m1;
-    r.vel_mult = -rcp;
-    const float speed = vdot(axis, rel) + vdot(an0, ld3(s.b_w[a])) - vdot(an1, ld3(s.b_w[b]));
-    const float err = dist - s.j_len[j];
-    r.constant = -rcp * (err * inv_dt + speed);
-    r.unbiased = -rcp * speed;
-    r.applied = 0.0f;
-    r.pad = 0.0f;
-    s.jrow[j] = r;
+    const v3 wa = ld3(s.b_w[a]), wb = ld3(s.b_w[b]);
+    const SBody A = load_sbody(s, da ? int32_t(a) : -1), B = load_sbody(s, db ? int32_t(b) : -1);
+    JointRow* out = s.jrow + s.j_row[j];
+    uint32_t emitted = 0;
+    auto emit = [&](v3 axis, v3 a0, v3 a1, v3 ja, v3 jb, float error, float response) {
+        if (!(response > 0.0f) || !isfinite(response)) atomicOr(s.err, kErrLogic);
+        const float rcp = 1.0f / response;
+        JointRow r;
+        r.axis[0] = axis.x; r.axis[1] = axis.y; r.axis[2] = axis.z;
+        r.ang_a[0] = ja.x; r.ang_a[1] = ja.y; r.ang_a[2] = ja.z;
+        r.ang_b[0] = jb.x; r.ang_b[1] = jb.y; r.ang_b[2] = jb.z;
+        r.ima = m0; r.imb = m1;
+        r.vel_mult = -rcp;
+        const float speed = vdot(axis, rel) + vdot(a0, wa) - vdot(a1, wb);
+        r.constant = -rcp * (error * inv_dt + speed);
+        r.unbiased = -rcp * speed;
+        r.applied = 0.0f;
+        r.pad = 0.0f;
+        if (!isfinite(r.constant) || !isfinite(r.unbiased)) atomicOr(s.err, kErrNonFinite);
+        out[emitted++] = r;
+    };
+    if (kind <= kJointAnchored) {
+        const v3 off = {c0.x + ra.x - c1.x - rb.x, c0.y + ra.y - c1.y - rb.y, c0.z + ra.z - c1.z - rb.z};
+        const float dist = sqrtf(vdot(off, off));
+        const v3 axis = dist < 1.192092896e-07f ? v3{1, 0, 0} : v3{off.x / dist, off.y / dist, off.z / dist};
+        const v3 an0 = vcross(ra, axis), an1 = vcross(rb, axis);
+        const v3 ja = da ? xform(A, an0) : v3{0, 0, 0};
+        const v3 jb = db ? xform(B, an1) : v3{0, 0, 0};
+        emit(axis, an0, an1, ja, jb, dist - s.j_len[j], m0 + m1 + vdot(ja, ja) + vdot(jb, jb));
+        return;
+    }
+    const qt qa = qmul(qa0, ldq(s.j_qa[j]));
+    const v3 error_p = rotinv_sc(qa, vsub(world0, world1));
+    v3 ea = {0, 0, 0}, va = {0, 0, 0}, vb = {0, 0, 0}, c = {0, 0, 0};
+    float dd = 0.0f, overlap = 0.0f;
+    if (kind != kJointSpherical) {
+        qt qb = qmul(qb0, ldq(s.j_qb[j]));
+        if (qa.x * qb.x + qa.y * qb.y + qa.z * qb.z + qa.w * qb.w < 0.0f) qb = {-qb.x, -qb.y, -qb.z, -qb.w};
+        const qt eq = qmul(qconj(qa), qb);
+        ea = {eq.x, eq.y, eq.z};
+        va = {qa.x, qa.y, qa.z};
+        vb = {qb.x, qb.y, qb.z};
+        dd = qa.w * qb.w - vdot(va, vb);
+        overlap = qa.w * qb.w + vdot(va, vb);
+        c = {qa.w * vb.x + qb.w * va.x, qa.w * vb.y + qb.w * va.y, qa.w * vb.z + qb.w * va.z};
+    }
+    const float errors[6] = {error_p.x, error_p.y, error_p.z, -ea.x, -ea.y, -ea.z};
+    const float avc[3] = {va.x, va.y, va.z}, bvc[3] = {vb.x, vb.y, vb.z};
+    const v3 diag[3] = {{dd, c.z, -c.y}, {-c.z, dd, c.x}, {c.y, -c.x, dd}};
+    struct Eq { v3 lin, a0, a1, ja, jb; float err, inv; };
+    Eq er[6];
+    const uint32_t count = joint_row_count(kind);
+    for (uint32_t k = 0; k < count; ++k) {
+        const uint32_t comp = k + (kind == kJointPrismatic ? 1u : 0u) + (kind == kJointRevolute && k >= 3u ? 1u : 0u);
+        Eq e;
+        e.err = errors[comp];
+        if (comp < 3u) {
+            const v3 basis = {comp == 0u ? 1.0f : 0.0f, comp == 1u ? 1.0f : 0.0f, comp == 2u ? 1.0f : 0.0f};
+            e.lin = rot_sc(qa, basis);
+            const v3 arm = kind == kJointPrismatic ? vsub(world1, c0) : ra;
+            e.a0 = vcross(arm, e.lin);
+            e.a1 = vcross(rb, e.lin);
+        } else {
+            const uint32_t q = comp - 3u;
+            const v3 v = diag[q];
+            e.lin = {0, 0, 0};
+            e.a0 = {0.5f * (va.x * bvc[q] + vb.x * avc[q] + v.x), 0.5f * (va.y * bvc[q] + vb.y * avc[q] + v.y),
+                    0.5f * (va.z * bvc[q] + vb.z * avc[q] + v.z)};
+            if (overlap == 0.0f) {
+                // the relative quaternion's Jacobian is singular at 180 degrees
+                const float t = -FLT_EPSILON;
+                const v3 basis = {q == 0u ? 1.0f : 0.0f, q == 1u ? 1.0f : 0.0f, q == 2u ? 1.0f : 0.0f};
+                e.a0 = {e.a0.x - basis.x * t, e.a0.y - basis.y * t, e.a0.z - basis.z * t};
+            }
+            e.a1 = e.a0;
+        }
+        e.ja = da ? xform(A, e.a0) : v3{0, 0, 0};
+        e.jb = db ? xform(B, e.a1) : v3{0, 0, 0};
+        for (uint32_t p = 0; p < k; ++p) {
+            const Eq& f = er[p];
+            const float t = ((m0 + m1) * vdot(e.lin, f.lin) + vdot(e.ja, f.ja) + vdot(e.jb, f.jb)) * f.inv;
+            e.lin = {e.lin.x - f.lin.x * t, e.lin.y - f.lin.y * t, e.lin.z - f.lin.z * t};
+            e.a0 = {e.a0.x - f.a0.x * t, e.a0.y - f.a0.y * t, e.a0.z - f.a0.z * t};
+            e.a1 = {e.a1.x - f.a1.x * t, e.a1.y - f.a1.y * t, e.a1.z - f.a1.z * t};
+            e.ja = {e.ja.x - f.ja.x * t, e.ja.y - f.ja.y * t, e.ja.z - f.ja.z * t};
+            e.jb = {e.jb.x - f.jb.x * t, e.jb.y - f.jb.y * t, e.jb.z - f.jb.z * t};
+            e.err -= f.err * t;
+        }
+        const float response = (m0 + m1) * vdot(e.lin, e.lin) + vdot(e.ja, e.ja) + vdot(e.jb, e.jb);
+        e.inv = response > 0.0f ? 1.0f / response : 0.0f;
+        er[k] = e;
+        emit(e.lin, e.a0, e.a1, e.ja, e.jb, e.err, response);
+    }
 }
 
 __global__ void k_prep_contacts(DevState s) {
@@ -1203,7 +1285,6 @@ __device__ __forceinline__ int32_t unpack_local(uint32_t v) { return v == 0xffff
 template <class D, bool kEagerFriction = true>
 __device__ void solve_desc(const DevState& s, uint32_t d, uint32_t lid, int it, int pos, int vel, const D& D_) {
     if (d < s.n_joints) {
-        JointRow& r = s.jrow[d];
         int32_t b0, b1;
         if constexpr (D::kLocal) {
             b0 = unpack_local(lid & 0xffffu);
@@ -1215,20 +1296,26 @@ __device__ void solve_desc(const DevState& s, uint32_t d, uint32_t lid, int it, 
         v3 av, aw, bv, bw;
         D_.load(b0, av, aw);
         D_.load(b1, bv, bw);
-        const v3 ax = lv(r.axis), ja = lv(r.ang_a), jb = lv(r.ang_b);
-        const float nd = ax.x * (av.x - bv.x) + ax.y * (av.y - bv.y) + ax.z * (av.z - bv.z) + vdot(ja, aw) - vdot(jb, bw);
-        const float cst = it < pos ? r.constant : r.unbiased;
-        const float nx = sclamp(r.applied + nd * r.vel_mult + cst, -FLT_MAX, FLT_MAX);
-        const float imp = nx - r.applied;
-        const float ia = imp * r.ima, ib = imp * r.imb;
-        av = {av.x + ia * ax.x, av.y + ia * ax.y, av.z + ia * ax.z};
-        bv = {bv.x - ib * ax.x, bv.y - ib * ax.y, bv.z - ib * ax.z};
-        aw = {aw.x + imp * ja.x, aw.y + imp * ja.y, aw.z + imp * ja.z};
-        bw = {bw.x - imp * jb.x, bw.y - imp * jb.y, bw.z - imp * jb.z};
+        // the joint's rows in order (scene.cpp:8905-8945)
+        const uint32_t r0 = s.j_row[d], nr = joint_row_count(s.j_kind[d]);
+        for (uint32_t q = 0; q < nr; ++q) {
+            JointRow& r = s.jrow[r0 + q];
+            const v3 ax = lv(r.axis), ja = lv(r.ang_a), jb = lv(r.ang_b);
+            const float nd = ax.x * (av.x - bv.x) + ax.y * (av.y - bv.y) + ax.z * (av.z - bv.z) + vdot(ja, aw) -
+                             vdot(jb, bw);
+            const float cst = it < pos ? r.constant : r.unbiased;
+            const float nx = sclamp(r.applied + nd * r.vel_mult + cst, -FLT_MAX, FLT_MAX);
+            const float imp = nx - r.applied;
+            const float ia = imp * r.ima, ib = imp * r.imb;
+            av = {av.x + ia * ax.x, av.y + ia * ax.y, av.z + ia * ax.z};
+            bv = {bv.x - ib * ax.x, bv.y - ib * ax.y, bv.z - ib * ax.z};
+            aw = {aw.x + imp * ja.x, aw.y + imp * ja.y, aw.z + imp * ja.z};
+            bw = {bw.x - imp * jb.x, bw.y - imp * jb.y, bw.z - imp * jb.z};
+            r.applied = nx;
+            if (s.tape_j) s.tape_j[size_t(it) * s.n_jrows + r0 + q] = nx;
+        }
         D_.store(b0, av, aw);
         D_.store(b1, bv, bw);
-        r.applied = nx;
-        if (s.tape_j) s.tape_j[size_t(it) * s.n_joints + d] = nx;
         return;
     }
     const uint32_t m = d - s.n_joints;

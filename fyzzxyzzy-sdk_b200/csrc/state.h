@@ -91,9 +91,14 @@ struct DevState {
     FrictionRow* frow = nullptr;       // 4 per touching manager
 
     // joints (static, sorted by scene then constraint slot descending)
-    uint32_t *j_a = nullptr, *j_b = nullptr;
+    uint32_t *j_a = nullptr, *j_b = nullptr;  // descriptor bodies (distance: ordered pair; others: authored)
+    uint32_t* j_kind = nullptr;         // kJoint*
+    uint32_t* j_row = nullptr;          // first row in jrow (rows in joint order)
+    float4 *j_la = nullptr, *j_lb = nullptr;   // local anchor positions
+    float4 *j_qa = nullptr, *j_qb = nullptr;   // local frame orientations (fixed .. prismatic)
     float* j_len = nullptr;
-    JointRow* jrow = nullptr;
+    JointRow* jrow = nullptr;           // n_jrows rows
+    uint32_t n_jrows = 0;
 
     // solver bodies
     float4 *sb_dv = nullptr, *sb_dw = nullptr, *sb_mdv = nullptr, *sb_mdw = nullptr;

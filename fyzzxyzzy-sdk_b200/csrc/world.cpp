@@ -62,7 +62,19 @@ struct HostShape {
     std::array<float, 4> mat{0.5f, 0.5f, 0.2f, 0.0f};   // static, dynamic, restitution, rest offset
     float contact_offset = 0.02f;
 };
-struct HostJoint { uint32_t a = 0, b = 0; float len = 0.0f; uint32_t scene = 0; uint32_t slot = 0; };
+// A joint: its descriptor bodies (distance kinds: the ordered pair with the
+// anchors as authored, scene.cpp:3097-3108; other kinds: the authored order,
+// record.swapped, scene.cpp:3050-3060), kind and local frames.
+struct HostJoint {
+    uint32_t a = 0, b = 0;
+    float len = 0.0f;
+    uint32_t scene = 0, slot = 0, kind = kJointCenter;
+    std::array<float, 3> la{0, 0, 0}, lb{0, 0, 0};
+    std::array<float, 4> qa{0, 0, 0, 1}, qb{0, 0, 0, 1};
+};
+uint32_t joint_rows(uint32_t kind) {
+    return kind <= kJointAnchored ? 1u : kind == kJointSpherical ? 3u : kind == kJointFixed ? 6u : 5u;
+}
 
 void check_cuda(cudaError_t e, const char* what) {
     if (e != cudaSuccess)
@@ -363,18 +375,36 @@ public:
         mass_dirty_ = true;
     }
     uint64_t add_distance(uint32_t a, uint32_t b, float len) {
+        const float zero7[7] = {0, 0, 0, 0, 0, 0, 1};
+        return add_joint(kJointCenter, a, b, zero7, zero7, len);
+    }
+    // World::add_*_constraint (src/world.cpp:231-276) then Scene::create_*
+    // (scene.cpp:3046-3141).  local_a / local_b: position 3 + orientation 4.
+    uint64_t add_joint(uint32_t kind, uint32_t a, uint32_t b, const float* local_a, const float* local_b, float len) {
+        if (kind > kJointPrismatic) throw std::invalid_argument("Unknown joint kind");
         const HostBody& A = require_body(a);
         const HostBody& B = require_body(b);
-        if (a == b || (!A.dynamic && !B.dynamic))
-            throw std::invalid_argument("Constraint requires two distinct actors and a rigid node");
-        if (A.scene != B.scene) throw std::invalid_argument("Constraint endpoints must share a scene");
-        if (!std::isfinite(len) || len < 0.0f)
+        if (a == b) throw std::invalid_argument("Joint requires distinct actors");
+        if (kind <= kJointAnchored && (!std::isfinite(len) || len < 0.0f))
             throw std::invalid_argument("Rigid 1D distance must be finite and nonnegative");
-        pull_state();
         HostJoint j;
-        j.a = std::min(a, b);
-        j.b = std::max(a, b);
-        j.len = len;
+        if (kind != kJointCenter) {
+            validate_position(local_a);
+            validate_position(local_b);
+            j.la = {local_a[0], local_a[1], local_a[2]};
+            j.lb = {local_b[0], local_b[1], local_b[2]};
+        }
+        if (kind >= kJointFixed) {
+            j.qa = validated_orientation(local_a + 3);
+            j.qb = validated_orientation(local_b + 3);
+        }
+        if (!A.dynamic && !B.dynamic) throw std::logic_error("Rigid constraint requires a dynamic solver node");
+        if (A.scene != B.scene) throw std::invalid_argument("Constraint endpoints must share a scene");
+        pull_state();
+        j.kind = kind;
+        j.a = kind <= kJointAnchored ? std::min(a, b) : a;
+        j.b = kind <= kJointAnchored ? std::max(a, b) : b;
+        j.len = kind <= kJointAnchored ? len : 0.0f;
         j.scene = A.scene;
         uint32_t slot = 0;
         for (const auto& o : joints_) if (o.scene == j.scene) ++slot;
@@ -567,11 +597,11 @@ public:
         dalloc(f.sb_sqrt_i, 3 * nb, o);
         dalloc(f.man_list, cap, o); dalloc(f.mh, cap, o);
         dalloc(f.nrow, 4 * cap, o); dalloc(f.frow, 4 * cap, o);
-        dalloc(f.jrow, std::max<size_t>(d_.n_joints, 1), o);
+        dalloc(f.jrow, std::max<size_t>(d_.n_jrows, 1), o);
         dalloc(f.pts, 4 * cap, o);
         dalloc(f.cur.key, cap, o); dalloc(f.cur.fric, cap, o); dalloc(f.cur.count, cap, o); dalloc(f.cur.n, 1, o);
         dalloc(f.tn, passes * cap * 4, o); dalloc(f.tf, passes * cap * 4, o);
-        dalloc(f.tj, passes * std::max<size_t>(d_.n_joints, 1), o);
+        dalloc(f.tj, passes * std::max<size_t>(d_.n_jrows, 1), o);
         dalloc(f.d_val2, dc, o); dalloc(f.d_lbod, dc, o);
         dalloc(f.lvl_bound, 2 * dc + 2, o); dalloc(f.isl_bod, 2 * dc + 2, o);
         dalloc(f.isl_begin, dc + 1, o); dalloc(f.isl_end, dc + 1, o); dalloc(f.isl_nbod, dc + 1, o);
@@ -611,6 +641,9 @@ public:
     }
     void rollout_begin(uint32_t steps, uint32_t every) {
         if (steps == 0 || every == 0) throw std::invalid_argument("Rollout needs steps and a checkpoint interval");
+        for (const auto& j : joints_)
+            if (j.kind != kJointCenter)
+                throw std::logic_error("Differentiable rollouts support center distance joints only");
         check_cuda(cudaSetDevice(device_), "cudaSetDevice");
         ensure_device();
         pull_state();
@@ -645,10 +678,10 @@ public:
         dalloc(A.im, nb, roll_owned_); dalloc(A.g_im, nb, roll_owned_);
         dalloc(A.g_fs, d_.n_shapes, roll_owned_); dalloc(A.g_fd, d_.n_shapes, roll_owned_);
         dalloc(A.nrow, 4 * cap, roll_owned_); dalloc(A.frow, 4 * cap, roll_owned_);
-        dalloc(A.jrow, std::max<size_t>(d_.n_joints, 1), roll_owned_);
+        dalloc(A.jrow, std::max<size_t>(d_.n_jrows, 1), roll_owned_);
         dalloc(A.hd, cap, roll_owned_);
         dalloc(A.yn, 4 * cap, roll_owned_); dalloc(A.yf, 4 * cap, roll_owned_);
-        dalloc(A.yj, std::max<size_t>(d_.n_joints, 1), roll_owned_);
+        dalloc(A.yj, std::max<size_t>(d_.n_jrows, 1), roll_owned_);
         dalloc(A.mark, nb, roll_owned_);
         dalloc(A.epoch, 1, roll_owned_);
         check_cuda(cudaMemsetAsync(A.mark, 0, nb * 4, stream_), "memset");
@@ -1453,7 +1486,10 @@ private:
         dalloc(d_.sw_found, nf, owned_);
         dalloc(d_.own_cnt, ns, owned_); dalloc(d_.own_off, ns, owned_); dalloc(d_.own_cur, ns, owned_);
         dalloc(d_.j_a, joints_.size(), owned_); dalloc(d_.j_b, joints_.size(), owned_);
-        dalloc(d_.j_len, joints_.size(), owned_); dalloc(d_.jrow, joints_.size(), owned_);
+        dalloc(d_.j_len, joints_.size(), owned_);
+        dalloc(d_.j_kind, joints_.size(), owned_); dalloc(d_.j_row, joints_.size(), owned_);
+        dalloc(d_.j_la, joints_.size(), owned_); dalloc(d_.j_lb, joints_.size(), owned_);
+        dalloc(d_.j_qa, joints_.size(), owned_); dalloc(d_.j_qb, joints_.size(), owned_);
         dalloc(d_.sb_dv, nb, owned_); dalloc(d_.sb_dw, nb, owned_); dalloc(d_.sb_mdv, nb, owned_);
         dalloc(d_.sb_mdw, nb, owned_); dalloc(d_.sb_v, nb, owned_); dalloc(d_.sb_w, nb, owned_);
         dalloc(d_.sb_sqrt_i, size_t(nb) * 3, owned_);
@@ -1489,9 +1525,21 @@ private:
         std::stable_sort(js.begin(), js.end(), [](const HostJoint& a, const HostJoint& b) {
             return a.scene != b.scene ? a.scene < b.scene : a.slot > b.slot;
         });
-        std::vector<uint32_t> ja(js.size()), jb(js.size());
+        std::vector<uint32_t> ja(js.size()), jb(js.size()), jk(js.size()), jr(js.size());
         std::vector<float> jl(js.size());
-        for (size_t i = 0; i < js.size(); ++i) { ja[i] = js[i].a; jb[i] = js[i].b; jl[i] = js[i].len; }
+        std::vector<float4> jla(js.size()), jlb(js.size()), jqa(js.size()), jqb(js.size());
+        uint32_t nrows = 0;
+        for (size_t i = 0; i < js.size(); ++i) {
+            const HostJoint& h = js[i];
+            ja[i] = h.a; jb[i] = h.b; jl[i] = h.len; jk[i] = h.kind; jr[i] = nrows;
+            nrows += joint_rows(h.kind);
+            jla[i] = make_float4(h.la[0], h.la[1], h.la[2], 0);
+            jlb[i] = make_float4(h.lb[0], h.lb[1], h.lb[2], 0);
+            jqa[i] = make_float4(h.qa[0], h.qa[1], h.qa[2], h.qa[3]);
+            jqb[i] = make_float4(h.qb[0], h.qb[1], h.qb[2], h.qb[3]);
+        }
+        d_.n_jrows = nrows;
+        dalloc(d_.jrow, nrows, owned_);
         // constraints counted on their dynamic endpoints (scene.cpp:2728-2749)
         std::vector<uint32_t> jcount(nb, 0u);
         for (const auto& j : js) {
@@ -1508,6 +1556,9 @@ private:
         upload(d_.s_frank, frank, stream_); upload(d_.s_dynrank, dynrank, stream_);
         upload(d_.s_static_pairs, static_pairs, stream_);
         upload(d_.j_a, ja, stream_); upload(d_.j_b, jb, stream_); upload(d_.j_len, jl, stream_);
+        upload(d_.j_kind, jk, stream_); upload(d_.j_row, jr, stream_);
+        upload(d_.j_la, jla, stream_); upload(d_.j_lb, jlb, stream_);
+        upload(d_.j_qa, jqa, stream_); upload(d_.j_qb, jqb, stream_);
         uploaded_ = true;
         upload_bodies();
         // pair capacity: every plane pair plus a generous overlap budget
@@ -1782,6 +1833,37 @@ uint64_t fyzz_b200_read_sorted_min_x(fyzz_b200_world* w, uint32_t scene, uint32_
     uint64_t n = 0;
     if (guarded(w, [&](auto& W) { n = W.read_sorted_min_x(scene, values, ids, cap); })) return 0;
     return n;
+}
+static int add_joint_abi(fyzz_b200_world* w, uint32_t kind, uint32_t a, uint32_t b, const float* la,
+                         const float* lb, float distance, uint64_t* out) {
+    if (!la || !lb) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) {
+        const uint64_t id = W.add_joint(kind, a, b, la, lb, distance);
+        if (out) *out = id;
+    });
+}
+int fyzz_b200_add_anchored_distance_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b, const float local_a[3],
+                                               const float local_b[3], float distance, uint64_t* id_out) {
+    if (!local_a || !local_b) return FYZZ_B200_INVALID_ARGUMENT;
+    const float la[7] = {local_a[0], local_a[1], local_a[2], 0, 0, 0, 1};
+    const float lb[7] = {local_b[0], local_b[1], local_b[2], 0, 0, 0, 1};
+    return add_joint_abi(w, fyzz::b200::kJointAnchored, a, b, la, lb, distance, id_out);
+}
+int fyzz_b200_add_fixed_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b, const float local_a[7],
+                                   const float local_b[7], uint64_t* id_out) {
+    return add_joint_abi(w, fyzz::b200::kJointFixed, a, b, local_a, local_b, 0.0f, id_out);
+}
+int fyzz_b200_add_spherical_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b, const float local_a[7],
+                                       const float local_b[7], uint64_t* id_out) {
+    return add_joint_abi(w, fyzz::b200::kJointSpherical, a, b, local_a, local_b, 0.0f, id_out);
+}
+int fyzz_b200_add_revolute_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b, const float local_a[7],
+                                      const float local_b[7], uint64_t* id_out) {
+    return add_joint_abi(w, fyzz::b200::kJointRevolute, a, b, local_a, local_b, 0.0f, id_out);
+}
+int fyzz_b200_add_prismatic_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b, const float local_a[7],
+                                       const float local_b[7], uint64_t* id_out) {
+    return add_joint_abi(w, fyzz::b200::kJointPrismatic, a, b, local_a, local_b, 0.0f, id_out);
 }
 int fyzz_b200_set_sleeping(fyzz_b200_world* w, int enabled) {
     return guarded(w, [&](auto& W) { W.set_sleeping(enabled != 0); });

@@ -99,6 +99,26 @@ int fyzz_b200_set_body_angular_velocity(fyzz_b200_world* w, uint32_t body, const
 /* World::add_center_distance_constraint (world.h:438) */
 int fyzz_b200_add_center_distance_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b,
                                              float distance, uint64_t* id_out);
+/* World::add_anchored_distance_constraint (world.h:441): equal-limit 1D
+ * joint between body-local anchors.  As in the reference, the anchors are
+ * applied to the lower and higher BodyId in the order given. */
+int fyzz_b200_add_anchored_distance_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b, const float local_a[3],
+                                               const float local_b[3], float distance, uint64_t* id_out);
+/* World::add_fixed_constraint / add_spherical_constraint /
+ * add_revolute_constraint / add_prismatic_constraint (world.h:445-457):
+ * local frames are position(3) + orientation xyzw(4) in each body's frame.
+ * Fixed locks the relative pose (6 rows); spherical makes the frame origins
+ * coincide (3 rows); revolute also aligns the local X axes (5 rows, free
+ * rotation about X); prismatic keeps the relative orientation and the
+ * transverse position (5 rows, free translation along frame A's X). */
+int fyzz_b200_add_fixed_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b, const float local_a[7],
+                                   const float local_b[7], uint64_t* id_out);
+int fyzz_b200_add_spherical_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b, const float local_a[7],
+                                       const float local_b[7], uint64_t* id_out);
+int fyzz_b200_add_revolute_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b, const float local_a[7],
+                                      const float local_b[7], uint64_t* id_out);
+int fyzz_b200_add_prismatic_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b, const float local_a[7],
+                                       const float local_b[7], uint64_t* id_out);
 
 /* Bulk authoring of one scene with the seeded-workload record layout:
  * bodies(14 floats: position 3, orientation 4, velocity 3, angular 3,
