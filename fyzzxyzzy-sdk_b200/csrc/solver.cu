@@ -1752,6 +1752,37 @@ static void join_branches(const Branches* br, cudaStream_t st, int n) {
     }
 }
 
+// Host-buffer transfers: the 14-float body records of read_bodies packed
+// on the device (one D2H), and write_velocities' 6-float records unpacked
+// on the device (one H2D) into the velocities, waking every dynamic body.
+__global__ void k_pack_bodies(DevState s, float* out) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= s.n_bodies) return;
+    const float4 p = s.b_p[b], v = s.b_v[b], q = s.b_q[b], w = s.b_w[b];
+    float* o = out + 14 * size_t(b);
+    o[0] = p.x; o[1] = p.y; o[2] = p.z;
+    o[3] = v.x; o[4] = v.y; o[5] = v.z;
+    o[6] = q.x; o[7] = q.y; o[8] = q.z; o[9] = q.w;
+    o[10] = w.x; o[11] = w.y; o[12] = w.z;
+    o[13] = (s.b_sleep[b] & kSleeping) ? 1.0f : 0.0f;
+}
+__global__ void k_unpack_velocities(DevState s, const float* v6) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= s.n_bodies) return;
+    const bool dyn = is_dyn(s, b);
+    const float* r = v6 + 6 * size_t(b);
+    s.b_v[b] = dyn ? make_float4(r[0], r[1], r[2], 0.0f) : make_float4(0, 0, 0, 0);
+    s.b_w[b] = dyn ? make_float4(r[3], r[4], r[5], 0.0f) : make_float4(0, 0, 0, 0);
+}
+void enqueue_pack_bodies(const DevState& s, float* out, cudaStream_t st) {
+    if (s.n_bodies) k_pack_bodies<<<grid_for(s.n_bodies, 256, 1u << 30), 256, 0, st>>>(s, out);
+}
+void enqueue_unpack_velocities(const DevState& s, const float* v6, cudaStream_t st) {
+    if (!s.n_bodies) return;
+    k_unpack_velocities<<<grid_for(s.n_bodies, 256, 1u << 30), 256, 0, st>>>(s, v6);
+    k_wake_bodies<<<grid_for(s.n_bodies, 256, 1u << 30), 256, 0, st>>>(s);
+}
+
 void enqueue_wake_bodies(const DevState& s, cudaStream_t st) {
     if (s.n_bodies) k_wake_bodies<<<grid_for(s.n_bodies, 256, 1u << 30), 256, 0, st>>>(s);
 }

@@ -240,6 +240,11 @@ void enqueue_events(const DevState& s, cudaStream_t st);
 // current before the first step or capture.
 // Wakes every dynamic body (as an authored velocity on each would).
 void enqueue_wake_bodies(const DevState& s, cudaStream_t st);
+// 14-float body records (position, velocity, orientation, angular
+// velocity, sleeping) into out (device memory).
+void enqueue_pack_bodies(const DevState& s, float* out, cudaStream_t st);
+// 6-float velocity records (device memory) into the bodies; wakes them.
+void enqueue_unpack_velocities(const DevState& s, const float* v6, cudaStream_t st);
 void init_solver_kernels();
 // Island size classes (descriptors per island).
 constexpr uint32_t kSmallIsland = 96;     // one warp

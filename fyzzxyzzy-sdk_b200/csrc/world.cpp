@@ -1017,23 +1017,12 @@ public:
             for (uint32_t i = 0; i < n; ++i) pack_host(i, out + 14 * size_t(i));
             return;
         }
-        stage_.resize(size_t(n) * 4);
-        check_cuda(cudaMemcpyAsync(stage_.data(), d_.b_p, size_t(n) * 16, cudaMemcpyDeviceToHost, stream_), "read");
-        check_cuda(cudaMemcpyAsync(stage_.data() + n, d_.b_v, size_t(n) * 16, cudaMemcpyDeviceToHost, stream_), "read");
-        check_cuda(cudaMemcpyAsync(stage_.data() + 2 * size_t(n), d_.b_q, size_t(n) * 16, cudaMemcpyDeviceToHost, stream_), "read");
-        check_cuda(cudaMemcpyAsync(stage_.data() + 3 * size_t(n), d_.b_w, size_t(n) * 16, cudaMemcpyDeviceToHost, stream_), "read");
-        sleep_stage_.resize(n);
-        check_cuda(cudaMemcpyAsync(sleep_stage_.data(), d_.b_sleep, size_t(n) * 4, cudaMemcpyDeviceToHost, stream_), "read");
+        // packed on the device, one copy into the caller's buffer
+        if (!d_pack_) dalloc(d_pack_, 14 * size_t(d_.n_bodies), owned_);
+        enqueue_pack_bodies(d_, d_pack_, stream_);
+        check_cuda(cudaGetLastError(), "pack");
+        check_cuda(cudaMemcpyAsync(out, d_pack_, size_t(n) * 56, cudaMemcpyDeviceToHost, stream_), "read");
         check_cuda(cudaStreamSynchronize(stream_), "read sync");
-        for (uint32_t i = 0; i < n; ++i) {
-            float* o = out + 14 * size_t(i);
-            const float4 p = stage_[i], v = stage_[n + i], q = stage_[2 * size_t(n) + i], w = stage_[3 * size_t(n) + i];
-            o[0] = p.x; o[1] = p.y; o[2] = p.z;
-            o[3] = v.x; o[4] = v.y; o[5] = v.z;
-            o[6] = q.x; o[7] = q.y; o[8] = q.z; o[9] = q.w;
-            o[10] = w.x; o[11] = w.y; o[12] = w.z;
-            o[13] = (sleep_stage_[i] & kSleeping) ? 1.0f : 0.0f;
-        }
     }
     void body_state(uint32_t id, fyzz_b200_body_state_t* out) {
         require_body(id);
@@ -1062,17 +1051,12 @@ public:
     void write_velocities(const float* v6, uint32_t n) {
         if (n != bodies_.size()) throw std::invalid_argument("Body count mismatch");
         ensure_device();
-        stage_.resize(size_t(n) * 2);
-        for (uint32_t i = 0; i < n; ++i) {
-            const float* r = v6 + 6 * size_t(i);
-            const bool dyn = bodies_[i].dynamic;
-            stage_[i] = dyn ? make_float4(r[0], r[1], r[2], 0.0f) : make_float4(0, 0, 0, 0);
-            stage_[n + i] = dyn ? make_float4(r[3], r[4], r[5], 0.0f) : make_float4(0, 0, 0, 0);
-        }
-        check_cuda(cudaMemcpyAsync(d_.b_v, stage_.data(), size_t(n) * 16, cudaMemcpyHostToDevice, stream_), "write");
-        check_cuda(cudaMemcpyAsync(d_.b_w, stage_.data() + n, size_t(n) * 16, cudaMemcpyHostToDevice, stream_), "write");
-        enqueue_wake_bodies(d_, stream_);
-        check_cuda(cudaGetLastError(), "wake");
+        // one copy of the caller's records, unpacked (and every body woken)
+        // on the device; the caller's buffer is free again on return
+        if (!d_vel6_) dalloc(d_vel6_, 6 * size_t(d_.n_bodies), owned_);
+        check_cuda(cudaMemcpyAsync(d_vel6_, v6, size_t(n) * 24, cudaMemcpyHostToDevice, stream_), "write");
+        enqueue_unpack_velocities(d_, d_vel6_, stream_);
+        check_cuda(cudaGetLastError(), "unpack");
         check_cuda(cudaStreamSynchronize(stream_), "write sync");
     }
     void counts(uint64_t* out) {
@@ -1306,6 +1290,8 @@ private:
         release_segment_graphs();
         for (void* p : owned_) cudaFree(p);
         owned_.clear();
+        d_pack_ = nullptr;
+        d_vel6_ = nullptr;
         for (void* p : pair_owned_) cudaFree(p);
         pair_owned_.clear();
         uploaded_ = false;
@@ -1585,6 +1571,8 @@ private:
     std::vector<void*> owned_, pair_owned_;
     float4 *bk_p_ = nullptr, *bk_q_ = nullptr, *bk_v_ = nullptr, *bk_w_ = nullptr, *bk_sacc_ = nullptr;
     float* bk_wake_ = nullptr;
+    float* d_pack_ = nullptr;    // read_bodies records (owned, allocated on first use)
+    float* d_vel6_ = nullptr;    // write_velocities records
     uint32_t* bk_sleep_ = nullptr;
     bool sleep_enabled_ = true;
     cudaGraphExec_t graphs_[4] = {nullptr, nullptr, nullptr, nullptr};   // [parity + 2 * sleeping]
@@ -1609,21 +1597,6 @@ private:
     uint32_t last_err_ = 0;
     uint32_t* host_err_ = nullptr;
     uint32_t kernels_per_step_ = 0;
-    // Pinned staging for the host-buffer API (read_bodies, write_velocities).
-    struct PinnedStage {
-        float4* p = nullptr;
-        size_t n = 0;
-        void resize(size_t m) {
-            if (m <= n) return;
-            if (p) cudaFreeHost(p);
-            check_cuda(cudaMallocHost(reinterpret_cast<void**>(&p), m * sizeof(float4)), "cudaMallocHost");
-            n = m;
-        }
-        float4* data() { return p; }
-        float4& operator[](size_t i) { return p[i]; }
-        ~PinnedStage() { if (p) cudaFreeHost(p); }
-    } stage_;
-    std::vector<uint32_t> sleep_stage_;
 };
 
 }  // namespace fyzz::b200
