@@ -39,7 +39,8 @@ EXPORTS = (
     "fyzz_b200_read_step_counters", "fyzz_b200_set_contact_notifications",
     "fyzz_b200_contact_events", "fyzz_b200_rollout_begin", "fyzz_b200_rollout_forward",
     "fyzz_b200_rollout_backward", "fyzz_b200_read_mass_frames", "fyzz_b200_read_friction_anchors",
-    "fyzz_b200_fit_pair_budget", "fyzz_b200_set_sleeping", "fyzz_b200_read_sleep_state", "fyzz_b200_rollout_rewind",
+    "fyzz_b200_fit_pair_budget", "fyzz_b200_set_sleeping", "fyzz_b200_read_sleep_state", "fyzz_b200_set_body_kinematic",
+    "fyzz_b200_set_body_kinematic_target", "fyzz_b200_rollout_rewind",
 )
 STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 
@@ -139,6 +140,8 @@ def lib():
         L.fyzz_b200_read_step_counters.argtypes = [vp, vp, u32]
         L.fyzz_b200_set_contact_notifications.argtypes = [vp, i32]
         L.fyzz_b200_set_sleeping.argtypes = [vp, i32]
+        L.fyzz_b200_set_body_kinematic.argtypes = [vp, u32, i32]
+        L.fyzz_b200_set_body_kinematic_target.argtypes = [vp, u32, vp]
         L.fyzz_b200_read_sleep_state.argtypes = [vp, vp, vp, vp, vp, u32]
         L.fyzz_b200_rollout_begin.argtypes = [vp, u32, u32]
         L.fyzz_b200_rollout_rewind.argtypes = [vp]
@@ -398,6 +401,15 @@ class World:
         out = np.zeros(n, np.uint32)
         lib().fyzz_b200_read_levels(self.h, _p(out), n)
         return out
+
+    def set_body_kinematic(self, body: int, enabled: bool = True):
+        """World::set_body_kinematic (reference world.h:505)."""
+        self._check(lib().fyzz_b200_set_body_kinematic(self.h, body, 1 if enabled else 0))
+
+    def set_body_kinematic_target(self, body: int, pose):
+        """World::set_body_kinematic_target: position(3) + quaternion xyzw(4)."""
+        p = np.asarray(pose, np.float32).reshape(7).copy()
+        self._check(lib().fyzz_b200_set_body_kinematic_target(self.h, body, _p(p)))
 
     def set_sleeping(self, enabled: bool = True):
         """Sleeping on (default, as in the reference scene) or off (wakes every body)."""

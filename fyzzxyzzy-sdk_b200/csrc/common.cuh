@@ -15,9 +15,13 @@ namespace fyzz::b200 {
 using std::isfinite;
 
 enum : uint32_t { kBox = 0, kSphere = 1, kPlane = 2 };
-enum : uint32_t { kBodyDynamic = 1u };
-// b_sleep bits
-enum : uint32_t { kSleeping = 1u, kReady = 2u };
+enum : uint32_t { kBodyDynamic = 1u, kBodyKinematic = 2u };
+// b_sleep bits.  A kinematic body also uses the last three: a target
+// waiting for the step (kKinPending, set on the host; cleared when the step
+// moves the body there), a target set since the last step (kKinNew: its
+// touching partners are woken) and the step after it reached its target
+// (kKinSettling: at rest, still reported active).
+enum : uint32_t { kSleeping = 1u, kReady = 2u, kKinPending = 4u, kKinNew = 8u, kKinSettling = 16u };
 // joint kinds: the two distance authorings, then JointKind (scene.h:1528)
 enum : uint32_t { kJointCenter = 0u, kJointAnchored = 1u, kJointFixed = 2u, kJointSpherical = 3u,
                   kJointRevolute = 4u, kJointPrismatic = 5u };

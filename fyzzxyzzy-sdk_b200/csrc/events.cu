@@ -73,7 +73,10 @@ __global__ void k_ev_lost_scatter(DevState s, const uint32_t* flags, const uint3
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < np; j += stride)
         if (flags[j]) s.ev_lost_key[pos[j]] = s.prev.key[j];
 }
+// Sc's active actor (scene.cpp:9207-9216): an awake dynamic body, or a
+// kinematic body moving to its target or settling after it.
 __device__ __forceinline__ bool awake_dynamic(const DevState& s, uint32_t body) {
+    if (s.b_flags[body] & kBodyKinematic) return (s.b_sleep[body] & (kKinPending | kKinSettling)) != 0u;
     return (s.b_flags[body] & kBodyDynamic) && !(s.sleep && (s.b_sleep[body] & kSleeping));
 }
 // Touching managers with an event (rep, scanned into rep_pos) and their

@@ -270,6 +270,20 @@ __global__ void k_desc_keys(DevState s) {
 // ones, each joining the two touch-graph roots of its bodies.
 
 // Counted interactions and activations of current pair k.
+// sl_act bits: activating this step; linked to a kinematic body whose
+// target is pending (its island may not sleep, mark_kinematic_awake,
+// scene.cpp:6430-6463); linked to a kinematic body given a new target (its
+// sleeping or sleep-ready partners wake, scene.cpp:893-911).
+constexpr uint32_t kActActivating = 1u, kActKinematic = 2u, kActKinWake = 4u;
+__device__ __forceinline__ void kinematic_link(const DevState& s, uint32_t a, uint32_t b) {
+    const bool ka = s.b_flags[a] & kBodyKinematic, kb = s.b_flags[b] & kBodyKinematic;
+    if (ka == kb) return;
+    const uint32_t kin = ka ? a : b, dyn = ka ? b : a;
+    if (!is_dyn(s, dyn)) return;
+    const uint32_t f = s.b_sleep[kin];
+    if (f & kKinPending) atomicOr(&s.sl_act[dyn], kActKinematic);
+    if (f & kKinNew) atomicOr(&s.sl_act[dyn], kActKinWake | kActActivating);
+}
 __device__ void sleep_pair(const DevState& s, uint32_t k, bool touch) {
     const uint64_t key = s.cur.key[k];
     const uint32_t ba = s.s_body[uint32_t(key >> 32)], bb = s.s_body[uint32_t(key)];
@@ -280,13 +294,19 @@ __device__ void sleep_pair(const DevState& s, uint32_t k, bool touch) {
     const bool found = pj < 0;
     const bool touched = !found && s.prev.count[pj] > 0u;
     if (found && da && db && (!is_asleep(s, ba) || !is_asleep(s, bb))) {
-        s.sl_act[ba] = 1u;
-        s.sl_act[bb] = 1u;
+        atomicOr(&s.sl_act[ba], kActActivating);
+        atomicOr(&s.sl_act[bb], kActActivating);
     }
     if (touch && !touched) {
-        if (da) { s.sl_act[ba] = 1u; atomicAnd(&s.b_sleep[ba], ~kReady); }
-        if (db) { s.sl_act[bb] = 1u; atomicAnd(&s.b_sleep[bb], ~kReady); }
+        if (da) { atomicOr(&s.sl_act[ba], kActActivating); atomicAnd(&s.b_sleep[ba], ~kReady); }
+        if (db) { atomicOr(&s.sl_act[bb], kActActivating); atomicAnd(&s.b_sleep[bb], ~kReady); }
     }
+    if (touch && s.n_kinematic) kinematic_link(s, ba, bb);
+}
+// Joints linking a dynamic body to a kinematic one act on sleep as touches do.
+__global__ void k_sleep_kinematic_joints(DevState s) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < s.n_joints) kinematic_link(s, s.j_a[j], s.j_b[j]);
 }
 // The overlap graph's union-find runs over touch-graph island roots: a
 // body's overlap-graph island is that of its touch-graph root.
@@ -322,7 +342,7 @@ __device__ __forceinline__ uint32_t spec_root(const DevState& s, uint32_t acc_ro
 constexpr uint32_t kRootWake = 1u, kRootUnready = 2u, kRootAwake = 4u;
 __global__ void k_sleep_wake_roots(DevState s) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= s.n_bodies || s.counters[kCntSleeping] == 0u || !s.sl_act[b]) return;
+    if (b >= s.n_bodies || s.counters[kCntSleeping] == 0u || !(s.sl_act[b] & kActActivating)) return;
     atomicOr(&s.sl_root[spec_root(s, uf_find(s.uf_parent, b))], kRootWake);
 }
 // Wakes the sleeping bodies of marked overlap-graph islands, then adds each
@@ -333,7 +353,9 @@ __global__ void k_sleep_wake_flags(DevState s) {
     if (b >= s.n_bodies || !is_dyn(s, b)) return;
     uint32_t f = s.b_sleep[b];
     const uint32_t root = uf_find(s.uf_parent, b);
-    if ((f & kSleeping) && s.counters[kCntSleeping] != 0u && (s.sl_root[spec_root(s, root)] & kRootWake)) {
+    const uint32_t act = s.sl_act[b];
+    if (((f & kSleeping) && s.counters[kCntSleeping] != 0u && (s.sl_root[spec_root(s, root)] & kRootWake)) ||
+        ((act & kActKinWake) && (f & (kSleeping | kReady)))) {
         f = 0u;
         s.b_sleep[b] = 0u;
         s.b_wake[b] = smax(s.b_wake[b], 0.4f);
@@ -342,7 +364,8 @@ __global__ void k_sleep_wake_flags(DevState s) {
         s.b_sacc[2 * size_t(b) + 1] = z;
     }
     if (s.counters[kCntReady] == 0u) return;
-    const uint32_t bits = ((f & kReady) ? 0u : kRootUnready) | ((f & kSleeping) ? 0u : kRootAwake);
+    const uint32_t bits = ((f & kReady) && !(act & kActKinematic) ? 0u : kRootUnready) |
+                          ((f & kSleeping) ? 0u : kRootAwake);
     if (bits) atomicOr(&s.sl_root[root], bits);
 }
 __global__ void k_sleep_decide(DevState s) {
@@ -944,7 +967,7 @@ __global__ void k_prep_joints(DevState s) {
     const float m0 = da ? s.b_inv[a].w : 0.0f, m1 = db ? s.b_inv[b].w : 0.0f;
     const v3 rel = vsub(ld3(s.b_v[a]), ld3(s.b_v[b]));
     const v3 wa = ld3(s.b_w[a]), wb = ld3(s.b_w[b]);
-    const SBody A = load_sbody(s, da ? int32_t(a) : -1), B = load_sbody(s, db ? int32_t(b) : -1);
+    const SBody A = load_sbody_any(s, a, da ? int32_t(a) : -1), B = load_sbody_any(s, b, db ? int32_t(b) : -1);
     JointRow* out = s.jrow + s.j_row[j];
     uint32_t emitted = 0;
     auto emit = [&](v3 axis, v3 a0, v3 a1, v3 ja, v3 jb, float error, float response) {
@@ -1053,7 +1076,7 @@ __global__ void k_prep_contacts(DevState s) {
         const int32_t b1 = is_dyn(s, a1) ? int32_t(a1) : -1;
         // managers of sleeping islands are not solved (their history stays)
         if (is_asleep(s, uint32_t(b0 >= 0 ? b0 : b1))) continue;
-        const SBody A = load_sbody(s, b0), B = load_sbody(s, b1);
+        const SBody A = load_sbody_any(s, a0, b0), B = load_sbody_any(s, a1, b1);
         const float4 m0 = s.s_mat[sh0], m1 = s.s_mat[sh1];
         const float4 d0 = s.b_dyn1[a0], d1 = s.b_dyn1[a1];
         const float rest_d = m0.w + m1.w;
@@ -1752,6 +1775,52 @@ static void join_branches(const Branches* br, cudaStream_t st, int n) {
     }
 }
 
+// Kinematic target velocities (scene.cpp:2005-2043): the velocities that
+// carry the body's mass centre and orientation to its target in one step;
+// zero without a pending target.
+__global__ void k_kinematic_velocities(DevState s) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= s.n_bodies || !(s.b_flags[b] & kBodyKinematic)) return;
+    const float4 z = make_float4(0, 0, 0, 0);
+    if (!(s.b_sleep[b] & kKinPending)) { s.b_v[b] = z; s.b_w[b] = z; return; }
+    const float inv_dt = 1.0f / s.dt;
+    const v3 tp = ld3(s.b_ktarget[2 * size_t(b)]);
+    const qt tq = ldq(s.b_ktarget[2 * size_t(b) + 1]);
+    const v3 off = rot_sc(tq, ld3(s.b_ml_p[b]));
+    const v3 target = {tp.x + off.x, tp.y + off.y, tp.z + off.z};
+    const v3 center = mass_position(s, b);
+    const v3 v = {(target.x - center.x) * inv_dt, (target.y - center.y) * inv_dt, (target.z - center.z) * inv_dt};
+    qt rel = qmul(tq, qconj(ldq(s.b_q[b])));
+    if (rel.w < 0.0f) rel = {-rel.x, -rel.y, -rel.z, -rel.w};
+    const float len = sqrtf(rel.x * rel.x + rel.y * rel.y + rel.z * rel.z);
+    v3 w = {0, 0, 0};
+    if (len > 0.0f) {
+        const float angle = 2.0f * atan2f(len, rel.w);
+        const float scale = angle * inv_dt / len;
+        w = {rel.x * scale, rel.y * scale, rel.z * scale};
+    }
+    if (!(vfinite(v) && vfinite(w))) atomicOr(s.err, kErrNonFinite);
+    s.b_v[b] = st4(v, 0.0f);
+    s.b_w[b] = st4(w, 0.0f);
+}
+// After the solve (scene.cpp:2045-2065): a kinematic body with a pending
+// target takes it and is ready for sleep; the step after (settling), its
+// velocity is zero (scene.cpp:10992-11005).
+__global__ void k_kinematic_publish(DevState s) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= s.n_bodies || !(s.b_flags[b] & kBodyKinematic)) return;
+    uint32_t f = s.b_sleep[b];
+    if (f & kKinPending) {
+        const float4 tp = s.b_ktarget[2 * size_t(b)];
+        s.b_p[b] = make_float4(tp.x, tp.y, tp.z, s.b_p[b].w);
+        s.b_q[b] = s.b_ktarget[2 * size_t(b) + 1];
+        f = (f & ~(kKinPending | kKinNew)) | kReady | kKinSettling;
+    } else {
+        f &= ~kKinSettling;
+    }
+    s.b_sleep[b] = f & ~kKinNew;
+}
+
 // Host-buffer transfers: the 14-float body records of read_bodies packed
 // on the device (one D2H), and write_velocities' 6-float records unpacked
 // on the device (one H2D) into the velocities, waking every dynamic body.
@@ -1817,11 +1886,14 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     k_union<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     if (s.sleep) {
         const uint32_t bb = grid_for(s.n_bodies, T, 1u << 30);
+        if (s.n_kinematic && s.n_joints)
+            k_sleep_kinematic_joints<<<grid_for(s.n_joints, T, 1u << 30), T, 0, st>>>(s);
         k_sleep_spec<<<grid_for(2u * s.pair_cap, T, cap_blocks), T, 0, st>>>(s);
         k_sleep_wake_roots<<<bb, T, 0, st>>>(s);
         k_sleep_wake_flags<<<bb, T, 0, st>>>(s);
         k_sleep_decide<<<bb, T, 0, st>>>(s);
     }
+    if (s.n_kinematic) k_kinematic_velocities<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
     k_bodies_velocity<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
     k_desc_keys<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     // keys are island roots < n_bodies, or n_bodies for sleeping islands
@@ -1861,6 +1933,7 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     join_branches(br, st, 3);
     hook(kStIntegrate, st);
     k_integrate<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
+    if (s.n_kinematic) k_kinematic_publish<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
     if (s.events) enqueue_events(s, st);
     hook(kStEnd, st);
 }

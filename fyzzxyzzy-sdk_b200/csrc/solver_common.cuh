@@ -45,6 +45,19 @@ __device__ __forceinline__ SBody load_sbody(const DevState& s, int32_t b) {
     r.c0 = ld3(si[0]); r.c1 = ld3(si[1]); r.c2 = ld3(si[2]);
     return r;
 }
+// Solver-body data of any actor: a dynamic body's (index b >= 0), or for an
+// actor `a` that is not dynamic, the infinite-mass record of the world or
+// of a kinematic body moving with its target velocity (scene.cpp:6956-6973).
+__device__ __forceinline__ SBody load_sbody_any(const DevState& s, uint32_t a, int32_t b) {
+    if (b >= 0 || !(s.b_flags[a] & kBodyKinematic)) return load_sbody(s, b);
+    SBody r;
+    r.v = ld3(s.b_v[a]);
+    r.w = ld3(s.b_w[a]);
+    r.p = mass_position(s, a);
+    r.inv_mass = 0.0f;
+    r.c0 = r.c1 = r.c2 = {0, 0, 0};
+    return r;
+}
 __device__ __forceinline__ v3 xform(const SBody& d, v3 v) {
     return {d.c0.x * v.x + d.c1.x * v.y + d.c2.x * v.z,
             d.c0.y * v.x + d.c1.y * v.y + d.c2.y * v.z,

@@ -58,6 +58,8 @@ struct DevState {
     uint32_t* sl_act = nullptr;        // per step: activating this step
     uint32_t* sl_spec = nullptr;       // per step: overlap-graph union-find parent (over touch-graph roots)
     uint32_t* sl_root = nullptr;       // per step: flags of the union-find roots
+    float4* b_ktarget = nullptr;       // 2 per body: kinematic target position, orientation
+    uint32_t n_kinematic = 0;          // kinematic bodies in the world
     bool sleep = true;                 // sleeping enabled for this step
 
     // shapes

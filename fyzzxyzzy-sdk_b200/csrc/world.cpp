@@ -41,6 +41,10 @@ struct HostBody {
     std::array<float, 3> ml_p{0, 0, 0};
     std::array<float, 4> ml_q{0, 0, 0, 1};
     std::vector<uint32_t> shapes;   // attachment order
+    // kinematic: moved to its target each step, infinite mass in contacts
+    bool kinematic = false;
+    std::array<float, 3> kp{0, 0, 0};
+    std::array<float, 4> kq{0, 0, 0, 1};
     // sleep state (scene.h:1147-1153 Actor defaults)
     float wake = 0.4f;
     uint32_t sleep = 0;              // kSleeping | kReady
@@ -364,6 +368,46 @@ public:
         shapes_[shape].mat[2] = m.restitution;
         mass_dirty_ = true;
     }
+    // World::set_body_kinematic (scene.cpp:916-1003): a dynamic body becomes
+    // kinematic (at rest, asleep until it gets a target) or back (awake).
+    // The pair set changes (kinematic bodies pair with dynamic ones only), so
+    // the device state is rebuilt and the contact-manager history restarts.
+    void set_kinematic(uint32_t body, bool on) {
+        HostBody& b = require_body(body);
+        if (!b.dynamic && !b.kinematic) throw std::logic_error("Kinematic flag requires a rigid box");
+        if (b.kinematic == on) return;
+        pull_state();
+        b.kinematic = on;
+        b.dynamic = !on;
+        b.v = {0, 0, 0};
+        b.w = {0, 0, 0};
+        b.sacc = {};
+        if (on) {
+            b.sleep = kSleeping | kReady;
+        } else {
+            b.sleep = 0u;
+            b.wake = 0.4f;
+        }
+        topology_dirty_ = true;
+    }
+    // World::set_body_kinematic_target (scene.cpp:858-912): the pose the
+    // body reaches at the end of the next step; touching partners wake.
+    void set_kinematic_target(uint32_t body, const float* pose) {
+        HostBody& b = require_body(body);
+        if (!b.kinematic) throw std::logic_error("Source kinematic target requires eKINEMATIC rigid body");
+        validate_position(pose);
+        const float* q = pose + 3;
+        const float m = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+        if (!std::isfinite(q[0]) || !std::isfinite(q[1]) || !std::isfinite(q[2]) || !std::isfinite(q[3]) ||
+            !std::isfinite(m) || std::abs(m - 1.0f) >= 1.0e-2f)
+            throw std::invalid_argument("Native kinematic target is not sane");
+        pull_state();
+        b.kp = {pose[0], pose[1], pose[2]};
+        b.kq = {q[0] / m, q[1] / m, q[2] / m, q[3] / m};
+        b.sleep = kKinPending | kKinNew;
+        b.wake = 0.4f;
+        mass_dirty_ = true;
+    }
     void set_velocity(uint32_t body, const float* v, bool angular) {
         HostBody& b = require_body(body);
         if (!std::isfinite(v[0]) || !std::isfinite(v[1]) || !std::isfinite(v[2]))
@@ -451,6 +495,14 @@ public:
         }
         for (size_t i = 0; i < n; ++i) {
             auto& b = bodies_[i];
+            if (b.kinematic) {   // pose moved to its targets, velocity derived, flags
+                b.p = {p[i].x, p[i].y, p[i].z};
+                b.q = {q[i].x, q[i].y, q[i].z, q[i].w};
+                b.v = {v[i].x, v[i].y, v[i].z};
+                b.w = {w[i].x, w[i].y, w[i].z};
+                b.sleep = sl[i];
+                continue;
+            }
             if (!b.dynamic) continue;
             b.p = {p[i].x, p[i].y, p[i].z};
             b.q = {q[i].x, q[i].y, q[i].z, q[i].w};
@@ -1202,7 +1254,7 @@ private:
         o[3] = b.v[0]; o[4] = b.v[1]; o[5] = b.v[2];
         o[6] = b.q[0]; o[7] = b.q[1]; o[8] = b.q[2]; o[9] = b.q[3];
         o[10] = b.w[0]; o[11] = b.w[1]; o[12] = b.w[2];
-        o[13] = (b.dynamic && (b.sleep & kSleeping)) ? 1.0f : 0.0f;
+        o[13] = ((b.dynamic || b.kinematic) && (b.sleep & kSleeping)) ? 1.0f : 0.0f;
     }
     DevState view(int parity) const {
         DevState s = d_;
@@ -1362,13 +1414,16 @@ private:
 
     void upload_bodies() {
         const uint32_t nb = uint32_t(bodies_.size());
-        std::vector<float4> p(nb), q(nb), v(nb), w(nb), inv(nb), mlp(nb), mlq(nb), acc(2 * size_t(nb));
+        std::vector<float4> p(nb), q(nb), v(nb), w(nb), inv(nb), mlp(nb), mlq(nb), acc(2 * size_t(nb)),
+            kt(2 * size_t(nb));
         std::vector<float> wake(nb);
         std::vector<uint32_t> sl(nb);
         for (uint32_t i = 0; i < nb; ++i) {
             const HostBody& b = bodies_[i];
             wake[i] = b.wake;
-            sl[i] = b.dynamic ? b.sleep : 0u;
+            sl[i] = (b.dynamic || b.kinematic) ? b.sleep : 0u;
+            kt[2 * i] = make_float4(b.kp[0], b.kp[1], b.kp[2], 0);
+            kt[2 * i + 1] = make_float4(b.kq[0], b.kq[1], b.kq[2], b.kq[3]);
             acc[2 * i] = make_float4(b.sacc[0], b.sacc[1], b.sacc[2], 0);
             acc[2 * i + 1] = make_float4(b.sacc[3], b.sacc[4], b.sacc[5], 0);
             p[i] = make_float4(b.p[0], b.p[1], b.p[2], b.inv_mass);
@@ -1383,6 +1438,7 @@ private:
         upload(d_.b_w, w, stream_); upload(d_.b_inv, inv, stream_);
         upload(d_.b_ml_p, mlp, stream_); upload(d_.b_ml_q, mlq, stream_);
         upload(d_.b_wake, wake, stream_); upload(d_.b_sleep, sl, stream_); upload(d_.b_sacc, acc, stream_);
+        upload(d_.b_ktarget, kt, stream_);
         std::vector<float4> mat(shapes_.size());
         for (size_t i = 0; i < shapes_.size(); ++i)
             mat[i] = make_float4(shapes_[i].mat[0], shapes_[i].mat[1], shapes_[i].mat[2], shapes_[i].mat[3]);
@@ -1456,6 +1512,7 @@ private:
         dalloc(d_.b_dyn0, nb, owned_); dalloc(d_.b_dyn1, nb, owned_);
         dalloc(d_.b_flags, nb, owned_); dalloc(d_.b_scene, nb, owned_);
         dalloc(d_.b_wake, nb, owned_); dalloc(d_.b_sacc, 2 * size_t(nb), owned_); dalloc(d_.b_sleep, nb, owned_);
+        dalloc(d_.b_ktarget, 2 * size_t(nb), owned_);
         dalloc(d_.b_jcount, nb, owned_); dalloc(d_.b_counted, nb, owned_);
         dalloc(d_.sl_act, nb, owned_); dalloc(d_.sl_spec, nb, owned_); dalloc(d_.sl_root, nb, owned_);
         dalloc(bk_p_, nb, owned_); dalloc(bk_q_, nb, owned_); dalloc(bk_v_, nb, owned_); dalloc(bk_w_, nb, owned_);
@@ -1496,7 +1553,8 @@ private:
         std::vector<float4> dyn1(nb, make_float4(1.0e32f, FLT_MAX, 0.0f, 0.0f));
         std::vector<uint32_t> flags(nb), bscene(nb);
         for (uint32_t i = 0; i < nb; ++i) {
-            flags[i] = bodies_[i].dynamic ? kBodyDynamic : 0u;
+            flags[i] = (bodies_[i].dynamic ? kBodyDynamic : 0u) | (bodies_[i].kinematic ? kBodyKinematic : 0u);
+            d_.n_kinematic += bodies_[i].kinematic ? 1u : 0u;
             bscene[i] = bodies_[i].scene;
         }
         std::vector<float4> geom(ns), lp(ns), lq(ns);
@@ -1837,6 +1895,13 @@ int fyzz_b200_add_revolute_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b
 int fyzz_b200_add_prismatic_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b, const float local_a[7],
                                        const float local_b[7], uint64_t* id_out) {
     return add_joint_abi(w, fyzz::b200::kJointPrismatic, a, b, local_a, local_b, 0.0f, id_out);
+}
+int fyzz_b200_set_body_kinematic(fyzz_b200_world* w, uint32_t body, int enabled) {
+    return guarded(w, [&](auto& W) { W.set_kinematic(body, enabled != 0); });
+}
+int fyzz_b200_set_body_kinematic_target(fyzz_b200_world* w, uint32_t body, const float pose[7]) {
+    if (!pose) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) { W.set_kinematic_target(body, pose); });
 }
 int fyzz_b200_set_sleeping(fyzz_b200_world* w, int enabled) {
     return guarded(w, [&](auto& W) { W.set_sleeping(enabled != 0); });

@@ -356,3 +356,22 @@ def joint_mechanisms(n_chains: int = 24, seed: int = 0, links: int = 4, kinds=No
     spec.joint_kind = np.asarray(jk, np.uint32)
     spec.joint_local = np.asarray(jl, np.float32).reshape(-1, 14)
     return spec
+
+
+def kinematic_platform(n: int = 12, seed: int = 0) -> SceneSpec:
+    """A 3 x 0.2 x 3 m platform (body 0, to be made kinematic) at 0.6 m with
+    n random boxes (half extents U[0.1,0.2]) dropped onto it from 1-3 m."""
+    spec = random_boxes(n + 1, seed=seed, xz=0.8, y=(1.0, 3.0), half=(0.1, 0.2))
+    spec.bodies[0, 0:3] = [0, 0.6, 0]
+    spec.bodies[0, 3:7] = [0, 0, 0, 1]
+    spec.shape_geom[0, :3] = [1.5, 0.1, 1.5]
+    return spec
+
+
+def platform_target(step: int, dt: float = 1.0 / 120.0) -> np.ndarray:
+    """Target pose of the platform after `step`: drifting along x at 0.4 m/s,
+    bobbing 0.2 m in y and turning about y at 0.3 rad/s."""
+    t = (step + 1) * dt
+    ang = 0.3 * t
+    return np.array([0.4 * t, 0.6 + 0.2 * np.sin(2 * t), 0.0, 0.0, np.sin(ang / 2), 0.0, np.cos(ang / 2)],
+                    np.float32)

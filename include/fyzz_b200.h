@@ -201,6 +201,19 @@ int fyzz_b200_contact_events(fyzz_b200_world* w, const fyzz_b200_contact_event_t
                              uint64_t* n_events, const fyzz_b200_contact_event_point_t** points,
                              uint64_t* n_points);
 
+/* ---- kinematic bodies: World::set_body_kinematic / set_body_kinematic_target
+ *      (world.h:505-506; Scene::set_kinematic, set_kinematic_target,
+ *      scene.cpp:858-1003) ----
+ * A kinematic body has infinite mass in contacts and joints and pairs with
+ * dynamic bodies only.  Each step it moves to its pending target: contacts
+ * see the velocity that carries it there in one step (scene.cpp:2005-2043),
+ * and its pose becomes the target after the solve.  Switching a body in or
+ * out of kinematic mode rebuilds the device state (the contact-manager
+ * history restarts). */
+int fyzz_b200_set_body_kinematic(fyzz_b200_world* w, uint32_t body, int enabled);
+/* pose: position(3) + orientation xyzw(4), normalised once. */
+int fyzz_b200_set_body_kinematic_target(fyzz_b200_world* w, uint32_t body, const float pose[7]);
+
 /* ---- sleeping ----
  * Bodies fall asleep and wake as in the reference scene: the sleep check
  * after integration (scene.cpp:10640-10705), deactivation of touch-graph

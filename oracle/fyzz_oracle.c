@@ -39,6 +39,10 @@ typedef struct {
     v3 lin_acc, ang_acc;
     int sleeping, ready;
     uint32_t counted, joints;
+    /* kinematic body (scene.h Actor kinematic_target_*): target, a target
+     * waiting for the step, set since the last step, settling after it */
+    int kinematic, kin_pending, kin_new, kin_settling;
+    v3 kp; qt kq;
 } actor_t;
 typedef struct {
     uint32_t body, type;
@@ -575,8 +579,31 @@ int fo_scene_advance_collision(fo_scene* s) { return collide(s); }
 
 /* ------------------------- dynamics ------------------------- */
 /* scene.cpp:10383-10507 prepare_unconstrained_velocities */
+/* scene.cpp:2005-2043 calculate_kinematic_velocities */
+static void kinematic_velocities(fo_scene* s, float inv_dt) {
+    for (uint32_t i = 0; i < s->na; ++i) {
+        actor_t* a = &s->actors[i];
+        if (!a->kinematic) continue;
+        if (!a->kin_pending) { a->v = V3(0, 0, 0); a->w = V3(0, 0, 0); continue; }
+        const v3 off = rot_sc(a->kq, a->ml_p);
+        const v3 target = V3(a->kp.x + off.x, a->kp.y + off.y, a->kp.z + off.z);
+        const v3 center = mass_position(a);
+        a->v = V3((target.x - center.x) * inv_dt, (target.y - center.y) * inv_dt, (target.z - center.z) * inv_dt);
+        qt rel = qmul(a->kq, qconj(a->q));
+        if (rel.w < 0.0f) rel = Q4(-rel.x, -rel.y, -rel.z, -rel.w);
+        const float len = sqrtf(rel.x * rel.x + rel.y * rel.y + rel.z * rel.z);
+        if (len > 0.0f) {
+            const float angle = 2.0f * atan2f(len, rel.w);
+            const float scale = angle * inv_dt / len;
+            a->w = V3(rel.x * scale, rel.y * scale, rel.z * scale);
+        } else {
+            a->w = V3(0, 0, 0);
+        }
+    }
+}
 static void pre_integrate(fo_scene* s, float dt) {
     const float gravity = -9.81f;
+    kinematic_velocities(s, 1.0f / dt);
     for (uint32_t i = 0; i < s->na; ++i) {
         actor_t* a = &s->actors[i];
         if (!a->dynamic || a->sleeping) continue;
@@ -693,6 +720,39 @@ static void sleep_islands(fo_scene* s) {
             if (B->dynamic) { act[b] = 1; B->ready = 0; }
         }
     }
+    /* kinematic links (touching managers and joints): a pending target
+     * keeps the dynamic partner's island awake (scene.cpp:6430-6463); a new
+     * target wakes a sleeping or sleep-ready partner (scene.cpp:893-911) */
+    uint8_t* kin = (uint8_t*)calloc(na + 1, 1);
+    for (uint64_t i = 0; i < s->nmgr + s->nj; ++i) {
+        uint32_t a, b;
+        if (i < s->nmgr) {
+            const mgr_t* m = &s->mgr[i];
+            if (!m->touching) continue;
+            a = s->shapes[(uint32_t)(m->key >> 32)].body;
+            b = s->shapes[(uint32_t)m->key].body;
+        } else {
+            a = s->joint_a[i - s->nmgr];
+            b = s->joint_b[i - s->nmgr];
+        }
+        const actor_t* A = &s->actors[a];
+        const actor_t* B = &s->actors[b];
+        if (A->kinematic == B->kinematic) continue;
+        const actor_t* K = A->kinematic ? A : B;
+        const uint32_t d = A->kinematic ? b : a;
+        if (!s->actors[d].dynamic) continue;
+        if (K->kin_pending) kin[d] |= 1;
+        if (K->kin_new) { kin[d] |= 2; act[d] = 1; }
+    }
+    for (uint32_t i = 0; i < na; ++i) {
+        actor_t* a = &s->actors[i];
+        if (!(kin[i] & 2) || !a->dynamic || (!a->sleeping && !a->ready)) continue;
+        if (a->sleeping) any_asleep = 1;
+        a->sleeping = 0;
+        a->ready = 0;
+        a->wake = fmaxf_(a->wake, 0.4f);
+        clear_sleep_filter(a);
+    }
     uint32_t* par = (uint32_t*)malloc(4 * (na + 1));
     uint8_t* flag = (uint8_t*)calloc(na + 1, 1);
     if (any_asleep) {
@@ -740,7 +800,7 @@ static void sleep_islands(fo_scene* s) {
         const actor_t* a = &s->actors[i];
         if (!a->dynamic) continue;
         const uint32_t r = uf_root(par, i);
-        if (!a->ready) flag[r] |= 1;
+        if (!a->ready || (kin[i] & 1)) flag[r] |= 1;
         if (!a->sleeping) flag[r] |= 2;
     }
     for (uint32_t i = 0; i < na; ++i) {
@@ -752,7 +812,7 @@ static void sleep_islands(fo_scene* s) {
         a->w = V3(0, 0, 0);
         clear_sleep_filter(a);
     }
-    free(act); free(par); free(flag);
+    free(act); free(par); free(flag); free(kin);
 }
 /* Dy sleepCheck without stabilization (scene.cpp:10640-10705). */
 static void sleep_check(actor_t* a, qt q, v3 ml, v3 mw, float dt) {
@@ -847,7 +907,19 @@ int fo_scene_step(fo_scene* s, float dt, const uint64_t* manager_order, uint64_t
         r->inv_mass = a->inv_mass;
         sqrt_inertia(a, r);
     }
-#define ROW(b) (s->actors[b].dynamic ? &rows[b] : &world)
+    /* a kinematic body's solver record: its target velocity, no inverse
+     * mass or inertia (scene.cpp:6956-6973) */
+    for (uint32_t i = 0; i < s->na; ++i) {
+        const actor_t* a = &s->actors[i];
+        if (!a->kinematic) continue;
+        srow_t* r = &rows[i];
+        r->p = mass_position(a);
+        r->q = mass_orientation(a);
+        r->v = a->v;
+        r->w = a->w;
+        r->inv_mass = 0.0f;
+    }
+#define ROW(b) ((s->actors[b].dynamic || s->actors[b].kinematic) ? &rows[b] : &world)
     /* ---- partition (scene.cpp:7113-7488, one task) ---- */
     const uint64_t nd = njo + nmo;
     uint32_t jrow_n = 0;
@@ -1401,6 +1473,22 @@ int fo_scene_step(fo_scene* s, float dt, const uint64_t* manager_order, uint64_t
         a->q = q;
         if (s->sleep) sleep_check(a, q, ml, mw, dt);
     }
+    /* kinematic bodies take their targets after the solve and settle for
+     * one step (scene.cpp:2045-2065, 10992-11005) */
+    for (uint32_t i = 0; i < s->na; ++i) {
+        actor_t* a = &s->actors[i];
+        if (!a->kinematic) continue;
+        if (a->kin_pending) {
+            a->p = a->kp;
+            a->q = a->kq;
+            a->kin_pending = 0;
+            a->ready = 1;
+            a->kin_settling = 1;
+        } else {
+            a->kin_settling = 0;
+        }
+        a->kin_new = 0;
+    }
 #undef ROW
     free(mo); free(jo); free(rows); free(d); free(part); free(pending); free(ordered);
     free(jr); free(cr); free(fr); free(mp);
@@ -1423,8 +1511,38 @@ void fo_scene_body_states(const fo_scene* s, float* out) {
         o[3] = a->v.x; o[4] = a->v.y; o[5] = a->v.z;
         o[6] = a->q.x; o[7] = a->q.y; o[8] = a->q.z; o[9] = a->q.w;
         o[10] = a->w.x; o[11] = a->w.y; o[12] = a->w.z;
-        o[13] = a->dynamic && a->sleeping ? 1.0f : 0.0f;
+        o[13] = (a->dynamic || a->kinematic) && a->sleeping ? 1.0f : 0.0f;
     }
+}
+/* Scene::set_kinematic (scene.cpp:916-1003) before the first step. */
+int fo_scene_set_kinematic(fo_scene* s, uint32_t actor, int on) {
+    if (actor >= s->na) FAIL(FO_INVALID, "actor out of range");
+    actor_t* a = &s->actors[actor];
+    if (!a->dynamic && !a->kinematic) FAIL(FO_LOGIC, "Kinematic flag requires a rigid box");
+    if (a->kinematic == (on != 0)) return 0;
+    a->kinematic = on != 0;
+    a->dynamic = on == 0;
+    a->v = V3(0, 0, 0);
+    a->w = V3(0, 0, 0);
+    clear_sleep_filter(a);
+    a->kin_pending = a->kin_new = a->kin_settling = 0;
+    if (on) { a->sleeping = 1; a->ready = 1; }
+    else { a->sleeping = 0; a->ready = 0; a->wake = 0.4f; }
+    return 0;
+}
+/* Scene::set_kinematic_target (scene.cpp:858-912): normalised once. */
+int fo_scene_set_kinematic_target(fo_scene* s, uint32_t actor, const float* pose) {
+    if (actor >= s->na || !s->actors[actor].kinematic) FAIL(FO_LOGIC, "target requires a kinematic body");
+    actor_t* a = &s->actors[actor];
+    const float m = sqrtf(pose[3] * pose[3] + pose[4] * pose[4] + pose[5] * pose[5] + pose[6] * pose[6]);
+    if (!isfinite(m) || fabsf(m - 1.0f) >= 1.0e-2f) FAIL(FO_INVALID, "Native kinematic target is not sane");
+    a->kp = V3(pose[0], pose[1], pose[2]);
+    a->kq = Q4(pose[3] / m, pose[4] / m, pose[5] / m, pose[6] / m);
+    a->kin_pending = a->kin_new = 1;
+    a->sleeping = 0;
+    a->ready = 0;
+    a->wake = 0.4f;
+    return 0;
 }
 void fo_scene_set_sleeping(fo_scene* s, int on) {
     if (!on)

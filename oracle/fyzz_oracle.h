@@ -84,6 +84,10 @@ uint64_t fo_scene_sorted_min_x(const fo_scene* s, uint32_t* values, uint32_t* id
  * each; orientations are validated and normalised as World and Scene do;
  * the distance kinds use the positions only).  Call before stepping. */
 int fo_scene_set_joint(fo_scene* s, uint32_t j, uint32_t kind, const float* local_a7, const float* local_b7);
+/* Kinematic mode of an actor (before stepping) and its target pose
+ * (position 3 + quaternion xyzw 4). */
+int fo_scene_set_kinematic(fo_scene* s, uint32_t actor, int on);
+int fo_scene_set_kinematic_target(fo_scene* s, uint32_t actor, const float* pose7);
 /* Sleeping on (default) or off (wakes every body). */
 void fo_scene_set_sleeping(fo_scene* s, int on);
 /* Per actor: wake counter, sleeping, ready, counted interactions, linear

@@ -45,6 +45,8 @@ def lib():
         L.fo_scene_normal_impulses.argtypes = [vp, vp]
         L.fo_scene_set_sleeping.argtypes = [vp, i32]
         L.fo_scene_set_joint.argtypes = [vp, u32, u32, vp, vp]
+        L.fo_scene_set_kinematic.argtypes = [vp, u32, i32]
+        L.fo_scene_set_kinematic_target.argtypes = [vp, u32, vp]
         L.fo_scene_sleep_state.argtypes = [vp, vp]
         L.fo_scene_sorted_min_x.restype = u64
         L.fo_scene_sorted_min_x.argtypes = [vp, vp, vp]
@@ -123,6 +125,17 @@ class OracleScene:
         out = np.zeros((self.counts()["actors"], 14), np.float32)
         lib().fo_scene_body_states(self.h, _p(out))
         return out
+
+    def _actor(self, body: int) -> int:
+        return body + (0 if self.spec.floor is None else 1)
+
+    def set_kinematic(self, body: int, on: bool = True):
+        """Kinematic mode of dynamic body `body` (0-based index in the spec)."""
+        self._check(lib().fo_scene_set_kinematic(self.h, self._actor(body), 1 if on else 0))
+
+    def set_kinematic_target(self, body: int, pose):
+        p = np.ascontiguousarray(pose, np.float32).reshape(7)
+        self._check(lib().fo_scene_set_kinematic_target(self.h, self._actor(body), _p(p)))
 
     def set_sleeping(self, on: bool):
         lib().fo_scene_set_sleeping(self.h, 1 if on else 0)

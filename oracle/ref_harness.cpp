@@ -202,6 +202,24 @@ int fz_ref_add_joint(void* p, int kind, uint32_t a, uint32_t b, const float* la,
     });
 }
 
+// Scene::set_kinematic / set_kinematic_target (scene.cpp:858-1003) for the
+// 0-based dynamic body index i; the target is validated as World does
+// (src/world.cpp:361-366) and normalised once by the scene.
+int fz_ref_set_kinematic(void* p, uint32_t i, int on) {
+    auto* h = static_cast<Handle*>(p);
+    return guarded([&] { h->scene->set_kinematic(h->bodies.at(i), on != 0); });
+}
+int fz_ref_set_kinematic_target(void* p, uint32_t i, const float* pose) {
+    auto* h = static_cast<Handle*>(p);
+    return guarded([&] {
+        const float m = std::sqrt(pose[3]*pose[3] + pose[4]*pose[4] + pose[5]*pose[5] + pose[6]*pose[6]);
+        if (!std::isfinite(m) || std::abs(m - 1.0f) >= 1.0e-2f)
+            throw std::invalid_argument("Rigid pose orientation is not sane");
+        h->scene->set_kinematic_target(h->bodies.at(i), {pose[0], pose[1], pose[2]},
+                                       {pose[3], pose[4], pose[5], pose[6]});
+    });
+}
+
 int fz_ref_step(void* p, float dt, int steps) {
     auto* h = static_cast<Handle*>(p);
     return guarded([&] {

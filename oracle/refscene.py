@@ -39,6 +39,8 @@ def lib():
         L.fz_ref_mass_props.argtypes = [vp, vp]
         L.fz_ref_sleep_state.argtypes = [vp, vp]
         L.fz_ref_add_joint.argtypes = [vp, i32, u32, u32, vp, vp, f32]
+        L.fz_ref_set_kinematic.argtypes = [vp, u32, i32]
+        L.fz_ref_set_kinematic_target.argtypes = [vp, u32, vp]
         L.fz_ref_encoded_bounds.argtypes = [vp, vp]
         for name in ("fz_ref_endpoints",):
             getattr(L, name).restype = u64
@@ -129,6 +131,14 @@ class RefScene:
         out = np.zeros((n, 14), np.float32)
         lib().fz_ref_body_states(self.h, _p(out))
         return out
+
+    def set_kinematic(self, body: int, on: bool = True):
+        """Kinematic mode of dynamic body `body` (0-based index in the spec)."""
+        self._check(lib().fz_ref_set_kinematic(self.h, body, 1 if on else 0))
+
+    def set_kinematic_target(self, body: int, pose):
+        p = np.ascontiguousarray(pose, np.float32).reshape(7)
+        self._check(lib().fz_ref_set_kinematic_target(self.h, body, _p(p)))
 
     def sleep_state(self) -> dict:
         """Per actor: wake counter, sleeping, ready, counted interactions and
