@@ -7,12 +7,15 @@ record layout is the one both C ABIs consume:
 * ``bodies``   (nb, 14) float32: position(3) orientation xyzw(4) linear
   velocity(3) angular velocity(3) density(1)
 * ``shape_body`` (ns,) uint32: owning dynamic-body index (grouped, ascending)
-* ``shape_type`` (ns,) uint32: 0 = box, 1 = sphere
-* ``shape_geom`` (ns, 4) float32: half extents (box) or radius (sphere)
+* ``shape_type`` (ns,) uint32: 0 = box, 1 = sphere, 3 = cooked convex hull
+* ``shape_geom`` (ns, 4) float32: half extents (box), radius (sphere) or the
+  index into ``convex_meshes`` (hull)
 * ``shape_local`` (ns, 7) float32: shape pose in the body frame
 * ``shape_mat``  (ns, 3) float32: static friction, dynamic friction, restitution
 * ``joints`` (nj, 2) uint32 and ``joint_dist`` (nj,) float32: centre-anchored
   distance constraints (``World::add_center_distance_constraint``)
+* ``convex_meshes``: list of (vertices (nv, 3) float32, outward triangles
+  (nt, 3) uint32) for ``cook_convex_mesh`` / ``World::attach_convex_shape``
 * ``floor``: static floor height or ``None``.  When present the floor is the
   first actor (BodyId 0, ShapeId 0), so dynamic body ``i`` is BodyId ``i+1``;
   ``floor_mat`` is its (static friction, dynamic friction, restitution).
@@ -27,7 +30,7 @@ from __future__ import annotations
 from dataclasses import dataclass, field
 import numpy as np
 
-BOX, SPHERE = 0, 1
+BOX, SPHERE, CONVEX = 0, 1, 3
 # Joint kinds: World::add_center_distance_constraint, add_anchored_distance_
 # constraint, add_fixed / spherical / revolute / prismatic_constraint.
 JOINT_CENTER, JOINT_ANCHORED, JOINT_FIXED, JOINT_SPHERICAL, JOINT_REVOLUTE, JOINT_PRISMATIC = range(6)
@@ -51,6 +54,7 @@ class SceneSpec:
     joint_local: np.ndarray | None = None
     floor: float | None = 0.0
     floor_mat: tuple = (0.5, 0.5, 0.0)
+    convex_meshes: list = field(default_factory=list)
 
     @property
     def n_bodies(self) -> int:
@@ -80,6 +84,19 @@ class SceneSpec:
         """True when some joint is not a plain center distance joint."""
         return bool(self.joints.shape[0]) and (bool(np.any(self.joint_kinds() != JOINT_CENTER)) or
                                                bool(np.any(self.joints == FLOOR_BODY)))
+
+    def mesh_arrays(self):
+        """Meshes concatenated for the C ABIs: (vertex counts, vertices,
+        triangle counts, triangles), indices local to each mesh."""
+        nv = np.asarray([m[0].shape[0] for m in self.convex_meshes], np.uint32)
+        nt = np.asarray([m[1].shape[0] for m in self.convex_meshes], np.uint32)
+        v = np.ascontiguousarray(np.concatenate([np.asarray(m[0], np.float32).reshape(-1, 3)
+                                                 for m in self.convex_meshes]) if self.convex_meshes
+                                 else np.zeros((0, 3), np.float32))
+        t = np.ascontiguousarray(np.concatenate([np.asarray(m[1], np.uint32).reshape(-1, 3)
+                                                 for m in self.convex_meshes]) if self.convex_meshes
+                                 else np.zeros((0, 3), np.uint32))
+        return nv, v, nt, t
 
     def validate(self) -> "SceneSpec":
         assert self.bodies.dtype == np.float32 and self.bodies.shape[1] == 14
@@ -375,3 +392,110 @@ def platform_target(step: int, dt: float = 1.0 / 120.0) -> np.ndarray:
     ang = 0.3 * t
     return np.array([0.4 * t, 0.6 + 0.2 * np.sin(2 * t), 0.0, 0.0, np.sin(ang / 2), 0.0, np.cos(ang / 2)],
                     np.float32)
+
+
+# ---------------- cooked convex hulls ----------------
+def _outward(verts: np.ndarray, tris: np.ndarray) -> np.ndarray:
+    """Winds every triangle of a convex surface outward (about the vertex
+    mean, which lies inside)."""
+    c = verts.mean(0)
+    t = np.asarray(tris, np.int64).copy()
+    a, b, d = verts[t[:, 0]], verts[t[:, 1]], verts[t[:, 2]]
+    flip = np.einsum("ij,ij->i", np.cross(b - a, d - a), a - c) < 0
+    t[flip, 1], t[flip, 2] = t[flip, 2].copy(), t[flip, 1].copy()
+    return t.astype(np.uint32)
+
+
+def hull_prism(sides: int, radius: float, half_height: float, taper: float = 1.0, phase: float = 0.0):
+    """An n-sided prism (taper 1) or frustum along y: two n-gon caps, each
+    a triangle fan that cooks to one planar face, and quad sides."""
+    ang = phase + 2 * np.pi * np.arange(sides) / sides
+    bot = np.stack([radius * np.cos(ang), np.full(sides, -half_height), radius * np.sin(ang)], 1)
+    top = np.stack([taper * radius * np.cos(ang), np.full(sides, half_height), taper * radius * np.sin(ang)], 1)
+    v = np.concatenate([bot, top]).astype(np.float32)
+    tris = [(0, i, i + 1) for i in range(1, sides - 1)]
+    tris += [(sides, sides + i, sides + i + 1) for i in range(1, sides - 1)]
+    for i in range(sides):
+        j = (i + 1) % sides
+        tris += [(i, j, sides + j), (i, sides + j, sides + i)]
+    return v, _outward(v.astype(np.float64), np.asarray(tris))
+
+
+def hull_bipyramid(sides: int, radius: float, half_height: float):
+    """Two n-gon pyramids joined at their base (apexes on +-y)."""
+    ang = 2 * np.pi * np.arange(sides) / sides
+    ring = np.stack([radius * np.cos(ang), np.zeros(sides), radius * np.sin(ang)], 1)
+    v = np.concatenate([ring, [[0, half_height, 0], [0, -half_height, 0]]]).astype(np.float32)
+    tris = []
+    for i in range(sides):
+        j = (i + 1) % sides
+        tris += [(i, j, sides), (i, j, sides + 1)]
+    return v, _outward(v.astype(np.float64), np.asarray(tris))
+
+
+def hull_box(h):
+    """A box as a cooked hull: 8 vertices, 12 triangles, 6 quad faces."""
+    v = np.array([[sx * h[0], sy * h[1], sz * h[2]] for sx in (-1, 1) for sy in (-1, 1) for sz in (-1, 1)],
+                 np.float32)
+    quads = [(0, 1, 3, 2), (4, 5, 7, 6), (0, 1, 5, 4), (2, 3, 7, 6), (0, 2, 6, 4), (1, 3, 7, 5)]
+    tris = [t for a, b, c, d in quads for t in ((a, b, c), (a, c, d))]
+    return v, _outward(v.astype(np.float64), np.asarray(tris))
+
+
+def hull_random(rng: np.random.Generator, n_points: int, radii=(0.2, 0.2, 0.2)):
+    """The convex hull of n points on an ellipsoid with the given radii
+    (scipy's Quickhull; only hull vertices are kept)."""
+    from scipy.spatial import ConvexHull
+    p = rng.normal(size=(n_points, 3))
+    p /= np.linalg.norm(p, axis=1, keepdims=True)
+    p *= np.asarray(radii)
+    h = ConvexHull(p)
+    keep = np.asarray(h.vertices)
+    remap = np.full(n_points, -1, np.int64)
+    remap[keep] = np.arange(keep.size)
+    v = p[keep].astype(np.float32)
+    return v, _outward(v.astype(np.float64), remap[h.simplices])
+
+
+def convex_pile(n: int = 48, seed: int = 0, xz: float = 2.0, y=(0.5, 4.0), frac_other: float = 0.25,
+                size=(0.12, 0.3), density: float = 1000.0, friction: float = 0.5, offset_frac: float = 0.2,
+                n_meshes: int = 6) -> SceneSpec:
+    """Cooked hulls dropped onto the floor: a few shared meshes (prisms,
+    frustums, bipyramids, a box-shaped hull and random ellipsoid hulls),
+    some attached with an off-centre local pose, mixed with frac_other boxes
+    and spheres."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    meshes = []
+    for m in range(n_meshes):
+        r = float(rng.uniform(*size))
+        kind = m % 5
+        if kind == 0:
+            meshes.append(hull_prism(int(rng.integers(5, 9)), r, 0.6 * r))
+        elif kind == 1:
+            meshes.append(hull_prism(int(rng.integers(4, 7)), r, 0.7 * r, taper=0.55))
+        elif kind == 2:
+            meshes.append(hull_bipyramid(int(rng.integers(4, 7)), r, 0.9 * r))
+        elif kind == 3:
+            meshes.append(hull_box(rng.uniform(0.6, 1.0, 3) * r))
+        else:
+            meshes.append(hull_random(rng, int(rng.integers(12, 40)), rng.uniform(0.6, 1.0, 3) * r))
+    pos = np.stack([rng.uniform(-xz, xz, n), rng.uniform(y[0], y[1], n), rng.uniform(-xz, xz, n)], 1)
+    quat = random_quaternions(rng, n)
+    z = np.zeros((n, 3), np.float32)
+    mats = np.tile(np.array([friction, friction, 0.0], np.float32), (n, 1))
+    shapes = []
+    for i in range(n):
+        u = rng.uniform()
+        if u < frac_other / 2:
+            shapes.append([_box(rng.uniform(*size, 3))])
+        elif u < frac_other:
+            shapes.append([_sphere(float(rng.uniform(*size)))])
+        else:
+            local = IDENTITY.copy()
+            if rng.uniform() < offset_frac:
+                local[:3] = rng.uniform(-0.05, 0.05, 3)
+                local[3:] = random_quaternions(rng, 1)[0]
+            shapes.append([(CONVEX, np.array([float(rng.integers(0, n_meshes)), 0, 0, 0], np.float32), local)])
+    spec = _assemble(pos.astype(np.float32), quat, z, z, density, shapes, mats)
+    spec.convex_meshes = meshes
+    return spec

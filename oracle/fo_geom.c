@@ -5,6 +5,7 @@
 #include "fyzz_oracle.h"
 #include "fo_math.h"
 #include <string.h>
+#include <stdlib.h>
 
 /* ---------------- bounds (scene.cpp:26-35, 1233-1316) ---------------- */
 static uint32_t encode_float(float v) {
@@ -337,19 +338,43 @@ int fo_pcm_batch_selection(const fo_candidate* c, int n, float tol, uint8_t sel[
     return 0;
 }
 
-/* ---------------- GJK / EPA (GuPCMGjkEpa.cpp:44-570, box path) ------------- */
+/* ---------------- GJK / EPA (GuPCMGjkEpa.cpp:44-570) ----------------------
+ * One pair of finite shapes in B's frame: boxes (extents), sphere point
+ * cores (radius > 0; the radius is applied after the search) and cooked
+ * hulls (extreme-vertex supports, scale-relative facet admission). */
 typedef struct { v3 a, b, q; uint32_t ai, bi; } sup_t;
-typedef struct { v3 ha, hb, a_in_b; qt rel; } bpair_t;
+typedef struct {
+    v3 ha, hb, a_in_b; qt rel;
+    const float* va; uint32_t nva;
+    const float* vb; uint32_t nvb;
+    float ra, rb;
+} bpair_t;
+static int bp_hull(const bpair_t* p) { return p->nva > 0 || p->nvb > 0; }
 static v3 box_vertex(v3 e, v3 d, uint32_t* idx) {
     const int x = d.x > 0.f, y = d.y > 0.f, z = d.z > 0.f;
     *idx = (x ? 1u : 0u) | (y ? 2u : 0u) | (z ? 4u : 0u);
     return V3(x ? e.x : -e.x, y ? e.y : -e.y, z ? e.z : -e.z);
 }
+/* GuPCMGjkEpa.cpp:53-75 BoxPair::vertex: a point core is its centre; a hull
+ * returns its first vertex of largest projection. */
+static v3 shape_vertex(v3 e, v3 d, const float* hull, uint32_t n, float radius, uint32_t* idx) {
+    *idx = 0;
+    if (radius > 0.f) return V3(0, 0, 0);
+    if (n) {
+        float best = vdot(V3(hull[0], hull[1], hull[2]), d);
+        for (uint32_t i = 1; i < n; ++i) {
+            const float pr = vdot(V3(hull[3 * i], hull[3 * i + 1], hull[3 * i + 2]), d);
+            if (pr > best) { best = pr; *idx = i; }
+        }
+        return V3(hull[3 * *idx], hull[3 * *idx + 1], hull[3 * *idx + 2]);
+    }
+    return box_vertex(e, d, idx);
+}
 static sup_t bp_support(const bpair_t* p, v3 dir) {
     sup_t s;
     const v3 da = rotinv_gu(p->rel, dir);
-    const v3 pa = box_vertex(p->ha, da, &s.ai);
-    s.b = box_vertex(p->hb, vneg(dir), &s.bi);
+    const v3 pa = shape_vertex(p->ha, da, p->va, p->nva, p->ra, &s.ai);
+    s.b = shape_vertex(p->hb, vneg(dir), p->vb, p->nvb, p->rb, &s.bi);
     s.a = vadd(p->a_in_b, rot_gu(p->rel, pa));
     s.q = vsub(s.a, s.b);
     return s;
@@ -444,14 +469,16 @@ static int contact_from_gjk(const bpair_t* p, const closest_t* n, fo_candidate* 
     return 1;
 }
 typedef struct { int i, j, k; v3 normal; float distance; int valid, in_heap; } facet_t;
-static facet_t make_facet(const sup_t* vtx, int i, int j, int k) {
+static facet_t make_facet(const bpair_t* p, const sup_t* vtx, int i, int j, int k) {
     facet_t f;
     memset(&f, 0, sizeof f);
     const v3 a = vtx[i].q, b = vtx[j].q, c = vtx[k].q;
     const v3 e0 = vsub(b, a), e1 = vsub(c, a);
     v3 n = vcross(e0, e1);
     const float norm2 = vlen2(n);
-    if (!(norm2 > FLT_EPSILON)) return f;
+    float min_area = FLT_EPSILON;
+    if (bp_hull(p)) min_area *= vlen2(e0) * vlen2(e1);   /* GuPCMGjkEpa.cpp:210-213 */
+    if (!(norm2 > min_area)) return f;
     n = vmul(n, 1.0f / sqrtf(norm2));
     f.i = i; f.j = j; f.k = k; f.normal = n; f.distance = vdot(n, a);
     f.valid = 1; f.in_heap = 1;
@@ -477,7 +504,7 @@ static int init_epa(const bpair_t* p, sup_t* vtx, int* count, facet_t* facets, i
         vtx[(*count)++] = bp_support(p, perp);
     }
     if (*count == 3) {
-        const facet_t f0 = make_facet(vtx, 0, 1, 2), f1 = make_facet(vtx, 1, 0, 2);
+        const facet_t f0 = make_facet(p, vtx, 0, 1, 2), f1 = make_facet(p, vtx, 1, 0, 2);
         if (!f0.valid || !f1.valid) return 0;
         facets[(*fc)++] = f0;
         facets[(*fc)++] = f1;
@@ -490,7 +517,7 @@ static int init_epa(const bpair_t* p, sup_t* vtx, int* count, facet_t* facets, i
     }
     static const int faces[4][3] = {{0, 1, 2}, {0, 3, 1}, {0, 2, 3}, {1, 3, 2}};
     for (int i = 0; i < 4; ++i) {
-        const facet_t f = make_facet(vtx, faces[i][0], faces[i][1], faces[i][2]);
+        const facet_t f = make_facet(p, vtx, faces[i][0], faces[i][1], faces[i][2]);
         if (!f.valid) return 0;
         facets[(*fc)++] = f;
     }
@@ -520,7 +547,9 @@ static int contact_from_facet(const bpair_t* p, const sup_t* vtx, const facet_t*
     out->nb[0] = normal.x; out->nb[1] = normal.y; out->nb[2] = normal.z;
     out->sep = -depth;
     const v3 diff = vsub(pa, pb);
-    return sqrtf(vlen2(diff)) <= depth + 1.0e-3f;
+    const float scale = fmaxf_(fmaxf_(fmaxf_(p->ha.x, p->ha.y), fmaxf_(p->ha.z, p->hb.x)), fmaxf_(p->hb.y, p->hb.z));
+    const float tol = bp_hull(p) ? 1.0e-3f * scale : 1.0e-3f;     /* GuPCMGjkEpa.cpp:297-301 */
+    return sqrtf(vlen2(diff)) <= depth + tol;
 }
 static int run_epa(const bpair_t* p, const sup_t* simplex, int sc, fo_candidate* out) {
     sup_t vtx[64];
@@ -579,7 +608,7 @@ static int run_epa(const bpair_t* p, const sup_t* simplex, int sc, fo_candidate*
         for (int i = 0; i < fc; ++i) avail += !facets[i].valid;
         if (bc > avail) return 0;
         for (int i = 0; i < bc; ++i) {
-            facet_t f = make_facet(vtx, bfrom[i], bto[i], ni);
+            facet_t f = make_facet(p, vtx, bfrom[i], bto[i], ni);
             if (!f.valid) return 0;
             f.in_heap = f.distance <= upper;
             int slot = -1;
@@ -591,17 +620,23 @@ static int run_epa(const bpair_t* p, const sup_t* simplex, int sc, fo_candidate*
     }
     return 0;
 }
+/* GuPCMGjkEpa.cpp:411-516 gjk_epa.  A sphere point core converges its
+ * separated distance before EPA is admitted. */
 static int gjk_epa(const bpair_t* p, float cd, fo_candidate* out) {
     const float eps = 0.1f * fminf_(box_min_margin(p->ha), box_min_margin(p->hb));
     const float progress = 1.0f - 0.000225f;
+    const int point_core = p->ra > 0.f || p->rb > 0.f;
     sup_t simplex[4];
     int count = 0;
     v3 closest = vlen2(p->a_in_b) > 0.0f ? p->a_in_b : V3(1, 0, 0);
     float previous = FLT_MAX;
     for (int it = 0; it < 32; ++it) {
         const float dist = sqrtf(vlen2(closest));
-        if (count > 0 && dist <= eps) return run_epa(p, simplex, count, out);
-        if (dist <= 0.0f) return 0;
+        if (count > 0 && dist <= eps && !point_core) return run_epa(p, simplex, count, out);
+        if (dist <= 0.0f) {
+            if (!point_core || count == 0) return 0;
+            return run_epa(p, simplex, count, out);
+        }
         const v3 normal = vmul(closest, 1.0f / dist);
         const sup_t s = bp_support(p, vneg(closest));
         const float proj = vdot(normal, s.q);
@@ -616,7 +651,7 @@ static int gjk_epa(const bpair_t* p, float cd, fo_candidate* out) {
                     const closest_t cur = closest_simplex(simplex, count);
                     return cur.mask && contact_from_gjk(p, &cur, out) && out->sep <= cd;
                 }
-                return 0;
+                return point_core && run_epa(p, simplex, count, out);
             }
         if (count == 4) return run_epa(p, simplex, count, out);
         simplex[count++] = s;
@@ -625,9 +660,16 @@ static int gjk_epa(const bpair_t* p, float cd, fo_candidate* out) {
         closest = nx.point;
         const float nd = sqrtf(nx.dist2);
         compact_simplex(simplex, &count, &nx);
-        if (nd >= previous) return 0;
+        if (nd >= previous) {
+            if (point_core) {
+                if (proj > 0.f) return contact_from_gjk(p, &nx, out);
+                return run_epa(p, simplex, count, out);
+            }
+            return 0;
+        }
         previous = nd;
     }
+    if (point_core && count > 0) return run_epa(p, simplex, count, out);
     return 0;
 }
 /* GuPCMGjkEpa.cpp:517-568 source_pcm_box_box_gjk_epa (box/box, no radii). */
@@ -635,6 +677,7 @@ int fo_pcm_box_box_gjk_epa(const float* ra, const float* rb, float cd, fo_candid
     const qt q0 = Q4(ra[6], ra[7], ra[8], ra[9]);
     const qt q1 = Q4(rb[6], rb[7], rb[8], rb[9]);
     bpair_t p;
+    memset(&p, 0, sizeof p);
     p.ha = V3(ra[0], ra[1], ra[2]);
     p.hb = V3(rb[0], rb[1], rb[2]);
     p.a_in_b = rotinv_gu(q1, vsub(V3(ra[3], ra[4], ra[5]), V3(rb[3], rb[4], rb[5])));
@@ -936,10 +979,10 @@ int fo_generate_pcm_box_box(const float* first, const float* second, float cd,
 /* scene.cpp:3774-3955 generate_pcm_plane_box.  plane: position(3);
  * box: half(3) position(3) orientation(4).  Emits the raw plane-first
  * normal (0,-1,0); the scene flips plane manifolds afterwards. */
-int fo_generate_pcm_plane_box(const float* plane_p, const float* box, float cd,
-                              fo_pcm_cache* cache, fo_point out[4]) {
-    const v3 h = ptv(box), bp = ptv(box + 3);
-    const qt q = Q4(box[6], box[7], box[8], box[9]);
+/* Candidates are the box corners, or a cooked hull's vertices in vertex
+ * order (scene.cpp:3826-3846). */
+static int plane_generate(const float* plane_p, v3 h, v3 bp, qt q, const fo_mesh* hull, float cd,
+                          fo_pcm_cache* cache, fo_point out[4]) {
     const v3 rel = V3(bp.x - plane_p[0], bp.y - plane_p[1], bp.z - plane_p[2]);
     const float margin = pcm_box_margin(h);
     const float brk = margin * 0.2f;
@@ -957,11 +1000,14 @@ int fo_generate_pcm_plane_box(const float* plane_p, const float* box, float cd,
         cache->rel_q[0] = q.x; cache->rel_q[1] = q.y; cache->rel_q[2] = q.z; cache->rel_q[3] = q.w;
         cache->initialized = 1;
         cache->count = 0;
-        fo_candidate cands[8];
+        const unsigned nc = hull ? hull->nv : 8u;
+        fo_candidate* cands = (fo_candidate*)malloc(sizeof(fo_candidate) * nc);
+        int* chosen = (int*)calloc(nc, sizeof(int));
         int n = 0;
-        for (unsigned corner = 0; corner < 8u; ++corner) {
-            const v3 local = V3((corner & 4u) ? -h.x : h.x, (corner & 2u) ? -h.y : h.y,
-                                (corner & 1u) ? -h.z : h.z);
+        for (unsigned corner = 0; corner < nc; ++corner) {
+            const v3 local = hull ? V3(hull->verts[3 * corner], hull->verts[3 * corner + 1], hull->verts[3 * corner + 2])
+                                  : V3((corner & 4u) ? -h.x : h.x, (corner & 2u) ? -h.y : h.y,
+                                       (corner & 1u) ? -h.z : h.z);
             const v3 r = rot_sc(q, local);
             const v3 ip = V3(rel.x + r.x, rel.y + r.y, rel.z + r.z);
             if (ip.y >= cd) continue;
@@ -975,7 +1021,6 @@ int fo_generate_pcm_plane_box(const float* plane_p, const float* box, float cd,
             for (int i = 0; i < n; ++i) cache->pts[i] = cands[i];
             cache->count = (uint8_t)n;
         } else {
-            int chosen[8] = {0};
             int idx[4];
             int first = 0;
             for (int i = 1; i < n; ++i)
@@ -1034,6 +1079,8 @@ int fo_generate_pcm_plane_box(const float* plane_p, const float* box, float cd,
             for (int k = 0; k < 4; ++k) cache->pts[k] = cands[idx[k]];
             cache->count = 4;
         }
+        free(cands);
+        free(chosen);
     }
     int emitted = 0;
     for (int k = 0; k < cache->count; ++k) {
@@ -1043,6 +1090,318 @@ int fo_generate_pcm_plane_box(const float* plane_p, const float* box, float cd,
         o->p[0] = plane_p[0] + pt->lb[0]; o->p[1] = plane_p[1]; o->p[2] = plane_p[2] + pt->lb[2];
         o->n[0] = 0.0f; o->n[1] = -1.0f; o->n[2] = 0.0f;
         o->sep = pt->sep;
+    }
+    return emitted;
+}
+
+int fo_generate_pcm_plane_box(const float* plane_p, const float* box, float cd,
+                              fo_pcm_cache* cache, fo_point out[4]) {
+    return plane_generate(plane_p, ptv(box), ptv(box + 3), Q4(box[6], box[7], box[8], box[9]), NULL, cd, cache, out);
+}
+int fo_generate_pcm_plane_convex(const float* plane_p, const float* shape_half, const float* pose7,
+                                 const fo_mesh* hull, float cd, fo_pcm_cache* cache, fo_point out[4]) {
+    return plane_generate(plane_p, ptv(shape_half), ptv(pose7), Q4(pose7[3], pose7[4], pose7[5], pose7[6]), hull, cd,
+                          cache, out);
+}
+
+/* ---------------- cooked convex hulls ---------------- */
+/* scene.cpp:1258-1298: the world AABB of the rotated hull vertices, centred
+ * where the hull is, plus the contact offset. */
+int fo_convex_bounds(const float* pose7, const fo_mesh* hull, float contact_offset, uint32_t* out6) {
+    const v3 p = V3(pose7[0], pose7[1], pose7[2]);
+    const qt q = Q4(pose7[3], pose7[4], pose7[5], pose7[6]);
+    v3 lo = V3(INFINITY, INFINITY, INFINITY), hi = V3(-INFINITY, -INFINITY, -INFINITY);
+    for (uint32_t i = 0; i < hull->nv; ++i) {
+        const v3 r = rot_sc(q, V3(hull->verts[3 * i], hull->verts[3 * i + 1], hull->verts[3 * i + 2]));
+        lo = V3(fminf_(lo.x, r.x), fminf_(lo.y, r.y), fminf_(lo.z, r.z));
+        hi = V3(fmaxf_(hi.x, r.x), fmaxf_(hi.y, r.y), fmaxf_(hi.z, r.z));
+    }
+    const v3 c = V3((hi.x + lo.x) * 0.5f, (hi.y + lo.y) * 0.5f, (hi.z + lo.z) * 0.5f);
+    const v3 e = V3((hi.x - lo.x) * 0.5f, (hi.y - lo.y) * 0.5f, (hi.z - lo.z) * 0.5f);
+    const v3 add = V3(e.x + contact_offset, e.y + contact_offset, e.z + contact_offset);
+    const float b[6] = {p.x + c.x - add.x, p.y + c.y - add.y, p.z + c.z - add.z,
+                        p.x + c.x + add.x, p.y + c.y + add.y, p.z + c.z + add.z};
+    for (int i = 0; i < 6; ++i)
+        if (!isfinite(b[i])) return FO_OVERFLOW;
+    for (int a = 0; a < 3; ++a) {
+        out6[a] = fo_encode_min(b[a]);
+        out6[a + 3] = fo_encode_max(b[a + 3]);
+    }
+    return 0;
+}
+
+static void setcand(fo_candidate* c, v3 la, v3 lb, v3 nb, float sep) {
+    setv(c->la, la); setv(c->lb, lb); setv(c->nb, nb); c->sep = sep;
+}
+
+/* GuPCMGjkEpa.cpp:528-569 source_pcm_convex_gjk_epa */
+int fo_pcm_convex_gjk_epa(const fo_finite* a, const fo_finite* b, float cd, fo_candidate* out) {
+    const qt qb = Q4(b->q[0], b->q[1], b->q[2], b->q[3]);
+    const qt q0 = Q4(a->q[0], a->q[1], a->q[2], a->q[3]);
+    bpair_t p;
+    memset(&p, 0, sizeof p);
+    p.ha = ptv(a->half);
+    p.hb = ptv(b->half);
+    p.a_in_b = rotinv_gu(qb, vsub(ptv(a->p), ptv(b->p)));
+    p.rel = qmul(qconj(qb), q0);
+    if (a->hull) { p.va = a->hull->verts; p.nva = a->hull->nv; }
+    if (b->hull) { p.vb = b->hull->verts; p.nvb = b->hull->nv; }
+    p.ra = a->radius;
+    p.rb = b->radius;
+    memset(out, 0, sizeof *out);
+    if (!gjk_epa(&p, cd + a->radius + b->radius, out)) return 0;
+    if (a->radius > 0.f) {
+        const v3 off = rotinv_gu(p.rel, vmul(ptv(out->nb), -a->radius));
+        setv(out->la, vadd(ptv(out->la), off));
+        out->sep -= a->radius;
+    }
+    if (b->radius > 0.f) {
+        setv(out->lb, vadd(ptv(out->lb), vmul(ptv(out->nb), b->radius)));
+        out->sep -= b->radius;
+    }
+    return out->sep <= cd;
+}
+
+/* Face geometry of a finite shape: a hull's planar polygons or the six box
+ * faces (GuPCMGjkEpa.cpp:580-621). */
+static const v3 kAxis[3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}};
+static unsigned face_count(const fo_finite* s) { return s->hull ? s->hull->nf : 6u; }
+static v3 face_normal(const fo_finite* s, unsigned f) {
+    if (s->hull) return ptv(s->hull->faces[f].n);
+    return vmul(kAxis[f / 2u], (f & 1u) ? 1.f : -1.f);
+}
+static unsigned vertex_count(const fo_finite* s, unsigned f) { return s->hull ? s->hull->faces[f].count : 4u; }
+static v3 vertex_local(const fo_finite* s, unsigned f, unsigned k) {
+    if (s->hull) {
+        const uint32_t v = s->hull->idx[s->hull->faces[f].first + k];
+        return V3(s->hull->verts[3 * v], s->hull->verts[3 * v + 1], s->hull->verts[3 * v + 2]);
+    }
+    static const float corners[4][2] = {{1.f, 1.f}, {-1.f, 1.f}, {-1.f, -1.f}, {1.f, -1.f}};
+    const v3 n = face_normal(s, f);
+    const unsigned c = f / 2u;
+    const v3 u = kAxis[(c + 1u) % 3u];
+    const v3 v = vcross(n, u);
+    const v3 h = ptv(s->half);
+    const float hu = vcomp(h, (c + 1u) % 3u), hv = vcomp(h, (c + 2u) % 3u);
+    return vadd(vmul(n, vcomp(h, c)), vadd(vmul(u, corners[k][0] * hu), vmul(v, corners[k][1] * hv)));
+}
+typedef struct {
+    const fo_finite *a, *b;
+    qt qa, qb;
+    v3 pa, pb;
+} fc_ctx;
+static v3 fc_to_b(const fc_ctx* c, v3 p) { return rotinv_gu(c->qb, vsub(vadd(c->pa, rot_gu(c->qa, p)), c->pb)); }
+static v3 fc_vertex(const fc_ctx* c, const fo_finite* s, int is_a, unsigned f, unsigned k) {
+    const v3 l = vertex_local(s, f, k);
+    return is_a ? fc_to_b(c, l) : l;
+}
+static v3 fc_normal_b(const fc_ctx* c, const fo_finite* s, int is_a, unsigned f) {
+    const v3 n = face_normal(s, f);
+    return is_a ? rotinv_gu(c->qb, rot_gu(c->qa, n)) : n;
+}
+typedef struct {
+    const fc_ctx* c;
+    const fo_finite *ref, *inc;
+    int ref_is_a, inc_is_a, reference_b;
+    unsigned rf, inf, nr, ni;
+    v3 rn, anchor;
+    float cd, tol_sq;
+    fo_candidate* out;
+    unsigned count;
+} fc_clip;
+static v3 fc_r(const fc_clip* k, unsigned i) { return fc_vertex(k->c, k->ref, k->ref_is_a, k->rf, i % k->nr); }
+static v3 fc_q(const fc_clip* k, unsigned i) { return fc_vertex(k->c, k->inc, k->inc_is_a, k->inf, i % k->ni); }
+static float fc_cross2(const fc_clip* k, v3 a, v3 b) { return vdot(k->rn, vcross(a, b)); }
+/* GuPCMGjkEpa.cpp:710-765 emit: projected reference point, duplicate merge
+ * and the greedy five-point reduction. */
+static void fc_emit(fc_clip* k, v3 ip) {
+    const float sep = vdot(k->rn, vsub(ip, k->anchor));
+    if (!isfinite(sep) || sep > k->cd) return;
+    const v3 proj = vsub(ip, vmul(k->rn, sep));
+    const v3 a = k->reference_b ? ip : proj;
+    const v3 b = k->reference_b ? proj : ip;
+    const fc_ctx* c = k->c;
+    const v3 al = rotinv_gu(c->qa, vsub(vadd(c->pb, rot_gu(c->qb, a)), c->pa));
+    fo_candidate cand;
+    setcand(&cand, al, b, k->reference_b ? k->rn : vneg(k->rn), sep);
+    if (!isfinite(al.x) || !isfinite(b.x)) return;
+    for (unsigned i = 0; i < k->count; ++i)
+        if (vlen2(vsub(ptv(k->out[i].lb), ptv(cand.lb))) <= k->tol_sq) {
+            if (cand.sep < k->out[i].sep) k->out[i] = cand;
+            return;
+        }
+    if (k->count < 4u) {
+        k->out[k->count++] = cand;
+        return;
+    }
+    fo_candidate ch[5] = {k->out[0], k->out[1], k->out[2], k->out[3], cand};
+    unsigned deepest = 0;
+    for (unsigned i = 1; i < 5; ++i)
+        if (ch[i].sep < ch[deepest].sep) deepest = i;
+    float best = -1.f;
+    unsigned omit = 4;
+    for (unsigned ex = 0; ex < 5; ++ex) {
+        if (ex == deepest) continue;
+        float score = 0.f;
+        for (unsigned i = 0; i < 5; ++i) {
+            if (i == ex) continue;
+            for (unsigned j = i + 1; j < 5; ++j)
+                if (j != ex) score += vlen2(vsub(ptv(ch[i].lb), ptv(ch[j].lb)));
+        }
+        if (score > best) { best = score; omit = ex; }
+    }
+    if (omit != 4u) k->out[omit] = cand;
+}
+/* GuPCMGjkEpa.cpp:571-804 source_pcm_convex_face_contacts */
+int fo_pcm_convex_face_contacts(const fo_finite* a, const fo_finite* b, float cd,
+                                const fo_candidate* witness, fo_candidate out[4]) {
+    if (a->radius > 0.f || b->radius > 0.f || (a->hull && !a->hull->nf) || (b->hull && !b->hull->nf)) return 0;
+    fc_ctx c = {a, b, Q4(a->q[0], a->q[1], a->q[2], a->q[3]), Q4(b->q[0], b->q[1], b->q[2], b->q[3]), ptv(a->p),
+                ptv(b->p)};
+    const v3 normal = ptv(witness->nb);
+    if (!(vlen2(normal) > 0.f)) return 0;
+    unsigned fa = 0, fb = 0;
+    float ala = -2.f, alb = -2.f;
+    for (unsigned i = 0; i < face_count(a); ++i) {
+        const float d = vdot(vneg(normal), fc_normal_b(&c, a, 1, i));
+        if (d > ala) { ala = d; fa = i; }
+    }
+    for (unsigned i = 0; i < face_count(b); ++i) {
+        const float d = vdot(normal, fc_normal_b(&c, b, 0, i));
+        if (d > alb) { alb = d; fb = i; }
+    }
+    fc_clip k;
+    memset(&k, 0, sizeof k);
+    k.c = &c;
+    k.reference_b = alb >= ala;
+    if (fmaxf_(ala, alb) < 0.95f) return 0;
+    k.ref = k.reference_b ? b : a;
+    k.inc = k.reference_b ? a : b;
+    k.ref_is_a = !k.reference_b;
+    k.inc_is_a = k.reference_b;
+    k.rf = k.reference_b ? fb : fa;
+    k.rn = fc_normal_b(&c, k.ref, k.ref_is_a, k.rf);
+    float ial = -2.f;
+    for (unsigned i = 0; i < face_count(k.inc); ++i) {
+        const float d = vdot(vneg(k.rn), fc_normal_b(&c, k.inc, k.inc_is_a, i));
+        if (d > ial) { ial = d; k.inf = i; }
+    }
+    const v3 in_n = fc_normal_b(&c, k.inc, k.inc_is_a, k.inf);
+    const float den = vdot(in_n, k.rn);
+    if (!(den < -0.25f)) return 0;
+    k.nr = vertex_count(k.ref, k.rf);
+    k.ni = vertex_count(k.inc, k.inf);
+    if (k.nr < 3u || k.ni < 3u) return 0;
+    k.anchor = fc_r(&k, 0);
+    const v3 in_anchor = fc_q(&k, 0);
+    float el = 0.f;
+    for (unsigned i = 0; i < k.nr; ++i) el = fmaxf_(el, vlen2(vsub(fc_r(&k, i + 1), fc_r(&k, i))));
+    for (unsigned i = 0; i < k.ni; ++i) el = fmaxf_(el, vlen2(vsub(fc_q(&k, i + 1), fc_q(&k, i))));
+    const float scale = sqrtf(el);
+    if (!(scale > 0.f) || !isfinite(scale)) return 0;
+    const float tol = fmaxf_(scale * 1.e-5f, 1.e-6f);
+    const float ftol = tol / scale;
+    k.tol_sq = tol * tol;
+    k.cd = cd;
+    k.out = out;
+    for (unsigned i = 0; i < k.ni; ++i) {
+        const v3 v = fc_q(&k, i);
+        int inside = 1;
+        for (unsigned j = 0; j < k.nr && inside; ++j)
+            if (fc_cross2(&k, vsub(fc_r(&k, j + 1), fc_r(&k, j)), vsub(v, fc_r(&k, j))) < -tol * scale) inside = 0;
+        if (inside) fc_emit(&k, v);
+    }
+    for (unsigned i = 0; i < k.nr; ++i) {
+        const v3 v = fc_r(&k, i);
+        int inside = 1;
+        for (unsigned j = 0; j < k.ni && inside; ++j)
+            if (fc_cross2(&k, vsub(fc_q(&k, j + 1), fc_q(&k, j)), vsub(v, fc_q(&k, j))) > tol * scale) inside = 0;
+        if (!inside) continue;
+        const float height = vdot(in_n, vsub(in_anchor, v)) / den;
+        if (isfinite(height)) fc_emit(&k, vadd(v, vmul(k.rn, height)));
+    }
+    for (unsigned i = 0; i < k.ni; ++i) {
+        const v3 qa = fc_q(&k, i), e = vsub(fc_q(&k, i + 1), qa);
+        for (unsigned j = 0; j < k.nr; ++j) {
+            const v3 rb = fc_r(&k, j), f = vsub(fc_r(&k, j + 1), rb);
+            const float det = fc_cross2(&k, e, f);
+            if (fabsf(det) <= k.tol_sq) continue;
+            const v3 d = vsub(rb, qa);
+            const float t = fc_cross2(&k, d, f) / det;
+            const float u = fc_cross2(&k, d, e) / det;
+            if (t >= -ftol && t <= 1.f + ftol && u >= -ftol && u <= 1.f + ftol)
+                fc_emit(&k, vadd(qa, vmul(e, fclamp(t, 0.f, 1.f))));
+        }
+    }
+    return (int)k.count;
+}
+
+/* scene.cpp:3655-3772 Scene::generate_pcm_convex_pair */
+static float finite_margin(const fo_finite* s) {
+    float extent;
+    if (s->radius > 0.f) extent = s->radius;
+    else if (s->hull) extent = 0.5f * fminf_(fminf_(s->hull->hi[0] - s->hull->lo[0], s->hull->hi[1] - s->hull->lo[1]),
+                                             s->hull->hi[2] - s->hull->lo[2]);
+    else extent = fminf_(fminf_(s->half[0], s->half[1]), s->half[2]);
+    return fminf_(0.15f * extent, 0.15f);
+}
+int fo_generate_pcm_convex_pair(const fo_finite* first, const float* first_shape_half,
+                                const fo_finite* second, const float* second_shape_half, float cd,
+                                fo_pcm_cache* cache, fo_point out[4]) {
+    const qt q0 = Q4(first->q[0], first->q[1], first->q[2], first->q[3]);
+    const qt q1 = Q4(second->q[0], second->q[1], second->q[2], second->q[3]);
+    const v3 p0 = ptv(first->p), p1 = ptv(second->p);
+    const v3 delta = V3(p0.x - p1.x, p0.y - p1.y, p0.z - p1.z);
+    const v3 relative = rotinv_sc(q1, delta);
+    const qt rotation = qmul(qconj(q1), q0);
+    const float mm = fminf_(finite_margin(first), finite_margin(second));
+    const int prev = cache->count;
+    refresh_points(cache, relative, rotation, mm * 0.8f);
+    const float tr = cache->initialized
+        ? fmaxf_(fmaxf_(fabsf(relative.x - cache->rel_p[0]), fabsf(relative.y - cache->rel_p[1])),
+                 fabsf(relative.z - cache->rel_p[2]))
+        : INFINITY;
+    const float qa = qdot(q0, Q4(cache->qa[0], cache->qa[1], cache->qa[2], cache->qa[3]));
+    const float qb = qdot(q1, Q4(cache->qb[0], cache->qb[1], cache->qb[2], cache->qb[3]));
+    const float thr = mm * (cache->count == 0 ? 0.5f : 0.125f);
+    int regen = !cache->initialized || cache->count != prev || tr > thr || qa < 0.9999f || qb < 0.9999f;
+    if (!regen) {
+        const v3 ha = ptv(first_shape_half), hb = ptv(second_shape_half);
+        const float ta = (qa < 1.f ? acosf(fmaxf_(-1.f, qa)) : 0.f) * sqrtf(ha.x * ha.x + ha.y * ha.y + ha.z * ha.z);
+        const float tb = (qb < 1.f ? acosf(fmaxf_(-1.f, qb)) : 0.f) * sqrtf(hb.x * hb.x + hb.y * hb.y + hb.z * hb.z);
+        regen = ta > thr || tb > thr;
+    }
+    if (regen) {
+        setv(cache->rel_p, relative);
+        cache->rel_q[0] = rotation.x; cache->rel_q[1] = rotation.y; cache->rel_q[2] = rotation.z; cache->rel_q[3] = rotation.w;
+        memcpy(cache->qa, first->q, 16);
+        memcpy(cache->qb, second->q, 16);
+        cache->initialized = 1;
+        cache->count = 0;
+        fo_candidate w;
+        if (fo_pcm_convex_gjk_epa(first, second, cd, &w)) {
+            fo_candidate clipped[4];
+            const int n = fo_pcm_convex_face_contacts(first, second, cd, &w, clipped);
+            if (n) {
+                for (int i = 0; i < n; ++i) cache->pts[i] = clipped[i];
+                cache->count = (uint8_t)n;
+            } else {
+                cache->pts[0] = w;
+                cache->count = 1;
+            }
+        }
+    }
+    int emitted = 0;
+    for (int i = 0; i < cache->count; ++i) {
+        const fo_candidate* pt = &cache->pts[i];
+        if (pt->sep > cd) continue;
+        const v3 n = rot_sc(q1, ptv(pt->nb));
+        const v3 l = rot_sc(q1, ptv(pt->lb));
+        fo_point* o = &out[emitted++];
+        o->p[0] = p1.x + l.x; o->p[1] = p1.y + l.y; o->p[2] = p1.z + l.z;
+        setv(o->n, n);
+        o->sep = pt->sep;
+        if (!vfinite(ptv(o->p)) || !vfinite(n) || !isfinite(o->sep)) return -1;
     }
     return emitted;
 }

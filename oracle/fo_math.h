@@ -48,6 +48,15 @@ static inline v3 rot_gu(qt q, v3 v) {
     return vadd(v, vadd(vmul(t, q.w), vcross(u, t)));
 }
 static inline v3 rotinv_gu(qt q, v3 v) { return rot_gu(Q4(-q.x, -q.y, -q.z, q.w), v); }
+/* src/physx_port/foundation/PxQuat.h:262-271 PxQuat::rotate (compound.cpp) */
+static inline v3 rot_px(qt q, v3 v) {
+    const float vx = 2.0f * v.x, vy = 2.0f * v.y, vz = 2.0f * v.z;
+    const float w2 = q.w * q.w - 0.5f;
+    const float dot2 = q.x * vx + q.y * vy + q.z * vz;
+    return V3(vx * w2 + (q.y * vz - q.z * vy) * q.w + q.x * dot2,
+              vy * w2 + (q.z * vx - q.x * vz) * q.w + q.y * dot2,
+              vz * w2 + (q.x * vy - q.y * vx) * q.w + q.z * dot2);
+}
 /* scene.cpp:105-112 PxQuat::operator* */
 static inline qt qmul(qt a, qt b) {
     return Q4(a.w * b.x + b.w * a.x + a.y * b.z - a.z * b.y,

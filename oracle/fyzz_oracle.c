@@ -52,6 +52,7 @@ typedef struct {
     float sf, df, rest, damping;
     float contact_offset, rest_offset;
     uint32_t bounds[6];
+    const fo_mesh* hull;       /* cooked hull of an FO_CONVEX shape */
 } shape_t;
 typedef struct {
     v3 body0_normal, body1_normal, normal;
@@ -117,6 +118,7 @@ struct fo_scene {
     double* impulses; uint64_t nimp;
     uint32_t* sorted_minx_val; uint32_t* sorted_minx_id; uint64_t nsorted;
     int sleep;                 /* sleeping enabled */
+    fo_mesh* meshes; uint32_t nmeshes;
 };
 
 /* ------------------------- setup ------------------------- */
@@ -206,13 +208,19 @@ static int update_mass(fo_scene* s, uint32_t body, const uint32_t* shape_ids, in
     v3 center = V3(0, 0, 0);
     const float pi = 3.14159265358979323846f;
     float um[8];
+    v3 lc[8];
     for (int k = n - 1, i = 0; k >= 0; --k, ++i) {
         const shape_t* sh = &s->shapes[shape_ids[k]];
         um[i] = sh->type == FO_BOX ? sh->half.x * sh->half.y * sh->half.z * 8.0f
-                                   : (4.0f / 3.0f) * pi * sh->radius * sh->radius * sh->radius;
+              : sh->type == FO_CONVEX ? (float)sh->hull->volume
+                                      : (4.0f / 3.0f) * pi * sh->radius * sh->radius * sh->radius;
         const float m = um[i] * density;
         mass += m;
-        center = vadd(center, vmul(sh->lp, m));
+        /* a hull's centre of mass sits away from its authoring origin */
+        lc[i] = sh->type == FO_CONVEX ? vadd(sh->lp, rot_px(sh->lq, V3(sh->hull->center[0], sh->hull->center[1],
+                                                                       sh->hull->center[2])))
+                                      : sh->lp;
+        center = vadd(center, vmul(lc[i], m));
     }
     if (!(mass > 0.0f) || !isfinite(mass)) FAIL(FO_INVALID, "Compound mass outside supported range");
     center = vmul(center, 1.0f / mass);
@@ -221,20 +229,25 @@ static int update_mass(fo_scene* s, uint32_t body, const uint32_t* shape_ids, in
     for (int k = n - 1, i = 0; k >= 0; --k, ++i) {
         const shape_t* sh = &s->shapes[shape_ids[k]];
         const float m = um[i] * density;
-        v3 diag;
-        if (sh->type == FO_BOX) {
-            const v3 h = sh->half;
-            diag = vmul(V3(h.y * h.y + h.z * h.z, h.x * h.x + h.z * h.z, h.x * h.x + h.y * h.y), m / 3.0f);
-        } else {
-            const float v = (2.0f / 5.0f) * m * sh->radius * sh->radius;
-            diag = V3(v, v, v);
-        }
         m33 local;
         memset(&local, 0, sizeof local);
-        local.c[0].x = diag.x; local.c[1].y = diag.y; local.c[2].z = diag.z;
+        if (sh->type == FO_CONVEX) {
+            const float* I = sh->hull->inertia;
+            for (int c = 0; c < 3; ++c) local.c[c] = vmul(V3(I[3 * c], I[3 * c + 1], I[3 * c + 2]), density);
+        } else {
+            v3 diag;
+            if (sh->type == FO_BOX) {
+                const v3 h = sh->half;
+                diag = vmul(V3(h.y * h.y + h.z * h.z, h.x * h.x + h.z * h.z, h.x * h.x + h.y * h.y), m / 3.0f);
+            } else {
+                const float v = (2.0f / 5.0f) * m * sh->radius * sh->radius;
+                diag = V3(v, v, v);
+            }
+            local.c[0].x = diag.x; local.c[1].y = diag.y; local.c[2].z = diag.z;
+        }
         const m33 rot = m_from_q(sh->lq);
         const m33 rt = m_mul(m_mul(rot, local), m_t(rot));
-        const v3 d = vsub(sh->lp, center);
+        const v3 d = vsub(lc[i], center);
         const float dd = vdot(d, d);
         for (int c = 0; c < 3; ++c) {
             tensor.c[c] = vadd(tensor.c[c], rt.c[c]);
@@ -260,7 +273,25 @@ fo_scene* fo_scene_create(uint32_t nb, const float* bodies, uint32_t ns,
                           const float* shape_mat, uint32_t nj,
                           const uint32_t* joint_bodies, const float* joint_dist,
                           int has_floor, float floor_height, const float* floor_mat) {
+    return fo_scene_create_ex(nb, bodies, ns, shape_body, shape_type, shape_geom, shape_local, shape_mat, nj,
+                              joint_bodies, joint_dist, has_floor, floor_height, floor_mat, 0, NULL, NULL, NULL, NULL);
+}
+fo_scene* fo_scene_create_ex(uint32_t nb, const float* bodies, uint32_t ns,
+                             const uint32_t* shape_body, const uint32_t* shape_type,
+                             const float* shape_geom, const float* shape_local,
+                             const float* shape_mat, uint32_t nj,
+                             const uint32_t* joint_bodies, const float* joint_dist,
+                             int has_floor, float floor_height, const float* floor_mat,
+                             uint32_t n_meshes, const uint32_t* mesh_nv, const float* mesh_verts,
+                             const uint32_t* mesh_nt, const uint32_t* mesh_tris) {
     fo_scene* s = (fo_scene*)calloc(1, sizeof *s);
+    s->meshes = (fo_mesh*)calloc(n_meshes + 1, sizeof(fo_mesh));
+    s->nmeshes = n_meshes;
+    for (uint32_t m = 0, vo = 0, to = 0; m < n_meshes; vo += mesh_nv[m], to += mesh_nt[m], ++m)
+        if (fo_cook_convex(mesh_verts + 3ull * vo, mesh_nv[m], mesh_tris + 3ull * to, mesh_nt[m], &s->meshes[m])) {
+            fo_scene_destroy(s);
+            return NULL;
+        }
     const uint32_t off = has_floor ? 1u : 0u;
     s->na = nb + off;
     s->ns = ns + off;
@@ -308,6 +339,18 @@ fo_scene* fo_scene_create(uint32_t nb, const float* bodies, uint32_t ns,
             const float* g = shape_geom + 4ull * si;
             sh->half = V3(g[0], g[1], g[2]);
             sh->radius = g[0];
+            if (sh->type == FO_CONVEX) {
+                /* Scene::attach_convex (scene.cpp:301-305): half extents
+                 * are the larger absolute bound per axis */
+                const uint32_t mi = (uint32_t)g[0];
+                if (mi >= n_meshes) { fo_scene_destroy(s); return NULL; }
+                sh->hull = &s->meshes[mi];
+                const float* lo = sh->hull->lo;
+                const float* hi = sh->hull->hi;
+                sh->half = V3(fmaxf_(fabsf(lo[0]), fabsf(hi[0])), fmaxf_(fabsf(lo[1]), fabsf(hi[1])),
+                              fmaxf_(fabsf(lo[2]), fabsf(hi[2])));
+                sh->radius = 0.0f;
+            }
             const float* l = shape_local + 7ull * si;
             sh->lp = V3(l[0], l[1], l[2]);
             sh->lq = normalize_q(l + 3);
@@ -389,6 +432,8 @@ void fo_scene_destroy(fo_scene* s) {
     free(s->joint_kind); free(s->joint_auth); free(s->joint_lp); free(s->joint_lq);
     free(s->mgr); free(s->found); free(s->lost); free(s->man); free(s->desc); free(s->pend);
     free(s->impulses); free(s->sorted_minx_val); free(s->sorted_minx_id);
+    for (uint32_t m = 0; m < s->nmeshes; ++m) fo_mesh_free(&s->meshes[m]);
+    free(s->meshes);
     free(s);
 }
 
@@ -420,7 +465,10 @@ static int build_pairs(fo_scene* s, uint64_t** out, uint64_t* nout) {
         const float pose[7] = {sh->wp.x, sh->wp.y, sh->wp.z, sh->wq.x, sh->wq.y, sh->wq.z, sh->wq.w};
         const float geom[4] = {sh->half.x, sh->half.y, sh->half.z, 0};
         const float sg[4] = {sh->radius, 0, 0, 0};
-        if (fo_shape_bounds(sh->type, pose, sh->type == FO_SPHERE ? sg : geom, sh->contact_offset, sh->bounds))
+        if (sh->type == FO_CONVEX) {
+            if (fo_convex_bounds(pose, sh->hull, sh->contact_offset, sh->bounds))
+                FAIL(FO_OVERFLOW, "Convex scene AABB is not finite");
+        } else if (fo_shape_bounds(sh->type, pose, sh->type == FO_SPHERE ? sg : geom, sh->contact_offset, sh->bounds))
             FAIL(FO_OVERFLOW, "Native scene AABB is not finite");
     }
     ep_t* ep = (ep_t*)malloc(sizeof(ep_t) * (s->ns + 1));
@@ -476,6 +524,22 @@ static void shape_record(const shape_t* sh, float out[10]) {
     out[3] = sh->wp.x; out[4] = sh->wp.y; out[5] = sh->wp.z;
     out[6] = sh->wq.x; out[7] = sh->wq.y; out[8] = sh->wq.z; out[9] = sh->wq.w;
 }
+/* The PcmFiniteShape descriptor of scene.cpp:3712-3731: spheres carry their
+ * radius, hulls the half size of their vertex bounds. */
+static void finite_of(const shape_t* sh, fo_finite* f) {
+    memset(f, 0, sizeof *f);
+    f->half[0] = sh->half.x; f->half[1] = sh->half.y; f->half[2] = sh->half.z;
+    if (sh->type == FO_SPHERE) {
+        f->radius = sh->radius;
+        f->half[0] = f->half[1] = f->half[2] = sh->radius;
+    }
+    if (sh->type == FO_CONVEX) {
+        f->hull = sh->hull;
+        for (int k = 0; k < 3; ++k) f->half[k] = 0.5f * (sh->hull->hi[k] - sh->hull->lo[k]);
+    }
+    f->p[0] = sh->wp.x; f->p[1] = sh->wp.y; f->p[2] = sh->wp.z;
+    f->q[0] = sh->wq.x; f->q[1] = sh->wq.y; f->q[2] = sh->wq.z; f->q[3] = sh->wq.w;
+}
 
 /* Scene::publish_pairs + update_contacts, CPU Gu path (scene.cpp:3230-3304,
  * 4012-4758): carry each surviving manager's persistent PCM cache, generate
@@ -525,7 +589,10 @@ static int collide(fo_scene* s) {
         const shape_t* B = &s->shapes[(uint32_t)m->key];
         const float cd = A->contact_offset + B->contact_offset;
         const int plane = A->type == FO_PLANE || B->type == FO_PLANE;
-        const int sphere = A->type == FO_SPHERE || B->type == FO_SPHERE;
+        /* cooked hulls take the PCM plane or convex generator, whatever the
+         * other shape is (scene.cpp:4307-4317) */
+        const int convex = A->type == FO_CONVEX || B->type == FO_CONVEX;
+        const int sphere = !convex && (A->type == FO_SPHERE || B->type == FO_SPHERE);
         const shape_t* first = plane ? (A->type == FO_PLANE ? A : B) : (m->reversed ? B : A);
         const shape_t* second = plane ? (A->type == FO_PLANE ? B : A) : (m->reversed ? A : B);
         int count = 0;
@@ -534,7 +601,20 @@ static int collide(fo_scene* s) {
             float box[10];
             shape_record(second, box);
             const float pp[3] = {first->wp.x, first->wp.y, first->wp.z};
-            count = fo_generate_pcm_plane_box(pp, box, cd, &m->cache, pts);
+            if (second->type == FO_CONVEX)
+                count = fo_generate_pcm_plane_convex(pp, box, box + 3, second->hull, cd, &m->cache, pts);
+            else
+                count = fo_generate_pcm_plane_box(pp, box, cd, &m->cache, pts);
+        } else if (!plane && convex) {
+            fo_finite f0, f1;
+            finite_of(first, &f0);
+            finite_of(second, &f1);
+            const float h0[3] = {first->type == FO_SPHERE ? 0.f : first->half.x, first->type == FO_SPHERE ? 0.f : first->half.y,
+                                 first->type == FO_SPHERE ? 0.f : first->half.z};
+            const float h1[3] = {second->type == FO_SPHERE ? 0.f : second->half.x,
+                                 second->type == FO_SPHERE ? 0.f : second->half.y,
+                                 second->type == FO_SPHERE ? 0.f : second->half.z};
+            count = fo_generate_pcm_convex_pair(&f0, h0, &f1, h1, cd, &m->cache, pts);
         } else if (!plane && !sphere) {
             float r0[10], r1[10];
             shape_record(first, r0);

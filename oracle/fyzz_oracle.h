@@ -13,7 +13,7 @@
 extern "C" {
 #endif
 
-enum { FO_BOX = 0, FO_SPHERE = 1, FO_PLANE = 2 };
+enum { FO_BOX = 0, FO_SPHERE = 1, FO_PLANE = 2, FO_CONVEX = 3 };
 enum { FO_OK = 0, FO_INVALID = 1, FO_LOGIC = 2, FO_OVERFLOW = 3 };
 /* Joint kinds (scene.h:1528 JointKind, plus the two distance authorings). */
 enum { FO_JOINT_CENTER = 0, FO_JOINT_ANCHORED = 1, FO_JOINT_FIXED = 2, FO_JOINT_SPHERICAL = 3,
@@ -31,6 +31,38 @@ typedef struct {
     float rel_p[3], rel_q[4], qa[4], qb[4];
     uint8_t count, initialized, pad[2];
 } fo_pcm_cache;
+
+/* Cooked convex mesh (include/fyzzxyzzy/convex.h:19-53): planar faces
+ * (outward normal, plane distance, boundary loop in idx[first, first+count)),
+ * density-one volume, centre of mass and inertia columns about it. */
+typedef struct { float n[3], d; uint32_t first, count; } fo_face;
+typedef struct {
+    uint32_t nv, nf, ni;
+    float* verts;
+    fo_face* faces;
+    uint32_t* idx;
+    double volume;
+    float center[3], inertia[9], lo[3], hi[3];
+} fo_mesh;
+int fo_cook_convex(const float* verts, uint32_t nv, const uint32_t* tris, uint32_t nt, fo_mesh* out);
+void fo_mesh_free(fo_mesh* m);
+/* PcmFiniteShape (scene.h:589-599): half extents, pose, sphere radius and
+ * an optional cooked hull in the shape's own frame. */
+typedef struct { float half[3], p[3], q[4], radius; const fo_mesh* hull; } fo_finite;
+int fo_pcm_convex_gjk_epa(const fo_finite* a, const fo_finite* b, float cd, fo_candidate* out);
+int fo_pcm_convex_face_contacts(const fo_finite* a, const fo_finite* b, float cd,
+                                const fo_candidate* witness, fo_candidate out[4]);
+/* Scene::generate_pcm_convex_pair (scene.cpp:3655-3772).  shape_half is the
+ * attached shape's half extents (zero for spheres), used by the rotation
+ * travel test. */
+int fo_generate_pcm_convex_pair(const fo_finite* first, const float* first_shape_half,
+                                const fo_finite* second, const float* second_shape_half, float cd,
+                                fo_pcm_cache* cache, fo_point out[4]);
+/* Scene::generate_pcm_plane_box with a cooked hull (scene.cpp:3774-3972). */
+int fo_generate_pcm_plane_convex(const float* plane_p, const float* shape_half, const float* pose7,
+                                 const fo_mesh* hull, float cd, fo_pcm_cache* cache, fo_point out[4]);
+/* Scene::update_shape_bounds for a cooked hull (scene.cpp:1258-1298). */
+int fo_convex_bounds(const float* pose7, const fo_mesh* hull, float contact_offset, uint32_t* out6);
 
 uint32_t fo_encode_min(float v);
 uint32_t fo_encode_max(float v);
@@ -57,6 +89,18 @@ fo_scene* fo_scene_create(uint32_t nb, const float* bodies, uint32_t ns,
                           const float* shape_mat, uint32_t nj,
                           const uint32_t* joint_bodies, const float* joint_dist,
                           int has_floor, float floor_height, const float* floor_mat);
+/* As fo_scene_create, with cooked convex shapes: shape_type FO_CONVEX takes
+ * its mesh index in shape_geom[0]; mesh m has mesh_nv[m] vertices and
+ * mesh_nt[m] triangles, concatenated in mesh order in mesh_verts (3 floats
+ * each) and mesh_tris (3 indices each, local to the mesh). */
+fo_scene* fo_scene_create_ex(uint32_t nb, const float* bodies, uint32_t ns,
+                             const uint32_t* shape_body, const uint32_t* shape_type,
+                             const float* shape_geom, const float* shape_local,
+                             const float* shape_mat, uint32_t nj,
+                             const uint32_t* joint_bodies, const float* joint_dist,
+                             int has_floor, float floor_height, const float* floor_mat,
+                             uint32_t n_meshes, const uint32_t* mesh_nv, const float* mesh_verts,
+                             const uint32_t* mesh_nt, const uint32_t* mesh_tris);
 void fo_scene_destroy(fo_scene* s);
 const char* fo_error(void);
 /* One Scene::step.  manager_order / joint_order (optional) replay the

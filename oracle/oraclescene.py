@@ -29,6 +29,9 @@ def lib():
         L.fo_error.restype = C.c_char_p
         L.fo_scene_create.restype = vp
         L.fo_scene_create.argtypes = [u32, vp, u32, vp, vp, vp, vp, vp, u32, vp, vp, i32, f32, vp]
+        L.fo_scene_create_ex.restype = vp
+        L.fo_scene_create_ex.argtypes = [u32, vp, u32, vp, vp, vp, vp, vp, u32, vp, vp, i32, f32, vp,
+                                         u32, vp, vp, vp, vp]
         L.fo_scene_destroy.argtypes = [vp]
         L.fo_scene_step.argtypes = [vp, f32, vp, u64, vp, u64]
         L.fo_scene_advance_collision.argtypes = [vp]
@@ -77,12 +80,14 @@ class OracleScene:
             spec.shape_local, spec.shape_mat, spec.joints, spec.joint_dist)]
         self._keep = arrs
         self._floor_mat = np.asarray(spec.floor_mat, np.float32)
-        self.h = L.fo_scene_create(spec.n_bodies, _p(arrs[0]), spec.n_shapes, _p(arrs[1]),
-                                   _p(arrs[2]), _p(arrs[3]), _p(arrs[4]), _p(arrs[5]),
-                                   arrs[6].shape[0], _p(arrs[6]), _p(arrs[7]),
-                                   0 if spec.floor is None else 1,
-                                   0.0 if spec.floor is None else float(spec.floor),
-                                   _p(self._floor_mat))
+        self._meshes = spec.mesh_arrays()
+        nv, v, nt, t = self._meshes
+        self.h = L.fo_scene_create_ex(spec.n_bodies, _p(arrs[0]), spec.n_shapes, _p(arrs[1]),
+                                      _p(arrs[2]), _p(arrs[3]), _p(arrs[4]), _p(arrs[5]),
+                                      arrs[6].shape[0], _p(arrs[6]), _p(arrs[7]),
+                                      0 if spec.floor is None else 1,
+                                      0.0 if spec.floor is None else float(spec.floor),
+                                      _p(self._floor_mat), len(spec.convex_meshes), _p(nv), _p(v), _p(nt), _p(t))
         if not self.h:
             raise RuntimeError(L.fo_error().decode())
         if spec.has_joint_kinds():
@@ -218,3 +223,82 @@ def pcm_box_box_gjk_epa(a, b, cd):
     out = np.zeros(10, np.float32)
     ok = lib().fo_pcm_box_box_gjk_epa(_p(np.asarray(a, np.float32)), _p(np.asarray(b, np.float32)), cd, _p(out))
     return bool(ok), out
+
+
+# ---------------- cooked convex hulls ----------------
+class _Face(C.Structure):
+    _fields_ = [("n", C.c_float * 3), ("d", C.c_float), ("first", C.c_uint32), ("count", C.c_uint32)]
+
+
+class _Mesh(C.Structure):
+    _fields_ = [("nv", C.c_uint32), ("nf", C.c_uint32), ("ni", C.c_uint32),
+                ("verts", C.POINTER(C.c_float)), ("faces", C.POINTER(_Face)), ("idx", C.POINTER(C.c_uint32)),
+                ("volume", C.c_double), ("center", C.c_float * 3), ("inertia", C.c_float * 9),
+                ("lo", C.c_float * 3), ("hi", C.c_float * 3)]
+
+
+class _Finite(C.Structure):
+    _fields_ = [("half", C.c_float * 3), ("p", C.c_float * 3), ("q", C.c_float * 4), ("radius", C.c_float),
+                ("hull", C.POINTER(_Mesh))]
+
+
+def _cook(verts, tris):
+    L = lib()
+    L.fo_cook_convex.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.POINTER(_Mesh)]
+    v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+    t = np.ascontiguousarray(tris, np.uint32).reshape(-1, 3)
+    m = _Mesh()
+    if L.fo_cook_convex(_p(v), v.shape[0], _p(t), t.shape[0], C.byref(m)):
+        raise ValueError("oracle cooking rejected the mesh")
+    return m
+
+
+def cook_convex(verts, tris):
+    """The oracle's cooking, in the format of refscene.cook_convex."""
+    m = _cook(verts, tris)
+    faces = np.array([[*m.faces[i].n, m.faces[i].d, m.faces[i].first, m.faces[i].count] for i in range(m.nf)],
+                     np.float32).reshape(-1, 6)
+    out = {"faces": faces, "idx": np.array([m.idx[i] for i in range(m.ni)], np.uint32), "volume": m.volume,
+           "center": np.array(m.center, np.float32), "inertia": np.array(m.inertia, np.float32).reshape(3, 3).T.copy(),
+           "lo": np.array(m.lo, np.float32), "hi": np.array(m.hi, np.float32)}
+    lib().fo_mesh_free(C.byref(m))
+    return out
+
+
+class OracleConvexGu:
+    """fo_pcm_convex_gjk_epa / fo_pcm_convex_face_contacts over cooked
+    meshes, with the argument format of refscene.RefConvexGu."""
+
+    def __init__(self, meshes):
+        self.meshes = [_cook(v, t) for (v, t) in meshes]
+        L = lib()
+        L.fo_pcm_convex_gjk_epa.argtypes = [C.POINTER(_Finite), C.POINTER(_Finite), C.c_float, C.c_void_p]
+        L.fo_pcm_convex_face_contacts.argtypes = [C.POINTER(_Finite), C.POINTER(_Finite), C.c_float, C.c_void_p,
+                                                  C.c_void_p]
+
+    def __del__(self):
+        for m in getattr(self, "meshes", []):
+            lib().fo_mesh_free(C.byref(m))
+
+    def _finite(self, d, mesh):
+        f = _Finite()
+        d = np.asarray(d, np.float32)
+        f.half[:] = d[0:3].tolist()
+        f.p[:] = d[3:6].tolist()
+        f.q[:] = d[6:10].tolist()
+        f.radius = float(d[10])
+        if mesh >= 0:
+            f.hull = C.pointer(self.meshes[mesh])
+        return f
+
+    def gjk_epa(self, a, ma, b, mb, cd):
+        out = np.zeros(10, np.float32)
+        ok = lib().fo_pcm_convex_gjk_epa(C.byref(self._finite(a, ma)), C.byref(self._finite(b, mb)), cd, _p(out))
+        return bool(ok), out
+
+    def face_contacts(self, a, ma, b, mb, cd, witness):
+        out = np.zeros((4, 10), np.float32)
+        w = np.ascontiguousarray(witness, np.float32)
+        n = lib().fo_pcm_convex_face_contacts(C.byref(self._finite(a, ma)), C.byref(self._finite(b, mb)), cd,
+                                             _p(w), _p(out))
+        return out[:n]

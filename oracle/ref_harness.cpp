@@ -21,6 +21,7 @@
 // fixtures the reference's Scene declares (src/native/scene.h:1082-1089).
 
 #include "native/scene.h"
+#include "fyzzxyzzy/convex.h"
 
 #include <cmath>
 #include <cstdint>
@@ -60,6 +61,7 @@ struct Handle {
     std::unique_ptr<Scene> scene;
     std::vector<fyzz::BodyId> bodies;   // dynamic body index -> BodyId
     std::vector<fyzz::ShapeId> shapes;  // shape index -> ShapeId
+    std::vector<std::shared_ptr<const fyzz::ConvexMesh>> meshes;  // convex shape_geom[0] -> mesh
     bool has_floor = false;
 };
 
@@ -143,6 +145,8 @@ int fz_ref_build(void* p, uint32_t nb, const float* bodies, uint32_t ns,
                 const float* g = shape_geom + 4ull * i;
                 if (shape_type[i] == 0)
                     h->shapes[i] = s.attach_box(h->bodies[b], {g[0], g[1], g[2]}, local);
+                else if (shape_type[i] == 3)
+                    h->shapes[i] = s.attach_convex(h->bodies[b], h->meshes.at(static_cast<std::size_t>(g[0])), local);
                 else
                     h->shapes[i] = s.attach_sphere(h->bodies[b], g[0], local);
             }
@@ -438,6 +442,118 @@ uint64_t fz_ref_contact_event_points(void* p, float* pts, double* impulse) {
 }
 
 // ---- stateless Gu generators (public free functions of the reference) ----
+// ---- cooked convex meshes (include/fyzzxyzzy/convex.h, cooked_convex.cpp) ----
+// Cooks through fyzz::cook_convex_mesh.  Outputs, sized by the caller for
+// 3 * nt faces and indices: faces as normal(3) distance(1) first(1)
+// count(1) floats, the face index stream, counts {nf, ni}, the volume and
+// center(3) inertia columns(9) bounds min(3) max(3).
+int fz_ref_cook_convex(const float* verts, uint32_t nv, const uint32_t* tris, uint32_t nt,
+                       float* faces6, uint32_t* idx, uint32_t* counts, double* volume, float* mass18) {
+    return guarded([&] {
+        std::vector<fyzz::Vec3> v(nv);
+        for (uint32_t i = 0; i < nv; ++i) v[i] = {verts[3*i], verts[3*i+1], verts[3*i+2]};
+        std::vector<fyzz::ConvexTriangle> t(nt);
+        for (uint32_t i = 0; i < nt; ++i) t[i] = {tris[3*i], tris[3*i+1], tris[3*i+2]};
+        const auto m = fyzz::cook_convex_mesh(v, t);
+        const auto f = m->faces();
+        const auto fi = m->face_indices();
+        counts[0] = static_cast<uint32_t>(f.size());
+        counts[1] = static_cast<uint32_t>(fi.size());
+        for (std::size_t i = 0; i < f.size(); ++i) {
+            float* o = faces6 + 6 * i;
+            o[0] = f[i].normal.x; o[1] = f[i].normal.y; o[2] = f[i].normal.z; o[3] = f[i].distance;
+            o[4] = static_cast<float>(f[i].first_index); o[5] = static_cast<float>(f[i].index_count);
+        }
+        for (std::size_t i = 0; i < fi.size(); ++i) idx[i] = fi[i];
+        const auto& mp = m->mass_properties();
+        *volume = mp.volume;
+        mass18[0] = mp.center.x; mass18[1] = mp.center.y; mass18[2] = mp.center.z;
+        for (int c = 0; c < 3; ++c) {
+            mass18[3 + 3*c] = mp.inertia_columns[c].x;
+            mass18[4 + 3*c] = mp.inertia_columns[c].y;
+            mass18[5 + 3*c] = mp.inertia_columns[c].z;
+        }
+        const auto lo = m->bounds_min(), hi = m->bounds_max();
+        mass18[12] = lo.x; mass18[13] = lo.y; mass18[14] = lo.z;
+        mass18[15] = hi.x; mass18[16] = hi.y; mass18[17] = hi.z;
+    });
+}
+
+// Meshes for fz_ref_build's convex shapes (shape_type 3, mesh index in
+// shape_geom[0]); call before fz_ref_build.  Mesh m has mesh_nv[m] vertices
+// and mesh_nt[m] triangles, concatenated in mesh order.
+int fz_ref_set_meshes(void* p, uint32_t n, const uint32_t* mesh_nv, const float* verts,
+                      const uint32_t* mesh_nt, const uint32_t* tris) {
+    auto* h = static_cast<Handle*>(p);
+    return guarded([&] {
+        h->meshes.clear();
+        std::size_t vo = 0, to = 0;
+        for (uint32_t m = 0; m < n; ++m) {
+            std::vector<fyzz::Vec3> v(mesh_nv[m]);
+            for (uint32_t i = 0; i < mesh_nv[m]; ++i)
+                v[i] = {verts[3*(vo+i)], verts[3*(vo+i)+1], verts[3*(vo+i)+2]};
+            std::vector<fyzz::ConvexTriangle> t(mesh_nt[m]);
+            for (uint32_t i = 0; i < mesh_nt[m]; ++i)
+                t[i] = {tris[3*(to+i)], tris[3*(to+i)+1], tris[3*(to+i)+2]};
+            h->meshes.push_back(fyzz::cook_convex_mesh(v, t));
+            vo += mesh_nv[m];
+            to += mesh_nt[m];
+        }
+    });
+}
+
+// Finite shape descriptors for the convex Gu functions: half extents(3)
+// position(3) orientation xyzw(4) sphere radius(1), plus a mesh index into
+// the handle's meshes (-1 for none).
+static fyzz::native::PcmFiniteShape finite_of(const Handle* h, const float* d, int mesh) {
+    fyzz::native::PcmFiniteShape f{};
+    f.half_extents = {d[0], d[1], d[2]};
+    f.position = {d[3], d[4], d[5]};
+    f.orientation = {d[6], d[7], d[8], d[9]};
+    f.sphere_radius = d[10];
+    if (mesh >= 0) {
+        const auto& m = h->meshes.at(static_cast<std::size_t>(mesh));
+        f.hull_vertices = m->vertices();
+        f.hull_faces = m->faces();
+        f.hull_face_indices = m->face_indices();
+    }
+    return f;
+}
+static void put_candidate(const fyzz::native::PcmContactCandidate& k, float* o) {
+    o[0]=k.local_a.x; o[1]=k.local_a.y; o[2]=k.local_a.z;
+    o[3]=k.local_b.x; o[4]=k.local_b.y; o[5]=k.local_b.z;
+    o[6]=k.normal_b.x; o[7]=k.normal_b.y; o[8]=k.normal_b.z;
+    o[9]=k.separation;
+}
+int fz_ref_pcm_convex_gjk_epa(void* p, const float* a, int mesh_a, const float* b, int mesh_b,
+                              float cd, float* out) {
+    const auto* h = static_cast<const Handle*>(p);
+    fyzz::native::PcmContactCandidate k{};
+    bool ok = false;
+    const int rc = guarded([&] {
+        ok = fyzz::native::source_pcm_convex_gjk_epa(finite_of(h, a, mesh_a), finite_of(h, b, mesh_b), cd, k,
+                                                     nullptr);
+    });
+    if (rc) return -rc;
+    put_candidate(k, out);
+    return ok ? 1 : 0;
+}
+int fz_ref_pcm_convex_face_contacts(void* p, const float* a, int mesh_a, const float* b, int mesh_b,
+                                    float cd, const float* witness, float* out) {
+    const auto* h = static_cast<const Handle*>(p);
+    std::array<fyzz::native::PcmContactCandidate, 4> c{};
+    int n = 0;
+    const int rc = guarded([&] {
+        const float* w = witness;
+        const fyzz::native::PcmContactCandidate k{{w[0],w[1],w[2]}, {w[3],w[4],w[5]}, {w[6],w[7],w[8]}, w[9]};
+        n = fyzz::native::source_pcm_convex_face_contacts(finite_of(h, a, mesh_a), finite_of(h, b, mesh_b), cd,
+                                                          k, c);
+    });
+    if (rc) return -rc;
+    for (int i = 0; i < n; ++i) put_candidate(c[i], out + 10 * i);
+    return n;
+}
+
 // Shape records: half extents(3) position(3) orientation xyzw(4).
 // Candidate records: local_a(3) local_b(3) normal_b(3) separation(1).
 int fz_ref_pcm_box_box_candidates(const float* a, const float* b, float cd,

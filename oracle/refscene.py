@@ -42,6 +42,10 @@ def lib():
         L.fz_ref_set_kinematic.argtypes = [vp, u32, i32]
         L.fz_ref_set_kinematic_target.argtypes = [vp, u32, vp]
         L.fz_ref_encoded_bounds.argtypes = [vp, vp]
+        L.fz_ref_set_meshes.argtypes = [vp, u32, vp, vp, vp, vp]
+        L.fz_ref_cook_convex.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, vp]
+        L.fz_ref_pcm_convex_gjk_epa.argtypes = [vp, vp, i32, vp, i32, f32, vp]
+        L.fz_ref_pcm_convex_face_contacts.argtypes = [vp, vp, i32, vp, i32, f32, vp, vp]
         for name in ("fz_ref_endpoints",):
             getattr(L, name).restype = u64
         L.fz_ref_endpoints.argtypes = [vp, i32, vp, vp, vp]
@@ -88,6 +92,10 @@ class RefScene:
         self._keep = arrs
         self._floor_mat = np.asarray(spec.floor_mat, np.float32)
         kinds = spec.has_joint_kinds()
+        if spec.convex_meshes:
+            self._meshes = spec.mesh_arrays()
+            nv, v, nt, t = self._meshes
+            self._check(L.fz_ref_set_meshes(self.h, len(spec.convex_meshes), _p(nv), _p(v), _p(nt), _p(t)))
         rc = L.fz_ref_build(self.h, spec.n_bodies, _p(arrs[0]), spec.n_shapes,
                             _p(arrs[1]), _p(arrs[2]), _p(arrs[3]), _p(arrs[4]),
                             _p(arrs[5]), 0 if kinds else arrs[6].shape[0], _p(arrs[6]), _p(arrs[7]),
@@ -259,3 +267,73 @@ def pcm_box_box_gjk_epa(a, b, cd):
     if ok < 0:
         raise RuntimeError(lib().fz_ref_error().decode())
     return bool(ok), out
+
+
+def cook_convex(verts, tris):
+    """fyzz::cook_convex_mesh: dict of faces (nf, 6: normal, distance, first,
+    count), idx, volume (float64), center (3), inertia (3x3, column j =
+    inertia[:, j]), lo, hi.  Raises ValueError when cooking rejects the mesh."""
+    L = lib()
+    v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+    t = np.ascontiguousarray(tris, np.uint32).reshape(-1, 3)
+    cap = 3 * t.shape[0]
+    faces = np.zeros((cap, 6), np.float32)
+    idx = np.zeros(cap, np.uint32)
+    counts = np.zeros(2, np.uint32)
+    vol = np.zeros(1, np.float64)
+    m = np.zeros(18, np.float32)
+    rc = L.fz_ref_cook_convex(_p(v), v.shape[0], _p(t), t.shape[0], _p(faces), _p(idx), _p(counts), _p(vol), _p(m))
+    if rc:
+        raise ValueError(L.fz_ref_error().decode())
+    return {"faces": faces[:counts[0]], "idx": idx[:counts[1]], "volume": float(vol[0]), "center": m[0:3],
+            "inertia": m[3:12].reshape(3, 3).T.copy(), "lo": m[12:15], "hi": m[15:18]}
+
+
+class RefConvexGu:
+    """The reference's free convex Gu functions (source_pcm_convex_gjk_epa,
+    source_pcm_convex_face_contacts) over a fixed list of cooked meshes.
+    Shapes are 11 floats: half extents, position, quaternion xyzw, radius."""
+
+    def __init__(self, meshes):
+        L = lib()
+        self.h = L.fz_ref_create(0)
+        self.spec_meshes = SceneMeshes(meshes)
+        nv, v, nt, t = self.spec_meshes.arrays
+        rc = L.fz_ref_set_meshes(self.h, len(meshes), _p(nv), _p(v), _p(nt), _p(t))
+        if rc:
+            raise ValueError(L.fz_ref_error().decode())
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().fz_ref_destroy(self.h)
+            self.h = None
+
+    def gjk_epa(self, a, ma, b, mb, cd):
+        out = np.zeros(10, np.float32)
+        a = np.ascontiguousarray(a, np.float32)
+        b = np.ascontiguousarray(b, np.float32)
+        rc = lib().fz_ref_pcm_convex_gjk_epa(self.h, _p(a), ma, _p(b), mb, cd, _p(out))
+        if rc < 0:
+            raise RuntimeError(lib().fz_ref_error().decode())
+        return bool(rc), out
+
+    def face_contacts(self, a, ma, b, mb, cd, witness):
+        out = np.zeros((4, 10), np.float32)
+        a = np.ascontiguousarray(a, np.float32)
+        b = np.ascontiguousarray(b, np.float32)
+        w = np.ascontiguousarray(witness, np.float32)
+        n = lib().fz_ref_pcm_convex_face_contacts(self.h, _p(a), ma, _p(b), mb, cd, _p(w), _p(out))
+        if n < 0:
+            raise RuntimeError(lib().fz_ref_error().decode())
+        return out[:n]
+
+
+class SceneMeshes:
+    """Concatenated mesh arrays for the C ABIs."""
+
+    def __init__(self, meshes):
+        nv = np.asarray([m[0].shape[0] for m in meshes], np.uint32)
+        nt = np.asarray([m[1].shape[0] for m in meshes], np.uint32)
+        v = np.ascontiguousarray(np.concatenate([np.asarray(m[0], np.float32).reshape(-1, 3) for m in meshes]))
+        t = np.ascontiguousarray(np.concatenate([np.asarray(m[1], np.uint32).reshape(-1, 3) for m in meshes]))
+        self.arrays = (nv, v, nt, t)
