@@ -41,6 +41,8 @@ EXPORTS = (
     "fyzz_b200_rollout_backward", "fyzz_b200_read_mass_frames", "fyzz_b200_read_friction_anchors",
     "fyzz_b200_fit_pair_budget", "fyzz_b200_set_sleeping", "fyzz_b200_read_sleep_state", "fyzz_b200_set_body_kinematic",
     "fyzz_b200_set_body_kinematic_target", "fyzz_b200_rollout_rewind",
+    "fyzz_b200_cook_convex_mesh", "fyzz_b200_convex_mesh_release", "fyzz_b200_cook_error",
+    "fyzz_b200_convex_mesh_info", "fyzz_b200_attach_convex_shape", "fyzz_b200_add_scene_ex",
 )
 STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 
@@ -117,6 +119,15 @@ def lib():
         for name in ("fixed", "spherical", "revolute", "prismatic"):
             getattr(L, f"fyzz_b200_add_{name}_constraint").argtypes = [vp, u32, u32, vp, vp, P(u64)]
         L.fyzz_b200_add_scene.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, vp, u32, vp, vp, i32, f32, vp, P(u32)]
+        L.fyzz_b200_add_scene_ex.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, vp, u32, vp, vp, i32, f32, vp,
+                                             u32, P(vp), P(u32)]
+        L.fyzz_b200_cook_convex_mesh.argtypes = [vp, u32, vp, u32, P(vp)]
+        L.fyzz_b200_convex_mesh_release.argtypes = [vp]
+        L.fyzz_b200_convex_mesh_release.restype = None
+        L.fyzz_b200_cook_error.argtypes = []
+        L.fyzz_b200_cook_error.restype = C.c_char_p
+        L.fyzz_b200_convex_mesh_info.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.fyzz_b200_attach_convex_shape.argtypes = [vp, u32, vp, vp, P(u32)]
         L.fyzz_b200_step.argtypes = [vp, f32]
         L.fyzz_b200_step_n.argtypes = [vp, f32, u32]
         L.fyzz_b200_collide.argtypes = [vp]
@@ -232,6 +243,13 @@ class World:
         self._check(lib().fyzz_b200_attach_sphere_shape(self.h, body, radius, _p(l), C.byref(out)))
         return out.value
 
+    def attach_convex_shape(self, body: int, mesh: "ConvexMesh", local_pose=_IDENTITY) -> int:
+        """World::attach_convex_shape (reference world.h:412)."""
+        l = _f32(local_pose, 7)
+        out = C.c_uint32()
+        self._check(lib().fyzz_b200_attach_convex_shape(self.h, body, mesh.h, _p(l), C.byref(out)))
+        return out.value
+
     def update_mass_properties(self, body: int, density: float):
         self._check(lib().fyzz_b200_update_mass_properties(self.h, body, density))
 
@@ -293,11 +311,13 @@ class World:
         fm = np.asarray(spec.floor_mat, np.float32)
         out = C.c_uint32()
         kinds = spec.has_joint_kinds()
-        self._check(lib().fyzz_b200_add_scene(
+        meshes = [ConvexMesh(v, t) for (v, t) in getattr(spec, "convex_meshes", [])]
+        handles = (C.c_void_p * max(1, len(meshes)))(*[m.h for m in meshes])
+        self._check(lib().fyzz_b200_add_scene_ex(
             self.h, spec.n_bodies, _p(arrs[0]), spec.n_shapes, _p(arrs[1]), _p(arrs[2]),
             _p(arrs[3]), _p(arrs[4]), _p(arrs[5]), 0 if kinds else arrs[6].shape[0], _p(arrs[6]), _p(arrs[7]),
             0 if spec.floor is None else 1, 0.0 if spec.floor is None else float(spec.floor),
-            _p(fm), C.byref(out)))
+            _p(fm), len(meshes), handles, C.byref(out)))
         first = out.value
         if kinds:   # every joint in authoring order, each with its kind
             from .scenes import FLOOR_BODY
@@ -499,9 +519,10 @@ class World:
 
     def step_counters(self) -> dict:
         """Device counters of the last step (see fyzz_b200_read_step_counters)."""
-        out = np.zeros(16, np.uint32)
-        self._check(lib().fyzz_b200_read_step_counters(self.h, _p(out), 16))
+        out = np.zeros(17, np.uint32)
+        self._check(lib().fyzz_b200_read_step_counters(self.h, _p(out), 17))
         return {"managers": int(out[0]), "descriptors": int(out[1]), "gjk_pairs": int(out[5]),
+                "convex_pairs": int(out[16]),
                 "islands_32_512": int(out[8]), "islands_96_512": int(out[9]),
                 "islands_512_4096": int(out[10]), "islands_4096_up": int(out[11])}
 
@@ -509,3 +530,41 @@ class World:
         out = C.c_uint32()
         lib().fyzz_b200_error_bits(self.h, C.byref(out))
         return out.value
+
+
+class ConvexMesh:
+    """fyzz::cook_convex_mesh (reference include/fyzzxyzzy/convex.h:56-60):
+    a cooked, reference-counted convex hull.  Host code only; usable
+    without a GPU.  Raises ValueError for meshes the reference rejects."""
+
+    def __init__(self, vertices, triangles):
+        v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(triangles, np.uint32).reshape(-1, 3)
+        h = C.c_void_p()
+        rc = lib().fyzz_b200_cook_convex_mesh(_p(v), v.shape[0], _p(t), t.shape[0], C.byref(h))
+        if rc:
+            raise (ValueError if rc == 1 else RuntimeError)(lib().fyzz_b200_cook_error().decode())
+        self.h = h.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().fyzz_b200_convex_mesh_release(self.h)
+            self.h = None
+
+    def info(self) -> dict:
+        """Faces (n, 6: normal, distance, first, count), face indices,
+        volume, centre, inertia (3x3, columns), bounds lo / hi."""
+        counts = np.zeros(3, np.uint32)
+        self._info(counts, None, None, None, None)
+        faces = np.zeros((counts[1], 6), np.float32)
+        idx = np.zeros(counts[2], np.uint32)
+        vol = np.zeros(1, np.float64)
+        m = np.zeros(18, np.float32)
+        self._info(counts, faces, idx, vol, m)
+        return {"faces": faces, "idx": idx, "volume": float(vol[0]), "center": m[0:3],
+                "inertia": m[3:12].reshape(3, 3).T.copy(), "lo": m[12:15], "hi": m[15:18]}
+
+    def _info(self, counts, faces, idx, vol, m):
+        rc = lib().fyzz_b200_convex_mesh_info(self.h, _p(counts), _p(faces), _p(idx), _p(vol), _p(m))
+        if rc:
+            raise RuntimeError("invalid convex mesh handle")

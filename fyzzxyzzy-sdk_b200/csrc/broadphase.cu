@@ -46,16 +46,29 @@ __global__ void k_shape_bounds(DevState s) {
     const float4 g = s.s_geom[i];
     const v3 h = {g.x, g.y, g.z};
     v3 e = type == kSphere ? v3{g.w, g.w, g.w} : h;
+    v3 c = wp;
     if (type == kBox && (wq.x != 0.0f || wq.y != 0.0f || wq.z != 0.0f || wq.w != 1.0f)) {
         const v3 x = rot_sc(wq, {1, 0, 0}), y = rot_sc(wq, {0, 1, 0}), z = rot_sc(wq, {0, 0, 1});
         e = {fabsf(x.x) * h.x + fabsf(y.x) * h.y + fabsf(z.x) * h.z,
              fabsf(x.y) * h.x + fabsf(y.y) * h.y + fabsf(z.y) * h.z,
              fabsf(x.z) * h.x + fabsf(y.z) * h.y + fabsf(z.z) * h.z};
+    } else if (type == kConvex) {
+        // the rotated hull's vertex bounds, centred where the hull is
+        // (scene.cpp:1258-1298)
+        const uint4 mt = s.m_tab[s.s_mesh[i]];
+        v3 vlo = {INFINITY, INFINITY, INFINITY}, vhi = {-INFINITY, -INFINITY, -INFINITY};
+        for (uint32_t v = 0; v < mt.y; ++v) {
+            const v3 r = rot_sc(wq, ld3(s.hv[mt.x + v]));
+            vlo = {smin(vlo.x, r.x), smin(vlo.y, r.y), smin(vlo.z, r.z)};
+            vhi = {smax(vhi.x, r.x), smax(vhi.y, r.y), smax(vhi.z, r.z)};
+        }
+        c = {wp.x + (vhi.x + vlo.x) * 0.5f, wp.y + (vhi.y + vlo.y) * 0.5f, wp.z + (vhi.z + vlo.z) * 0.5f};
+        e = {(vhi.x - vlo.x) * 0.5f, (vhi.y - vlo.y) * 0.5f, (vhi.z - vlo.z) * 0.5f};
     }
     const float co = lp.w;
     e.x += co; e.y += co; e.z += co;
-    const float lo[3] = {wp.x - e.x, wp.y - e.y, wp.z - e.z};
-    const float hi[3] = {wp.x + e.x, wp.y + e.y, wp.z + e.z};
+    const float lo[3] = {c.x - e.x, c.y - e.y, c.z - e.z};
+    const float hi[3] = {c.x + e.x, c.y + e.y, c.z + e.z};
     if (!(isfinite(lo[0]) && isfinite(lo[1]) && isfinite(lo[2]) &&
           isfinite(hi[0]) && isfinite(hi[1]) && isfinite(hi[2])))
         atomicOr(s.err, kErrNonFinite);

@@ -14,7 +14,7 @@
 namespace fyzz::b200 {
 using std::isfinite;
 
-enum : uint32_t { kBox = 0, kSphere = 1, kPlane = 2 };
+enum : uint32_t { kBox = 0, kSphere = 1, kPlane = 2, kConvex = 3 };
 enum : uint32_t { kBodyDynamic = 1u, kBodyKinematic = 2u };
 // b_sleep bits.  A kinematic body also uses the last three: a target
 // waiting for the step (kKinPending, set on the host; cleared when the step

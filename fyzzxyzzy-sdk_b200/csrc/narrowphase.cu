@@ -308,18 +308,48 @@ __device__ void batch_selection(const Cand* c, int n, float tol, int sel[4]) {
 }
 
 // ---------------- GJK / EPA ----------------
+// The search is instantiated twice: G = false for box/box pairs, G = true
+// for pairs with a cooked hull, where a hull's support is its first vertex
+// of largest projection, a sphere is a point core (its radius applied after
+// the search), and facet admission and the witness tolerance scale with the
+// shapes (GuPCMGjkEpa.cpp:53-75, 201-218, 296-302, 411-516).
 struct Sup { v3 a, b, q; uint32_t ai, bi; };
-struct BPair { v3 ha, hb, a_in_b; qt rel; };
+struct BPair {
+    v3 ha, hb, a_in_b; qt rel;
+    const float4* va; uint32_t nva;    // hull vertices of A / B (G only)
+    const float4* vb; uint32_t nvb;
+    float ra, rb;                      // sphere point-core radii (G only)
+};
 __device__ __forceinline__ v3 box_vertex(v3 e, v3 d, uint32_t& idx) {
     const bool x = d.x > 0.f, y = d.y > 0.f, z = d.z > 0.f;
     idx = (x ? 1u : 0u) | (y ? 2u : 0u) | (z ? 4u : 0u);
     return {x ? e.x : -e.x, y ? e.y : -e.y, z ? e.z : -e.z};
 }
-__device__ Sup bp_support(const BPair& p, v3 dir) {
+__device__ __forceinline__ v3 shape_vertex(v3 e, v3 d, const float4* hull, uint32_t n, float radius,
+                                           uint32_t& idx) {
+    idx = 0;
+    if (radius > 0.f) return {0.f, 0.f, 0.f};
+    if (n) {
+        float best = vdot(ld3(hull[0]), d);
+        for (uint32_t i = 1; i < n; ++i) {
+            const float pr = vdot(ld3(hull[i]), d);
+            if (pr > best) { best = pr; idx = i; }
+        }
+        return ld3(hull[idx]);
+    }
+    return box_vertex(e, d, idx);
+}
+template <bool G> __device__ Sup bp_support(const BPair& p, v3 dir) {
     Sup s;
     const v3 da = rotinv_gu(p.rel, dir);
-    const v3 pa = box_vertex(p.ha, da, s.ai);
-    s.b = box_vertex(p.hb, vneg(dir), s.bi);
+    v3 pa;
+    if (G) {
+        pa = shape_vertex(p.ha, da, p.va, p.nva, p.ra, s.ai);
+        s.b = shape_vertex(p.hb, vneg(dir), p.vb, p.nvb, p.rb, s.bi);
+    } else {
+        pa = box_vertex(p.ha, da, s.ai);
+        s.b = box_vertex(p.hb, vneg(dir), s.bi);
+    }
     s.a = vadd(p.a_in_b, rot_gu(p.rel, pa));
     s.q = vsub(s.a, s.b);
     return s;
@@ -442,22 +472,24 @@ __device__ bool contact_from_gjk(const BPair& p, const Closest& n, Cand& out) {
     return true;
 }
 struct Facet { int i, j, k; v3 normal; float distance; bool valid, in_heap; };
-__device__ Facet make_facet(const Sup* vtx, int i, int j, int k) {
+template <bool G> __device__ Facet make_facet(const Sup* vtx, int i, int j, int k) {
     Facet f;
     f.i = f.j = f.k = 0; f.normal = {0, 0, 0}; f.distance = 0.0f; f.valid = false; f.in_heap = true;
     const v3 a = vtx[i].q, b = vtx[j].q, c = vtx[k].q;
     const v3 e0 = vsub(b, a), e1 = vsub(c, a);
     v3 n = vcross(e0, e1);
     const float norm2 = vlen2(n);
-    if (!(norm2 > FLT_EPSILON)) return f;
+    float min_area = FLT_EPSILON;
+    if (G) min_area *= vlen2(e0) * vlen2(e1);
+    if (!(norm2 > min_area)) return f;
     n = vmul(n, 1.0f / sqrtf(norm2));
     f.i = i; f.j = j; f.k = k; f.normal = n; f.distance = vdot(n, a); f.valid = true;
     return f;
 }
-__device__ bool init_epa(const BPair& p, Sup* vtx, int& count, Facet* facets, int& fc) {
+template <bool G> __device__ bool init_epa(const BPair& p, Sup* vtx, int& count, Facet* facets, int& fc) {
     if (count <= 0 || count > 4) return false;
     if (count == 1) {
-        const Sup nx = bp_support(p, {1, 0, 0});
+        const Sup nx = bp_support<G>(p, {1, 0, 0});
         if (vlen2(vsub(nx.q, vtx[0].q)) == 0.0f) return false;
         vtx[count++] = nx;
     }
@@ -471,10 +503,10 @@ __device__ bool init_epa(const BPair& p, Sup* vtx, int& count, Facet* facets, in
         const float sq = vlen2(perp);
         if (!(sq > 0.0f)) return false;
         perp = vmul(perp, 1.0f / sqrtf(sq));
-        vtx[count++] = bp_support(p, perp);
+        vtx[count++] = bp_support<G>(p, perp);
     }
     if (count == 3) {
-        const Facet f0 = make_facet(vtx, 0, 1, 2), f1 = make_facet(vtx, 1, 0, 2);
+        const Facet f0 = make_facet<G>(vtx, 0, 1, 2), f1 = make_facet<G>(vtx, 1, 0, 2);
         if (!f0.valid || !f1.valid) return false;
         facets[fc++] = f0;
         facets[fc++] = f1;
@@ -487,13 +519,13 @@ __device__ bool init_epa(const BPair& p, Sup* vtx, int& count, Facet* facets, in
     }
     const int faces[4][3] = {{0, 1, 2}, {0, 3, 1}, {0, 2, 3}, {1, 3, 2}};
     for (int i = 0; i < 4; ++i) {
-        const Facet f = make_facet(vtx, faces[i][0], faces[i][1], faces[i][2]);
+        const Facet f = make_facet<G>(vtx, faces[i][0], faces[i][1], faces[i][2]);
         if (!f.valid) return false;
         facets[fc++] = f;
     }
     return true;
 }
-__device__ bool contact_from_facet(const BPair& p, const Sup* vtx, const Facet& f, Cand& out) {
+template <bool G> __device__ bool contact_from_facet(const BPair& p, const Sup* vtx, const Facet& f, Cand& out) {
     const Sup& P = vtx[f.i];
     const Sup& Qv = vtx[f.j];
     const Sup& R = vtx[f.k];
@@ -510,25 +542,30 @@ __device__ bool contact_from_facet(const BPair& p, const Sup* vtx, const Facet& 
     if (!isfinite(pa.x) || !isfinite(pb.x) || !isfinite(f.distance)) return false;
     const float depth = fabsf(f.distance);
     out = {bp_local_a(p, pa), pb, vneg(f.normal), -depth};
-    return sqrtf(vlen2(vsub(pa, pb))) <= depth + 1.0e-3f;
+    float tol = 1.0e-3f;
+    if (G) tol *= smax(smax(smax(p.ha.x, p.ha.y), smax(p.ha.z, p.hb.x)), smax(p.hb.y, p.hb.z));
+    return sqrtf(vlen2(vsub(pa, pb))) <= depth + tol;
 }
 // GJK (GuPCMGjkEpa.cpp) up to the point where EPA starts: returns 0 (no
 // witness), 1 (witness in out) or 2 (EPA needed from simplex[0, sc)).  The
 // whole warp runs it in step on the same pair (every lane holds the same
 // simplex; the sub-simplex search is spread over the lanes), so every lane
 // returns the same mode, witness and simplex.
-__device__ int gjk_phase(const BPair& p, float cd, Cand& out, Sup* simplex, int& count) {
+// A sphere point core (G only) converges its separated distance before EPA
+// is admitted and falls back to EPA where the polyhedral search gives up.
+template <bool G> __device__ int gjk_phase(const BPair& p, float cd, Cand& out, Sup* simplex, int& count) {
     const float eps = 0.1f * smin(box_min_margin(p.ha), box_min_margin(p.hb));
     const float progress = 1.0f - 0.000225f;
+    const bool pc = G && (p.ra > 0.f || p.rb > 0.f);
     count = 0;
     v3 closest = vlen2(p.a_in_b) > 0.0f ? p.a_in_b : v3{1, 0, 0};
     float previous = FLT_MAX;
     for (int it = 0; it < 32; ++it) {
         const float dist = sqrtf(vlen2(closest));
-        if (count > 0 && dist <= eps) return 2;
-        if (dist <= 0.0f) return 0;
+        if (count > 0 && dist <= eps && !pc) return 2;
+        if (dist <= 0.0f) return pc && count > 0 ? 2 : 0;
         const v3 normal = vmul(closest, 1.0f / dist);
-        const Sup s = bp_support(p, vneg(closest));
+        const Sup s = bp_support<G>(p, vneg(closest));
         const float proj = vdot(normal, s.q);
         if (proj > cd) return 0;
         if (count > 0 && proj > dist * progress) {
@@ -541,7 +578,7 @@ __device__ int gjk_phase(const BPair& p, float cd, Cand& out, Sup* simplex, int&
                     const Closest cur = closest_simplex_warp(simplex, count);
                     return cur.mask && contact_from_gjk(p, cur, out) && out.sep <= cd ? 1 : 0;
                 }
-                return 0;
+                return pc ? 2 : 0;
             }
         if (count == 4) return 2;
         simplex[count++] = s;
@@ -550,10 +587,13 @@ __device__ int gjk_phase(const BPair& p, float cd, Cand& out, Sup* simplex, int&
         closest = nx.point;
         const float nd = sqrtf(nx.dist2);
         compact_simplex(simplex, count, nx);
-        if (nd >= previous) return 0;
+        if (nd >= previous) {
+            if (pc) return proj > 0.f ? (contact_from_gjk(p, nx, out) ? 1 : 0) : 2;
+            return 0;
+        }
         previous = nd;
     }
-    return 0;
+    return pc && count > 0 ? 2 : 0;
 }
 
 // EPA (GuPCMGjkEpa.cpp) with one warp: the polytope lives in shared memory; the closest
@@ -569,14 +609,14 @@ struct EpaShared {
     int bc;
     int status;
 };
-__device__ bool run_epa_warp(const BPair& p, const Sup* simplex, int sc, Cand& out, EpaShared& E) {
+template <bool G> __device__ bool run_epa_warp(const BPair& p, const Sup* simplex, int sc, Cand& out, EpaShared& E) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t full = 0xffffffffu;
     if (lane == 0) {
         int vc0 = sc;
         for (int i = 0; i < sc; ++i) E.vtx[i] = simplex[i];
         int fc0 = 0;
-        E.status = init_epa(p, E.vtx, vc0, E.facets, fc0) ? fc0 : -1;
+        E.status = init_epa<G>(p, E.vtx, vc0, E.facets, fc0) ? fc0 : -1;
         E.bc = vc0;
     }
     __syncwarp();
@@ -600,14 +640,14 @@ __device__ bool run_epa_warp(const BPair& p, const Sup* simplex, int sc, Cand& o
         }
         if (closest < 0) return false;
         const Facet sel = E.facets[closest];
-        const Sup np = bp_support(p, sel.normal);
+        const Sup np = bp_support<G>(p, sel.normal);
         const float proj = vdot(np.q, sel.normal);
-        if (fabsf(proj - dist) <= eps) return contact_from_facet(p, E.vtx, sel, out);
+        if (fabsf(proj - dist) <= eps) return contact_from_facet<G>(p, E.vtx, sel, out);
         if (vc == 64) return false;
         upper = smin(upper, proj);
         bool dup = false;
         for (int i = int(lane); i < vc; i += 32) dup |= E.vtx[i].ai == np.ai && E.vtx[i].bi == np.bi;
-        if (__any_sync(full, dup)) return contact_from_facet(p, E.vtx, sel, out);
+        if (__any_sync(full, dup)) return contact_from_facet<G>(p, E.vtx, sel, out);
         const int ni = vc++;
         // visibility (independent per facet)
         bool vis0 = false, vis1 = false;
@@ -668,7 +708,7 @@ __device__ bool run_epa_warp(const BPair& p, const Sup* simplex, int sc, Cand& o
         bool ok = true;
         int slot = -1;
         if (int(lane) < bc) {
-            nf = make_facet(E.vtx, E.bfrom[lane], E.bto[lane], ni);
+            nf = make_facet<G>(E.vtx, E.bfrom[lane], E.bto[lane], ni);
             ok = nf.valid;
             nf.in_heap = nf.distance <= upper;
             const int k = int(lane);
@@ -1105,7 +1145,7 @@ __device__ int sphere_box(v3 center, float r, v3 h, v3 bc, qt bq, float cd, Cont
 // ScNPhaseCore::shouldSwapBodies orientation (scene.cpp:3275-3283).
 struct PairShapes {
     uint32_t sa, sb, ta, tb, first, second;
-    bool plane, sphere;
+    bool plane, sphere, convex;
     float cd;
 };
 __device__ __forceinline__ PairShapes pair_shapes(const DevState& s, uint64_t key) {
@@ -1118,7 +1158,10 @@ __device__ __forceinline__ PairShapes pair_shapes(const DevState& s, uint64_t ke
     const bool da = s.b_flags[ba] & kBodyDynamic, db = s.b_flags[bb] & kBodyDynamic;
     const bool reversed = !da || (da && db && ba < bb);
     p.plane = p.ta == kPlane || p.tb == kPlane;
-    p.sphere = p.ta == kSphere || p.tb == kSphere;
+    // a pair with a cooked hull takes the convex generators whatever the
+    // other shape is (scene.cpp:4307-4317)
+    p.convex = p.ta == kConvex || p.tb == kConvex;
+    p.sphere = !p.convex && (p.ta == kSphere || p.tb == kSphere);
     p.first = p.plane ? (p.ta == kPlane ? p.sa : p.sb) : (reversed ? p.sb : p.sa);
     p.second = p.plane ? (p.ta == kPlane ? p.sb : p.sa) : (reversed ? p.sa : p.sb);
     p.cd = s.s_lp[p.sa].w + s.s_lp[p.sb].w;
@@ -1134,6 +1177,14 @@ __global__ void __launch_bounds__(128) k_narrowphase(DevState s) {
         if (pj >= 0) cache = s.prev.cache[pj];
         else cache.meta = 0u;
         const PairShapes ps = pair_shapes(s, s.cur.key[k]);
+        if (ps.convex) {
+            // carried forward here, generated by k_narrowphase_convex
+            s.cur.cache[k] = cache;
+            if (pj >= 0) s.cur.fric[k] = s.prev.fric[pj];
+            else s.cur.fric[k].epoch = 0u;
+            s.cvx_list[atomicAdd(&s.counters[kCntConvex], 1u)] = k;
+            continue;
+        }
         const uint32_t sa = ps.sa, sb = ps.sb, ta = ps.ta, tb = ps.tb, first = ps.first, second = ps.second;
         const bool plane = ps.plane, sphere = ps.sphere;
         const float cd = ps.cd;
@@ -1198,7 +1249,7 @@ __global__ void __launch_bounds__(kGjkWarps * 32, 1) k_narrowphase_gjk(DevState 
         const v3 h0 = {g0.x, g0.y, g0.z}, h1 = {g1.x, g1.y, g1.z};
         const v3 p0 = ld3(s.s_wp[ps.first]), p1 = ld3(s.s_wp[ps.second]);
         const qt q0 = ldq(s.s_wq[ps.first]), q1 = ldq(s.s_wq[ps.second]);
-        BPair bp;
+        BPair bp = {};
         bp.ha = h0;
         bp.hb = h1;
         bp.a_in_b = rotinv_gu(q1, vsub(p0, p1));
@@ -1206,14 +1257,470 @@ __global__ void __launch_bounds__(kGjkWarps * 32, 1) k_narrowphase_gjk(DevState 
         Cand w = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0.0f};
         Sup simplex[4];
         int sc = 0;
-        const int mode = gjk_phase(bp, ps.cd, w, simplex, sc);
+        const int mode = gjk_phase<false>(bp, ps.cd, w, simplex, sc);
         bool have = mode == 1;
-        if (mode == 2) have = run_epa_warp(bp, simplex, sc, w, epa[wib]);
+        if (mode == 2) have = run_epa_warp<false>(bp, simplex, sc, w, epa[wib]);
         if (lane == 0) {
             have = have && w.sep <= ps.cd;
             PcmCache cache = s.cur.cache[k];
             ContactPt out[4];
             int count = finish_box_box_gjk(h0, h1, p1, q1, ps.cd, cache, have, w, out);
+            if (count < 0) {
+                atomicOr(s.err, kErrContactOverflow);
+                count = 0;
+            }
+            s.cur.cache[k] = cache;
+            s.cur.count[k] = uint32_t(count);
+            for (int j = 0; j < count; ++j) s.pts[4 * size_t(k) + j] = out[j];
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------- cooked convex hulls ----------------
+// A finite shape as the convex generators see it (the PcmFiniteShape of
+// scene.cpp:3712-3731 plus the attached shape's half extents, which the
+// rotation travel test uses).
+struct Fin {
+    v3 half;            // box: half extents; sphere: radius; hull: half bound size
+    v3 shalf;           // attached half extents (zero for spheres)
+    v3 p;
+    qt q;
+    float radius;       // sphere radius, else 0
+    float extent;       // margin extent (scene.cpp:3666-3677)
+    uint32_t vo, nv, fo, nf;
+};
+__device__ Fin load_fin(const DevState& s, uint32_t sh) {
+    Fin f;
+    const uint32_t t = s.s_type[sh];
+    const float4 g = s.s_geom[sh];
+    f.p = ld3(s.s_wp[sh]);
+    f.q = ldq(s.s_wq[sh]);
+    f.radius = 0.f;
+    f.vo = f.nv = f.fo = f.nf = 0;
+    f.shalf = {g.x, g.y, g.z};
+    if (t == kConvex) {
+        const uint32_t m = s.s_mesh[sh];
+        const uint4 mt = s.m_tab[m];
+        const float4 mh = s.m_half[m];
+        f.half = {mh.x, mh.y, mh.z};
+        f.extent = mh.w;
+        f.vo = mt.x; f.nv = mt.y; f.fo = mt.z; f.nf = mt.w;
+    } else if (t == kSphere) {
+        f.radius = g.w;
+        f.half = {g.w, g.w, g.w};
+        f.extent = g.w;
+        f.shalf = {0.f, 0.f, 0.f};
+    } else {
+        f.half = {g.x, g.y, g.z};
+        f.extent = smin(smin(g.x, g.y), g.z);
+    }
+    return f;
+}
+
+// Face geometry for the clipping of GuPCMGjkEpa.cpp:571-804: a hull's planar
+// polygons or the six faces of a box, in the shape's frame.
+__device__ __forceinline__ unsigned fc_count(const Fin& f) { return f.nv ? f.nf : 6u; }
+__device__ __forceinline__ v3 fc_axis(unsigned i) { return i == 0 ? v3{1, 0, 0} : i == 1 ? v3{0, 1, 0} : v3{0, 0, 1}; }
+__device__ __forceinline__ v3 fc_normal(const DevState& s, const Fin& f, unsigned k) {
+    if (f.nv) return ld3(s.hf[f.fo + k]);
+    return vmul(fc_axis(k / 2u), (k & 1u) ? 1.f : -1.f);
+}
+__device__ __forceinline__ unsigned fc_nvert(const DevState& s, const Fin& f, unsigned k) {
+    return f.nv ? s.hfr[f.fo + k].y : 4u;
+}
+__device__ v3 fc_vertex_local(const DevState& s, const Fin& f, unsigned k, unsigned o) {
+    if (f.nv) return ld3(s.hv[f.vo + s.hidx[s.hfr[f.fo + k].x + o]]);
+    const float cu = (o == 0 || o == 3) ? 1.f : -1.f;
+    const float cv = (o < 2) ? 1.f : -1.f;
+    const v3 n = fc_normal(s, f, k);
+    const unsigned c = k / 2u;
+    const v3 u = fc_axis((c + 1u) % 3u);
+    const v3 v = vcross(n, u);
+    const float hu = vcomp(f.half, (c + 1u) % 3u), hv = vcomp(f.half, (c + 2u) % 3u);
+    return vadd(vmul(n, vcomp(f.half, c)), vadd(vmul(u, cu * hu), vmul(v, cv * hv)));
+}
+struct Clip {
+    const DevState* s;
+    const Fin *a, *b, *ref, *inc;
+    bool ref_is_a, inc_is_a, reference_b;
+    unsigned rf, inf, nr, ni;
+    v3 rn, anchor;
+    float cd, tol_sq;
+    Cand* out;
+    unsigned count;
+};
+__device__ __forceinline__ v3 clip_to_b(const Clip& k, v3 p) {
+    return rotinv_gu(k.b->q, vsub(vadd(k.a->p, rot_gu(k.a->q, p)), k.b->p));
+}
+__device__ __forceinline__ v3 clip_vertex(const Clip& k, const Fin& f, bool is_a, unsigned face, unsigned o) {
+    const v3 l = fc_vertex_local(*k.s, f, face, o);
+    return is_a ? clip_to_b(k, l) : l;
+}
+__device__ __forceinline__ v3 clip_normal(const Clip& k, const Fin& f, bool is_a, unsigned face) {
+    const v3 n = fc_normal(*k.s, f, face);
+    return is_a ? rotinv_gu(k.b->q, rot_gu(k.a->q, n)) : n;
+}
+__device__ __forceinline__ v3 clip_r(const Clip& k, unsigned i) { return clip_vertex(k, *k.ref, k.ref_is_a, k.rf, i % k.nr); }
+__device__ __forceinline__ v3 clip_q(const Clip& k, unsigned i) { return clip_vertex(k, *k.inc, k.inc_is_a, k.inf, i % k.ni); }
+__device__ __forceinline__ float clip_cross(const Clip& k, v3 a, v3 b) { return vdot(k.rn, vcross(a, b)); }
+// One clipped point: projected onto the reference plane, merged with a
+// nearby one (keeping the deeper), or reduced greedily to four.
+__device__ void clip_emit(Clip& k, v3 ip) {
+    const float sep = vdot(k.rn, vsub(ip, k.anchor));
+    if (!isfinite(sep) || sep > k.cd) return;
+    const v3 proj = vsub(ip, vmul(k.rn, sep));
+    const v3 a = k.reference_b ? ip : proj;
+    const v3 b = k.reference_b ? proj : ip;
+    const v3 al = rotinv_gu(k.a->q, vsub(vadd(k.b->p, rot_gu(k.b->q, a)), k.a->p));
+    const Cand c = {al, b, k.reference_b ? k.rn : vneg(k.rn), sep};
+    if (!isfinite(al.x) || !isfinite(b.x)) return;
+    for (unsigned i = 0; i < k.count; ++i)
+        if (vlen2(vsub(k.out[i].lb, c.lb)) <= k.tol_sq) {
+            if (c.sep < k.out[i].sep) k.out[i] = c;
+            return;
+        }
+    if (k.count < 4u) {
+        k.out[k.count++] = c;
+        return;
+    }
+    Cand ch[5] = {k.out[0], k.out[1], k.out[2], k.out[3], c};
+    unsigned deepest = 0;
+    for (unsigned i = 1; i < 5; ++i)
+        if (ch[i].sep < ch[deepest].sep) deepest = i;
+    float best = -1.f;
+    unsigned omit = 4;
+    for (unsigned ex = 0; ex < 5; ++ex) {
+        if (ex == deepest) continue;
+        float score = 0.f;
+        for (unsigned i = 0; i < 5; ++i) {
+            if (i == ex) continue;
+            for (unsigned j = i + 1; j < 5; ++j)
+                if (j != ex) score += vlen2(vsub(ch[i].lb, ch[j].lb));
+        }
+        if (score > best) { best = score; omit = ex; }
+    }
+    if (omit != 4u) k.out[omit] = c;
+}
+// GuPCMGjkEpa.cpp:571-804: reference and incident faces most aligned with
+// the witness normal, incident vertices inside the reference polygon,
+// reference vertices inside the incident one, and edge crossings.
+__device__ int face_contacts(const DevState& s, const Fin& a, const Fin& b, float cd, const Cand& w, Cand out[4]) {
+    if (a.radius > 0.f || b.radius > 0.f || (a.nv && !a.nf) || (b.nv && !b.nf)) return 0;
+    Clip k;
+    k.s = &s; k.a = &a; k.b = &b;
+    const v3 normal = w.nb;
+    if (!(vlen2(normal) > 0.f)) return 0;
+    unsigned fa = 0, fb = 0;
+    float ala = -2.f, alb = -2.f;
+    for (unsigned i = 0; i < fc_count(a); ++i) {
+        const float d = vdot(vneg(normal), clip_normal(k, a, true, i));
+        if (d > ala) { ala = d; fa = i; }
+    }
+    for (unsigned i = 0; i < fc_count(b); ++i) {
+        const float d = vdot(normal, clip_normal(k, b, false, i));
+        if (d > alb) { alb = d; fb = i; }
+    }
+    k.reference_b = alb >= ala;
+    if (smax(ala, alb) < 0.95f) return 0;
+    k.ref = k.reference_b ? &b : &a;
+    k.inc = k.reference_b ? &a : &b;
+    k.ref_is_a = !k.reference_b;
+    k.inc_is_a = k.reference_b;
+    k.rf = k.reference_b ? fb : fa;
+    k.rn = clip_normal(k, *k.ref, k.ref_is_a, k.rf);
+    float ial = -2.f;
+    k.inf = 0;
+    for (unsigned i = 0; i < fc_count(*k.inc); ++i) {
+        const float d = vdot(vneg(k.rn), clip_normal(k, *k.inc, k.inc_is_a, i));
+        if (d > ial) { ial = d; k.inf = i; }
+    }
+    const v3 in_n = clip_normal(k, *k.inc, k.inc_is_a, k.inf);
+    const float den = vdot(in_n, k.rn);
+    if (!(den < -0.25f)) return 0;
+    k.nr = fc_nvert(s, *k.ref, k.rf);
+    k.ni = fc_nvert(s, *k.inc, k.inf);
+    if (k.nr < 3u || k.ni < 3u) return 0;
+    k.anchor = clip_r(k, 0);
+    const v3 in_anchor = clip_q(k, 0);
+    float el = 0.f;
+    for (unsigned i = 0; i < k.nr; ++i) el = smax(el, vlen2(vsub(clip_r(k, i + 1), clip_r(k, i))));
+    for (unsigned i = 0; i < k.ni; ++i) el = smax(el, vlen2(vsub(clip_q(k, i + 1), clip_q(k, i))));
+    const float scale = sqrtf(el);
+    if (!(scale > 0.f) || !isfinite(scale)) return 0;
+    const float tol = smax(scale * 1.e-5f, 1.e-6f);
+    const float ftol = tol / scale;
+    k.tol_sq = tol * tol;
+    k.cd = cd;
+    k.out = out;
+    k.count = 0;
+    for (unsigned i = 0; i < k.ni; ++i) {
+        const v3 v = clip_q(k, i);
+        bool inside = true;
+        for (unsigned j = 0; j < k.nr && inside; ++j)
+            if (clip_cross(k, vsub(clip_r(k, j + 1), clip_r(k, j)), vsub(v, clip_r(k, j))) < -tol * scale) inside = false;
+        if (inside) clip_emit(k, v);
+    }
+    for (unsigned i = 0; i < k.nr; ++i) {
+        const v3 v = clip_r(k, i);
+        bool inside = true;
+        for (unsigned j = 0; j < k.ni && inside; ++j)
+            if (clip_cross(k, vsub(clip_q(k, j + 1), clip_q(k, j)), vsub(v, clip_q(k, j))) > tol * scale) inside = false;
+        if (!inside) continue;
+        const float height = vdot(in_n, vsub(in_anchor, v)) / den;
+        if (isfinite(height)) clip_emit(k, vadd(v, vmul(k.rn, height)));
+    }
+    for (unsigned i = 0; i < k.ni; ++i) {
+        const v3 qa = clip_q(k, i), e = vsub(clip_q(k, i + 1), qa);
+        for (unsigned j = 0; j < k.nr; ++j) {
+            const v3 rb = clip_r(k, j), f = vsub(clip_r(k, j + 1), rb);
+            const float det = clip_cross(k, e, f);
+            if (fabsf(det) <= k.tol_sq) continue;
+            const v3 d = vsub(rb, qa);
+            const float t = clip_cross(k, d, f) / det;
+            const float u = clip_cross(k, d, e) / det;
+            if (t >= -ftol && t <= 1.f + ftol && u >= -ftol && u <= 1.f + ftol)
+                clip_emit(k, vadd(qa, vmul(e, sclamp(t, 0.f, 1.f))));
+        }
+    }
+    return int(k.count);
+}
+
+// Hull vertices against the floor plane (scene.cpp:3774-3972): candidates
+// are the vertices below the contact distance in vertex order; more than
+// four are reduced to the deepest, the farthest from it, the two sideways
+// extremes and the deepest of each cluster around those.  Candidates are
+// recomputed from their vertex on every pass instead of being stored.
+__device__ __forceinline__ bool plane_cand(const DevState& s, uint32_t vo, uint32_t v, v3 rel, qt q, float cd,
+                                           Cand& c) {
+    const v3 local = ld3(s.hv[vo + v]);
+    const v3 r = rot_sc(q, local);
+    const v3 ip = {rel.x + r.x, rel.y + r.y, rel.z + r.z};
+    if (ip.y >= cd) return false;
+    c = {local, {ip.x, 0.0f, ip.z}, {0.0f, 1.0f, 0.0f}, ip.y};
+    return true;
+}
+__device__ int plane_hull(const DevState& s, const PairShapes& ps, PcmCache& cache, ContactPt* out) {
+    const v3 pp = ld3(s.s_wp[ps.first]);
+    const uint32_t sh = ps.second;
+    const float4 g = s.s_geom[sh];
+    const v3 bp = ld3(s.s_wp[sh]);
+    const qt q = ldq(s.s_wq[sh]);
+    const uint4 mt = s.m_tab[s.s_mesh[sh]];
+    const float cd = ps.cd;
+    const v3 rel = {bp.x - pp.x, bp.y - pp.y, bp.z - pp.z};
+    const float brk = pcm_box_margin({g.x, g.y, g.z}) * 0.2f;
+    const uint32_t prev = cache_count(cache);
+    refresh_points(cache, rel, q, brk);
+    const bool init = cache_init(cache);
+    float md = INFINITY;
+    if (init)
+        md = smax(smax(fabsf(rel.x - cache.rel_p[0]), fabsf(rel.y - cache.rel_p[1])), fabsf(rel.z - cache.rel_p[2]));
+    const float rd = q.x * cache.rel_q[0] + q.y * cache.rel_q[1] + q.z * cache.rel_q[2] + q.w * cache.rel_q[3];
+    if (!init || cache_count(cache) != prev || md > brk || rd < 0.99996f) {
+        sv(cache.rel_p, rel);
+        cache.rel_q[0] = q.x; cache.rel_q[1] = q.y; cache.rel_q[2] = q.z; cache.rel_q[3] = q.w;
+        Cand c;
+        uint32_t n = 0, i0 = 0, first = 0;
+        float fsep = 0.f;
+        for (uint32_t v = 0; v < mt.y; ++v) {
+            if (!plane_cand(s, mt.x, v, rel, q, cd, c)) continue;
+            if (n == 0 || c.sep < fsep) { first = v; fsep = c.sep; }
+            if (n == 0) i0 = v;
+            if (n < 4) cache.pts[n] = to_pt(c);
+            ++n;
+        }
+        if (n <= 4) {
+            set_meta(cache, n, true);
+        } else {
+            uint32_t idx[4];
+            int nch = 0;
+            const auto chosen = [&](uint32_t v) {
+                for (int j = 0; j < nch; ++j)
+                    if (idx[j] == v) return true;
+                return false;
+            };
+            Cand cf, cv;
+            plane_cand(s, mt.x, first, rel, q, cd, cf);
+            idx[nch++] = first;
+            uint32_t far = i0;
+            plane_cand(s, mt.x, i0, rel, q, cd, cv);
+            float maxd = vlen2(vsub(cv.lb, cf.lb));
+            for (uint32_t v = i0 + 1; v < mt.y; ++v) {
+                if (!plane_cand(s, mt.x, v, rel, q, cd, cv)) continue;
+                const float d = vlen2(vsub(cv.lb, cf.lb));
+                if (d > maxd) { maxd = d; far = v; }
+            }
+            idx[nch++] = far;
+            Cand cfar;
+            plane_cand(s, mt.x, far, rel, q, cd, cfar);
+            const v3 seg = vsub(cfar.lb, cf.lb);
+            v3 side = {-seg.z, 0.0f, seg.x};
+            const float ns = vlen2(side);
+            if (ns > 0.0f) {
+                const float inv = 1.0f / sqrtf(ns);
+                side = {side.x * inv, 0.0f, side.z * inv};
+            } else {
+                side = {0.0f, 1.0f, 0.0f};
+            }
+            float largest = -FLT_MAX, smallest = FLT_MAX;
+            uint32_t third = i0, fourth = i0;
+            for (uint32_t v = 0; v < mt.y; ++v) {
+                if (!plane_cand(s, mt.x, v, rel, q, cd, cv) || chosen(v)) continue;
+                const float d = vdot(vsub(cv.lb, cf.lb), side);
+                if (d > largest) { largest = d; third = v; }
+                if (d < smallest) { smallest = d; fourth = v; }
+            }
+            idx[nch++] = third;
+            if (smallest * largest > 0.0f) {
+                largest = -FLT_MAX;
+                for (uint32_t v = 0; v < mt.y; ++v) {
+                    if (!plane_cand(s, mt.x, v, rel, q, cd, cv) || chosen(v)) continue;
+                    const float d = vdot(vsub(cv.lb, cf.lb), side);
+                    if (d > largest) { largest = d; fourth = v; }
+                }
+            }
+            idx[nch++] = fourth;
+            v3 centre[4];
+            float cur_sep[4];
+            for (int j = 0; j < 4; ++j) {
+                plane_cand(s, mt.x, idx[j], rel, q, cd, cv);
+                centre[j] = cv.lb;
+                cur_sep[j] = cv.sep;
+            }
+            uint32_t best[4] = {idx[0], idx[1], idx[2], idx[3]};
+            for (uint32_t v = 0; v < mt.y; ++v) {
+                if (!plane_cand(s, mt.x, v, rel, q, cd, cv) || chosen(v)) continue;
+                float nearest = FLT_MAX;
+                int slot = 0;
+                for (int j = 0; j < 4; ++j) {
+                    const float d = vlen2(vsub(cv.lb, centre[j]));
+                    if (d < nearest) { nearest = d; slot = j; }
+                }
+                if (cv.sep < cur_sep[slot]) { best[slot] = v; cur_sep[slot] = cv.sep; }
+            }
+            for (int j = 0; j < 4; ++j) {
+                plane_cand(s, mt.x, best[j], rel, q, cd, cv);
+                cache.pts[j] = to_pt(cv);
+            }
+            set_meta(cache, 4, true);
+        }
+    }
+    int emitted = 0;
+    const uint32_t n = cache_count(cache);
+    for (uint32_t k = 0; k < n; ++k) {
+        const PcmPoint& pt = cache.pts[k];
+        if (pt.sep > cd) continue;
+        ContactPt& o = out[emitted++];
+        o.p[0] = pp.x + pt.lb[0]; o.p[1] = pp.y; o.p[2] = pp.z + pt.lb[2];
+        o.n[0] = 0.0f; o.n[1] = 1.0f; o.n[2] = 0.0f;
+        o.sep = pt.sep;
+    }
+    return emitted;
+}
+
+// Pairs with a cooked hull (scene.cpp:3655-3772, 3774-3972).  One warp takes
+// a pair: plane pairs run on lane 0; finite pairs decide refresh and
+// regeneration in step on every lane, run GJK/EPA together (hull supports
+// are each lane's own scan of the vertices) and clip faces on lane 0.
+constexpr int kCvxWarps = 4;
+__global__ void __launch_bounds__(kCvxWarps * 32, 1) k_narrowphase_convex(DevState s) {
+    __shared__ EpaShared epa[kCvxWarps];
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    const uint32_t n = s.counters[kCntConvex];
+    const uint32_t nwarps = gridDim.x * kCvxWarps;
+    for (uint32_t i = blockIdx.x * kCvxWarps + wib; i < n; i += nwarps) {
+        const uint32_t k = s.cvx_list[i];
+        const PairShapes ps = pair_shapes(s, s.cur.key[k]);
+        PcmCache cache = s.cur.cache[k];
+        ContactPt out[4];
+        int count = 0;
+        if (ps.plane) {
+            if (lane == 0) count = plane_hull(s, ps, cache, out);
+        } else {
+            const Fin f0 = load_fin(s, ps.first), f1 = load_fin(s, ps.second);
+            const float cd = ps.cd;
+            const v3 delta = {f0.p.x - f1.p.x, f0.p.y - f1.p.y, f0.p.z - f1.p.z};
+            const v3 relative = rotinv_sc(f1.q, delta);
+            const qt rotation = qmul(qconj(f1.q), f0.q);
+            const float mm = smin(smin(0.15f * f0.extent, 0.15f), smin(0.15f * f1.extent, 0.15f));
+            const uint32_t prev = cache_count(cache);
+            refresh_points(cache, relative, rotation, mm * 0.8f);
+            const bool init = cache_init(cache);
+            const float tr = init ? smax(smax(fabsf(relative.x - cache.rel_p[0]), fabsf(relative.y - cache.rel_p[1])),
+                                         fabsf(relative.z - cache.rel_p[2]))
+                                  : INFINITY;
+            const float qa = qdot(f0.q, {cache.qa[0], cache.qa[1], cache.qa[2], cache.qa[3]});
+            const float qb = qdot(f1.q, {cache.qb[0], cache.qb[1], cache.qb[2], cache.qb[3]});
+            const float thr = mm * (cache_count(cache) == 0 ? 0.5f : 0.125f);
+            bool regen = !init || cache_count(cache) != prev || tr > thr || qa < 0.9999f || qb < 0.9999f;
+            if (!regen) {
+                const v3 ha = f0.shalf, hb = f1.shalf;
+                const float ta = (qa < 1.f ? acosf(smax(-1.f, qa)) : 0.f) * sqrtf(ha.x * ha.x + ha.y * ha.y + ha.z * ha.z);
+                const float tb = (qb < 1.f ? acosf(smax(-1.f, qb)) : 0.f) * sqrtf(hb.x * hb.x + hb.y * hb.y + hb.z * hb.z);
+                regen = ta > thr || tb > thr;
+            }
+            if (regen) {
+                sv(cache.rel_p, relative);
+                cache.rel_q[0] = rotation.x; cache.rel_q[1] = rotation.y; cache.rel_q[2] = rotation.z; cache.rel_q[3] = rotation.w;
+                cache.qa[0] = f0.q.x; cache.qa[1] = f0.q.y; cache.qa[2] = f0.q.z; cache.qa[3] = f0.q.w;
+                cache.qb[0] = f1.q.x; cache.qb[1] = f1.q.y; cache.qb[2] = f1.q.z; cache.qb[3] = f1.q.w;
+                set_meta(cache, 0, true);
+                BPair bp;
+                bp.ha = f0.half;
+                bp.hb = f1.half;
+                bp.a_in_b = rotinv_gu(f1.q, vsub(f0.p, f1.p));
+                bp.rel = qmul(qconj(f1.q), f0.q);
+                bp.va = s.hv + f0.vo; bp.nva = f0.nv;
+                bp.vb = s.hv + f1.vo; bp.nvb = f1.nv;
+                bp.ra = f0.radius; bp.rb = f1.radius;
+                Cand w = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0.0f};
+                Sup simplex[4];
+                int sc = 0;
+                const int mode = gjk_phase<true>(bp, cd + f0.radius + f1.radius, w, simplex, sc);
+                bool have = mode == 1;
+                if (mode == 2) have = run_epa_warp<true>(bp, simplex, sc, w, epa[wib]);
+                if (lane == 0 && have) {
+                    // sphere radii applied along the final normal
+                    if (f0.radius > 0.f) {
+                        w.la = vadd(w.la, rotinv_gu(bp.rel, vmul(w.nb, -f0.radius)));
+                        w.sep -= f0.radius;
+                    }
+                    if (f1.radius > 0.f) {
+                        w.lb = vadd(w.lb, vmul(w.nb, f1.radius));
+                        w.sep -= f1.radius;
+                    }
+                    if (w.sep <= cd) {
+                        Cand clipped[4];
+                        const int nc = face_contacts(s, f0, f1, cd, w, clipped);
+                        if (nc) {
+                            for (int j = 0; j < nc; ++j) cache.pts[j] = to_pt(clipped[j]);
+                            set_meta(cache, uint32_t(nc), true);
+                        } else {
+                            cache.pts[0] = to_pt(w);
+                            set_meta(cache, 1, true);
+                        }
+                    }
+                }
+            }
+            if (lane == 0) {
+                const uint32_t nc = cache_count(cache);
+                for (uint32_t j = 0; j < nc && count >= 0; ++j) {
+                    const PcmPoint& pt = cache.pts[j];
+                    if (pt.sep > cd) continue;
+                    const v3 nrm = rot_sc(f1.q, lv(pt.nb));
+                    const v3 l = rot_sc(f1.q, lv(pt.lb));
+                    ContactPt& o = out[count++];
+                    o.p[0] = f1.p.x + l.x; o.p[1] = f1.p.y + l.y; o.p[2] = f1.p.z + l.z;
+                    o.n[0] = nrm.x; o.n[1] = nrm.y; o.n[2] = nrm.z;
+                    o.sep = pt.sep;
+                    if (!isfinite(o.p[0]) || !isfinite(o.p[1]) || !isfinite(o.p[2]) || !isfinite(nrm.x) ||
+                        !isfinite(nrm.y) || !isfinite(nrm.z) || !isfinite(o.sep))
+                        count = -1;
+                }
+            }
+        }
+        if (lane == 0) {
             if (count < 0) {
                 atomicOr(s.err, kErrContactOverflow);
                 count = 0;
@@ -1232,10 +1739,15 @@ void enqueue_narrowphase(const DevState& s, cudaStream_t st, const StageHook& ho
     const int T = 128;
     hook(kStNarrow, st);
     cudaMemsetAsync(s.counters + kCntGjk, 0, 4, st);
+    cudaMemsetAsync(s.counters + kCntConvex, 0, 4, st);
     const uint32_t blocks = (s.pair_cap + T - 1) / T;
     k_narrowphase<<<blocks < 148u * 16u ? blocks : 148u * 16u, T, 0, st>>>(s);
     const uint32_t gb = (s.pair_cap + kGjkWarps - 1) / kGjkWarps;
     k_narrowphase_gjk<<<gb < 148u * 8u ? gb : 148u * 8u, kGjkWarps * 32, 0, st>>>(s);
+    if (s.n_meshes) {
+        const uint32_t cb = (s.pair_cap + kCvxWarps - 1) / kCvxWarps;
+        k_narrowphase_convex<<<cb < 148u * 8u ? cb : 148u * 8u, kCvxWarps * 32, 0, st>>>(s);
+    }
 }
 
 }  // namespace fyzz::b200

@@ -65,6 +65,19 @@ struct DevState {
     // shapes
     uint32_t *s_body = nullptr, *s_type = nullptr, *s_scene = nullptr;
     float4 *s_geom = nullptr;          // half extents xyz, radius
+    uint32_t* s_mesh = nullptr;        // cooked hull index, ~0u for other shapes
+    // cooked hulls: per mesh its vertex and face ranges and the half size of
+    // its vertex bounds (w: half the smallest bound extent); the arenas hold
+    // every mesh's vertices, face planes (normal, distance), face boundary
+    // loops (first index into hidx, count) and the loop indices (local to
+    // the mesh's vertex range)
+    uint4* m_tab = nullptr;            // vertex offset, vertex count, face offset, face count
+    float4* m_half = nullptr;
+    float4* hv = nullptr;
+    float4* hf = nullptr;
+    uint2* hfr = nullptr;
+    uint32_t* hidx = nullptr;
+    uint32_t n_meshes = 0;
     float4 *s_lp = nullptr;            // local position, w = contact offset
     float4 *s_lq = nullptr;
     float4 *s_mat = nullptr;           // static f, dynamic f, restitution, rest offset
@@ -84,6 +97,7 @@ struct DevState {
     uint32_t* lost_flag = nullptr;     // per previous pair
     ContactPt* pts = nullptr;          // 4 per current pair
     uint32_t* gjk_list = nullptr;      // pairs awaiting the GJK/EPA continuation
+    uint32_t* cvx_list = nullptr;      // pairs with a cooked hull (plane or finite partner)
 
     // touching managers
     uint32_t* man_list = nullptr;      // current-pair indices, canonical order
@@ -257,7 +271,8 @@ enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels =
              kCntAwake = 6 /* descriptors of awake islands */, kCntSleeping = 7 /* asleep at step start */,
              kCntList = 8 /* 4 island-class list lengths */, kCntLost = 12, kCntEvPts = 13,
              kCntReported = 14 /* touching managers with an event */,
-             kCntReady = 15 /* ready for sleep at step start */, kCntSlots = 16 };
+             kCntReady = 15 /* ready for sleep at step start */,
+             kCntConvex = 16 /* pairs with a cooked hull */, kCntSlots = 17 };
 
 // Contact event records in device memory; the layouts of
 // fyzz_b200_contact_event_t and fyzz_b200_contact_event_point_t.

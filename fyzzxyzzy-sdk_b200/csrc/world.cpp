@@ -16,6 +16,7 @@
 // contact-manager history (the reference's invalidate_after_rollback,
 // source_sc_owned_gpu_broadphase_native.h:479-484) and replays the steps.
 #include "state.h"
+#include "convex.h"
 #include "../../include/fyzz_b200.h"
 
 #include <algorithm>
@@ -65,6 +66,7 @@ struct HostShape {
     std::array<float, 4> lq{0, 0, 0, 1};
     std::array<float, 4> mat{0.5f, 0.5f, 0.2f, 0.0f};   // static, dynamic, restitution, rest offset
     float contact_offset = 0.02f;
+    uint32_t mesh = ~0u;            // cooked hull (index into the world's meshes)
 };
 // A joint: its descriptor bodies (distance kinds: the ordered pair with the
 // anchors as authored, scene.cpp:3097-3108; other kinds: the authored order,
@@ -128,6 +130,16 @@ M3 m_mul(const M3& a, const M3& b) {
         r.c[c] = vadd(vadd(vmul(a.c[0], bc.x), vmul(a.c[1], bc.y)), vmul(a.c[2], bc.z));
     }
     return r;
+}
+// PxQuat::rotate (src/physx_port/foundation/PxQuat.h:262-271), which the
+// compound mass uses to place a hull's centre of mass.
+v3 rot_px(const std::array<float, 4>& q, v3 v) {
+    const float vx = 2.0f * v.x, vy = 2.0f * v.y, vz = 2.0f * v.z;
+    const float w2 = q[3] * q[3] - 0.5f;
+    const float dot2 = q[0] * vx + q[1] * vy + q[2] * vz;
+    return {vx * w2 + (q[1] * vz - q[2] * vy) * q[3] + q[0] * dot2,
+            vy * w2 + (q[2] * vx - q[0] * vz) * q[3] + q[1] * dot2,
+            vz * w2 + (q[0] * vy - q[1] * vx) * q[3] + q[2] * dot2};
 }
 M3 m_t(const M3& a) {
     M3 r;
@@ -295,6 +307,40 @@ public:
         topology_dirty_ = true;
         return uint32_t(shapes_.size() - 1);
     }
+    // World::attach_convex_shape (scene.cpp:283-340): the shape's half
+    // extents are the larger absolute vertex bound per axis; instances of one
+    // cooked mesh share its device vertex range.
+    uint32_t attach_convex(uint32_t body, std::shared_ptr<const CookedMesh> mesh, const float* local) {
+        if (!mesh || mesh->verts.empty()) throw std::invalid_argument("Cooked convex geometry is missing");
+        HostBody& b = require_body(body);
+        if (!b.dynamic) throw std::logic_error("Shapes attach to dynamic bodies on this backend");
+        if (b.scene != current_scene()) throw std::logic_error("Bodies of a closed scene cannot gain shapes");
+        validate_position(local);
+        const auto lq = validated_orientation(local + 3);
+        if (b.shapes.size() >= 8) throw std::logic_error("At most 8 shapes per body are supported");
+        uint32_t m = 0;
+        while (m < meshes_.size() && meshes_[m] != mesh) ++m;
+        if (m == meshes_.size()) {
+            uint64_t nv = mesh->verts.size();
+            for (const auto& x : meshes_) nv += x->verts.size();
+            if (nv > std::numeric_limits<uint32_t>::max())
+                throw std::overflow_error("Convex vertex arena exceeds 32-bit device indexing");
+        }
+        pull_state();
+        if (m == meshes_.size()) meshes_.push_back(mesh);
+        HostShape s;
+        s.body = body;
+        s.scene = b.scene;
+        s.type = kConvex;
+        for (int k = 0; k < 3; ++k) s.half[k] = std::max(std::abs(mesh->lo[k]), std::abs(mesh->hi[k]));
+        s.mesh = m;
+        s.lp = {local[0], local[1], local[2]};
+        s.lq = lq;
+        b.shapes.push_back(uint32_t(shapes_.size()));
+        shapes_.push_back(s);
+        topology_dirty_ = true;
+        return uint32_t(shapes_.size() - 1);
+    }
     void update_mass_properties(uint32_t body, float density) {
         HostBody& b = require_body(body);
         if (!b.dynamic) throw std::logic_error("Static body has no mass properties");
@@ -305,15 +351,22 @@ public:
         // Shapes are visited in list order: most recently attached first.
         std::vector<uint32_t> order(b.shapes.rbegin(), b.shapes.rend());
         std::vector<float> um(order.size());
+        std::vector<v3> lc(order.size());   // shape centre of mass in the body frame
         float mass = 0.0f;
         v3 center = {0, 0, 0};
         for (size_t i = 0; i < order.size(); ++i) {
             const HostShape& s = shapes_[order[i]];
             um[i] = s.type == kBox ? s.half[0] * s.half[1] * s.half[2] * 8.0f
-                                   : (4.0f / 3.0f) * pi * s.radius * s.radius * s.radius;
+                  : s.type == kConvex ? static_cast<float>(meshes_[s.mesh]->volume)
+                                      : (4.0f / 3.0f) * pi * s.radius * s.radius * s.radius;
             const float m = um[i] * density;
             mass += m;
-            center = vadd(center, vmul({s.lp[0], s.lp[1], s.lp[2]}, m));
+            lc[i] = {s.lp[0], s.lp[1], s.lp[2]};
+            if (s.type == kConvex) {
+                const auto& c = meshes_[s.mesh]->center;
+                lc[i] = vadd(lc[i], rot_px(s.lq, {c[0], c[1], c[2]}));
+            }
+            center = vadd(center, vmul(lc[i], m));
         }
         if (!std::isfinite(mass) || !(mass > 0.0f)) throw std::invalid_argument("Compound mass outside supported range");
         center = vmul(center, 1.0f / mass);
@@ -321,19 +374,24 @@ public:
         for (size_t i = 0; i < order.size(); ++i) {
             const HostShape& s = shapes_[order[i]];
             const float m = um[i] * density;
-            v3 diag;
-            if (s.type == kBox) {
-                const v3 h = {s.half[0], s.half[1], s.half[2]};
-                diag = vmul({h.y * h.y + h.z * h.z, h.x * h.x + h.z * h.z, h.x * h.x + h.y * h.y}, m / 3.0f);
-            } else {
-                const float v = (2.0f / 5.0f) * m * s.radius * s.radius;
-                diag = {v, v, v};
-            }
             M3 local{};
-            local.c[0].x = diag.x; local.c[1].y = diag.y; local.c[2].z = diag.z;
+            if (s.type == kConvex) {
+                const auto& I = meshes_[s.mesh]->inertia;
+                for (int c = 0; c < 3; ++c) local.c[c] = vmul({I[c][0], I[c][1], I[c][2]}, density);
+            } else {
+                v3 diag;
+                if (s.type == kBox) {
+                    const v3 h = {s.half[0], s.half[1], s.half[2]};
+                    diag = vmul({h.y * h.y + h.z * h.z, h.x * h.x + h.z * h.z, h.x * h.x + h.y * h.y}, m / 3.0f);
+                } else {
+                    const float v = (2.0f / 5.0f) * m * s.radius * s.radius;
+                    diag = {v, v, v};
+                }
+                local.c[0].x = diag.x; local.c[1].y = diag.y; local.c[2].z = diag.z;
+            }
             const M3 rot = m_from_q({s.lq[0], s.lq[1], s.lq[2], s.lq[3]});
             const M3 rt = m_mul(m_mul(rot, local), m_t(rot));
-            const v3 d = vsub({s.lp[0], s.lp[1], s.lp[2]}, center);
+            const v3 d = vsub(lc[i], center);
             const float dd = vdot(d, d);
             for (int c = 0; c < 3; ++c) {
                 tensor.c[c] = vadd(tensor.c[c], rt.c[c]);
@@ -1369,6 +1427,7 @@ private:
         dalloc(d_.lost_flag, cap, pair_owned_);
         dalloc(d_.pts, size_t(cap) * 4, pair_owned_);
         dalloc(d_.gjk_list, cap, pair_owned_);
+        dalloc(d_.cvx_list, cap, pair_owned_);
         dalloc(d_.man_list, cap, pair_owned_);
         dalloc(d_.mh, cap, pair_owned_);
         dalloc(d_.nrow, size_t(cap) * 4, pair_owned_);
@@ -1558,12 +1617,41 @@ private:
             bscene[i] = bodies_[i].scene;
         }
         std::vector<float4> geom(ns), lp(ns), lq(ns);
+        std::vector<uint32_t> smesh(ns);
         for (uint32_t i = 0; i < ns; ++i) {
             const HostShape& s = shapes_[i];
             geom[i] = make_float4(s.half[0], s.half[1], s.half[2], s.radius);
             lp[i] = make_float4(s.lp[0], s.lp[1], s.lp[2], s.contact_offset);
             lq[i] = make_float4(s.lq[0], s.lq[1], s.lq[2], s.lq[3]);
+            smesh[i] = s.mesh;
         }
+        // cooked hull arenas: every mesh's vertices, faces and loops
+        std::vector<uint4> mtab;
+        std::vector<float4> mhalf, hv, hf;
+        std::vector<uint2> hfr;
+        std::vector<uint32_t> hidx;
+        for (const auto& m : meshes_) {
+            mtab.push_back(make_uint4(uint32_t(hv.size()), uint32_t(m->verts.size()), uint32_t(hf.size()),
+                                      uint32_t(m->faces.size())));
+            const float ex = m->hi[0] - m->lo[0], ey = m->hi[1] - m->lo[1], ez = m->hi[2] - m->lo[2];
+            mhalf.push_back(make_float4(0.5f * ex, 0.5f * ey, 0.5f * ez, 0.5f * std::min({ex, ey, ez})));
+            for (const auto& v : m->verts) hv.push_back(make_float4(v[0], v[1], v[2], 0.0f));
+            const uint32_t i0 = uint32_t(hidx.size());
+            for (const auto& f : m->faces) {
+                hf.push_back(make_float4(f.n[0], f.n[1], f.n[2], f.d));
+                hfr.push_back(make_uint2(i0 + f.first, f.count));
+            }
+            hidx.insert(hidx.end(), m->idx.begin(), m->idx.end());
+        }
+        d_.n_meshes = uint32_t(meshes_.size());
+        dalloc(d_.s_mesh, ns, owned_);
+        dalloc(d_.m_tab, mtab.size(), owned_); dalloc(d_.m_half, mhalf.size(), owned_);
+        dalloc(d_.hv, hv.size(), owned_); dalloc(d_.hf, hf.size(), owned_);
+        dalloc(d_.hfr, hfr.size(), owned_); dalloc(d_.hidx, hidx.size(), owned_);
+        upload(d_.s_mesh, smesh, stream_);
+        upload(d_.m_tab, mtab, stream_); upload(d_.m_half, mhalf, stream_);
+        upload(d_.hv, hv, stream_); upload(d_.hf, hf, stream_);
+        upload(d_.hfr, hfr, stream_); upload(d_.hidx, hidx, stream_);
         // joints: per scene, constraint slot descending (scene.cpp:7153-7162)
         std::vector<HostJoint> js = joints_;
         std::stable_sort(js.begin(), js.end(), [](const HostJoint& a, const HostJoint& b) {
@@ -1619,6 +1707,7 @@ private:
     Branches br_;
     std::vector<HostBody> bodies_;
     std::vector<HostShape> shapes_;
+    std::vector<std::shared_ptr<const CookedMesh>> meshes_;
     std::vector<HostJoint> joints_;
     std::vector<uint32_t> scene_body_begin_, scene_shape_begin_;
     std::vector<bool> scene_has_floor_;
@@ -1663,6 +1752,9 @@ private:
 struct fyzz_b200_world {
     fyzz::b200::World* impl = nullptr;
     std::string error;
+};
+struct fyzz_b200_convex_mesh {
+    std::shared_ptr<const fyzz::b200::CookedMesh> mesh;
 };
 
 namespace {
@@ -1760,13 +1852,83 @@ int fyzz_b200_set_body_angular_velocity(fyzz_b200_world* w, uint32_t body, const
 int fyzz_b200_add_center_distance_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b, float d, uint64_t* out) {
     return guarded(w, [&](auto& W) { const uint64_t id = W.add_distance(a, b, d); if (out) *out = id; });
 }
+namespace {
+thread_local std::string g_cook_error;
+}
+int fyzz_b200_cook_convex_mesh(const float* verts, uint32_t nv, const uint32_t* tris, uint32_t nt,
+                               fyzz_b200_convex_mesh** out) {
+    if (!out) return FYZZ_B200_INVALID_ARGUMENT;
+    *out = nullptr;
+    try {
+        auto m = fyzz::b200::cook_convex(verts, nv, tris, nt);
+        *out = new fyzz_b200_convex_mesh{std::move(m)};
+        g_cook_error.clear();
+        return FYZZ_B200_OK;
+    } catch (const std::invalid_argument& e) {
+        g_cook_error = e.what(); return FYZZ_B200_INVALID_ARGUMENT;
+    } catch (const std::overflow_error& e) {
+        g_cook_error = e.what(); return FYZZ_B200_OVERFLOW;
+    } catch (const std::exception& e) {
+        g_cook_error = e.what(); return FYZZ_B200_RUNTIME_ERROR;
+    }
+}
+void fyzz_b200_convex_mesh_release(fyzz_b200_convex_mesh* mesh) { delete mesh; }
+const char* fyzz_b200_cook_error(void) { return g_cook_error.c_str(); }
+int fyzz_b200_convex_mesh_info(const fyzz_b200_convex_mesh* mesh, uint32_t counts[3], float* faces6,
+                               uint32_t* face_indices, double* volume, float* mass18) {
+    if (!mesh || !mesh->mesh) return FYZZ_B200_INVALID_ARGUMENT;
+    const auto& m = *mesh->mesh;
+    if (counts) {
+        counts[0] = uint32_t(m.verts.size());
+        counts[1] = uint32_t(m.faces.size());
+        counts[2] = uint32_t(m.idx.size());
+    }
+    if (faces6)
+        for (size_t i = 0; i < m.faces.size(); ++i) {
+            const auto& f = m.faces[i];
+            float* o = faces6 + 6 * i;
+            o[0] = f.n[0]; o[1] = f.n[1]; o[2] = f.n[2]; o[3] = f.d;
+            o[4] = float(f.first); o[5] = float(f.count);
+        }
+    if (face_indices) std::copy(m.idx.begin(), m.idx.end(), face_indices);
+    if (volume) *volume = m.volume;
+    if (mass18) {
+        for (int k = 0; k < 3; ++k) mass18[k] = m.center[k];
+        for (int c = 0; c < 3; ++c)
+            for (int k = 0; k < 3; ++k) mass18[3 + 3 * c + k] = m.inertia[c][k];
+        for (int k = 0; k < 3; ++k) {
+            mass18[12 + k] = m.lo[k];
+            mass18[15 + k] = m.hi[k];
+        }
+    }
+    return FYZZ_B200_OK;
+}
+int fyzz_b200_attach_convex_shape(fyzz_b200_world* w, uint32_t body, const fyzz_b200_convex_mesh* mesh,
+                                  const float local[7], uint32_t* out) {
+    static const float identity[7] = {0, 0, 0, 0, 0, 0, 1};
+    if (!mesh) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) {
+        const uint32_t s = W.attach_convex(body, mesh->mesh, local ? local : identity);
+        if (out) *out = s;
+    });
+}
 int fyzz_b200_add_scene(fyzz_b200_world* w, uint32_t nb, const float* bodies, uint32_t ns,
                         const uint32_t* shape_body, const uint32_t* shape_type, const float* shape_geom,
                         const float* shape_local, const float* shape_mat, uint32_t nj,
                         const uint32_t* joint_bodies, const float* joint_dist, int has_floor,
                         float floor_height, const float* floor_mat, uint32_t* first_body_out) {
+    return fyzz_b200_add_scene_ex(w, nb, bodies, ns, shape_body, shape_type, shape_geom, shape_local, shape_mat, nj,
+                                  joint_bodies, joint_dist, has_floor, floor_height, floor_mat, 0, nullptr,
+                                  first_body_out);
+}
+int fyzz_b200_add_scene_ex(fyzz_b200_world* w, uint32_t nb, const float* bodies, uint32_t ns,
+                           const uint32_t* shape_body, const uint32_t* shape_type, const float* shape_geom,
+                           const float* shape_local, const float* shape_mat, uint32_t nj,
+                           const uint32_t* joint_bodies, const float* joint_dist, int has_floor,
+                           float floor_height, const float* floor_mat, uint32_t n_meshes,
+                           fyzz_b200_convex_mesh* const* meshes, uint32_t* first_body_out) {
     if ((nb && !bodies) || (ns && (!shape_body || !shape_type || !shape_geom || !shape_local || !shape_mat)) ||
-        (nj && (!joint_bodies || !joint_dist)))
+        (nj && (!joint_bodies || !joint_dist)) || (n_meshes && !meshes))
         return FYZZ_B200_INVALID_ARGUMENT;
     return guarded(w, [&](auto& W) {
         W.begin_scene();
@@ -1785,9 +1947,16 @@ int fyzz_b200_add_scene(fyzz_b200_world* w, uint32_t nb, const float* bodies, ui
             if (b == 0 && first_body_out) *first_body_out = body_id[b];
             while (si < ns && shape_body[si] == b) {
                 const float* g = shape_geom + 4 * size_t(si);
-                shape_id[si] = shape_type[si] == 0
-                    ? W.attach(body_id[b], fyzz::b200::kBox, g, 0.0f, shape_local + 7 * size_t(si))
-                    : W.attach(body_id[b], fyzz::b200::kSphere, g, g[0], shape_local + 7 * size_t(si));
+                const float* l = shape_local + 7 * size_t(si);
+                if (shape_type[si] == 3) {
+                    const uint32_t m = static_cast<uint32_t>(g[0]);
+                    if (!(g[0] >= 0.0f) || m >= n_meshes || !meshes[m])
+                        throw std::invalid_argument("Convex shape names no cooked mesh");
+                    shape_id[si] = W.attach_convex(body_id[b], meshes[m]->mesh, l);
+                } else {
+                    shape_id[si] = shape_type[si] == 0 ? W.attach(body_id[b], fyzz::b200::kBox, g, 0.0f, l)
+                                                       : W.attach(body_id[b], fyzz::b200::kSphere, g, g[0], l);
+                }
                 ++si;
             }
             W.update_mass_properties(body_id[b], r[13]);

@@ -86,6 +86,30 @@ int fyzz_b200_attach_box_shape(fyzz_b200_world* w, uint32_t body, const float ha
 /* World::attach_sphere_shape (world.h:411) */
 int fyzz_b200_attach_sphere_shape(fyzz_b200_world* w, uint32_t body, float radius,
                                   const float local_pose[7], uint32_t* shape_out);
+/* ---- cooked convex hulls: cook_convex_mesh (include/fyzzxyzzy/convex.h:56-60,
+ * src/native/cooked_convex.cpp:41-330) and World::attach_convex_shape
+ * (world.h:412-413, scene.cpp:283-340) ---- */
+typedef struct fyzz_b200_convex_mesh fyzz_b200_convex_mesh;
+/* Cooks an outward-wound, closed, convex, manifold triangle surface
+ * (n_vertices x 3 floats, n_triangles x 3 indices).  Coplanar triangles
+ * become one polygon face.  Rejected meshes return FYZZ_B200_INVALID_ARGUMENT
+ * with the reason in fyzz_b200_cook_error().  The mesh is reference
+ * counted: worlds that attach it keep their own reference, so the caller
+ * may release it at any time. */
+int fyzz_b200_cook_convex_mesh(const float* vertices, uint32_t n_vertices, const uint32_t* triangles,
+                               uint32_t n_triangles, fyzz_b200_convex_mesh** mesh_out);
+void fyzz_b200_convex_mesh_release(fyzz_b200_convex_mesh* mesh);
+/* Message of this thread's last failed cook. */
+const char* fyzz_b200_cook_error(void);
+/* ConvexMesh accessors (convex.h:34-53); any output may be NULL.
+ * counts: vertices, faces, face indices.  faces6: per face normal(3),
+ * distance, first index, index count.  mass18: centre of mass(3), inertia
+ * columns(9) about it for density one, bounds min(3), max(3). */
+int fyzz_b200_convex_mesh_info(const fyzz_b200_convex_mesh* mesh, uint32_t counts[3], float* faces6,
+                               uint32_t* face_indices, double* volume, float* mass18);
+/* World::attach_convex_shape (world.h:412) */
+int fyzz_b200_attach_convex_shape(fyzz_b200_world* w, uint32_t body, const fyzz_b200_convex_mesh* mesh,
+                                  const float local_pose[7], uint32_t* shape_out);
 /* World::update_mass_properties (world.h:420, compound.cpp:113-203) */
 int fyzz_b200_update_mass_properties(fyzz_b200_world* w, uint32_t body, float density);
 /* World::body_mass_properties (world.h:421): inverse mass, inverse inertia(3),
@@ -134,6 +158,14 @@ int fyzz_b200_add_scene(fyzz_b200_world* w, uint32_t n_bodies, const float* bodi
                         uint32_t n_joints, const uint32_t* joint_bodies, const float* joint_dist,
                         int has_floor, float floor_height, const float* floor_mat,
                         uint32_t* first_body_out);
+/* fyzz_b200_add_scene with cooked hulls: shape type 3 attaches
+ * meshes[(uint32_t)shape_geom[4 * i]] (World::attach_convex_shape). */
+int fyzz_b200_add_scene_ex(fyzz_b200_world* w, uint32_t n_bodies, const float* bodies,
+                           uint32_t n_shapes, const uint32_t* shape_body, const uint32_t* shape_type,
+                           const float* shape_geom, const float* shape_local, const float* shape_mat,
+                           uint32_t n_joints, const uint32_t* joint_bodies, const float* joint_dist,
+                           int has_floor, float floor_height, const float* floor_mat,
+                           uint32_t n_meshes, fyzz_b200_convex_mesh* const* meshes, uint32_t* first_body_out);
 
 /* ---- stepping: World::step (world.h:459, scene.cpp:10725) ---- */
 int fyzz_b200_step(fyzz_b200_world* w, float seconds);
@@ -298,9 +330,10 @@ uint64_t fyzz_b200_read_friction_anchors(fyzz_b200_world* w, uint32_t* anchors, 
 /* Partition level of every descriptor of the last step, in canonical
  * descriptor order (joints then touching managers). */
 uint64_t fyzz_b200_read_levels(fyzz_b200_world* w, uint32_t* levels, uint64_t cap);
-/* Device counters of the last step, n <= 16: 0 touching managers,
+/* Device counters of the last step, n <= 17: 0 touching managers,
  * 1 descriptors, 5 box pairs finished by GJK/EPA, 8-11 islands per size
- * class ((32,512], (96,512], (512,4096], >4096 descriptors). */
+ * class ((32,512], (96,512], (512,4096], >4096 descriptors), 16 pairs with
+ * a cooked hull. */
 int fyzz_b200_read_step_counters(fyzz_b200_world* w, uint32_t* out, uint32_t n);
 
 /* ---- allocation-free sweep-and-prune (no counterpart in the reference) ----

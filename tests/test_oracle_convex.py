@@ -116,3 +116,27 @@ def test_convex_pile_sleeps_like_reference(ref, oracle, scenes):
         o.step(DT, r.manager_order(), r.joint_order())
     np.testing.assert_array_equal(o.body_states(), r.body_states())
     assert r.body_states()[1:, 13].sum() >= 12
+
+
+def test_product_cooking_matches_reference(pkg, ref, scenes):
+    """The product's cooking (host code behind fyzz_b200_cook_convex_mesh)
+    gives the reference's faces, loops, volume, centre, inertia and bounds
+    bit for bit, and rejects what the reference rejects."""
+    for k, (v, t) in enumerate(meshes_under_test(scenes)):
+        got = pkg.ConvexMesh(v, t).info()
+        want = ref.cook_convex(v, t)
+        for key in ("faces", "idx", "center", "inertia", "lo", "hi"):
+            np.testing.assert_array_equal(got[key], want[key], err_msg=f"mesh {k} {key}")
+        assert got["volume"] == want["volume"]
+    v, t = scenes.hull_box((0.2, 0.2, 0.2))
+    bad = [(v, t[:-1]),                                     # open
+           (v, t[:, ::-1]),                                 # inward
+           (v[:3], t[:4] % 3),                              # too few vertices
+           (np.vstack([v, [[0.0, 0.0, 0.0]]]), t),          # unused (interior) vertex
+           (v * np.float32(np.nan), t),                     # not finite
+           (v, np.vstack([t, t[:1]]))]                      # duplicated triangle
+    for i, (bv, bt) in enumerate(bad):
+        with pytest.raises(ValueError):
+            ref.cook_convex(bv, bt)
+        with pytest.raises(ValueError):
+            pkg.ConvexMesh(bv, bt)
