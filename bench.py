@@ -42,6 +42,9 @@ PLAIN_WORKLOAD = ("plain method at scale, one scene: 131,072 bodies (70% boxes, 
 BATCHED_WORKLOAD = ("batched forward: 4,096 independent scenes, body count log-uniform in [16,512] "
                     "(random piles and 5-20 high unit-cube stacks), own floor each, one launch per stage, "
                     "step captured as a CUDA graph")
+CONVEX_WORKLOAD = ("cooked convex hulls: one scene of 32,768 bodies (75% cooked hulls of 6 shared meshes: "
+                   "prisms, frustums, bipyramids, a box hull, random ellipsoid hulls; 25% boxes and spheres), "
+                   "size U[0.12,0.3] m, dropped from 0.5-20 m over 120x120 m onto a floor, steps 121..360")
 L2_BYTES = 126 * 1024 * 1024
 
 
@@ -75,6 +78,10 @@ def parse_args():
     ap.add_argument("--diff4-every", type=int, default=8)
     ap.add_argument("--settle", type=int, default=0,
                     help="untimed steps of the plain scene before warm-up (profiling a settled pile)")
+    ap.add_argument("--convex-bodies", type=int, default=32768)
+    ap.add_argument("--convex-steps", type=int, default=240)
+    ap.add_argument("--convex-settle", type=int, default=120)
+    ap.add_argument("--no-convex", action="store_true", help="skip the cooked-hull leg")
     ap.add_argument("--plain-only", action="store_true",
                     help="time the plain scene only (no e2e, batched or CPU legs; for profiler runs)")
     return ap.parse_args()
@@ -341,6 +348,51 @@ def differentiable_leg_at_scale(torch, pkg, local_rank, args):
                       "untimed rollout of the same shape from the same start state"}
 
 
+def convex_spec(n):
+    return scenes_mod().convex_pile(n, seed=11, xz=60.0, y=(0.5, 20.0))
+
+
+def convex_leg(torch, pkg, local_rank, rank, world, args, barrier, max_over_ranks, sum_over_ranks):
+    """The cooked-hull path: a convex pile stepped past its first impacts,
+    then timed with CUDA events; on rank 0 of a one-GPU run the reference
+    NativeCpu scene steps the same scene on the host for a bounded sample."""
+    spec = convex_spec(args.convex_bodies)
+    w = pkg.World(local_rank)
+    w.add_scene(spec)
+    w.step(DT, args.convex_settle)
+    stream = torch.cuda.ExternalStream(w.device_view().stream)
+    barrier()
+    ms = timed_steps(torch, w, args.convex_steps, stream)
+    ms_max = max_over_ranks(ms)
+    value = sum_over_ranks(spec.n_bodies * args.convex_steps) / (ms_max / 1e3)
+    prof = w.profile_step(DT)
+    counts = w.counts()
+    sc = w.step_counters()
+    w.close()
+    out = {"workload": CONVEX_WORKLOAD, "bodies": spec.n_bodies * world, "steps": args.convex_steps,
+           "value": value, "unit": UNIT, "ms_per_step": ms_max / args.convex_steps,
+           "stages_ms": {k: round(v, 4) for k, v in prof.items()}, "counts": counts,
+           "convex_pairs": sc["convex_pairs"], "convex_regenerated": sc["convex_regenerated"],
+           "cpu_reference": None}
+    if rank == 0 and world == 1:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import refscene
+        if refscene.available():
+            r = refscene.RefScene(spec)
+            r.step(DT, args.convex_settle)
+            n, t0 = 0, time.perf_counter()
+            while n < args.convex_steps and time.perf_counter() - t0 < 10.0:
+                r.step(DT, 1)
+                n += 1
+            el = time.perf_counter() - t0
+            r.close()
+            out["cpu_reference"] = {"value": spec.n_bodies * n / el, "unit": UNIT, "cores": 2, "kind": "reference",
+                                    "sample": f"steps {args.convex_settle + 1}..{args.convex_settle + n} of the same "
+                                              f"scene ({el:.1f} s)"}
+            out["vs_cpu_reference"] = value / out["cpu_reference"]["value"]
+    return out
+
+
 def plain_same_bodies(torch, pkg, specs, local_rank, n_sample, steps):
     """The plain single-scene path on the batched workload's own bodies: a
     sample of the scenes (evenly spaced over the list, so over the size
@@ -505,6 +557,11 @@ def run_b200(args, rank, world, local_rank):
         diff = differentiable_leg(torch, pkg, local_rank, args)
     diff4 = differentiable_leg_at_scale(torch, pkg, local_rank, args) if args.diff4 and not args.plain_only else None
 
+    # ---- cooked convex hulls ----
+    convex = None
+    if not args.no_convex and not args.plain_only:
+        convex = convex_leg(torch, pkg, local_rank, rank, world, args, barrier, max_over_ranks, sum_over_ranks)
+
     # ---- CPU baseline: the reference NativeCpu scene on this host ----
     cpu = None
     if rank == 0 and world == 1 and not args.plain_only:
@@ -528,6 +585,7 @@ def run_b200(args, rank, world, local_rank):
             "e2e": e2e,
             "differentiable": diff,
             "differentiable_at_scale": diff4,
+            "convex": convex,
             "backward_forward_ratio": diff["backward_forward_ratio"] if diff else None,
             "gpu_launches": kernels * args.steps,
             "roofline": roofline,

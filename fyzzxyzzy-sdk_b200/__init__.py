@@ -519,10 +519,10 @@ class World:
 
     def step_counters(self) -> dict:
         """Device counters of the last step (see fyzz_b200_read_step_counters)."""
-        out = np.zeros(17, np.uint32)
-        self._check(lib().fyzz_b200_read_step_counters(self.h, _p(out), 17))
+        out = np.zeros(18, np.uint32)
+        self._check(lib().fyzz_b200_read_step_counters(self.h, _p(out), 18))
         return {"managers": int(out[0]), "descriptors": int(out[1]), "gjk_pairs": int(out[5]),
-                "convex_pairs": int(out[16]),
+                "convex_pairs": int(out[16]), "convex_regenerated": int(out[17]),
                 "islands_32_512": int(out[8]), "islands_96_512": int(out[9]),
                 "islands_512_4096": int(out[10]), "islands_4096_up": int(out[11])}
 

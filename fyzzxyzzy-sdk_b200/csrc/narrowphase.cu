@@ -325,16 +325,30 @@ __device__ __forceinline__ v3 box_vertex(v3 e, v3 d, uint32_t& idx) {
     idx = (x ? 1u : 0u) | (y ? 2u : 0u) | (z ? 4u : 0u);
     return {x ? e.x : -e.x, y ? e.y : -e.y, z ? e.z : -e.z};
 }
+// A hull's support: its first vertex of largest projection.  The warp
+// splits the scan (lane l takes vertices l, l + 32, ...) and reduces to the
+// largest projection, lowest index on ties, which is the vertex the
+// sequential first-maximum scan returns; lane 0's result is broadcast so
+// every lane holds the same vertex whatever the inputs.  Every lane of the
+// warp must call it together.
 __device__ __forceinline__ v3 shape_vertex(v3 e, v3 d, const float4* hull, uint32_t n, float radius,
                                            uint32_t& idx) {
     idx = 0;
     if (radius > 0.f) return {0.f, 0.f, 0.f};
     if (n) {
-        float best = vdot(ld3(hull[0]), d);
-        for (uint32_t i = 1; i < n; ++i) {
+        const uint32_t lane = threadIdx.x & 31u;
+        float best = 0.f;
+        uint32_t bi = 0xffffffffu;
+        for (uint32_t i = lane; i < n; i += 32) {
             const float pr = vdot(ld3(hull[i]), d);
-            if (pr > best) { best = pr; idx = i; }
+            if (bi == 0xffffffffu || pr > best) { best = pr; bi = i; }
         }
+        for (int off = 16; off > 0; off >>= 1) {
+            const float ob = __shfl_xor_sync(0xffffffffu, best, off);
+            const uint32_t oi = __shfl_xor_sync(0xffffffffu, bi, off);
+            if (oi != 0xffffffffu && (bi == 0xffffffffu || ob > best || (ob == best && oi < bi))) { best = ob; bi = oi; }
+        }
+        idx = __shfl_sync(0xffffffffu, bi, 0);
         return ld3(hull[idx]);
     }
     return box_vertex(e, d, idx);
@@ -612,7 +626,21 @@ struct EpaShared {
 template <bool G> __device__ bool run_epa_warp(const BPair& p, const Sup* simplex, int sc, Cand& out, EpaShared& E) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t full = 0xffffffffu;
-    if (lane == 0) {
+    if (G) {
+        // every lane builds the initial polytope (its supports are warp
+        // scans); lane 0 publishes it
+        Sup v0[4];
+        Facet f0[4];
+        int vc0 = sc, fc0 = 0;
+        for (int i = 0; i < sc; ++i) v0[i] = simplex[i];
+        const bool ok = init_epa<G>(p, v0, vc0, f0, fc0);
+        if (lane == 0) {
+            for (int i = 0; i < vc0; ++i) E.vtx[i] = v0[i];
+            for (int i = 0; i < fc0; ++i) E.facets[i] = f0[i];
+            E.status = ok ? fc0 : -1;
+            E.bc = vc0;
+        }
+    } else if (lane == 0) {
         int vc0 = sc;
         for (int i = 0; i < sc; ++i) E.vtx[i] = simplex[i];
         int fc0 = 0;
@@ -1619,115 +1647,149 @@ __device__ int plane_hull(const DevState& s, const PairShapes& ps, PcmCache& cac
     return emitted;
 }
 
-// Pairs with a cooked hull (scene.cpp:3655-3772, 3774-3972).  One warp takes
-// a pair: plane pairs run on lane 0; finite pairs decide refresh and
-// regeneration in step on every lane, run GJK/EPA together (hull supports
-// are each lane's own scan of the vertices) and clip faces on lane 0.
-constexpr int kCvxWarps = 4;
-__global__ void __launch_bounds__(kCvxWarps * 32, 1) k_narrowphase_convex(DevState s) {
-    __shared__ EpaShared epa[kCvxWarps];
-    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+// Refresh and regeneration test of a finite pair with a cooked hull
+// (scene.cpp:3655-3700): the refreshed cache, B-local pose of A, and whether
+// the manifold must be regenerated.
+__device__ bool convex_refresh(const Fin& f0, const Fin& f1, PcmCache& cache, v3& relative, qt& rotation) {
+    const v3 delta = {f0.p.x - f1.p.x, f0.p.y - f1.p.y, f0.p.z - f1.p.z};
+    relative = rotinv_sc(f1.q, delta);
+    rotation = qmul(qconj(f1.q), f0.q);
+    const float mm = smin(smin(0.15f * f0.extent, 0.15f), smin(0.15f * f1.extent, 0.15f));
+    const uint32_t prev = cache_count(cache);
+    refresh_points(cache, relative, rotation, mm * 0.8f);
+    const bool init = cache_init(cache);
+    const float tr = init ? smax(smax(fabsf(relative.x - cache.rel_p[0]), fabsf(relative.y - cache.rel_p[1])),
+                                 fabsf(relative.z - cache.rel_p[2]))
+                          : INFINITY;
+    const float qa = qdot(f0.q, {cache.qa[0], cache.qa[1], cache.qa[2], cache.qa[3]});
+    const float qb = qdot(f1.q, {cache.qb[0], cache.qb[1], cache.qb[2], cache.qb[3]});
+    const float thr = mm * (cache_count(cache) == 0 ? 0.5f : 0.125f);
+    if (!init || cache_count(cache) != prev || tr > thr || qa < 0.9999f || qb < 0.9999f) return true;
+    const v3 ha = f0.shalf, hb = f1.shalf;
+    const float ta = (qa < 1.f ? acosf(smax(-1.f, qa)) : 0.f) * sqrtf(ha.x * ha.x + ha.y * ha.y + ha.z * ha.z);
+    const float tb = (qb < 1.f ? acosf(smax(-1.f, qb)) : 0.f) * sqrtf(hb.x * hb.x + hb.y * hb.y + hb.z * hb.z);
+    return ta > thr || tb > thr;
+}
+// Cached witnesses within the contact distance, each with its own normal,
+// in world space (scene.cpp:3752-3771).  -1 on a non-finite contact.
+__device__ int convex_emit(const Fin& f1, float cd, const PcmCache& cache, ContactPt* out) {
+    int count = 0;
+    const uint32_t nc = cache_count(cache);
+    for (uint32_t j = 0; j < nc; ++j) {
+        const PcmPoint& pt = cache.pts[j];
+        if (pt.sep > cd) continue;
+        const v3 nrm = rot_sc(f1.q, lv(pt.nb));
+        const v3 l = rot_sc(f1.q, lv(pt.lb));
+        ContactPt& o = out[count++];
+        o.p[0] = f1.p.x + l.x; o.p[1] = f1.p.y + l.y; o.p[2] = f1.p.z + l.z;
+        o.n[0] = nrm.x; o.n[1] = nrm.y; o.n[2] = nrm.z;
+        o.sep = pt.sep;
+        if (!isfinite(o.p[0]) || !isfinite(o.p[1]) || !isfinite(o.p[2]) || !isfinite(nrm.x) || !isfinite(nrm.y) ||
+            !isfinite(nrm.z) || !isfinite(o.sep))
+            return -1;
+    }
+    return count;
+}
+__device__ __forceinline__ void store_manifold(const DevState& s, uint32_t k, const PcmCache& cache, int count,
+                                               const ContactPt* out) {
+    if (count < 0) {
+        atomicOr(s.err, kErrContactOverflow);
+        count = 0;
+    }
+    s.cur.cache[k] = cache;
+    s.cur.count[k] = uint32_t(count);
+    for (int j = 0; j < count; ++j) s.pts[4 * size_t(k) + j] = out[j];
+}
+
+// Pairs with a cooked hull, one thread each: hull vertices against the
+// floor, and finite pairs whose cached manifold stays valid.  Finite pairs
+// that regenerate go on to the warp kernel below.
+__global__ void __launch_bounds__(128) k_narrowphase_convex(DevState s) {
     const uint32_t n = s.counters[kCntConvex];
-    const uint32_t nwarps = gridDim.x * kCvxWarps;
-    for (uint32_t i = blockIdx.x * kCvxWarps + wib; i < n; i += nwarps) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint32_t k = s.cvx_list[i];
         const PairShapes ps = pair_shapes(s, s.cur.key[k]);
         PcmCache cache = s.cur.cache[k];
         ContactPt out[4];
-        int count = 0;
         if (ps.plane) {
-            if (lane == 0) count = plane_hull(s, ps, cache, out);
-        } else {
-            const Fin f0 = load_fin(s, ps.first), f1 = load_fin(s, ps.second);
-            const float cd = ps.cd;
-            const v3 delta = {f0.p.x - f1.p.x, f0.p.y - f1.p.y, f0.p.z - f1.p.z};
-            const v3 relative = rotinv_sc(f1.q, delta);
-            const qt rotation = qmul(qconj(f1.q), f0.q);
-            const float mm = smin(smin(0.15f * f0.extent, 0.15f), smin(0.15f * f1.extent, 0.15f));
-            const uint32_t prev = cache_count(cache);
-            refresh_points(cache, relative, rotation, mm * 0.8f);
-            const bool init = cache_init(cache);
-            const float tr = init ? smax(smax(fabsf(relative.x - cache.rel_p[0]), fabsf(relative.y - cache.rel_p[1])),
-                                         fabsf(relative.z - cache.rel_p[2]))
-                                  : INFINITY;
-            const float qa = qdot(f0.q, {cache.qa[0], cache.qa[1], cache.qa[2], cache.qa[3]});
-            const float qb = qdot(f1.q, {cache.qb[0], cache.qb[1], cache.qb[2], cache.qb[3]});
-            const float thr = mm * (cache_count(cache) == 0 ? 0.5f : 0.125f);
-            bool regen = !init || cache_count(cache) != prev || tr > thr || qa < 0.9999f || qb < 0.9999f;
-            if (!regen) {
-                const v3 ha = f0.shalf, hb = f1.shalf;
-                const float ta = (qa < 1.f ? acosf(smax(-1.f, qa)) : 0.f) * sqrtf(ha.x * ha.x + ha.y * ha.y + ha.z * ha.z);
-                const float tb = (qb < 1.f ? acosf(smax(-1.f, qb)) : 0.f) * sqrtf(hb.x * hb.x + hb.y * hb.y + hb.z * hb.z);
-                regen = ta > thr || tb > thr;
-            }
-            if (regen) {
-                sv(cache.rel_p, relative);
-                cache.rel_q[0] = rotation.x; cache.rel_q[1] = rotation.y; cache.rel_q[2] = rotation.z; cache.rel_q[3] = rotation.w;
-                cache.qa[0] = f0.q.x; cache.qa[1] = f0.q.y; cache.qa[2] = f0.q.z; cache.qa[3] = f0.q.w;
-                cache.qb[0] = f1.q.x; cache.qb[1] = f1.q.y; cache.qb[2] = f1.q.z; cache.qb[3] = f1.q.w;
-                set_meta(cache, 0, true);
-                BPair bp;
-                bp.ha = f0.half;
-                bp.hb = f1.half;
-                bp.a_in_b = rotinv_gu(f1.q, vsub(f0.p, f1.p));
-                bp.rel = qmul(qconj(f1.q), f0.q);
-                bp.va = s.hv + f0.vo; bp.nva = f0.nv;
-                bp.vb = s.hv + f1.vo; bp.nvb = f1.nv;
-                bp.ra = f0.radius; bp.rb = f1.radius;
-                Cand w = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0.0f};
-                Sup simplex[4];
-                int sc = 0;
-                const int mode = gjk_phase<true>(bp, cd + f0.radius + f1.radius, w, simplex, sc);
-                bool have = mode == 1;
-                if (mode == 2) have = run_epa_warp<true>(bp, simplex, sc, w, epa[wib]);
-                if (lane == 0 && have) {
-                    // sphere radii applied along the final normal
-                    if (f0.radius > 0.f) {
-                        w.la = vadd(w.la, rotinv_gu(bp.rel, vmul(w.nb, -f0.radius)));
-                        w.sep -= f0.radius;
-                    }
-                    if (f1.radius > 0.f) {
-                        w.lb = vadd(w.lb, vmul(w.nb, f1.radius));
-                        w.sep -= f1.radius;
-                    }
-                    if (w.sep <= cd) {
-                        Cand clipped[4];
-                        const int nc = face_contacts(s, f0, f1, cd, w, clipped);
-                        if (nc) {
-                            for (int j = 0; j < nc; ++j) cache.pts[j] = to_pt(clipped[j]);
-                            set_meta(cache, uint32_t(nc), true);
-                        } else {
-                            cache.pts[0] = to_pt(w);
-                            set_meta(cache, 1, true);
-                        }
-                    }
-                }
-            }
-            if (lane == 0) {
-                const uint32_t nc = cache_count(cache);
-                for (uint32_t j = 0; j < nc && count >= 0; ++j) {
-                    const PcmPoint& pt = cache.pts[j];
-                    if (pt.sep > cd) continue;
-                    const v3 nrm = rot_sc(f1.q, lv(pt.nb));
-                    const v3 l = rot_sc(f1.q, lv(pt.lb));
-                    ContactPt& o = out[count++];
-                    o.p[0] = f1.p.x + l.x; o.p[1] = f1.p.y + l.y; o.p[2] = f1.p.z + l.z;
-                    o.n[0] = nrm.x; o.n[1] = nrm.y; o.n[2] = nrm.z;
-                    o.sep = pt.sep;
-                    if (!isfinite(o.p[0]) || !isfinite(o.p[1]) || !isfinite(o.p[2]) || !isfinite(nrm.x) ||
-                        !isfinite(nrm.y) || !isfinite(nrm.z) || !isfinite(o.sep))
-                        count = -1;
-                }
-            }
+            const int count = plane_hull(s, ps, cache, out);
+            store_manifold(s, k, cache, count, out);
+            continue;
         }
+        const Fin f0 = load_fin(s, ps.first), f1 = load_fin(s, ps.second);
+        v3 relative;
+        qt rotation;
+        if (convex_refresh(f0, f1, cache, relative, rotation)) {
+            s.cvx_gjk_list[atomicAdd(&s.counters[kCntConvexGjk], 1u)] = k;
+            continue;
+        }
+        store_manifold(s, k, cache, convex_emit(f1, ps.cd, cache, out), out);
+    }
+}
+
+// Finite hull pairs whose manifold regenerates (scene.cpp:3701-3751).  One
+// warp takes a pair: GJK/EPA run together on every lane (hull supports are
+// each lane's own scan of the vertices), faces are clipped on lane 0.
+constexpr int kCvxWarps = 4;
+__global__ void __launch_bounds__(kCvxWarps * 32, 1) k_narrowphase_convex_gjk(DevState s) {
+    __shared__ EpaShared epa[kCvxWarps];
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    const uint32_t n = s.counters[kCntConvexGjk];
+    const uint32_t nwarps = gridDim.x * kCvxWarps;
+    for (uint32_t i = blockIdx.x * kCvxWarps + wib; i < n; i += nwarps) {
+        const uint32_t k = s.cvx_gjk_list[i];
+        const PairShapes ps = pair_shapes(s, s.cur.key[k]);
+        PcmCache cache = s.cur.cache[k];
+        const Fin f0 = load_fin(s, ps.first), f1 = load_fin(s, ps.second);
+        const float cd = ps.cd;
+        v3 relative;
+        qt rotation;
+        convex_refresh(f0, f1, cache, relative, rotation);     // regenerates: listed by the kernel above
+        sv(cache.rel_p, relative);
+        cache.rel_q[0] = rotation.x; cache.rel_q[1] = rotation.y; cache.rel_q[2] = rotation.z; cache.rel_q[3] = rotation.w;
+        cache.qa[0] = f0.q.x; cache.qa[1] = f0.q.y; cache.qa[2] = f0.q.z; cache.qa[3] = f0.q.w;
+        cache.qb[0] = f1.q.x; cache.qb[1] = f1.q.y; cache.qb[2] = f1.q.z; cache.qb[3] = f1.q.w;
+        set_meta(cache, 0, true);
+        BPair bp;
+        bp.ha = f0.half;
+        bp.hb = f1.half;
+        bp.a_in_b = rotinv_gu(f1.q, vsub(f0.p, f1.p));
+        bp.rel = qmul(qconj(f1.q), f0.q);
+        bp.va = s.hv + f0.vo; bp.nva = f0.nv;
+        bp.vb = s.hv + f1.vo; bp.nvb = f1.nv;
+        bp.ra = f0.radius; bp.rb = f1.radius;
+        Cand w = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0.0f};
+        Sup simplex[4];
+        int sc = 0;
+        const int mode = gjk_phase<true>(bp, cd + f0.radius + f1.radius, w, simplex, sc);
+        bool have = mode == 1;
+        if (mode == 2) have = run_epa_warp<true>(bp, simplex, sc, w, epa[wib]);
         if (lane == 0) {
-            if (count < 0) {
-                atomicOr(s.err, kErrContactOverflow);
-                count = 0;
+            if (have) {
+                // sphere radii applied along the final normal
+                if (f0.radius > 0.f) {
+                    w.la = vadd(w.la, rotinv_gu(bp.rel, vmul(w.nb, -f0.radius)));
+                    w.sep -= f0.radius;
+                }
+                if (f1.radius > 0.f) {
+                    w.lb = vadd(w.lb, vmul(w.nb, f1.radius));
+                    w.sep -= f1.radius;
+                }
+                if (w.sep <= cd) {
+                    Cand clipped[4];
+                    const int nc = face_contacts(s, f0, f1, cd, w, clipped);
+                    if (nc) {
+                        for (int j = 0; j < nc; ++j) cache.pts[j] = to_pt(clipped[j]);
+                        set_meta(cache, uint32_t(nc), true);
+                    } else {
+                        cache.pts[0] = to_pt(w);
+                        set_meta(cache, 1, true);
+                    }
+                }
             }
-            s.cur.cache[k] = cache;
-            s.cur.count[k] = uint32_t(count);
-            for (int j = 0; j < count; ++j) s.pts[4 * size_t(k) + j] = out[j];
+            ContactPt out[4];
+            store_manifold(s, k, cache, convex_emit(f1, cd, cache, out), out);
         }
         __syncwarp();
     }
@@ -1739,14 +1801,15 @@ void enqueue_narrowphase(const DevState& s, cudaStream_t st, const StageHook& ho
     const int T = 128;
     hook(kStNarrow, st);
     cudaMemsetAsync(s.counters + kCntGjk, 0, 4, st);
-    cudaMemsetAsync(s.counters + kCntConvex, 0, 4, st);
+    cudaMemsetAsync(s.counters + kCntConvex, 0, 8, st);
     const uint32_t blocks = (s.pair_cap + T - 1) / T;
     k_narrowphase<<<blocks < 148u * 16u ? blocks : 148u * 16u, T, 0, st>>>(s);
     const uint32_t gb = (s.pair_cap + kGjkWarps - 1) / kGjkWarps;
     k_narrowphase_gjk<<<gb < 148u * 8u ? gb : 148u * 8u, kGjkWarps * 32, 0, st>>>(s);
     if (s.n_meshes) {
+        k_narrowphase_convex<<<blocks < 148u * 16u ? blocks : 148u * 16u, T, 0, st>>>(s);
         const uint32_t cb = (s.pair_cap + kCvxWarps - 1) / kCvxWarps;
-        k_narrowphase_convex<<<cb < 148u * 8u ? cb : 148u * 8u, kCvxWarps * 32, 0, st>>>(s);
+        k_narrowphase_convex_gjk<<<cb < 148u * 8u ? cb : 148u * 8u, kCvxWarps * 32, 0, st>>>(s);
     }
 }
 

@@ -98,6 +98,7 @@ struct DevState {
     ContactPt* pts = nullptr;          // 4 per current pair
     uint32_t* gjk_list = nullptr;      // pairs awaiting the GJK/EPA continuation
     uint32_t* cvx_list = nullptr;      // pairs with a cooked hull (plane or finite partner)
+    uint32_t* cvx_gjk_list = nullptr;  // hull pairs whose manifold regenerates (GJK/EPA)
 
     // touching managers
     uint32_t* man_list = nullptr;      // current-pair indices, canonical order
@@ -272,7 +273,8 @@ enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels =
              kCntList = 8 /* 4 island-class list lengths */, kCntLost = 12, kCntEvPts = 13,
              kCntReported = 14 /* touching managers with an event */,
              kCntReady = 15 /* ready for sleep at step start */,
-             kCntConvex = 16 /* pairs with a cooked hull */, kCntSlots = 17 };
+             kCntConvex = 16 /* pairs with a cooked hull */,
+             kCntConvexGjk = 17 /* hull pairs regenerated through GJK/EPA */, kCntSlots = 18 };
 
 // Contact event records in device memory; the layouts of
 // fyzz_b200_contact_event_t and fyzz_b200_contact_event_point_t.

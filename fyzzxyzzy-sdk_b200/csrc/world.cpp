@@ -1428,6 +1428,7 @@ private:
         dalloc(d_.pts, size_t(cap) * 4, pair_owned_);
         dalloc(d_.gjk_list, cap, pair_owned_);
         dalloc(d_.cvx_list, cap, pair_owned_);
+        dalloc(d_.cvx_gjk_list, cap, pair_owned_);
         dalloc(d_.man_list, cap, pair_owned_);
         dalloc(d_.mh, cap, pair_owned_);
         dalloc(d_.nrow, size_t(cap) * 4, pair_owned_);

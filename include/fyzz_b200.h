@@ -330,10 +330,10 @@ uint64_t fyzz_b200_read_friction_anchors(fyzz_b200_world* w, uint32_t* anchors, 
 /* Partition level of every descriptor of the last step, in canonical
  * descriptor order (joints then touching managers). */
 uint64_t fyzz_b200_read_levels(fyzz_b200_world* w, uint32_t* levels, uint64_t cap);
-/* Device counters of the last step, n <= 17: 0 touching managers,
+/* Device counters of the last step, n <= 18: 0 touching managers,
  * 1 descriptors, 5 box pairs finished by GJK/EPA, 8-11 islands per size
  * class ((32,512], (96,512], (512,4096], >4096 descriptors), 16 pairs with
- * a cooked hull. */
+ * a cooked hull, 17 of those regenerated through GJK/EPA. */
 int fyzz_b200_read_step_counters(fyzz_b200_world* w, uint32_t* out, uint32_t n);
 
 /* ---- allocation-free sweep-and-prune (no counterpart in the reference) ----
