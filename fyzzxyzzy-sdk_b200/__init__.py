@@ -43,6 +43,7 @@ EXPORTS = (
     "fyzz_b200_set_body_kinematic_target", "fyzz_b200_rollout_rewind",
     "fyzz_b200_cook_convex_mesh", "fyzz_b200_convex_mesh_release", "fyzz_b200_cook_error",
     "fyzz_b200_convex_mesh_info", "fyzz_b200_attach_convex_shape", "fyzz_b200_add_scene_ex",
+    "fyzz_b200_write_velocities_strided",
 )
 STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 
@@ -135,6 +136,7 @@ def lib():
         L.fyzz_b200_body_state.argtypes = [vp, u32, P(BodyState)]
         L.fyzz_b200_read_bodies.argtypes = [vp, vp, u32]
         L.fyzz_b200_write_velocities.argtypes = [vp, vp, u32]
+        L.fyzz_b200_write_velocities_strided.argtypes = [vp, vp, u32, u32, u32, u32]
         L.fyzz_b200_counts.argtypes = [vp, vp]
         L.fyzz_b200_device_view.argtypes = [vp, P(DeviceView)]
         L.fyzz_b200_read_pairs.argtypes = [vp, i32, vp, u64]
@@ -383,6 +385,13 @@ class World:
     def write_velocities(self, v6: np.ndarray):
         v6 = np.ascontiguousarray(v6, np.float32)
         self._check(lib().fyzz_b200_write_velocities(self.h, _p(v6), v6.shape[0]))
+
+    def write_states(self, states: np.ndarray):
+        """Writes back the velocities of (n, 14) body records as read_bodies
+        returns them (one host-to-device copy of the records as they are)."""
+        if states.dtype != np.float32 or states.ndim != 2 or states.shape[1] != 14 or not states.flags.c_contiguous:
+            raise ValueError("states must be a contiguous (n, 14) float32 array")
+        self._check(lib().fyzz_b200_write_velocities_strided(self.h, _p(states), states.shape[0], 14, 3, 10))
 
     def device_view(self) -> DeviceView:
         out = DeviceView()

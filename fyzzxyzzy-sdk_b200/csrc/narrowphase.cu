@@ -612,14 +612,14 @@ template <bool G> __device__ int gjk_phase(const BPair& p, float cd, Cand& out, 
 
 // EPA (GuPCMGjkEpa.cpp) with one warp: the polytope lives in shared memory; the closest
 // facet search, the duplicate-vertex test, the visibility marking, the free
-// slot count and the new facets are spread over the lanes, while the
-// horizon walk (whose order decides where new facets land) stays on lane 0
-// and visits the visible facets in index order, as the sequential search does.  Every
-// lane returns the same result; out is valid on every lane.
+// slot count and the new facets are spread over the lanes; the horizon walk
+// (whose order decides where new facets land) visits the visible facets in
+// index order, as the sequential search does, with the edge list held one
+// edge per lane.  Every lane returns the same result; out is valid on every
+// lane.
 struct EpaShared {
     Sup vtx[64];
     Facet facets[64];
-    int bfrom[32], bto[32];
     int bc;
     int status;
 };
@@ -689,42 +689,43 @@ template <bool G> __device__ bool run_epa_warp(const BPair& p, const Sup* simple
             (r ? vis1 : vis0) = vis;
         }
         const uint32_t vmask0 = __ballot_sync(full, vis0), vmask1 = __ballot_sync(full, vis1);
-        __syncwarp();
-        if (lane == 0) {
-            E.vtx[ni] = np;
-            // horizon edges in the order the sequential search finds them
-            int bc = 0;
-            bool fail = false;
-            for (int r = 0; r < 2 && !fail; ++r) {
-                uint32_t m = r ? vmask1 : vmask0;
-                while (m && !fail) {
-                    const int i = __ffs(m) - 1 + 32 * r;
-                    m &= m - 1;
-                    Facet& f = E.facets[i];
-                    f.valid = false;
-                    const int ef[3] = {f.i, f.j, f.k}, et[3] = {f.j, f.k, f.i};
-                    for (int e = 0; e < 3; ++e) {
-                        int rev = -1;
-                        for (int j = 0; j < bc; ++j)
-                            if (E.bfrom[j] == et[e] && E.bto[j] == ef[e]) { rev = j; break; }
-                        if (rev >= 0) {
-                            --bc;
-                            E.bfrom[rev] = E.bfrom[bc];
-                            E.bto[rev] = E.bto[bc];
-                        } else {
-                            if (bc == 32) { fail = true; break; }
-                            E.bfrom[bc] = ef[e];
-                            E.bto[bc] = et[e];
-                            ++bc;
-                        }
+        if (lane == 0) E.vtx[ni] = np;
+        // Horizon edges in the order the sequential search finds them: the
+        // visible facets in index order, each edge appended or, when its
+        // reverse is listed, removed by moving the last edge into its slot.
+        // The list lives in registers, lane t holding edge t, so each test
+        // is one ballot.
+        int ef0 = -1, et0 = -1;     // this lane's boundary edge
+        int bc = 0;
+        bool fail = false;
+        for (int r = 0; r < 2 && !fail; ++r) {
+            uint32_t m = r ? vmask1 : vmask0;
+            while (m && !fail) {
+                const int i = __ffs(m) - 1 + 32 * r;
+                m &= m - 1;
+                const Facet& f = E.facets[i];
+                const int ef[3] = {f.i, f.j, f.k}, et[3] = {f.j, f.k, f.i};
+                for (int e = 0; e < 3; ++e) {
+                    const uint32_t hit = __ballot_sync(full, int(lane) < bc && ef0 == et[e] && et0 == ef[e]);
+                    if (hit) {
+                        const int rev = __ffs(hit) - 1;
+                        --bc;
+                        const int lf = __shfl_sync(full, ef0, bc), lt = __shfl_sync(full, et0, bc);
+                        if (int(lane) == rev) { ef0 = lf; et0 = lt; }
+                    } else {
+                        if (bc == 32) { fail = true; break; }
+                        if (int(lane) == bc) { ef0 = ef[e]; et0 = et[e]; }
+                        ++bc;
                     }
                 }
             }
-            E.bc = fail ? -1 : bc;
         }
+        if (fail || bc <= 0) return false;
         __syncwarp();
-        const int bc = E.bc;
-        if (bc <= 0) return false;
+        // the visible facets leave the polytope
+        if (vis0) E.facets[lane].valid = false;
+        if (vis1) E.facets[lane + 32].valid = false;
+        __syncwarp();
         // free slots among [0, fc): invalid facets, in index order
         bool inv0 = int(lane) < fc && !E.facets[lane].valid;
         bool inv1 = int(lane) + 32 < fc && !E.facets[lane + 32].valid;
@@ -736,7 +737,7 @@ template <bool G> __device__ bool run_epa_warp(const BPair& p, const Sup* simple
         bool ok = true;
         int slot = -1;
         if (int(lane) < bc) {
-            nf = make_facet<G>(E.vtx, E.bfrom[lane], E.bto[lane], ni);
+            nf = make_facet<G>(E.vtx, ef0, et0, ni);
             ok = nf.valid;
             nf.in_heap = nf.distance <= upper;
             const int k = int(lane);
@@ -1265,7 +1266,7 @@ __global__ void __launch_bounds__(128) k_narrowphase(DevState s) {
 // search one subset per lane) and EPA together (run_epa_warp) with the
 // polytope in shared memory.
 constexpr int kGjkWarps = 4;
-__global__ void __launch_bounds__(kGjkWarps * 32, 1) k_narrowphase_gjk(DevState s) {
+__global__ void __launch_bounds__(kGjkWarps * 32, 3) k_narrowphase_gjk(DevState s) {
     __shared__ EpaShared epa[kGjkWarps];
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     const uint32_t n = s.counters[kCntGjk];
@@ -1514,6 +1515,156 @@ __device__ int face_contacts(const DevState& s, const Fin& a, const Fin& b, floa
     return int(k.count);
 }
 
+// The same clipping with the whole warp: the face searches are warp
+// argmax reductions (largest alignment, lowest face on ties: the face the
+// sequential first-maximum scan keeps), both polygons are staged once in
+// shared memory in B's frame, and each clipping loop tests 32 points at a
+// time with lane 0 emitting the accepted ones in the sequential order.
+// Every lane calls it; the result is on lane 0.  Polygons of more than
+// kClipPoly vertices take the lane-0 version above.
+constexpr unsigned kClipPoly = 64;
+struct ClipShared {
+    float4 rv[kClipPoly], qv[kClipPoly];
+};
+__device__ __forceinline__ void warp_argmax_first(float& best, unsigned& idx) {
+    for (int off = 16; off > 0; off >>= 1) {
+        const float ob = __shfl_xor_sync(0xffffffffu, best, off);
+        const unsigned oi = __shfl_xor_sync(0xffffffffu, idx, off);
+        if (oi != 0xffffffffu && (idx == 0xffffffffu || ob > best || (ob == best && oi < idx))) { best = ob; idx = oi; }
+    }
+    best = __shfl_sync(0xffffffffu, best, 0);
+    idx = __shfl_sync(0xffffffffu, idx, 0);
+}
+__device__ int face_contacts_warp(const DevState& s, const Fin& a, const Fin& b, float cd, const Cand& w, Cand out[4],
+                                  ClipShared& C) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t full = 0xffffffffu;
+    if (a.radius > 0.f || b.radius > 0.f || (a.nv && !a.nf) || (b.nv && !b.nf)) return 0;
+    Clip k;
+    k.s = &s; k.a = &a; k.b = &b;
+    const v3 normal = w.nb;
+    if (!(vlen2(normal) > 0.f)) return 0;
+    // a lane's first maximum over its faces, then the warp's; the scan's
+    // initial value -2 is below every alignment, so "no face" never wins
+    float ala = -2.f, alb = -2.f;
+    unsigned fa = 0xffffffffu, fb = 0xffffffffu;
+    for (unsigned i = lane; i < fc_count(a); i += 32) {
+        const float d = vdot(vneg(normal), clip_normal(k, a, true, i));
+        if (fa == 0xffffffffu ? d > -2.f : d > ala) { ala = d; fa = i; }
+    }
+    for (unsigned i = lane; i < fc_count(b); i += 32) {
+        const float d = vdot(normal, clip_normal(k, b, false, i));
+        if (fb == 0xffffffffu ? d > -2.f : d > alb) { alb = d; fb = i; }
+    }
+    warp_argmax_first(ala, fa);
+    warp_argmax_first(alb, fb);
+    if (fa == 0xffffffffu) { ala = -2.f; fa = 0; }
+    if (fb == 0xffffffffu) { alb = -2.f; fb = 0; }
+    k.reference_b = alb >= ala;
+    if (smax(ala, alb) < 0.95f) return 0;
+    k.ref = k.reference_b ? &b : &a;
+    k.inc = k.reference_b ? &a : &b;
+    k.ref_is_a = !k.reference_b;
+    k.inc_is_a = k.reference_b;
+    k.rf = k.reference_b ? fb : fa;
+    k.rn = clip_normal(k, *k.ref, k.ref_is_a, k.rf);
+    float ial = -2.f;
+    unsigned inf = 0xffffffffu;
+    for (unsigned i = lane; i < fc_count(*k.inc); i += 32) {
+        const float d = vdot(vneg(k.rn), clip_normal(k, *k.inc, k.inc_is_a, i));
+        if (inf == 0xffffffffu ? d > -2.f : d > ial) { ial = d; inf = i; }
+    }
+    warp_argmax_first(ial, inf);
+    k.inf = inf == 0xffffffffu ? 0u : inf;
+    const v3 in_n = clip_normal(k, *k.inc, k.inc_is_a, k.inf);
+    const float den = vdot(in_n, k.rn);
+    if (!(den < -0.25f)) return 0;
+    k.nr = fc_nvert(s, *k.ref, k.rf);
+    k.ni = fc_nvert(s, *k.inc, k.inf);
+    if (k.nr < 3u || k.ni < 3u) return 0;
+    if (k.nr > kClipPoly || k.ni > kClipPoly) {
+        int n = 0;
+        if (lane == 0) n = face_contacts(s, a, b, cd, w, out);
+        return n;
+    }
+    for (unsigned i = lane; i < k.nr; i += 32) C.rv[i] = st4(clip_vertex(k, *k.ref, k.ref_is_a, k.rf, i), 0.f);
+    for (unsigned i = lane; i < k.ni; i += 32) C.qv[i] = st4(clip_vertex(k, *k.inc, k.inc_is_a, k.inf, i), 0.f);
+    __syncwarp();
+    const auto R = [&](unsigned i) { return ld3(C.rv[i % k.nr]); };
+    const auto Q = [&](unsigned i) { return ld3(C.qv[i % k.ni]); };
+    k.anchor = R(0);
+    const v3 in_anchor = Q(0);
+    float el = 0.f;
+    for (unsigned i = lane; i < k.nr; i += 32) el = smax(el, vlen2(vsub(R(i + 1), R(i))));
+    for (unsigned i = lane; i < k.ni; i += 32) el = smax(el, vlen2(vsub(Q(i + 1), Q(i))));
+    for (int off = 16; off > 0; off >>= 1) el = smax(el, __shfl_xor_sync(full, el, off));
+    el = __shfl_sync(full, el, 0);
+    const float scale = sqrtf(el);
+    if (!(scale > 0.f) || !isfinite(scale)) return 0;
+    const float tol = smax(scale * 1.e-5f, 1.e-6f);
+    const float ftol = tol / scale;
+    k.tol_sq = tol * tol;
+    k.cd = cd;
+    k.out = out;
+    k.count = 0;
+    // lane 0 emits the chunk's accepted points in order
+    const auto emit_chunk = [&](bool ok, v3 p) {
+        uint32_t m = __ballot_sync(full, ok);
+        while (m) {
+            const int src = __ffs(m) - 1;
+            m &= m - 1;
+            const v3 q = {__shfl_sync(full, p.x, src), __shfl_sync(full, p.y, src), __shfl_sync(full, p.z, src)};
+            if (lane == 0) clip_emit(k, q);
+        }
+    };
+    for (unsigned c = 0; c < k.ni; c += 32) {
+        const unsigned i = c + lane;
+        bool inside = i < k.ni;
+        const v3 v = inside ? Q(i) : v3{0, 0, 0};
+        for (unsigned j = 0; j < k.nr && inside; ++j)
+            if (clip_cross(k, vsub(R(j + 1), R(j)), vsub(v, R(j))) < -tol * scale) inside = false;
+        emit_chunk(inside, v);
+    }
+    for (unsigned c = 0; c < k.nr; c += 32) {
+        const unsigned i = c + lane;
+        bool ok = i < k.nr;
+        v3 p = {0, 0, 0};
+        if (ok) {
+            const v3 v = R(i);
+            for (unsigned j = 0; j < k.ni && ok; ++j)
+                if (clip_cross(k, vsub(Q(j + 1), Q(j)), vsub(v, Q(j))) > tol * scale) ok = false;
+            if (ok) {
+                const float height = vdot(in_n, vsub(in_anchor, v)) / den;
+                ok = isfinite(height);
+                p = vadd(v, vmul(k.rn, height));
+            }
+        }
+        emit_chunk(ok, p);
+    }
+    const unsigned np = k.ni * k.nr;
+    for (unsigned c = 0; c < np; c += 32) {
+        const unsigned t = c + lane;
+        bool ok = false;
+        v3 p = {0, 0, 0};
+        if (t < np) {
+            const unsigned i = t / k.nr, j = t % k.nr;
+            const v3 qa = Q(i), e = vsub(Q(i + 1), qa);
+            const v3 rb = R(j), f = vsub(R(j + 1), rb);
+            const float det = clip_cross(k, e, f);
+            if (!(fabsf(det) <= k.tol_sq)) {
+                const v3 d = vsub(rb, qa);
+                const float tt = clip_cross(k, d, f) / det;
+                const float u = clip_cross(k, d, e) / det;
+                ok = tt >= -ftol && tt <= 1.f + ftol && u >= -ftol && u <= 1.f + ftol;
+                p = vadd(qa, vmul(e, sclamp(tt, 0.f, 1.f)));
+            }
+        }
+        emit_chunk(ok, p);
+    }
+    __syncwarp();
+    return int(k.count);
+}
+
 // Hull vertices against the floor plane (scene.cpp:3774-3972): candidates
 // are the vertices below the contact distance in vertex order; more than
 // four are reduced to the deepest, the farthest from it, the two sideways
@@ -1732,8 +1883,9 @@ __global__ void __launch_bounds__(128) k_narrowphase_convex(DevState s) {
 // warp takes a pair: GJK/EPA run together on every lane (hull supports are
 // each lane's own scan of the vertices), faces are clipped on lane 0.
 constexpr int kCvxWarps = 4;
-__global__ void __launch_bounds__(kCvxWarps * 32, 1) k_narrowphase_convex_gjk(DevState s) {
+__global__ void __launch_bounds__(kCvxWarps * 32, 3) k_narrowphase_convex_gjk(DevState s) {
     __shared__ EpaShared epa[kCvxWarps];
+    __shared__ ClipShared clip[kCvxWarps];
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     const uint32_t n = s.counters[kCntConvexGjk];
     const uint32_t nwarps = gridDim.x * kCvxWarps;
@@ -1765,20 +1917,21 @@ __global__ void __launch_bounds__(kCvxWarps * 32, 1) k_narrowphase_convex_gjk(De
         const int mode = gjk_phase<true>(bp, cd + f0.radius + f1.radius, w, simplex, sc);
         bool have = mode == 1;
         if (mode == 2) have = run_epa_warp<true>(bp, simplex, sc, w, epa[wib]);
-        if (lane == 0) {
-            if (have) {
-                // sphere radii applied along the final normal
-                if (f0.radius > 0.f) {
-                    w.la = vadd(w.la, rotinv_gu(bp.rel, vmul(w.nb, -f0.radius)));
-                    w.sep -= f0.radius;
-                }
-                if (f1.radius > 0.f) {
-                    w.lb = vadd(w.lb, vmul(w.nb, f1.radius));
-                    w.sep -= f1.radius;
-                }
-                if (w.sep <= cd) {
-                    Cand clipped[4];
-                    const int nc = face_contacts(s, f0, f1, cd, w, clipped);
+        if (have) {
+            // sphere radii applied along the final normal (every lane holds
+            // the same witness)
+            if (f0.radius > 0.f) {
+                w.la = vadd(w.la, rotinv_gu(bp.rel, vmul(w.nb, -f0.radius)));
+                w.sep -= f0.radius;
+            }
+            if (f1.radius > 0.f) {
+                w.lb = vadd(w.lb, vmul(w.nb, f1.radius));
+                w.sep -= f1.radius;
+            }
+            if (w.sep <= cd) {
+                Cand clipped[4];
+                const int nc = face_contacts_warp(s, f0, f1, cd, w, clipped, clip[wib]);
+                if (lane == 0) {
                     if (nc) {
                         for (int j = 0; j < nc; ++j) cache.pts[j] = to_pt(clipped[j]);
                         set_meta(cache, uint32_t(nc), true);
@@ -1788,6 +1941,8 @@ __global__ void __launch_bounds__(kCvxWarps * 32, 1) k_narrowphase_convex_gjk(De
                     }
                 }
             }
+        }
+        if (lane == 0) {
             ContactPt out[4];
             store_manifold(s, k, cache, convex_emit(f1, cd, cache, out), out);
         }

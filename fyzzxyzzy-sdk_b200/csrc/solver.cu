@@ -1835,20 +1835,23 @@ __global__ void k_pack_bodies(DevState s, float* out) {
     o[10] = w.x; o[11] = w.y; o[12] = w.z;
     o[13] = (s.b_sleep[b] & kSleeping) ? 1.0f : 0.0f;
 }
-__global__ void k_unpack_velocities(DevState s, const float* v6) {
+// Velocities from host records of `stride` floats: linear at lin, angular
+// at ang (6-float records: 0 / 3; the 14-float body records: 3 / 10).
+__global__ void k_unpack_velocities(DevState s, const float* rec, uint32_t stride, uint32_t lin, uint32_t ang) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= s.n_bodies) return;
     const bool dyn = is_dyn(s, b);
-    const float* r = v6 + 6 * size_t(b);
-    s.b_v[b] = dyn ? make_float4(r[0], r[1], r[2], 0.0f) : make_float4(0, 0, 0, 0);
-    s.b_w[b] = dyn ? make_float4(r[3], r[4], r[5], 0.0f) : make_float4(0, 0, 0, 0);
+    const float* r = rec + stride * size_t(b);
+    s.b_v[b] = dyn ? make_float4(r[lin], r[lin + 1], r[lin + 2], 0.0f) : make_float4(0, 0, 0, 0);
+    s.b_w[b] = dyn ? make_float4(r[ang], r[ang + 1], r[ang + 2], 0.0f) : make_float4(0, 0, 0, 0);
 }
 void enqueue_pack_bodies(const DevState& s, float* out, cudaStream_t st) {
     if (s.n_bodies) k_pack_bodies<<<grid_for(s.n_bodies, 256, 1u << 30), 256, 0, st>>>(s, out);
 }
-void enqueue_unpack_velocities(const DevState& s, const float* v6, cudaStream_t st) {
+void enqueue_unpack_velocities(const DevState& s, const float* rec, uint32_t stride, uint32_t lin, uint32_t ang,
+                               cudaStream_t st) {
     if (!s.n_bodies) return;
-    k_unpack_velocities<<<grid_for(s.n_bodies, 256, 1u << 30), 256, 0, st>>>(s, v6);
+    k_unpack_velocities<<<grid_for(s.n_bodies, 256, 1u << 30), 256, 0, st>>>(s, rec, stride, lin, ang);
     k_wake_bodies<<<grid_for(s.n_bodies, 256, 1u << 30), 256, 0, st>>>(s);
 }
 

@@ -261,7 +261,8 @@ void enqueue_wake_bodies(const DevState& s, cudaStream_t st);
 // velocity, sleeping) into out (device memory).
 void enqueue_pack_bodies(const DevState& s, float* out, cudaStream_t st);
 // 6-float velocity records (device memory) into the bodies; wakes them.
-void enqueue_unpack_velocities(const DevState& s, const float* v6, cudaStream_t st);
+void enqueue_unpack_velocities(const DevState& s, const float* rec, uint32_t stride, uint32_t lin, uint32_t ang,
+                               cudaStream_t st);
 void init_solver_kernels();
 // Island size classes (descriptors per island).
 constexpr uint32_t kSmallIsland = 96;     // one warp

@@ -1158,14 +1158,19 @@ public:
         std::memcpy(out->angular_velocity, rec + 10, 12);
         out->sleeping = rec[13] != 0.0f ? 1 : 0;
     }
-    void write_velocities(const float* v6, uint32_t n) {
+    void write_velocities(const float* rec, uint32_t n, uint32_t stride = 6, uint32_t lin = 0, uint32_t ang = 3) {
         if (n != bodies_.size()) throw std::invalid_argument("Body count mismatch");
+        if (stride < 3 || lin + 3 > stride || ang + 3 > stride)
+            throw std::invalid_argument("Velocity offsets must lie inside the record");
         ensure_device();
         // one copy of the caller's records, unpacked (and every body woken)
         // on the device; the caller's buffer is free again on return
-        if (!d_vel6_) dalloc(d_vel6_, 6 * size_t(d_.n_bodies), owned_);
-        check_cuda(cudaMemcpyAsync(d_vel6_, v6, size_t(n) * 24, cudaMemcpyHostToDevice, stream_), "write");
-        enqueue_unpack_velocities(d_, d_vel6_, stream_);
+        if (stride > vel_stride_cap_) {
+            dalloc(d_vel6_, size_t(stride) * d_.n_bodies, owned_);
+            vel_stride_cap_ = stride;
+        }
+        check_cuda(cudaMemcpyAsync(d_vel6_, rec, size_t(n) * stride * 4, cudaMemcpyHostToDevice, stream_), "write");
+        enqueue_unpack_velocities(d_, d_vel6_, stride, lin, ang, stream_);
         check_cuda(cudaGetLastError(), "unpack");
         check_cuda(cudaStreamSynchronize(stream_), "write sync");
     }
@@ -1402,6 +1407,7 @@ private:
         owned_.clear();
         d_pack_ = nullptr;
         d_vel6_ = nullptr;
+        vel_stride_cap_ = 0;
         for (void* p : pair_owned_) cudaFree(p);
         pair_owned_.clear();
         uploaded_ = false;
@@ -1721,6 +1727,7 @@ private:
     float* bk_wake_ = nullptr;
     float* d_pack_ = nullptr;    // read_bodies records (owned, allocated on first use)
     float* d_vel6_ = nullptr;    // write_velocities records
+    uint32_t vel_stride_cap_ = 0; // floats per record d_vel6_ holds
     uint32_t* bk_sleep_ = nullptr;
     bool sleep_enabled_ = true;
     cudaGraphExec_t graphs_[4] = {nullptr, nullptr, nullptr, nullptr};   // [parity + 2 * sleeping]
@@ -2007,6 +2014,11 @@ int fyzz_b200_read_bodies(fyzz_b200_world* w, float* out, uint32_t n) {
 int fyzz_b200_write_velocities(fyzz_b200_world* w, const float* v6, uint32_t n) {
     if (!v6) return FYZZ_B200_INVALID_ARGUMENT;
     return guarded(w, [&](auto& W) { W.write_velocities(v6, n); });
+}
+int fyzz_b200_write_velocities_strided(fyzz_b200_world* w, const float* records, uint32_t n, uint32_t stride,
+                                       uint32_t linear_offset, uint32_t angular_offset) {
+    if (!records) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) { W.write_velocities(records, n, stride, linear_offset, angular_offset); });
 }
 int fyzz_b200_counts(fyzz_b200_world* w, uint64_t out[12]) {
     if (!out) return FYZZ_B200_INVALID_ARGUMENT;

@@ -194,6 +194,12 @@ int fyzz_b200_read_bodies(fyzz_b200_world* w, float* out, uint32_t n_bodies);
 /* Overwrite linear(3) + angular(3) velocities of all bodies from a host
  * buffer (6 floats per body; statics ignored). */
 int fyzz_b200_write_velocities(fyzz_b200_world* w, const float* v6, uint32_t n_bodies);
+/* The same from records of `stride` floats per body with the linear and
+ * angular velocity at the given float offsets: a loop that edits the
+ * 14-float records of fyzz_b200_read_bodies writes them back as they are
+ * (stride 14, offsets 3 and 10).  No reference counterpart. */
+int fyzz_b200_write_velocities_strided(fyzz_b200_world* w, const float* records, uint32_t n_bodies,
+                                       uint32_t stride, uint32_t linear_offset, uint32_t angular_offset);
 /* Counts: [bodies, shapes, scenes, pairs, touching managers, contact points,
  * descriptors, islands, joints, steps, friction rows, found + lost pairs] */
 int fyzz_b200_counts(fyzz_b200_world* w, uint64_t out[12]);

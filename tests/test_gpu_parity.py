@@ -281,3 +281,23 @@ def test_fit_pair_budget_keeps_the_trajectory(pkg, scenes):
     wb.step(DT, steps=20)
     np.testing.assert_array_equal(wa.read_bodies(), wb.read_bodies())
     np.testing.assert_array_equal(wa.pairs(0), wb.pairs(0))
+
+
+def test_write_states_equals_write_velocities(pkg, scenes):
+    # the 14-float records written back as they are give the same state as
+    # the 6-float velocity records
+    spec = scenes.random_boxes(300, seed=12, xz=3.0, y=(0.3, 4.0))
+    wa, _ = make_world(pkg, [spec])
+    wb, _ = make_world(pkg, [spec])
+    wa.step(DT, steps=20)
+    wb.step(DT, steps=20)
+    st = wa.read_bodies()
+    rng = np.random.default_rng(0)
+    st[:, 3:6] += rng.normal(0, 0.5, (st.shape[0], 3)).astype(np.float32)
+    st[:, 10:13] += rng.normal(0, 0.5, (st.shape[0], 3)).astype(np.float32)
+    wa.write_states(np.ascontiguousarray(st))
+    wb.write_velocities(np.concatenate([st[:, 3:6], st[:, 10:13]], 1))
+    np.testing.assert_array_equal(wa.read_bodies(), wb.read_bodies())
+    wa.step(DT, steps=5)
+    wb.step(DT, steps=5)
+    np.testing.assert_array_equal(wa.read_bodies(), wb.read_bodies())
