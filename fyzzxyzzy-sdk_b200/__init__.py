@@ -43,7 +43,7 @@ EXPORTS = (
     "fyzz_b200_set_body_kinematic_target", "fyzz_b200_rollout_rewind",
     "fyzz_b200_cook_convex_mesh", "fyzz_b200_convex_mesh_release", "fyzz_b200_cook_error",
     "fyzz_b200_convex_mesh_info", "fyzz_b200_attach_convex_shape", "fyzz_b200_add_scene_ex",
-    "fyzz_b200_write_velocities_strided",
+    "fyzz_b200_write_velocities_strided", "fyzz_b200_remove_constraint",
 )
 STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 
@@ -137,6 +137,7 @@ def lib():
         L.fyzz_b200_read_bodies.argtypes = [vp, vp, u32]
         L.fyzz_b200_write_velocities.argtypes = [vp, vp, u32]
         L.fyzz_b200_write_velocities_strided.argtypes = [vp, vp, u32, u32, u32, u32]
+        L.fyzz_b200_remove_constraint.argtypes = [vp, u64]
         L.fyzz_b200_counts.argtypes = [vp, vp]
         L.fyzz_b200_device_view.argtypes = [vp, P(DeviceView)]
         L.fyzz_b200_read_pairs.argtypes = [vp, i32, vp, u64]
@@ -290,6 +291,10 @@ class World:
         out = C.c_uint64()
         self._check(getattr(lib(), f"fyzz_b200_add_{name}_constraint")(self.h, a, b, _p(la), _p(lb), C.byref(out)))
         return out.value
+
+    def remove_constraint(self, cid: int):
+        """World::remove_constraint (reference world.h:458)."""
+        self._check(lib().fyzz_b200_remove_constraint(self.h, int(cid)))
 
     def add_fixed_constraint(self, a: int, b: int, local_a, local_b) -> int:
         """World::add_fixed_constraint: local frames are position(3) + xyzw(4)."""

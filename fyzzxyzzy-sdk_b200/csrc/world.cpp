@@ -75,6 +75,8 @@ struct HostJoint {
     uint32_t a = 0, b = 0;
     float len = 0.0f;
     uint32_t scene = 0, slot = 0, kind = kJointCenter;
+    uint32_t gen = 1;      // constraint slot generation (scene.cpp:3129-3137)
+    bool live = true;      // retired slots wait on their scene's free list
     std::array<float, 3> la{0, 0, 0}, lb{0, 0, 0};
     std::array<float, 4> qa{0, 0, 0, 1}, qb{0, 0, 0, 1};
 };
@@ -508,12 +510,41 @@ public:
         j.b = kind <= kJointAnchored ? std::max(a, b) : b;
         j.len = kind <= kJointAnchored ? len : 0.0f;
         j.scene = A.scene;
-        uint32_t slot = 0;
-        for (const auto& o : joints_) if (o.scene == j.scene) ++slot;
-        j.slot = slot;
-        joints_.push_back(j);
-        topology_dirty_ = true;
-        return (uint64_t(1) << 32) | slot;   // generation 1, slot (scene.cpp:3042-3045)
+        // Constraint slots (scene.cpp:3110-3140): the scene's most recently
+        // retired slot is reused with its generation bumped, else a new one
+        // is appended.  Slots index joints_, so they are unique in the
+        // world; in a one-scene world they are the reference's slots.
+        if (free_joints_.size() <= j.scene) free_joints_.resize(j.scene + 1);
+        auto& fl = free_joints_[j.scene];
+        uint32_t slot;
+        if (!fl.empty()) {
+            slot = fl.back();
+            fl.pop_back();
+            j.gen = joints_[slot].gen + 1;
+            j.slot = slot;
+            joints_[slot] = j;
+        } else {
+            slot = uint32_t(joints_.size());
+            j.slot = slot;
+            joints_.push_back(j);
+        }
+        joints_dirty_ = true;
+        mass_dirty_ = true;     // the pulled host copy goes back with the joint tables
+        return (uint64_t(j.gen) << 32) | slot;
+    }
+    // World::remove_constraint (Scene::retire_constraint, scene.cpp:3088-
+    // 3096, 3195-3228): the joint leaves the step; its slot is reused next.
+    void remove_joint(uint64_t id) {
+        const uint32_t slot = uint32_t(id), gen = uint32_t(id >> 32);
+        if (slot >= joints_.size() || !gen || !joints_[slot].live || joints_[slot].gen != gen)
+            throw std::out_of_range("Unknown or expired rigid constraint");
+        pull_state();
+        HostJoint& j = joints_[slot];
+        j.live = false;
+        if (free_joints_.size() <= j.scene) free_joints_.resize(j.scene + 1);
+        free_joints_[j.scene].push_back(slot);
+        joints_dirty_ = true;
+        mass_dirty_ = true;
     }
     void mass_props(uint32_t body, float* out) const {
         const HostBody& b = require_body(body);
@@ -528,10 +559,12 @@ public:
     void ensure_device() {
         if (topology_dirty_ || !uploaded_) {
             build_device();
-        } else if (mass_dirty_) {
-            upload_bodies();
+        } else {
+            if (joints_dirty_) refresh_joints();
+            if (mass_dirty_) upload_bodies();
         }
         mass_dirty_ = false;
+        joints_dirty_ = false;
     }
     // Device -> host body state, before any host authoring edit.
     void pull_state() {
@@ -752,7 +785,7 @@ public:
     void rollout_begin(uint32_t steps, uint32_t every) {
         if (steps == 0 || every == 0) throw std::invalid_argument("Rollout needs steps and a checkpoint interval");
         for (const auto& j : joints_)
-            if (j.kind != kJointCenter)
+            if (j.live && j.kind != kJointCenter)
                 throw std::logic_error("Differentiable rollouts support center distance joints only");
         check_cuda(cudaSetDevice(device_), "cudaSetDevice");
         ensure_device();
@@ -1177,7 +1210,7 @@ public:
     void counts(uint64_t* out) {
         out[0] = bodies_.size(); out[1] = shapes_.size(); out[2] = scene_body_begin_.size();
         out[3] = out[4] = out[5] = out[6] = out[7] = out[10] = out[11] = 0;
-        out[8] = joints_.size(); out[9] = steps_done_;
+        out[8] = live_joints(); out[9] = steps_done_;
         if (!uploaded_) return;
         const auto c = read_counters();
         out[3] = c.pairs; out[4] = c.man; out[6] = c.desc; out[7] = c.isl;
@@ -1419,7 +1452,7 @@ private:
         for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
         release_segment_graphs();
         d_.pair_cap = cap;
-        d_.desc_cap = cap + d_.n_joints;
+        d_.desc_cap = cap + d_.n_joints + kJointReserve;
         for (int k = 0; k < 2; ++k) {
             dalloc(sets_[k].key, cap, pair_owned_);
             dalloc(sets_[k].cache, cap, pair_owned_);
@@ -1513,6 +1546,71 @@ private:
         host_authoritative_ = false;
     }
 
+    uint32_t live_joints() const {
+        uint32_t n = 0;
+        for (const auto& j : joints_) n += j.live ? 1u : 0u;
+        return n;
+    }
+    // The device joint tables: live joints per scene, constraint slot
+    // descending (scene.cpp:7153-7162), their rows, and the constraints
+    // counted on each dynamic endpoint (scene.cpp:2728-2749).  Arrays are
+    // allocated for the current count (the old ones stay owned until the
+    // device state is released).
+    void upload_joints() {
+        std::vector<HostJoint> js;
+        for (const auto& j : joints_)
+            if (j.live) js.push_back(j);
+        std::stable_sort(js.begin(), js.end(), [](const HostJoint& a, const HostJoint& b) {
+            return a.scene != b.scene ? a.scene < b.scene : a.slot > b.slot;
+        });
+        const size_t n = js.size();
+        std::vector<uint32_t> ja(n), jb(n), jk(n), jr(n);
+        std::vector<float> jl(n);
+        std::vector<float4> jla(n), jlb(n), jqa(n), jqb(n);
+        uint32_t nrows = 0;
+        for (size_t i = 0; i < n; ++i) {
+            const HostJoint& h = js[i];
+            ja[i] = h.a; jb[i] = h.b; jl[i] = h.len; jk[i] = h.kind; jr[i] = nrows;
+            nrows += joint_rows(h.kind);
+            jla[i] = make_float4(h.la[0], h.la[1], h.la[2], 0);
+            jlb[i] = make_float4(h.lb[0], h.lb[1], h.lb[2], 0);
+            jqa[i] = make_float4(h.qa[0], h.qa[1], h.qa[2], h.qa[3]);
+            jqb[i] = make_float4(h.qb[0], h.qb[1], h.qb[2], h.qb[3]);
+        }
+        d_.n_joints = uint32_t(n);
+        d_.n_jrows = nrows;
+        dalloc(d_.j_a, n, owned_); dalloc(d_.j_b, n, owned_); dalloc(d_.j_len, n, owned_);
+        dalloc(d_.j_kind, n, owned_); dalloc(d_.j_row, n, owned_);
+        dalloc(d_.j_la, n, owned_); dalloc(d_.j_lb, n, owned_);
+        dalloc(d_.j_qa, n, owned_); dalloc(d_.j_qb, n, owned_);
+        dalloc(d_.jrow, nrows, owned_);
+        std::vector<uint32_t> jcount(bodies_.size(), 0u);
+        for (const auto& j : js) {
+            if (bodies_[j.a].dynamic) ++jcount[j.a];
+            if (bodies_[j.b].dynamic) ++jcount[j.b];
+        }
+        upload(d_.b_jcount, jcount, stream_);
+        upload(d_.j_a, ja, stream_); upload(d_.j_b, jb, stream_); upload(d_.j_len, jl, stream_);
+        upload(d_.j_kind, jk, stream_); upload(d_.j_row, jr, stream_);
+        upload(d_.j_la, jla, stream_); upload(d_.j_lb, jlb, stream_);
+        upload(d_.j_qa, jqa, stream_); upload(d_.j_qb, jqb, stream_);
+    }
+    // Joints added or retired after the device state exists: new joint
+    // tables, while bodies, pairs, PCM caches and friction histories stay
+    // (the reference keeps its contact managers across constraint edits).
+    // Descriptor arrays hold kJointReserve joints beyond the built count;
+    // past that the device state is rebuilt.
+    void refresh_joints() {
+        if (live_joints() > d_.desc_cap - d_.pair_cap) {
+            build_device();
+            return;
+        }
+        release_rollout();
+        for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        release_segment_graphs();
+        upload_joints();
+        check_cuda(cudaStreamSynchronize(stream_), "joint upload");
+    }
     void build_device() {
         release_device();
         DevState d;
@@ -1521,7 +1619,7 @@ private:
         d.n_scenes = nsc;
         d.n_bodies = nb;
         d.n_shapes = ns;
-        d.n_joints = uint32_t(joints_.size());
+        d.n_joints = live_joints();
         // finite ranks, scene ranges, plane pairs
         std::vector<int32_t> frank(ns, -1), dynrank(ns, -1);
         std::vector<uint32_t> sscene(ns), sbody(ns), stype(ns), static_pairs(ns, 0);
@@ -1594,11 +1692,6 @@ private:
         dalloc(d_.sw_cache, size_t(nf) * DevState::kSweepCache, owned_);
         dalloc(d_.sw_found, nf, owned_);
         dalloc(d_.own_cnt, ns, owned_); dalloc(d_.own_off, ns, owned_); dalloc(d_.own_cur, ns, owned_);
-        dalloc(d_.j_a, joints_.size(), owned_); dalloc(d_.j_b, joints_.size(), owned_);
-        dalloc(d_.j_len, joints_.size(), owned_);
-        dalloc(d_.j_kind, joints_.size(), owned_); dalloc(d_.j_row, joints_.size(), owned_);
-        dalloc(d_.j_la, joints_.size(), owned_); dalloc(d_.j_lb, joints_.size(), owned_);
-        dalloc(d_.j_qa, joints_.size(), owned_); dalloc(d_.j_qb, joints_.size(), owned_);
         dalloc(d_.sb_dv, nb, owned_); dalloc(d_.sb_dw, nb, owned_); dalloc(d_.sb_mdv, nb, owned_);
         dalloc(d_.sb_mdw, nb, owned_); dalloc(d_.sb_v, nb, owned_); dalloc(d_.sb_w, nb, owned_);
         dalloc(d_.sb_sqrt_i, size_t(nb) * 3, owned_);
@@ -1659,33 +1752,7 @@ private:
         upload(d_.m_tab, mtab, stream_); upload(d_.m_half, mhalf, stream_);
         upload(d_.hv, hv, stream_); upload(d_.hf, hf, stream_);
         upload(d_.hfr, hfr, stream_); upload(d_.hidx, hidx, stream_);
-        // joints: per scene, constraint slot descending (scene.cpp:7153-7162)
-        std::vector<HostJoint> js = joints_;
-        std::stable_sort(js.begin(), js.end(), [](const HostJoint& a, const HostJoint& b) {
-            return a.scene != b.scene ? a.scene < b.scene : a.slot > b.slot;
-        });
-        std::vector<uint32_t> ja(js.size()), jb(js.size()), jk(js.size()), jr(js.size());
-        std::vector<float> jl(js.size());
-        std::vector<float4> jla(js.size()), jlb(js.size()), jqa(js.size()), jqb(js.size());
-        uint32_t nrows = 0;
-        for (size_t i = 0; i < js.size(); ++i) {
-            const HostJoint& h = js[i];
-            ja[i] = h.a; jb[i] = h.b; jl[i] = h.len; jk[i] = h.kind; jr[i] = nrows;
-            nrows += joint_rows(h.kind);
-            jla[i] = make_float4(h.la[0], h.la[1], h.la[2], 0);
-            jlb[i] = make_float4(h.lb[0], h.lb[1], h.lb[2], 0);
-            jqa[i] = make_float4(h.qa[0], h.qa[1], h.qa[2], h.qa[3]);
-            jqb[i] = make_float4(h.qb[0], h.qb[1], h.qb[2], h.qb[3]);
-        }
-        d_.n_jrows = nrows;
-        dalloc(d_.jrow, nrows, owned_);
-        // constraints counted on their dynamic endpoints (scene.cpp:2728-2749)
-        std::vector<uint32_t> jcount(nb, 0u);
-        for (const auto& j : js) {
-            if (bodies_[j.a].dynamic) ++jcount[j.a];
-            if (bodies_[j.b].dynamic) ++jcount[j.b];
-        }
-        upload(d_.b_jcount, jcount, stream_);
+        upload_joints();
         upload(d_.sc_fbegin, fbegin, stream_); upload(d_.sc_plane, plane, stream_);
         upload(d_.small_scenes, small, stream_);
         upload(d_.b_dyn0, dyn0, stream_); upload(d_.b_dyn1, dyn1, stream_);
@@ -1694,10 +1761,6 @@ private:
         upload(d_.s_geom, geom, stream_); upload(d_.s_lp, lp, stream_); upload(d_.s_lq, lq, stream_);
         upload(d_.s_frank, frank, stream_); upload(d_.s_dynrank, dynrank, stream_);
         upload(d_.s_static_pairs, static_pairs, stream_);
-        upload(d_.j_a, ja, stream_); upload(d_.j_b, jb, stream_); upload(d_.j_len, jl, stream_);
-        upload(d_.j_kind, jk, stream_); upload(d_.j_row, jr, stream_);
-        upload(d_.j_la, jla, stream_); upload(d_.j_lb, jlb, stream_);
-        upload(d_.j_qa, jqa, stream_); upload(d_.j_qb, jqb, stream_);
         uploaded_ = true;
         upload_bodies();
         // pair capacity: every plane pair plus a generous overlap budget
@@ -1716,6 +1779,9 @@ private:
     std::vector<HostShape> shapes_;
     std::vector<std::shared_ptr<const CookedMesh>> meshes_;
     std::vector<HostJoint> joints_;
+    std::vector<std::vector<uint32_t>> free_joints_;   // per scene: retired slots, most recent last
+    bool joints_dirty_ = false;
+    static constexpr uint32_t kJointReserve = 256;
     std::vector<uint32_t> scene_body_begin_, scene_shape_begin_;
     std::vector<bool> scene_has_floor_;
     std::vector<uint32_t> h_fbegin_;
@@ -1919,6 +1985,9 @@ int fyzz_b200_attach_convex_shape(fyzz_b200_world* w, uint32_t body, const fyzz_
         const uint32_t s = W.attach_convex(body, mesh->mesh, local ? local : identity);
         if (out) *out = s;
     });
+}
+int fyzz_b200_remove_constraint(fyzz_b200_world* w, uint64_t id) {
+    return guarded(w, [&](auto& W) { W.remove_joint(id); });
 }
 int fyzz_b200_add_scene(fyzz_b200_world* w, uint32_t nb, const float* bodies, uint32_t ns,
                         const uint32_t* shape_body, const uint32_t* shape_type, const float* shape_geom,

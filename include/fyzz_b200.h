@@ -143,6 +143,12 @@ int fyzz_b200_add_revolute_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b
                                       const float local_b[7], uint64_t* id_out);
 int fyzz_b200_add_prismatic_constraint(fyzz_b200_world* w, uint32_t a, uint32_t b, const float local_a[7],
                                        const float local_b[7], uint64_t* id_out);
+/* World::remove_constraint (world.h:458, Scene::retire_constraint): the
+ * joint leaves the next step; ids are generation << 32 | slot and a
+ * retired slot is reused (generation + 1) by the scene's next joint.
+ * Unknown or expired ids return FYZZ_B200_INVALID_ARGUMENT.  Joints added
+ * or removed between steps keep the contact-manager history. */
+int fyzz_b200_remove_constraint(fyzz_b200_world* w, uint64_t id);
 
 /* Bulk authoring of one scene with the seeded-workload record layout:
  * bodies(14 floats: position 3, orientation 4, velocity 3, angular 3,

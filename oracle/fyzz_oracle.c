@@ -103,6 +103,9 @@ struct fo_scene {
     /* joint kind, authored endpoints and local frames (ConstraintRecord,
      * scene.h:1529-1545) */
     uint8_t* joint_kind; uint32_t* joint_auth; v3* joint_lp; qt* joint_lq;
+    /* constraint slots (scene.cpp:3110-3140, 3195-3228): live flag,
+     * generation, LIFO free list of retired slots; nj counts slots */
+    uint8_t* joint_live; uint32_t* joint_gen; uint32_t* joint_free; uint32_t nfree, jcap;
     int has_floor;
     uint32_t plane_shape;
     /* pair state */
@@ -370,7 +373,13 @@ fo_scene* fo_scene_create_ex(uint32_t nb, const float* bodies, uint32_t ns,
     s->joint_auth = (uint32_t*)calloc(2 * nj + 2, 4);
     s->joint_lp = (v3*)calloc(2 * nj + 2, sizeof(v3));
     s->joint_lq = (qt*)calloc(2 * nj + 2, sizeof(qt));
+    s->joint_live = (uint8_t*)calloc(nj + 1, 1);
+    s->joint_gen = (uint32_t*)calloc(nj + 1, 4);
+    s->joint_free = (uint32_t*)calloc(nj + 1, 4);
+    s->jcap = nj + 1;
     for (uint32_t j = 0; j < nj; ++j) {
+        s->joint_live[j] = 1;
+        s->joint_gen[j] = 1;
         /* 0xffffffff names the floor (actor 0) */
         const uint32_t a = joint_bodies[2 * j] == 0xffffffffu ? 0u : joint_bodies[2 * j] + off;
         const uint32_t b = joint_bodies[2 * j + 1] == 0xffffffffu ? 0u : joint_bodies[2 * j + 1] + off;
@@ -422,6 +431,70 @@ int fo_scene_set_joint(fo_scene* s, uint32_t j, uint32_t kind, const float* la, 
     }
     return 0;
 }
+/* Scene::add_joint / create_*_constraint after creation (scene.cpp:3110-
+ * 3140): the most recently retired slot is reused with its generation
+ * bumped, else a new slot is appended; counted interactions follow. */
+int fo_scene_add_joint(fo_scene* s, uint32_t kind, uint32_t a_in, uint32_t b_in, const float* la, const float* lb,
+                       float dist, uint64_t* id_out) {
+    const uint32_t off = s->has_floor ? 1u : 0u;
+    const uint32_t a = a_in == 0xffffffffu ? 0u : a_in + off;
+    const uint32_t b = b_in == 0xffffffffu ? 0u : b_in + off;
+    if (kind > FO_JOINT_PRISMATIC || a >= s->na || b >= s->na || a == b) FAIL(FO_INVALID, "joint endpoints or kind");
+    if (!s->actors[a].dynamic && !s->actors[b].dynamic)
+        FAIL(FO_LOGIC, "Rigid constraint requires a dynamic solver node");
+    uint32_t j;
+    if (s->nfree) {
+        j = s->joint_free[--s->nfree];
+    } else {
+        j = s->nj;
+        if (j + 1 >= s->jcap) {
+            const uint32_t cap = 2 * s->jcap + 4;
+            s->joint_a = (uint32_t*)realloc(s->joint_a, 4ull * cap);
+            s->joint_b = (uint32_t*)realloc(s->joint_b, 4ull * cap);
+            s->joint_len = (float*)realloc(s->joint_len, 4ull * cap);
+            s->joint_kind = (uint8_t*)realloc(s->joint_kind, cap);
+            s->joint_auth = (uint32_t*)realloc(s->joint_auth, 8ull * cap);
+            s->joint_lp = (v3*)realloc(s->joint_lp, 2 * sizeof(v3) * cap);
+            s->joint_lq = (qt*)realloc(s->joint_lq, 2 * sizeof(qt) * cap);
+            s->joint_live = (uint8_t*)realloc(s->joint_live, cap);
+            s->joint_gen = (uint32_t*)realloc(s->joint_gen, 4ull * cap);
+            s->joint_free = (uint32_t*)realloc(s->joint_free, 4ull * cap);
+            s->jcap = cap;
+        }
+        s->joint_gen[j] = 0;
+        ++s->nj;
+    }
+    s->joint_a[j] = a < b ? a : b;
+    s->joint_b[j] = a < b ? b : a;
+    s->joint_len[j] = dist;
+    s->joint_kind[j] = FO_JOINT_CENTER;
+    s->joint_auth[2 * j] = a;
+    s->joint_auth[2 * j + 1] = b;
+    s->joint_lp[2 * j] = s->joint_lp[2 * j + 1] = V3(0, 0, 0);
+    s->joint_lq[2 * j] = s->joint_lq[2 * j + 1] = Q4(0, 0, 0, 1);
+    s->joint_live[j] = 1;
+    s->joint_gen[j] += 1;
+    if (kind != FO_JOINT_CENTER) {
+        const int rc = fo_scene_set_joint(s, j, kind, la, lb);
+        if (rc) return rc;
+    }
+    if (s->actors[a].dynamic) ++s->actors[a].joints;
+    if (s->actors[b].dynamic) ++s->actors[b].joints;
+    if (id_out) *id_out = ((uint64_t)s->joint_gen[j] << 32) | j;
+    return 0;
+}
+/* Scene::retire_constraint (scene.cpp:3088-3096, 3195-3228) */
+int fo_scene_remove_joint(fo_scene* s, uint64_t id) {
+    const uint32_t j = (uint32_t)id, gen = (uint32_t)(id >> 32);
+    if (j >= s->nj || !gen || !s->joint_live[j] || s->joint_gen[j] != gen)
+        FAIL(FO_INVALID, "Unknown or expired rigid constraint");
+    s->joint_live[j] = 0;
+    s->joint_free[s->nfree++] = j;
+    const uint32_t a = s->joint_a[j], b = s->joint_b[j];
+    if (s->actors[a].dynamic) --s->actors[a].joints;
+    if (s->actors[b].dynamic) --s->actors[b].joints;
+    return 0;
+}
 static uint32_t joint_rows(uint8_t kind) {
     return kind <= FO_JOINT_ANCHORED ? 1u : kind == FO_JOINT_SPHERICAL ? 3u : kind == FO_JOINT_FIXED ? 6u : 5u;
 }
@@ -430,6 +503,7 @@ void fo_scene_destroy(fo_scene* s) {
     if (!s) return;
     free(s->actors); free(s->shapes); free(s->joint_a); free(s->joint_b); free(s->joint_len);
     free(s->joint_kind); free(s->joint_auth); free(s->joint_lp); free(s->joint_lq);
+    free(s->joint_live); free(s->joint_gen); free(s->joint_free);
     free(s->mgr); free(s->found); free(s->lost); free(s->man); free(s->desc); free(s->pend);
     free(s->impulses); free(s->sorted_minx_val); free(s->sorted_minx_id);
     for (uint32_t m = 0; m < s->nmeshes; ++m) fo_mesh_free(&s->meshes[m]);
@@ -812,6 +886,7 @@ static void sleep_islands(fo_scene* s) {
             a = s->shapes[(uint32_t)(m->key >> 32)].body;
             b = s->shapes[(uint32_t)m->key].body;
         } else {
+            if (!s->joint_live[i - s->nmgr]) continue;
             a = s->joint_a[i - s->nmgr];
             b = s->joint_b[i - s->nmgr];
         }
@@ -853,7 +928,7 @@ static void sleep_islands(fo_scene* s) {
             if (s->actors[a].dynamic && s->actors[b].dynamic) uf_join(par, a, b);
         }
         for (uint32_t j = 0; j < s->nj; ++j)
-            if (s->actors[s->joint_a[j]].dynamic && s->actors[s->joint_b[j]].dynamic)
+            if (s->joint_live[j] && s->actors[s->joint_a[j]].dynamic && s->actors[s->joint_b[j]].dynamic)
                 uf_join(par, s->joint_a[j], s->joint_b[j]);
         for (uint32_t i = 0; i < na; ++i)
             if (act[i]) flag[uf_root(par, i)] = 1;
@@ -874,7 +949,7 @@ static void sleep_islands(fo_scene* s) {
         if (s->actors[a].dynamic && s->actors[b].dynamic) uf_join(par, a, b);
     }
     for (uint32_t j = 0; j < s->nj; ++j)
-        if (s->actors[s->joint_a[j]].dynamic && s->actors[s->joint_b[j]].dynamic)
+        if (s->joint_live[j] && s->actors[s->joint_a[j]].dynamic && s->actors[s->joint_b[j]].dynamic)
             uf_join(par, s->joint_a[j], s->joint_b[j]);
     for (uint32_t i = 0; i < na; ++i) {
         const actor_t* a = &s->actors[i];
@@ -955,6 +1030,7 @@ int fo_scene_step(fo_scene* s, float dt, const uint64_t* manager_order, uint64_t
     uint64_t* jo = (uint64_t*)malloc(8 * (njo_in + 1));
     for (uint64_t i = 0; i < njo_in; ++i) {
         const uint64_t ji = joint_order ? joint_order[i] : (s->nj - 1 - i);
+        if (ji >= s->nj || !s->joint_live[ji]) continue;
         if (ASLEEP(s->joint_a[ji]) || ASLEEP(s->joint_b[ji])) continue;
         jo[njo++] = ji;
     }

@@ -128,6 +128,13 @@ uint64_t fo_scene_sorted_min_x(const fo_scene* s, uint32_t* values, uint32_t* id
  * each; orientations are validated and normalised as World and Scene do;
  * the distance kinds use the positions only).  Call before stepping. */
 int fo_scene_set_joint(fo_scene* s, uint32_t j, uint32_t kind, const float* local_a7, const float* local_b7);
+/* A joint added after creation (kind, 0-based dynamic bodies or 0xffffffff
+ * for the floor, local frames, distance): reuses the most recently retired
+ * constraint slot; id = generation << 32 | slot. */
+int fo_scene_add_joint(fo_scene* s, uint32_t kind, uint32_t a, uint32_t b, const float* local_a7,
+                       const float* local_b7, float distance, uint64_t* id_out);
+/* Retires a joint by id (World::remove_constraint). */
+int fo_scene_remove_joint(fo_scene* s, uint64_t id);
 /* Kinematic mode of an actor (before stepping) and its target pose
  * (position 3 + quaternion xyzw 4). */
 int fo_scene_set_kinematic(fo_scene* s, uint32_t actor, int on);

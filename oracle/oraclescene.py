@@ -48,6 +48,8 @@ def lib():
         L.fo_scene_normal_impulses.argtypes = [vp, vp]
         L.fo_scene_set_sleeping.argtypes = [vp, i32]
         L.fo_scene_set_joint.argtypes = [vp, u32, u32, vp, vp]
+        L.fo_scene_add_joint.argtypes = [vp, u32, u32, u32, vp, vp, f32, vp]
+        L.fo_scene_remove_joint.argtypes = [vp, u64]
         L.fo_scene_set_kinematic.argtypes = [vp, u32, i32]
         L.fo_scene_set_kinematic_target.argtypes = [vp, u32, vp]
         L.fo_scene_sleep_state.argtypes = [vp, vp]
@@ -133,6 +135,18 @@ class OracleScene:
 
     def _actor(self, body: int) -> int:
         return body + (0 if self.spec.floor is None else 1)
+
+    def add_joint(self, kind, a, b, local_a=None, local_b=None, distance=0.0) -> int:
+        ident = np.array([0, 0, 0, 0, 0, 0, 1], np.float32)
+        la = np.ascontiguousarray(ident if local_a is None else local_a, np.float32).reshape(7)
+        lb = np.ascontiguousarray(ident if local_b is None else local_b, np.float32).reshape(7)
+        out = np.zeros(1, np.uint64)
+        self._check(lib().fo_scene_add_joint(self.h, int(kind), int(a), int(b), _p(la), _p(lb), float(distance),
+                                             _p(out)))
+        return int(out[0])
+
+    def remove_joint(self, cid: int):
+        self._check(lib().fo_scene_remove_joint(self.h, int(cid)))
 
     def set_kinematic(self, body: int, on: bool = True):
         """Kinematic mode of dynamic body `body` (0-based index in the spec)."""

@@ -179,7 +179,7 @@ int fz_ref_build(void* p, uint32_t nb, const float* bodies, uint32_t ns,
 // 2 fixed, 3 spherical, 4 revolute, 5 prismatic.  a / b are 0-based dynamic
 // body indices, 0xffffffff for the floor; local poses are 7 floats.
 int fz_ref_add_joint(void* p, int kind, uint32_t a, uint32_t b, const float* la, const float* lb,
-                     float distance) {
+                     float distance, uint64_t* id_out) {
     auto* h = static_cast<Handle*>(p);
     return guarded([&] {
         auto body = [&](uint32_t i) -> fyzz::BodyId {
@@ -191,19 +191,27 @@ int fz_ref_add_joint(void* p, int kind, uint32_t a, uint32_t b, const float* la,
         };
         Scene& s = *h->scene;
         const fyzz::BodyId A = body(a), B = body(b);
+        fyzz::ConstraintId id{};
         if (kind == 0) {
-            s.create_center_distance_constraint(A, B, distance);
+            id = s.create_center_distance_constraint(A, B, distance);
         } else if (kind == 1) {
-            s.create_anchored_distance_constraint(A, B, {la[0], la[1], la[2]}, {lb[0], lb[1], lb[2]}, distance);
+            id = s.create_anchored_distance_constraint(A, B, {la[0], la[1], la[2]}, {lb[0], lb[1], lb[2]}, distance);
         } else {
             const fyzz::Transform ta = transform_of(la), tb = transform_of(lb);
-            if (kind == 2) s.create_fixed_constraint(A, B, ta, tb);
-            else if (kind == 3) s.create_spherical_constraint(A, B, ta, tb);
-            else if (kind == 4) s.create_revolute_constraint(A, B, ta, tb);
-            else if (kind == 5) s.create_prismatic_constraint(A, B, ta, tb);
+            if (kind == 2) id = s.create_fixed_constraint(A, B, ta, tb);
+            else if (kind == 3) id = s.create_spherical_constraint(A, B, ta, tb);
+            else if (kind == 4) id = s.create_revolute_constraint(A, B, ta, tb);
+            else if (kind == 5) id = s.create_prismatic_constraint(A, B, ta, tb);
             else throw std::invalid_argument("joint kind");
         }
+        if (id_out) *id_out = static_cast<uint64_t>(id);
     });
+}
+
+// World::remove_constraint (src/world.cpp:277-279 -> Scene::retire_constraint).
+int fz_ref_remove_joint(void* p, uint64_t id) {
+    auto* h = static_cast<Handle*>(p);
+    return guarded([&] { h->scene->retire_constraint(static_cast<fyzz::ConstraintId>(id)); });
 }
 
 // Scene::set_kinematic / set_kinematic_target (scene.cpp:858-1003) for the

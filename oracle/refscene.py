@@ -38,7 +38,8 @@ def lib():
         L.fz_ref_body_states.argtypes = [vp, vp]
         L.fz_ref_mass_props.argtypes = [vp, vp]
         L.fz_ref_sleep_state.argtypes = [vp, vp]
-        L.fz_ref_add_joint.argtypes = [vp, i32, u32, u32, vp, vp, f32]
+        L.fz_ref_add_joint.argtypes = [vp, i32, u32, u32, vp, vp, f32, vp]
+        L.fz_ref_remove_joint.argtypes = [vp, u64]
         L.fz_ref_set_kinematic.argtypes = [vp, u32, i32]
         L.fz_ref_set_kinematic_target.argtypes = [vp, u32, vp]
         L.fz_ref_encoded_bounds.argtypes = [vp, vp]
@@ -108,7 +109,7 @@ class RefScene:
             for j in range(spec.joints.shape[0]):
                 la, lb = np.ascontiguousarray(local[j, :7]), np.ascontiguousarray(local[j, 7:])
                 self._check(L.fz_ref_add_joint(self.h, int(jk[j]), int(spec.joints[j, 0]), int(spec.joints[j, 1]),
-                                               _p(la), _p(lb), float(spec.joint_dist[j])))
+                                               _p(la), _p(lb), float(spec.joint_dist[j]), None))
 
     def _check(self, rc):
         if rc:
@@ -139,6 +140,20 @@ class RefScene:
         out = np.zeros((n, 14), np.float32)
         lib().fz_ref_body_states(self.h, _p(out))
         return out
+
+    def add_joint(self, kind, a, b, local_a=None, local_b=None, distance=0.0) -> int:
+        """A joint between 0-based dynamic bodies (0xffffffff: the floor);
+        returns its ConstraintId."""
+        ident = np.array([0, 0, 0, 0, 0, 0, 1], np.float32)
+        la = np.ascontiguousarray(ident if local_a is None else local_a, np.float32).reshape(7)
+        lb = np.ascontiguousarray(ident if local_b is None else local_b, np.float32).reshape(7)
+        out = np.zeros(1, np.uint64)
+        self._check(lib().fz_ref_add_joint(self.h, int(kind), int(a), int(b), _p(la), _p(lb), float(distance),
+                                           _p(out)))
+        return int(out[0])
+
+    def remove_joint(self, cid: int):
+        self._check(lib().fz_ref_remove_joint(self.h, int(cid)))
 
     def set_kinematic(self, body: int, on: bool = True):
         """Kinematic mode of dynamic body `body` (0-based index in the spec)."""

@@ -145,3 +145,26 @@ def test_convex_validation(pkg, scenes):
         w.attach_convex_shape(b, mesh, (0, 0, 0, 0, 0, 0, 2.0))
     s = w.attach_convex_shape(b, mesh)
     assert s == 0
+
+
+def test_many_sided_faces_take_the_lane_zero_clipping(pkg, ref, scenes):
+    # 70-sided prisms stacked flat: their caps have more vertices than the
+    # warp clipping stages, so the lane-0 clipping runs; fresh manifolds
+    # still match the reference
+    spec = scenes.convex_pile(6, seed=1, xz=0.0, frac_other=0.0)
+    spec.convex_meshes = [scenes.hull_prism(70, 0.3, 0.1)]
+    spec.shape_geom[:, 0] = 0
+    spec.shape_local[:] = [0, 0, 0, 0, 0, 0, 1]
+    spec.bodies[:, 3:7] = [0, 0, 0, 1]
+    for i in range(6):
+        spec.bodies[i, 0:3] = [0.01 * i, 0.099 + 0.199 * i, 0.0]
+    w = world_of(pkg, spec)
+    w.collide()
+    r = ref.RefScene(spec)
+    r.advance_collision()
+    wp, wc, wpts = w.manifolds()
+    rp, rc, _, rpts = r.manifolds()
+    np.testing.assert_array_equal(wp, rp)
+    np.testing.assert_array_equal(wc, rc)
+    assert wc.sum() >= 20
+    assert rel_err(wpts, rpts) <= CONTACT_RTOL

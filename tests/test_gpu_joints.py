@@ -107,3 +107,44 @@ def test_joint_validation(pkg, scenes):
     assert np.all(np.isfinite(w.read_bodies()))
     with pytest.raises(RuntimeError):
         w.rollout_begin(4, 2)
+
+
+def test_removed_and_added_joints_track_oracle(pkg, oracle, scenes):
+    # a pile settling onto the floor with eight center distance joints: at
+    # step 10 (19 touching managers) two joints are retired and two new ones
+    # take their slots; the run goes on from the same contact history and
+    # tracks the oracle (which keeps it, like the reference) as closely as
+    # an unedited short run does
+    spec = scenes.random_boxes(30, seed=5, xz=2.0, y=(0.4, 2.0))
+    pairs = np.array([[2 * i, 2 * i + 1] for i in range(8)], np.uint32)
+    spec.joints = pairs
+    spec.joint_dist = np.linalg.norm(spec.bodies[pairs[:, 0], 0:3] - spec.bodies[pairs[:, 1], 0:3],
+                                     axis=1).astype(np.float32)
+    w = pkg.World(0)
+    first = w.add_scene(spec)
+    o = oracle.OracleScene(spec)
+    for k in range(10):
+        w.step(DT)
+        o.step(DT)
+    assert w.counts()["managers"] > 10
+    for cid in ((1 << 32) | 3, (1 << 32) | 6):
+        w.remove_constraint(cid)
+        o.remove_joint(cid)
+    st = o.body_states()
+    da = float(np.linalg.norm(st[21, 0:3] - st[22, 0:3]))
+    db = float(np.linalg.norm(st[7, 0:3] - st[10, 0:3]))
+    got = [w.add_center_distance_constraint(first + 20, first + 21, da),
+           w.add_center_distance_constraint(first + 6, first + 9, db)]
+    want = [o.add_joint(0, 20, 21, None, None, da), o.add_joint(0, 6, 9, None, None, db)]
+    assert got == want == [(2 << 32) | 6, (2 << 32) | 3]
+    assert w.counts()["joints"] == 8
+    for k in range(14):
+        w.step(DT)
+        o.step(DT)
+    ws, os_ = w.read_bodies(), o.body_states()
+    assert rel_err(ws[:, 0:3], os_[:, 0:3], floor=1.0) <= 1e-4
+    assert rel_err(ws[:, 3:6], os_[:, 3:6], floor=0.1) <= 1e-2
+    with pytest.raises((ValueError, RuntimeError)):
+        w.remove_constraint((1 << 32) | 3)       # expired generation
+    with pytest.raises((ValueError, RuntimeError)):
+        w.remove_constraint((1 << 32) | 9999)    # unknown slot
