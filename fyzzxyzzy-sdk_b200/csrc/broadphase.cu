@@ -294,7 +294,7 @@ void enqueue_broadphase(const DevState& s, cudaStream_t st, const StageHook& hoo
     for (uint32_t i = 0; i < s.n_large; ++i)
         radix_sort_pairs(s.srt_key + s.large_begin[i], s.srt_id + s.large_begin[i],
                          s.srt_key2, s.srt_id2, s.large_n[i], nullptr, 0, 32,
-                         s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st);
+                         s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err);
     hook(kStPairs, st);
     if (s.n_finite) {
         k_sweep_gather<<<(s.n_finite + T - 1) / T, T, 0, st>>>(s, rec, meta);
@@ -304,7 +304,7 @@ void enqueue_broadphase(const DevState& s, cudaStream_t st, const StageHook& hoo
     const uint32_t sweep_threads = kSweepWarps * 32;
     const uint32_t sweep_blocks = s.n_finite ? (s.n_finite + sweep_threads - 1) / sweep_threads : 0;
     if (sweep_blocks) k_sweep<<<sweep_blocks, sweep_threads, 0, st>>>(s, rec, meta, 0);
-    scan_exclusive(s.own_cnt, s.own_off, s.n_shapes, nullptr, s.cur.n, s.scan_tmp, s.scan_tmp_words, st);
+    scan_exclusive(s.own_cnt, s.own_off, s.n_shapes, nullptr, s.cur.n, s.scan_tmp, s.scan_tmp_words, st, s.err);
     k_pair_total<<<1, 32, 0, st>>>(s);
     if (sweep_blocks) k_sweep<<<sweep_blocks, sweep_threads, 0, st>>>(s, rec, meta, 1);
     k_owner_sort<<<(s.n_shapes + T - 1) / T, T, 0, st>>>(s);

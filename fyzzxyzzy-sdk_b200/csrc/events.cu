@@ -168,15 +168,15 @@ void enqueue_events(const DevState& s, cudaStream_t st) {
     const uint32_t T = 256;
     k_ev_lost_flags<<<blocks_for(s.pair_cap, T), T, 0, st>>>(s, s.tmp_flags);
     scan_exclusive(s.tmp_flags, s.tmp_pos, s.pair_cap, s.prev.n, s.counters + kCntLost, s.scan_tmp,
-                   s.scan_tmp_words, st);
+                   s.scan_tmp_words, st, s.err);
     k_ev_lost_scatter<<<blocks_for(s.pair_cap, T), T, 0, st>>>(s, s.tmp_flags, s.tmp_pos);
     // the lost-touch flags are consumed: tmp_flags / tmp_pos now hold the
     // reported managers
     k_ev_counts<<<blocks_for(s.pair_cap, T), T, 0, st>>>(s, s.tmp_flags);
     scan_exclusive(s.tmp_flags, s.tmp_pos, s.pair_cap, s.counters + kCntMan, s.counters + kCntReported,
-                   s.scan_tmp, s.scan_tmp_words, st);
+                   s.scan_tmp, s.scan_tmp_words, st, s.err);
     scan_exclusive(s.ev_cnt, s.ev_pt_off, s.pair_cap, s.counters + kCntMan, s.counters + kCntEvPts,
-                   s.scan_tmp, s.scan_tmp_words, st);
+                   s.scan_tmp, s.scan_tmp_words, st, s.err);
     k_ev_managers<<<blocks_for(s.pair_cap, T), T, 0, st>>>(s, s.tmp_flags, s.tmp_pos);
     k_ev_lost<<<blocks_for(s.pair_cap, T), T, 0, st>>>(s, s.tmp_pos);
 }

@@ -1,6 +1,14 @@
 // Data-parallel primitives used by the step: exclusive scan and a stable
 // LSD radix sort of (u32 key, u32 value) pairs.
 //
+// The scan is one launch with decoupled look-back (Merrill and Garland,
+// "Single-pass Parallel Prefix Scan with Decoupled Look-back", 2016): tiles
+// take ids in the order their blocks start, publish their sum, then walk back
+// one warp-width of predecessors at a time until an inclusive prefix is
+// found, and publish their own.  Tile states carry the launch's epoch, so
+// they need no reset between scans; every wait is bounded and reports
+// kErrLogic instead of hanging.
+//
 // The radix sort processes 8-bit digits.  Each pass is three launches:
 //   histogram  per 2048-key tile, 256 bins in shared memory
 //   scan       exclusive scan of the digit-major histogram (tile order
@@ -49,57 +57,97 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t& excl, 
     return total;
 }
 
-__global__ void k_scan_reduce(const uint32_t* __restrict__ in, uint32_t n, const uint32_t* n_dev,
-                              uint32_t* __restrict__ sums) {
-    __shared__ uint32_t sm[kScanThreads / 32 + 1];
-    const uint32_t lim = n_dev ? min(n, *n_dev) : n;
-    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
-    uint32_t s = 0;
-#pragma unroll
-    for (int i = 0; i < kScanItems; ++i)
-        if (base + i < lim) s += in[base + i];
-    uint32_t excl;
-    const uint32_t total = block_excl_scan<kScanThreads>(s, excl, sm);
-    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+// Scan scratch: [0] epoch, [1] tile ticket, [2] finished blocks, [3] pad,
+// then one 64-bit state per tile: epoch (30 bits) | status (2 bits: 1 sum
+// of the tile, 2 inclusive prefix) | value (32 bits).
+constexpr uint32_t kScanHeader = 4;
+constexpr uint32_t kLookbackSpin = 1u << 18;
+__device__ __forceinline__ unsigned long long scan_state_load(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
 }
-
-__global__ void k_scan_sums(uint32_t* sums, uint32_t nb, uint32_t* total) {
-    __shared__ uint32_t sm[1024 / 32 + 1];
-    __shared__ uint32_t carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (uint32_t base = 0; base < nb; base += 1024) {
-        const uint32_t i = base + threadIdx.x;
-        const uint32_t v = i < nb ? sums[i] : 0u;
-        uint32_t excl;
-        const uint32_t t = block_excl_scan<1024>(v, excl, sm);
-        if (i < nb) sums[i] = excl + carry;
-        __syncthreads();
-        if (threadIdx.x == 0) carry += t;
-        __syncthreads();
+__device__ __forceinline__ void scan_state_store(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__global__ void __launch_bounds__(kScanThreads) k_scan_lookback(const uint32_t* in, uint32_t* out, uint32_t n,
+                                                               const uint32_t* n_dev, uint32_t* total,
+                                                               uint32_t* tmp, uint32_t* err) {
+    __shared__ uint32_t sm[kScanThreads / 32 + 1];
+    __shared__ uint32_t s_tile, s_epoch, s_prefix;
+    unsigned long long* state = reinterpret_cast<unsigned long long*>(tmp + kScanHeader);
+    if (threadIdx.x == 0) {
+        s_tile = atomicAdd(&tmp[1], 1u);
+        s_epoch = *reinterpret_cast<volatile uint32_t*>(&tmp[0]) & 0x3fffffffu;
     }
-    if (threadIdx.x == 0 && total) *total = carry;
-}
-
-__global__ void k_scan_apply(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t n,
-                             const uint32_t* n_dev, const uint32_t* __restrict__ sums) {
-    __shared__ uint32_t sm[kScanThreads / 32 + 1];
+    __syncthreads();
+    const uint32_t tile = s_tile, epoch = s_epoch;
     const uint32_t lim = n_dev ? min(n, *n_dev) : n;
-    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    const uint32_t base = tile * kScanTile + threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
-    uint32_t s = 0;
+    uint32_t sum = 0;
 #pragma unroll
     for (int i = 0; i < kScanItems; ++i) {
         v[i] = base + i < lim ? in[base + i] : 0u;
-        s += v[i];
+        sum += v[i];
     }
     uint32_t excl;
-    block_excl_scan<kScanThreads>(s, excl, sm);
-    uint32_t run = excl + sums[blockIdx.x];
+    const uint32_t agg = block_excl_scan<kScanThreads>(sum, excl, sm);
+    const bool live = tile * kScanTile < lim;
+    if (live && threadIdx.x < 32) {
+        const uint32_t lane = threadIdx.x;
+        const unsigned long long tag = (unsigned long long)epoch << 34;
+        if (lane == 0)
+            scan_state_store(&state[tile], tag | ((tile == 0 ? 2ull : 1ull) << 32) | agg);
+        uint32_t prefix = 0;
+        int64_t look = int64_t(tile) - 1;
+        bool failed = false;
+        while (look >= 0) {
+            const int64_t idx = look - int64_t(lane);
+            uint32_t status = 2u, value = 0u;     // before tile 0: an empty prefix
+            if (idx >= 0) {
+                uint32_t spins = 0;
+                for (;;) {
+                    const unsigned long long st = scan_state_load(&state[idx]);
+                    status = uint32_t(st >> 32) & 3u;
+                    if ((st >> 34) == epoch && status != 0u) { value = uint32_t(st); break; }
+                    if (++spins == kLookbackSpin) { failed = true; status = 2u; value = 0u; break; }
+                }
+            }
+            const uint32_t pmask = __ballot_sync(0xffffffffu, status == 2u);
+            const int stop = pmask ? __ffs(pmask) - 1 : 31;
+            uint32_t part = int(lane) <= stop ? value : 0u;
+            for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
+            prefix += part;
+            if (pmask) break;
+            look -= 32;
+        }
+        if (__any_sync(0xffffffffu, failed) && lane == 0 && err) atomicOr(err, kErrLogic);
+        if (lane == 0) {
+            if (tile != 0) scan_state_store(&state[tile], tag | (2ull << 32) | (prefix + agg));
+            s_prefix = prefix;
+            if (total && (tile + 1) * kScanTile >= lim) *total = prefix + agg;
+        }
+    }
+    if (!live && tile == 0 && threadIdx.x == 0 && total) *total = 0u;
+    __syncthreads();
+    if (live) {
+        uint32_t run = excl + s_prefix;
 #pragma unroll
-    for (int i = 0; i < kScanItems; ++i) {
-        if (base + i < lim) out[base + i] = run;
-        run += v[i];
+        for (int i = 0; i < kScanItems; ++i) {
+            if (base + i < lim) out[base + i] = run;
+            run += v[i];
+        }
+    }
+    // the last block to finish opens the next epoch and resets the ticket
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&tmp[2], 1u) == gridDim.x - 1) {
+            tmp[0] = (epoch + 1u) & 0x3fffffffu;
+            tmp[1] = 0u;
+            tmp[2] = 0u;
+            __threadfence();
+        }
     }
 }
 
@@ -173,20 +221,22 @@ __global__ void k_radix_scatter(const uint32_t* __restrict__ kin, const uint32_t
 }  // namespace
 
 size_t scan_tmp_words_for(uint32_t n_cap) {
-    return (n_cap + kScanTile - 1) / kScanTile + 1;
+    return kScanHeader + 2 * (size_t((n_cap + kScanTile - 1) / kScanTile) + 1);
 }
 
+// The scratch must be zero when first used (world allocation clears it).
 void scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, const uint32_t* n_dev,
-                    uint32_t* total, uint32_t* tmp, size_t tmp_words, cudaStream_t st) {
+                    uint32_t* total, uint32_t* tmp, size_t tmp_words, cudaStream_t st, uint32_t* err) {
     const uint32_t nb = (n + kScanTile - 1) / kScanTile;
     if (nb == 0) {
         if (total) cudaMemsetAsync(total, 0, 4, st);
         return;
     }
-    (void)tmp_words;
-    k_scan_reduce<<<nb, kScanThreads, 0, st>>>(in, n, n_dev, tmp);
-    k_scan_sums<<<1, 1024, 0, st>>>(tmp, nb, total);
-    k_scan_apply<<<nb, kScanThreads, 0, st>>>(in, out, n, n_dev, tmp);
+    if (scan_tmp_words_for(n) > tmp_words) {   // never: callers size the scratch for their largest scan
+        if (err) cudaMemsetAsync(err, 0xff, 4, st);
+        return;
+    }
+    k_scan_lookback<<<nb, kScanThreads, 0, st>>>(in, out, n, n_dev, total, tmp, err);
 }
 
 size_t radix_hist_words(uint32_t n_cap) {
@@ -198,7 +248,7 @@ size_t radix_hist_words(uint32_t n_cap) {
 void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
                       uint32_t n_cap, const uint32_t* n_dev, int begin_bit, int end_bit,
                       uint32_t* hist, size_t hist_words, uint32_t* scan_tmp, size_t scan_words,
-                      cudaStream_t st) {
+                      cudaStream_t st, uint32_t* err) {
     const uint32_t ntiles = (n_cap + kSortTile - 1) / kSortTile;
     if (ntiles == 0) return;
     (void)hist_words;
@@ -206,7 +256,7 @@ void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32
     int passes = 0;
     for (int shift = begin_bit; shift < end_bit; shift += 8, ++passes) {
         k_radix_hist<<<ntiles, kSortThreads, 0, st>>>(ki, n_cap, n_dev, shift, hist, ntiles);
-        scan_exclusive(hist, hist, 256u * ntiles, nullptr, nullptr, scan_tmp, scan_words, st);
+        scan_exclusive(hist, hist, 256u * ntiles, nullptr, nullptr, scan_tmp, scan_words, st, err);
         k_radix_scatter<<<ntiles, kSortThreads, 0, st>>>(ki, vi, ko, vo, n_cap, n_dev, shift, hist, ntiles);
         uint32_t* t = ki; ki = ko; ko = t;
         t = vi; vi = vo; vo = t;

@@ -1882,7 +1882,7 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     k_bodies_begin<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
     // touching managers in canonical pair order
     k_touch_flags<<<grid_for(s.pair_cap, T, cap_blocks), T, 0, st>>>(s, flags);
-    scan_exclusive(flags, pos, s.pair_cap, s.cur.n, s.counters + kCntMan, s.scan_tmp, s.scan_tmp_words, st);
+    scan_exclusive(flags, pos, s.pair_cap, s.cur.n, s.counters + kCntMan, s.scan_tmp, s.scan_tmp_words, st, s.err);
     k_touch_scatter<<<grid_for(s.pair_cap, T, cap_blocks), T, 0, st>>>(s, flags, pos);
     // islands
     k_desc_bodies<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
@@ -1903,9 +1903,10 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     int bits = 1;
     while ((1ull << bits) < uint64_t(s.n_bodies) + 1u) ++bits;
     radix_sort_pairs(s.d_key, s.d_val, s.d_key2, s.d_val2, s.desc_cap, s.counters + kCntDesc, 0,
-                     (bits + 7) / 8 * 8, s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st);
+                     (bits + 7) / 8 * 8, s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err);
     k_island_flags<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
-    scan_exclusive(s.isl_flag, pos, s.desc_cap, s.counters + kCntAwake, s.n_isl, s.scan_tmp, s.scan_tmp_words, st);
+    scan_exclusive(s.isl_flag, pos, s.desc_cap, s.counters + kCntAwake, s.n_isl, s.scan_tmp, s.scan_tmp_words, st,
+                   s.err);
     k_island_scatter<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s, pos);
     cudaMemsetAsync(s.counters + kCntList, 0, 4 * sizeof(uint32_t), st);
     k_island_classes<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);

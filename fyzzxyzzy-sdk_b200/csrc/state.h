@@ -186,11 +186,11 @@ struct DevState {
 
 // primitives.cu
 void scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, const uint32_t* n_dev,
-                    uint32_t* total, uint32_t* tmp, size_t tmp_words, cudaStream_t st);
+                    uint32_t* total, uint32_t* tmp, size_t tmp_words, cudaStream_t st, uint32_t* err = nullptr);
 void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
                       uint32_t n_cap, const uint32_t* n_dev, int begin_bit, int end_bit,
                       uint32_t* hist, size_t hist_words, uint32_t* scan_tmp, size_t scan_words,
-                      cudaStream_t st);
+                      cudaStream_t st, uint32_t* err = nullptr);
 size_t radix_hist_words(uint32_t n_cap);
 size_t scan_tmp_words_for(uint32_t n_cap);
 

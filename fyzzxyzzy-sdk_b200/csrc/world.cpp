@@ -1493,6 +1493,7 @@ private:
         const uint32_t big = std::max({cap, dc, d_.n_shapes, d_.n_finite, 256u * 64u});
         d_.scan_tmp_words = scan_tmp_words_for(std::max<uint32_t>(big, uint32_t(radix_hist_words(big))));
         dalloc(d_.scan_tmp, d_.scan_tmp_words, pair_owned_);
+        check_cuda(cudaMemsetAsync(d_.scan_tmp, 0, d_.scan_tmp_words * 4, stream_), "memset");   // scan epochs start clear
         d_.sort_hist_words = radix_hist_words(big);
         dalloc(d_.sort_hist, d_.sort_hist_words, pair_owned_);
         if (notify_) alloc_events();
