@@ -74,64 +74,66 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lookback(const uint32_t* 
                                                                const uint32_t* n_dev, uint32_t* total,
                                                                uint32_t* tmp, uint32_t* err) {
     __shared__ uint32_t sm[kScanThreads / 32 + 1];
-    __shared__ uint32_t s_tile, s_epoch, s_prefix;
+    __shared__ uint32_t s_tile, s_prefix;
     unsigned long long* state = reinterpret_cast<unsigned long long*>(tmp + kScanHeader);
-    if (threadIdx.x == 0) {
-        s_tile = atomicAdd(&tmp[1], 1u);
-        s_epoch = *reinterpret_cast<volatile uint32_t*>(&tmp[0]) & 0x3fffffffu;
-    }
-    __syncthreads();
-    const uint32_t tile = s_tile, epoch = s_epoch;
+    const uint32_t epoch = *reinterpret_cast<volatile uint32_t*>(&tmp[0]) & 0x3fffffffu;
     const uint32_t lim = n_dev ? min(n, *n_dev) : n;
-    const uint32_t base = tile * kScanTile + threadIdx.x * kScanItems;
-    uint32_t v[kScanItems];
-    uint32_t sum = 0;
+    const unsigned long long tag = (unsigned long long)epoch << 34;
+    // A resident grid takes tiles in ticket order until the input ends, so
+    // every tile a block waits on belongs to a running block.
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(&tmp[1], 1u);
+        __syncthreads();
+        const uint32_t tile = s_tile;
+        __syncthreads();
+        if (uint64_t(tile) * kScanTile >= lim) {
+            if (tile == 0 && threadIdx.x == 0 && total) *total = 0u;
+            break;
+        }
+        const uint32_t base = tile * kScanTile + threadIdx.x * kScanItems;
+        uint32_t v[kScanItems];
+        uint32_t sum = 0;
 #pragma unroll
-    for (int i = 0; i < kScanItems; ++i) {
-        v[i] = base + i < lim ? in[base + i] : 0u;
-        sum += v[i];
-    }
-    uint32_t excl;
-    const uint32_t agg = block_excl_scan<kScanThreads>(sum, excl, sm);
-    const bool live = tile * kScanTile < lim;
-    if (live && threadIdx.x < 32) {
-        const uint32_t lane = threadIdx.x;
-        const unsigned long long tag = (unsigned long long)epoch << 34;
-        if (lane == 0)
-            scan_state_store(&state[tile], tag | ((tile == 0 ? 2ull : 1ull) << 32) | agg);
-        uint32_t prefix = 0;
-        int64_t look = int64_t(tile) - 1;
-        bool failed = false;
-        while (look >= 0) {
-            const int64_t idx = look - int64_t(lane);
-            uint32_t status = 2u, value = 0u;     // before tile 0: an empty prefix
-            if (idx >= 0) {
-                uint32_t spins = 0;
-                for (;;) {
-                    const unsigned long long st = scan_state_load(&state[idx]);
-                    status = uint32_t(st >> 32) & 3u;
-                    if ((st >> 34) == epoch && status != 0u) { value = uint32_t(st); break; }
-                    if (++spins == kLookbackSpin) { failed = true; status = 2u; value = 0u; break; }
+        for (int i = 0; i < kScanItems; ++i) {
+            v[i] = base + i < lim ? in[base + i] : 0u;
+            sum += v[i];
+        }
+        uint32_t excl;
+        const uint32_t agg = block_excl_scan<kScanThreads>(sum, excl, sm);
+        if (threadIdx.x < 32) {
+            const uint32_t lane = threadIdx.x;
+            if (lane == 0) scan_state_store(&state[tile], tag | ((tile == 0 ? 2ull : 1ull) << 32) | agg);
+            uint32_t prefix = 0;
+            int64_t look = int64_t(tile) - 1;
+            bool failed = false;
+            while (look >= 0) {
+                const int64_t idx = look - int64_t(lane);
+                uint32_t status = 2u, value = 0u;     // before tile 0: an empty prefix
+                if (idx >= 0) {
+                    uint32_t spins = 0;
+                    for (;;) {
+                        const unsigned long long st = scan_state_load(&state[idx]);
+                        status = uint32_t(st >> 32) & 3u;
+                        if ((st >> 34) == epoch && status != 0u) { value = uint32_t(st); break; }
+                        if (++spins == kLookbackSpin) { failed = true; status = 2u; value = 0u; break; }
+                    }
                 }
+                const uint32_t pmask = __ballot_sync(0xffffffffu, status == 2u);
+                const int stop = pmask ? __ffs(pmask) - 1 : 31;
+                uint32_t part = int(lane) <= stop ? value : 0u;
+                for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
+                prefix += part;
+                if (pmask) break;
+                look -= 32;
             }
-            const uint32_t pmask = __ballot_sync(0xffffffffu, status == 2u);
-            const int stop = pmask ? __ffs(pmask) - 1 : 31;
-            uint32_t part = int(lane) <= stop ? value : 0u;
-            for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
-            prefix += part;
-            if (pmask) break;
-            look -= 32;
+            if (__any_sync(0xffffffffu, failed) && lane == 0 && err) atomicOr(err, kErrLogic);
+            if (lane == 0) {
+                if (tile != 0) scan_state_store(&state[tile], tag | (2ull << 32) | (prefix + agg));
+                s_prefix = prefix;
+                if (total && uint64_t(tile + 1) * kScanTile >= lim) *total = prefix + agg;
+            }
         }
-        if (__any_sync(0xffffffffu, failed) && lane == 0 && err) atomicOr(err, kErrLogic);
-        if (lane == 0) {
-            if (tile != 0) scan_state_store(&state[tile], tag | (2ull << 32) | (prefix + agg));
-            s_prefix = prefix;
-            if (total && (tile + 1) * kScanTile >= lim) *total = prefix + agg;
-        }
-    }
-    if (!live && tile == 0 && threadIdx.x == 0 && total) *total = 0u;
-    __syncthreads();
-    if (live) {
+        __syncthreads();
         uint32_t run = excl + s_prefix;
 #pragma unroll
         for (int i = 0; i < kScanItems; ++i) {
@@ -236,7 +238,8 @@ void scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, const uint32_
         if (err) cudaMemsetAsync(err, 0xff, 4, st);
         return;
     }
-    k_scan_lookback<<<nb, kScanThreads, 0, st>>>(in, out, n, n_dev, total, tmp, err);
+    // two blocks per SM at most: the whole grid is resident
+    k_scan_lookback<<<nb < 296u ? nb : 296u, kScanThreads, 0, st>>>(in, out, n, n_dev, total, tmp, err);
 }
 
 size_t radix_hist_words(uint32_t n_cap) {
