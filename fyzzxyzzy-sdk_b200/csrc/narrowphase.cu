@@ -1209,8 +1209,6 @@ __global__ void __launch_bounds__(128) k_narrowphase(DevState s) {
         if (ps.convex) {
             // carried forward here, generated by k_narrowphase_convex
             s.cur.cache[k] = cache;
-            if (pj >= 0) s.cur.fric[k] = s.prev.fric[pj];
-            else s.cur.fric[k].epoch = 0u;
             s.cvx_list[atomicAdd(&s.counters[kCntConvex], 1u)] = k;
             continue;
         }
@@ -1253,9 +1251,8 @@ __global__ void __launch_bounds__(128) k_narrowphase(DevState s) {
         s.cur.cache[k] = cache;
         s.cur.count[k] = uint32_t(count);
         for (int i = 0; i < count; ++i) s.pts[4 * size_t(k) + i] = out[i];
-        // friction history follows its manager
-        if (pj >= 0) s.cur.fric[k] = s.prev.fric[pj];
-        else s.cur.fric[k].epoch = 0u;
+        // friction histories are not carried here: row preparation reads a
+        // touching manager's history from the previous generation
     }
 }
 

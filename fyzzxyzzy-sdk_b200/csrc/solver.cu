@@ -1098,8 +1098,13 @@ __global__ void k_prep_contacts(DevState s) {
         const qt q0 = mass_orientation(s, a0), q1 = mass_orientation(s, a1);
         const v3 p0 = mass_position(s, a0), p1 = mass_position(s, a1);
         // correlatePatches: a valid previous anchor patch comes first
-        // (cached_friction_patch_valid, scene.cpp:3981-4011).
-        FrictionHist h = s.cur.fric[pair];
+        // (cached_friction_patch_valid, scene.cpp:3981-4011).  The history
+        // is the manager's record in the previous generation; it counts only
+        // when that step prepared it.
+        FrictionHist h;
+        const int32_t pj = s.prev_idx[pair];
+        if (pj >= 0) h = s.prev.fric[pj];
+        else h.epoch = 0u;
         bool have_old = false;
         if (h.epoch != 0u && h.epoch + 1u == frame && (h.meta & 512u)) {
             bool valid = !((h.meta >> 8) & 1u) && (h.meta & 255u) != 0u;

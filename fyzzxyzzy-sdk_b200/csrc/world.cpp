@@ -1457,6 +1457,9 @@ private:
             dalloc(sets_[k].key, cap, pair_owned_);
             dalloc(sets_[k].cache, cap, pair_owned_);
             dalloc(sets_[k].fric, cap, pair_owned_);
+            // friction records count only with the epoch of the previous
+            // step, so unwritten ones must start at epoch 0
+            check_cuda(cudaMemsetAsync(sets_[k].fric, 0, size_t(cap) * sizeof(FrictionHist), stream_), "memset");
             dalloc(sets_[k].count, cap, pair_owned_);
             dalloc(sets_[k].n, 1, pair_owned_);
             check_cuda(cudaMemsetAsync(sets_[k].n, 0, 4, stream_), "memset");
