@@ -140,3 +140,30 @@ def test_product_cooking_matches_reference(pkg, ref, scenes):
             ref.cook_convex(bv, bt)
         with pytest.raises(ValueError):
             pkg.ConvexMesh(bv, bt)
+
+
+@pytest.mark.parametrize("scale", [0.02, 25.0])
+def test_convex_gu_functions_match_reference_at_scale(ref, oracle, scenes, scale):
+    # tiny and large hulls: the scale-relative facet admission and witness
+    # tolerance of the hull EPA (GuPCMGjkEpa.cpp:210-213, 296-302)
+    meshes = [(v * np.float32(scale), t) for v, t in meshes_under_test(scenes)]
+    cooked = [ref.cook_convex(v, t) for v, t in meshes]
+    R = ref.RefConvexGu(meshes)
+    O = oracle.OracleConvexGu(meshes)
+    rng = np.random.Generator(np.random.PCG64(int(scale * 100)))
+    hits = 0
+    for it in range(300):
+        a, ma = random_shape(rng, len(meshes), "hull")
+        b, mb = random_shape(rng, len(meshes), "hull")
+        a[3:6] *= scale
+        b[3:6] *= scale
+        a, b = half_of(cooked, a, ma), half_of(cooked, b, mb)
+        cd = 0.04 * scale
+        ok_r, wr = R.gjk_epa(a, ma, b, mb, cd)
+        ok_o, wo = O.gjk_epa(a, ma, b, mb, cd)
+        assert ok_r == ok_o, it
+        np.testing.assert_array_equal(wo, wr, err_msg=f"pair {it}")
+        if ok_r:
+            hits += 1
+            np.testing.assert_array_equal(O.face_contacts(a, ma, b, mb, cd, wr), R.face_contacts(a, ma, b, mb, cd, wr))
+    assert hits >= 80, hits
