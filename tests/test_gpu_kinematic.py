@@ -73,3 +73,28 @@ def test_kinematic_authoring_errors(pkg, scenes):
     w.set_body_kinematic(first, False)     # dynamic again: falls under gravity
     w.step(DT, steps=5)
     assert w.read_bodies()[first, 4] < 0.0
+
+
+def test_hull_riders_on_a_hull_platform_track_oracle(pkg, oracle, scenes):
+    # the platform is a cooked box hull and the riders cooked hulls: the
+    # convex generators against an infinite-mass kinematic partner
+    spec = scenes.kinematic_platform(12, seed=5)
+    spec.convex_meshes = [scenes.hull_box((1.5, 0.1, 1.5)), scenes.hull_prism(6, 0.15, 0.1),
+                          scenes.hull_bipyramid(5, 0.12, 0.15)]
+    spec.shape_type[:] = scenes.CONVEX
+    spec.shape_geom[:, 0] = [0] + [1 + (i % 2) for i in range(12)]
+    w = pkg.World(0)
+    first = w.add_scene(spec)
+    o = oracle.OracleScene(spec)
+    w.set_body_kinematic(first)
+    o.set_kinematic(0)
+    for k in range(40):
+        tg = scenes.platform_target(k)
+        w.set_body_kinematic_target(first, tg)
+        o.set_kinematic_target(0, tg)
+        w.step(DT)
+        o.step(DT)
+    ws, os_ = w.read_bodies(), o.body_states()
+    assert rel_err(ws[:, 0:3], os_[:, 0:3], 1.0) <= 1e-4
+    assert rel_err(ws[:, 3:6], os_[:, 3:6], 0.1) <= 1e-2
+    assert w.step_counters()["convex_pairs"] > 0

@@ -167,3 +167,24 @@ def test_convex_gu_functions_match_reference_at_scale(ref, oracle, scenes, scale
             hits += 1
             np.testing.assert_array_equal(O.face_contacts(a, ma, b, mb, cd, wr), R.face_contacts(a, ma, b, mb, cd, wr))
     assert hits >= 80, hits
+
+
+def test_hull_riders_on_a_kinematic_hull_platform(ref, oracle, scenes):
+    spec = scenes.kinematic_platform(12, seed=5)
+    spec.convex_meshes = [scenes.hull_box((1.5, 0.1, 1.5)), scenes.hull_prism(6, 0.15, 0.1),
+                          scenes.hull_bipyramid(5, 0.12, 0.15)]
+    spec.shape_type[:] = scenes.CONVEX
+    spec.shape_geom[:, 0] = [0] + [1 + (i % 2) for i in range(12)]
+    r = ref.RefScene(spec)
+    o = oracle.OracleScene(spec)
+    r.set_kinematic(0)
+    o.set_kinematic(0)
+    for k in range(200):
+        if k < 120:
+            tg = scenes.platform_target(k)
+            r.set_kinematic_target(0, tg)
+            o.set_kinematic_target(0, tg)
+        r.step(DT)
+        o.step(DT, r.manager_order(), r.joint_order())
+        np.testing.assert_array_equal(o.body_states(), r.body_states(), err_msg=f"step {k}")
+    assert r.counts()["manifolds"] >= 8
