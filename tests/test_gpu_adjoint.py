@@ -278,3 +278,48 @@ def test_rewind_reruns_the_same_rollout(pkg, scenes):
     for a, b in zip(runs[0], runs[1]):
         np.testing.assert_array_equal(a, b)
     assert np.abs(runs[0][1]).max() > 0
+
+
+def sliding_hull(scenes, density=1000.0, friction=0.5):
+    """The sliding box as a cooked hull (8 vertices, 6 quad faces), so its
+    floor contacts come from the hull-vertex generator.  A face of exactly
+    four vertices keeps the forward smooth: with more vertices on the
+    resting face the four kept witnesses change with the tilt, and finite
+    differences straddle those switches."""
+    spec = sliding_box(scenes, density, friction)
+    spec.shape_type[:] = scenes.CONVEX
+    spec.shape_geom[0] = (0.0, 0.0, 0.0, 0.0)
+    spec.convex_meshes = [scenes.hull_box((0.25, 0.25, 0.25))]
+    return spec
+
+
+def test_gradients_through_a_sliding_hull(pkg, scenes):
+    # the adjoint moves hull contacts with the body like any other
+    # persistent manifold
+    steps, eps, settle = 8, 1e-3, 30
+    spec = sliding_hull(scenes)
+    nb = spec.n_actors
+    v0 = np.zeros((nb, 3), np.float32)
+    w0 = np.zeros((nb, 3), np.float32)
+    v0[1] = (1.5, 0.0, 0.4)
+    weights = np.zeros((nb, 3))
+    weights[1] = (1.0, 0.3, 0.5)
+    w = pkg.World(0)
+    w.add_scene(spec)
+    w.step(DT, steps=settle)
+    assert w.counts()["points"] >= 4
+    set_velocities(w, v0, w0)
+    w.rollout_begin(steps, 4)
+    w.rollout_forward(DT)
+    g = w.rollout_backward(grad_center=weights)
+    for axis in range(3):
+        dv = np.zeros((nb, 3), np.float32)
+        dv[1, axis] = eps
+        fd = (rollout_loss(pkg, spec, v0 + dv, w0, steps, weights, settle) -
+              rollout_loss(pkg, spec, v0 - dv, w0, steps, weights, settle)) / (2 * eps)
+        assert abs(fd - g["v0"][1, axis]) <= 2e-2 * max(abs(fd), 1e-2), (axis, fd, g["v0"][1, axis])
+    mu = 0.5
+    fd_f = (rollout_loss(pkg, sliding_hull(scenes, friction=mu + eps), v0, w0, steps, weights, settle) -
+            rollout_loss(pkg, sliding_hull(scenes, friction=mu - eps), v0, w0, steps, weights, settle)) / (2 * eps)
+    adj_f = float(np.sum(g["static_friction"] + g["dynamic_friction"]))
+    assert abs(fd_f - adj_f) <= 2e-2 * max(abs(fd_f), 1e-3), (fd_f, adj_f)
