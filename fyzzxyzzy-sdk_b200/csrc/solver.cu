@@ -282,7 +282,10 @@ __device__ __forceinline__ void kinematic_link(const DevState& s, uint32_t a, ui
     if (!is_dyn(s, dyn)) return;
     const uint32_t f = s.b_sleep[kin];
     if (f & kKinPending) atomicOr(&s.sl_act[dyn], kActKinematic);
-    if (f & kKinNew) atomicOr(&s.sl_act[dyn], kActKinWake | kActActivating);
+    if (f & kKinNew) {
+        atomicOr(&s.sl_act[dyn], kActKinWake | kActActivating);
+        atomicOr(&s.counters[kCntActivating], 1u);
+    }
 }
 __device__ void sleep_pair(const DevState& s, uint32_t k, bool touch) {
     const uint64_t key = s.cur.key[k];
@@ -296,10 +299,12 @@ __device__ void sleep_pair(const DevState& s, uint32_t k, bool touch) {
     if (found && da && db && (!is_asleep(s, ba) || !is_asleep(s, bb))) {
         atomicOr(&s.sl_act[ba], kActActivating);
         atomicOr(&s.sl_act[bb], kActActivating);
+        atomicOr(&s.counters[kCntActivating], 1u);
     }
     if (touch && !touched) {
         if (da) { atomicOr(&s.sl_act[ba], kActActivating); atomicAnd(&s.b_sleep[ba], ~kReady); }
         if (db) { atomicOr(&s.sl_act[bb], kActActivating); atomicAnd(&s.b_sleep[bb], ~kReady); }
+        if (da || db) atomicOr(&s.counters[kCntActivating], 1u);
     }
     if (touch && s.n_kinematic) kinematic_link(s, ba, bb);
 }
@@ -327,8 +332,10 @@ __device__ __forceinline__ bool spec_pair(const DevState& s, uint32_t i, uint32_
     rb = uf_find(s.uf_parent, bb);
     return ra != rb;
 }
+// Only an activating body can wake a sleeping island, so without one the
+// overlap graph is not needed this step.
 __global__ void k_sleep_spec(DevState s) {
-    if (s.counters[kCntSleeping] == 0u) return;
+    if (s.counters[kCntSleeping] == 0u || s.counters[kCntActivating] == 0u) return;
     const uint32_t n = *s.cur.n, np = *s.prev.n;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n + np; i += stride) {
@@ -1884,6 +1891,7 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     k_frame_begin<<<1, 32, 0, st>>>(s);
     cudaMemsetAsync(s.counters + kCntAwake, 0, 2 * sizeof(uint32_t), st);
     cudaMemsetAsync(s.counters + kCntReady, 0, sizeof(uint32_t), st);
+    cudaMemsetAsync(s.counters + kCntActivating, 0, sizeof(uint32_t), st);
     k_bodies_begin<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
     // touching managers in canonical pair order
     k_touch_flags<<<grid_for(s.pair_cap, T, cap_blocks), T, 0, st>>>(s, flags);

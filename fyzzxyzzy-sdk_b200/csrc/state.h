@@ -275,7 +275,8 @@ enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels =
              kCntReported = 14 /* touching managers with an event */,
              kCntReady = 15 /* ready for sleep at step start */,
              kCntConvex = 16 /* pairs with a cooked hull */,
-             kCntConvexGjk = 17 /* hull pairs regenerated through GJK/EPA */, kCntSlots = 18 };
+             kCntConvexGjk = 17 /* hull pairs regenerated through GJK/EPA */,
+             kCntActivating = 18 /* nonzero when some body activates this step */, kCntSlots = 19 };
 
 // Contact event records in device memory; the layouts of
 // fyzz_b200_contact_event_t and fyzz_b200_contact_event_point_t.
