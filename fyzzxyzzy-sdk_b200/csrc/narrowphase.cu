@@ -1882,7 +1882,6 @@ __global__ void __launch_bounds__(128) k_narrowphase_convex(DevState s) {
 constexpr int kCvxWarps = 4;
 __global__ void __launch_bounds__(kCvxWarps * 32, 3) k_narrowphase_convex_gjk(DevState s) {
     __shared__ EpaShared epa[kCvxWarps];
-    __shared__ ClipShared clip[kCvxWarps];
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     const uint32_t n = s.counters[kCntConvexGjk];
     const uint32_t nwarps = gridDim.x * kCvxWarps;
@@ -1926,22 +1925,54 @@ __global__ void __launch_bounds__(kCvxWarps * 32, 3) k_narrowphase_convex_gjk(De
                 w.sep -= f1.radius;
             }
             if (w.sep <= cd) {
-                Cand clipped[4];
-                const int nc = face_contacts_warp(s, f0, f1, cd, w, clipped, clip[wib]);
+                // faces are clipped around the witness by the next kernel
                 if (lane == 0) {
-                    if (nc) {
-                        for (int j = 0; j < nc; ++j) cache.pts[j] = to_pt(clipped[j]);
-                        set_meta(cache, uint32_t(nc), true);
-                    } else {
-                        cache.pts[0] = to_pt(w);
-                        set_meta(cache, 1, true);
-                    }
+                    s.cur.cache[k] = cache;
+                    const uint32_t j = atomicAdd(&s.counters[kCntConvexClip], 1u);
+                    s.cvx_clip_list[j] = k;
+                    s.cvx_wit[3 * size_t(j)] = make_float4(w.la.x, w.la.y, w.la.z, w.lb.x);
+                    s.cvx_wit[3 * size_t(j) + 1] = make_float4(w.lb.y, w.lb.z, w.nb.x, w.nb.y);
+                    s.cvx_wit[3 * size_t(j) + 2] = make_float4(w.nb.z, w.sep, 0.f, 0.f);
                 }
+                __syncwarp();
+                continue;
             }
         }
         if (lane == 0) {
             ContactPt out[4];
             store_manifold(s, k, cache, convex_emit(f1, cd, cache, out), out);
+        }
+        __syncwarp();
+    }
+}
+
+// Face clipping around the witnesses of the kernel above (its own kernel so
+// that neither carries the other's code), one warp per pair, then the
+// manifold's emission.
+__global__ void __launch_bounds__(kCvxWarps * 32) k_narrowphase_convex_clip(DevState s) {
+    __shared__ ClipShared clip[kCvxWarps];
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    const uint32_t n = s.counters[kCntConvexClip];
+    const uint32_t nwarps = gridDim.x * kCvxWarps;
+    for (uint32_t i = blockIdx.x * kCvxWarps + wib; i < n; i += nwarps) {
+        const uint32_t k = s.cvx_clip_list[i];
+        const PairShapes ps = pair_shapes(s, s.cur.key[k]);
+        PcmCache cache = s.cur.cache[k];
+        const Fin f0 = load_fin(s, ps.first), f1 = load_fin(s, ps.second);
+        const float4 w0 = s.cvx_wit[3 * size_t(i)], w1 = s.cvx_wit[3 * size_t(i) + 1], w2 = s.cvx_wit[3 * size_t(i) + 2];
+        const Cand w = {{w0.x, w0.y, w0.z}, {w0.w, w1.x, w1.y}, {w1.z, w1.w, w2.x}, w2.y};
+        Cand clipped[4];
+        const int nc = face_contacts_warp(s, f0, f1, ps.cd, w, clipped, clip[wib]);
+        if (lane == 0) {
+            if (nc) {
+                for (int j = 0; j < nc; ++j) cache.pts[j] = to_pt(clipped[j]);
+                set_meta(cache, uint32_t(nc), true);
+            } else {
+                cache.pts[0] = to_pt(w);
+                set_meta(cache, 1, true);
+            }
+            ContactPt out[4];
+            store_manifold(s, k, cache, convex_emit(f1, ps.cd, cache, out), out);
         }
         __syncwarp();
     }
@@ -1959,9 +1990,11 @@ void enqueue_narrowphase(const DevState& s, cudaStream_t st, const StageHook& ho
     const uint32_t gb = (s.pair_cap + kGjkWarps - 1) / kGjkWarps;
     k_narrowphase_gjk<<<gb < 148u * 8u ? gb : 148u * 8u, kGjkWarps * 32, 0, st>>>(s);
     if (s.n_meshes) {
+        cudaMemsetAsync(s.counters + kCntConvexClip, 0, 4, st);
         k_narrowphase_convex<<<blocks < 148u * 16u ? blocks : 148u * 16u, T, 0, st>>>(s);
         const uint32_t cb = (s.pair_cap + kCvxWarps - 1) / kCvxWarps;
         k_narrowphase_convex_gjk<<<cb < 148u * 8u ? cb : 148u * 8u, kCvxWarps * 32, 0, st>>>(s);
+        k_narrowphase_convex_clip<<<cb < 148u * 8u ? cb : 148u * 8u, kCvxWarps * 32, 0, st>>>(s);
     }
 }
 

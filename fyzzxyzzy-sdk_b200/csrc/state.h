@@ -99,6 +99,8 @@ struct DevState {
     uint32_t* gjk_list = nullptr;      // pairs awaiting the GJK/EPA continuation
     uint32_t* cvx_list = nullptr;      // pairs with a cooked hull (plane or finite partner)
     uint32_t* cvx_gjk_list = nullptr;  // hull pairs whose manifold regenerates (GJK/EPA)
+    uint32_t* cvx_clip_list = nullptr; // regenerated hull pairs with a witness to clip faces around
+    float4* cvx_wit = nullptr;         // their witnesses: local a, local b, normal, separation (3 per entry)
 
     // touching managers
     uint32_t* man_list = nullptr;      // current-pair indices, canonical order
@@ -276,7 +278,8 @@ enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels =
              kCntReady = 15 /* ready for sleep at step start */,
              kCntConvex = 16 /* pairs with a cooked hull */,
              kCntConvexGjk = 17 /* hull pairs regenerated through GJK/EPA */,
-             kCntActivating = 18 /* nonzero when some body activates this step */, kCntSlots = 19 };
+             kCntActivating = 18 /* nonzero when some body activates this step */,
+             kCntConvexClip = 19 /* regenerated hull pairs whose faces are clipped */, kCntSlots = 20 };
 
 // Contact event records in device memory; the layouts of
 // fyzz_b200_contact_event_t and fyzz_b200_contact_event_point_t.

@@ -1471,6 +1471,8 @@ private:
         dalloc(d_.gjk_list, cap, pair_owned_);
         dalloc(d_.cvx_list, cap, pair_owned_);
         dalloc(d_.cvx_gjk_list, cap, pair_owned_);
+        dalloc(d_.cvx_clip_list, cap, pair_owned_);
+        dalloc(d_.cvx_wit, 3 * size_t(cap), pair_owned_);
         dalloc(d_.man_list, cap, pair_owned_);
         dalloc(d_.mh, cap, pair_owned_);
         dalloc(d_.nrow, size_t(cap) * 4, pair_owned_);
