@@ -1469,10 +1469,12 @@ private:
         dalloc(d_.lost_flag, cap, pair_owned_);
         dalloc(d_.pts, size_t(cap) * 4, pair_owned_);
         dalloc(d_.gjk_list, cap, pair_owned_);
-        dalloc(d_.cvx_list, cap, pair_owned_);
-        dalloc(d_.cvx_gjk_list, cap, pair_owned_);
-        dalloc(d_.cvx_clip_list, cap, pair_owned_);
-        dalloc(d_.cvx_wit, 3 * size_t(cap), pair_owned_);
+        // the hull lists and witnesses exist only in worlds with cooked hulls
+        const size_t hcap = d_.n_meshes ? size_t(cap) : 1;
+        dalloc(d_.cvx_list, hcap, pair_owned_);
+        dalloc(d_.cvx_gjk_list, hcap, pair_owned_);
+        dalloc(d_.cvx_clip_list, hcap, pair_owned_);
+        dalloc(d_.cvx_wit, 3 * hcap, pair_owned_);
         dalloc(d_.man_list, cap, pair_owned_);
         dalloc(d_.mh, cap, pair_owned_);
         dalloc(d_.nrow, size_t(cap) * 4, pair_owned_);
