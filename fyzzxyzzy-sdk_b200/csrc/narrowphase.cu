@@ -1880,8 +1880,53 @@ __global__ void __launch_bounds__(128) k_narrowphase_convex(DevState s) {
 // warp takes a pair: GJK/EPA run together on every lane (hull supports are
 // each lane's own scan of the vertices), faces are clipped on lane 0.
 constexpr int kCvxWarps = 4;
+// The regenerated pair's cache, B-local pose of A and GJK pair setup
+// (shared by the GJK and EPA kernels).
+__device__ __forceinline__ BPair convex_pair(const DevState& s, const Fin& f0, const Fin& f1) {
+    BPair bp;
+    bp.ha = f0.half;
+    bp.hb = f1.half;
+    bp.a_in_b = rotinv_gu(f1.q, vsub(f0.p, f1.p));
+    bp.rel = qmul(qconj(f1.q), f0.q);
+    bp.va = s.hv + f0.vo; bp.nva = f0.nv;
+    bp.vb = s.hv + f1.vo; bp.nvb = f1.nv;
+    bp.ra = f0.radius; bp.rb = f1.radius;
+    return bp;
+}
+// After GJK or EPA: a witness within the contact distance goes to face
+// clipping (the cache is stored for it); otherwise the manifold is stored
+// now.  Every lane calls it with the same values.
+__device__ void convex_finish(const DevState& s, uint32_t k, bool have, Cand w, const Fin& f0, const Fin& f1,
+                              qt rel, float cd, PcmCache& cache) {
+    const uint32_t lane = threadIdx.x & 31u;
+    if (have) {
+        // sphere radii applied along the final normal
+        if (f0.radius > 0.f) {
+            w.la = vadd(w.la, rotinv_gu(rel, vmul(w.nb, -f0.radius)));
+            w.sep -= f0.radius;
+        }
+        if (f1.radius > 0.f) {
+            w.lb = vadd(w.lb, vmul(w.nb, f1.radius));
+            w.sep -= f1.radius;
+        }
+        if (w.sep <= cd) {
+            if (lane == 0) {
+                s.cur.cache[k] = cache;
+                const uint32_t j = atomicAdd(&s.counters[kCntConvexClip], 1u);
+                s.cvx_clip_list[j] = k;
+                s.cvx_wit[3 * size_t(j)] = make_float4(w.la.x, w.la.y, w.la.z, w.lb.x);
+                s.cvx_wit[3 * size_t(j) + 1] = make_float4(w.lb.y, w.lb.z, w.nb.x, w.nb.y);
+                s.cvx_wit[3 * size_t(j) + 2] = make_float4(w.nb.z, w.sep, 0.f, 0.f);
+            }
+            return;
+        }
+    }
+    if (lane == 0) {
+        ContactPt out[4];
+        store_manifold(s, k, cache, convex_emit(f1, cd, cache, out), out);
+    }
+}
 __global__ void __launch_bounds__(kCvxWarps * 32, 3) k_narrowphase_convex_gjk(DevState s) {
-    __shared__ EpaShared epa[kCvxWarps];
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     const uint32_t n = s.counters[kCntConvexGjk];
     const uint32_t nwarps = gridDim.x * kCvxWarps;
@@ -1899,49 +1944,59 @@ __global__ void __launch_bounds__(kCvxWarps * 32, 3) k_narrowphase_convex_gjk(De
         cache.qa[0] = f0.q.x; cache.qa[1] = f0.q.y; cache.qa[2] = f0.q.z; cache.qa[3] = f0.q.w;
         cache.qb[0] = f1.q.x; cache.qb[1] = f1.q.y; cache.qb[2] = f1.q.z; cache.qb[3] = f1.q.w;
         set_meta(cache, 0, true);
-        BPair bp;
-        bp.ha = f0.half;
-        bp.hb = f1.half;
-        bp.a_in_b = rotinv_gu(f1.q, vsub(f0.p, f1.p));
-        bp.rel = qmul(qconj(f1.q), f0.q);
-        bp.va = s.hv + f0.vo; bp.nva = f0.nv;
-        bp.vb = s.hv + f1.vo; bp.nvb = f1.nv;
-        bp.ra = f0.radius; bp.rb = f1.radius;
+        const BPair bp = convex_pair(s, f0, f1);
         Cand w = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0.0f};
         Sup simplex[4];
         int sc = 0;
         const int mode = gjk_phase<true>(bp, cd + f0.radius + f1.radius, w, simplex, sc);
-        bool have = mode == 1;
-        if (mode == 2) have = run_epa_warp<true>(bp, simplex, sc, w, epa[wib]);
-        if (have) {
-            // sphere radii applied along the final normal (every lane holds
-            // the same witness)
-            if (f0.radius > 0.f) {
-                w.la = vadd(w.la, rotinv_gu(bp.rel, vmul(w.nb, -f0.radius)));
-                w.sep -= f0.radius;
-            }
-            if (f1.radius > 0.f) {
-                w.lb = vadd(w.lb, vmul(w.nb, f1.radius));
-                w.sep -= f1.radius;
-            }
-            if (w.sep <= cd) {
-                // faces are clipped around the witness by the next kernel
-                if (lane == 0) {
-                    s.cur.cache[k] = cache;
-                    const uint32_t j = atomicAdd(&s.counters[kCntConvexClip], 1u);
-                    s.cvx_clip_list[j] = k;
-                    s.cvx_wit[3 * size_t(j)] = make_float4(w.la.x, w.la.y, w.la.z, w.lb.x);
-                    s.cvx_wit[3 * size_t(j) + 1] = make_float4(w.lb.y, w.lb.z, w.nb.x, w.nb.y);
-                    s.cvx_wit[3 * size_t(j) + 2] = make_float4(w.nb.z, w.sep, 0.f, 0.f);
+        if (mode == 2) {
+            // EPA continues in its own kernel from this simplex
+            if (lane == 0) {
+                s.cur.cache[k] = cache;
+                const uint32_t j = atomicAdd(&s.counters[kCntConvexEpa], 1u);
+                s.cvx_epa_list[j] = k;
+                float4* o = s.cvx_simplex + 12 * size_t(j);
+                for (int q = 0; q < 4; ++q) {
+                    const Sup& u = simplex[q];
+                    o[3 * q] = make_float4(u.a.x, u.a.y, u.a.z, u.b.x);
+                    o[3 * q + 1] = make_float4(u.b.y, u.b.z, u.q.x, u.q.y);
+                    o[3 * q + 2] = make_float4(u.q.z, __uint_as_float(u.ai), __uint_as_float(u.bi),
+                                               q == 3 ? __int_as_float(sc) : 0.f);
                 }
-                __syncwarp();
-                continue;
             }
+            __syncwarp();
+            continue;
         }
-        if (lane == 0) {
-            ContactPt out[4];
-            store_manifold(s, k, cache, convex_emit(f1, cd, cache, out), out);
+        convex_finish(s, k, mode == 1, w, f0, f1, bp.rel, cd, cache);
+        __syncwarp();
+    }
+}
+// EPA of the regenerated hull pairs whose GJK reached it, one warp per pair.
+__global__ void __launch_bounds__(kCvxWarps * 32, 3) k_narrowphase_convex_epa(DevState s) {
+    __shared__ EpaShared epa[kCvxWarps];
+    const uint32_t wib = threadIdx.x >> 5;
+    const uint32_t n = s.counters[kCntConvexEpa];
+    const uint32_t nwarps = gridDim.x * kCvxWarps;
+    for (uint32_t i = blockIdx.x * kCvxWarps + wib; i < n; i += nwarps) {
+        const uint32_t k = s.cvx_epa_list[i];
+        const PairShapes ps = pair_shapes(s, s.cur.key[k]);
+        PcmCache cache = s.cur.cache[k];
+        const Fin f0 = load_fin(s, ps.first), f1 = load_fin(s, ps.second);
+        const BPair bp = convex_pair(s, f0, f1);
+        const float4* o = s.cvx_simplex + 12 * size_t(i);
+        Sup simplex[4];
+        for (int q = 0; q < 4; ++q) {
+            const float4 x = o[3 * q], y = o[3 * q + 1], z = o[3 * q + 2];
+            simplex[q].a = {x.x, x.y, x.z};
+            simplex[q].b = {x.w, y.x, y.y};
+            simplex[q].q = {y.z, y.w, z.x};
+            simplex[q].ai = __float_as_uint(z.y);
+            simplex[q].bi = __float_as_uint(z.z);
         }
+        const int sc = __float_as_int(o[11].w);
+        Cand w = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0.0f};
+        const bool have = run_epa_warp<true>(bp, simplex, sc, w, epa[wib]);
+        convex_finish(s, k, have, w, f0, f1, bp.rel, ps.cd, cache);
         __syncwarp();
     }
 }
@@ -1990,10 +2045,11 @@ void enqueue_narrowphase(const DevState& s, cudaStream_t st, const StageHook& ho
     const uint32_t gb = (s.pair_cap + kGjkWarps - 1) / kGjkWarps;
     k_narrowphase_gjk<<<gb < 148u * 8u ? gb : 148u * 8u, kGjkWarps * 32, 0, st>>>(s);
     if (s.n_meshes) {
-        cudaMemsetAsync(s.counters + kCntConvexClip, 0, 4, st);
+        cudaMemsetAsync(s.counters + kCntConvexClip, 0, 8, st);   // clip and EPA lists
         k_narrowphase_convex<<<blocks < 148u * 16u ? blocks : 148u * 16u, T, 0, st>>>(s);
         const uint32_t cb = (s.pair_cap + kCvxWarps - 1) / kCvxWarps;
         k_narrowphase_convex_gjk<<<cb < 148u * 8u ? cb : 148u * 8u, kCvxWarps * 32, 0, st>>>(s);
+        k_narrowphase_convex_epa<<<cb < 148u * 8u ? cb : 148u * 8u, kCvxWarps * 32, 0, st>>>(s);
         k_narrowphase_convex_clip<<<cb < 148u * 8u ? cb : 148u * 8u, kCvxWarps * 32, 0, st>>>(s);
     }
 }

@@ -101,6 +101,8 @@ struct DevState {
     uint32_t* cvx_gjk_list = nullptr;  // hull pairs whose manifold regenerates (GJK/EPA)
     uint32_t* cvx_clip_list = nullptr; // regenerated hull pairs with a witness to clip faces around
     float4* cvx_wit = nullptr;         // their witnesses: local a, local b, normal, separation (3 per entry)
+    uint32_t* cvx_epa_list = nullptr;  // regenerated hull pairs whose GJK ended in EPA
+    float4* cvx_simplex = nullptr;     // their GJK simplices (4 supports x 3 float4; count in [11].w)
 
     // touching managers
     uint32_t* man_list = nullptr;      // current-pair indices, canonical order
@@ -279,7 +281,8 @@ enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels =
              kCntConvex = 16 /* pairs with a cooked hull */,
              kCntConvexGjk = 17 /* hull pairs regenerated through GJK/EPA */,
              kCntActivating = 18 /* nonzero when some body activates this step */,
-             kCntConvexClip = 19 /* regenerated hull pairs whose faces are clipped */, kCntSlots = 20 };
+             kCntConvexClip = 19 /* regenerated hull pairs whose faces are clipped */,
+             kCntConvexEpa = 20 /* regenerated hull pairs continuing in EPA */, kCntSlots = 21 };
 
 // Contact event records in device memory; the layouts of
 // fyzz_b200_contact_event_t and fyzz_b200_contact_event_point_t.

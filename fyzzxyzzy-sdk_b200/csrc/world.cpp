@@ -1475,6 +1475,8 @@ private:
         dalloc(d_.cvx_gjk_list, hcap, pair_owned_);
         dalloc(d_.cvx_clip_list, hcap, pair_owned_);
         dalloc(d_.cvx_wit, 3 * hcap, pair_owned_);
+        dalloc(d_.cvx_epa_list, hcap, pair_owned_);
+        dalloc(d_.cvx_simplex, 12 * hcap, pair_owned_);
         dalloc(d_.man_list, cap, pair_owned_);
         dalloc(d_.mh, cap, pair_owned_);
         dalloc(d_.nrow, size_t(cap) * 4, pair_owned_);
