@@ -1,20 +1,26 @@
 #!/usr/bin/env python3
 """Rigid-body step benchmark: body-steps/s of the B200 step.
 
-Headline workload (one scene, all steps on the GPU): 131,072 dynamic bodies
-(70% boxes, 20% spheres, 10% box+sphere compounds, 2% in distance-joined
-pairs) in a 200 x 50 x 200 m region above a floor; dt = 1/120 s, 4 position
-+ 1 velocity iteration; 600 steps.  Also measured on the same line: the
-batched forward (4,096 independent scenes, 16-512 bodies each, one launch
-per stage) and the batched / plain throughput ratio.
+Headline workload: the plain at-scale scene -- 131,072 dynamic bodies (70%
+boxes, 20% spheres, 10% box+sphere compounds, 2% in distance-joined pairs)
+in a 200 x 50 x 200 m region above a floor; dt = 1/120 s, 4 position + 1
+velocity iteration -- taken from the state it reaches after its 600 steps in
+the reference's own run (tests/golden/plain_131k_step600.npz: a settled pile
+of ~270k contact managers, where the solver dominates).  W untimed warm-up
+steps, then K timed steps.  The same line carries the run from the seeded
+start (600 steps), the batched forward (4,096 independent scenes, one launch
+per stage), the differentiable rollouts (1,024 x 64 boxes, 128 steps; and at
+scale: 16,384 mixed scenes, 64 steps), the cooked-hull leg, the end-to-end
+loop through the C ABI with host buffers, the whole-step HBM roofline and the
+reference NativeCpu scene timed on the host cores.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
 For N > 1 (torchrun, one rank per GPU) every rank steps its own replica of
-the plain scene and its own shard of 4,096 batched scenes (weak scaling, no
+the plain scene and its own shard of the batched scenes (weak scaling, no
 data-path collective); times are the maximum over ranks.  --impl reference
 times the reference SDK's NativeCpu scene (built from the reference sources
-by oracle/Makefile) on the host cores.
+by oracle/Makefile) on the host cores, from the same settled state.
 """
 from __future__ import annotations
 
@@ -39,6 +45,10 @@ UNIT = "body-steps/s"
 PLAIN_WORKLOAD = ("plain method at scale, one scene: 131,072 bodies (70% boxes, 20% spheres, "
                   "10% box+sphere compounds, 2% distance-joined pairs), 200x50x200 m above a floor, "
                   "dt=1/120 s, 4 position + 1 velocity iterations")
+SETTLED_FIXTURE = os.path.join(ROOT, "tests", "golden", "plain_131k_step600.npz")
+SETTLED_START = ("settled: every body's pose and velocity after the workload's 600 steps in the reference "
+                 "NativeCpu run (tests/golden/plain_131k_step600.npz), all bodies awake, contact history "
+                 "rebuilt by the warm-up steps")
 BATCHED_WORKLOAD = ("batched forward: 4,096 independent scenes, body count log-uniform in [16,512] "
                     "(random piles and 5-20 high unit-cube stacks), own floor each, one launch per stage, "
                     "step captured as a CUDA graph")
@@ -84,6 +94,13 @@ def parse_args():
     ap.add_argument("--no-convex", action="store_true", help="skip the cooked-hull leg")
     ap.add_argument("--plain-only", action="store_true",
                     help="time the plain scene only (no e2e, batched or CPU legs; for profiler runs)")
+    ap.add_argument("--fresh", action="store_true",
+                    help="start the plain scene from its seeded initial state instead of the settled fixture")
+    ap.add_argument("--run-steps", type=int, default=600,
+                    help="steps of the plain run from the seeded start (0 skips the leg)")
+    ap.add_argument("--no-diff4", action="store_true", help="skip the differentiable rollout at scale")
+    ap.add_argument("--ref-budget", type=float, default=120.0,
+                    help="seconds the reference arm may spend on timed steps")
     return ap.parse_args()
 
 
@@ -96,6 +113,30 @@ def plain_spec(n):
     density (the 200 x 200 m footprint shrinks with sqrt(n / 131,072))."""
     side = 200.0 * (n / 131072.0) ** 0.5
     return scenes_mod().mixed_scale(n, seed=1, region=(side, 50.0, side))
+
+
+def headline_spec(args):
+    """The headline scene and a description of its start: the settled
+    fixture for the full-size scene, else the seeded start (smaller
+    profiling cases settle on the device with --settle)."""
+    spec = plain_spec(args.bodies)
+    if args.fresh or args.bodies != 131072:
+        return spec, "seeded initial state" + (f", then {args.settle} untimed steps" if args.settle else "")
+    if not os.path.exists(SETTLED_FIXTURE):
+        raise SystemExit(f"settled fixture missing: {SETTLED_FIXTURE} (tests/golden/make_settled.py)")
+    with np.load(SETTLED_FIXTURE) as f:
+        st = np.asarray(f["state"], np.float32)
+    rec = np.zeros((st.shape[0], 14), np.float32)
+    rec[:, :13] = st
+    return scenes_mod().with_state(spec, rec), SETTLED_START
+
+
+def plain_config(spec, start, world):
+    """The config object both arms print (identical for the same scene)."""
+    return {"workload": PLAIN_WORKLOAD, "start": start, "bodies": spec.n_bodies, "shapes": spec.n_shapes,
+            "joints": int(spec.joints.shape[0]), "dt": DT, "position_iterations": 4, "velocity_iterations": 1,
+            "l2": "resident working set (~200-400 MB) > 126 MB L2; not flushed between steps",
+            "parallelism": f"replicas x{world}" if world > 1 else "single scene"}
 
 
 def batched_specs(n, rank):
@@ -115,7 +156,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", idx, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
 
@@ -128,7 +169,7 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
             out, _ = self.proc.communicate()
-        sm, smax, reasons = [], [], set()
+        sm, smax, power, reasons = [], [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in out.strip().splitlines():
             parts = [p.strip() for p in line.split(",")]
@@ -137,6 +178,7 @@ class ClockSampler:
             try:
                 sm.append(float(parts[0]))
                 smax.append(float(parts[1]))
+                power.append(float(parts[2]))
             except ValueError:
                 continue
             for name, val in zip(names, parts[4:8]):
@@ -144,8 +186,13 @@ class ClockSampler:
                     reasons.add(name)
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        # samples under load: power above the idle floor (the sampler runs
+        # from before the warm-up through the plain legs)
+        floor = min(power) + 0.25 * (max(power) - min(power))
+        loaded = [c for c, w in zip(sm, power) if w >= floor] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm), "samples_under_load": len(loaded), "power_w_max": max(power),
+                "window": "from before the warm-up through the timed, profiled and end-to-end plain steps"}
 
 
 def clocks_bad(c: dict) -> bool:
@@ -157,22 +204,52 @@ def clocks_bad(c: dict) -> bool:
 
 
 # --------------------------------------------------------------- roofline
-def algorithmic_bytes(stage: str, c: dict, iters: int = 5) -> float:
-    """Per-step algorithmic bytes of each stage: the fixed per-unit
-    accounting constants of the hot-path scope (bytes per body / shape /
-    pair / contact / friction row), independent of tuning."""
+# Algorithmic bytes per step: the fixed per-unit accounting constants of the
+# hot path (bytes per body / shape / pair / contact point / friction row /
+# joint row), independent of tuning.  PGS runs I = 4 + 1 passes.
+def step_bytes(c: dict, iters: int = 5) -> dict:
     nb, ns, npair = c["bodies"], c["shapes"], c["pairs"]
     nc, nf, nj = c["points"], c["friction_rows"], c["joints"]
     return {
-        "bounds": 68.0 * ns,
-        "sort": 384.0 * ns,
-        "pairs": 48.0 * ns + 8.0 * c["found_lost"],
-        "narrowphase": 212.0 * npair,
-        "islands": 16.0 * (c["managers"] + nj) * 3,
-        "prep": 92.0 * nc + 56.0 * nf + 64.0 * nj,
+        "bounds": 68.0 * ns,                                        # pose + geometry in, encoded bounds out
+        "sort": 384.0 * ns,                                         # 3 axes x 2 endpoints x 8 B x r+w x 4 passes
+        "pairs": 48.0 * ns + 8.0 * c["found_lost"],                 # sweep of sorted endpoints, publication
+        "narrowphase": 212.0 * npair,                               # 2 x 64 B shape records + 84 B result
+        "prep": 92.0 * nc + 56.0 * nf + 64.0 * nj,                  # contact / friction / joint rows
         "pgs": iters * (68.0 * nc + 60.0 * nf + 68.0 * nj + 48.0 * nb),
-        "integrate": 120.0 * nb,
-    }[stage]
+        "integrate": 120.0 * nb,                                    # body state: read 68 B, write 52 B
+    }
+
+
+def roofline_of(counts: dict, ms_per_step: float, stages: dict, peak: float, peak_kind: str) -> dict:
+    """Whole-step roofline (all algorithmic bytes of a step / device time of
+    a step) plus per-stage fractions for the stages the accounting covers;
+    the island / partition stage has no algorithmic bytes (latency-bound
+    integer work) and is listed with its time only."""
+    per = step_bytes(counts)
+    total = sum(per.values())
+    achieved = total / (ms_per_step / 1e3) / 1e9
+    tr = ncu_traffic()
+    traffic = None
+    if tr and tr.get("step_bytes_per_body"):
+        traffic = round(tr["step_bytes_per_body"] * counts["bodies"])
+    st = {}
+    for k, ms in stages.items():
+        if k in per and ms > 0:
+            a = per[k] / (ms / 1e3) / 1e9
+            st[k] = {"ms": round(ms, 4), "algorithmic_bytes": per[k], "achieved": round(a, 1),
+                     "frac": round(a / peak, 4)}
+        else:
+            st[k] = {"ms": round(ms, 4), "algorithmic_bytes": None,
+                     "bound": "latency (partition rounds, union-find; no algorithmic bytes)"}
+    dom = max((k for k in stages if k in per), key=lambda k: stages[k], default=None)
+    out = {"bound": "hbm", "kernel_stage": "whole step (one CUDA graph)", "achieved": round(achieved, 1),
+           "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+           "traffic": traffic, "algorithmic_bytes": total, "ms_per_step": round(ms_per_step, 4),
+           "traffic_source": (tr or {}).get("_source"), "stages": st, "dominant_stage": dom}
+    if dom and tr and tr.get(dom + "_bytes_per_manager"):
+        out["dominant_stage_traffic"] = round(tr[dom + "_bytes_per_manager"] * counts["managers"])
+    return out
 
 
 def measured_peaks():
@@ -184,15 +261,14 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(stage: str):
-    """Per-unit DRAM traffic of the dominant kernel from the committed ncu
-    summary (profiles/ncu_traffic.json), or None."""
+def ncu_traffic():
+    """Per-unit DRAM traffic from the committed ncu summary
+    (profiles/ncu_traffic.json), or None."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if not os.path.exists(path):
         return None
     with open(path) as f:
-        t = json.load(f)
-    return t.get(stage)
+        return json.load(f)
 
 
 # --------------------------------------------------------------- ranks
@@ -427,6 +503,23 @@ def timed_steps(torch, w, steps, stream):
     return start.elapsed_time(end)
 
 
+def plain_run_leg(torch, pkg, local_rank, args, max_over_ranks, sum_over_ranks, barrier):
+    """The plain scene's full run from its seeded start (the workload's 600
+    steps: free fall, impacts, settling), one timed region."""
+    spec = plain_spec(args.bodies)
+    w = pkg.World(local_rank)
+    w.add_scene(spec)
+    w.step(DT, 1)                      # device state built, graphs captured
+    stream = torch.cuda.ExternalStream(w.device_view().stream)
+    barrier()
+    ms = max_over_ranks(timed_steps(torch, w, args.run_steps, stream))
+    counts = w.counts()
+    w.close()
+    return {"start": "seeded initial state (step 1 untimed)", "steps": args.run_steps,
+            "value": sum_over_ranks(spec.n_bodies * args.run_steps) / (ms / 1e3), "unit": UNIT,
+            "ms_per_step": ms / args.run_steps, "counts_at_end": counts}
+
+
 def run_b200(args, rank, world, local_rank):
     import torch
     if args.diff_only:
@@ -447,79 +540,69 @@ def run_b200(args, rank, world, local_rank):
     red = RankReducer(dist, "cuda")
     barrier, max_over_ranks, sum_over_ranks = red.barrier, red.max, red.sum
 
-    # ---- plain scene (replica per rank) ----
-    spec = plain_spec(args.bodies)
-    w = pkg.World(local_rank)
-    w.add_scene(spec)
+    # ---- plain scene (replica per rank), settled ----
+    spec, start = headline_spec(args)
     n_dyn = spec.n_bodies
-    if args.settle:
-        w.step(DT, args.settle)
-    if args.warmup:
-        w.step(DT, args.warmup)
-    stream = torch.cuda.ExternalStream(w.device_view().stream)
-    barrier()
-    torch.cuda.synchronize()
     for attempt in range(2):
-        sampler = ClockSampler(local_rank)
+        sampler = ClockSampler(local_rank)      # from before the warm-up
+        w = pkg.World(local_rank)
+        w.add_scene(spec)
+        if args.settle:
+            w.step(DT, args.settle)
+        if args.warmup:
+            w.step(DT, args.warmup)
+        stream = torch.cuda.ExternalStream(w.device_view().stream)
+        barrier()
+        torch.cuda.synchronize()
         torch.cuda.nvtx.range_push("timed")
         ms = timed_steps(torch, w, args.steps, stream)
         torch.cuda.nvtx.range_pop()
-        clocks = sampler.stop()
-        if not clocks_bad(clocks):
-            break
-        if attempt == 0:
-            w = pkg.World(local_rank)
-            w.add_scene(spec)
-            if args.settle:
-                w.step(DT, args.settle)
-            w.step(DT, args.warmup)
-            stream = torch.cuda.ExternalStream(w.device_view().stream)
-    barrier()
-    ms_max = max_over_ranks(ms)
-    value = sum_over_ranks(n_dyn * args.steps) / (ms_max / 1e3)
-    counts = w.counts()
-    kernels = w.kernels_per_step()
-
-    # ---- roofline of the dominant stage (CUDA events per stage) ----
-    prof = {}
-    for _ in range(max(1, args.profile_steps)):
-        st = w.profile_step(DT)
-        for k, v in st.items():
-            prof[k] = prof.get(k, 0.0) + v / max(1, args.profile_steps)
-    counts = w.counts()
-    dom = max(prof, key=prof.get)
-    alg = algorithmic_bytes(dom, counts)
-    peak, peak_kind = measured_peaks()
-    achieved = alg / (prof[dom] / 1e3) / 1e9
-    per_unit = ncu_traffic(dom)
-    units = {"narrowphase": counts["pairs"], "pgs": counts["managers"], "pairs": counts["shapes"],
-             "sort": counts["shapes"], "bounds": counts["shapes"], "integrate": counts["bodies"],
-             "prep": counts["managers"], "islands": counts["managers"]}[dom]
-    roofline = {"bound": "hbm", "kernel_stage": dom, "achieved": round(achieved, 2), "peak": peak,
-                "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                "traffic": (per_unit * units if per_unit is not None else None),
-                "algorithmic_bytes": alg, "stage_ms": round(prof[dom], 4)}
-
-    # ---- end to end through the C ABI with host buffers ----
-    e2e = None
-    if not args.plain_only:
-        e2e_steps = max(1, min(args.e2e_steps, args.steps))
-        # host buffers in pinned (page-locked) memory, as a host loop that
-        # streams state every step would keep them
-        buf = torch.empty((spec.n_actors, 14), dtype=torch.float32, pin_memory=True).numpy()
         barrier()
-        t0 = time.perf_counter()
-        for _ in range(e2e_steps):
-            w.read_bodies(buf)
-            w.write_states(buf)
-            w.step(DT)
-        w.synchronize()
-        e2e_s = max_over_ranks(time.perf_counter() - t0)
-        e2e = {"value": sum_over_ranks(n_dyn * e2e_steps) / e2e_s, "unit": UNIT,
-               "h2d_bytes_per_step": 56 * spec.n_actors, "d2h_bytes_per_step": 56 * spec.n_actors,
-               "steps": e2e_steps,
-               "loop": "read_bodies (D2H of the 14-float records) -> write_states (H2D of the same records, "
-                       "velocities unpacked on the device) -> step, one pinned host buffer"}
+        ms_max = max_over_ranks(ms)
+        counts = w.counts()
+        kernels = w.kernels_per_step()
+
+        # ---- per-stage device times (CUDA events at stage boundaries) ----
+        prof = {}
+        for _ in range(max(1, args.profile_steps)):
+            st = w.profile_step(DT)
+            for k, v in st.items():
+                prof[k] = prof.get(k, 0.0) + v / max(1, args.profile_steps)
+
+        # ---- end to end through the C ABI with host buffers ----
+        e2e = None
+        if not args.plain_only:
+            e2e_steps = max(1, min(args.e2e_steps, args.steps))
+            # host buffers in pinned (page-locked) memory, as a host loop that
+            # streams state every step would keep them
+            buf = torch.empty((spec.n_actors, 14), dtype=torch.float32, pin_memory=True).numpy()
+            barrier()
+            t0 = time.perf_counter()
+            for _ in range(e2e_steps):
+                w.read_bodies(buf)
+                w.write_states(buf)
+                w.step(DT)
+            w.synchronize()
+            e2e_s = max_over_ranks(time.perf_counter() - t0)
+            e2e = {"value": sum_over_ranks(n_dyn * e2e_steps) / e2e_s, "unit": UNIT,
+                   "h2d_bytes_per_step": 56 * spec.n_actors, "d2h_bytes_per_step": 56 * spec.n_actors,
+                   "steps": e2e_steps,
+                   "loop": "read_bodies (D2H of the 14-float records) -> write_states (H2D of the same records, "
+                           "velocities unpacked on the device) -> step, one pinned host buffer, host clock"}
+        clocks = sampler.stop()
+        if not clocks_bad(clocks) or attempt == 1:
+            break
+        w.close()
+    value = sum_over_ranks(n_dyn * args.steps) / (ms_max / 1e3)
+    ms_step = ms_max / args.steps
+    peak, peak_kind = measured_peaks()
+    roofline = roofline_of(counts, ms_step, prof, peak, peak_kind)
+    w.close()
+
+    # ---- the plain run from its seeded start ----
+    plain_run = None
+    if args.run_steps and not args.plain_only:
+        plain_run = plain_run_leg(torch, pkg, local_rank, args, max_over_ranks, sum_over_ranks, barrier)
 
     # ---- batched forward ----
     batched = None
@@ -539,21 +622,25 @@ def run_b200(args, rank, world, local_rank):
         bms_max = max_over_ranks(bms)
         bvalue = sum_over_ranks(nb_dyn * args.batched_steps) / (bms_max / 1e3)
         bprof = wb.profile_step(DT)
+        bcounts = wb.counts()
+        bkernels = wb.kernels_per_step()
+        wb.close()
         same = plain_same_bodies(torch, pkg, specs, local_rank, args.same_scenes, args.same_steps)
         batched = {"workload": BATCHED_WORKLOAD, "scenes": len(specs) * world, "bodies": nb_dyn * world,
                    "steps": args.batched_steps, "value": bvalue, "unit": UNIT,
                    "ms_per_step": bms_max / args.batched_steps, "clocks": bclocks,
                    "stages_ms": {k: round(v, 4) for k, v in bprof.items()},
-                   "counts": wb.counts(), "gpu_launches": wb.kernels_per_step() * args.batched_steps,
+                   "counts": bcounts, "gpu_launches": bkernels * args.batched_steps,
                    "plain_same_bodies": same,
                    "vs_plain_same_bodies": bvalue / world / same["value"] if same else None}
-        wb.close()
 
-    # ---- differentiable rollout (forward + adjoint) ----
+    # ---- differentiable rollouts (forward + adjoint) ----
     diff = None
     if not args.no_diff and not args.plain_only:
         diff = differentiable_leg(torch, pkg, local_rank, args)
-    diff4 = differentiable_leg_at_scale(torch, pkg, local_rank, args) if args.diff4 and not args.plain_only else None
+    diff4 = None
+    if not args.no_diff4 and not args.no_diff and not args.plain_only:
+        diff4 = differentiable_leg_at_scale(torch, pkg, local_rank, args)
 
     # ---- cooked convex hulls ----
     convex = None
@@ -563,57 +650,77 @@ def run_b200(args, rank, world, local_rank):
     # ---- CPU baseline: the reference NativeCpu scene on this host ----
     cpu = None
     if rank == 0 and world == 1 and not args.plain_only:
-        cpu = cpu_baseline(spec, args.cpu_seconds)
+        cpu = cpu_baseline(spec, start, args.cpu_seconds)
 
     if rank == 0:
-        ws_mb = (counts["pairs"] * (2 * 332 + 112 + 16) + counts["bodies"] * 400 + counts["shapes"] * 250) / 2**20
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic: seeded generator with the workload's distributions (no dataset)",
-            "config": {"workload": PLAIN_WORKLOAD, "bodies": n_dyn, "shapes": spec.n_shapes,
-                       "joints": int(spec.joints.shape[0]), "dt": DT, "position_iterations": 4,
-                       "velocity_iterations": 1,
-                       "l2": f"resident working set ~{ws_mb:.0f} MB > 126 MB L2 (not flushed)",
-                       "parallelism": "replicas" if world > 1 else "single GPU"},
-            "batched": batched,
-            "batched_vs_plain": batched["vs_plain_same_bodies"] if batched else None,
-            "batched_vs_plain_scene": (batched["value"] / value) if batched else None,
-            "e2e": e2e,
-            "differentiable": diff,
-            "differentiable_at_scale": diff4,
-            "convex": convex,
-            "backward_forward_ratio": diff["backward_forward_ratio"] if diff else None,
+            "data": "synthetic: seeded generator with the workload's distributions (no dataset); settled "
+                    "start state from the reference's own run of the same workload",
+            "config": plain_config(spec, start, world),
             "gpu_launches": kernels * args.steps,
+            "kernels_per_step": kernels,
+            "clocks": clocks,
+            "counts": counts,
             "roofline": roofline,
             "cpu_baseline": cpu,
-            "clocks": clocks,
-            "stages_ms": {k: round(v, 4) for k, v in prof.items()},
-            "counts": counts,
+            "e2e": e2e,
+            "plain_run": plain_run,
+            "convex": convex,
+            "differentiable": diff,
+            "differentiable_at_scale": diff4,
+            "batched": batched,
+            "summary": {
+                "settled_value": value, "settled_ms_per_step": ms_step,
+                "settled_vs_cpu_baseline": (value / cpu["value"]) if cpu and cpu.get("value") else None,
+                "e2e_value": e2e["value"] if e2e else None,
+                "plain_run_value": plain_run["value"] if plain_run else None,
+                "batched_value": batched["value"] if batched else None,
+                "batched_vs_plain_same_bodies": batched["vs_plain_same_bodies"] if batched else None,
+                "batched_vs_plain_scene_run": (batched["value"] / plain_run["value"])
+                if batched and plain_run else None,
+                "backward_forward_ratio": diff["backward_forward_ratio"] if diff else None,
+                "backward_forward_ratio_at_scale": diff4["backward_forward_ratio"] if diff4 else None,
+                "roofline_frac": roofline["frac"],
+            },
         }
         print(json.dumps(line), flush=True)
-    w.close()
 
 
-def cpu_baseline(spec, seconds):
+def ref_settled_sample(spec, warmup, max_steps, budget_s, warmup_budget_s=None):
+    """The reference NativeCpu scene from the same start: `warmup` untimed
+    steps (bounded by warmup_budget_s), then up to `max_steps` timed steps
+    within `budget_s` seconds.  Returns (steps, seconds, warm-up steps)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refscene
+    r = refscene.RefScene(spec)
+    t0 = time.perf_counter()
+    done_w = 0
+    while done_w < warmup and (warmup_budget_s is None or time.perf_counter() - t0 < warmup_budget_s):
+        r.step(DT, 1)
+        done_w += 1
+    n = 0
+    t0 = time.perf_counter()
+    while n < max_steps and (n == 0 or time.perf_counter() - t0 < budget_s):
+        r.step(DT, 1)
+        n += 1
+    el = time.perf_counter() - t0
+    r.close()
+    return n, el, done_w
+
+
+def cpu_baseline(spec, start, seconds):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import refscene
     if not refscene.available():
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                 "sample": "reference harness not built"}
-    r = refscene.RefScene(spec)
-    r.step(DT, 1)   # first step rebuilds the SAP endpoint lists; not timed
-    n = 0
-    t0 = time.perf_counter()
-    while time.perf_counter() - t0 < seconds and n < 200:
-        r.step(DT, 1)
-        n += 1
-    el = time.perf_counter() - t0
-    r.close()
+    n, el, wu = ref_settled_sample(spec, 1, 200, seconds)
     return {"value": spec.n_bodies * n / el, "unit": UNIT, "cores": 2, "kind": "reference",
-            "sample": f"steps 2..{n + 1} of the same {spec.n_bodies}-body scene "
-                      f"({el:.1f} s; NativeCpu uses the caller plus one worker thread)"}
+            "sample": f"{n} steps after {wu} untimed step of the same {spec.n_bodies}-body scene from the same "
+                      f"start ({el:.1f} s; NativeCpu uses the caller plus one worker thread)"}
 
 
 # --------------------------------------------------------------- reference arm
@@ -623,17 +730,10 @@ def run_reference(args):
     if not refscene.available():
         print(json.dumps({"impl": "reference", "unavailable": "reference NativeCpu harness not built (oracle/_ref)"}))
         return
-    spec = plain_spec(args.bodies)
-    r = refscene.RefScene(spec)
-    r.step(DT, max(1, min(args.warmup, 2)))
-    budget = 120.0
-    n = 0
-    t0 = time.perf_counter()
-    while n < args.steps and time.perf_counter() - t0 < budget:
-        r.step(DT, 1)
-        n += 1
-    el = time.perf_counter() - t0
-    r.close()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    spec, start = headline_spec(args)
+    # warm-up aligned with the B200 arm's (W steps), bounded in time
+    n, el, wu = ref_settled_sample(spec, args.warmup, args.steps, args.ref_budget, warmup_budget_s=90.0)
     value = spec.n_bodies * n / el
     cores = os.cpu_count() or 1
     batched = None
@@ -649,18 +749,19 @@ def run_reference(args):
         batched = {"value": nb * bsteps / bel, "unit": UNIT, "scenes": len(specs),
                    "sample": f"{len(specs)} of the 4,096 batched scenes x {bsteps} steps, "
                              f"one NativeCpu scene per batched scene over {cores} host threads"}
-    sample = (f"steps {2 if args.warmup else 1}..{n + 1} of the {spec.n_bodies}-body scene "
-              f"({el:.1f} s; {n} of the requested {args.steps} steps within a {budget:.0f} s budget)")
+    sample = (f"{n} timed steps after {wu} untimed warm-up steps of the {spec.n_bodies}-body scene from the same "
+              f"start as the B200 arm ({el:.1f} s; {n} of the requested {args.steps} steps within a "
+              f"{args.ref_budget:.0f} s budget; NativeCpu runs on the caller plus one worker thread)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
-            "steps": n, "requested_steps": args.steps, "warmup": args.warmup,
+            "steps": args.steps, "timed_steps": n, "warmup": args.warmup, "warmup_done": wu,
             "ms_per_step": el / max(n, 1) * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic: seeded generator with the workload's distributions (no dataset)",
-            "config": {"workload": PLAIN_WORKLOAD, "bodies": spec.n_bodies, "shapes": spec.n_shapes},
-            "cpu_baseline": {"value": value, "unit": UNIT, "kind": "reference", "cores": 2,
-                             "sample": sample},
-            "batched": batched,
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "data": "synthetic: seeded generator with the workload's distributions (no dataset); settled "
+                    "start state from the reference's own run of the same workload",
+            "config": plain_config(spec, start, world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "kind": "reference", "cores": 2, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "batched": batched}
     print(json.dumps(line), flush=True)
 
 

@@ -44,6 +44,7 @@ EXPORTS = (
     "fyzz_b200_cook_convex_mesh", "fyzz_b200_convex_mesh_release", "fyzz_b200_cook_error",
     "fyzz_b200_convex_mesh_info", "fyzz_b200_attach_convex_shape", "fyzz_b200_add_scene_ex",
     "fyzz_b200_write_velocities_strided", "fyzz_b200_remove_constraint",
+    "fyzz_b200_set_pair_budget", "fyzz_b200_test_scan",
 )
 STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 
@@ -160,6 +161,8 @@ def lib():
         L.fyzz_b200_rollout_begin.argtypes = [vp, u32, u32]
         L.fyzz_b200_rollout_rewind.argtypes = [vp]
         L.fyzz_b200_fit_pair_budget.argtypes = [vp, f32, P(u32)]
+        L.fyzz_b200_set_pair_budget.argtypes = [vp, u32, P(u32)]
+        L.fyzz_b200_test_scan.argtypes = [vp, u32, i32, P(u32), P(u64)]
         L.fyzz_b200_rollout_forward.argtypes = [vp, f32]
         L.fyzz_b200_rollout_backward.argtypes = [vp] + [vp] * 9
         L.fyzz_b200_read_mass_frames.argtypes = [vp, vp, vp]
@@ -185,6 +188,12 @@ def _f32(x, n):
 
 
 _IDENTITY = np.array([0, 0, 0, 0, 0, 0, 1], np.float32)
+
+
+class LogicError(RuntimeError):
+    """FYZZ_B200_LOGIC_ERROR: the reference's std::logic_error (an operation
+    the world's state does not allow, or a bounded device wait that gave
+    up)."""
 
 
 class World:
@@ -215,6 +224,8 @@ class World:
             raise ValueError(msg)
         if rc == 3:
             raise OverflowError(msg)
+        if rc == 2:
+            raise LogicError(msg)
         raise RuntimeError(msg)
 
     # ---- authoring ----
@@ -485,6 +496,21 @@ class World:
         out = C.c_uint32()
         self._check(lib().fyzz_b200_fit_pair_budget(self.h, headroom, C.byref(out)))
         return out.value
+
+    def set_pair_budget(self, pairs: int) -> int:
+        """Sets the pair budget (at least the live pairs; history kept)."""
+        out = C.c_uint32()
+        self._check(lib().fyzz_b200_set_pair_budget(self.h, pairs, C.byref(out)))
+        return out.value
+
+    def test_scan(self, n: int, skip_first_tile: bool = False):
+        """Test hook of the step's look-back scan: (error bits, mismatches).
+        Raises LogicError when the scan's bounded wait gave up."""
+        bits, bad = C.c_uint32(), C.c_uint64()
+        rc = lib().fyzz_b200_test_scan(self.h, n, 1 if skip_first_tile else 0, C.byref(bits), C.byref(bad))
+        self.last_scan = (bits.value, bad.value)
+        self._check(rc)
+        return bits.value, bad.value
 
     def rollout_begin(self, steps: int, checkpoint_every: int):
         self._check(lib().fyzz_b200_rollout_begin(self.h, steps, checkpoint_every))

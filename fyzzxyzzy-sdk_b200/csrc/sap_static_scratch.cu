@@ -27,7 +27,13 @@
 //  * the first call on a device resolves the scratch array's address with
 //    cudaGetSymbolAddress (which loads this module on that device) and
 //    raises the kernel's dynamic shared-memory limit; make that first call
-//    before any stream capture on the device.
+//    before any stream capture on the device.  The resolved address is kept
+//    per CUDA context, so a context made after cudaDeviceReset resolves it
+//    again on its first call;
+//  * when the pair total exceeds the caller's capacity, only whole owner
+//    buckets that end within the capacity are written: the list is then a
+//    prefix of the full canonical list (deterministic), and the total tells
+//    the caller how much room a complete list needs.
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
@@ -105,6 +111,7 @@ __global__ void __launch_bounds__(kThreads) k_sap_static(const uint32_t* __restr
                                                          uint32_t cap, uint32_t* __restrict__ count,
                                                          unsigned char* scratch) {
     extern __shared__ unsigned long long sk[];
+    __shared__ uint32_t s_total;
     uint4* rec = reinterpret_cast<uint4*>(scratch + kRecOff);
     uint2* meta = reinterpret_cast<uint2*>(scratch + kMetaOff);
     uint32_t* cnt = reinterpret_cast<uint32_t*>(scratch + kCntOff);
@@ -156,8 +163,11 @@ __global__ void __launch_bounds__(kThreads) k_sap_static(const uint32_t* __restr
                 if (!fill) {
                     atomicAdd(cnt + owner, 1u);
                 } else {
-                    const uint32_t pos = atomicAdd(off + owner, 1u);   // off ends at bucket end
-                    if (pos < cap) {
+                    // bucket [off[owner], off[owner + 1]): written only when
+                    // all of it fits, so a truncated list is a canonical prefix
+                    const uint32_t end = owner + 1 < n ? __ldcg(off + owner + 1) : s_total;
+                    if (end <= cap) {
+                        const uint32_t pos = __ldcg(off + owner) + atomicSub(cnt + owner, 1u) - 1u;
                         pairs[2 * size_t(pos)] = owner;
                         pairs[2 * size_t(pos) + 1] = partner;
                     }
@@ -167,18 +177,22 @@ __global__ void __launch_bounds__(kThreads) k_sap_static(const uint32_t* __restr
         __syncthreads();
         if (!fill) {
             const uint32_t total = block_scan(cnt, off, n);
-            if (threadIdx.x == 0) *count = total;
+            if (threadIdx.x == 0) {
+                *count = total;
+                s_total = total;
+            }
+            __syncthreads();
         }
     }
-    // each owner's bucket [off - cnt, off) sorted by partner (insertion sort;
-    // buckets are short)
+    // each written owner bucket [off[o], off[o + 1]) sorted by partner
+    // (insertion sort; buckets are short)
     for (uint32_t o = threadIdx.x; o < n; o += kThreads) {
-        const uint32_t c = __ldcg(cnt + o);
-        const uint32_t end = __ldcg(off + o), begin = end - c;
-        if (c < 2 || begin >= cap) continue;
-        const uint32_t kk = end <= cap ? c : cap - begin;
+        const uint32_t begin = __ldcg(off + o);
+        const uint32_t end = o + 1 < n ? __ldcg(off + o + 1) : s_total;
+        const uint32_t c = end - begin;
+        if (c < 2 || end > cap) continue;
         uint32_t* p = pairs + 2 * size_t(begin) + 1;
-        for (uint32_t i = 1; i < kk; ++i) {
+        for (uint32_t i = 1; i < c; ++i) {
             const uint32_t v = p[2 * size_t(i)];
             uint32_t j = i;
             while (j > 0 && p[2 * size_t(j - 1)] > v) { p[2 * size_t(j)] = p[2 * size_t(j - 1)]; --j; }
@@ -190,6 +204,9 @@ __global__ void __launch_bounds__(kThreads) k_sap_static(const uint32_t* __restr
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 unsigned char* g_scratch[kMaxDevices] = {};
+void* g_scratch_ctx[kMaxDevices] = {};       // the CUDA context g_scratch[dev] was resolved in
+using CtxGetCurrent = int (*)(void**);       // the driver's cuCtxGetCurrent
+CtxGetCurrent g_ctx_get = nullptr;
 
 // Copies a message into the caller's buffer (no formatting, no allocation).
 void put_message(char* out, size_t len, const char* a, const char* b = "") {
@@ -200,11 +217,28 @@ void put_message(char* out, size_t len, const char* a, const char* b = "") {
     out[k] = '\0';
 }
 
-// Once per device, with that device current: resolve the scratch array's
-// address and allow the kernel the shared memory its largest sort needs.
+// Once per device (per CUDA context of the device: a context made after
+// cudaDeviceReset loads this module again), with that device current:
+// resolve the scratch array's address and allow the kernel the shared
+// memory its largest sort needs.
 int setup_device(int dev, unsigned char** out, char* msg, size_t msg_len) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch[dev]) {
+    if (!g_ctx_get) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        const cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) {
+            put_message(msg, msg_len, "cuCtxGetCurrent unavailable: ", cudaGetErrorString(e));
+            return FYZZ_B200_RUNTIME_ERROR;
+        }
+        g_ctx_get = reinterpret_cast<CtxGetCurrent>(fn);
+    }
+    void* ctx = nullptr;
+    if (g_ctx_get(&ctx) != 0 || !ctx) {
+        put_message(msg, msg_len, "no current CUDA context");
+        return FYZZ_B200_RUNTIME_ERROR;
+    }
+    if (!g_scratch[dev] || g_scratch_ctx[dev] != ctx) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_sap_scratch);
         if (e != cudaSuccess || !p) {
@@ -218,6 +252,7 @@ int setup_device(int dev, unsigned char** out, char* msg, size_t msg_len) {
             return FYZZ_B200_RUNTIME_ERROR;
         }
         g_scratch[dev] = static_cast<unsigned char*>(p);
+        g_scratch_ctx[dev] = ctx;
     }
     *out = g_scratch[dev];
     return FYZZ_B200_OK;

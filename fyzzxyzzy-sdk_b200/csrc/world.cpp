@@ -150,8 +150,11 @@ M3 m_t(const M3& a) {
     r.c[2] = {a.c[0].z, a.c[1].z, a.c[2].z};
     return r;
 }
-// Jacobi diagonalisation with quaternion rotations (S. Melax): at most 24
-// sweeps, each rotating away the largest off-diagonal element.
+// Jacobi diagonalisation with quaternion rotations (S. Melax), as PhysX's
+// PxDiagonalize does it (src/physx_port/foundation_source/FdMathUtils.cpp:
+// 66-110 of the reference, which compound.cpp calls for the mass frame): at
+// most 24 sweeps, each rotating away the largest off-diagonal element, with
+// the same cut-offs, so the principal frames are bit-identical.
 v3 diagonalize(const M3& m, qt& frame) {
     qt q = {0, 0, 0, 1};
     M3 d = m;
@@ -612,7 +615,7 @@ public:
         ensure_device();
         if (steps == 0) return;
         for (int attempt = 0; attempt < 8; ++attempt) {
-            snapshot();
+            snapshot(steps);
             run_steps(dt, steps);
             const uint32_t err = read_err();
             if (!err) {
@@ -626,7 +629,7 @@ public:
                 continue;
             }
             ev_device_valid_ = false;
-            throw std::overflow_error("Device step reported error bits " + std::to_string(err));
+            raise_step_error(err);
         }
         ev_device_valid_ = false;
         throw std::overflow_error("Pair capacity could not be satisfied");
@@ -647,6 +650,25 @@ public:
         const uint64_t want = uint64_t(double(std::max(live[0], live[1])) * headroom) + 4096;
         const uint32_t cap = uint32_t(std::min<uint64_t>(want, 0x7fffffffull));
         if (cap < std::max(live[0], live[1])) throw std::overflow_error("Pair budget below the live pairs");
+        resize_pairs_keeping(cap, live);
+    }
+    // Sets the pair budget to `cap` pairs (at least the live pairs of both
+    // generations), keeping the contact-manager history.
+    uint32_t set_pair_budget(uint32_t cap) {
+        if (cap == 0 || cap > 0x7fffffffu) throw std::invalid_argument("Pair budget must be in [1, 2^31)");
+        check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+        ensure_device();
+        release_rollout();
+        uint32_t live[2] = {0, 0};
+        for (int k = 0; k < 2; ++k)
+            check_cuda(cudaMemcpy(&live[k], sets_[k].n, 4, cudaMemcpyDeviceToHost), "read");
+        resize_pairs_keeping(std::max({cap, live[0], live[1], 1u}), live);
+        return d_.pair_cap;
+    }
+    // Re-allocates the pair arrays for `cap` pairs; both generations' live
+    // records (keys, PCM caches, friction histories, touch counts) are
+    // carried over, so the next step continues exactly as it would have.
+    void resize_pairs_keeping(uint32_t cap, const uint32_t live[2]) {
         std::vector<void*> tmp;
         ManagerSet keep[2];
         for (int k = 0; k < 2; ++k) {
@@ -665,6 +687,43 @@ public:
         last_cur_ = last;
     }
     uint32_t pair_budget() const { return d_.pair_cap; }
+    // Test hook of the step's exclusive scan (the look-back scan every
+    // step runs, on this world's scan scratch): scans n ones into a
+    // temporary buffer.  With skip_first_tile the scan's tile ticket starts
+    // at 1, so no block ever takes tile 0 and the block that takes tile 1
+    // waits for a tile state that is never published: its bounded wait
+    // gives up and sets the logic error bit.  The scan's last block still
+    // resets the ticket, so later scans (and steps) run clean.  Returns the
+    // device error bits; mismatches counts outputs other than their index.
+    uint32_t scan_selftest(uint32_t n, bool skip_first_tile, uint64_t* mismatches) {
+        if (n == 0 || n > (1u << 26)) throw std::invalid_argument("Scan self-test size must be in [1, 2^26]");
+        check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+        ensure_device();
+        if (scan_tmp_words_for(n) > d_.scan_tmp_words)
+            throw std::invalid_argument("Scan self-test larger than the world's scan scratch");
+        std::vector<void*> tmp;
+        uint32_t *in = nullptr, *out = nullptr, *err = nullptr, *total = nullptr;
+        dalloc(in, n, tmp); dalloc(out, n, tmp); dalloc(err, 1, tmp); dalloc(total, 1, tmp);
+        upload(in, std::vector<uint32_t>(n, 1u), stream_);
+        check_cuda(cudaMemsetAsync(out, 0xff, size_t(n) * 4, stream_), "memset");
+        check_cuda(cudaMemsetAsync(err, 0, 4, stream_), "memset");
+        if (skip_first_tile) {
+            const uint32_t one = 1u;
+            check_cuda(cudaMemcpyAsync(d_.scan_tmp + 1, &one, 4, cudaMemcpyHostToDevice, stream_), "ticket");
+        }
+        scan_exclusive(in, out, n, nullptr, total, d_.scan_tmp, d_.scan_tmp_words, stream_, err);
+        check_cuda(cudaGetLastError(), "scan launch");
+        std::vector<uint32_t> h(n);
+        uint32_t bits = 0;
+        check_cuda(cudaMemcpyAsync(h.data(), out, size_t(n) * 4, cudaMemcpyDeviceToHost, stream_), "read");
+        check_cuda(cudaMemcpyAsync(&bits, err, 4, cudaMemcpyDeviceToHost, stream_), "read");
+        check_cuda(cudaStreamSynchronize(stream_), "scan sync");
+        for (void* p : tmp) cudaFree(p);
+        uint64_t bad = 0;
+        for (uint32_t i = 0; i < n; ++i) bad += h[i] != i ? 1u : 0u;
+        if (mismatches) *mismatches = bad;
+        return bits;
+    }
     // ---------------- differentiable rollouts ----------------
     // A rollout of `steps` steps keeps a full-state checkpoint every `every`
     // steps.  The backward pass walks the segments in reverse: it restores
@@ -1094,7 +1153,7 @@ public:
         check_cuda(cudaSetDevice(device_), "cudaSetDevice");
         ensure_device();
         for (int attempt = 0; attempt < 8; ++attempt) {
-            snapshot();
+            snapshot(1);
             check_cuda(cudaMemsetAsync(d_.err, 0, 4, stream_), "memset");
             const DevState s = view(parity_);
             enqueue_broadphase(s, stream_);
@@ -1108,7 +1167,7 @@ public:
             }
             restore();
             if (err & kErrPairCapacity) { grow_pairs(d_.pair_cap * 2u); continue; }
-            throw std::overflow_error("Device collision reported error bits " + std::to_string(err));
+            raise_step_error(err);
         }
     }
     void synchronize() { check_cuda(cudaStreamSynchronize(stream_), "synchronize"); }
@@ -1129,7 +1188,7 @@ public:
             cudaEventRecord(x->ev[stage], st);
             x->seen[stage] = true;
         };
-        snapshot();
+        snapshot(1);
         d_.dt = dt;
         check_cuda(cudaMemsetAsync(d_.err, 0, 4, stream_), "memset");
         const DevState s = view(parity_);
@@ -1148,7 +1207,7 @@ public:
         for (int i = 0; i <= kStEnd; ++i) cudaEventDestroy(ctx.ev[i]);
         if (err) {
             restore();
-            throw std::overflow_error("Device step reported error bits " + std::to_string(err));
+            raise_step_error(err);
         }
         ++steps_done_;
     }
@@ -1402,8 +1461,28 @@ private:
             parity_ ^= 1;
         }
     }
-    void snapshot() {
+    // Failure atomicity (Scene::step's checkpoint and rollback,
+    // scene.cpp:9706-10020, 11013-11016): the bodies and the device
+    // counters (the friction-history epoch among them) are saved before each
+    // launch.  The contact-manager generation the first step reads is only
+    // read by that step; a batch of several steps writes it again from its
+    // second step on, so for a batch its live records are saved as well.  A
+    // rollback therefore keeps every PCM cache, friction history and touch
+    // count, and a retried batch runs exactly as a batch that never failed.
+    void snapshot(uint32_t steps) {
         const size_t n = size_t(d_.n_bodies) * 16;
+        check_cuda(cudaMemcpyAsync(bk_counters_, d_.counters, kCntSlots * 4, cudaMemcpyDeviceToDevice, stream_),
+                   "snapshot");
+        snap_multi_ = steps > 1;
+        if (snap_multi_) {
+            if (!bk_set_.key) {
+                const size_t cap = d_.pair_cap;
+                dalloc(bk_set_.key, cap, pair_owned_); dalloc(bk_set_.cache, cap, pair_owned_);
+                dalloc(bk_set_.fric, cap, pair_owned_); dalloc(bk_set_.count, cap, pair_owned_);
+                dalloc(bk_set_.n, 1, pair_owned_);
+            }
+            enqueue_copy_set(bk_set_, sets_[last_cur_], d_.pair_cap, stream_);
+        }
         check_cuda(cudaMemcpyAsync(bk_p_, d_.b_p, n, cudaMemcpyDeviceToDevice, stream_), "snapshot");
         check_cuda(cudaMemcpyAsync(bk_q_, d_.b_q, n, cudaMemcpyDeviceToDevice, stream_), "snapshot");
         check_cuda(cudaMemcpyAsync(bk_v_, d_.b_v, n, cudaMemcpyDeviceToDevice, stream_), "snapshot");
@@ -1423,9 +1502,11 @@ private:
         check_cuda(cudaMemcpyAsync(d_.b_wake, bk_wake_, n / 4, cudaMemcpyDeviceToDevice, stream_), "restore");
         check_cuda(cudaMemcpyAsync(d_.b_sleep, bk_sleep_, n / 4, cudaMemcpyDeviceToDevice, stream_), "restore");
         check_cuda(cudaMemcpyAsync(d_.b_sacc, bk_sacc_, 2 * n, cudaMemcpyDeviceToDevice, stream_), "restore");
-        // contact-manager history is discarded, as after a reference rollback
-        check_cuda(cudaMemsetAsync(sets_[0].n, 0, 4, stream_), "restore");
-        check_cuda(cudaMemsetAsync(sets_[1].n, 0, 4, stream_), "restore");
+        check_cuda(cudaMemcpyAsync(d_.counters, bk_counters_, kCntSlots * 4, cudaMemcpyDeviceToDevice, stream_),
+                   "restore");
+        // the generation the batch started from, as the reference's journal
+        // restores its contact managers
+        if (snap_multi_) enqueue_copy_set(sets_[snap_last_], bk_set_, d_.pair_cap, stream_);
         check_cuda(cudaMemsetAsync(d_.err, 0, 4, stream_), "restore");
         check_cuda(cudaStreamSynchronize(stream_), "restore sync");
         parity_ = snap_parity_;
@@ -1438,6 +1519,11 @@ private:
         release_segment_graphs();
         for (void* p : owned_) cudaFree(p);
         owned_.clear();
+        d_.j_a = d_.j_b = d_.j_kind = d_.j_row = nullptr;
+        d_.j_len = nullptr;
+        d_.j_la = d_.j_lb = d_.j_qa = d_.j_qb = nullptr;
+        d_.jrow = nullptr;
+        joint_cap_ = jrow_cap_ = 0;
         d_pack_ = nullptr;
         d_vel6_ = nullptr;
         vel_stride_cap_ = 0;
@@ -1449,6 +1535,7 @@ private:
     void alloc_pairs(uint32_t cap) {
         for (void* p : pair_owned_) cudaFree(p);
         pair_owned_.clear();
+        bk_set_ = ManagerSet{};
         for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
         release_segment_graphs();
         d_.pair_cap = cap;
@@ -1515,10 +1602,20 @@ private:
         dalloc(d_.ev_cnt, cap, pair_owned_);
         dalloc(d_.ev_pt_off, cap + 1, pair_owned_);
     }
+    // After a rollback: a larger budget, with the generation the next step
+    // reads carried over.
     void grow_pairs(uint32_t cap) {
-        alloc_pairs(cap);
-        parity_ = 0;
-        last_cur_ = 1;
+        uint32_t live[2] = {0, 0};
+        for (int k = 0; k < 2; ++k)
+            check_cuda(cudaMemcpy(&live[k], sets_[k].n, 4, cudaMemcpyDeviceToHost), "read");
+        live[last_cur_ ^ 1] = 0;   // the failed step's partial generation is not kept
+        check_cuda(cudaMemsetAsync(sets_[last_cur_ ^ 1].n, 0, 4, stream_), "memset");
+        resize_pairs_keeping(cap, live);
+    }
+    [[noreturn]] void raise_step_error(uint32_t err) {
+        const std::string bits = "Device step reported error bits " + std::to_string(err);
+        if (err & kErrLogic) throw std::logic_error(bits + " (a bounded device wait gave up)");
+        throw std::overflow_error(bits);
     }
 
     void upload_bodies() {
@@ -1563,9 +1660,24 @@ private:
     }
     // The device joint tables: live joints per scene, constraint slot
     // descending (scene.cpp:7153-7162), their rows, and the constraints
-    // counted on each dynamic endpoint (scene.cpp:2728-2749).  Arrays are
-    // allocated for the current count (the old ones stay owned until the
-    // device state is released).
+    // counted on each dynamic endpoint (scene.cpp:2728-2749).  The tables
+    // hold kJointReserve joints (and their rows) beyond the count they were
+    // sized for, so joint edits between steps only upload; a table that
+    // must grow is freed and allocated again.
+    void free_joint_tables() {
+        void* tabs[] = {d_.j_a, d_.j_b, d_.j_len, d_.j_kind, d_.j_row, d_.j_la, d_.j_lb, d_.j_qa, d_.j_qb, d_.jrow};
+        for (void* p : tabs) {
+            if (!p) continue;
+            auto it = std::find(owned_.begin(), owned_.end(), p);
+            if (it != owned_.end()) owned_.erase(it);
+            cudaFree(p);
+        }
+        d_.j_a = d_.j_b = d_.j_kind = d_.j_row = nullptr;
+        d_.j_len = nullptr;
+        d_.j_la = d_.j_lb = d_.j_qa = d_.j_qb = nullptr;
+        d_.jrow = nullptr;
+        joint_cap_ = jrow_cap_ = 0;
+    }
     void upload_joints() {
         std::vector<HostJoint> js;
         for (const auto& j : joints_)
@@ -1589,11 +1701,19 @@ private:
         }
         d_.n_joints = uint32_t(n);
         d_.n_jrows = nrows;
-        dalloc(d_.j_a, n, owned_); dalloc(d_.j_b, n, owned_); dalloc(d_.j_len, n, owned_);
-        dalloc(d_.j_kind, n, owned_); dalloc(d_.j_row, n, owned_);
-        dalloc(d_.j_la, n, owned_); dalloc(d_.j_lb, n, owned_);
-        dalloc(d_.j_qa, n, owned_); dalloc(d_.j_qb, n, owned_);
-        dalloc(d_.jrow, nrows, owned_);
+        if (n > joint_cap_ || nrows > jrow_cap_ || !d_.j_a) {
+            // synchronise before freeing: earlier launches may still read the old tables
+            check_cuda(cudaStreamSynchronize(stream_), "joint tables");
+            free_joint_tables();
+            const size_t jc = n + kJointReserve, rc = size_t(nrows) + 6u * kJointReserve;
+            dalloc(d_.j_a, jc, owned_); dalloc(d_.j_b, jc, owned_); dalloc(d_.j_len, jc, owned_);
+            dalloc(d_.j_kind, jc, owned_); dalloc(d_.j_row, jc, owned_);
+            dalloc(d_.j_la, jc, owned_); dalloc(d_.j_lb, jc, owned_);
+            dalloc(d_.j_qa, jc, owned_); dalloc(d_.j_qb, jc, owned_);
+            dalloc(d_.jrow, rc, owned_);
+            joint_cap_ = uint32_t(jc);
+            jrow_cap_ = uint32_t(rc);
+        }
         std::vector<uint32_t> jcount(bodies_.size(), 0u);
         for (const auto& j : js) {
             if (bodies_[j.a].dynamic) ++jcount[j.a];
@@ -1691,6 +1811,7 @@ private:
         dalloc(d_.sl_act, nb, owned_); dalloc(d_.sl_spec, nb, owned_); dalloc(d_.sl_root, nb, owned_);
         dalloc(bk_p_, nb, owned_); dalloc(bk_q_, nb, owned_); dalloc(bk_v_, nb, owned_); dalloc(bk_w_, nb, owned_);
         dalloc(bk_wake_, nb, owned_); dalloc(bk_sleep_, nb, owned_); dalloc(bk_sacc_, 2 * size_t(nb), owned_);
+        dalloc(bk_counters_, kCntSlots, owned_);
         dalloc(d_.s_body, ns, owned_); dalloc(d_.s_type, ns, owned_); dalloc(d_.s_scene, ns, owned_);
         dalloc(d_.s_geom, ns, owned_); dalloc(d_.s_lp, ns, owned_); dalloc(d_.s_lq, ns, owned_);
         dalloc(d_.s_mat, ns, owned_); dalloc(d_.s_wp, ns, owned_); dalloc(d_.s_wq, ns, owned_);
@@ -1792,6 +1913,7 @@ private:
     std::vector<std::vector<uint32_t>> free_joints_;   // per scene: retired slots, most recent last
     bool joints_dirty_ = false;
     static constexpr uint32_t kJointReserve = 256;
+    uint32_t joint_cap_ = 0, jrow_cap_ = 0;   // joints / joint rows the device tables hold
     std::vector<uint32_t> scene_body_begin_, scene_shape_begin_;
     std::vector<bool> scene_has_floor_;
     std::vector<uint32_t> h_fbegin_;
@@ -1805,6 +1927,9 @@ private:
     float* d_vel6_ = nullptr;    // write_velocities records
     uint32_t vel_stride_cap_ = 0; // floats per record d_vel6_ holds
     uint32_t* bk_sleep_ = nullptr;
+    uint32_t* bk_counters_ = nullptr;
+    ManagerSet bk_set_;          // a batch's starting generation (allocated on the first batch)
+    bool snap_multi_ = false;
     bool sleep_enabled_ = true;
     cudaGraphExec_t graphs_[4] = {nullptr, nullptr, nullptr, nullptr};   // [parity + 2 * sleeping]
     float graph_dt_ = -1.0f;
@@ -2191,6 +2316,21 @@ int fyzz_b200_fit_pair_budget(fyzz_b200_world* w, float headroom, uint32_t* budg
     return guarded(w, [&](auto& W) {
         W.fit_pair_budget(headroom);
         if (budget_out) *budget_out = W.pair_budget();
+    });
+}
+int fyzz_b200_set_pair_budget(fyzz_b200_world* w, uint32_t pairs, uint32_t* budget_out) {
+    return guarded(w, [&](auto& W) {
+        const uint32_t cap = W.set_pair_budget(pairs);
+        if (budget_out) *budget_out = cap;
+    });
+}
+int fyzz_b200_test_scan(fyzz_b200_world* w, uint32_t n, int skip_first_tile, uint32_t* error_bits,
+                        uint64_t* mismatches) {
+    return guarded(w, [&](auto& W) {
+        const uint32_t bits = W.scan_selftest(n, skip_first_tile != 0, mismatches);
+        if (error_bits) *error_bits = bits;
+        if (bits & fyzz::b200::kErrLogic)
+            throw std::logic_error("Scan look-back wait gave up (error bits " + std::to_string(bits) + ")");
     });
 }
 int fyzz_b200_rollout_begin(fyzz_b200_world* w, uint32_t steps, uint32_t checkpoint_every) {

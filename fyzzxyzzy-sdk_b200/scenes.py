@@ -236,6 +236,43 @@ def box_stack_scene(n: int, seed: int, height_range=(5, 20), jitter=1.0e-3,
                      [[_box((0.5, 0.5, 0.5))] for _ in range(n)], mats)
 
 
+def cube_block(nx: int, ny: int, nz: int, half: float = 0.25, jitter: float = 1.0e-4, seed: int = 0,
+               density: float = 1000.0, friction: float = 0.5) -> SceneSpec:
+    """One block of nx x ny x nz touching cubes (half extent `half`) resting
+    on the floor, with N(0, jitter) placement noise: every cube touches its
+    neighbours, so the block is a single island with several contact
+    managers per cube."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    g = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"), -1).reshape(-1, 3)
+    pos = (g * (2.0 * half) + np.array([-(nx - 1) * half, half, -(nz - 1) * half])).astype(np.float32)
+    pos += rng.normal(0.0, jitter, pos.shape).astype(np.float32)
+    pos[:, 1] = np.maximum(pos[:, 1], half)
+    n = pos.shape[0]
+    quat = np.tile(np.array([0, 0, 0, 1], np.float32), (n, 1))
+    z = np.zeros((n, 3), np.float32)
+    mats = np.tile(np.array([friction, friction, 0.0], np.float32), (n, 1))
+    return _assemble(pos, quat, z, z, density, [[_box((half, half, half))] for _ in range(n)], mats)
+
+
+def with_state(spec: SceneSpec, states: np.ndarray) -> SceneSpec:
+    """A copy of `spec` whose dynamic bodies start from `states`: per actor
+    (the floor first when the scene has one) the 14-float records of
+    World.read_bodies / the reference's body states (position 3, linear
+    velocity 3, orientation xyzw 4, angular velocity 3, sleeping 1).
+    Shapes, materials, densities and joints are kept."""
+    st = np.asarray(states, np.float32)
+    first = 1 if spec.floor is not None else 0
+    st = st[first: first + spec.n_bodies]
+    bodies = spec.bodies.copy()
+    bodies[:, 0:3] = st[:, 0:3]
+    bodies[:, 3:7] = st[:, 6:10]
+    bodies[:, 7:10] = st[:, 3:6]
+    bodies[:, 10:13] = st[:, 10:13]
+    out = SceneSpec(**{k: getattr(spec, k) for k in spec.__dataclass_fields__})
+    out.bodies = bodies
+    return out
+
+
 def batched_scenes(n_scenes: int = 4096, low: int = 16, high: int = 512,
                    base_seed: int = 0) -> list[SceneSpec]:
     """Batched forward: per-scene body count log-uniform in [low, high];

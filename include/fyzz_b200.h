@@ -173,7 +173,15 @@ int fyzz_b200_add_scene_ex(fyzz_b200_world* w, uint32_t n_bodies, const float* b
                            int has_floor, float floor_height, const float* floor_mat,
                            uint32_t n_meshes, fyzz_b200_convex_mesh* const* meshes, uint32_t* first_body_out);
 
-/* ---- stepping: World::step (world.h:459, scene.cpp:10725) ---- */
+/* ---- stepping: World::step (world.h:459, scene.cpp:10725) ----
+ * Failure-atomic like Scene::step (scene.cpp:11013-11016): when the device
+ * reports an error the world returns to its state before the call (bodies,
+ * sleep state and the contact-manager history: PCM caches, friction
+ * histories, touch counts).  A pair-budget overflow grows the budget and
+ * runs the steps again; non-finite state returns FYZZ_B200_OVERFLOW and a
+ * bounded device wait that gave up FYZZ_B200_LOGIC_ERROR.  Velocities
+ * written in bulk (fyzz_b200_write_velocities*) are not checked on the
+ * host: a non-finite one makes the next step fail this way. */
 int fyzz_b200_step(fyzz_b200_world* w, float seconds);
 /* `steps` consecutive steps launched as one captured CUDA graph per step,
  * with a single error check at the end. */
@@ -302,6 +310,15 @@ int fyzz_b200_rollout_rewind(fyzz_b200_world* w);
  * A later step that needs more pairs grows it again (and a rollout that
  * sees it grow fails with FYZZ_B200_LOGIC_ERROR). */
 int fyzz_b200_fit_pair_budget(fyzz_b200_world* w, float headroom, uint32_t* budget_out);
+/* Sets the pair budget to `pairs` (raised to the live pairs of both
+ * contact-manager generations), keeping the history like
+ * fyzz_b200_fit_pair_budget; for callers that size device memory up front.
+ * A step that finds more overlap pairs than the budget is rolled back (the
+ * contact-manager history included), the budget doubles and the step runs
+ * again, with the same result as a step that had room.  No reference
+ * counterpart (the reference's GPU owner has a fixed 32,768-pair capacity,
+ * native_gpu_world.cpp). */
+int fyzz_b200_set_pair_budget(fyzz_b200_world* w, uint32_t pairs, uint32_t* budget_out);
 int fyzz_b200_rollout_forward(fyzz_b200_world* w, float seconds);
 /* Loss gradients with respect to the final mass-frame centres (3 per body),
  * orientations (4 per body, may be NULL), linear and angular velocities
@@ -316,6 +333,16 @@ int fyzz_b200_rollout_backward(fyzz_b200_world* w, const float* grad_center,
 /* Mass-frame centres (3 per body) and orientations (4 per body) of all
  * bodies (either may be NULL). */
 int fyzz_b200_read_mass_frames(fyzz_b200_world* w, float* centers, float* orientations);
+
+/* Test hook of the step's exclusive scan (no reference counterpart): scans
+ * n ones with this world's scan scratch.  skip_first_tile starts the scan's
+ * tile ticket at 1, so one block waits for a tile that never publishes; the
+ * wait is bounded (2^18 polls), then the scan sets the logic error bit and
+ * this call returns FYZZ_B200_LOGIC_ERROR.  error_bits receives the device
+ * error bits, mismatches the outputs that differ from their index.  Later
+ * scans and steps run normally. */
+int fyzz_b200_test_scan(fyzz_b200_world* w, uint32_t n, int skip_first_tile, uint32_t* error_bits,
+                        uint64_t* mismatches);
 
 /* ---- broadphase / narrowphase views (Scene::pairs, found_pairs,
  *      lost_pairs, contacts: scene.h:827-833) ---- */
@@ -361,14 +388,18 @@ int fyzz_b200_read_step_counters(fyzz_b200_world* w, uint32_t* out, uint32_t n);
  *    in time (other streams, other threads) race; order them on one stream;
  *  - the first call on a device (with that device current) resolves the
  *    array's address and the kernel's shared-memory limit; make it before
- *    any stream capture on that device.
+ *    any stream capture on that device (after a cudaDeviceReset the next
+ *    call resolves them again in the new context).
  * Inputs (device pointers): bounds_dev n_shapes x 6 encoded values (min x,
  * y, z, max x, y, z: the layout of fyzz_b200_read_encoded_bounds), body_dev
  * n_shapes values of body id | (1 << 31 if the body is dynamic).  Pairs
  * follow the reference's full sweep (scene.cpp:2635-2704: 3-axis overlap,
  * different bodies, at least one dynamic), are written as (a, b) with a < b
  * in ascending order to pairs_dev (at most pair_cap pairs), and their total
- * to *count_dev; when the total exceeds pair_cap the list is incomplete.
+ * to *count_dev.  When the total exceeds pair_cap, only whole owner buckets
+ * (all pairs of one lower shape id) that end within pair_cap are written:
+ * the written pairs are a prefix of the full list and the rest of pairs_dev
+ * is left as it was; call again with pair_cap >= *count_dev for all pairs.
  * Enqueued on stream (a cudaStream_t, NULL = legacy default stream); the
  * results are ready when that stream reaches this point.  message (may be
  * NULL) receives the reason for a non-zero status. */

@@ -148,3 +148,25 @@ def test_removed_and_added_joints_track_oracle(pkg, oracle, scenes):
         w.remove_constraint((1 << 32) | 3)       # expired generation
     with pytest.raises((ValueError, RuntimeError)):
         w.remove_constraint((1 << 32) | 9999)    # unknown slot
+
+
+def test_joint_edits_keep_device_memory_flat(pkg, scenes):
+    # grab-and-release between steps: 200 add / remove edits reuse the
+    # device joint tables instead of allocating new ones
+    import torch
+    spec = scenes.random_boxes(40, seed=8, xz=2.0, y=(0.4, 2.0))
+    w = pkg.World(0)
+    first = w.add_scene(spec)
+    w.step(DT)
+    held = w.add_center_distance_constraint(first, first + 1, 0.7)
+    w.step(DT)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for k in range(200):
+        w.remove_constraint(held)
+        held = w.add_center_distance_constraint(first + (k % 20), first + 20 + (k % 20), 0.7)
+        w.step(DT)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free0 - free1 < 4 << 20, (free0, free1)
+    assert np.all(np.isfinite(w.read_bodies()))

@@ -2,7 +2,6 @@
 itself (tests/golden/make_golden.py).  Integer work must be bit-exact; the
 float work is also bit-exact because the oracle evaluates every expression
 in the reference's order without FMA contraction."""
-import importlib
 import os
 
 import numpy as np
@@ -10,8 +9,6 @@ import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden")
-scenes_mod = importlib.import_module("fyzzxyzzy-sdk_b200.scenes")
-mg = importlib.import_module("golden.make_golden") if False else None
 
 
 def _golden_specs():

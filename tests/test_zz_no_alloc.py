@@ -89,9 +89,17 @@ def test_capacity_and_empty(pkg, scenes):
     w.collide()
     want = w.pairs(0)
     flags = spec.shape_body.astype(np.uint32) | DYNAMIC
-    total, got = static_pairs(pkg, w.encoded_bounds(), flags, cap=len(want) // 3)
+    cap = len(want) // 3
+    total, got = static_pairs(pkg, w.encoded_bounds(), flags, cap=cap)
     assert total == len(want)             # the full total, list truncated
-    assert got.shape[0] == len(want) // 3
+    # only whole owner buckets that fit are written: a prefix of the full
+    # list ending at a bucket boundary, the rest of the buffer untouched
+    written = got[:, 0] != 0xFFFFFFFF
+    k = int(written.sum())
+    assert 0 < k <= cap and np.all(written[:k])
+    np.testing.assert_array_equal(got[:k], want[:k])
+    assert want[k, 0] != want[k - 1, 0]
+    assert np.all(got[k:] == 0xFFFFFFFF)
     total0, got0 = static_pairs(pkg, np.zeros((0, 6), np.uint32), np.zeros(0, np.uint32))
     assert total0 == 0 and got0.shape[0] == 0
 
