@@ -45,6 +45,7 @@ EXPORTS = (
     "fyzz_b200_convex_mesh_info", "fyzz_b200_attach_convex_shape", "fyzz_b200_add_scene_ex",
     "fyzz_b200_write_velocities_strided", "fyzz_b200_remove_constraint",
     "fyzz_b200_set_pair_budget", "fyzz_b200_test_scan",
+    "fyzz_b200_set_body_contact_report_threshold", "fyzz_b200_force_threshold_changes",
 )
 STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 
@@ -84,6 +85,16 @@ EVENT_DTYPE = np.dtype([("body0", "<u4"), ("body1", "<u4"), ("shape0", "<u4"), (
 EVENT_POINT_DTYPE = np.dtype([("position", "<f4", 3), ("normal", "<f4", 3), ("separation", "<f4"),
                               ("reserved", "<u4"), ("normal_impulse", "<f8")])
 FOUND, PERSISTS, LOST = 0, 1, 2
+
+
+class ForceThresholdReport(C.Structure):
+    _fields_ = [("actor0", C.c_uint32), ("actor1", C.c_uint32), ("static_world", C.c_uint32),
+                ("change", C.c_uint32), ("normal_impulse", C.c_double), ("threshold", C.c_float),
+                ("reserved", C.c_uint32)]
+
+
+THRESHOLD_DTYPE = np.dtype([("actor0", "<u4"), ("actor1", "<u4"), ("static_world", "<u4"), ("change", "<u4"),
+                            ("normal_impulse", "<f8"), ("threshold", "<f4"), ("reserved", "<u4")])
 
 
 class DeviceView(C.Structure):
@@ -162,6 +173,8 @@ def lib():
         L.fyzz_b200_rollout_rewind.argtypes = [vp]
         L.fyzz_b200_fit_pair_budget.argtypes = [vp, f32, P(u32)]
         L.fyzz_b200_set_pair_budget.argtypes = [vp, u32, P(u32)]
+        L.fyzz_b200_set_body_contact_report_threshold.argtypes = [vp, u32, f32]
+        L.fyzz_b200_force_threshold_changes.argtypes = [vp, P(P(ForceThresholdReport)), P(u64)]
         L.fyzz_b200_test_scan.argtypes = [vp, u32, i32, P(u32), P(u64)]
         L.fyzz_b200_rollout_forward.argtypes = [vp, f32]
         L.fyzz_b200_rollout_backward.argtypes = [vp] + [vp] * 9
@@ -489,6 +502,23 @@ class World:
         if npt.value:
             C.memmove(points.ctypes.data, pt, npt.value * EVENT_POINT_DTYPE.itemsize)
         return events, points
+
+    # ---- force-threshold stream ----
+    def set_body_contact_report_threshold(self, body: int, force: float):
+        """World::set_body_contact_report_threshold (FLT_MAX disables)."""
+        self._check(lib().fyzz_b200_set_body_contact_report_threshold(self.h, body, force))
+
+    def force_threshold_changes(self) -> np.ndarray:
+        """The last step's force-threshold changes (structured array:
+        actor0, actor1, static_world, change 0 Found / 1 Persists / 2 Lost,
+        normal_impulse, threshold), in key order."""
+        ptr = C.POINTER(ForceThresholdReport)()
+        n = C.c_uint64()
+        self._check(lib().fyzz_b200_force_threshold_changes(self.h, C.byref(ptr), C.byref(n)))
+        if not n.value:
+            return np.zeros(0, THRESHOLD_DTYPE)
+        raw = C.string_at(ptr, n.value * THRESHOLD_DTYPE.itemsize)
+        return np.frombuffer(raw, THRESHOLD_DTYPE).copy()
 
     # ---- differentiable rollouts ----
     def fit_pair_budget(self, headroom: float = 1.5) -> int:

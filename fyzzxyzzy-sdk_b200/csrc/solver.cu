@@ -1951,6 +1951,7 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     hook(kStIntegrate, st);
     k_integrate<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
     if (s.n_kinematic) k_kinematic_publish<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
+    if (s.thresholds) enqueue_thresholds(s, st);
     if (s.events) enqueue_events(s, st);
     hook(kStEnd, st);
 }

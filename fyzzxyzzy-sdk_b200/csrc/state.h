@@ -26,6 +26,17 @@ struct ManagerSet {
     uint32_t* n = nullptr;         // device-side pair count of this generation
 };
 
+// Pairs whose accumulated normal impulse exceeded their report threshold in
+// one step (the force-threshold stream's generation): sorted by key
+// (actor0 << 33 | static world << 32 | actor1), with the aggregated impulse
+// and the pair's threshold.
+struct ThresholdSet {
+    uint64_t* key = nullptr;
+    double* impulse = nullptr;
+    float* thr = nullptr;
+    uint32_t* n = nullptr;
+};
+
 struct DevState {
     // static topology sizes (host-known)
     uint32_t n_scenes = 0, n_bodies = 0, n_shapes = 0, n_finite = 0, n_joints = 0;
@@ -186,6 +197,20 @@ struct DevState {
     uint32_t* ev_pt_off = nullptr;     // first event point per touching manager
     uint32_t* counters = nullptr;      // small device counters
     uint32_t* err = nullptr;           // error bits
+
+    // force-threshold stream (arrays exist once some body has a report
+    // threshold; World::set_body_contact_report_threshold)
+    bool thresholds = false;
+    float* b_thresh = nullptr;         // per body; FLT_MAX disables reporting
+    ThresholdSet th_cur, th_prev;      // this step's exceeded pairs / the previous step's
+    uint32_t *th_hi = nullptr, *th_lo = nullptr;   // per touching manager: key halves
+    double* th_sum = nullptr;          // per touching manager: summed normal impulse
+    float* th_thr = nullptr;           // per touching manager: pair threshold
+    uint32_t *th_k = nullptr, *th_v = nullptr, *th_k2 = nullptr, *th_v2 = nullptr;   // sort keys / rows
+    double* th_run_sum = nullptr;      // per sorted row (run heads): aggregated impulse
+    float* th_run_thr = nullptr;
+    uint32_t *th_f0 = nullptr, *th_p0 = nullptr, *th_f1 = nullptr, *th_p1 = nullptr;   // flags / scans
+    void* th_changes = nullptr;        // ForceThresholdRecord, 2 * pair_cap
 };
 
 // primitives.cu
@@ -257,6 +282,11 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook = 
                     const Branches* br = nullptr);
 // events.cu: the step's contact events into s.ev / s.ev_pts (after PGS).
 void enqueue_events(const DevState& s, cudaStream_t st);
+// thresholds.cu: the step's force-threshold changes into s.th_changes
+// (after PGS; s.th_cur becomes this step's exceeded set).
+void enqueue_thresholds(const DevState& s, cudaStream_t st);
+// Copies the live records of a threshold generation (n from the device).
+void enqueue_copy_threshold_set(const ThresholdSet& dst, const ThresholdSet& src, uint32_t cap, cudaStream_t st);
 // Per-device kernel attributes (shared-memory limits); call with the device
 // current before the first step or capture.
 // Wakes every dynamic body (as an authored velocity on each would).
@@ -282,7 +312,10 @@ enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels =
              kCntConvexGjk = 17 /* hull pairs regenerated through GJK/EPA */,
              kCntActivating = 18 /* nonzero when some body activates this step */,
              kCntConvexClip = 19 /* regenerated hull pairs whose faces are clipped */,
-             kCntConvexEpa = 20 /* regenerated hull pairs continuing in EPA */, kCntSlots = 21 };
+             kCntConvexEpa = 20 /* regenerated hull pairs continuing in EPA */,
+             kCntThRows = 21 /* managers with a reportable impulse */,
+             kCntThChanges = 22 /* force-threshold changes of the step */,
+             kCntThCommon = 23 /* pairs exceeding in this step and the previous one */, kCntSlots = 24 };
 
 // Contact event records in device memory; the layouts of
 // fyzz_b200_contact_event_t and fyzz_b200_contact_event_point_t.
@@ -298,5 +331,13 @@ struct EventPoint {
     double normal_impulse;
 };
 static_assert(sizeof(EventPoint) == 40, "EventPoint layout");
+// fyzz_b200_force_threshold_report_t.
+struct ForceThresholdRecord {
+    uint32_t actor0, actor1, static_world, change;
+    double normal_impulse;
+    float threshold;
+    uint32_t pad;
+};
+static_assert(sizeof(ForceThresholdRecord) == 32, "ForceThresholdRecord layout");
 
 }  // namespace fyzz::b200

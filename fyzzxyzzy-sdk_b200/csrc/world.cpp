@@ -50,6 +50,8 @@ struct HostBody {
     float wake = 0.4f;
     uint32_t sleep = 0;              // kSleeping | kReady
     std::array<float, 6> sacc{};     // accumulated linear, local angular motion
+    // ScBodyCore::contactReportThreshold (scene.h:1122): FLT_MAX disables
+    float report_threshold = FLT_MAX;
     // NpRigidDynamic wake on an authored velocity (scene.cpp:728-783): a
     // sleeping body starts with cleared sleep filters.
     void wake_up() {
@@ -481,6 +483,29 @@ public:
         b.wake_up();
         mass_dirty_ = true;
     }
+    // World::set_body_contact_report_threshold (src/world.cpp:355-359) then
+    // Scene::set_contact_report_threshold (scene.cpp:1148-1161).  The first
+    // finite threshold turns the world's force-threshold stream on (its
+    // device arrays are allocated and the step graphs rebuilt); it then
+    // stays on, so pairs that stop exceeding still report Lost.
+    void set_report_threshold(uint32_t body, float force) {
+        if (!std::isfinite(force) || force < 0.0f) throw std::invalid_argument("Invalid source contact report threshold");
+        HostBody& b = require_body(body);
+        if (!b.dynamic && !b.kinematic) throw std::logic_error("Source contact report threshold requires PxRigidDynamic");
+        pull_state();
+        b.report_threshold = force;
+        mass_dirty_ = true;
+        if (force != FLT_MAX && !thresholds_) {
+            thresholds_ = true;
+            if (uploaded_) {
+                check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+                alloc_threshold_arrays();
+                d_.thresholds = true;
+                for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+                release_segment_graphs();
+            }
+        }
+    }
     uint64_t add_distance(uint32_t a, uint32_t b, float len) {
         const float zero7[7] = {0, 0, 0, 0, 0, 0, 1};
         return add_joint(kJointCenter, a, b, zero7, zero7, len);
@@ -621,6 +646,7 @@ public:
             if (!err) {
                 steps_done_ += steps;
                 ev_device_valid_ = true;
+                th_device_valid_ = true;
                 return;
             }
             restore();
@@ -629,9 +655,11 @@ public:
                 continue;
             }
             ev_device_valid_ = false;
+            th_device_valid_ = false;
             raise_step_error(err);
         }
         ev_device_valid_ = false;
+        th_device_valid_ = false;
         throw std::overflow_error("Pair capacity could not be satisfied");
     }
 
@@ -677,10 +705,22 @@ public:
             dalloc(keep[k].n, 1, tmp);
             enqueue_copy_set(keep[k], sets_[k], live[k], stream_);
         }
+        ThresholdSet keep_th[2];
+        uint32_t live_th[2] = {0, 0};
+        if (d_.thresholds)
+            for (int k = 0; k < 2; ++k) {
+                check_cuda(cudaMemcpy(&live_th[k], th_sets_[k].n, 4, cudaMemcpyDeviceToHost), "read");
+                const size_t c = std::max(live_th[k], 1u);
+                dalloc(keep_th[k].key, c, tmp); dalloc(keep_th[k].impulse, c, tmp);
+                dalloc(keep_th[k].thr, c, tmp); dalloc(keep_th[k].n, 1, tmp);
+                enqueue_copy_threshold_set(keep_th[k], th_sets_[k], live_th[k], stream_);
+            }
         check_cuda(cudaStreamSynchronize(stream_), "sync");
         const int parity = parity_, last = last_cur_;
         alloc_pairs(cap);
         for (int k = 0; k < 2; ++k) enqueue_copy_set(sets_[k], keep[k], live[k], stream_);
+        if (d_.thresholds)
+            for (int k = 0; k < 2; ++k) enqueue_copy_threshold_set(th_sets_[k], keep_th[k], live_th[k], stream_);
         check_cuda(cudaStreamSynchronize(stream_), "sync");
         for (void* p : tmp) cudaFree(p);
         parity_ = parity;
@@ -1149,6 +1189,24 @@ public:
         *pts = have ? h_ev_pts_.data() : nullptr;
         *npts = have ? h_ev_pts_.size() : 0;
     }
+    // World::force_threshold_changes (world.h:472): the last completed
+    // step's changes, copied from the device on the first request after it,
+    // valid until the next step.  Empty after a collision pass.
+    void threshold_changes(const ForceThresholdRecord** out, uint64_t* n) {
+        if (thresholds_ && uploaded_ && steps_done_ && th_device_valid_ && th_fetched_ != steps_done_) {
+            check_cuda(cudaStreamSynchronize(stream_), "sync");
+            uint32_t cnt = 0;
+            check_cuda(cudaMemcpy(&cnt, d_.counters + kCntThChanges, 4, cudaMemcpyDeviceToHost), "read");
+            h_th_.resize(cnt);
+            if (cnt)
+                check_cuda(cudaMemcpy(h_th_.data(), d_.th_changes, size_t(cnt) * sizeof(ForceThresholdRecord),
+                                      cudaMemcpyDeviceToHost), "read");
+            th_fetched_ = steps_done_;
+        }
+        const bool have = thresholds_ && th_device_valid_ && th_fetched_ == steps_done_ && steps_done_;
+        *out = have ? h_th_.data() : nullptr;
+        *n = have ? h_th_.size() : 0;
+    }
     void collide() {
         check_cuda(cudaSetDevice(device_), "cudaSetDevice");
         ensure_device();
@@ -1161,8 +1219,13 @@ public:
             check_cuda(cudaGetLastError(), "collide launch");
             const uint32_t err = read_err();
             if (!err) {
+                // a collision pass solves nothing: the last step's exceeded
+                // force pairs stay the previous generation of the next step
+                if (d_.thresholds) enqueue_copy_threshold_set(th_sets_[parity_], th_sets_[last_cur_], d_.pair_cap, stream_);
+                check_cuda(cudaStreamSynchronize(stream_), "collide sync");
                 last_cur_ = parity_;
                 parity_ ^= 1;
+                th_device_valid_ = false;
                 return;
             }
             restore();
@@ -1207,9 +1270,11 @@ public:
         for (int i = 0; i <= kStEnd; ++i) cudaEventDestroy(ctx.ev[i]);
         if (err) {
             restore();
+            th_device_valid_ = false;
             raise_step_error(err);
         }
         ++steps_done_;
+        th_device_valid_ = true;
     }
     uint32_t kernels_per_step() const { return kernels_per_step_; }
 
@@ -1415,6 +1480,8 @@ private:
         DevState s = d_;
         s.cur = sets_[parity];
         s.prev = sets_[parity ^ 1];
+        s.th_cur = th_sets_[parity];
+        s.th_prev = th_sets_[parity ^ 1];
         return s;
     }
     uint32_t read_err() {
@@ -1482,6 +1549,7 @@ private:
                 dalloc(bk_set_.n, 1, pair_owned_);
             }
             enqueue_copy_set(bk_set_, sets_[last_cur_], d_.pair_cap, stream_);
+            if (d_.thresholds) enqueue_copy_threshold_set(bk_th_, th_sets_[last_cur_], d_.pair_cap, stream_);
         }
         check_cuda(cudaMemcpyAsync(bk_p_, d_.b_p, n, cudaMemcpyDeviceToDevice, stream_), "snapshot");
         check_cuda(cudaMemcpyAsync(bk_q_, d_.b_q, n, cudaMemcpyDeviceToDevice, stream_), "snapshot");
@@ -1506,7 +1574,10 @@ private:
                    "restore");
         // the generation the batch started from, as the reference's journal
         // restores its contact managers
-        if (snap_multi_) enqueue_copy_set(sets_[snap_last_], bk_set_, d_.pair_cap, stream_);
+        if (snap_multi_) {
+            enqueue_copy_set(sets_[snap_last_], bk_set_, d_.pair_cap, stream_);
+            if (d_.thresholds) enqueue_copy_threshold_set(th_sets_[snap_last_], bk_th_, d_.pair_cap, stream_);
+        }
         check_cuda(cudaMemsetAsync(d_.err, 0, 4, stream_), "restore");
         check_cuda(cudaStreamSynchronize(stream_), "restore sync");
         parity_ = snap_parity_;
@@ -1536,6 +1607,8 @@ private:
         for (void* p : pair_owned_) cudaFree(p);
         pair_owned_.clear();
         bk_set_ = ManagerSet{};
+        bk_th_ = ThresholdSet{};
+        th_sets_[0] = th_sets_[1] = ThresholdSet{};
         for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
         release_segment_graphs();
         d_.pair_cap = cap;
@@ -1593,6 +1666,29 @@ private:
         d_.sort_hist_words = radix_hist_words(big);
         dalloc(d_.sort_hist, d_.sort_hist_words, pair_owned_);
         if (notify_) alloc_events();
+        if (d_.thresholds) alloc_threshold_arrays();
+    }
+    // The force-threshold stream's generations (both start empty), the
+    // batch backup of one, and its per-manager scratch, for the current pair
+    // budget.
+    void alloc_threshold_arrays() {
+        const size_t cap = d_.pair_cap;
+        for (auto& t : th_sets_) {
+            dalloc(t.key, cap, pair_owned_); dalloc(t.impulse, cap, pair_owned_);
+            dalloc(t.thr, cap, pair_owned_); dalloc(t.n, 1, pair_owned_);
+            check_cuda(cudaMemsetAsync(t.n, 0, 4, stream_), "memset");
+        }
+        dalloc(bk_th_.key, cap, pair_owned_); dalloc(bk_th_.impulse, cap, pair_owned_);
+        dalloc(bk_th_.thr, cap, pair_owned_); dalloc(bk_th_.n, 1, pair_owned_);
+        dalloc(d_.th_hi, cap, pair_owned_); dalloc(d_.th_lo, cap, pair_owned_);
+        dalloc(d_.th_sum, cap, pair_owned_); dalloc(d_.th_thr, cap, pair_owned_);
+        dalloc(d_.th_k, cap, pair_owned_); dalloc(d_.th_v, cap, pair_owned_);
+        dalloc(d_.th_k2, cap, pair_owned_); dalloc(d_.th_v2, cap, pair_owned_);
+        dalloc(d_.th_run_sum, cap, pair_owned_); dalloc(d_.th_run_thr, cap, pair_owned_);
+        dalloc(d_.th_f0, cap, pair_owned_); dalloc(d_.th_p0, cap, pair_owned_);
+        dalloc(d_.th_f1, cap, pair_owned_); dalloc(d_.th_p1, cap, pair_owned_);
+        dalloc(reinterpret_cast<ForceThresholdRecord*&>(d_.th_changes), 2 * cap, pair_owned_);
+        check_cuda(cudaStreamSynchronize(stream_), "threshold arrays");
     }
     void alloc_events() {
         const size_t cap = d_.pair_cap;
@@ -1645,6 +1741,9 @@ private:
         upload(d_.b_ml_p, mlp, stream_); upload(d_.b_ml_q, mlq, stream_);
         upload(d_.b_wake, wake, stream_); upload(d_.b_sleep, sl, stream_); upload(d_.b_sacc, acc, stream_);
         upload(d_.b_ktarget, kt, stream_);
+        std::vector<float> thr(nb);
+        for (uint32_t i = 0; i < nb; ++i) thr[i] = bodies_[i].report_threshold;
+        upload(d_.b_thresh, thr, stream_);
         std::vector<float4> mat(shapes_.size());
         for (size_t i = 0; i < shapes_.size(); ++i)
             mat[i] = make_float4(shapes_[i].mat[0], shapes_[i].mat[1], shapes_[i].mat[2], shapes_[i].mat[3]);
@@ -1797,6 +1896,7 @@ private:
         d.n_small = uint32_t(small.size());
         d.events = notify_;
         d.sleep = sleep_enabled_;
+        d.thresholds = thresholds_;
         d_ = d;
         // allocations
         dalloc(d_.sc_fbegin, nsc + 1, owned_); dalloc(d_.sc_plane, nsc, owned_);
@@ -1812,6 +1912,7 @@ private:
         dalloc(bk_p_, nb, owned_); dalloc(bk_q_, nb, owned_); dalloc(bk_v_, nb, owned_); dalloc(bk_w_, nb, owned_);
         dalloc(bk_wake_, nb, owned_); dalloc(bk_sleep_, nb, owned_); dalloc(bk_sacc_, 2 * size_t(nb), owned_);
         dalloc(bk_counters_, kCntSlots, owned_);
+        dalloc(d_.b_thresh, nb, owned_);
         dalloc(d_.s_body, ns, owned_); dalloc(d_.s_type, ns, owned_); dalloc(d_.s_scene, ns, owned_);
         dalloc(d_.s_geom, ns, owned_); dalloc(d_.s_lp, ns, owned_); dalloc(d_.s_lq, ns, owned_);
         dalloc(d_.s_mat, ns, owned_); dalloc(d_.s_wp, ns, owned_); dalloc(d_.s_wq, ns, owned_);
@@ -1929,6 +2030,12 @@ private:
     uint32_t* bk_sleep_ = nullptr;
     uint32_t* bk_counters_ = nullptr;
     ManagerSet bk_set_;          // a batch's starting generation (allocated on the first batch)
+    ThresholdSet th_sets_[2];    // force-threshold generations, paired with sets_
+    ThresholdSet bk_th_;         // a batch's starting threshold generation
+    bool thresholds_ = false;    // some body has had a report threshold
+    bool th_device_valid_ = false;
+    uint64_t th_fetched_ = ~0ull;
+    std::vector<ForceThresholdRecord> h_th_;
     bool snap_multi_ = false;
     bool sleep_enabled_ = true;
     cudaGraphExec_t graphs_[4] = {nullptr, nullptr, nullptr, nullptr};   // [parity + 2 * sleeping]
@@ -2316,6 +2423,20 @@ int fyzz_b200_fit_pair_budget(fyzz_b200_world* w, float headroom, uint32_t* budg
     return guarded(w, [&](auto& W) {
         W.fit_pair_budget(headroom);
         if (budget_out) *budget_out = W.pair_budget();
+    });
+}
+int fyzz_b200_set_body_contact_report_threshold(fyzz_b200_world* w, uint32_t body, float force) {
+    return guarded(w, [&](auto& W) { W.set_report_threshold(body, force); });
+}
+int fyzz_b200_force_threshold_changes(fyzz_b200_world* w, const fyzz_b200_force_threshold_report_t** reports,
+                                      uint64_t* n) {
+    static_assert(sizeof(fyzz_b200_force_threshold_report_t) == sizeof(fyzz::b200::ForceThresholdRecord),
+                  "record layout");
+    if (!reports || !n) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) {
+        const fyzz::b200::ForceThresholdRecord* r = nullptr;
+        W.threshold_changes(&r, n);
+        *reports = reinterpret_cast<const fyzz_b200_force_threshold_report_t*>(r);
     });
 }
 int fyzz_b200_set_pair_budget(fyzz_b200_world* w, uint32_t pairs, uint32_t* budget_out) {

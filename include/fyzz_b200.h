@@ -253,6 +253,36 @@ int fyzz_b200_contact_events(fyzz_b200_world* w, const fyzz_b200_contact_event_t
                              uint64_t* n_events, const fyzz_b200_contact_event_point_t** points,
                              uint64_t* n_points);
 
+/* ---- force-threshold stream: World::set_body_contact_report_threshold /
+ *      World::force_threshold_changes (world.h:150-173, 472, 493;
+ *      Scene::update_threshold_stream, scene.cpp:9391-9508) ----
+ * Body pairs whose summed final normal impulse in a step is strictly above
+ * threshold * dt.  A pair against the static world is keyed (dynamic body,
+ * world) with that body's threshold; any other pair (actor0 < actor1, a
+ * kinematic body keeping its own id) with the smaller of the two
+ * thresholds.  Only managers the step solved count (a dynamic body awake).
+ * Changes against the previous step, in key order: Found (this step's
+ * impulse and threshold), Persists (the previous step's impulse and
+ * threshold, as the reference reports them), Lost (zero impulse, the
+ * previous threshold). */
+typedef struct {
+    uint32_t actor0, actor1;   /* ForceThresholdKey; actor1 is 0 against the world */
+    uint32_t static_world;     /* 1: actor1 is the static world */
+    uint32_t change;           /* ForceThresholdChange: 0 Found, 1 Persists, 2 Lost */
+    double normal_impulse;
+    float threshold;
+    uint32_t reserved;
+} fyzz_b200_force_threshold_report_t;
+/* World::set_body_contact_report_threshold (world.h:493): force >= 0 and
+ * finite (FLT_MAX, the default, disables); dynamic or kinematic bodies only
+ * (FYZZ_B200_LOGIC_ERROR otherwise). */
+int fyzz_b200_set_body_contact_report_threshold(fyzz_b200_world* w, uint32_t body, float force);
+/* World::force_threshold_changes (world.h:472): the last completed step's
+ * changes; the array is owned by the world and valid until the next step
+ * (empty after fyzz_b200_collide or a failed step). */
+int fyzz_b200_force_threshold_changes(fyzz_b200_world* w, const fyzz_b200_force_threshold_report_t** reports,
+                                      uint64_t* n);
+
 /* ---- kinematic bodies: World::set_body_kinematic / set_body_kinematic_target
  *      (world.h:505-506; Scene::set_kinematic, set_kinematic_target,
  *      scene.cpp:858-1003) ----

@@ -449,6 +449,30 @@ uint64_t fz_ref_contact_event_points(void* p, float* pts, double* impulse) {
     return e.size();
 }
 
+// Scene::set_contact_report_threshold (scene.cpp:1148-1161) on an actor
+// (BodyId: the floor, when present, is 0).
+int fz_ref_set_contact_report_threshold(void* p, uint32_t actor, float force) {
+    return guarded([&] { static_cast<Handle*>(p)->scene->set_contact_report_threshold(actor, force); });
+}
+
+// Scene::force_threshold_changes (scene.h:853): per report actor0, actor1,
+// static_world, change (ForceThresholdChange) as u32, the impulse and the
+// threshold.
+uint64_t fz_ref_force_threshold_changes(void* p, uint32_t* rows, double* impulse, float* threshold) {
+    const Scene& s = *static_cast<Handle*>(p)->scene;
+    const auto t = s.force_threshold_changes();
+    if (rows)
+        for (std::size_t i = 0; i < t.size(); ++i) {
+            rows[4 * i] = t[i].key.actor0;
+            rows[4 * i + 1] = t[i].key.actor1;
+            rows[4 * i + 2] = t[i].key.static_world ? 1u : 0u;
+            rows[4 * i + 3] = static_cast<uint32_t>(t[i].change);
+            impulse[i] = t[i].normal_impulse;
+            threshold[i] = t[i].threshold;
+        }
+    return t.size();
+}
+
 // ---- stateless Gu generators (public free functions of the reference) ----
 // ---- cooked convex meshes (include/fyzzxyzzy/convex.h, cooked_convex.cpp) ----
 // Cooks through fyzz::cook_convex_mesh.  Outputs, sized by the caller for

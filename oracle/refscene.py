@@ -72,6 +72,9 @@ def lib():
         L.fz_ref_pcm_sphere_sphere.argtypes = [vp, f32, vp, f32, f32, vp]
         L.fz_ref_pcm_sphere_box.argtypes = [vp, f32, vp, f32, vp]
         L.fz_ref_step_many.argtypes = [P(vp), u32, f32, i32, i32]
+        L.fz_ref_set_contact_report_threshold.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
+        L.fz_ref_force_threshold_changes.restype = C.c_uint64
+        L.fz_ref_force_threshold_changes.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -228,6 +231,20 @@ class RefScene:
         out = np.zeros(n, np.float64)
         lib().fz_ref_normal_impulses(self.h, _p(out))
         return out
+
+    def set_contact_report_threshold(self, actor: int, force: float):
+        """Scene::set_contact_report_threshold on BodyId `actor`."""
+        self._check(lib().fz_ref_set_contact_report_threshold(self.h, int(actor), float(force)))
+
+    def force_threshold_changes(self):
+        """(rows (n, 4) u32: actor0, actor1, static_world, change; impulse
+        (n,) f64; threshold (n,) f32) of the last step."""
+        n = lib().fz_ref_force_threshold_changes(self.h, None, None, None)
+        rows = np.zeros((n, 4), np.uint32)
+        imp = np.zeros(n, np.float64)
+        thr = np.zeros(n, np.float32)
+        lib().fz_ref_force_threshold_changes(self.h, _p(rows), _p(imp), _p(thr))
+        return rows, imp, thr
 
     def contact_events(self):
         """Events as (n, 7) u32: body0, body1, kind, count, point offset,
