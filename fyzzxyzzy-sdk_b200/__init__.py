@@ -46,6 +46,7 @@ EXPORTS = (
     "fyzz_b200_write_velocities_strided", "fyzz_b200_remove_constraint",
     "fyzz_b200_set_pair_budget", "fyzz_b200_test_scan",
     "fyzz_b200_set_body_contact_report_threshold", "fyzz_b200_force_threshold_changes",
+    "fyzz_b200_read_islands",
 )
 STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 
@@ -160,6 +161,8 @@ def lib():
         L.fyzz_b200_read_sorted_min_x.argtypes = [vp, u32, vp, vp, u64]
         L.fyzz_b200_read_sorted_min_x.restype = u64
         L.fyzz_b200_read_levels.argtypes = [vp, vp, u64]
+        L.fyzz_b200_read_islands.argtypes = [vp, vp, vp, u64]
+        L.fyzz_b200_read_islands.restype = u64
         L.fyzz_b200_read_levels.restype = u64
         L.fyzz_b200_profile_step.argtypes = [vp, f32, vp, u32]
         L.fyzz_b200_kernels_per_step.argtypes = [vp, P(u32)]
@@ -459,6 +462,14 @@ class World:
         out = np.zeros(n, np.uint32)
         lib().fyzz_b200_read_levels(self.h, _p(out), n)
         return out
+
+    def islands(self):
+        """Awake islands of the last step: (descriptors, levels) per island."""
+        n = lib().fyzz_b200_read_islands(self.h, None, None, 0)
+        d = np.zeros(n, np.uint32)
+        lv = np.zeros(n, np.uint32)
+        lib().fyzz_b200_read_islands(self.h, _p(d), _p(lv), n)
+        return d, lv
 
     def set_body_kinematic(self, body: int, enabled: bool = True):
         """World::set_body_kinematic (reference world.h:505)."""

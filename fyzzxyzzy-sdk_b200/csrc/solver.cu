@@ -1312,6 +1312,20 @@ struct LocalDeltas {
 };
 __device__ __forceinline__ int32_t unpack_local(uint32_t v) { return v == 0xffffu ? -1 : int32_t(v); }
 
+// 32 bytes per thread in one load (sm_100's 256-bit global loads): a solver
+// row is two loads instead of four 128-bit ones.  Scattered rows (one
+// manager per thread) cost one L1 wavefront per thread and load instruction,
+// so halving the instructions halves the L1 work of the row loads, which is
+// what bounds the CTA solvers.  The rows are written by this kernel in an
+// earlier pass, so the load is ordered against memory (no caching across
+// the asm).
+__device__ __forceinline__ void ldg256(const void* p, float4& a, float4& b) {
+    asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+                 : "l"(p)
+                 : "memory");
+}
+
 // One descriptor's rows for pass `it` (scene.cpp:8853-9148).  lid carries
 // the island-local bodies when D addresses shared memory.
 // kEagerFriction issues the friction-row loads together with the normal
@@ -1359,7 +1373,14 @@ __device__ void solve_desc(const DevState& s, uint32_t d, uint32_t lid, int it, 
     // NormalRow float4s: {n.xyz, ra.x} {ra.yz, rb.xy} {rb.z, vel_mult,
     // imp_mult, biased} {unbiased, applied, max_impulse, -}; FrictionRow:
     // {t.xyz, ra.x} {ra.yz, rb.xy} {rb.z, vel_mult, bias, target} {applied}.
-    const ManagerHeader hd = s.mh[m];
+    ManagerHeader hd;
+    {
+        float4 h0, h1;
+        ldg256(s.mh + m, h0, h1);
+        hd.b0 = __float_as_int(h0.x); hd.b1 = __float_as_int(h0.y);
+        hd.count = __float_as_uint(h0.z); hd.anchors = __float_as_uint(h0.w);
+        hd.sf = h1.x; hd.df = h1.y; hd.ima = h1.z; hd.imb = h1.w;
+    }
     const float ima = hd.ima, imb = hd.imb;   // 0 for the static world
     const bool friction = (it >= pos || pos - it <= 3) && hd.anchors;
     const float4* nr = reinterpret_cast<const float4*>(s.nrow + 4 * size_t(m));
@@ -1373,17 +1394,21 @@ __device__ void solve_desc(const DevState& s, uint32_t d, uint32_t lid, int it, 
         const bool friction_pass = it >= pos || pos - it <= 3;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            n0[j] = nr[4 * j]; n1[j] = nr[4 * j + 1]; n2[j] = nr[4 * j + 2]; n3[j] = nr[4 * j + 3];
+            ldg256(nr + 4 * j, n0[j], n1[j]);
+            ldg256(nr + 4 * j + 2, n2[j], n3[j]);
             if (friction_pass) {
-                f0[j] = fq[4 * j]; f1[j] = fq[4 * j + 1]; f2[j] = fq[4 * j + 2];
-                fa[j] = reinterpret_cast<const float*>(fq + 4 * j + 3)[0];
+                float4 f3;
+                ldg256(fq + 4 * j, f0[j], f1[j]);
+                ldg256(fq + 4 * j + 2, f2[j], f3);
+                fa[j] = f3.x;
             }
         }
     } else {
 #pragma unroll
         for (int j = 0; j < 4; ++j)
             if (uint32_t(j) < hd.count) {
-                n0[j] = nr[4 * j]; n1[j] = nr[4 * j + 1]; n2[j] = nr[4 * j + 2]; n3[j] = nr[4 * j + 3];
+                ldg256(nr + 4 * j, n0[j], n1[j]);
+                ldg256(nr + 4 * j + 2, n2[j], n3[j]);
             }
     }
     int32_t h0, h1;
@@ -1425,8 +1450,10 @@ __device__ void solve_desc(const DevState& s, uint32_t d, uint32_t lid, int it, 
 #pragma unroll
             for (int j = 0; j < 4; ++j)
                 if (uint32_t(j) < 2 * hd.anchors) {
-                    f0[j] = fq[4 * j]; f1[j] = fq[4 * j + 1]; f2[j] = fq[4 * j + 2];
-                    fa[j] = reinterpret_cast<const float*>(fq + 4 * j + 3)[0];
+                    float4 f3;
+                    ldg256(fq + 4 * j, f0[j], f1[j]);
+                    ldg256(fq + 4 * j + 2, f2[j], f3);
+                    fa[j] = f3.x;
                 }
         }
         const float coeff = hd.anchors == 2 ? 0.5f : 1.0f;
@@ -1581,6 +1608,11 @@ template <uint32_t MAXN> struct PgsSmem {
     static constexpr size_t kBytes = 2 * size_t(MAXN + 1) * sizeof(float4) + 2 * size_t(MAXN) * 4 +
                                      size_t(kMaxLevels + 1) * 4;
 };
+// Threads of the CTA that solves an island of (kMidIsland, kBigIsland]
+// descriptors: 12 warps, the most the register budget of the solver (about
+// 160 registers a thread) allows on one SM; a level of such an island holds
+// a few hundred descriptors, so more threads mean fewer rounds per level.
+constexpr uint32_t kBigPgsThreads = 384;
 template <uint32_t MAXN, uint32_t NT>
 __global__ void __launch_bounds__(NT) k_pgs_block_smem(DevState s, const uint32_t* lvl_bound, int list_class) {
     extern __shared__ float4 shb[];
@@ -1876,7 +1908,7 @@ void init_solver_kernels() {
     if (cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess) g_high_priority = greatest;
     cudaFuncSetAttribute(k_partition_smem<kBigIsland>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          int(PartSmem<kBigIsland>::kBytes));
-    cudaFuncSetAttribute(k_pgs_block_smem<kBigIsland, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_pgs_block_smem<kBigIsland, kBigPgsThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          int(PgsSmem<kBigIsland>::kBytes));
 }
 
@@ -1939,8 +1971,8 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     // PGS: islands by size class, independent
     hook(kStPgs, st);
     fork_branches(br, st, 3);
-    launch_high(k_pgs_block_smem<kBigIsland, 256>, grid_for(s.desc_cap, kMidIsland + 1, 148u), 256u,
-                PgsSmem<kBigIsland>::kBytes, side(1), s, lvl_bound, 2);
+    launch_high(k_pgs_block_smem<kBigIsland, kBigPgsThreads>, grid_for(s.desc_cap, kMidIsland + 1, 148u),
+                kBigPgsThreads, PgsSmem<kBigIsland>::kBytes, side(1), s, lvl_bound, 2);
     launch_high(k_pgs_block, grid_for(s.desc_cap, kBigIsland + 1, 148u), 256u, size_t(0), side(1), s, lvl_bound);
     k_pgs_warp<<<grid_for(s.desc_cap * 32u, kPgsWarpsPerBlock * 32u, 148u * 3u), kPgsWarpsPerBlock * 32u, 0, st>>>(
         s, lvl_bound);

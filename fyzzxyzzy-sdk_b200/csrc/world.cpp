@@ -1446,6 +1446,22 @@ public:
             check_cuda(cudaMemcpy(levels, d_.d_level, std::min<uint64_t>(c.desc, cap) * 4, cudaMemcpyDeviceToHost), "read");
         return c.desc;
     }
+    // Awake islands of the last step: descriptors and partition levels each.
+    uint64_t read_islands(uint32_t* descriptors, uint32_t* levels, uint64_t cap) {
+        if (!uploaded_) return 0;
+        const auto c = read_counters();
+        const uint64_t n = std::min<uint64_t>(c.isl, cap);
+        if ((descriptors || levels) && n) {
+            std::vector<uint32_t> b(n + 1), e(n);
+            check_cuda(cudaMemcpy(b.data(), d_.isl_begin, (n + 1) * 4, cudaMemcpyDeviceToHost), "read");
+            check_cuda(cudaMemcpy(e.data(), d_.isl_end, n * 4, cudaMemcpyDeviceToHost), "read");
+            for (uint64_t i = 0; i < n; ++i) {
+                if (descriptors) descriptors[i] = b[i + 1] - b[i];
+                if (levels) levels[i] = e[i];
+            }
+        }
+        return c.isl;
+    }
     void read_step_counters(uint32_t* out, uint32_t n) {
         if (n > uint32_t(kCntSlots)) throw std::invalid_argument("At most kCntSlots counters");
         if (!uploaded_) { for (uint32_t i = 0; i < n; ++i) out[i] = 0; return; }
@@ -2484,6 +2500,11 @@ int fyzz_b200_read_mass_frames(fyzz_b200_world* w, float* centers, float* orient
 int fyzz_b200_read_step_counters(fyzz_b200_world* w, uint32_t* out, uint32_t n) {
     if (!out) return FYZZ_B200_INVALID_ARGUMENT;
     return guarded(w, [&](auto& W) { W.read_step_counters(out, n); });
+}
+uint64_t fyzz_b200_read_islands(fyzz_b200_world* w, uint32_t* descriptors, uint32_t* levels, uint64_t cap) {
+    uint64_t n = 0;
+    guarded(w, [&](auto& W) { n = W.read_islands(descriptors, levels, cap); });
+    return n;
 }
 uint64_t fyzz_b200_read_levels(fyzz_b200_world* w, uint32_t* levels, uint64_t cap) {
     uint64_t n = 0;

@@ -399,6 +399,10 @@ uint64_t fyzz_b200_read_friction_anchors(fyzz_b200_world* w, uint32_t* anchors, 
 /* Partition level of every descriptor of the last step, in canonical
  * descriptor order (joints then touching managers). */
 uint64_t fyzz_b200_read_levels(fyzz_b200_world* w, uint32_t* levels, uint64_t cap);
+/* Awake islands of the last step (the solver's units of work): per island
+ * its descriptor count and partition level count.  Returns the island
+ * count; writes at most cap.  No reference counterpart. */
+uint64_t fyzz_b200_read_islands(fyzz_b200_world* w, uint32_t* descriptors, uint32_t* levels, uint64_t cap);
 /* Device counters of the last step, n <= 18: 0 touching managers,
  * 1 descriptors, 5 box pairs finished by GJK/EPA, 8-11 islands per size
  * class ((32,512], (96,512], (512,4096], >4096 descriptors), 16 pairs with
