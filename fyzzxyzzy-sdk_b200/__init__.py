@@ -46,7 +46,7 @@ EXPORTS = (
     "fyzz_b200_write_velocities_strided", "fyzz_b200_remove_constraint",
     "fyzz_b200_set_pair_budget", "fyzz_b200_test_scan",
     "fyzz_b200_set_body_contact_report_threshold", "fyzz_b200_force_threshold_changes",
-    "fyzz_b200_read_islands",
+    "fyzz_b200_read_islands", "fyzz_b200_set_caller_validated_transforms",
 )
 STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 

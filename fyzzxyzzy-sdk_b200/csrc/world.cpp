@@ -95,10 +95,12 @@ std::array<float, 4> normalize_once(std::array<float, 4> q) {
     const float len = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
     return {q[0] / len, q[1] / len, q[2] / len, q[3] / len};
 }
-// World::validated_transform then Scene::validated_pose.
-std::array<float, 4> validated_orientation(const float* q4) {
+// World::validated_transform then Scene::validated_pose (passes = 2), or
+// only the latter when fyzz::World already validated the transform (a
+// WorldBackend caller, passes = 1).
+std::array<float, 4> validated_orientation(const float* q4, int passes = 2) {
     std::array<float, 4> q{q4[0], q4[1], q4[2], q4[3]};
-    for (int pass = 0; pass < 2; ++pass) {
+    for (int pass = 0; pass < passes; ++pass) {
         const float len = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
         if (!std::isfinite(q[0]) || !std::isfinite(q[1]) || !std::isfinite(q[2]) || !std::isfinite(q[3]) ||
             !std::isfinite(len) || std::abs(len - 1.0f) >= 1.0e-2f)
@@ -244,6 +246,10 @@ public:
         return uint32_t(scene_body_begin_.size() - 1);
     }
     uint32_t current_scene() const { return uint32_t(scene_body_begin_.size() - 1); }
+    // Authoring transforms arrive validated and normalised by fyzz::World
+    // (src/world.cpp:38-55) when this world sits behind a WorldBackend; only
+    // the scene's own normalisation (Scene::validated_pose) is applied then.
+    void set_caller_validated(bool on) { norm_passes_ = on ? 1 : 2; }
     uint32_t add_static_floor(float height) {
         if (!std::isfinite(height)) throw std::invalid_argument("Native scene floor must be finite");
         if (scene_has_floor_.back()) throw std::logic_error("One static floor per scene is supported");
@@ -265,7 +271,7 @@ public:
     }
     uint32_t create_dynamic_body(const float* pose) {
         validate_position(pose);
-        const auto q = validated_orientation(pose + 3);
+        const auto q = validated_orientation(pose + 3, norm_passes_);
         pull_state();
         HostBody b;
         b.scene = current_scene();
@@ -291,7 +297,7 @@ public:
         if (!b.dynamic) throw std::logic_error("Shapes attach to dynamic bodies on this backend");
         if (b.scene != current_scene()) throw std::logic_error("Bodies of a closed scene cannot gain shapes");
         validate_position(local);
-        const auto lq = validated_orientation(local + 3);
+        const auto lq = validated_orientation(local + 3, norm_passes_);
         if (type == kBox) {
             if (!std::isfinite(half[0]) || !std::isfinite(half[1]) || !std::isfinite(half[2]) ||
                 half[0] <= 0.0f || half[1] <= 0.0f || half[2] <= 0.0f)
@@ -323,7 +329,7 @@ public:
         if (!b.dynamic) throw std::logic_error("Shapes attach to dynamic bodies on this backend");
         if (b.scene != current_scene()) throw std::logic_error("Bodies of a closed scene cannot gain shapes");
         validate_position(local);
-        const auto lq = validated_orientation(local + 3);
+        const auto lq = validated_orientation(local + 3, norm_passes_);
         if (b.shapes.size() >= 8) throw std::logic_error("At most 8 shapes per body are supported");
         uint32_t m = 0;
         while (m < meshes_.size() && meshes_[m] != mesh) ++m;
@@ -527,8 +533,8 @@ public:
             j.lb = {local_b[0], local_b[1], local_b[2]};
         }
         if (kind >= kJointFixed) {
-            j.qa = validated_orientation(local_a + 3);
-            j.qb = validated_orientation(local_b + 3);
+            j.qa = validated_orientation(local_a + 3, norm_passes_);
+            j.qb = validated_orientation(local_b + 3, norm_passes_);
         }
         if (!A.dynamic && !B.dynamic) throw std::logic_error("Rigid constraint requires a dynamic solver node");
         if (A.scene != B.scene) throw std::invalid_argument("Constraint endpoints must share a scene");
@@ -2031,6 +2037,7 @@ private:
     bool joints_dirty_ = false;
     static constexpr uint32_t kJointReserve = 256;
     uint32_t joint_cap_ = 0, jrow_cap_ = 0;   // joints / joint rows the device tables hold
+    int norm_passes_ = 2;                      // orientation normalisations of authored transforms
     std::vector<uint32_t> scene_body_begin_, scene_shape_begin_;
     std::vector<bool> scene_has_floor_;
     std::vector<uint32_t> h_fbegin_;
@@ -2454,6 +2461,9 @@ int fyzz_b200_force_threshold_changes(fyzz_b200_world* w, const fyzz_b200_force_
         W.threshold_changes(&r, n);
         *reports = reinterpret_cast<const fyzz_b200_force_threshold_report_t*>(r);
     });
+}
+int fyzz_b200_set_caller_validated_transforms(fyzz_b200_world* w, int enabled) {
+    return guarded(w, [&](auto& W) { W.set_caller_validated(enabled != 0); });
 }
 int fyzz_b200_set_pair_budget(fyzz_b200_world* w, uint32_t pairs, uint32_t* budget_out) {
     return guarded(w, [&](auto& W) {

@@ -72,7 +72,14 @@ const char* fyzz_b200_last_error(const fyzz_b200_world* w);
 /* Device error bits of the last step (source_dy_distance_native.h:1336-1345). */
 int fyzz_b200_error_bits(const fyzz_b200_world* w, uint32_t* bits);
 
-/* ---- authoring: WorldBackend (world.h:226-394) ---- */
+/* ---- authoring: WorldBackend (world.h:226-394) ----
+ * Transforms are validated and normalised as fyzz::World does before its
+ * backend (src/world.cpp:38-55) and once more as the scene does
+ * (Scene::validated_pose, src/native/compound.cpp:9-18). */
+/* For a caller that is itself fyzz::World (this world behind a
+ * WorldBackend): transforms arrive validated, so only the scene's
+ * normalisation is applied.  No reference counterpart. */
+int fyzz_b200_set_caller_validated_transforms(fyzz_b200_world* w, int enabled);
 /* New independent scene; later bodies belong to it.  (No reference
  * counterpart: the reference World holds exactly one scene.) */
 int fyzz_b200_begin_scene(fyzz_b200_world* w, uint32_t* scene_out);
