@@ -5,8 +5,8 @@ Headline workload: the plain at-scale scene -- 131,072 dynamic bodies (70%
 boxes, 20% spheres, 10% box+sphere compounds, 2% in distance-joined pairs)
 in a 200 x 50 x 200 m region above a floor; dt = 1/120 s, 4 position + 1
 velocity iteration -- taken from the state it reaches after its 600 steps in
-the reference's own run (tests/golden/plain_131k_step600.npz: a settled pile
-of ~270k contact managers, where the solver dominates).  W untimed warm-up
+its run (tests/golden/plain_131k_step600.npz: a settled pile of ~270k
+contact managers, where the solver dominates).  W untimed warm-up
 steps, then K timed steps.  The same line carries the run from the seeded
 start (600 steps), the batched forward (4,096 independent scenes, one launch
 per stage), the differentiable rollouts (1,024 x 64 boxes, 128 steps; and at
@@ -46,9 +46,9 @@ PLAIN_WORKLOAD = ("plain method at scale, one scene: 131,072 bodies (70% boxes, 
                   "10% box+sphere compounds, 2% distance-joined pairs), 200x50x200 m above a floor, "
                   "dt=1/120 s, 4 position + 1 velocity iterations")
 SETTLED_FIXTURE = os.path.join(ROOT, "tests", "golden", "plain_131k_step600.npz")
-SETTLED_START = ("settled: every body's pose and velocity after the workload's 600 steps in the reference "
-                 "NativeCpu run (tests/golden/plain_131k_step600.npz), all bodies awake, contact history "
-                 "rebuilt by the warm-up steps")
+SETTLED_START = ("settled: every body's pose and velocity after the workload's 600 steps from its seeded start "
+                 "(tests/golden/plain_131k_step600.npz, made by tests/golden/make_settled.py), all bodies awake, "
+                 "contact history rebuilt by the warm-up steps; both arms start from it")
 BATCHED_WORKLOAD = ("batched forward: 4,096 independent scenes, body count log-uniform in [16,512] "
                     "(random piles and 5-20 high unit-cube stacks), own floor each, one launch per stage, "
                     "step captured as a CUDA graph")
@@ -658,7 +658,7 @@ def run_b200(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: seeded generator with the workload's distributions (no dataset); settled "
-                    "start state from the reference's own run of the same workload",
+                    "start state committed as a fixture (the workload's own 600-step run)",
             "config": plain_config(spec, start, world),
             "gpu_launches": kernels * args.steps,
             "kernels_per_step": kernels,
@@ -757,7 +757,7 @@ def run_reference(args):
             "ms_per_step": el / max(n, 1) * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: seeded generator with the workload's distributions (no dataset); settled "
-                    "start state from the reference's own run of the same workload",
+                    "start state committed as a fixture (the workload's own 600-step run)",
             "config": plain_config(spec, start, world),
             "cpu_baseline": {"value": value, "unit": UNIT, "kind": "reference", "cores": 2, "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

@@ -47,6 +47,7 @@ EXPORTS = (
     "fyzz_b200_set_pair_budget", "fyzz_b200_test_scan",
     "fyzz_b200_set_body_contact_report_threshold", "fyzz_b200_force_threshold_changes",
     "fyzz_b200_read_islands", "fyzz_b200_set_caller_validated_transforms",
+    "fyzz_b200_set_descriptor_order",
 )
 STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 
@@ -176,6 +177,7 @@ def lib():
         L.fyzz_b200_rollout_rewind.argtypes = [vp]
         L.fyzz_b200_fit_pair_budget.argtypes = [vp, f32, P(u32)]
         L.fyzz_b200_set_pair_budget.argtypes = [vp, u32, P(u32)]
+        L.fyzz_b200_set_descriptor_order.argtypes = [vp, vp, u64, vp, u64]
         L.fyzz_b200_set_body_contact_report_threshold.argtypes = [vp, u32, f32]
         L.fyzz_b200_force_threshold_changes.argtypes = [vp, P(P(ForceThresholdReport)), P(u64)]
         L.fyzz_b200_test_scan.argtypes = [vp, u32, i32, P(u32), P(u64)]
@@ -537,6 +539,13 @@ class World:
         out = C.c_uint32()
         self._check(lib().fyzz_b200_fit_pair_budget(self.h, headroom, C.byref(out)))
         return out.value
+
+    def set_descriptor_order(self, pairs, joint_ids=None):
+        """Gauss-Seidel order of the next step: touching-manager shape pairs
+        (n, 2) in order, joint constraint ids in order."""
+        p = np.ascontiguousarray(np.asarray(pairs, np.uint32).reshape(-1, 2))
+        j = np.ascontiguousarray(np.zeros(0, np.uint64) if joint_ids is None else np.asarray(joint_ids, np.uint64))
+        self._check(lib().fyzz_b200_set_descriptor_order(self.h, _p(p), p.shape[0], _p(j), j.size))
 
     def set_pair_budget(self, pairs: int) -> int:
         """Sets the pair budget (at least the live pairs; history kept)."""

@@ -245,6 +245,40 @@ __global__ void k_desc_keys(DevState s) {
     }
 }
 
+// Replayed order (one step): descriptors are first sorted by their rank in
+// the given order -- joints by rp_jrank, then the listed touching managers
+// by their position in the list, then unlisted managers in pair order --
+// while d_level holds each descriptor's island key; the stable sort by
+// island key that follows keeps that order inside every island.
+__device__ __forceinline__ uint32_t replay_rank(const DevState& s, uint32_t d) {
+    if (d < s.n_joints) return s.rp_jrank[d];
+    const uint32_t m = d - s.n_joints;
+    const uint64_t key = s.cur.key[s.man_list[m]];
+    uint32_t lo = 0, hi = s.rp_n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s.rp_keys[mid] < key) lo = mid + 1; else hi = mid;
+    }
+    return s.n_joints + ((lo < s.rp_n && s.rp_keys[lo] == key) ? s.rp_pos[lo] : s.rp_n + m);
+}
+__global__ void k_replay_keys(DevState s) {
+    const uint32_t n = s.counters[kCntDesc];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += stride) {
+        s.d_level[d] = s.d_key[d];
+        s.d_key[d] = replay_rank(s, d);
+    }
+}
+__global__ void k_replay_rekey(DevState s) {
+    const uint32_t n = s.counters[kCntDesc];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+        const uint32_t d = s.d_val[p];
+        s.d_key[p] = s.d_level[d];
+        s.d_level[d] = kInvalid;
+    }
+}
+
 // ---------------- sleep ----------------
 // Reference behaviour (src/native/scene.cpp), per step:
 //   activate_published_islands 6148-6250: a newly found overlap pair of two
@@ -1944,6 +1978,14 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     if (s.n_kinematic) k_kinematic_velocities<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
     k_bodies_velocity<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
     k_desc_keys<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
+    if (s.replay) {
+        int rbits = 1;
+        while ((1ull << rbits) < uint64_t(s.n_joints) + 2ull * s.pair_cap + 1u) ++rbits;
+        k_replay_keys<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
+        radix_sort_pairs(s.d_key, s.d_val, s.d_key2, s.d_val2, s.desc_cap, s.counters + kCntDesc, 0,
+                         (rbits + 7) / 8 * 8, s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err);
+        k_replay_rekey<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
+    }
     // keys are island roots < n_bodies, or n_bodies for sleeping islands
     int bits = 1;
     while ((1ull << bits) < uint64_t(s.n_bodies) + 1u) ++bits;

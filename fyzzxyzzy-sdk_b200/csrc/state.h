@@ -211,6 +211,16 @@ struct DevState {
     float* th_run_thr = nullptr;
     uint32_t *th_f0 = nullptr, *th_p0 = nullptr, *th_f1 = nullptr, *th_p1 = nullptr;   // flags / scans
     void* th_changes = nullptr;        // ForceThresholdRecord, 2 * pair_cap
+
+    // Replayed descriptor order of one step (fyzz_b200_set_descriptor_order):
+    // the touching managers' pair keys, sorted, with their positions in the
+    // order, and each joint descriptor's rank.  Off (replay = false) in
+    // ordinary steps.
+    bool replay = false;
+    uint64_t* rp_keys = nullptr;
+    uint32_t* rp_pos = nullptr;
+    uint32_t rp_n = 0;
+    uint32_t* rp_jrank = nullptr;
 };
 
 // primitives.cu

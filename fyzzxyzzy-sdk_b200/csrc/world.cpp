@@ -733,6 +733,61 @@ public:
         last_cur_ = last;
     }
     uint32_t pair_budget() const { return d_.pair_cap; }
+    // The solver order of the next step, as the reference's Scene chose it
+    // (partition_constraints' input: joints in constraint order, then the
+    // touching managers in its island-edge order, scene.cpp:7153-7216):
+    // pairs (shape a < shape b) in order, joint constraint ids (matched by
+    // slot) in order.  Managers and joints the lists do not name follow in
+    // canonical order.  Applies to exactly one step.
+    void set_descriptor_order(const uint32_t* pairs, uint64_t n_pairs, const uint64_t* joint_ids, uint64_t n_joint_ids) {
+        check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+        ensure_device();
+        if (n_pairs > d_.pair_cap) throw std::invalid_argument("Descriptor order names more pairs than the pair budget");
+        std::vector<std::pair<uint64_t, uint32_t>> keyed(n_pairs);
+        for (uint64_t i = 0; i < n_pairs; ++i) {
+            const uint32_t a = pairs[2 * i], b = pairs[2 * i + 1];
+            if (a >= b || b >= shapes_.size()) throw std::invalid_argument("Descriptor order pair must be (a < b) shapes");
+            keyed[i] = {(uint64_t(a) << 32) | b, uint32_t(i)};
+        }
+        std::sort(keyed.begin(), keyed.end());
+        for (uint64_t i = 1; i < n_pairs; ++i)
+            if (keyed[i].first == keyed[i - 1].first) throw std::invalid_argument("Descriptor order names a pair twice");
+        std::vector<uint64_t> keys(n_pairs);
+        std::vector<uint32_t> pos(n_pairs);
+        for (uint64_t i = 0; i < n_pairs; ++i) { keys[i] = keyed[i].first; pos[i] = keyed[i].second; }
+        // joint descriptors are the live joints by scene, slot descending
+        std::vector<uint32_t> slots;
+        for (const auto& j : joints_) if (j.live) slots.push_back(j.slot);
+        std::stable_sort(slots.begin(), slots.end(), [&](uint32_t x, uint32_t y) {
+            return joints_[x].scene != joints_[y].scene ? joints_[x].scene < joints_[y].scene : x > y;
+        });
+        std::vector<uint32_t> jrank(slots.size(), ~0u);
+        uint32_t next = 0;
+        for (uint64_t i = 0; i < n_joint_ids; ++i) {
+            const uint32_t slot = uint32_t(joint_ids[i]);
+            for (size_t d = 0; d < slots.size(); ++d)
+                if (slots[d] == slot && jrank[d] == ~0u) jrank[d] = next++;
+        }
+        for (auto& r : jrank) if (r == ~0u) r = next++;
+        if (replay_cap_ < std::max<uint64_t>(n_pairs, 1) || replay_jcap_ < std::max<size_t>(jrank.size(), 1)) {
+            check_cuda(cudaStreamSynchronize(stream_), "sync");
+            for (void* p : {static_cast<void*>(d_.rp_keys), static_cast<void*>(d_.rp_pos), static_cast<void*>(d_.rp_jrank)})
+                if (p) {
+                    owned_.erase(std::find(owned_.begin(), owned_.end(), p));
+                    cudaFree(p);
+                }
+            replay_cap_ = std::max<uint64_t>(n_pairs, 1);
+            replay_jcap_ = std::max<size_t>(jrank.size(), 1);
+            dalloc(d_.rp_keys, replay_cap_, owned_); dalloc(d_.rp_pos, replay_cap_, owned_);
+            dalloc(d_.rp_jrank, replay_jcap_, owned_);
+        }
+        upload(d_.rp_keys, keys, stream_);
+        upload(d_.rp_pos, pos, stream_);
+        upload(d_.rp_jrank, jrank, stream_);
+        check_cuda(cudaStreamSynchronize(stream_), "replay upload");
+        d_.rp_n = uint32_t(n_pairs);
+        replay_pending_ = true;
+    }
     // Test hook of the step's exclusive scan (the look-back scan every
     // step runs, on this world's scan scratch): scans n ones into a
     // temporary buffer.  With skip_first_tile the scan's tile ticket starts
@@ -1521,6 +1576,20 @@ private:
         d_.dt = dt;
         check_cuda(cudaMemsetAsync(d_.err, 0, 4, stream_), "memset");
         for (uint32_t i = 0; i < steps; ++i) {
+            if (replay_pending_) {
+                // the replayed order is one step's input: launched eagerly,
+                // outside the cached step graphs
+                DevState s = view(parity_);
+                s.replay = true;
+                enqueue_broadphase(s, stream_);
+                enqueue_narrowphase(s, stream_);
+                enqueue_solver(s, stream_, {}, &br_);
+                check_cuda(cudaGetLastError(), "replay launch");
+                replay_pending_ = false;
+                last_cur_ = parity_;
+                parity_ ^= 1;
+                continue;
+            }
             cudaGraphExec_t& exec = graphs_[parity_ + (d_.sleep ? 2 : 0)];
             if (!exec) {
                 cudaGraph_t g;
@@ -1559,6 +1628,7 @@ private:
     // rollback therefore keeps every PCM cache, friction history and touch
     // count, and a retried batch runs exactly as a batch that never failed.
     void snapshot(uint32_t steps) {
+        snap_replay_ = replay_pending_;
         const size_t n = size_t(d_.n_bodies) * 16;
         check_cuda(cudaMemcpyAsync(bk_counters_, d_.counters, kCntSlots * 4, cudaMemcpyDeviceToDevice, stream_),
                    "snapshot");
@@ -1602,6 +1672,7 @@ private:
         }
         check_cuda(cudaMemsetAsync(d_.err, 0, 4, stream_), "restore");
         check_cuda(cudaStreamSynchronize(stream_), "restore sync");
+        replay_pending_ = snap_replay_;
         parity_ = snap_parity_;
         last_cur_ = snap_last_;
     }
@@ -1617,6 +1688,9 @@ private:
         d_.j_la = d_.j_lb = d_.j_qa = d_.j_qb = nullptr;
         d_.jrow = nullptr;
         joint_cap_ = jrow_cap_ = 0;
+        d_.rp_keys = nullptr; d_.rp_pos = nullptr; d_.rp_jrank = nullptr;
+        replay_cap_ = replay_jcap_ = 0;
+        replay_pending_ = false;
         d_pack_ = nullptr;
         d_vel6_ = nullptr;
         vel_stride_cap_ = 0;
@@ -2038,6 +2112,8 @@ private:
     static constexpr uint32_t kJointReserve = 256;
     uint32_t joint_cap_ = 0, jrow_cap_ = 0;   // joints / joint rows the device tables hold
     int norm_passes_ = 2;                      // orientation normalisations of authored transforms
+    bool replay_pending_ = false, snap_replay_ = false;   // a replayed descriptor order for the next step
+    uint64_t replay_cap_ = 0, replay_jcap_ = 0;
     std::vector<uint32_t> scene_body_begin_, scene_shape_begin_;
     std::vector<bool> scene_has_floor_;
     std::vector<uint32_t> h_fbegin_;
@@ -2464,6 +2540,11 @@ int fyzz_b200_force_threshold_changes(fyzz_b200_world* w, const fyzz_b200_force_
 }
 int fyzz_b200_set_caller_validated_transforms(fyzz_b200_world* w, int enabled) {
     return guarded(w, [&](auto& W) { W.set_caller_validated(enabled != 0); });
+}
+int fyzz_b200_set_descriptor_order(fyzz_b200_world* w, const uint32_t* pairs, uint64_t n_pairs,
+                                   const uint64_t* joint_ids, uint64_t n_joint_ids) {
+    if ((n_pairs && !pairs) || (n_joint_ids && !joint_ids)) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) { W.set_descriptor_order(pairs, n_pairs, joint_ids, n_joint_ids); });
 }
 int fyzz_b200_set_pair_budget(fyzz_b200_world* w, uint32_t pairs, uint32_t* budget_out) {
     return guarded(w, [&](auto& W) {

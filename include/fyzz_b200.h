@@ -371,6 +371,17 @@ int fyzz_b200_rollout_backward(fyzz_b200_world* w, const float* grad_center,
  * bodies (either may be NULL). */
 int fyzz_b200_read_mass_frames(fyzz_b200_world* w, float* centers, float* orientations);
 
+/* The Gauss-Seidel order of the next step only, in the reference Scene's
+ * terms: the input order of partition_constraints (scene.cpp:7153-7216) --
+ * joint constraint ids (matched by slot) in order, then the touching
+ * managers' shape pairs (a < b) in order; within each island the
+ * partition's greedy levels and the solve follow this order.  Managers and
+ * joints not named keep canonical order after the named ones.  The
+ * reference builds its order from the insertion history of its island
+ * graph; with this hook a caller that knows it (a replay of a reference
+ * run) reproduces the reference's sweep.  No reference counterpart. */
+int fyzz_b200_set_descriptor_order(fyzz_b200_world* w, const uint32_t* pairs, uint64_t n_pairs,
+                                   const uint64_t* joint_ids, uint64_t n_joint_ids);
 /* Test hook of the step's exclusive scan (no reference counterpart): scans
  * n ones with this world's scan scratch.  skip_first_tile starts the scan's
  * tile ticket at 1, so one block waits for a tile that never publishes; the

@@ -387,6 +387,18 @@ uint64_t fz_ref_manager_order(void* p, uint64_t* out) {
     if (out) for (std::size_t i = 0; i < v.size(); ++i) out[i] = v[i];
     return v.size();
 }
+// The same order as shape pairs (a < b, 2 u32 each).
+uint64_t fz_ref_manager_order_pairs(void* p, uint32_t* out) {
+    const Scene& s = *static_cast<Handle*>(p)->scene;
+    const auto& v = Fix::indexed_managers(s);
+    const auto& m = Fix::manifolds(s);
+    if (out)
+        for (std::size_t i = 0; i < v.size(); ++i) {
+            out[2 * i] = m[v[i]].pair.a;
+            out[2 * i + 1] = m[v[i]].pair.b;
+        }
+    return v.size();
+}
 uint64_t fz_ref_joint_order(void* p, uint64_t* out) {
     const Scene& s = *static_cast<Handle*>(p)->scene;
     const auto& v = Fix::indexed_joints(s);

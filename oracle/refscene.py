@@ -72,6 +72,8 @@ def lib():
         L.fz_ref_pcm_sphere_sphere.argtypes = [vp, f32, vp, f32, f32, vp]
         L.fz_ref_pcm_sphere_box.argtypes = [vp, f32, vp, f32, vp]
         L.fz_ref_step_many.argtypes = [P(vp), u32, f32, i32, i32]
+        L.fz_ref_manager_order_pairs.restype = C.c_uint64
+        L.fz_ref_manager_order_pairs.argtypes = [C.c_void_p, C.c_void_p]
         L.fz_ref_set_contact_report_threshold.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
         L.fz_ref_force_threshold_changes.restype = C.c_uint64
         L.fz_ref_force_threshold_changes.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -211,6 +213,13 @@ class RefScene:
         n = lib().fz_ref_manager_order(self.h, None)
         out = np.zeros(n, np.uint64)
         lib().fz_ref_manager_order(self.h, _p(out))
+        return out
+
+    def manager_order_pairs(self) -> np.ndarray:
+        """The last step's manager order as shape pairs (n, 2)."""
+        n = lib().fz_ref_manager_order_pairs(self.h, None)
+        out = np.zeros((n, 2), np.uint32)
+        lib().fz_ref_manager_order_pairs(self.h, _p(out))
         return out
 
     def joint_order(self) -> np.ndarray:
