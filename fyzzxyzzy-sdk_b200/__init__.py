@@ -47,7 +47,7 @@ EXPORTS = (
     "fyzz_b200_set_pair_budget", "fyzz_b200_test_scan",
     "fyzz_b200_set_body_contact_report_threshold", "fyzz_b200_force_threshold_changes",
     "fyzz_b200_read_islands", "fyzz_b200_set_caller_validated_transforms",
-    "fyzz_b200_set_descriptor_order",
+    "fyzz_b200_set_descriptor_order", "fyzz_b200_set_tuning", "fyzz_b200_get_tuning",
 )
 STAGES = ("bounds", "sort", "pairs", "narrowphase", "islands", "prep", "pgs", "integrate")
 
@@ -97,6 +97,14 @@ class ForceThresholdReport(C.Structure):
 
 THRESHOLD_DTYPE = np.dtype([("actor0", "<u4"), ("actor1", "<u4"), ("static_world", "<u4"), ("change", "<u4"),
                             ("normal_impulse", "<f8"), ("threshold", "<f4"), ("reserved", "<u4")])
+
+
+class Tuning(C.Structure):
+    _fields_ = [("island_thread", C.c_uint32), ("island_warp", C.c_uint32), ("island_cta", C.c_uint32),
+                ("radix_bits", C.c_uint32), ("elem_block", C.c_uint32), ("work_queue", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
 
 
 class DeviceView(C.Structure):
@@ -178,6 +186,8 @@ def lib():
         L.fyzz_b200_fit_pair_budget.argtypes = [vp, f32, P(u32)]
         L.fyzz_b200_set_pair_budget.argtypes = [vp, u32, P(u32)]
         L.fyzz_b200_set_descriptor_order.argtypes = [vp, vp, u64, vp, u64]
+        L.fyzz_b200_set_tuning.argtypes = [vp, P(Tuning)]
+        L.fyzz_b200_get_tuning.argtypes = [vp, P(Tuning)]
         L.fyzz_b200_set_body_contact_report_threshold.argtypes = [vp, u32, f32]
         L.fyzz_b200_force_threshold_changes.argtypes = [vp, P(P(ForceThresholdReport)), P(u64)]
         L.fyzz_b200_test_scan.argtypes = [vp, u32, i32, P(u32), P(u64)]
@@ -546,6 +556,19 @@ class World:
         p = np.ascontiguousarray(np.asarray(pairs, np.uint32).reshape(-1, 2))
         j = np.ascontiguousarray(np.zeros(0, np.uint64) if joint_ids is None else np.asarray(joint_ids, np.uint64))
         self._check(lib().fyzz_b200_set_descriptor_order(self.h, _p(p), p.shape[0], _p(j), j.size))
+
+    def set_tuning(self, **params):
+        """Performance parameters (fyzz_b200_tuning_t fields); unnamed ones
+        keep their current values.  Results are unchanged by any setting."""
+        t = self.tuning()
+        for k, v in params.items():
+            t[k] = int(v)
+        self._check(lib().fyzz_b200_set_tuning(self.h, C.byref(Tuning(**t))))
+
+    def tuning(self) -> dict:
+        t = Tuning()
+        self._check(lib().fyzz_b200_get_tuning(self.h, C.byref(t)))
+        return t.as_dict()
 
     def set_pair_budget(self, pairs: int) -> int:
         """Sets the pair budget (at least the live pairs; history kept)."""

@@ -490,7 +490,7 @@ __global__ void __launch_bounds__(kRevWarps * 32) k_adj_pgs_warp_smem(DevState s
     const RevLocal D{sh[wib]};
     for (uint32_t isl = warp; isl < ni; isl += nwarps) {
         const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
-        if (end - begin > kSmallIsland || end - begin <= kRevTiny) continue;
+        if (end - begin > s.isl_warp || end - begin <= kRevTiny) continue;
         const uint32_t nlev = s.isl_end[isl];
         const uint32_t nb = s.isl_nbod[isl];
         const int32_t* ib = s.isl_bod + begin + isl;
@@ -522,10 +522,11 @@ __global__ void __launch_bounds__(kRevWarps * 32) k_adj_pgs_warp_smem(DevState s
         __syncwarp();
     }
 }
-// The same with one CTA per island of (kSmallIsland, kMidIsland] descriptors.
+// The same with one CTA per island of the forward's list 1: (isl_warp,
+// isl_mid] descriptors.
 __global__ void __launch_bounds__(128) k_adj_pgs_mid_smem(DevState s, AdjState A, const uint32_t* lvl_bound) {
     extern __shared__ float4 shm[];
-    const uint32_t n_list = s.counters[kCntList + 1];
+    const uint32_t n_list = s.counters[list_counter(1)];
     const uint32_t* list = s.isl_list[1];
     const int pos = s.pos_iters, vel = s.vel_iters < 1 ? 1 : s.vel_iters;
     const RevLocal D{shm};
@@ -565,14 +566,14 @@ __global__ void __launch_bounds__(128) k_adj_pgs_mid_smem(DevState s, AdjState A
     }
 }
 
-// Reverse PGS sweep on global memory: one CTA per island beyond kMidIsland.
+// Reverse PGS sweep on global memory: one CTA per island beyond isl_mid.
 __global__ void __launch_bounds__(256) k_adj_pgs_block(DevState s, AdjState A, const uint32_t* lvl_bound) {
     const uint32_t ni = *s.n_isl;
     const uint32_t epoch = *A.epoch;
     const int pos = s.pos_iters, vel = s.vel_iters < 1 ? 1 : s.vel_iters;
     for (uint32_t isl = blockIdx.x; isl < ni; isl += gridDim.x) {
         const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
-        if (end - begin <= kMidIsland) continue;
+        if (end - begin <= s.isl_mid) continue;
         const uint32_t nlev = s.isl_end[isl];
         const uint32_t* bound = lvl_bound + begin + isl;
         for (int it = pos + vel - 1; it >= 0; --it) {

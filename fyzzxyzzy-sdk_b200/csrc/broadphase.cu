@@ -294,7 +294,7 @@ void enqueue_broadphase(const DevState& s, cudaStream_t st, const StageHook& hoo
     for (uint32_t i = 0; i < s.n_large; ++i)
         radix_sort_pairs(s.srt_key + s.large_begin[i], s.srt_id + s.large_begin[i],
                          s.srt_key2, s.srt_id2, s.large_n[i], nullptr, 0, 32,
-                         s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err);
+                         s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err, s.radix_bits);
     hook(kStPairs, st);
     if (s.n_finite) {
         k_sweep_gather<<<(s.n_finite + T - 1) / T, T, 0, st>>>(s, rec, meta);

@@ -9,8 +9,9 @@
 // they need no reset between scans; every wait is bounded and reports
 // kErrLogic instead of hanging.
 //
-// The radix sort processes 8-bit digits.  Each pass is three launches:
-//   histogram  per 2048-key tile, 256 bins in shared memory
+// The radix sort processes digits of 8 to 11 bits (a runtime choice: wider
+// digits mean fewer passes, larger histograms).  Each pass is three launches:
+//   histogram  per 2048-key tile, 2^B bins in shared memory
 //   scan       exclusive scan of the digit-major histogram (tile order
 //              inside a digit preserves stability)
 //   scatter    per tile: warp-level multi-split ranking with __match_any_sync
@@ -158,66 +159,90 @@ constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortThreads * kSortItems;
 constexpr int kSortWarps = kSortThreads / 32;
 
-__global__ void k_radix_hist(const uint32_t* __restrict__ keys, uint32_t n, const uint32_t* n_dev,
-                             int shift, uint32_t* __restrict__ hist, uint32_t ntiles) {
-    __shared__ uint32_t h[256];
+template <int B>
+__global__ void __launch_bounds__(kSortThreads) k_radix_hist(const uint32_t* __restrict__ keys, uint32_t n,
+                                                            const uint32_t* n_dev, int shift,
+                                                            uint32_t* __restrict__ hist, uint32_t ntiles) {
+    constexpr uint32_t R = 1u << B;
+    __shared__ uint32_t h[R];
     const uint32_t lim = n_dev ? min(n, *n_dev) : n;
-    h[threadIdx.x] = 0;
+    for (uint32_t d = threadIdx.x; d < R; d += kSortThreads) h[d] = 0;
     __syncthreads();
     const uint32_t base = blockIdx.x * kSortTile;
     for (int i = threadIdx.x; i < kSortTile; i += kSortThreads) {
         const uint32_t idx = base + i;
-        if (idx < lim) atomicAdd(&h[(keys[idx] >> shift) & 255u], 1u);
+        if (idx < lim) atomicAdd(&h[(keys[idx] >> shift) & (R - 1u)], 1u);
     }
     __syncthreads();
-    hist[threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+    for (uint32_t d = threadIdx.x; d < R; d += kSortThreads) hist[d * ntiles + blockIdx.x] = h[d];
 }
 
-__global__ void k_radix_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
-                                uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
-                                uint32_t n, const uint32_t* n_dev, int shift,
-                                const uint32_t* __restrict__ offs, uint32_t ntiles) {
-    __shared__ uint32_t wcount[kSortWarps][257];
-    __shared__ uint32_t wofs[kSortWarps][257];
+// Shared memory of k_radix_scatter<B>: running digit counts of each warp
+// and their exclusive scan across warps (one invalid-key bin each).
+template <int B> constexpr size_t scatter_smem() { return 2 * size_t(kSortWarps) * ((1u << B) + 1) * 4; }
+
+template <int B>
+__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const uint32_t* __restrict__ kin,
+                                                               const uint32_t* __restrict__ vin,
+                                                               uint32_t* __restrict__ kout,
+                                                               uint32_t* __restrict__ vout, uint32_t n,
+                                                               const uint32_t* n_dev, int shift,
+                                                               const uint32_t* __restrict__ offs, uint32_t ntiles) {
+    constexpr uint32_t R = 1u << B;
+    extern __shared__ uint32_t sm[];
+    uint32_t* wcount = sm;                         // [warp][R + 1]
+    uint32_t* wofs = sm + kSortWarps * (R + 1);    // [warp][R + 1]
     const uint32_t lim = n_dev ? min(n, *n_dev) : n;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < kSortWarps * 257; i += kSortThreads) (&wcount[0][0])[i] = 0;
+    for (uint32_t i = threadIdx.x; i < kSortWarps * (R + 1); i += kSortThreads) wcount[i] = 0;
     __syncthreads();
     const uint32_t wbase = blockIdx.x * kSortTile + warp * 32 * kSortItems;
     uint32_t key[kSortItems], val[kSortItems], dig[kSortItems], rank[kSortItems];
     const uint32_t lt = (1u << lane) - 1u;
+    uint32_t* wc = wcount + warp * (R + 1);
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
         const uint32_t idx = wbase + r * 32 + lane;
         const bool valid = idx < lim;
         key[r] = valid ? kin[idx] : 0u;
         val[r] = valid ? vin[idx] : 0u;
-        dig[r] = valid ? ((key[r] >> shift) & 255u) : 256u;
+        dig[r] = valid ? ((key[r] >> shift) & (R - 1u)) : R;
         const uint32_t peers = __match_any_sync(0xffffffffu, dig[r]);
         const int leader = __ffs(peers) - 1;
-        const uint32_t base = wcount[warp][dig[r]];
+        const uint32_t base = wc[dig[r]];
         __syncwarp();
-        if (lane == leader) wcount[warp][dig[r]] = base + __popc(peers);
+        if (lane == leader) wc[dig[r]] = base + __popc(peers);
         __syncwarp();
         rank[r] = base + __popc(peers & lt);
     }
     __syncthreads();
-    {
+    for (uint32_t d = threadIdx.x; d < R; d += kSortThreads) {
         uint32_t s = 0;
         for (int w = 0; w < kSortWarps; ++w) {
-            wofs[w][threadIdx.x] = s;
-            s += wcount[w][threadIdx.x];
+            wofs[w * (R + 1) + d] = s;
+            s += wcount[w * (R + 1) + d];
         }
     }
     __syncthreads();
+    const uint32_t* wo = wofs + warp * (R + 1);
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
-        if (dig[r] < 256u) {
-            const uint32_t pos = offs[dig[r] * ntiles + blockIdx.x] + wofs[warp][dig[r]] + rank[r];
+        if (dig[r] < R) {
+            const uint32_t pos = offs[dig[r] * ntiles + blockIdx.x] + wo[dig[r]] + rank[r];
             kout[pos] = key[r];
             vout[pos] = val[r];
         }
     }
+}
+
+template <int B>
+void radix_pass(const uint32_t* ki, const uint32_t* vi, uint32_t* ko, uint32_t* vo, uint32_t n_cap,
+                const uint32_t* n_dev, int shift, uint32_t* hist, uint32_t ntiles, uint32_t* scan_tmp,
+                size_t scan_words, cudaStream_t st, uint32_t* err) {
+    k_radix_hist<B><<<ntiles, kSortThreads, 0, st>>>(ki, n_cap, n_dev, shift, hist, ntiles);
+    scan_exclusive(hist, hist, (1u << B) * ntiles, nullptr, nullptr, scan_tmp, scan_words, st, err);
+    k_radix_scatter<B><<<ntiles, kSortThreads, scatter_smem<B>(), st>>>(ki, vi, ko, vo, n_cap, n_dev, shift, hist,
+                                                                         ntiles);
 }
 
 }  // namespace
@@ -244,23 +269,37 @@ void scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, const uint32_
 
 size_t radix_hist_words(uint32_t n_cap) {
     const uint32_t ntiles = (n_cap + kSortTile - 1) / kSortTile;
-    return size_t(256) * ntiles + 1;
+    return (size_t(1) << kRadixMaxBits) * ntiles + 1;
 }
 
-// Sorts bits [begin_bit, end_bit) of the keys; the result ends in keys/vals.
+void init_primitive_kernels() {
+    cudaFuncSetAttribute(k_radix_scatter<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(scatter_smem<10>()));
+    cudaFuncSetAttribute(k_radix_scatter<11>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(scatter_smem<11>()));
+}
+
+// Sorts bits [begin_bit, end_bit) of the keys (the other bits must be equal
+// across keys or zero) in passes of digit_bits (8..11) bits; the result
+// ends in keys/vals.
 void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
                       uint32_t n_cap, const uint32_t* n_dev, int begin_bit, int end_bit,
                       uint32_t* hist, size_t hist_words, uint32_t* scan_tmp, size_t scan_words,
-                      cudaStream_t st, uint32_t* err) {
+                      cudaStream_t st, uint32_t* err, int digit_bits) {
     const uint32_t ntiles = (n_cap + kSortTile - 1) / kSortTile;
     if (ntiles == 0) return;
-    (void)hist_words;
+    const int B = digit_bits >= 8 && digit_bits <= kRadixMaxBits ? digit_bits : 8;
+    if ((size_t(1) << B) * ntiles > hist_words) {   // never: the world sizes the histogram for the widest digit
+        if (err) cudaMemsetAsync(err, 0xff, 4, st);
+        return;
+    }
     uint32_t *ki = keys, *vi = vals, *ko = keys_alt, *vo = vals_alt;
     int passes = 0;
-    for (int shift = begin_bit; shift < end_bit; shift += 8, ++passes) {
-        k_radix_hist<<<ntiles, kSortThreads, 0, st>>>(ki, n_cap, n_dev, shift, hist, ntiles);
-        scan_exclusive(hist, hist, 256u * ntiles, nullptr, nullptr, scan_tmp, scan_words, st, err);
-        k_radix_scatter<<<ntiles, kSortThreads, 0, st>>>(ki, vi, ko, vo, n_cap, n_dev, shift, hist, ntiles);
+    for (int shift = begin_bit; shift < end_bit; shift += B, ++passes) {
+        switch (B) {
+            case 9: radix_pass<9>(ki, vi, ko, vo, n_cap, n_dev, shift, hist, ntiles, scan_tmp, scan_words, st, err); break;
+            case 10: radix_pass<10>(ki, vi, ko, vo, n_cap, n_dev, shift, hist, ntiles, scan_tmp, scan_words, st, err); break;
+            case 11: radix_pass<11>(ki, vi, ko, vo, n_cap, n_dev, shift, hist, ntiles, scan_tmp, scan_words, st, err); break;
+            default: radix_pass<8>(ki, vi, ko, vo, n_cap, n_dev, shift, hist, ntiles, scan_tmp, scan_words, st, err); break;
+        }
         uint32_t* t = ki; ki = ko; ko = t;
         t = vi; vi = vo; vo = t;
     }

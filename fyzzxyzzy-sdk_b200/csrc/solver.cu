@@ -446,11 +446,15 @@ __global__ void k_island_classes(DevState s) {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < ni; isl += stride) {
         const uint32_t n = s.isl_begin[isl + 1] - s.isl_begin[isl];
-        auto push = [&](int c) { s.isl_list[c][atomicAdd(&s.counters[kCntList + c], 1u)] = isl; };
+        auto push = [&](int c) { s.isl_list[c][atomicAdd(&s.counters[list_counter(c)], 1u)] = isl; };
+        // partitions
         if (n > kSerialIsland && n <= kMidIsland) push(0);
-        if (n > kSmallIsland && n <= kMidIsland) push(1);
         else if (n > kMidIsland && n <= kBigIsland) push(2);
         else if (n > kBigIsland) push(3);
+        // PGS
+        if (n > s.isl_thread && n <= s.isl_warp) push(5);
+        else if (n > s.isl_warp && n <= s.isl_mid) push(1);
+        else if (n > s.isl_mid && n <= kBigIsland) push(4);
     }
 }
 
@@ -1567,7 +1571,7 @@ __global__ void __launch_bounds__(kPgsThreadBlock) k_pgs_thread(DevState s) {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < ni; isl += stride) {
         const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
-        if (end - begin > kTinyIsland) continue;
+        if (end - begin > s.isl_thread) continue;
         const uint32_t nb = s.isl_nbod[isl];
         const int32_t* ib = s.isl_bod + begin + isl;
         for (uint32_t l = 0; l < nb; ++l) { sdv[l] = zero; sdw[l] = zero; }
@@ -1589,7 +1593,8 @@ __global__ void __launch_bounds__(kPgsWarpsPerBlock * 32, 3) k_pgs_warp(DevState
     __shared__ float4 sh[kPgsWarpsPerBlock][2][kWarpBodies];
     __shared__ uint32_t sdesc[kPgsWarpsPerBlock][2][kSmallIsland];   // descriptor, local bodies per slot
     __shared__ uint32_t sbound[kPgsWarpsPerBlock][kSmallIsland + 1];
-    const uint32_t ni = *s.n_isl;
+    const uint32_t n_list = s.counters[list_counter(5)];
+    const uint32_t* list = s.isl_list[5];
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t wib = threadIdx.x >> 5;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1599,9 +1604,16 @@ __global__ void __launch_bounds__(kPgsWarpsPerBlock * 32, 3) k_pgs_warp(DevState
     float4* sdw = sh[wib][1];
     const LocalDeltas D{sdv, sdw};
     const float4 zero = make_float4(0, 0, 0, 0);
-    for (uint32_t isl = warp; isl < ni; isl += nwarps) {
+    for (uint32_t k = warp;;) {
+        if (s.work_queue) {
+            uint32_t t = 0;
+            if (lane == 0) t = atomicAdd(&s.counters[kCntQueue], 1u);
+            k = __shfl_sync(0xffffffffu, t, 0);
+        }
+        if (k >= n_list) break;
+        const uint32_t isl = list[k];
+        if (!s.work_queue) k += nwarps;
         const uint32_t begin = s.isl_begin[isl], end = s.isl_begin[isl + 1];
-        if (end - begin > kSmallIsland || end - begin <= kTinyIsland) continue;
         const uint32_t nlev = s.isl_end[isl];
         const uint32_t nb = s.isl_nbod[isl];
         const int32_t* ib = s.isl_bod + begin + isl;
@@ -1656,12 +1668,21 @@ __global__ void __launch_bounds__(NT) k_pgs_block_smem(DevState s, const uint32_
     uint32_t* sl = sd + MAXN;                                             // local bodies per placed slot
     uint32_t* sb = sl + MAXN;                                             // partition bounds (island-relative)
     const LocalDeltas D{sdv, sdw};
-    const uint32_t n_list = s.counters[kCntList + list_class];
+    const uint32_t n_list = s.counters[list_counter(list_class)];
     const uint32_t* list = s.isl_list[list_class];
     const int pos = s.pos_iters, vel = s.vel_iters < 1 ? 1 : s.vel_iters;
     const float4 zero = make_float4(0, 0, 0, 0);
-    for (uint32_t k = blockIdx.x; k < n_list; k += gridDim.x) {
+    uint32_t* ticket = s.counters + kCntQueue + (list_class == 1 ? 1 : 2);
+    __shared__ uint32_t s_next;
+    for (uint32_t k = blockIdx.x;;) {
+        if (s.work_queue) {
+            if (threadIdx.x == 0) s_next = atomicAdd(ticket, 1u);
+            __syncthreads();
+            k = s_next;
+        }
+        if (k >= n_list) break;
         const uint32_t isl = list[k];
+        if (!s.work_queue) k += gridDim.x;
         const uint32_t begin = s.isl_begin[isl];
         const uint32_t nlev = s.isl_end[isl];
         const uint32_t nb = s.isl_nbod[isl];
@@ -1938,6 +1959,7 @@ void enqueue_wake_bodies(const DevState& s, cudaStream_t st) {
 }
 
 void init_solver_kernels() {
+    init_primitive_kernels();
     int least = 0, greatest = 0;
     if (cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess) g_high_priority = greatest;
     cudaFuncSetAttribute(k_partition_smem<kBigIsland>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1950,7 +1972,7 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     uint32_t* flags = s.tmp_flags;
     uint32_t* pos = s.tmp_pos;
     uint32_t* lvl_bound = s.lvl_bound;
-    const uint32_t T = 256;
+    const uint32_t T = s.elem_block;   // elementwise kernels (at most 56 registers, no launch bounds)
     const uint32_t cap_blocks = 148u * 8u;
     auto side = [&](int i) { return br ? br->st[i] : st; };
     hook(kStIslands, st);
@@ -1982,20 +2004,21 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
         int rbits = 1;
         while ((1ull << rbits) < uint64_t(s.n_joints) + 2ull * s.pair_cap + 1u) ++rbits;
         k_replay_keys<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
-        radix_sort_pairs(s.d_key, s.d_val, s.d_key2, s.d_val2, s.desc_cap, s.counters + kCntDesc, 0,
-                         (rbits + 7) / 8 * 8, s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err);
+        radix_sort_pairs(s.d_key, s.d_val, s.d_key2, s.d_val2, s.desc_cap, s.counters + kCntDesc, 0, rbits,
+                         s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err, s.radix_bits);
         k_replay_rekey<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     }
     // keys are island roots < n_bodies, or n_bodies for sleeping islands
     int bits = 1;
     while ((1ull << bits) < uint64_t(s.n_bodies) + 1u) ++bits;
-    radix_sort_pairs(s.d_key, s.d_val, s.d_key2, s.d_val2, s.desc_cap, s.counters + kCntDesc, 0,
-                     (bits + 7) / 8 * 8, s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err);
+    radix_sort_pairs(s.d_key, s.d_val, s.d_key2, s.d_val2, s.desc_cap, s.counters + kCntDesc, 0, bits,
+                     s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err, s.radix_bits);
     k_island_flags<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     scan_exclusive(s.isl_flag, pos, s.desc_cap, s.counters + kCntAwake, s.n_isl, s.scan_tmp, s.scan_tmp_words, st,
                    s.err);
     k_island_scatter<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s, pos);
     cudaMemsetAsync(s.counters + kCntList, 0, 4 * sizeof(uint32_t), st);
+    cudaMemsetAsync(s.counters + kCntList4, 0, 5 * sizeof(uint32_t), st);   // lists 4-5, work-queue tickets
     k_island_classes<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     // partitions by island size class, and row preparation: independent
     hook(kStPrep, st);
@@ -2007,18 +2030,18 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     k_partition<<<grid_for(s.desc_cap, kPartWarps, 148u * 16u), kPartWarps * 32, 0, st>>>(s, lvl_bound);
     k_partition_smem<kMidIsland><<<grid_for(s.desc_cap, kSerialIsland + 1, 148u * 8u), 256,
                                    PartSmem<kMidIsland>::kBytes, side(0)>>>(s, lvl_bound, 0);
-    if (s.n_joints) k_prep_joints<<<grid_for(s.n_joints, T, 1u << 30), T, 0, side(2)>>>(s);
+    if (s.n_joints) k_prep_joints<<<grid_for(s.n_joints, 128, 1u << 30), 128, 0, side(2)>>>(s);   // ~150 registers
     k_prep_contacts<<<grid_for(s.desc_cap, 128, cap_blocks), 128, 0, side(2)>>>(s);
     join_branches(br, st, 3);
     // PGS: islands by size class, independent
     hook(kStPgs, st);
     fork_branches(br, st, 3);
-    launch_high(k_pgs_block_smem<kBigIsland, kBigPgsThreads>, grid_for(s.desc_cap, kMidIsland + 1, 148u),
-                kBigPgsThreads, PgsSmem<kBigIsland>::kBytes, side(1), s, lvl_bound, 2);
+    launch_high(k_pgs_block_smem<kBigIsland, kBigPgsThreads>, grid_for(s.desc_cap, s.isl_mid + 1, 148u),
+                kBigPgsThreads, PgsSmem<kBigIsland>::kBytes, side(1), s, lvl_bound, 4);
     launch_high(k_pgs_block, grid_for(s.desc_cap, kBigIsland + 1, 148u), 256u, size_t(0), side(1), s, lvl_bound);
     k_pgs_warp<<<grid_for(s.desc_cap * 32u, kPgsWarpsPerBlock * 32u, 148u * 3u), kPgsWarpsPerBlock * 32u, 0, st>>>(
         s, lvl_bound);
-    k_pgs_block_smem<kMidIsland, 128><<<grid_for(s.desc_cap, kSmallIsland + 1, 148u * 3u), 128,
+    k_pgs_block_smem<kMidIsland, 128><<<grid_for(s.desc_cap, s.isl_warp + 1, 148u * 3u), 128,
                                         PgsSmem<kMidIsland>::kBytes, side(0)>>>(s, lvl_bound, 1);
     k_pgs_thread<<<grid_for(s.desc_cap, kPgsThreadBlock, 148u * 8u), kPgsThreadBlock, 0, side(2)>>>(s);
     join_branches(br, st, 3);

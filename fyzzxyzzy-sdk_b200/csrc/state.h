@@ -42,6 +42,18 @@ struct DevState {
     uint32_t n_scenes = 0, n_bodies = 0, n_shapes = 0, n_finite = 0, n_joints = 0;
     uint32_t pair_cap = 0, desc_cap = 0;
     uint32_t max_small_scene = 2048;   // finite shapes sorted inside one CTA
+    // Performance parameters (fyzz_b200_tuning_t; every choice gives the same
+    // results): islands of at most isl_thread descriptors are solved by one
+    // thread, up to isl_warp by one warp, up to isl_mid by a 128-thread CTA,
+    // up to kBigIsland by the 384-thread CTA; radix sorts take digits of
+    // radix_bits; elementwise kernels run elem_block threads a block.
+    uint32_t isl_thread = 8, isl_warp = 96, isl_mid = 512;
+    int radix_bits = 8;
+    uint32_t elem_block = 256;
+    // Island scheduling of the warp and CTA solvers: false = static (worker
+    // w takes list entries w, w + W, ...), true = a work queue (each worker
+    // takes the next entry from a per-step device counter).
+    bool work_queue = false;
     int pos_iters = 4, vel_iters = 1;
     float dt = 1.0f / 120.0f;
     uint32_t frame = 0;
@@ -155,9 +167,12 @@ struct DevState {
     int32_t* isl_bod = nullptr;        // island isl's bodies at [isl_begin + isl, + isl_nbod)
     uint32_t* isl_nbod = nullptr;      // per island
     // Islands by size class (descriptors), listed each step by
-    // k_island_classes: 0 (32, 512] shared-memory partition, 1 (96, 512]
-    // CTA solver, 2 (512, 4096] both, 3 beyond 4096 global-memory paths.
-    uint32_t* isl_list[4] = {};
+    // k_island_classes: 0 (32, 512] shared-memory partition, 1 (isl_warp,
+    // isl_mid] 128-thread CTA solver, 2 (512, 4096] shared-memory partition,
+    // 3 beyond 4096 global-memory paths, 4 (isl_mid, 4096] 384-thread CTA
+    // solver, 5 (isl_thread, isl_warp] warp solver.
+    static constexpr int kIslLists = 6;
+    uint32_t* isl_list[kIslLists] = {};
 
     // step scratch
     uint4* sw_rec = nullptr;           // sweep y/z bounds in sorted order
@@ -229,8 +244,10 @@ void scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, const uint32_
 void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
                       uint32_t n_cap, const uint32_t* n_dev, int begin_bit, int end_bit,
                       uint32_t* hist, size_t hist_words, uint32_t* scan_tmp, size_t scan_words,
-                      cudaStream_t st, uint32_t* err = nullptr);
+                      cudaStream_t st, uint32_t* err = nullptr, int digit_bits = 8);
+constexpr int kRadixMaxBits = 11;   // widest radix digit
 size_t radix_hist_words(uint32_t n_cap);
+void init_primitive_kernels();
 size_t scan_tmp_words_for(uint32_t n_cap);
 
 // Stage boundaries of one step, reported to an optional hook (the world uses
@@ -325,7 +342,14 @@ enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels =
              kCntConvexEpa = 20 /* regenerated hull pairs continuing in EPA */,
              kCntThRows = 21 /* managers with a reportable impulse */,
              kCntThChanges = 22 /* force-threshold changes of the step */,
-             kCntThCommon = 23 /* pairs exceeding in this step and the previous one */, kCntSlots = 24 };
+             kCntThCommon = 23 /* pairs exceeding in this step and the previous one */,
+             kCntList4 = 24 /* length of island list 4 */, kCntList5 = 25 /* length of island list 5 */,
+             kCntQueue = 26 /* 3 work-queue tickets: warp, mid CTA, big CTA solvers */, kCntSlots = 29 };
+// Counter slot of island list c.
+__host__ __device__ constexpr int list_counter(int c) { return c < 4 ? kCntList + c : kCntList4 + (c - 4); }
+// Each list holds islands of more than this many descriptors (its capacity
+// is descriptors / (bound + 1) + 2).
+constexpr uint32_t kListMinDesc[6] = {32, 32, 512, 4096, 128, 0};
 
 // Contact event records in device memory; the layouts of
 // fyzz_b200_contact_event_t and fyzz_b200_contact_event_point_t.

@@ -19,8 +19,14 @@
 #include "convex.h"
 #include "../../include/fyzz_b200.h"
 
+#include <dlfcn.h>
+
 #include <algorithm>
 #include <array>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <sstream>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -190,6 +196,49 @@ v3 diagonalize(const M3& m, qt& frame) {
     }
     frame = q;
     return {d.c[0].x, d.c[1].y, d.c[2].z};
+}
+
+// The tuning table next to the library (fyzzxyzzy-sdk_b200/tuning.txt for
+// fyzzxyzzy-sdk_b200/lib/libfyzz_b200.so), or FYZZ_B200_TUNING; lines
+// "<class> island_thread island_warp island_cta radix_bits elem_block
+// work_queue",
+// '#' comments.  Returns false when the class has no line.
+bool load_tuning(const std::string& cls, fyzz_b200_tuning_t& out) {
+    std::string path;
+    if (const char* e = std::getenv("FYZZ_B200_TUNING")) {
+        if (std::string(e) == "none") return false;
+        path = e;
+    } else {
+        Dl_info info{};
+        if (!dladdr(reinterpret_cast<void*>(&load_tuning), &info) || !info.dli_fname) return false;
+        std::string lib = info.dli_fname;
+        for (int up = 0; up < 2; ++up) {
+            const size_t slash = lib.find_last_of('/');
+            lib = slash == std::string::npos ? std::string(".") : lib.substr(0, slash);
+        }
+        path = lib + "/tuning.txt";
+    }
+    std::ifstream f(path);
+    std::string line;
+    while (std::getline(f, line)) {
+        if (line.empty() || line[0] == '#') continue;
+        std::istringstream in(line);
+        std::string name;
+        fyzz_b200_tuning_t t{};
+        if (in >> name >> t.island_thread >> t.island_warp >> t.island_cta >> t.radix_bits >> t.elem_block >>
+                t.work_queue &&
+            name == cls) {
+            out = t;
+            return true;
+        }
+    }
+    return false;
+}
+void validate_tuning(const fyzz_b200_tuning_t& t) {
+    if (t.island_thread > 8 || t.island_warp < 32 || t.island_warp > 96 || t.island_cta < 128 || t.island_cta > 512 ||
+        t.radix_bits < 8 || t.radix_bits > 11 || t.elem_block < 64 || t.elem_block > 1024 || t.elem_block % 32 ||
+        t.work_queue > 1)
+        throw std::invalid_argument("Tuning parameters outside their ranges");
 }
 
 template <class T> void dalloc(T*& p, size_t n, std::vector<void*>& owned) {
@@ -733,6 +782,21 @@ public:
         last_cur_ = last;
     }
     uint32_t pair_budget() const { return d_.pair_cap; }
+    // Performance parameters; an explicit setting outlives rebuilds of the
+    // device state, otherwise the world's class line of the tuning table
+    // applies when the device state is built.
+    void set_tuning(const fyzz_b200_tuning_t& t) {
+        validate_tuning(t);
+        tuning_ = t;
+        tuning_explicit_ = true;
+        apply_tuning();
+    }
+    fyzz_b200_tuning_t tuning() {
+        check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+        ensure_device();
+        return tuning_;
+    }
+    std::string tuning_class() const { return tuning_class_; }
     // The solver order of the next step, as the reference's Scene chose it
     // (partition_constraints' input: joints in constraint order, then the
     // touching managers in its island-edge order, scene.cpp:7153-7216):
@@ -887,7 +951,7 @@ public:
         float *tn = nullptr, *tf = nullptr, *tj = nullptr;
         uint32_t *d_val2 = nullptr, *d_lbod = nullptr, *lvl_bound = nullptr, *isl_begin = nullptr,
                  *isl_end = nullptr, *isl_nbod = nullptr, *n_isl = nullptr, *counters = nullptr;
-        uint32_t* lists[4] = {};
+        uint32_t* lists[DevState::kIslLists] = {};
         int32_t* isl_bod = nullptr;
         int parity = 0;
     };
@@ -909,10 +973,7 @@ public:
         dalloc(f.lvl_bound, 2 * dc + 2, o); dalloc(f.isl_bod, 2 * dc + 2, o);
         dalloc(f.isl_begin, dc + 1, o); dalloc(f.isl_end, dc + 1, o); dalloc(f.isl_nbod, dc + 1, o);
         dalloc(f.n_isl, 1, o); dalloc(f.counters, kCntSlots, o);
-        dalloc(f.lists[0], dc / 33 + 2, o);
-        dalloc(f.lists[1], dc / (kSmallIsland + 1) + 2, o);
-        dalloc(f.lists[2], dc / (kMidIsland + 1) + 2, o);
-        dalloc(f.lists[3], dc / (kBigIsland + 1) + 2, o);
+        for (int k = 0; k < DevState::kIslLists; ++k) dalloc(f.lists[k], dc / (kListMinDesc[k] + 1) + 2, o);
     }
     // The step's DevState with its per-step arrays in frame f.
     DevState framed(const Frame& f, int parity) const {
@@ -926,7 +987,7 @@ public:
         s.tape_n = f.tn; s.tape_f = f.tf; s.tape_j = d_.n_joints ? f.tj : nullptr;
         s.d_val2 = f.d_val2; s.d_lbod = f.d_lbod; s.lvl_bound = f.lvl_bound; s.isl_bod = f.isl_bod;
         s.isl_begin = f.isl_begin; s.isl_end = f.isl_end; s.isl_nbod = f.isl_nbod; s.n_isl = f.n_isl;
-        for (int k = 0; k < 4; ++k) s.isl_list[k] = f.lists[k];
+        for (int k = 0; k < DevState::kIslLists; ++k) s.isl_list[k] = f.lists[k];
         return s;
     }
     void release_segment_graphs() {
@@ -1745,10 +1806,8 @@ private:
         dalloc(d_.d_lbod, dc, pair_owned_);
         dalloc(d_.isl_bod, 2 * size_t(dc) + 2, pair_owned_);
         dalloc(d_.isl_nbod, size_t(dc) + 1, pair_owned_);
-        dalloc(d_.isl_list[0], size_t(dc) / 33 + 2, pair_owned_);
-        dalloc(d_.isl_list[1], size_t(dc) / (kSmallIsland + 1) + 2, pair_owned_);
-        dalloc(d_.isl_list[2], size_t(dc) / (kMidIsland + 1) + 2, pair_owned_);
-        dalloc(d_.isl_list[3], size_t(dc) / (kBigIsland + 1) + 2, pair_owned_);
+        for (int k = 0; k < DevState::kIslLists; ++k)
+            dalloc(d_.isl_list[k], size_t(dc) / (kListMinDesc[k] + 1) + 2, pair_owned_);
         dalloc(d_.isl_begin, size_t(dc) + 1, pair_owned_);
         dalloc(d_.isl_end, size_t(dc) + 1, pair_owned_);
         dalloc(d_.isl_flag, dc, pair_owned_);
@@ -1936,6 +1995,16 @@ private:
         upload_joints();
         check_cuda(cudaStreamSynchronize(stream_), "joint upload");
     }
+    void apply_tuning() {
+        d_.isl_thread = tuning_.island_thread;
+        d_.isl_warp = tuning_.island_warp;
+        d_.isl_mid = tuning_.island_cta;
+        d_.radix_bits = int(tuning_.radix_bits);
+        d_.elem_block = tuning_.elem_block;
+        d_.work_queue = tuning_.work_queue != 0;
+        for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        release_segment_graphs();
+    }
     void build_device() {
         release_device();
         DevState d;
@@ -1990,6 +2059,21 @@ private:
             }
         }
         d.n_small = uint32_t(small.size());
+        tuning_class_ = d.n_large ? "large_scene" : "many_scenes";
+        if (!tuning_explicit_) {
+            fyzz_b200_tuning_t t{8, 96, 512, 8, 256, 0};
+            fyzz_b200_tuning_t table{};
+            if (load_tuning(tuning_class_, table)) {
+                try { validate_tuning(table); t = table; } catch (const std::invalid_argument&) {}
+            }
+            tuning_ = t;
+        }
+        d.isl_thread = tuning_.island_thread;
+        d.isl_warp = tuning_.island_warp;
+        d.isl_mid = tuning_.island_cta;
+        d.radix_bits = int(tuning_.radix_bits);
+        d.elem_block = tuning_.elem_block;
+        d.work_queue = tuning_.work_queue != 0;
         d.events = notify_;
         d.sleep = sleep_enabled_;
         d.thresholds = thresholds_;
@@ -2112,6 +2196,9 @@ private:
     static constexpr uint32_t kJointReserve = 256;
     uint32_t joint_cap_ = 0, jrow_cap_ = 0;   // joints / joint rows the device tables hold
     int norm_passes_ = 2;                      // orientation normalisations of authored transforms
+    fyzz_b200_tuning_t tuning_{8, 96, 512, 8, 256, 0};
+    bool tuning_explicit_ = false;
+    std::string tuning_class_ = "many_scenes";
     bool replay_pending_ = false, snap_replay_ = false;   // a replayed descriptor order for the next step
     uint64_t replay_cap_ = 0, replay_jcap_ = 0;
     std::vector<uint32_t> scene_body_begin_, scene_shape_begin_;
@@ -2545,6 +2632,14 @@ int fyzz_b200_set_descriptor_order(fyzz_b200_world* w, const uint32_t* pairs, ui
                                    const uint64_t* joint_ids, uint64_t n_joint_ids) {
     if ((n_pairs && !pairs) || (n_joint_ids && !joint_ids)) return FYZZ_B200_INVALID_ARGUMENT;
     return guarded(w, [&](auto& W) { W.set_descriptor_order(pairs, n_pairs, joint_ids, n_joint_ids); });
+}
+int fyzz_b200_set_tuning(fyzz_b200_world* w, const fyzz_b200_tuning_t* t) {
+    if (!t) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) { W.set_tuning(*t); });
+}
+int fyzz_b200_get_tuning(fyzz_b200_world* w, fyzz_b200_tuning_t* t) {
+    if (!t) return FYZZ_B200_INVALID_ARGUMENT;
+    return guarded(w, [&](auto& W) { *t = W.tuning(); });
 }
 int fyzz_b200_set_pair_budget(fyzz_b200_world* w, uint32_t pairs, uint32_t* budget_out) {
     return guarded(w, [&](auto& W) {

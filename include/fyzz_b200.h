@@ -203,6 +203,26 @@ int fyzz_b200_synchronize(fyzz_b200_world* w);
  * 7 integration.  (Counterpart of the reference's
  * Context::profile_batch_gpu_nanoseconds, compute.h:299.) */
 int fyzz_b200_profile_step(fyzz_b200_world* w, float seconds, float* stage_ms, uint32_t n);
+/* ---- performance parameters (no reference counterpart) ----
+ * Choices that change how the step runs, not what it computes: every
+ * setting gives bit-identical results.  A world starts from the tuning
+ * table next to the library (tuning.txt, written by the package's
+ * autotune.py on a B200; FYZZ_B200_TUNING names another file, "none"
+ * keeps the defaults below), taking the line of its class: "large_scene"
+ * when some scene has more than 2,048 finite shapes, else "many_scenes".
+ * fyzz_b200_set_tuning overrides it for the world. */
+typedef struct {
+    uint32_t island_thread;  /* islands of at most this many descriptors are solved by one thread (0..8; 8) */
+    uint32_t island_warp;    /* ... up to this many by one warp (32..96; 96) */
+    uint32_t island_cta;     /* ... up to this many by one 128-thread CTA (128..512; 512); larger islands up to
+                                4,096 by one 384-thread CTA, beyond that from global memory */
+    uint32_t radix_bits;     /* digit width of the device-wide radix sorts (8..11; 8) */
+    uint32_t elem_block;     /* threads a block of the elementwise kernels (64..1024, multiple of 32; 256) */
+    uint32_t work_queue;     /* warp and CTA solvers take islands round-robin (0) or from a device work
+                                queue, the next list entry per worker from a per-step counter (1); 0 */
+} fyzz_b200_tuning_t;
+int fyzz_b200_set_tuning(fyzz_b200_world* w, const fyzz_b200_tuning_t* tuning);
+int fyzz_b200_get_tuning(fyzz_b200_world* w, fyzz_b200_tuning_t* tuning);
 /* Kernel launches in one captured step graph (0 before the first step). */
 int fyzz_b200_kernels_per_step(fyzz_b200_world* w, uint32_t* out);
 
