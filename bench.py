@@ -561,6 +561,7 @@ def run_b200(args, rank, world, local_rank):
         ms_max = max_over_ranks(ms)
         counts = w.counts()
         kernels = w.kernels_per_step()
+        tuning = w.tuning()
 
         # ---- per-stage device times (CUDA events at stage boundaries) ----
         prof = {}
@@ -624,6 +625,7 @@ def run_b200(args, rank, world, local_rank):
         bprof = wb.profile_step(DT)
         bcounts = wb.counts()
         bkernels = wb.kernels_per_step()
+        btuning = wb.tuning()
         wb.close()
         same = plain_same_bodies(torch, pkg, specs, local_rank, args.same_scenes, args.same_steps)
         batched = {"workload": BATCHED_WORKLOAD, "scenes": len(specs) * world, "bodies": nb_dyn * world,
@@ -631,6 +633,7 @@ def run_b200(args, rank, world, local_rank):
                    "ms_per_step": bms_max / args.batched_steps, "clocks": bclocks,
                    "stages_ms": {k: round(v, 4) for k, v in bprof.items()},
                    "counts": bcounts, "gpu_launches": bkernels * args.batched_steps,
+                   "tuning": dict(btuning, table_class="many_scenes"),
                    "plain_same_bodies": same,
                    "vs_plain_same_bodies": bvalue / world / same["value"] if same else None}
 
@@ -662,6 +665,8 @@ def run_b200(args, rank, world, local_rank):
             "config": plain_config(spec, start, world),
             "gpu_launches": kernels * args.steps,
             "kernels_per_step": kernels,
+            "tuning": dict(tuning, table_class="large_scene",
+                           source="fyzzxyzzy-sdk_b200/tuning.txt (fyzzxyzzy-sdk_b200/autotune.py)"),
             "clocks": clocks,
             "counts": counts,
             "roofline": roofline,
