@@ -25,6 +25,7 @@
 // barriers only: no grid-wide synchronisation and no host round trip.
 #include "solver_common.cuh"
 #include <cfloat>
+#include <type_traits>
 
 namespace fyzz::b200 {
 
@@ -1364,11 +1365,41 @@ __device__ __forceinline__ void ldg256(const void* p, float4& a, float4& b) {
                  : "memory");
 }
 
-// One descriptor's rows for pass `it` (scene.cpp:8853-9148).  lid carries
-// the island-local bodies when D addresses shared memory.
+// A joint's rows in order (scene.cpp:8905-8945) between bodies b0 / b1
+// (-1: the static world).
+template <class D>
+__device__ __forceinline__ void solve_joint(const DevState& s, uint32_t d, int32_t b0, int32_t b1, int it, int pos,
+                                            const D& D_) {
+    v3 av, aw, bv, bw;
+    D_.load(b0, av, aw);
+    D_.load(b1, bv, bw);
+    const uint32_t r0 = s.j_row[d], nr = joint_row_count(s.j_kind[d]);
+    for (uint32_t q = 0; q < nr; ++q) {
+        JointRow& r = s.jrow[r0 + q];
+        const v3 ax = lv(r.axis), ja = lv(r.ang_a), jb = lv(r.ang_b);
+        const float nd = ax.x * (av.x - bv.x) + ax.y * (av.y - bv.y) + ax.z * (av.z - bv.z) + vdot(ja, aw) -
+                         vdot(jb, bw);
+        const float cst = it < pos ? r.constant : r.unbiased;
+        const float nx = sclamp(r.applied + nd * r.vel_mult + cst, -FLT_MAX, FLT_MAX);
+        const float imp = nx - r.applied;
+        const float ia = imp * r.ima, ib = imp * r.imb;
+        av = {av.x + ia * ax.x, av.y + ia * ax.y, av.z + ia * ax.z};
+        bv = {bv.x - ib * ax.x, bv.y - ib * ax.y, bv.z - ib * ax.z};
+        aw = {aw.x + imp * ja.x, aw.y + imp * ja.y, aw.z + imp * ja.z};
+        bw = {bw.x - imp * jb.x, bw.y - imp * jb.y, bw.z - imp * jb.z};
+        r.applied = nx;
+        if (s.tape_j) s.tape_j[size_t(it) * s.n_jrows + r0 + q] = nx;
+    }
+    D_.store(b0, av, aw);
+    D_.store(b1, bv, bw);
+}
+
+// One descriptor's rows for pass `it` (scene.cpp:8853-9148), read from the
+// per-manager arrays prep writes.  lid carries the island-local bodies when
+// D addresses shared memory.
 // kEagerFriction issues the friction-row loads together with the normal
-// rows (lowest latency, for the CTA solvers); otherwise they are issued
-// after the normal rows are solved (fewer registers, for the warp solver).
+// rows (lowest latency); otherwise they are issued after the normal rows
+// are solved (fewer registers).
 template <class D, bool kEagerFriction = true>
 __device__ void solve_desc(const DevState& s, uint32_t d, uint32_t lid, int it, int pos, int vel, const D& D_) {
     if (d < s.n_joints) {
@@ -1380,34 +1411,12 @@ __device__ void solve_desc(const DevState& s, uint32_t d, uint32_t lid, int it, 
             b0 = is_dyn(s, s.j_a[d]) ? int32_t(s.j_a[d]) : -1;
             b1 = is_dyn(s, s.j_b[d]) ? int32_t(s.j_b[d]) : -1;
         }
-        v3 av, aw, bv, bw;
-        D_.load(b0, av, aw);
-        D_.load(b1, bv, bw);
-        // the joint's rows in order (scene.cpp:8905-8945)
-        const uint32_t r0 = s.j_row[d], nr = joint_row_count(s.j_kind[d]);
-        for (uint32_t q = 0; q < nr; ++q) {
-            JointRow& r = s.jrow[r0 + q];
-            const v3 ax = lv(r.axis), ja = lv(r.ang_a), jb = lv(r.ang_b);
-            const float nd = ax.x * (av.x - bv.x) + ax.y * (av.y - bv.y) + ax.z * (av.z - bv.z) + vdot(ja, aw) -
-                             vdot(jb, bw);
-            const float cst = it < pos ? r.constant : r.unbiased;
-            const float nx = sclamp(r.applied + nd * r.vel_mult + cst, -FLT_MAX, FLT_MAX);
-            const float imp = nx - r.applied;
-            const float ia = imp * r.ima, ib = imp * r.imb;
-            av = {av.x + ia * ax.x, av.y + ia * ax.y, av.z + ia * ax.z};
-            bv = {bv.x - ib * ax.x, bv.y - ib * ax.y, bv.z - ib * ax.z};
-            aw = {aw.x + imp * ja.x, aw.y + imp * ja.y, aw.z + imp * ja.z};
-            bw = {bw.x - imp * jb.x, bw.y - imp * jb.y, bw.z - imp * jb.z};
-            r.applied = nx;
-            if (s.tape_j) s.tape_j[size_t(it) * s.n_jrows + r0 + q] = nx;
-        }
-        D_.store(b0, av, aw);
-        D_.store(b1, bv, bw);
+        solve_joint(s, d, b0, b1, it, pos, D_);
         return;
     }
     const uint32_t m = d - s.n_joints;
-    // All of a manager's rows are loaded up front (128-bit loads, issued
-    // together) before the sequential Gauss-Seidel updates run on registers.
+    // All of a manager's rows are loaded up front (issued together) before
+    // the sequential Gauss-Seidel updates run on registers.
     // NormalRow float4s: {n.xyz, ra.x} {ra.yz, rb.xy} {rb.z, vel_mult,
     // imp_mult, biased} {unbiased, applied, max_impulse, -}; FrictionRow:
     // {t.xyz, ra.x} {ra.yz, rb.xy} {rb.z, vel_mult, bias, target} {applied}.
@@ -1528,6 +1537,207 @@ __device__ void solve_desc(const DevState& s, uint32_t d, uint32_t lid, int it, 
     D_.store(h0, av, aw);
     D_.store(h1, bv, bw);
 }
+
+// ---- placed-order planes (DevState::slot_rows) ----
+// The island solvers copy each manager's rows once per step into planes
+// indexed by placed slot, keeping only what the passes read.  Slots come in
+// blocks of 32; a block holds kSlotVecPlanes float4 planes of 32 records --
+// 0: {sf, df, ima, imb}; normal row j at 1 + 3j: {n.xyz, ra.x} {ra.yz,
+// rb.xy} {rb.z, vel_mult, imp_mult, max_impulse}; friction row k at
+// 13 + 3k: {t.xyz, ra.x} {ra.yz, rb.xy} {rb.z, vel_mult, bias, target} --
+// and, after all blocks' vector planes, kSlotScalarPlanes float planes of
+// 32 records -- biased j (0 + j), unbiased j (4 + j), normal applied j
+// (8 + j), friction applied k (12 + k).  Lanes solving consecutive slots
+// read consecutive records, a plane is a constant offset from the slot's
+// first record, and only the rows a manager has are read (its point and
+// anchor counts travel with its island-local bodies).
+struct SlotPtr {
+    float4* v;   // plane 0 record of the slot; plane p at v + 32 p
+    float* f;    // scalar plane 0 record; plane p at f + 32 p
+    __device__ __forceinline__ SlotPtr(const DevState& s, uint32_t slot) {
+        const size_t blk = slot >> 5, lane = slot & 31u;
+        v = s.slot_rows + blk * (32u * kSlotVecPlanes) + lane;
+        const size_t nblk = (size_t(s.desc_cap) + 31u) >> 5;
+        f = reinterpret_cast<float*>(s.slot_rows + nblk * (32u * kSlotVecPlanes)) + blk * (32u * kSlotScalarPlanes) +
+            lane;
+    }
+    __device__ __forceinline__ float4& vec(uint32_t p) const { return v[32 * p]; }
+    __device__ __forceinline__ float& sca(uint32_t p) const { return f[32 * p]; }
+};
+// Island-local bodies in 13 bits each (0x1fff: the static world), the
+// manager's point count in bits 13-15 and anchor count in bits 29-31.
+__device__ __forceinline__ uint32_t pack_slot_meta(uint32_t lid, uint32_t count, uint32_t anchors) {
+    const uint32_t lo = lid & 0xffffu, hi = lid >> 16;
+    const uint32_t lo13 = lo == 0xffffu ? 0x1fffu : lo, hi13 = hi == 0xffffu ? 0x1fffu : hi;
+    return lo13 | (count << 13) | (hi13 << 16) | (anchors << 29);
+}
+__device__ __forceinline__ int32_t unpack_local13(uint32_t v) {
+    v &= 0x1fffu;
+    return v == 0x1fffu ? -1 : int32_t(v);
+}
+// Copies manager m's rows to slot `slot` and returns its island-local
+// bodies with the counts (pack_slot_meta).
+__device__ __forceinline__ uint32_t stage_slot_rows(const DevState& s, uint32_t m, uint32_t slot, uint32_t lid) {
+    const float4* nr = reinterpret_cast<const float4*>(s.nrow + 4 * size_t(m));
+    const float4* fq = reinterpret_cast<const float4*>(s.frow + 4 * size_t(m));
+    const SlotPtr P(s, slot);
+    float4 h0, h1, q[2][4];
+    // rows 0-1 travel with the header; the rest once the counts are known
+    ldg256(s.mh + m, h0, h1);
+    ldg256(nr, q[0][0], q[0][1]);
+    ldg256(nr + 2, q[0][2], q[0][3]);
+    ldg256(nr + 4, q[1][0], q[1][1]);
+    ldg256(nr + 6, q[1][2], q[1][3]);
+    const uint32_t count = min(__float_as_uint(h0.z), 4u), anchors = min(__float_as_uint(h0.w), 2u);
+    P.vec(0) = h1;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (uint32_t(j) >= count) break;
+        if (j == 2) {
+            ldg256(nr + 8, q[0][0], q[0][1]);
+            ldg256(nr + 10, q[0][2], q[0][3]);
+            if (count > 3) {
+                ldg256(nr + 12, q[1][0], q[1][1]);
+                ldg256(nr + 14, q[1][2], q[1][3]);
+            }
+        }
+        const float4* r = q[j & 1];
+        P.vec(1 + 3 * j) = r[0];
+        P.vec(2 + 3 * j) = r[1];
+        P.vec(3 + 3 * j) = make_float4(r[2].x, r[2].y, r[2].z, r[3].z);
+        P.sca(0 + j) = r[2].w;
+        P.sca(4 + j) = r[3].x;
+        P.sca(8 + j) = r[3].y;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (uint32_t(k) >= 2 * anchors) break;
+        float4 f0, f1, f2, f3;
+        ldg256(fq + 4 * k, f0, f1);
+        ldg256(fq + 4 * k + 2, f2, f3);
+        P.vec(13 + 3 * k) = f0;
+        P.vec(14 + 3 * k) = f1;
+        P.vec(15 + 3 * k) = f2;
+        P.sca(12 + k) = f3.x;
+    }
+    return pack_slot_meta(lid, count, anchors);
+}
+
+// solve_desc on the placed-order planes: descriptor d in slot `slot`, its
+// island-local bodies and counts in meta (pack_slot_meta).  The same
+// arithmetic in the same order; the impulses of the last pass also go back
+// to the per-manager rows, where the events, the force thresholds and the
+// rollouts read them.
+template <class D, bool kEagerFriction = true>
+__device__ void solve_slot(const DevState& s, uint32_t d, uint32_t meta, int it, int pos, int vel, const D& D_,
+                           uint32_t slot) {
+    const int32_t h0 = unpack_local13(meta), h1 = unpack_local13(meta >> 16);
+    if (d < s.n_joints) {
+        solve_joint(s, d, h0, h1, it, pos, D_);
+        return;
+    }
+    const uint32_t m = d - s.n_joints;
+    const uint32_t count = (meta >> 13) & 7u, anchors = meta >> 29;
+    const bool last = it + 1 == pos + vel;
+    const bool friction = (it >= pos || pos - it <= 3) && anchors;
+    const SlotPtr P(s, slot);
+    const float4 hd = P.vec(0);   // {sf, df, ima, imb}
+    const float ima = hd.z, imb = hd.w;        // 0 for the static world
+    float4 n0[4], n1[4], n2[4], f0[4], f1[4], f2[4];
+    float ne[4], na[4], fa[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (uint32_t(j) < count) {
+            n0[j] = P.vec(1 + 3 * j);
+            n1[j] = P.vec(2 + 3 * j);
+            n2[j] = P.vec(3 + 3 * j);
+            ne[j] = P.sca((it < pos ? 0 : 4) + j);
+            na[j] = P.sca(8 + j);
+        }
+    if constexpr (kEagerFriction) {
+        if (friction) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (uint32_t(k) < 2 * anchors) {
+                    f0[k] = P.vec(13 + 3 * k);
+                    f1[k] = P.vec(14 + 3 * k);
+                    f2[k] = P.vec(15 + 3 * k);
+                    fa[k] = P.sca(12 + k);
+                }
+        }
+    }
+    v3 av, aw, bv, bw;
+    D_.load(h0, av, aw);
+    D_.load(h1, bv, bw);
+    float nsum = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (uint32_t(j) >= count) break;
+        const v3 n = {n0[j].x, n0[j].y, n0[j].z};
+        const v3 ra = {n0[j].w, n1[j].x, n1[j].y};
+        const v3 rb = {n1[j].z, n1[j].w, n2[j].x};
+        const float vel_mult = n2[j].y, imp_mult = n2[j].z, max_impulse = n2[j].w;
+        const float applied = na[j];
+        const float nvel = vdot(n, av) - vdot(n, bv) + vdot(aw, ra) - vdot(bw, rb);
+        const float dc = smax(-nvel * vel_mult + ne[j], -applied);
+        const float ni = smin(max_impulse, imp_mult * applied + dc);
+        const float dl = ni - applied;
+        const float da = dl * ima, db = dl * imb;
+        av = {av.x + n.x * da, av.y + n.y * da, av.z + n.z * da};
+        bv = {bv.x - n.x * db, bv.y - n.y * db, bv.z - n.z * db};
+        aw = {aw.x + ra.x * dl, aw.y + ra.y * dl, aw.z + ra.z * dl};
+        bw = {bw.x - rb.x * dl, bw.y - rb.y * dl, bw.z - rb.z * dl};
+        P.sca(8 + j) = ni;
+        if (last) s.nrow[4 * size_t(m) + j].applied = ni;
+        if (s.tape_n) s.tape_n[(size_t(it) * s.pair_cap + m) * 4 + j] = ni;
+        nsum += ni;
+    }
+    if (friction) {
+        if constexpr (!kEagerFriction) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (uint32_t(k) < 2 * anchors) {
+                    f0[k] = P.vec(13 + 3 * k);
+                    f1[k] = P.vec(14 + 3 * k);
+                    f2[k] = P.vec(15 + 3 * k);
+                    fa[k] = P.sca(12 + k);
+                }
+        }
+        const float coeff = anchors == 2 ? 0.5f : 1.0f;
+        const float ms = hd.x * coeff * nsum;
+        const float md = hd.y * coeff * nsum;
+        bool broken = false;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (uint32_t(k) >= 2 * anchors) break;
+            const v3 n = {f0[k].x, f0[k].y, f0[k].z};
+            const v3 ra = {f0[k].w, f1[k].x, f1[k].y};
+            const v3 rb = {f1[k].z, f1[k].w, f2[k].x};
+            const float vel_mult = f2[k].y, target = f2[k].w, applied = fa[k];
+            const float td = vdot(n, av) - vdot(n, bv) + vdot(aw, ra) - vdot(bw, rb);
+            const float bias = it < pos ? f2[k].z : 0.0f;
+            const float cand = applied + (target - bias - td) * vel_mult;
+            const bool clamped = fabsf(cand) > ms;
+            const float nx = clamped ? smin(md, smax(-md, cand)) : cand;
+            const float dl = nx - applied;
+            const float da = dl * ima, db = dl * imb;
+            av = {av.x + n.x * da, av.y + n.y * da, av.z + n.z * da};
+            bv = {bv.x - n.x * db, bv.y - n.y * db, bv.z - n.z * db};
+            aw = {aw.x + ra.x * dl, aw.y + ra.y * dl, aw.z + ra.z * dl};
+            bw = {bw.x - rb.x * dl, bw.y - rb.y * dl, bw.z - rb.z * dl};
+            P.sca(12 + k) = nx;
+            if (last) s.frow[4 * size_t(m) + k].applied = nx;
+            if (s.tape_f) s.tape_f[(size_t(it) * s.pair_cap + m) * 4 + k] = nx;
+            broken |= clamped;
+        }
+        if (last) {
+            FrictionHist& h = s.cur.fric[s.man_list[m]];
+            h.meta = (h.meta & ~256u) | (broken ? 256u : 0u);
+        }
+    }
+    D_.store(h0, av, aw);
+    D_.store(h1, bv, bw);
+}
 __device__ __forceinline__ void save_motion(const DevState& s, uint32_t d) {
     int32_t b0, b1;
     if (d < s.n_joints) {
@@ -1623,8 +1833,9 @@ __global__ void __launch_bounds__(kPgsWarpsPerBlock * 32, 3) k_pgs_warp(DevState
         uint32_t* sb = sbound[wib];
         for (uint32_t l = lane; l < nb; l += 32) { sdv[l] = zero; sdw[l] = zero; }
         for (uint32_t i = lane; i < end - begin; i += 32) {
-            sd[i] = s.d_val2[begin + i];
-            sl[i] = s.d_lbod[begin + i];
+            const uint32_t d = s.d_val2[begin + i], lid = s.d_lbod[begin + i];
+            sd[i] = d;
+            sl[i] = d >= s.n_joints ? stage_slot_rows(s, d - s.n_joints, begin + i, lid) : pack_slot_meta(lid, 0u, 0u);
         }
         for (uint32_t l = lane; l <= nlev; l += 32) sb[l] = bound[l] - begin;
         __syncwarp();
@@ -1632,7 +1843,7 @@ __global__ void __launch_bounds__(kPgsWarpsPerBlock * 32, 3) k_pgs_warp(DevState
             for (uint32_t l = 0; l < nlev; ++l) {
                 const uint32_t lb = sb[l], le = sb[l + 1];
                 for (uint32_t i = lb + lane; i < le; i += 32)
-                    solve_desc<LocalDeltas, false>(s, sd[i], sl[i], it, pos, vel, D);
+                    solve_slot<LocalDeltas, false>(s, sd[i], sl[i], it, pos, vel, D, begin + i);
                 __syncwarp();
             }
             if (it + 1 == pos) {
@@ -1691,8 +1902,9 @@ __global__ void __launch_bounds__(NT) k_pgs_block_smem(DevState s, const uint32_
         const uint32_t n = s.isl_begin[isl + 1] - begin;
         for (uint32_t l = threadIdx.x; l < nb; l += blockDim.x) { sdv[l] = zero; sdw[l] = zero; }
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-            sd[i] = s.d_val2[begin + i];
-            sl[i] = s.d_lbod[begin + i];
+            const uint32_t d = s.d_val2[begin + i], lid = s.d_lbod[begin + i];
+            sd[i] = d;
+            sl[i] = d >= s.n_joints ? stage_slot_rows(s, d - s.n_joints, begin + i, lid) : pack_slot_meta(lid, 0u, 0u);
         }
         for (uint32_t l = threadIdx.x; l <= nlev; l += blockDim.x) sb[l] = bound[l] - begin;
         __syncthreads();
@@ -1700,7 +1912,7 @@ __global__ void __launch_bounds__(NT) k_pgs_block_smem(DevState s, const uint32_
             for (uint32_t l = 0; l < nlev; ++l) {
                 const uint32_t lb = sb[l], le = sb[l + 1];
                 for (uint32_t i = lb + threadIdx.x; i < le; i += blockDim.x)
-                    solve_desc(s, sd[i], sl[i], it, pos, vel, D);
+                    solve_slot<LocalDeltas>(s, sd[i], sl[i], it, pos, vel, D, begin + i);
                 __syncthreads();
             }
             if (it + 1 == pos) {

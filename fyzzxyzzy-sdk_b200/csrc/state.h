@@ -133,6 +133,10 @@ struct DevState {
     ManagerHeader* mh = nullptr;       // per touching manager
     NormalRow* nrow = nullptr;         // 4 per touching manager
     FrictionRow* frow = nullptr;       // 4 per touching manager
+    // The island solvers' copy of the rows in placed-descriptor order (slot
+    // i = position in d_val2): kSlotVecPlanes float4 planes then
+    // kSlotScalarPlanes float planes of desc_cap records.
+    float4* slot_rows = nullptr;
 
     // joints (static, sorted by scene then constraint slot descending)
     uint32_t *j_a = nullptr, *j_b = nullptr;  // descriptor bodies (distance: ordered pair; others: authored)
@@ -329,6 +333,9 @@ void init_solver_kernels();
 constexpr uint32_t kSmallIsland = 96;     // one warp
 constexpr uint32_t kMidIsland = 512;      // one CTA, shared-memory deltas
 constexpr uint32_t kBigIsland = 4096;     // one CTA, shared-memory deltas (1 CTA / SM)
+// Planes of DevState::slot_rows, desc_cap records each: 25 of float4, then
+// 16 of float (the layout is described where the solver stages them).
+constexpr uint32_t kSlotVecPlanes = 25, kSlotScalarPlanes = 16;
 // counters[] slots
 enum : int { kCntMan = 0, kCntDesc = 1, kCntIsl = 2, kCntFrame = 3, kCntLevels = 4, kCntGjk = 5,
              kCntAwake = 6 /* descriptors of awake islands */, kCntSleeping = 7 /* asleep at step start */,

@@ -1799,6 +1799,7 @@ private:
         dalloc(d_.nrow, size_t(cap) * 4, pair_owned_);
         dalloc(d_.frow, size_t(cap) * 4, pair_owned_);
         const uint32_t dc = d_.desc_cap;
+        dalloc(d_.slot_rows, (size_t(dc) + 31u) / 32u * 32u * (kSlotVecPlanes + kSlotScalarPlanes / 4), pair_owned_);
         dalloc(d_.d_key, dc, pair_owned_); dalloc(d_.d_val, dc, pair_owned_);
         dalloc(d_.d_key2, dc, pair_owned_); dalloc(d_.d_val2, dc, pair_owned_);
         dalloc(d_.d_level, dc, pair_owned_);
