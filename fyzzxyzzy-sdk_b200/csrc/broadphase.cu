@@ -113,6 +113,137 @@ __global__ void __launch_bounds__(kSmallSortThreads) k_sort_small(DevState s) {
     }
 }
 
+// ---- z bands of large scenes ----
+// A one-axis sweep of a wide scene tests every shape against all shapes
+// whose x ranges overlap its own, most of them far away in z (a settled
+// 200 x 200 m pile: ~360 candidates per shape for 2.7 pairs).  Large scenes
+// are therefore swept per band of z: bands are at least as wide as the
+// widest shape's z extent, so a shape lies in one or two bands; each band's
+// entries keep the x order of the sorted endpoints, and a pair found in a
+// band counts only in the band of the larger of the two min z (a band both
+// shapes lie in, since the band index is monotone in z), which makes the
+// published pair set identical to the one-axis sweep's.
+__device__ __forceinline__ float decode_enc(uint32_t e) {
+    return __uint_as_float((e & 0x80000000u) ? (e & 0x7fffffffu) : ~e);
+}
+// Band of an encoded z bound: floor((z - z0) / width), clamped; monotone in
+// the encoded value (float subtraction and scaling by a non-negative
+// factor are monotone).
+__device__ __forceinline__ uint32_t band_of(uint32_t e, float4 par) {
+    const float t = (decode_enc(e) - par.x) * par.y;
+    if (!(t > 0.0f)) return 0u;
+    return t >= float(DevState::kBands - 1) ? DevState::kBands - 1 : uint32_t(t);
+}
+// Per block of one large scene (blockIdx.y): min z, max z and the widest z
+// extent of its shapes.
+__global__ void __launch_bounds__(256) k_band_stats(DevState s, const uint4* __restrict__ rec) {
+    const uint32_t L = blockIdx.y, begin = s.large_begin[L], n = s.large_n[L];
+    uint32_t zmin = ~0u, zmax = 0u;
+    float ext = 0.0f;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint4 r = rec[begin + k];
+        zmin = min(zmin, r.z);
+        zmax = max(zmax, r.w);
+        const float e = decode_enc(r.w) - decode_enc(r.z);
+        ext = e > ext ? e : ext;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        zmin = min(zmin, __shfl_xor_sync(0xffffffffu, zmin, o));
+        zmax = max(zmax, __shfl_xor_sync(0xffffffffu, zmax, o));
+        const float e = __shfl_xor_sync(0xffffffffu, ext, o);
+        ext = e > ext ? e : ext;
+    }
+    __shared__ uint4 part[8];
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    if (lane == 0) part[w] = make_uint4(zmin, zmax, __float_as_uint(ext), 0u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint4 r = part[0];
+        for (uint32_t k = 1; k < blockDim.x / 32u; ++k) {
+            r.x = min(r.x, part[k].x);
+            r.y = max(r.y, part[k].y);
+            r.z = __uint_as_float(part[k].z) > __uint_as_float(r.z) ? part[k].z : r.z;
+        }
+        s.bd_part[L * DevState::kBandStatBlocks + blockIdx.x] = r;
+    }
+}
+// One warp per large scene: band origin and width (the widest shape's z
+// extent with a margin, and at least 1/250 of the scene's z range).
+__global__ void k_band_params(DevState s) {
+    const uint32_t L = blockIdx.x, lane = threadIdx.x;
+    uint32_t zmin = ~0u, zmax = 0u;
+    float ext = 0.0f;
+    for (uint32_t k = lane; k < DevState::kBandStatBlocks; k += 32) {
+        const uint4 r = s.bd_part[L * DevState::kBandStatBlocks + k];
+        zmin = min(zmin, r.x);
+        zmax = max(zmax, r.y);
+        ext = __uint_as_float(r.z) > ext ? __uint_as_float(r.z) : ext;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        zmin = min(zmin, __shfl_xor_sync(0xffffffffu, zmin, o));
+        zmax = max(zmax, __shfl_xor_sync(0xffffffffu, zmax, o));
+        const float e = __shfl_xor_sync(0xffffffffu, ext, o);
+        ext = e > ext ? e : ext;
+    }
+    if (lane == 0) {
+        const float z0 = decode_enc(zmin), z1 = decode_enc(zmax);
+        float width = ext * 1.001f;
+        const float floor_w = (z1 - z0) / 250.0f;
+        if (floor_w > width) width = floor_w;
+        const bool ok = isfinite(z0) && isfinite(z1) && isfinite(width) && width > 0.0f;
+        s.bd_par[L] = make_float4(ok ? z0 : 0.0f, ok ? 1.0f / width : 0.0f, 0.0f, 0.0f);
+    }
+}
+// Bands each x-sorted finite shape of a large scene lies in (one or two).
+__global__ void k_band_count(DevState s, const uint4* __restrict__ rec) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= s.n_finite) return;
+    const int32_t L = s.sc_large[s.s_scene[s.srt_id[p]]];
+    uint32_t c = 0;
+    if (L >= 0) {
+        const float4 par = s.bd_par[L];
+        const uint4 r = rec[p];
+        const uint32_t b0 = band_of(r.z, par), b1 = band_of(r.w, par);
+        c = b1 >= b0 ? b1 - b0 + 1u : 1u;
+        if (c > 2u) {
+            // bands are wider than every extent: only non-finite bounds (an
+            // error of their own) get here
+            if (isfinite(decode_enc(r.z)) && isfinite(decode_enc(r.w))) atomicOr(s.err, kErrLogic);
+            c = 2u;
+        }
+    }
+    s.bd_cnt[p] = c;
+}
+// Band entries in x order: key (large scene << 8 | band), value the x-sorted
+// position.
+__global__ void k_band_expand(DevState s, const uint4* __restrict__ rec) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= s.n_finite) return;
+    const uint32_t c = s.bd_cnt[p];
+    if (c == 0u) return;
+    const int32_t L = s.sc_large[s.s_scene[s.srt_id[p]]];
+    const uint32_t b0 = band_of(rec[p].z, s.bd_par[L]);
+    const uint32_t q = s.bd_off[p];
+    for (uint32_t k = 0; k < c; ++k) {
+        if (q + k >= s.bx_cap) { atomicOr(s.err, kErrLogic); return; }   // never: 2 entries per shape at most
+        s.bx_key[q + k] = (uint32_t(L) << 8) | min(b0 + k, DevState::kBands - 1);
+        s.bx_val[q + k] = p;
+    }
+}
+// The band entries (sorted by key, x order within) appended to the sweep
+// list after the x-sorted finite shapes, and each band's end.
+__global__ void k_band_gather(DevState s, uint4* rec, uint2* meta) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = *s.bd_n;
+    if (q >= n) return;
+    const uint32_t key = s.bx_key[q], p = s.bx_val[q], nf = s.n_finite;
+    if (q + 1 == n || s.bx_key[q + 1] != key) s.bd_end[key] = q + 1;
+    s.srt_key[nf + q] = s.srt_key[p];
+    s.srt_id[nf + q] = s.srt_id[p];
+    rec[nf + q] = rec[p];
+    meta[nf + q] = meta[p];
+}
+
 // Gather the sweep records into sorted order: (min y, max y, min z, max z)
 // and (max x, body | dynamic << 31).
 __global__ void k_sweep_gather(DevState s, uint4* rec, uint2* meta) {
@@ -152,25 +283,40 @@ __global__ void __launch_bounds__(kSweepWarps * 32) k_sweep(DevState s, const ui
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     SweepCand* st = stage[wib];
     const uint32_t nwarps = gridDim.x * kSweepWarps;
-    const uint32_t n = s.n_finite;
+    const uint32_t nf = s.n_finite;
+    const uint32_t n = nf + (s.n_large ? *s.bd_n : 0u);
+    constexpr uint32_t kNoBand = ~0u;
     for (uint32_t base = (blockIdx.x * kSweepWarps + wib) * 32u; base < n; base += nwarps * 32u) {
         const uint32_t i = base + lane;
         const bool valid = i < n;
-        uint32_t id = 0, scene_end = 0, abody = 0;
+        uint32_t id = 0, scene_end = 0, abody = 0, band = kNoBand;
+        float4 par = make_float4(0, 0, 0, 0);
+        bool sweeps = valid;
         uint2 am = make_uint2(0, 0);
         uint4 a = make_uint4(0, 0, 0, 0);
         bool adyn = false;
         uint32_t nfound = 0;
         if (valid) {
             id = s.srt_id[i];
-            scene_end = s.sc_fbegin[s.s_scene[id] + 1];
+            if (i < nf) {
+                const uint32_t sc = s.s_scene[id];
+                scene_end = s.sc_fbegin[sc + 1];
+                // a large scene's x-sorted entries publish plane pairs only;
+                // its band entries sweep
+                if (s.n_large && s.sc_large[sc] >= 0) sweeps = false;
+            } else {
+                const uint32_t key = s.bx_key[i - nf];
+                scene_end = nf + s.bd_end[key];
+                band = key & (DevState::kBands - 1u);
+                par = s.bd_par[key >> 8];
+            }
             am = meta[i];
             a = rec[i];
             abody = am.y & 0x7fffffffu;
             adyn = (am.y >> 31) != 0u;
         }
         uint32_t* cache = s.sw_cache + size_t(i) * C;
-        bool scan = valid;
+        bool scan = sweeps;
         if (fill && valid) {
             nfound = s.sw_found[i];
             if (nfound <= C) {
@@ -203,6 +349,7 @@ __global__ void __launch_bounds__(kSweepWarps * 32) k_sweep(DevState s, const ui
                     if (!adyn && (c.body >> 31) == 0u) continue;
                     const uint4 b = c.yz;
                     if (a.x > b.y || b.x > a.y || a.z > b.w || b.z > a.w) continue;
+                    if (band != kNoBand && band_of(max(a.z, b.z), par) != band) continue;
                     if (!fill) {
                         atomicAdd(&s.own_cnt[min(id, c.id)], 1u);
                         if (found < C) cache[found] = c.id;
@@ -215,7 +362,7 @@ __global__ void __launch_bounds__(kSweepWarps * 32) k_sweep(DevState s, const ui
             __syncwarp();
         }
         if (!fill && valid) s.sw_found[i] = found;
-        if (fill && valid && adyn) {
+        if (fill && valid && i < nf && adyn) {
             const int32_t p = s.sc_plane[s.s_scene[id]];
             if (p >= 0) {
                 const uint32_t pp = uint32_t(p);
@@ -299,10 +446,23 @@ void enqueue_broadphase(const DevState& s, cudaStream_t st, const StageHook& hoo
     if (s.n_finite) {
         k_sweep_gather<<<(s.n_finite + T - 1) / T, T, 0, st>>>(s, rec, meta);
     }
+    if (s.n_large) {
+        int kbits = 0;
+        while ((1u << kbits) < s.n_large) ++kbits;
+        k_band_stats<<<dim3(DevState::kBandStatBlocks, s.n_large), 256, 0, st>>>(s, rec);
+        k_band_params<<<s.n_large, 32, 0, st>>>(s);
+        k_band_count<<<(s.n_finite + T - 1) / T, T, 0, st>>>(s, rec);
+        scan_exclusive(s.bd_cnt, s.bd_off, s.n_finite, nullptr, s.bd_n, s.scan_tmp, s.scan_tmp_words, st, s.err);
+        k_band_expand<<<(s.n_finite + T - 1) / T, T, 0, st>>>(s, rec);
+        radix_sort_pairs(s.bx_key, s.bx_val, s.bx_key2, s.bx_val2, s.bx_cap, s.bd_n, 0, 8 + kbits, s.sort_hist,
+                         s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err, 8);
+        k_band_gather<<<(s.bx_cap + T - 1) / T, T, 0, st>>>(s, rec, meta);
+    }
     cudaMemcpyAsync(s.own_cnt, s.s_static_pairs, size_t(s.n_shapes) * 4, cudaMemcpyDeviceToDevice, st);
     cudaMemsetAsync(s.own_cur, 0, size_t(s.n_shapes) * 4, st);
     const uint32_t sweep_threads = kSweepWarps * 32;
-    const uint32_t sweep_blocks = s.n_finite ? (s.n_finite + sweep_threads - 1) / sweep_threads : 0;
+    const uint32_t n_sweep = s.n_finite + s.bx_cap;
+    const uint32_t sweep_blocks = s.n_finite ? (n_sweep + sweep_threads - 1) / sweep_threads : 0;
     if (sweep_blocks) k_sweep<<<sweep_blocks, sweep_threads, 0, st>>>(s, rec, meta, 0);
     scan_exclusive(s.own_cnt, s.own_off, s.n_shapes, nullptr, s.cur.n, s.scan_tmp, s.scan_tmp_words, st, s.err);
     k_pair_total<<<1, 32, 0, st>>>(s);

@@ -1787,7 +1787,7 @@ __global__ void __launch_bounds__(kPgsThreadBlock) k_pgs_thread(DevState s) {
         for (uint32_t l = 0; l < nb; ++l) { sdv[l] = zero; sdw[l] = zero; }
         for (int it = 0; it < pos + vel; ++it) {
             for (uint32_t i = begin; i < end; ++i)
-                solve_desc<LocalDeltas, false>(s, s.d_val2[i], s.d_lbod[i], it, pos, vel, D);
+                solve_desc<LocalDeltas>(s, s.d_val2[i], s.d_lbod[i], it, pos, vel, D);
             if (it + 1 == pos) island_deltas_out(s.sb_mdv, s.sb_mdw, ib, nb, sdv, sdw, 0u, 1u);
         }
         island_deltas_out(s.sb_dv, s.sb_dw, ib, nb, sdv, sdw, 0u, 1u);
@@ -1843,7 +1843,7 @@ __global__ void __launch_bounds__(kPgsWarpsPerBlock * 32, 3) k_pgs_warp(DevState
             for (uint32_t l = 0; l < nlev; ++l) {
                 const uint32_t lb = sb[l], le = sb[l + 1];
                 for (uint32_t i = lb + lane; i < le; i += 32)
-                    solve_slot<LocalDeltas, false>(s, sd[i], sl[i], it, pos, vel, D, begin + i);
+                    solve_slot<LocalDeltas>(s, sd[i], sl[i], it, pos, vel, D, begin + i);
                 __syncwarp();
             }
             if (it + 1 == pos) {

@@ -194,6 +194,22 @@ struct DevState {
     static constexpr int kMaxLarge = 64;
     uint32_t n_large = 0;
     uint32_t large_begin[kMaxLarge] = {}, large_n[kMaxLarge] = {};
+    // Large scenes are swept in bands of z (every shape in each band its z
+    // extent touches, a pair kept in the one band holding the larger of the
+    // two min z).  The sweep list is the x-sorted list of every finite shape
+    // (large scenes' entries only publish their plane pairs) followed by the
+    // large scenes' band entries, sorted by (scene, band) and x within.
+    static constexpr uint32_t kBands = 256, kBandStatBlocks = 148;
+    int32_t* sc_large = nullptr;       // per scene: large-scene index or -1
+    uint4* bd_part = nullptr;          // kMaxLarge x kBandStatBlocks: min z, max z (encoded), max z extent bits
+    float4* bd_par = nullptr;          // per large scene: z origin, 1 / band width
+    uint32_t* bd_cnt = nullptr;        // per x-sorted finite shape: bands spanned (0 in small scenes)
+    uint32_t* bd_off = nullptr;
+    uint32_t* bd_n = nullptr;          // band entries this step
+    uint32_t* bd_end = nullptr;        // kMaxLarge x kBands: end of each band's entries (entry index)
+    uint32_t *bx_key = nullptr, *bx_val = nullptr, *bx_key2 = nullptr, *bx_val2 = nullptr;
+    uint32_t* bx_seg = nullptr;        // per band entry: end of its band in the sweep list
+    uint32_t bx_cap = 0;               // band entries at most (2 per large-scene shape)
 
     // scratch for scans / sorts
     uint32_t* scan_tmp = nullptr;

@@ -1815,7 +1815,7 @@ private:
         dalloc(d_.tmp_flags, cap, pair_owned_);
         dalloc(d_.tmp_pos, std::max(cap, dc), pair_owned_);
         dalloc(d_.lvl_bound, 2 * size_t(dc) + 2, pair_owned_);
-        const uint32_t big = std::max({cap, dc, d_.n_shapes, d_.n_finite, 256u * 64u});
+        const uint32_t big = std::max({cap, dc, d_.n_shapes, d_.n_finite, d_.bx_cap, 256u * 64u});
         d_.scan_tmp_words = scan_tmp_words_for(std::max<uint32_t>(big, uint32_t(radix_hist_words(big))));
         dalloc(d_.scan_tmp, d_.scan_tmp_words, pair_owned_);
         check_cuda(cudaMemsetAsync(d_.scan_tmp, 0, d_.scan_tmp_words * 4, stream_), "memset");   // scan epochs start clear
@@ -2047,18 +2047,23 @@ private:
         d.n_finite = nf;
         h_fbegin_ = fbegin;
         std::vector<uint32_t> small;
+        std::vector<int32_t> sc_large(nsc, -1);
         d.n_large = 0;
+        uint64_t large_items = 0;
         for (uint32_t sc = 0; sc < nsc; ++sc) {
             const uint32_t n = fbegin[sc + 1] - fbegin[sc];
             if (n == 0) continue;
             if (n <= d.max_small_scene) small.push_back(sc);
             else {
                 if (d.n_large >= DevState::kMaxLarge) throw std::logic_error("Too many scenes above the per-CTA sort size");
+                sc_large[sc] = int32_t(d.n_large);
                 d.large_begin[d.n_large] = fbegin[sc];
                 d.large_n[d.n_large] = n;
                 ++d.n_large;
+                large_items += n;
             }
         }
+        d.bx_cap = uint32_t(2 * large_items);   // a shape lies in at most two z bands
         d.n_small = uint32_t(small.size());
         tuning_class_ = d.n_large ? "large_scene" : "many_scenes";
         if (!tuning_explicit_) {
@@ -2099,11 +2104,22 @@ private:
         dalloc(d_.s_mat, ns, owned_); dalloc(d_.s_wp, ns, owned_); dalloc(d_.s_wq, ns, owned_);
         dalloc(d_.s_lo, ns, owned_); dalloc(d_.s_hi, ns, owned_);
         dalloc(d_.s_frank, ns, owned_); dalloc(d_.s_dynrank, ns, owned_); dalloc(d_.s_static_pairs, ns, owned_);
-        dalloc(d_.srt_key, nf, owned_); dalloc(d_.srt_id, nf, owned_);
+        // the sweep list: x-sorted finite shapes, then the large scenes' z-band entries
+        const size_t nsw = size_t(nf) + d_.bx_cap;
+        dalloc(d_.srt_key, nsw, owned_); dalloc(d_.srt_id, nsw, owned_);
         dalloc(d_.srt_key2, nf, owned_); dalloc(d_.srt_id2, nf, owned_);
-        dalloc(d_.sw_rec, nf, owned_); dalloc(d_.sw_meta, nf, owned_);
-        dalloc(d_.sw_cache, size_t(nf) * DevState::kSweepCache, owned_);
-        dalloc(d_.sw_found, nf, owned_);
+        dalloc(d_.sw_rec, nsw, owned_); dalloc(d_.sw_meta, nsw, owned_);
+        dalloc(d_.sw_cache, nsw * DevState::kSweepCache, owned_);
+        dalloc(d_.sw_found, nsw, owned_);
+        dalloc(d_.sc_large, nsc, owned_);
+        if (d_.n_large) {
+            dalloc(d_.bd_part, size_t(d_.n_large) * DevState::kBandStatBlocks, owned_);
+            dalloc(d_.bd_par, d_.n_large, owned_);
+            dalloc(d_.bd_cnt, nf, owned_); dalloc(d_.bd_off, nf, owned_); dalloc(d_.bd_n, 1, owned_);
+            dalloc(d_.bd_end, size_t(d_.n_large) * DevState::kBands, owned_);
+            dalloc(d_.bx_key, d_.bx_cap, owned_); dalloc(d_.bx_val, d_.bx_cap, owned_);
+            dalloc(d_.bx_key2, d_.bx_cap, owned_); dalloc(d_.bx_val2, d_.bx_cap, owned_);
+        }
         dalloc(d_.own_cnt, ns, owned_); dalloc(d_.own_off, ns, owned_); dalloc(d_.own_cur, ns, owned_);
         dalloc(d_.sb_dv, nb, owned_); dalloc(d_.sb_dw, nb, owned_); dalloc(d_.sb_mdv, nb, owned_);
         dalloc(d_.sb_mdw, nb, owned_); dalloc(d_.sb_v, nb, owned_); dalloc(d_.sb_w, nb, owned_);
@@ -2167,6 +2183,7 @@ private:
         upload(d_.hfr, hfr, stream_); upload(d_.hidx, hidx, stream_);
         upload_joints();
         upload(d_.sc_fbegin, fbegin, stream_); upload(d_.sc_plane, plane, stream_);
+        upload(d_.sc_large, sc_large, stream_);
         upload(d_.small_scenes, small, stream_);
         upload(d_.b_dyn0, dyn0, stream_); upload(d_.b_dyn1, dyn1, stream_);
         upload(d_.b_flags, flags, stream_); upload(d_.b_scene, bscene, stream_);
