@@ -441,7 +441,7 @@ void enqueue_broadphase(const DevState& s, cudaStream_t st, const StageHook& hoo
     for (uint32_t i = 0; i < s.n_large; ++i)
         radix_sort_pairs(s.srt_key + s.large_begin[i], s.srt_id + s.large_begin[i],
                          s.srt_key2, s.srt_id2, s.large_n[i], nullptr, 0, 32,
-                         s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err, s.radix_bits);
+                         s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err, s.radix_bits, s.sort_os, s.sort_os_words);
     hook(kStPairs, st);
     if (s.n_finite) {
         k_sweep_gather<<<(s.n_finite + T - 1) / T, T, 0, st>>>(s, rec, meta);
@@ -455,7 +455,7 @@ void enqueue_broadphase(const DevState& s, cudaStream_t st, const StageHook& hoo
         scan_exclusive(s.bd_cnt, s.bd_off, s.n_finite, nullptr, s.bd_n, s.scan_tmp, s.scan_tmp_words, st, s.err);
         k_band_expand<<<(s.n_finite + T - 1) / T, T, 0, st>>>(s, rec);
         radix_sort_pairs(s.bx_key, s.bx_val, s.bx_key2, s.bx_val2, s.bx_cap, s.bd_n, 0, 8 + kbits, s.sort_hist,
-                         s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err, 8);
+                         s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err, 8, s.sort_os, s.sort_os_words);
         k_band_gather<<<(s.bx_cap + T - 1) / T, T, 0, st>>>(s, rec, meta);
     }
     cudaMemcpyAsync(s.own_cnt, s.s_static_pairs, size_t(s.n_shapes) * 4, cudaMemcpyDeviceToDevice, st);

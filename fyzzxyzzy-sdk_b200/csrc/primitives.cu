@@ -9,8 +9,14 @@
 // they need no reset between scans; every wait is bounded and reports
 // kErrLogic instead of hanging.
 //
-// The radix sort processes digits of 8 to 11 bits (a runtime choice: wider
-// digits mean fewer passes, larger histograms).  Each pass is three launches:
+// The radix sort with 8-bit digits is a one-sweep LSD sort (Adinets and
+// Merrill, "Onesweep: A Faster Least Significant Digit Radix Sort for
+// GPUs", 2022): one launch counts the digits of every pass at once, then
+// each pass is one launch whose tiles (taken in ticket order) rank their
+// keys, publish their digit counts and find the counts of the tiles before
+// them by the same bounded, epoch-tagged look-back as the scan.  Other
+// digit widths (9 to 11 bits: fewer passes, larger histograms) run three
+// launches per pass:
 //   histogram  per 2048-key tile, 2^B bins in shared memory
 //   scan       exclusive scan of the digit-major histogram (tile order
 //              inside a digit preserves stability)
@@ -70,6 +76,11 @@ __device__ __forceinline__ unsigned long long scan_state_load(const unsigned lon
 }
 __device__ __forceinline__ void scan_state_store(unsigned long long* p, unsigned long long v) {
     asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+// A one-sweep digit state carries all its data in the word: no ordering
+// against other stores is needed.
+__device__ __forceinline__ void os_state_store(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 __global__ void __launch_bounds__(kScanThreads) k_scan_lookback(const uint32_t* in, uint32_t* out, uint32_t n,
                                                                const uint32_t* n_dev, uint32_t* total,
@@ -225,12 +236,155 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const uint32_t* 
     }
     __syncthreads();
     const uint32_t* wo = wofs + warp * (R + 1);
+    // offsets from a scan that gave up a wait are unknown: nothing lands
+    // outside the output (the scan reported the error)
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
         if (dig[r] < R) {
             const uint32_t pos = offs[dig[r] * ntiles + blockIdx.x] + wo[dig[r]] + rank[r];
-            kout[pos] = key[r];
-            vout[pos] = val[r];
+            if (pos < lim) {
+                kout[pos] = key[r];
+                vout[pos] = val[r];
+            }
+        }
+    }
+}
+
+// ---- one-sweep passes (8-bit digits) ----
+// Scratch (zeroed when allocated): [0] epoch, [1] tile ticket, [2] finished
+// blocks, [3] pad, then kOsMaxPasses x 256 digit totals, then one 64-bit
+// state per tile and digit: epoch (30 bits) | status (2 bits: 1 count of
+// the tile, 2 inclusive count) | value (32 bits).
+constexpr int kOsMaxPasses = 4;
+constexpr uint32_t kOsHeader = 4, kOsHist = kOsMaxPasses * 256;
+constexpr int kOsLook = 8;   // predecessors read together in the look-back
+
+// Digit totals of every pass (ghist must be zero).
+__global__ void __launch_bounds__(kSortThreads) k_os_hist(const uint32_t* __restrict__ keys, uint32_t n,
+                                                         const uint32_t* n_dev, int begin_bit, int passes,
+                                                         uint32_t* ghist) {
+    __shared__ uint32_t h[kOsHist];
+    for (int i = threadIdx.x; i < passes * 256; i += kSortThreads) h[i] = 0u;
+    __syncthreads();
+    const uint32_t lim = n_dev ? min(n, *n_dev) : n;
+    for (uint32_t idx = blockIdx.x * kSortThreads + threadIdx.x; idx < lim; idx += gridDim.x * kSortThreads) {
+        const uint32_t k = keys[idx];
+        for (int p = 0; p < passes; ++p) atomicAdd(&h[p * 256 + ((k >> (begin_bit + 8 * p)) & 255u)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += kSortThreads)
+        if (h[i]) atomicAdd(&ghist[i], h[i]);
+}
+
+// One pass: ranks a tile's keys by digit (stable), then places them at the
+// digit's global offset + the counts of the digit in earlier tiles + the
+// rank.
+__global__ void __launch_bounds__(kSortThreads) k_os_scatter(const uint32_t* __restrict__ kin,
+                                                            const uint32_t* __restrict__ vin,
+                                                            uint32_t* __restrict__ kout,
+                                                            uint32_t* __restrict__ vout, uint32_t n,
+                                                            const uint32_t* n_dev, int shift,
+                                                            const uint32_t* __restrict__ ghist, uint32_t* ctl,
+                                                            unsigned long long* state, uint32_t* err) {
+    constexpr uint32_t R = 256;
+    __shared__ uint32_t wcount[kSortWarps][R + 1];
+    __shared__ uint32_t wofs[kSortWarps][R + 1];
+    __shared__ uint32_t base_d[R];
+    __shared__ uint32_t sm_scan[kSortThreads / 32 + 1];
+    __shared__ uint32_t s_tile;
+    // blocks beyond the live tiles leave before taking a ticket
+    const uint32_t lim = n_dev ? min(n, *n_dev) : n;
+    const uint32_t live = uint32_t((uint64_t(lim) + kSortTile - 1) / kSortTile);
+    if (blockIdx.x >= live) return;
+    const uint32_t epoch = *reinterpret_cast<volatile uint32_t*>(&ctl[0]) & 0x3fffffffu;
+    const unsigned long long tag = (unsigned long long)epoch << 34;
+    if (threadIdx.x == 0) s_tile = atomicAdd(&ctl[1], 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (uint32_t i = threadIdx.x; i < kSortWarps * (R + 1); i += kSortThreads) (&wcount[0][0])[i] = 0u;
+        __syncthreads();
+        const uint32_t wbase = tile * kSortTile + warp * 32 * kSortItems;
+        uint32_t key[kSortItems], val[kSortItems], dig[kSortItems], rank[kSortItems];
+        const uint32_t lt = (1u << lane) - 1u;
+        uint32_t* wc = wcount[warp];
+#pragma unroll
+        for (int r = 0; r < kSortItems; ++r) {
+            const uint32_t idx = wbase + r * 32 + lane;
+            const bool valid = idx < lim;
+            key[r] = valid ? kin[idx] : 0u;
+            val[r] = valid ? vin[idx] : 0u;
+            dig[r] = valid ? ((key[r] >> shift) & (R - 1u)) : R;
+            const uint32_t peers = __match_any_sync(0xffffffffu, dig[r]);
+            const int leader = __ffs(peers) - 1;
+            const uint32_t base = wc[dig[r]];
+            __syncwarp();
+            if (lane == leader) wc[dig[r]] = base + __popc(peers);
+            __syncwarp();
+            rank[r] = base + __popc(peers & lt);
+        }
+        __syncthreads();
+        // thread d: digit d's warp offsets, tile count, global offset
+        const uint32_t d = threadIdx.x;
+        uint32_t cnt = 0;
+        for (int w = 0; w < kSortWarps; ++w) {
+            wofs[w][d] = cnt;
+            cnt += wcount[w][d];
+        }
+        uint32_t gx;
+        block_excl_scan<kSortThreads>(ghist[d], gx, sm_scan);
+        unsigned long long* my = state + size_t(tile) * R + d;
+        os_state_store(my, tag | ((tile == 0 ? 2ull : 1ull) << 32) | cnt);
+        // look-back over kOsLook predecessors at a time (their loads in
+        // flight together): sum tile counts until an inclusive count
+        uint32_t prefix = 0;
+        bool failed = false, found = tile == 0;
+        for (int64_t look = int64_t(tile) - 1; !found && !failed; look -= kOsLook) {
+            unsigned long long st[kOsLook];
+#pragma unroll
+            for (int k = 0; k < kOsLook; ++k)
+                st[k] = look - k >= 0 ? scan_state_load(state + size_t(look - k) * R + d) : (tag | (2ull << 32));
+#pragma unroll
+            for (int k = 0; k < kOsLook; ++k) {
+                if (found || failed) break;
+                uint32_t spins = 0;
+                while (!((st[k] >> 34) == epoch && ((st[k] >> 32) & 3u) != 0u)) {
+                    if (++spins == kLookbackSpin) { failed = true; break; }
+                    st[k] = scan_state_load(state + size_t(look - k) * R + d);
+                }
+                if (failed) break;
+                prefix += uint32_t(st[k]);
+                found = ((st[k] >> 32) & 3u) == 2u;
+            }
+        }
+        if (failed && err) atomicOr(err, kErrLogic);
+        if (tile != 0) os_state_store(my, tag | (2ull << 32) | (prefix + cnt));
+        base_d[d] = gx + prefix;
+        __syncthreads();
+        // a look-back that gave up leaves the offsets unknown: the step
+        // reports the error and nothing lands outside the output
+#pragma unroll
+        for (int r = 0; r < kSortItems; ++r) {
+            if (dig[r] < R) {
+                const uint32_t pos = base_d[dig[r]] + wofs[warp][dig[r]] + rank[r];
+                if (pos < lim) {
+                    kout[pos] = key[r];
+                    vout[pos] = val[r];
+                } else if (err) {
+                    atomicOr(err, kErrLogic);
+                }
+            }
+        }
+    }
+    // the last live block to finish opens the next epoch and resets the ticket
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&ctl[2], 1u) == live - 1) {
+            ctl[0] = (epoch + 1u) & 0x3fffffffu;
+            ctl[1] = 0u;
+            ctl[2] = 0u;
+            __threadfence();
         }
     }
 }
@@ -267,6 +421,11 @@ void scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, const uint32_
     k_scan_lookback<<<nb < 296u ? nb : 296u, kScanThreads, 0, st>>>(in, out, n, n_dev, total, tmp, err);
 }
 
+size_t onesweep_words(uint32_t n_cap) {
+    const size_t ntiles = (size_t(n_cap) + kSortTile - 1) / kSortTile;
+    return kOsHeader + kOsHist + 2 * 256 * ntiles;
+}
+
 size_t radix_hist_words(uint32_t n_cap) {
     const uint32_t ntiles = (n_cap + kSortTile - 1) / kSortTile;
     return (size_t(1) << kRadixMaxBits) * ntiles + 1;
@@ -283,10 +442,34 @@ void init_primitive_kernels() {
 void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
                       uint32_t n_cap, const uint32_t* n_dev, int begin_bit, int end_bit,
                       uint32_t* hist, size_t hist_words, uint32_t* scan_tmp, size_t scan_words,
-                      cudaStream_t st, uint32_t* err, int digit_bits) {
+                      cudaStream_t st, uint32_t* err, int digit_bits, uint32_t* os_scratch, size_t os_words) {
     const uint32_t ntiles = (n_cap + kSortTile - 1) / kSortTile;
     if (ntiles == 0) return;
     const int B = digit_bits >= 8 && digit_bits <= kRadixMaxBits ? digit_bits : 8;
+    const int os_passes = (end_bit - begin_bit + 7) / 8;
+    if (B == 8 && os_scratch && os_passes <= kOsMaxPasses) {
+        if (onesweep_words(n_cap) > os_words) {   // never: the world sizes the scratch for its largest sort
+            if (err) cudaMemsetAsync(err, 0xff, 4, st);
+            return;
+        }
+        uint32_t* ghist = os_scratch + kOsHeader;
+        auto* state = reinterpret_cast<unsigned long long*>(os_scratch + kOsHeader + kOsHist);
+        cudaMemsetAsync(ghist, 0, size_t(os_passes) * 256 * 4, st);
+        k_os_hist<<<ntiles < 296u ? ntiles : 296u, kSortThreads, 0, st>>>(keys, n_cap, n_dev, begin_bit, os_passes,
+                                                                          ghist);
+        uint32_t *ki = keys, *vi = vals, *ko = keys_alt, *vo = vals_alt;
+        for (int p = 0; p < os_passes; ++p) {
+            k_os_scatter<<<ntiles, kSortThreads, 0, st>>>(ki, vi, ko, vo, n_cap, n_dev, begin_bit + 8 * p,
+                                                           ghist + 256 * p, os_scratch, state, err);
+            uint32_t* t = ki; ki = ko; ko = t;
+            t = vi; vi = vo; vo = t;
+        }
+        if (os_passes & 1) {
+            cudaMemcpyAsync(keys, ki, size_t(n_cap) * 4, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(vals, vi, size_t(n_cap) * 4, cudaMemcpyDeviceToDevice, st);
+        }
+        return;
+    }
     if ((size_t(1) << B) * ntiles > hist_words) {   // never: the world sizes the histogram for the widest digit
         if (err) cudaMemsetAsync(err, 0xff, 4, st);
         return;

@@ -2217,14 +2217,14 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
         while ((1ull << rbits) < uint64_t(s.n_joints) + 2ull * s.pair_cap + 1u) ++rbits;
         k_replay_keys<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
         radix_sort_pairs(s.d_key, s.d_val, s.d_key2, s.d_val2, s.desc_cap, s.counters + kCntDesc, 0, rbits,
-                         s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err, s.radix_bits);
+                         s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err, s.radix_bits, s.sort_os, s.sort_os_words);
         k_replay_rekey<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     }
     // keys are island roots < n_bodies, or n_bodies for sleeping islands
     int bits = 1;
     while ((1ull << bits) < uint64_t(s.n_bodies) + 1u) ++bits;
     radix_sort_pairs(s.d_key, s.d_val, s.d_key2, s.d_val2, s.desc_cap, s.counters + kCntDesc, 0, bits,
-                     s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err, s.radix_bits);
+                     s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err, s.radix_bits, s.sort_os, s.sort_os_words);
     k_island_flags<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     scan_exclusive(s.isl_flag, pos, s.desc_cap, s.counters + kCntAwake, s.n_isl, s.scan_tmp, s.scan_tmp_words, st,
                    s.err);

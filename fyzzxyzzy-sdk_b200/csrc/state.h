@@ -214,6 +214,8 @@ struct DevState {
     // scratch for scans / sorts
     uint32_t* scan_tmp = nullptr;
     size_t scan_tmp_words = 0;
+    uint32_t* sort_os = nullptr;       // one-sweep radix passes (onesweep_words)
+    size_t sort_os_words = 0;
     uint32_t* sort_hist = nullptr;
     size_t sort_hist_words = 0;
     // Impulse tape of a differentiated step (null otherwise): the applied
@@ -264,9 +266,12 @@ void scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, const uint32_
 void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
                       uint32_t n_cap, const uint32_t* n_dev, int begin_bit, int end_bit,
                       uint32_t* hist, size_t hist_words, uint32_t* scan_tmp, size_t scan_words,
-                      cudaStream_t st, uint32_t* err = nullptr, int digit_bits = 8);
+                      cudaStream_t st, uint32_t* err = nullptr, int digit_bits = 8,
+                      uint32_t* os_scratch = nullptr, size_t os_words = 0);
 constexpr int kRadixMaxBits = 11;   // widest radix digit
 size_t radix_hist_words(uint32_t n_cap);
+// One-sweep scratch of radix_sort_pairs (8-bit digits); zero when allocated.
+size_t onesweep_words(uint32_t n_cap);
 void init_primitive_kernels();
 size_t scan_tmp_words_for(uint32_t n_cap);
 

@@ -229,11 +229,11 @@ void enqueue_thresholds(const DevState& s, cudaStream_t st) {
     // stable LSD sorts: by actor1, then by (actor0, static world)
     radix_sort_pairs(s.th_k, s.th_v, s.th_k2, s.th_v2, s.pair_cap, s.counters + kCntThRows, 0,
                      th_bits(s.n_bodies), s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err,
-                     s.radix_bits);
+                     s.radix_bits, s.sort_os, s.sort_os_words);
     k_th_gather_hi<<<g, T, 0, st>>>(s);
     radix_sort_pairs(s.th_k, s.th_v, s.th_k2, s.th_v2, s.pair_cap, s.counters + kCntThRows, 0,
                      th_bits(2ull * s.n_bodies + 1), s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words,
-                     st, s.err, s.radix_bits);
+                     st, s.err, s.radix_bits, s.sort_os, s.sort_os_words);
     k_th_aggregate<<<g, T, 0, st>>>(s, s.th_f0);
     scan_exclusive(s.th_f0, s.th_p0, s.pair_cap, s.counters + kCntThRows, s.th_cur.n, s.scan_tmp,
                    s.scan_tmp_words, st, s.err);

@@ -1821,6 +1821,9 @@ private:
         check_cuda(cudaMemsetAsync(d_.scan_tmp, 0, d_.scan_tmp_words * 4, stream_), "memset");   // scan epochs start clear
         d_.sort_hist_words = radix_hist_words(big);
         dalloc(d_.sort_hist, d_.sort_hist_words, pair_owned_);
+        d_.sort_os_words = onesweep_words(big);
+        dalloc(d_.sort_os, d_.sort_os_words, pair_owned_);
+        check_cuda(cudaMemsetAsync(d_.sort_os, 0, d_.sort_os_words * 4, stream_), "memset");   // epochs start clear
         if (notify_) alloc_events();
         if (d_.thresholds) alloc_threshold_arrays();
     }
