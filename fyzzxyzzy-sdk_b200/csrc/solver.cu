@@ -408,7 +408,10 @@ __global__ void k_sleep_wake_flags(DevState s) {
     if (s.counters[kCntReady] == 0u) return;
     const uint32_t bits = ((f & kReady) && !(act & kActKinematic) ? 0u : kRootUnready) |
                           ((f & kSleeping) ? 0u : kRootAwake);
-    if (bits) atomicOr(&s.sl_root[root], bits);
+    // the bits only accumulate: once a root holds them, the thousands of
+    // bodies of a large island skip the atomic on its one word
+    if (bits && (*reinterpret_cast<volatile uint32_t*>(&s.sl_root[root]) & bits) != bits)
+        atomicOr(&s.sl_root[root], bits);
 }
 __global__ void k_sleep_decide(DevState s) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
