@@ -1202,10 +1202,13 @@ __global__ void __launch_bounds__(128) k_narrowphase(DevState s) {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
         const int32_t pj = s.prev_idx[k];
-        PcmCache cache;
-        if (pj >= 0) cache = s.prev.cache[pj];
-        else cache.meta = 0u;
         const PairShapes ps = pair_shapes(s, s.cur.key[k]);
+        // only box and hull manifolds are persistent (PCM): sphere pairs
+        // neither read nor carry a cache (their slot is never consumed)
+        const bool pcm = !ps.sphere;
+        PcmCache cache;
+        if (pcm && pj >= 0) cache = s.prev.cache[pj];
+        else cache.meta = 0u;
         if (ps.convex) {
             // carried forward here, generated by k_narrowphase_convex
             s.cur.cache[k] = cache;
@@ -1248,7 +1251,7 @@ __global__ void __launch_bounds__(128) k_narrowphase(DevState s) {
             atomicOr(s.err, kErrContactOverflow);
             count = 0;
         }
-        s.cur.cache[k] = cache;
+        if (pcm) s.cur.cache[k] = cache;
         s.cur.count[k] = uint32_t(count);
         for (int i = 0; i < count; ++i) s.pts[4 * size_t(k) + i] = out[i];
         // friction histories are not carried here: row preparation reads a
