@@ -403,25 +403,51 @@ __global__ void k_pair_total(DevState s) {
     }
 }
 
-__device__ __forceinline__ int32_t find_key(const uint64_t* keys, uint32_t n, uint64_t key) {
-    uint32_t lo = 0, hi = n;
+__device__ __forceinline__ int32_t find_key(const uint64_t* keys, uint32_t lo, uint32_t hi, uint64_t key) {
+    const uint32_t end = hi;
     while (lo < hi) {
         const uint32_t mid = (lo + hi) >> 1;
         if (keys[mid] < key) lo = mid + 1; else hi = mid;
     }
-    return (lo < n && keys[lo] == key) ? int32_t(lo) : -1;
+    return (lo < end && keys[lo] == key) ? int32_t(lo) : -1;
 }
 
+// Each generation's keys are sorted by (owner, partner), owners being
+// contiguous buckets: the previous generation's bucket of every owner
+// (start, end; both zero for an owner without pairs), so that matching
+// searches a handful of keys instead of the whole list.
+__global__ void k_prev_buckets(DevState s) {
+    const uint32_t np = *s.prev.n;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < np; j += stride) {
+        const uint32_t a = uint32_t(s.prev.key[j] >> 32);
+        if (a >= s.n_shapes) continue;
+        if (j == 0 || uint32_t(s.prev.key[j - 1] >> 32) != a) s.prev_bkt[a].x = j;
+        if (j + 1 == np || uint32_t(s.prev.key[j + 1] >> 32) != a) s.prev_bkt[a].y = j + 1;
+    }
+}
+
+// Found and lost by matching the two generations bucket by bucket: a
+// current pair's owner bucket in the previous keys, a previous pair's in
+// the current ones (own_off / own_cnt of this step's sweep).
 __global__ void k_pair_match(DevState s) {
     const uint32_t n = *s.cur.n, np = *s.prev.n;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-        const int32_t j = find_key(s.prev.key, np, s.cur.key[k]);
+        const uint64_t key = s.cur.key[k];
+        const uint32_t a = uint32_t(key >> 32);
+        const uint2 b = a < s.n_shapes ? s.prev_bkt[a] : make_uint2(0u, 0u);
+        const int32_t j = find_key(s.prev.key, b.x, min(b.y, np), key);
         s.prev_idx[k] = j;
         s.found_flag[k] = j < 0 ? 1u : 0u;
     }
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += stride)
-        s.lost_flag[k] = find_key(s.cur.key, n, s.prev.key[k]) < 0 ? 1u : 0u;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += stride) {
+        const uint64_t key = s.prev.key[k];
+        const uint32_t a = uint32_t(key >> 32);
+        const uint32_t lo = a < s.n_shapes ? min(s.own_off[a], n) : 0u;
+        const uint32_t hi = a < s.n_shapes ? min(s.own_off[a] + s.own_cnt[a], n) : 0u;
+        s.lost_flag[k] = find_key(s.cur.key, lo, hi, key) < 0 ? 1u : 0u;
+    }
 }
 
 }  // namespace
@@ -469,6 +495,8 @@ void enqueue_broadphase(const DevState& s, cudaStream_t st, const StageHook& hoo
     if (sweep_blocks) k_sweep<<<sweep_blocks, sweep_threads, 0, st>>>(s, rec, meta, 1);
     k_owner_sort<<<(s.n_shapes + T - 1) / T, T, 0, st>>>(s);
     const uint32_t mb = (s.pair_cap + T - 1) / T;
+    cudaMemsetAsync(s.prev_bkt, 0, size_t(s.n_shapes) * sizeof(uint2), st);
+    k_prev_buckets<<<mb < 1184 ? mb : 1184, T, 0, st>>>(s);
     k_pair_match<<<mb < 1184 ? mb : 1184, T, 0, st>>>(s);
 }
 

@@ -97,12 +97,15 @@ __device__ __forceinline__ float4 stq(qt q) { return make_float4(q.x, q.y, q.z, 
 // carried from frame to frame by pair identity.
 // PcmPersistentContact / PcmManifoldCache (scene.h:1444-1459).
 struct PcmPoint { float la[3], lb[3], nb[3], sep; };
-struct alignas(16) PcmCache {
+// 256 bytes: a record is whole 32-byte sectors, so pairs that skip their
+// cache (sphere pairs) leave no partly written sector beside a neighbour's.
+struct alignas(32) PcmCache {
     PcmPoint pts[4];
     float rel_p[3], rel_q[4], qa[4], qb[4];
     uint32_t meta;  // bits 0-7 count, bit 8 initialized
+    uint32_t pad[8];
 };
-static_assert(sizeof(PcmCache) == 224, "PcmCache layout");
+static_assert(sizeof(PcmCache) == 256, "PcmCache layout");
 // One retained friction patch (FrictionPatch, scene.h:1588-1614) plus the
 // epoch of the step that prepared it (friction_by_edge_, scene.cpp:8082).
 struct alignas(16) FrictionHist {

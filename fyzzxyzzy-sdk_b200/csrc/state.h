@@ -114,6 +114,7 @@ struct DevState {
     uint32_t *srt_key = nullptr, *srt_id = nullptr;      // sorted min-x endpoints
     uint32_t *srt_key2 = nullptr, *srt_id2 = nullptr;
     uint32_t *own_cnt = nullptr, *own_off = nullptr, *own_cur = nullptr;
+    uint2* prev_bkt = nullptr;         // per shape: its bucket in the previous generation's keys
     ManagerSet cur, prev;
     int32_t* prev_idx = nullptr;
     uint32_t* found_flag = nullptr;    // per current pair

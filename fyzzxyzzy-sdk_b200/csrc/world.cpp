@@ -2124,6 +2124,7 @@ private:
             dalloc(d_.bx_key2, d_.bx_cap, owned_); dalloc(d_.bx_val2, d_.bx_cap, owned_);
         }
         dalloc(d_.own_cnt, ns, owned_); dalloc(d_.own_off, ns, owned_); dalloc(d_.own_cur, ns, owned_);
+        dalloc(d_.prev_bkt, ns, owned_);
         dalloc(d_.sb_dv, nb, owned_); dalloc(d_.sb_dw, nb, owned_); dalloc(d_.sb_mdv, nb, owned_);
         dalloc(d_.sb_mdw, nb, owned_); dalloc(d_.sb_v, nb, owned_); dalloc(d_.sb_w, nb, owned_);
         dalloc(d_.sb_sqrt_i, size_t(nb) * 3, owned_);
