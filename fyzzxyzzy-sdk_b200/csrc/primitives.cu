@@ -9,9 +9,10 @@
 // they need no reset between scans; every wait is bounded and reports
 // kErrLogic instead of hanging.
 //
-// The radix sort with 8-bit digits is a one-sweep LSD sort (Adinets and
-// Merrill, "Onesweep: A Faster Least Significant Digit Radix Sort for
-// GPUs", 2022): one launch counts the digits of every pass at once, then
+// The radix sort with 8-bit digits (the default) is a one-sweep LSD sort
+// (Adinets and Merrill, "Onesweep: A Faster Least Significant Digit Radix
+// Sort for GPUs", 2022), in 8- or 9-bit digits, whichever needs fewer
+// passes: one launch counts the digits of every pass at once, then
 // each pass is one launch whose tiles (taken in ticket order) rank their
 // keys, publish their digit counts and find the counts of the tiles before
 // them by the same bounded, epoch-tagged look-back as the scan.  Other
@@ -250,35 +251,38 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const uint32_t* 
     }
 }
 
-// ---- one-sweep passes (8-bit digits) ----
+// ---- one-sweep passes (8- or 9-bit digits) ----
 // Scratch (zeroed when allocated): [0] epoch, [1] tile ticket, [2] finished
-// blocks, [3] pad, then kOsMaxPasses x 256 digit totals, then one 64-bit
-// state per tile and digit: epoch (30 bits) | status (2 bits: 1 count of
-// the tile, 2 inclusive count) | value (32 bits).
-constexpr int kOsMaxPasses = 4;
-constexpr uint32_t kOsHeader = 4, kOsHist = kOsMaxPasses * 256;
+// blocks, [3] pad, then kOsMaxPasses x 512 digit totals, then one 64-bit
+// state per tile and digit (512 a tile): epoch (30 bits) | status (2 bits:
+// 1 count of the tile, 2 inclusive count) | value (32 bits).
+constexpr int kOsMaxPasses = 4, kOsMaxDigits = 512;
+constexpr uint32_t kOsHeader = 4, kOsHist = kOsMaxPasses * kOsMaxDigits;
 constexpr int kOsLook = 8;   // predecessors read together in the look-back
 
 // Digit totals of every pass (ghist must be zero).
+template <int B>
 __global__ void __launch_bounds__(kSortThreads) k_os_hist(const uint32_t* __restrict__ keys, uint32_t n,
                                                          const uint32_t* n_dev, int begin_bit, int passes,
                                                          uint32_t* ghist) {
-    __shared__ uint32_t h[kOsHist];
-    for (int i = threadIdx.x; i < passes * 256; i += kSortThreads) h[i] = 0u;
+    constexpr uint32_t R = 1u << B;
+    __shared__ uint32_t h[kOsMaxPasses * R];
+    for (int i = threadIdx.x; i < passes * int(R); i += kSortThreads) h[i] = 0u;
     __syncthreads();
     const uint32_t lim = n_dev ? min(n, *n_dev) : n;
     for (uint32_t idx = blockIdx.x * kSortThreads + threadIdx.x; idx < lim; idx += gridDim.x * kSortThreads) {
         const uint32_t k = keys[idx];
-        for (int p = 0; p < passes; ++p) atomicAdd(&h[p * 256 + ((k >> (begin_bit + 8 * p)) & 255u)], 1u);
+        for (int p = 0; p < passes; ++p) atomicAdd(&h[p * R + ((k >> (begin_bit + B * p)) & (R - 1u))], 1u);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < passes * 256; i += kSortThreads)
+    for (int i = threadIdx.x; i < passes * int(R); i += kSortThreads)
         if (h[i]) atomicAdd(&ghist[i], h[i]);
 }
 
 // One pass: ranks a tile's keys by digit (stable), then places them at the
 // digit's global offset + the counts of the digit in earlier tiles + the
-// rank.
+// rank.  Thread t looks after digits t, t + 256, ...
+template <int B>
 __global__ void __launch_bounds__(kSortThreads) k_os_scatter(const uint32_t* __restrict__ kin,
                                                             const uint32_t* __restrict__ vin,
                                                             uint32_t* __restrict__ kout,
@@ -286,7 +290,7 @@ __global__ void __launch_bounds__(kSortThreads) k_os_scatter(const uint32_t* __r
                                                             const uint32_t* n_dev, int shift,
                                                             const uint32_t* __restrict__ ghist, uint32_t* ctl,
                                                             unsigned long long* state, uint32_t* err) {
-    constexpr uint32_t R = 256;
+    constexpr uint32_t R = 1u << B, DPT = R / kSortThreads;   // digits a thread looks after
     __shared__ uint32_t wcount[kSortWarps][R + 1];
     __shared__ uint32_t wofs[kSortWarps][R + 1];
     __shared__ uint32_t base_d[R];
@@ -325,42 +329,59 @@ __global__ void __launch_bounds__(kSortThreads) k_os_scatter(const uint32_t* __r
             rank[r] = base + __popc(peers & lt);
         }
         __syncthreads();
-        // thread d: digit d's warp offsets, tile count, global offset
-        const uint32_t d = threadIdx.x;
-        uint32_t cnt = 0;
-        for (int w = 0; w < kSortWarps; ++w) {
-            wofs[w][d] = cnt;
-            cnt += wcount[w][d];
+        // thread t: digits t * DPT .. t * DPT + DPT - 1 (consecutive, so the
+        // block scan of their totals gives each its global offset)
+        uint32_t cnt[DPT], gtot = 0, gsum[DPT];
+#pragma unroll
+        for (uint32_t e = 0; e < DPT; ++e) {
+            const uint32_t d = threadIdx.x * DPT + e;
+            uint32_t c = 0;
+            for (int w = 0; w < kSortWarps; ++w) {
+                wofs[w][d] = c;
+                c += wcount[w][d];
+            }
+            cnt[e] = c;
+            gsum[e] = gtot;
+            gtot += ghist[d];
         }
         uint32_t gx;
-        block_excl_scan<kSortThreads>(ghist[d], gx, sm_scan);
-        unsigned long long* my = state + size_t(tile) * R + d;
-        os_state_store(my, tag | ((tile == 0 ? 2ull : 1ull) << 32) | cnt);
-        // look-back over kOsLook predecessors at a time (their loads in
-        // flight together): sum tile counts until an inclusive count
-        uint32_t prefix = 0;
-        bool failed = false, found = tile == 0;
-        for (int64_t look = int64_t(tile) - 1; !found && !failed; look -= kOsLook) {
-            unsigned long long st[kOsLook];
+        block_excl_scan<kSortThreads>(gtot, gx, sm_scan);
+        bool failed = false;
 #pragma unroll
-            for (int k = 0; k < kOsLook; ++k)
-                st[k] = look - k >= 0 ? scan_state_load(state + size_t(look - k) * R + d) : (tag | (2ull << 32));
+        for (uint32_t e = 0; e < DPT; ++e) {
+            const uint32_t d = threadIdx.x * DPT + e;
+            unsigned long long* my = state + size_t(tile) * R + d;
+            os_state_store(my, tag | ((tile == 0 ? 2ull : 1ull) << 32) | cnt[e]);
+        }
 #pragma unroll
-            for (int k = 0; k < kOsLook; ++k) {
-                if (found || failed) break;
-                uint32_t spins = 0;
-                while (!((st[k] >> 34) == epoch && ((st[k] >> 32) & 3u) != 0u)) {
-                    if (++spins == kLookbackSpin) { failed = true; break; }
-                    st[k] = scan_state_load(state + size_t(look - k) * R + d);
+        for (uint32_t e = 0; e < DPT; ++e) {
+            const uint32_t d = threadIdx.x * DPT + e;
+            // look-back over kOsLook predecessors at a time (their loads in
+            // flight together): sum tile counts until an inclusive count
+            uint32_t prefix = 0;
+            bool found = tile == 0;
+            for (int64_t look = int64_t(tile) - 1; !found && !failed; look -= kOsLook) {
+                unsigned long long st[kOsLook];
+#pragma unroll
+                for (int k = 0; k < kOsLook; ++k)
+                    st[k] = look - k >= 0 ? scan_state_load(state + size_t(look - k) * R + d) : (tag | (2ull << 32));
+#pragma unroll
+                for (int k = 0; k < kOsLook; ++k) {
+                    if (found || failed) break;
+                    uint32_t spins = 0;
+                    while (!((st[k] >> 34) == epoch && ((st[k] >> 32) & 3u) != 0u)) {
+                        if (++spins == kLookbackSpin) { failed = true; break; }
+                        st[k] = scan_state_load(state + size_t(look - k) * R + d);
+                    }
+                    if (failed) break;
+                    prefix += uint32_t(st[k]);
+                    found = ((st[k] >> 32) & 3u) == 2u;
                 }
-                if (failed) break;
-                prefix += uint32_t(st[k]);
-                found = ((st[k] >> 32) & 3u) == 2u;
             }
+            if (tile != 0) os_state_store(state + size_t(tile) * R + d, tag | (2ull << 32) | (prefix + cnt[e]));
+            base_d[d] = gx + gsum[e] + prefix;
         }
         if (failed && err) atomicOr(err, kErrLogic);
-        if (tile != 0) os_state_store(my, tag | (2ull << 32) | (prefix + cnt));
-        base_d[d] = gx + prefix;
         __syncthreads();
         // a look-back that gave up leaves the offsets unknown: the step
         // reports the error and nothing lands outside the output
@@ -386,6 +407,39 @@ __global__ void __launch_bounds__(kSortThreads) k_os_scatter(const uint32_t* __r
             ctl[2] = 0u;
             __threadfence();
         }
+    }
+}
+
+// The live entries of a sort that ended in the alternate buffers, copied
+// back.
+__global__ void k_copy_live(const uint32_t* __restrict__ ks, const uint32_t* __restrict__ vs, uint32_t* kd,
+                            uint32_t* vd, uint32_t n, const uint32_t* n_dev) {
+    const uint32_t lim = n_dev ? min(n, *n_dev) : n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < lim; i += gridDim.x * blockDim.x) {
+        kd[i] = ks[i];
+        vd[i] = vs[i];
+    }
+}
+
+template <int B>
+void onesweep_sort(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt, uint32_t n_cap,
+                   const uint32_t* n_dev, int begin_bit, int passes, uint32_t ntiles, uint32_t* os_scratch,
+                   cudaStream_t st, uint32_t* err) {
+    uint32_t* ghist = os_scratch + kOsHeader;
+    auto* state = reinterpret_cast<unsigned long long*>(os_scratch + kOsHeader + kOsHist);
+    cudaMemsetAsync(ghist, 0, size_t(passes) * (1u << B) * 4, st);
+    k_os_hist<B><<<ntiles < 296u ? ntiles : 296u, kSortThreads, 0, st>>>(keys, n_cap, n_dev, begin_bit, passes,
+                                                                         ghist);
+    uint32_t *ki = keys, *vi = vals, *ko = keys_alt, *vo = vals_alt;
+    for (int p = 0; p < passes; ++p) {
+        k_os_scatter<B><<<ntiles, kSortThreads, 0, st>>>(ki, vi, ko, vo, n_cap, n_dev, begin_bit + B * p,
+                                                          ghist + (1u << B) * p, os_scratch, state, err);
+        uint32_t* t = ki; ki = ko; ko = t;
+        t = vi; vi = vo; vo = t;
+    }
+    if (passes & 1) {
+        const uint32_t nb = (n_cap + 255) / 256;
+        k_copy_live<<<nb < 1184u ? nb : 1184u, 256, 0, st>>>(ki, vi, keys, vals, n_cap, n_dev);
     }
 }
 
@@ -423,7 +477,7 @@ void scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, const uint32_
 
 size_t onesweep_words(uint32_t n_cap) {
     const size_t ntiles = (size_t(n_cap) + kSortTile - 1) / kSortTile;
-    return kOsHeader + kOsHist + 2 * 256 * ntiles;
+    return kOsHeader + kOsHist + 2 * size_t(kOsMaxDigits) * ntiles;
 }
 
 size_t radix_hist_words(uint32_t n_cap) {
@@ -446,32 +500,19 @@ void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32
     const uint32_t ntiles = (n_cap + kSortTile - 1) / kSortTile;
     if (ntiles == 0) return;
     const int B = digit_bits >= 8 && digit_bits <= kRadixMaxBits ? digit_bits : 8;
-    const int os_passes = (end_bit - begin_bit + 7) / 8;
+    // one-sweep passes: 8- or 9-bit digits, whichever needs fewer passes
+    const int width = end_bit - begin_bit;
+    const int os_b = (width + 8) / 9 < (width + 7) / 8 ? 9 : 8;
+    const int os_passes = (width + os_b - 1) / os_b;
     if (B == 8 && os_scratch && os_passes <= kOsMaxPasses) {
         if (onesweep_words(n_cap) > os_words) {   // never: the world sizes the scratch for its largest sort
             if (err) cudaMemsetAsync(err, 0xff, 4, st);
             return;
         }
-        uint32_t* ghist = os_scratch + kOsHeader;
-        auto* state = reinterpret_cast<unsigned long long*>(os_scratch + kOsHeader + kOsHist);
-        cudaMemsetAsync(ghist, 0, size_t(os_passes) * 256 * 4, st);
-        k_os_hist<<<ntiles < 296u ? ntiles : 296u, kSortThreads, 0, st>>>(keys, n_cap, n_dev, begin_bit, os_passes,
-                                                                          ghist);
-        uint32_t *ki = keys, *vi = vals, *ko = keys_alt, *vo = vals_alt;
-        for (int p = 0; p < os_passes; ++p) {
-            k_os_scatter<<<ntiles, kSortThreads, 0, st>>>(ki, vi, ko, vo, n_cap, n_dev, begin_bit + 8 * p,
-                                                           ghist + 256 * p, os_scratch, state, err);
-            uint32_t* t = ki; ki = ko; ko = t;
-            t = vi; vi = vo; vo = t;
-        }
-        if (os_passes & 1) {
-            cudaMemcpyAsync(keys, ki, size_t(n_cap) * 4, cudaMemcpyDeviceToDevice, st);
-            cudaMemcpyAsync(vals, vi, size_t(n_cap) * 4, cudaMemcpyDeviceToDevice, st);
-        }
-        return;
-    }
-    if ((size_t(1) << B) * ntiles > hist_words) {   // never: the world sizes the histogram for the widest digit
-        if (err) cudaMemsetAsync(err, 0xff, 4, st);
+        if (os_b == 9) onesweep_sort<9>(keys, vals, keys_alt, vals_alt, n_cap, n_dev, begin_bit, os_passes, ntiles,
+                                        os_scratch, st, err);
+        else onesweep_sort<8>(keys, vals, keys_alt, vals_alt, n_cap, n_dev, begin_bit, os_passes, ntiles,
+                              os_scratch, st, err);
         return;
     }
     uint32_t *ki = keys, *vi = vals, *ko = keys_alt, *vo = vals_alt;
