@@ -412,6 +412,16 @@ __device__ __forceinline__ int32_t find_key(const uint64_t* keys, uint32_t lo, u
     return (lo < end && keys[lo] == key) ? int32_t(lo) : -1;
 }
 
+// Per shape, before the sweep: its bucket count starts at its plane pairs,
+// its fill cursor at zero, and its previous-generation bucket empty.
+__global__ void k_owner_init(DevState s) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.n_shapes) return;
+    s.own_cnt[i] = s.s_static_pairs[i];
+    s.own_cur[i] = 0u;
+    s.prev_bkt[i] = make_uint2(0u, 0u);
+}
+
 // Each generation's keys are sorted by (owner, partner), owners being
 // contiguous buckets: the previous generation's bucket of every owner
 // (start, end; both zero for an owner without pairs), so that matching
@@ -484,8 +494,7 @@ void enqueue_broadphase(const DevState& s, cudaStream_t st, const StageHook& hoo
                          s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err, 8, s.sort_os, s.sort_os_words);
         k_band_gather<<<(s.bx_cap + T - 1) / T, T, 0, st>>>(s, rec, meta);
     }
-    cudaMemcpyAsync(s.own_cnt, s.s_static_pairs, size_t(s.n_shapes) * 4, cudaMemcpyDeviceToDevice, st);
-    cudaMemsetAsync(s.own_cur, 0, size_t(s.n_shapes) * 4, st);
+    if (s.n_shapes) k_owner_init<<<(s.n_shapes + T - 1) / T, T, 0, st>>>(s);
     const uint32_t sweep_threads = kSweepWarps * 32;
     const uint32_t n_sweep = s.n_finite + s.bx_cap;
     const uint32_t sweep_blocks = s.n_finite ? (n_sweep + sweep_threads - 1) / sweep_threads : 0;
@@ -495,7 +504,6 @@ void enqueue_broadphase(const DevState& s, cudaStream_t st, const StageHook& hoo
     if (sweep_blocks) k_sweep<<<sweep_blocks, sweep_threads, 0, st>>>(s, rec, meta, 1);
     k_owner_sort<<<(s.n_shapes + T - 1) / T, T, 0, st>>>(s);
     const uint32_t mb = (s.pair_cap + T - 1) / T;
-    cudaMemsetAsync(s.prev_bkt, 0, size_t(s.n_shapes) * sizeof(uint2), st);
     k_prev_buckets<<<mb < 1184 ? mb : 1184, T, 0, st>>>(s);
     k_pair_match<<<mb < 1184 ? mb : 1184, T, 0, st>>>(s);
 }
