@@ -26,58 +26,11 @@
 //              shared memory, then an exclusive scan across the 8 warps.
 // Counts may live in device memory (n_dev) so the sort can follow a
 // data-dependent producer inside one captured CUDA graph.
-#include "state.h"
+#include "lookback.cuh"
 
 namespace fyzz::b200 {
 namespace {
 
-constexpr int kScanThreads = 256;
-constexpr int kScanItems = 8;
-constexpr int kScanTile = kScanThreads * kScanItems;
-
-__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v += t;
-    }
-    return v;
-}
-
-// Exclusive block scan of one value per thread; returns the block total.
-template <int THREADS>
-__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t& excl, uint32_t* smem) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t inc = warp_incl_scan(v);
-    if (lane == 31) smem[warp] = inc;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t w = lane < THREADS / 32 ? smem[lane] : 0u;
-        const uint32_t wi = warp_incl_scan(w);
-        if (lane < THREADS / 32) smem[lane] = wi - w;
-        if (lane == THREADS / 32 - 1) smem[THREADS / 32] = wi;
-    }
-    __syncthreads();
-    excl = inc - v + smem[warp];
-    const uint32_t total = smem[THREADS / 32];
-    __syncthreads();
-    return total;
-}
-
-// Scan scratch: [0] epoch, [1] tile ticket, [2] finished blocks, [3] pad,
-// then one 64-bit state per tile: epoch (30 bits) | status (2 bits: 1 sum
-// of the tile, 2 inclusive prefix) | value (32 bits).
-constexpr uint32_t kScanHeader = 4;
-constexpr uint32_t kLookbackSpin = 1u << 18;
-__device__ __forceinline__ unsigned long long scan_state_load(const unsigned long long* p) {
-    unsigned long long v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void scan_state_store(unsigned long long* p, unsigned long long v) {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
 // A one-sweep digit state carries all its data in the word: no ordering
 // against other stores is needed.
 __device__ __forceinline__ void os_state_store(unsigned long long* p, unsigned long long v) {

@@ -24,6 +24,7 @@
 // islands) per island, sweeping its partitions in order with warp / block
 // barriers only: no grid-wide synchronisation and no host round trip.
 #include "solver_common.cuh"
+#include "lookback.cuh"
 #include <cfloat>
 #include <type_traits>
 
@@ -127,24 +128,25 @@ __global__ void k_bodies_velocity(DevState s) {
 }
 
 __device__ void sleep_pair(const DevState& s, uint32_t k, bool touch);
-// Touch flags of the current pairs; with sleeping on, also each pair's
-// counted interactions and activations (sleep_pair).
-__global__ void k_touch_flags(DevState s, uint32_t* flags) {
-    const uint32_t n = *s.cur.n;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-        const bool touch = s.cur.count[k] > 0u;
-        flags[k] = touch ? 1u : 0u;
-        if (s.sleep) sleep_pair(s, k, touch);
-    }
-}
-__global__ void k_touch_scatter(DevState s, const uint32_t* flags, const uint32_t* pos) {
-    const uint32_t n = *s.cur.n;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
-        if (flags[k]) s.man_list[pos[k]] = k;
-    if (blockIdx.x == 0 && threadIdx.x == 0)
-        s.counters[kCntDesc] = s.n_joints + s.counters[kCntMan];
+// Touching managers in canonical pair order, in one pass: each tile flags
+// its pairs as touching (with sleeping on, also each pair's counted
+// interactions and activations, sleep_pair), scans the flags and writes the
+// touching pairs' indices; the last tile sets the manager and descriptor
+// counts.
+__global__ void __launch_bounds__(kScanThreads) k_touch_compact(DevState s) {
+    const uint32_t n = min(*s.cur.n, s.pair_cap);
+    compact_tiles(
+        n, s.scan_tmp, s.err,
+        [&](uint32_t k) {
+            const bool touch = s.cur.count[k] > 0u;
+            if (s.sleep) sleep_pair(s, k, touch);
+            return touch;
+        },
+        [&](uint32_t k, uint32_t at) { s.man_list[at] = k; },
+        [&](uint32_t total) {
+            s.counters[kCntMan] = total;
+            s.counters[kCntDesc] = s.n_joints + total;
+        });
 }
 
 // Lock-free union-find after ECL-CC (Jaiganesh and Burtscher, "A
@@ -426,21 +428,21 @@ __global__ void k_sleep_decide(DevState s) {
     s.b_sacc[2 * size_t(b)] = z;
     s.b_sacc[2 * size_t(b) + 1] = z;
 }
-__global__ void k_island_flags(DevState s) {
-    const uint32_t n = s.counters[kCntAwake];
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-        s.isl_flag[i] = (i == 0 || s.d_key[i] != s.d_key[i - 1]) ? 1u : 0u;
-}
-__global__ void k_island_scatter(DevState s, const uint32_t* pos) {
-    const uint32_t n = s.counters[kCntAwake];
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-        if (s.isl_flag[i]) s.isl_begin[pos[i]] = i;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        const uint32_t ni = *s.n_isl;
-        s.isl_begin[ni] = n;
-    }
+// Island starts in one pass: a descriptor whose key differs from its
+// predecessor's opens an island (descriptors sorted by island root); the
+// last tile sets the island count, the end sentinel, and clears the
+// island-class list counters that k_island_classes fills next.
+__global__ void __launch_bounds__(kScanThreads) k_island_compact(DevState s) {
+    const uint32_t n = min(s.counters[kCntAwake], s.desc_cap);
+    compact_tiles(
+        n, s.scan_tmp, s.err, [&](uint32_t i) { return i == 0 || s.d_key[i] != s.d_key[i - 1]; },
+        [&](uint32_t i, uint32_t at) { s.isl_begin[at] = i; },
+        [&](uint32_t total) {
+            *s.n_isl = total;
+            s.isl_begin[total] = n;
+            for (int c = 0; c < 4; ++c) s.counters[kCntList + c] = 0u;
+            for (int c = 0; c < 5; ++c) s.counters[kCntList4 + c] = 0u;   // lists 4-5, work-queue tickets
+        });
 }
 
 // Size classes of the islands (lists consumed by the partition and PGS
@@ -2184,8 +2186,6 @@ void init_solver_kernels() {
 }
 
 void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, const Branches* br) {
-    uint32_t* flags = s.tmp_flags;
-    uint32_t* pos = s.tmp_pos;
     uint32_t* lvl_bound = s.lvl_bound;
     const uint32_t T = s.elem_block;   // elementwise kernels (at most 56 registers, no launch bounds)
     const uint32_t cap_blocks = 148u * 8u;
@@ -2197,9 +2197,7 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     cudaMemsetAsync(s.counters + kCntActivating, 0, sizeof(uint32_t), st);
     k_bodies_begin<<<grid_for(s.n_bodies, T, 1u << 30), T, 0, st>>>(s);
     // touching managers in canonical pair order
-    k_touch_flags<<<grid_for(s.pair_cap, T, cap_blocks), T, 0, st>>>(s, flags);
-    scan_exclusive(flags, pos, s.pair_cap, s.cur.n, s.counters + kCntMan, s.scan_tmp, s.scan_tmp_words, st, s.err);
-    k_touch_scatter<<<grid_for(s.pair_cap, T, cap_blocks), T, 0, st>>>(s, flags, pos);
+    k_touch_compact<<<lookback_grid(s.pair_cap), kScanThreads, 0, st>>>(s);
     // islands
     k_desc_bodies<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     k_union<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
@@ -2228,12 +2226,7 @@ void enqueue_solver(const DevState& s, cudaStream_t st, const StageHook& hook, c
     while ((1ull << bits) < uint64_t(s.n_bodies) + 1u) ++bits;
     radix_sort_pairs(s.d_key, s.d_val, s.d_key2, s.d_val2, s.desc_cap, s.counters + kCntDesc, 0, bits,
                      s.sort_hist, s.sort_hist_words, s.scan_tmp, s.scan_tmp_words, st, s.err, s.radix_bits, s.sort_os, s.sort_os_words);
-    k_island_flags<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
-    scan_exclusive(s.isl_flag, pos, s.desc_cap, s.counters + kCntAwake, s.n_isl, s.scan_tmp, s.scan_tmp_words, st,
-                   s.err);
-    k_island_scatter<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s, pos);
-    cudaMemsetAsync(s.counters + kCntList, 0, 4 * sizeof(uint32_t), st);
-    cudaMemsetAsync(s.counters + kCntList4, 0, 5 * sizeof(uint32_t), st);   // lists 4-5, work-queue tickets
+    k_island_compact<<<lookback_grid(s.desc_cap), kScanThreads, 0, st>>>(s);
     k_island_classes<<<grid_for(s.desc_cap, T, cap_blocks), T, 0, st>>>(s);
     // partitions by island size class, and row preparation: independent
     hook(kStPrep, st);

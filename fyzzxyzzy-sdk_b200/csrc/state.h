@@ -159,7 +159,6 @@ struct DevState {
     uint32_t *d_key = nullptr, *d_val = nullptr, *d_key2 = nullptr, *d_val2 = nullptr;
     uint32_t* d_level = nullptr;
     uint32_t *isl_begin = nullptr, *isl_end = nullptr, *n_isl = nullptr;
-    uint32_t* isl_flag = nullptr;
     uint32_t* sb_mask = nullptr;       // partition masks per body
     uint32_t* sb_maxdyn = nullptr;
     uint32_t* sb_static = nullptr;

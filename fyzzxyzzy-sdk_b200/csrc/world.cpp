@@ -1811,7 +1811,6 @@ private:
             dalloc(d_.isl_list[k], size_t(dc) / (kListMinDesc[k] + 1) + 2, pair_owned_);
         dalloc(d_.isl_begin, size_t(dc) + 1, pair_owned_);
         dalloc(d_.isl_end, size_t(dc) + 1, pair_owned_);
-        dalloc(d_.isl_flag, dc, pair_owned_);
         dalloc(d_.tmp_flags, cap, pair_owned_);
         dalloc(d_.tmp_pos, std::max(cap, dc), pair_owned_);
         dalloc(d_.lvl_bound, 2 * size_t(dc) + 2, pair_owned_);
