@@ -3,9 +3,12 @@ of fyzz_b200_rollout_backward, never part of the product).
 
 An independent restatement, in torch float64 with autograd, of the
 differentiable model the adjoint kernels implement: the rigid-body step
-(pre-integration, sqrt-inverse-inertia tensor, contact / friction / distance
-rows, 4 + 1 Gauss-Seidel passes in partition order, integration; reference
-src/native/scene.cpp:114-143, 7490-8510, 8853-9148, 10383-10707) with its
+(pre-integration, sqrt-inverse-inertia tensor, contact / friction / joint
+rows -- centre and anchored distance, fixed, spherical, revolute and
+prismatic joints, their rows orthogonalised in the inverse-mass metric --,
+4 + 1 Gauss-Seidel passes in partition order, integration; reference
+src/native/scene.cpp:114-143, 7490-8510, 7615-7767, 8853-9148,
+10383-10707) with its
 discrete structure frozen from a recorded forward run of the B200 world:
 touching managers and their contact points, friction anchors (carried ones
 body-local, ones taken from the step's own contact points at those points),
@@ -110,12 +113,18 @@ class Model:
 
     bodies: per world body, dynamic flag, inverse mass, inverse principal
     inertia, mass-frame offset u of the body origin (for joint anchors),
-    damping; shapes: owning body, restitution, rest offset; joints: (a, b,
-    rest length) in the step's canonical order."""
+    damping; shapes: owning body, restitution, rest offset; joints: in the
+    step's canonical order, (a, b, rest length) for a centre distance joint
+    or (a, b, rest length, kind, local frame a (7), local frame b (7)) for
+    the other kinds (kind numbers of scenes.JOINT_*)."""
 
     def __init__(self, dynamic, inv_mass, inv_inertia, origin_offset, shape_body, restitution,
-                 rest_offset, joints, lin_damp=0.0, ang_damp=0.05):
+                 rest_offset, joints, lin_damp=0.0, ang_damp=0.05, mass_local_q=None):
         self.dyn = np.asarray(dynamic, bool)
+        # per body, the mass frame's orientation in the body frame (body
+        # orientation = mass-frame orientation * conj(mass_local_q))
+        self.mlq = (np.tile([0.0, 0.0, 0.0, 1.0], (len(self.dyn), 1)) if mass_local_q is None
+                    else np.asarray(mass_local_q, np.float64))
         self.im0 = np.asarray(inv_mass, np.float64)
         self.iI0 = np.asarray(inv_inertia, np.float64)
         self.u = np.asarray(origin_offset, np.float64)
@@ -165,8 +174,14 @@ class Model:
         # ---- rows
         nj = len(self.joints)
         desc = []
-        for (a, b, length) in self.joints:
-            desc.append(("joint",) + self._joint_row(a, b, length, c, q, v1, w1, C, im, dt))
+        for jt in self.joints:
+            a, b, length = jt[0], jt[1], jt[2]
+            if len(jt) == 3 or jt[3] == 0:
+                row = self._joint_row(a, b, length, c, q, v1, w1, C, im, dt)
+                desc.append(("joint", row[0], row[1], [row[2:]]))
+            else:
+                desc.append(("joint",) + self._frame_joint_rows(a, b, length, jt[3], jt[4], jt[5], c, q, v1, w1,
+                                                                C, im, dt))
         for k in range(len(rec.pairs)):
             desc.append(("contact",) + self._contact_rows(rec, k, c, q, v1, w1, C, im, mu_s, mu_d, dt))
         # ---- Gauss-Seidel in partition order, islands independent
@@ -175,7 +190,7 @@ class Model:
         dw = [zero3] * nb
         applied = [None] * len(desc)
         for d, item in enumerate(desc):
-            applied[d] = [_t(0.0)] * (1 if item[0] == "joint" else 8)
+            applied[d] = [_t(0.0)] * (len(item[3]) if item[0] == "joint" else 8)
         pos, passes = 4, 5
         dvm = dwm = None
         for it in range(passes):
@@ -198,7 +213,8 @@ class Model:
     def _order(self, rec, nj):
         """Descriptors island by island, partitions ascending."""
         bodies = []
-        for (a, b, _) in self.joints:
+        for jt in self.joints:
+            a, b = jt[0], jt[1]
             bodies.append((a if self.dyn[a] else -1, b if self.dyn[b] else -1))
         for (sa, sb) in rec.pairs:
             ba, bb = self.shape_body[sa], self.shape_body[sb]
@@ -234,6 +250,89 @@ class Model:
         err = dist - length
         return (a if da else -1, b if db else -1, axis, ja, jb, im[a], im[b], -rcp,
                 -rcp * (err / dt + speed), -rcp * speed)
+
+    def _frame_joint_rows(self, a, b, length, kind, la, lb, c, q, v1, w1, C, im, dt):
+        """Rows of an anchored distance, fixed, spherical, revolute or
+        prismatic joint (scene.cpp:7615-7767): anchors and frames from the
+        bodies' poses, translation locked along frame A's axes (prismatic:
+        not X), rotation through the relative quaternion's vector part
+        (spherical: none; revolute: not X), each row orthogonalised against
+        the earlier ones in the inverse-mass metric."""
+        da, db = self.dyn[a], self.dyn[b]
+        zero3 = _t([0.0, 0.0, 0.0])
+        qa0 = qmul(q[a], conj(_t(self.mlq[a])))
+        qb0 = qmul(q[b], conj(_t(self.mlq[b])))
+        pa0 = c[a] - rot(q[a], _t(self.u[a]))
+        pb0 = c[b] - rot(q[b], _t(self.u[b]))
+        la, lb = np.asarray(la, np.float64), np.asarray(lb, np.float64)
+        world0 = pa0 + rot(qa0, _t(la[:3]))
+        world1 = pb0 + rot(qb0, _t(lb[:3]))
+        ra, rb = world0 - c[a], world1 - c[b]
+        m0 = im[a] if da else _t(0.0)
+        m1 = im[b] if db else _t(0.0)
+        rel = v1[a] - v1[b]
+        wa, wb = w1[a], w1[b]
+        rows = []
+
+        def emit(axis, a0, a1, ja, jb, error, response):
+            rcp = 1.0 / response
+            speed = (axis * rel).sum() + (a0 * wa).sum() - (a1 * wb).sum()
+            rows.append((axis, ja, jb, m0, m1, -rcp, -rcp * (error / dt + speed), -rcp * speed))
+
+        if kind == 1:   # anchored distance: one row along the anchors' separation
+            off = world0 - world1
+            dist = torch.sqrt((off * off).sum())
+            axis = off / dist if _f(dist) >= 1.192092896e-07 else _t([1.0, 0.0, 0.0])
+            an0, an1 = cross(ra, axis), cross(rb, axis)
+            ja = C[a] @ an0 if da else zero3
+            jb = C[b] @ an1 if db else zero3
+            emit(axis, an0, an1, ja, jb, dist - length, m0 + m1 + (ja * ja).sum() + (jb * jb).sum())
+            return (a if da else -1, b if db else -1, rows)
+        qa = qmul(qa0, _t(la[3:7]))
+        error_p = rotinv(qa, world0 - world1)
+        ea = va = vb = cc = zero3
+        dd = overlap = _t(0.0)
+        if kind != 3:   # not spherical
+            qb = qmul(qb0, _t(lb[3:7]))
+            if _f((qa * qb).sum()) < 0.0:
+                qb = -qb
+            eq = qmul(conj(qa), qb)
+            ea, va, vb = eq[:3], qa[:3], qb[:3]
+            dd = qa[3] * qb[3] - (va * vb).sum()
+            overlap = qa[3] * qb[3] + (va * vb).sum()
+            cc = qa[3] * vb + qb[3] * va
+        errors = [error_p[0], error_p[1], error_p[2], -ea[0], -ea[1], -ea[2]]
+        diag = [torch.stack([dd, cc[2], -cc[1]]), torch.stack([-cc[2], dd, cc[0]]), torch.stack([cc[1], -cc[0], dd])]
+        count = {2: 6, 3: 3, 4: 5, 5: 5}[kind]
+        done = []   # (lin, a0, a1, ja, jb, err, inv) of the rows so far
+        for k in range(count):
+            comp = k + (1 if kind == 5 else 0) + (1 if kind == 4 and k >= 3 else 0)
+            err = errors[comp]
+            if comp < 3:
+                basis = _t([1.0 if comp == i else 0.0 for i in range(3)])
+                lin = rot(qa, basis)
+                arm = (world1 - c[a]) if kind == 5 else ra
+                a0, a1 = cross(arm, lin), cross(rb, lin)
+            else:
+                qq = comp - 3
+                lin = zero3
+                a0 = 0.5 * (va * vb[qq] + vb * va[qq] + diag[qq])
+                if _f(overlap) == 0.0:
+                    # the relative quaternion's Jacobian is singular at 180 degrees
+                    a0 = a0 + _t([1.0 if qq == i else 0.0 for i in range(3)]) * 1.1920928955078125e-07
+                a1 = a0
+            ja = C[a] @ a0 if da else zero3
+            jb = C[b] @ a1 if db else zero3
+            for (flin, fa0, fa1, fja, fjb, ferr, finv) in done:
+                t = ((m0 + m1) * (lin * flin).sum() + (ja * fja).sum() + (jb * fjb).sum()) * finv
+                lin, a0, a1 = lin - flin * t, a0 - fa0 * t, a1 - fa1 * t
+                ja, jb = ja - fja * t, jb - fjb * t
+                err = err - ferr * t
+            response = (m0 + m1) * (lin * lin).sum() + (ja * ja).sum() + (jb * jb).sum()
+            inv = 1.0 / response if _f(response) > 0.0 else _t(0.0)
+            done.append((lin, a0, a1, ja, jb, err, inv))
+            emit(lin, a0, a1, ja, jb, err, response)
+        return (a if da else -1, b if db else -1, rows)
 
     def _contact_rows(self, rec, k, c, q, v1, w1, C, im, mu_s, mu_d, dt):
         sa, sb = (int(x) for x in rec.pairs[k])
@@ -320,17 +419,20 @@ class Model:
         def get(b):
             return (dv[b], dw[b]) if b >= 0 else (zero3, zero3)
         if item[0] == "joint":
-            _, a, b, axis, ja, jb, ima, imb, vm, const, unb = item
+            _, a, b, rows = item
             av, aw = get(a)
             bv, bw = get(b)
-            nd = (axis * (av - bv)).sum() + (ja * aw).sum() - (jb * bw).sum()
-            nx = applied[0] + nd * vm + (const if it < pos else unb)
-            dl = nx - applied[0]
-            applied[0] = nx
+            for r, (axis, ja, jb, ima, imb, vm, const, unb) in enumerate(rows):
+                nd = (axis * (av - bv)).sum() + (ja * aw).sum() - (jb * bw).sum()
+                nx = applied[r] + nd * vm + (const if it < pos else unb)
+                dl = nx - applied[r]
+                applied[r] = nx
+                av = av + axis * (dl * ima); aw = aw + ja * dl
+                bv = bv - axis * (dl * imb); bw = bw - jb * dl
             if a >= 0:
-                dv[a] = av + axis * (dl * ima); dw[a] = aw + ja * dl
+                dv[a], dw[a] = av, aw
             if b >= 0:
-                dv[b] = bv - axis * (dl * imb); dw[b] = bw - jb * dl
+                dv[b], dw[b] = bv, bw
             return
         _, a, b, rows, frows, K, sf, df, ima, imb = item
         av, aw = get(a)
@@ -388,6 +490,27 @@ def model_for(pkg_world, spec):
     if spec.floor is not None:
         shape_body = np.concatenate([[0], shape_body])
         rest = np.concatenate([[spec.floor_mat[2]], rest])
-    joints = [(int(a) + first, int(b) + first, float(d)) for (a, b), d in zip(spec.joints, spec.joint_dist)]
-    joints = joints[::-1]   # canonical order: constraint slot descending
-    return Model(dyn, im, iI, u, shape_body, rest, np.zeros(len(shape_body)), joints)
+    mlq = np.tile([0.0, 0.0, 0.0, 1.0], (nb, 1))
+    for i in range(first, nb):
+        mlq[i] = pkg_world.body_mass_properties(i)[7:11]
+    return Model(dyn, im, iI, u, shape_body, rest, np.zeros(len(shape_body)), spec_joints(spec),
+                 mass_local_q=mlq)
+
+
+def spec_joints(spec):
+    """The model's joints of a SceneSpec, in the step's canonical order
+    (constraint slot descending); FLOOR_BODY endpoints are the floor actor."""
+    first = 1 if spec.floor is not None else 0
+    kinds = spec.joint_kinds()
+    local = spec.joint_locals()
+
+    def actor(i):
+        return 0 if int(i) == 0xFFFFFFFF else int(i) + first
+    joints = []
+    for j, ((a, b), d) in enumerate(zip(spec.joints, spec.joint_dist)):
+        if int(kinds[j]) == 0:
+            joints.append((actor(a), actor(b), float(d)))
+        else:
+            joints.append((actor(a), actor(b), float(d), int(kinds[j]), local[j, :7].astype(np.float64),
+                           local[j, 7:].astype(np.float64)))
+    return joints[::-1]
